@@ -1,0 +1,119 @@
+"""ctypes bindings of libcamp_b200.so (the C ABI in include/camp_b200.h).
+
+The library is built in-tree by ``camp_b200.build``.  There is no fallback:
+if the shared library is missing or cannot be loaded, importing the solver
+raises, so nothing can silently run on the CPU instead of the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libcamp_b200.so")
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+class CellStats(C.Structure):
+    _fields_ = [
+        ("status", C.c_int),
+        ("nst", C.c_int),
+        ("nfe", C.c_int),
+        ("nsetups", C.c_int),
+        ("netf", C.c_int),
+        ("nni", C.c_int),
+        ("ncfn", C.c_int),
+        ("nje", C.c_int),
+        ("hu", C.c_double),
+        ("hcur", C.c_double),
+    ]
+
+
+# every function include/camp_b200.h declares, for the export check
+EXPORTED = [
+    "solver_new", "solver_initialize", "solver_run", "solver_get_statistics",
+    "solver_reset_timers", "solver_free", "solver_free_update_data",
+    "solver_set_debug_out", "solver_set_eval_jac", "rxn_add_condensed_data",
+    "rxn_update_data", "rxn_print_data", "rxn_free_update_data",
+    "rxn_photolysis_create_rate_update_data", "rxn_photolysis_set_rate_update_data",
+    "aero_phase_add_condensed_data", "aero_rep_add_condensed_data", "aero_rep_update_data",
+    "sub_model_add_condensed_data", "sub_model_update_data", "aero_phase_print_data",
+    "aero_rep_print_data", "sub_model_print_data",
+    "camp_b200_last_error", "camp_b200_is_ready", "camp_b200_set_precision",
+    "camp_b200_set_launch", "camp_b200_set_cost_ordering", "camp_b200_run_device",
+    "camp_b200_launch_device", "camp_b200_sync_status", "camp_b200_n_photo",
+    "camp_b200_set_photo_rates", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
+    "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
+    "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
+    "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
+    "camp_b200_eval_jac",
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the library (raising if it is absent) and declares signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m camp_b200.build` "
+            "(the solver has no CPU fallback)"
+        )
+    lib = C.CDLL(path)
+    vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+    lib.solver_new.restype = vp
+    lib.solver_new.argtypes = [ip, ip, _i32p] + [ip] * 15
+    lib.solver_initialize.argtypes = [vp, _f64p, dp, ip, ip]
+    lib.solver_run.restype = ip
+    lib.solver_run.argtypes = [vp, _f64p, _f64p, dp, dp]
+    lib.solver_get_statistics.argtypes = [vp] + [C.POINTER(C.c_int)] * 9 + [C.POINTER(C.c_double)] * 2 + [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)] * 3
+    lib.solver_free.argtypes = [vp]
+    lib.solver_free_update_data.argtypes = [vp]
+    lib.rxn_add_condensed_data.argtypes = [ip, ip, ip, ip, _i32p, _f64p, vp]
+    lib.rxn_update_data.argtypes = [ip, C.POINTER(C.c_int), ip, vp, vp]
+    lib.rxn_photolysis_create_rate_update_data.restype = vp
+    lib.rxn_photolysis_set_rate_update_data.argtypes = [vp, ip, dp]
+    lib.camp_b200_last_error.restype = C.c_char_p
+    lib.camp_b200_is_ready.restype = ip
+    lib.camp_b200_is_ready.argtypes = [vp]
+    lib.camp_b200_set_precision.argtypes = [vp, ip]
+    lib.camp_b200_set_launch.argtypes = [vp, ip, ip]
+    lib.camp_b200_set_cost_ordering.argtypes = [vp, ip]
+    lib.camp_b200_run_device.restype = ip
+    lib.camp_b200_run_device.argtypes = [vp, vp, vp, ip, dp, dp, vp]
+    lib.camp_b200_launch_device.restype = ip
+    lib.camp_b200_launch_device.argtypes = [vp, vp, vp, ip, dp, dp, vp]
+    lib.camp_b200_sync_status.restype = ip
+    lib.camp_b200_sync_status.argtypes = [vp, vp]
+    lib.camp_b200_n_photo.restype = ip
+    lib.camp_b200_n_photo.argtypes = [vp]
+    lib.camp_b200_set_photo_rates.argtypes = [vp, _f64p, ip]
+    lib.camp_b200_get_cell_stats.restype = ip
+    lib.camp_b200_get_cell_stats.argtypes = [vp, C.POINTER(CellStats), ip]
+    lib.camp_b200_kernel_launches.restype = C.c_long
+    lib.camp_b200_kernel_launches.argtypes = [vp]
+    lib.camp_b200_last_kernel_ms.restype = dp
+    lib.camp_b200_last_kernel_ms.argtypes = [vp]
+    for name in ("camp_b200_n_dep_var", "camp_b200_n_jac_elem", "camp_b200_n_lu_elem",
+                 "camp_b200_rxn_int_data_size"):
+        getattr(lib, name).restype = ip
+        getattr(lib, name).argtypes = [vp]
+    lib.camp_b200_get_solver_jac.argtypes = [vp, _i32p, _i32p]
+    lib.camp_b200_get_rxn_int_data.argtypes = [vp, _i32p]
+    lib.camp_b200_get_lu_order.argtypes = [vp, _i32p]
+    lib.camp_b200_eval_deriv.restype = ip
+    lib.camp_b200_eval_deriv.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p, _f64p]
+    lib.camp_b200_eval_jac.restype = ip
+    lib.camp_b200_eval_jac.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p]
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().camp_b200_last_error().decode()

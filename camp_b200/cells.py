@@ -1,0 +1,96 @@
+"""Seeded synthetic cell states for the benchmark and parity workloads.
+
+Per-cell inputs follow the documented workload distributions:
+
+* temperature uniform 260-310 K, pressure uniform 5e4-1.013e5 Pa;
+* photolysis base rates = a fixed base set x one per-cell factor uniform in
+  [0, 1] (the day/night stiffness spread).  The cb05cl_ae5 base set is the
+  reference cb05 test's 1e-4 s^-1 for every photolysis reaction except jo2,
+  which is 0 (``test/chemistry/cb05cl_ae5/test_cb05cl_ae5.F90:349-362``);
+* initial concentrations of variable species log-uniform in
+  [conc_lo, conc_hi] ppm; constant species keep their "init conc" value.
+
+The generator is numpy ``PCG64`` with an explicit seed.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .mechanism import CHEM_SPEC_VARIABLE, RXN_PHOTOLYSIS, Mechanism
+
+
+@dataclass
+class CellBatch:
+    state: np.ndarray  # [n_cells, n_state_var] float64
+    env: np.ndarray  # [n_cells, 2] (T K, P Pa)
+    photo_rates: np.ndarray  # [n_cells, n_photo] base rates for ids 1..n_photo
+    seed: int
+
+    @property
+    def n_cells(self) -> int:
+        return self.state.shape[0]
+
+    def slice(self, a: int, b: int) -> "CellBatch":
+        return CellBatch(self.state[a:b].copy(), self.env[a:b].copy(), self.photo_rates[a:b].copy(), self.seed)
+
+
+def photo_base_rates(mech: Mechanism, base: float = 1.0e-4, zero_labels=("jo2",)) -> np.ndarray:
+    """Base rate per photolysis id (index id-1), 0 for the listed reactions."""
+    n_photo = len(mech.photo_ids)
+    out = np.full(n_photo, base, dtype=np.float64)
+    for pid, ridx in mech.photo_ids.items():
+        if mech.rxns[ridx].label in zero_labels:
+            out[pid - 1] = 0.0
+    return out
+
+
+def make_cells(
+    mech: Mechanism,
+    n_cells: int,
+    seed: int,
+    conc_lo: float = 1.0e-6,
+    conc_hi: float = 1.0e2,
+    photo_base: np.ndarray | None = None,
+    constants: dict[str, float] | None = None,
+) -> CellBatch:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    T = rng.uniform(260.0, 310.0, n_cells)
+    P = rng.uniform(5.0e4, 1.013e5, n_cells)
+    factor = rng.uniform(0.0, 1.0, n_cells)
+    if photo_base is None:
+        photo_base = photo_base_rates(mech)
+    photo = factor[:, None] * np.asarray(photo_base)[None, :]
+    ns = mech.n_state_var
+    state = np.zeros((n_cells, ns))
+    var = mech.var_type == CHEM_SPEC_VARIABLE
+    nvar = int(np.count_nonzero(var))
+    logc = rng.uniform(np.log(conc_lo), np.log(conc_hi), (n_cells, nvar))
+    state[:, var] = np.exp(logc)
+    for i, name in enumerate(mech.species):
+        if var[i]:
+            continue
+        v = None
+        if constants and name in constants:
+            v = constants[name]
+        elif "init conc" in mech.species_props.get(name, {}):
+            v = float(mech.species_props[name]["init conc"])
+        state[:, i] = 0.0 if v is None else v
+    env = np.stack([T, P], axis=1)
+    return CellBatch(state=state, env=env, photo_rates=photo, seed=seed)
+
+
+def constant_values(mech: Mechanism) -> dict[str, float]:
+    """'init conc' of each non-variable species (packed fixtures keep these)."""
+    out = {}
+    for i, name in enumerate(mech.species):
+        if mech.var_type[i] != CHEM_SPEC_VARIABLE:
+            v = mech.species_props.get(name, {}).get("init conc")
+            if v is not None:
+                out[name] = float(v)
+    return out
+
+
+def n_photo(mech: Mechanism) -> int:
+    return sum(1 for r in mech.rxns if r.rxn_type == RXN_PHOTOLYSIS)

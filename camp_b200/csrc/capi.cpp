@@ -1,0 +1,576 @@
+// C ABI of libcamp_b200: the reference's solver entry points plus the
+// camp_b200_* extensions (declared in include/camp_b200.h).
+#include "../../include/camp_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "model.hpp"
+
+using campb::CellStats;
+using campb::Engine;
+using campb::Model;
+using campb::SolveSettings;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) {
+  g_last_error = msg;
+  fprintf(stderr, "camp_b200: %s\n", msg.c_str());
+}
+
+constexpr double kTiny = 1.0e-60;
+
+struct Solver {
+  int n_state = 0, n_cells = 0;
+  std::vector<int> var_type;
+  int n_rxn = 0;
+  std::unique_ptr<Model> model;
+  std::unique_ptr<Engine> engine;
+  // aerosol phases, representations and sub-models (accepted, not solved)
+  int n_aero_phase = 0, n_aero_rep = 0, n_sub_model = 0;
+  int n_aero_phase_added = 0, n_aero_rep_added = 0, n_sub_model_added = 0;
+  bool add_error = false;
+  std::string add_error_msg;
+  // per-cell photolysis base rates [n_cells * n_photo]
+  std::vector<double> photo;
+  int n_photo = 0;
+  SolveSettings settings;
+  std::vector<double> atol_dep;
+  bool ready = false;
+  bool debug_out = false, eval_jac = false;
+  cudaStream_t stream = nullptr;
+  std::vector<CellStats> stats;
+  int last_n = 0;
+  bool cost_order = false;
+  std::vector<int> order;
+
+  int photo_count() const {
+    int c = 0;
+    for (const auto& r : model->rxns())
+      if (r.type == campb::RXN_PHOTOLYSIS) ++c;
+    return c;
+  }
+  void ensure_photo() {
+    int np = photo_count();
+    if (np != n_photo || photo.size() != (size_t)np * n_cells) {
+      std::vector<double> nw((size_t)np * n_cells, 0.0);
+      n_photo = np;
+      photo.swap(nw);
+    }
+  }
+};
+
+Solver* S(void* p) { return static_cast<Solver*>(p); }
+
+bool run_common(Solver* s, double* d_state, const double* d_env, int n_cells,
+                double t0, double t1, cudaStream_t st, bool sync) {
+  std::string err;
+  const double* d_photo = nullptr;
+  if (s->n_photo > 0) {
+    double* dp = s->engine->d_photo_buf(n_cells, &err);
+    if (!dp) {
+      set_error(err);
+      return false;
+    }
+    if (cudaMemcpyAsync(dp, s->photo.data(), sizeof(double) * (size_t)n_cells * s->n_photo,
+                        cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      set_error("photolysis rate upload failed");
+      return false;
+    }
+    d_photo = dp;
+  }
+  const int* d_order = nullptr;
+  if (s->cost_order && s->last_n == n_cells && (int)s->stats.size() >= n_cells) {
+    s->order.resize(n_cells);
+    std::iota(s->order.begin(), s->order.end(), 0);
+    std::stable_sort(s->order.begin(), s->order.end(), [&](int a, int b) {
+      return s->stats[a].nst > s->stats[b].nst;
+    });
+    int* dor = s->engine->d_order_buf(n_cells, &err);
+    if (!dor) {
+      set_error(err);
+      return false;
+    }
+    cudaMemcpyAsync(dor, s->order.data(), sizeof(int) * n_cells, cudaMemcpyHostToDevice, st);
+    d_order = dor;
+  }
+  if (!s->engine->launch_solve(d_state, d_env, d_photo, d_order, n_cells, t0, t1,
+                               s->settings, st, &err)) {
+    set_error(err);
+    return false;
+  }
+  if (sync) {
+    if (!s->engine->fetch_stats(&s->stats, n_cells, st, &err)) {
+      set_error(err);
+      return false;
+    }
+    s->last_n = n_cells;
+  }
+  return true;
+}
+
+int status_of(Solver* s, int n_cells) {
+  for (int c = 0; c < n_cells; ++c)
+    if (s->stats[c].status != 0) return 1;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* solver_new(int n_state_var, int n_cells, int* var_type, int n_rxn,
+                 int n_rxn_int_param, int n_rxn_float_param, int n_rxn_env_param,
+                 int n_aero_phase, int n_aero_phase_int_param,
+                 int n_aero_phase_float_param, int n_aero_rep,
+                 int n_aero_rep_int_param, int n_aero_rep_float_param,
+                 int n_aero_rep_env_param, int n_sub_model,
+                 int n_sub_model_int_param, int n_sub_model_float_param,
+                 int n_sub_model_env_param) {
+  (void)n_aero_phase_int_param;
+  (void)n_aero_phase_float_param;
+  (void)n_aero_rep_int_param;
+  (void)n_aero_rep_float_param;
+  (void)n_aero_rep_env_param;
+  (void)n_sub_model_int_param;
+  (void)n_sub_model_float_param;
+  (void)n_sub_model_env_param;
+  if (n_state_var <= 0 || n_cells <= 0 || !var_type) {
+    set_error("solver_new: invalid sizes");
+    return nullptr;
+  }
+  Solver* s = new Solver;
+  s->n_state = n_state_var;
+  s->n_cells = n_cells;
+  s->var_type.assign(var_type, var_type + n_state_var);
+  s->n_rxn = n_rxn;
+  s->n_aero_phase = n_aero_phase;
+  s->n_aero_rep = n_aero_rep;
+  s->n_sub_model = n_sub_model;
+  s->model.reset(new Model(n_state_var, n_cells, var_type, n_rxn, n_rxn_int_param,
+                           n_rxn_float_param, n_rxn_env_param));
+  return s;
+}
+
+void rxn_add_condensed_data(int rxn_type, int n_int_param, int n_float_param,
+                            int n_env_param, int* int_param, double* float_param,
+                            void* solver_data) {
+  Solver* s = S(solver_data);
+  std::string err;
+  if (!s->model->add_rxn(rxn_type, n_int_param, n_float_param, n_env_param, int_param,
+                         float_param, &err)) {
+    s->add_error = true;
+    if (s->add_error_msg.empty()) s->add_error_msg = err;
+  }
+}
+
+void aero_phase_add_condensed_data(int, int, int*, double*, void* solver_data) {
+  S(solver_data)->n_aero_phase_added++;
+}
+void aero_rep_add_condensed_data(int, int, int, int, int*, double*, void* solver_data) {
+  S(solver_data)->n_aero_rep_added++;
+}
+void sub_model_add_condensed_data(int, int, int, int, int*, double*, void* solver_data) {
+  S(solver_data)->n_sub_model_added++;
+}
+void aero_rep_update_data(int, int*, int, void*, void*) {}
+void sub_model_update_data(int, int*, int, void*, void*) {}
+
+void solver_initialize(void* solver_data, double* abs_tol, double rel_tol, int max_steps,
+                       int max_conv_fails) {
+  Solver* s = S(solver_data);
+  s->ready = false;
+  if (s->add_error) {
+    set_error("solver_initialize: " + s->add_error_msg);
+    return;
+  }
+  if (s->n_aero_phase + s->n_aero_rep + s->n_sub_model > 0) {
+    set_error(
+        "solver_initialize: aerosol phases, aerosol representations and "
+        "sub-models are not supported by this build (gas-phase mechanisms only)");
+    return;
+  }
+  std::string err;
+  if (!s->model->build(&err)) {
+    set_error("solver_initialize: " + err);
+    return;
+  }
+  s->atol_dep.clear();
+  for (int i = 0; i < s->n_state; ++i)
+    if (s->var_type[i] == campb::VAR_VARIABLE) s->atol_dep.push_back(abs_tol[i]);
+  s->settings.rtol = rel_tol;
+  s->settings.max_steps = max_steps;
+  s->settings.max_conv_fails = max_conv_fails;
+  s->ensure_photo();
+  if (!s->stream) {
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error("solver_initialize: no CUDA device available");
+      return;
+    }
+  }
+  s->engine.reset(new Engine);
+  if (!s->engine->init(*s->model, s->atol_dep, s->n_cells, &err)) {
+    set_error("solver_initialize: " + err);
+    return;
+  }
+  s->ready = true;
+}
+
+int solver_run(void* solver_data, double* state, double* env, double t_initial,
+               double t_final) {
+  Solver* s = S(solver_data);
+  if (!s || !s->ready) {
+    set_error("solver_run: solver is not initialized");
+    return 1;
+  }
+  const int nc = s->n_cells, ns = s->n_state;
+  if (s->n_rxn == 0) {
+    // no reactions: the reference skips CVODE and writes back the clamped
+    // values (src/camp_solver.c:554-567, 672-683)
+    for (int c = 0; c < nc; ++c)
+      for (int i = 0; i < ns; ++i) {
+        double& v = state[(size_t)c * ns + i];
+        if (s->var_type[i] == campb::VAR_VARIABLE || s->var_type[i] == campb::VAR_CONSTANT)
+          v = v > kTiny ? v : kTiny;
+      }
+    return 0;
+  }
+  std::string err;
+  double* ds = s->engine->d_state_buf(nc, &err);
+  double* de = ds ? s->engine->d_env_buf(nc, &err) : nullptr;
+  if (!ds || !de) {
+    set_error("solver_run: " + err);
+    return 1;
+  }
+  cudaStream_t st = s->stream;
+  size_t bytes = sizeof(double) * (size_t)nc * ns;
+  if (cudaMemcpyAsync(ds, state, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(de, env, sizeof(double) * 2 * nc, cudaMemcpyHostToDevice, st) !=
+          cudaSuccess) {
+    set_error("solver_run: host to device copy failed");
+    return 1;
+  }
+  if (!run_common(s, ds, de, nc, t_initial, t_final, st, false)) return 1;
+  if (cudaMemcpyAsync(state, ds, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+    set_error("solver_run: device to host copy failed");
+    return 1;
+  }
+  if (!s->engine->fetch_stats(&s->stats, nc, st, &err)) {
+    set_error("solver_run: " + err);
+    return 1;
+  }
+  s->last_n = nc;
+  return status_of(s, nc);
+}
+
+void solver_get_statistics(void* solver_data, int* solver_flag, int* num_steps,
+                           int* RHS_evals, int* LS_setups, int* error_test_fails,
+                           int* NLS_iters, int* NLS_convergence_fails, int* DLS_Jac_evals,
+                           int* DLS_RHS_evals, double* last_time_step__s,
+                           double* next_time_step__s, int* Jac_eval_fails,
+                           int* RHS_evals_total, int* Jac_evals_total, double* RHS_time__s,
+                           double* Jac_time__s, double* max_loss_precision) {
+  Solver* s = S(solver_data);
+  int flag = 0, nst = 0, nfe = 0, ns = 0, netf = 0, nni = 0, ncf = 0, nje = 0;
+  double hu = 0.0, hc = 0.0;
+  for (int c = 0; c < s->last_n; ++c) {
+    const CellStats& x = s->stats[c];
+    if (x.status != 0 && flag == 0) flag = x.status;
+    nst = std::max(nst, x.nst);
+    nfe = std::max(nfe, x.nfe);
+    ns = std::max(ns, x.nsetups);
+    netf = std::max(netf, x.netf);
+    nni = std::max(nni, x.nni);
+    ncf = std::max(ncf, x.ncfn);
+    nje = std::max(nje, x.nje);
+    if (c == 0 || x.hu < hu) hu = x.hu;
+    if (c == 0 || x.hcur < hc) hc = x.hcur;
+  }
+  *solver_flag = flag;
+  *num_steps = nst;
+  *RHS_evals = nfe;
+  *LS_setups = ns;
+  *error_test_fails = netf;
+  *NLS_iters = nni;
+  *NLS_convergence_fails = ncf;
+  *DLS_Jac_evals = nje;
+  *DLS_RHS_evals = 0;  // no difference-quotient Jacobian is used
+  *last_time_step__s = hu;
+  *next_time_step__s = hc;
+  *Jac_eval_fails = 0;
+  // the reference reports -1/0 for these outside CAMP_DEBUG builds
+  *RHS_evals_total = -1;
+  *Jac_evals_total = -1;
+  *RHS_time__s = 0.0;
+  *Jac_time__s = 0.0;
+  *max_loss_precision = 0.0;
+}
+
+void solver_reset_timers(void* solver_data) { (void)solver_data; }
+
+int solver_set_debug_out(void* solver_data, int do_output) {
+  S(solver_data)->debug_out = do_output != 0;
+  return 0;
+}
+int solver_set_eval_jac(void* solver_data, int eval_jac) {
+  S(solver_data)->eval_jac = eval_jac != 0;
+  return 0;
+}
+
+void solver_free(void* solver_data) {
+  Solver* s = S(solver_data);
+  if (!s) return;
+  s->engine.reset();
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+void solver_free_update_data(void* update_data) { free(update_data); }
+void rxn_free_update_data(void* update_data) { free(update_data); }
+
+void* rxn_photolysis_create_rate_update_data(void) {
+  void* p = malloc(sizeof(int) + sizeof(double));
+  if (!p) {
+    set_error("out of memory allocating photolysis update data");
+    exit(1);
+  }
+  return p;
+}
+
+// layout of src/rxns/rxn_photolysis.c:262-283: an int photo id followed,
+// unaligned, by the double base rate
+void rxn_photolysis_set_rate_update_data(void* update_data, int photo_id, double base_rate) {
+  memcpy(update_data, &photo_id, sizeof(int));
+  memcpy((char*)update_data + sizeof(int), &base_rate, sizeof(double));
+}
+
+void rxn_update_data(int cell_id, int* rxn_id, int update_rxn_type, void* update_data,
+                     void* solver_data) {
+  Solver* s = S(solver_data);
+  if (cell_id < 0 || cell_id >= s->n_cells) return;
+  const auto& rx = s->model->rxns();
+  const int n_rxn = (int)rx.size();
+  if (update_rxn_type != campb::RXN_PHOTOLYSIS) {
+    // emission, first-order loss, wet deposition and condensed-phase
+    // photolysis updates have no reaction of that type here
+    *rxn_id = n_rxn;
+    return;
+  }
+  s->ensure_photo();
+  int photo_id;
+  double base;
+  memcpy(&photo_id, update_data, sizeof(int));
+  memcpy(&base, (char*)update_data + sizeof(int), sizeof(double));
+  for (; *rxn_id < n_rxn; (*rxn_id)++) {
+    const auto& r = rx[*rxn_id];
+    if (r.type != update_rxn_type) continue;
+    int rid = s->model->rxn_int()[r.int_off + 2];
+    if (photo_id == rid && rid > 0) {
+      int slot = 0;
+      for (int i = 0; i < *rxn_id; ++i)
+        if (rx[i].type == campb::RXN_PHOTOLYSIS) ++slot;
+      s->photo[(size_t)cell_id * s->n_photo + slot] = base;
+      return;
+    }
+  }
+}
+
+void rxn_print_data(void* solver_data) {
+  Solver* s = S(solver_data);
+  printf("\n\nReaction data\n\nnumber of reactions: %d\n\n", s->n_rxn);
+  static const char* names[] = {"", "Arrhenius", "Troe", "CMAQ_H2O2", "CMAQ_OH_HNO3",
+                                "Photolysis"};
+  for (const auto& r : s->model->rxns())
+    printf("\n\n%s reaction\n", (r.type >= 1 && r.type <= 5) ? names[r.type] : "Unknown");
+  fflush(stdout);
+}
+void aero_phase_print_data(void* solver_data) {
+  printf("\n\nAerosol phase data\n\nnumber of aerosol phases: %d\n\n",
+         S(solver_data)->n_aero_phase);
+}
+void aero_rep_print_data(void* solver_data) {
+  printf("\n\nAerosol representation data\n\nnumber of aerosol representations: %d\n\n",
+         S(solver_data)->n_aero_rep);
+}
+void sub_model_print_data(void* solver_data) {
+  printf("\n\nSub-model data\n\nnumber of sub-models: %d\n\n", S(solver_data)->n_sub_model);
+}
+
+// ----------------------------------------------------------------------------
+// extension API
+// ----------------------------------------------------------------------------
+const char* camp_b200_last_error(void) { return g_last_error.c_str(); }
+
+int camp_b200_is_ready(void* solver_data) { return S(solver_data)->ready ? 1 : 0; }
+
+int camp_b200_set_precision(void* solver_data, int mode) {
+  if (mode != CAMP_B200_FP64 && mode != CAMP_B200_MIXED) {
+    set_error("camp_b200_set_precision: unknown mode");
+    return -1;
+  }
+  S(solver_data)->settings.precision = mode;
+  return 0;
+}
+
+int camp_b200_set_launch(void* solver_data, int warps_per_block, int blocks_per_sm) {
+  S(solver_data)->settings.warps_per_block = std::max(0, warps_per_block);
+  S(solver_data)->settings.blocks_per_sm = std::max(1, blocks_per_sm);
+  return 0;
+}
+
+int camp_b200_set_cost_ordering(void* solver_data, int enable) {
+  S(solver_data)->cost_order = enable != 0;
+  return 0;
+}
+
+int camp_b200_run_device(void* solver_data, double* d_state, const double* d_env, int n_cells,
+                         double t_initial, double t_final, void* stream) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells) {
+    set_error("camp_b200_run_device: solver not ready or n_cells out of range");
+    return -1;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+  if (!run_common(s, d_state, d_env, n_cells, t_initial, t_final, st, true)) return -1;
+  return status_of(s, n_cells);
+}
+
+int camp_b200_launch_device(void* solver_data, double* d_state, const double* d_env,
+                            int n_cells, double t_initial, double t_final, void* stream) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells) {
+    set_error("camp_b200_launch_device: solver not ready or n_cells out of range");
+    return -1;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+  if (!run_common(s, d_state, d_env, n_cells, t_initial, t_final, st, false)) return -1;
+  s->last_n = -n_cells;  // pending
+  return 0;
+}
+
+int camp_b200_sync_status(void* solver_data, void* stream) {
+  Solver* s = S(solver_data);
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+  int n = s->last_n < 0 ? -s->last_n : s->last_n;
+  std::string err;
+  if (!s->engine->fetch_stats(&s->stats, n, st, &err)) {
+    set_error(err);
+    return -1;
+  }
+  s->last_n = n;
+  return status_of(s, n);
+}
+
+int camp_b200_n_photo(void* solver_data) {
+  Solver* s = S(solver_data);
+  s->ensure_photo();
+  return s->n_photo;
+}
+
+int camp_b200_set_photo_rates(void* solver_data, const double* rates, int n_cells) {
+  Solver* s = S(solver_data);
+  s->ensure_photo();
+  if (n_cells < 0 || n_cells > s->n_cells) return -1;
+  std::copy(rates, rates + (size_t)n_cells * s->n_photo, s->photo.begin());
+  return 0;
+}
+
+int camp_b200_get_cell_stats(void* solver_data, camp_b200_cell_stats* out, int n_cells) {
+  Solver* s = S(solver_data);
+  int n = std::min(n_cells, std::abs(s->last_n));
+  for (int c = 0; c < n; ++c) {
+    const CellStats& x = s->stats[c];
+    out[c].status = x.status;
+    out[c].nst = x.nst;
+    out[c].nfe = x.nfe;
+    out[c].nsetups = x.nsetups;
+    out[c].netf = x.netf;
+    out[c].nni = x.nni;
+    out[c].ncfn = x.ncfn;
+    out[c].nje = x.nje;
+    out[c].hu = x.hu;
+    out[c].hcur = x.hcur;
+  }
+  for (int c = n; c < n_cells; ++c) {
+    memset(&out[c], 0, sizeof(out[c]));
+    out[c].status = CAMP_B200_NOT_RUN;
+  }
+  return n;
+}
+
+long camp_b200_kernel_launches(void* solver_data) {
+  Solver* s = S(solver_data);
+  return s->engine ? s->engine->launches() : 0;
+}
+
+double camp_b200_last_kernel_ms(void* solver_data) {
+  Solver* s = S(solver_data);
+  return s->engine ? s->engine->last_kernel_ms() : 0.0;
+}
+
+int camp_b200_n_dep_var(void* solver_data) { return S(solver_data)->model->n_dep(); }
+int camp_b200_n_jac_elem(void* solver_data) {
+  return (int)S(solver_data)->model->solver_rowid().size();
+}
+int camp_b200_n_lu_elem(void* solver_data) { return S(solver_data)->model->tables().n_lu; }
+int camp_b200_rxn_int_data_size(void* solver_data) {
+  return (int)S(solver_data)->model->rxn_int().size();
+}
+int camp_b200_get_solver_jac(void* solver_data, int* col_ptrs, int* row_ids) {
+  const Model& m = *S(solver_data)->model;
+  if (!m.built()) return -1;
+  std::copy(m.solver_colptr().begin(), m.solver_colptr().end(), col_ptrs);
+  std::copy(m.solver_rowid().begin(), m.solver_rowid().end(), row_ids);
+  return 0;
+}
+int camp_b200_get_rxn_int_data(void* solver_data, int* out) {
+  const Model& m = *S(solver_data)->model;
+  std::copy(m.rxn_int().begin(), m.rxn_int().end(), out);
+  return 0;
+}
+int camp_b200_get_lu_order(void* solver_data, int* perm) {
+  const Model& m = *S(solver_data)->model;
+  if (!m.built()) return -1;
+  std::copy(m.tables().lu_perm.begin(), m.tables().lu_perm.end(), perm);
+  return 0;
+}
+
+int camp_b200_eval_deriv(void* solver_data, const double* state, const double* env,
+                         int n_cells, double h, double* r_p, double* r_l, double* deriv) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells) return -1;
+  std::string err;
+  if (!s->engine->eval_deriv(state, env, s->n_photo ? s->photo.data() : nullptr, n_cells, h,
+                             r_p, r_l, deriv, &err)) {
+    set_error(err);
+    return -1;
+  }
+  return 0;
+}
+
+int camp_b200_eval_jac(void* solver_data, const double* state, const double* env, int n_cells,
+                       double h, double* j_prod, double* j_loss) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells) return -1;
+  std::string err;
+  if (!s->engine->eval_jac(state, env, s->n_photo ? s->photo.data() : nullptr, n_cells, h,
+                           j_prod, j_loss, &err)) {
+    set_error(err);
+    return -1;
+  }
+  return 0;
+}
+
+}  // extern "C"

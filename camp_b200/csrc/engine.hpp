@@ -1,0 +1,68 @@
+// Device engine: mechanism tables in device memory and the launches of the
+// per-cell solve and evaluation kernels.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "model.hpp"
+
+namespace campb {
+
+struct CellStats {
+  int status;
+  int nst, nfe, nsetups, netf, nni, ncfn, nje;
+  double hu, hcur;
+};
+
+struct SolveSettings {
+  double rtol = 1e-4;
+  int max_steps = 10000;
+  int max_conv_fails = 1000;
+  int precision = 0;       // 0 = FP64, 1 = mixed
+  int warps_per_block = 0; // 0 = as many as fit
+  int blocks_per_sm = 1;
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+  // Uploads the tables of a built model and the absolute tolerances of the
+  // dependent variables; sizes per-cell buffers for `capacity` cells.
+  bool init(const Model& model, const std::vector<double>& atol_dep, int capacity,
+            std::string* err);
+  // Launches the solve of n_cells cells whose state/env live on the device.
+  // photo (device, [n_cells * n_photo]) may be null when there is no
+  // photolysis.  order (device, n_cells) may be null for identity order.
+  bool launch_solve(double* d_state, const double* d_env, const double* d_photo,
+                    const int* d_order, int n_cells, double t0, double t1,
+                    const SolveSettings& s, void* stream, std::string* err);
+  // Copies per-cell stats of the last launch to the host (synchronising).
+  bool fetch_stats(std::vector<CellStats>* out, int n_cells, void* stream,
+                   std::string* err);
+  bool eval_deriv(const double* h_state, const double* h_env, const double* h_photo,
+                  int n_cells, double h, double* r_p, double* r_l, double* f,
+                  std::string* err);
+  bool eval_jac(const double* h_state, const double* h_env, const double* h_photo,
+                int n_cells, double h, double* jp, double* jl, std::string* err);
+
+  double* d_state_buf(int n_cells, std::string* err);
+  double* d_env_buf(int n_cells, std::string* err);
+  double* d_photo_buf(int n_cells, std::string* err);
+  int* d_order_buf(int n_cells, std::string* err);
+  bool sync(void* stream, std::string* err);
+  long launches() const { return launches_; }
+  double last_kernel_ms() const { return last_ms_; }
+  bool read_last_ms(void* stream);
+
+ private:
+  bool ensure(void** p, size_t* cap, size_t bytes, std::string* err);
+  struct Impl;
+  Impl* impl_;
+  long launches_ = 0;
+  double last_ms_ = 0.0;
+};
+
+}  // namespace campb

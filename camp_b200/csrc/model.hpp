@@ -1,0 +1,122 @@
+// Host-side mechanism model: packed reaction data, Jacobian sparsity, the
+// fixed elimination order of the per-cell LU and the flat tables the device
+// kernels read.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace campb {
+
+// reaction type ids, src/rxn_solver.c:19-35
+enum : int {
+  RXN_ARRHENIUS = 1,
+  RXN_TROE = 2,
+  RXN_CMAQ_H2O2 = 3,
+  RXN_CMAQ_OH_HNO3 = 4,
+  RXN_PHOTOLYSIS = 5,
+};
+
+// state variable types, src/camp_common.h:34-38
+enum : int { VAR_VARIABLE = 1, VAR_CONSTANT = 2 };
+
+// One reaction's view into the packed arrays.
+struct Rxn {
+  int type = 0;
+  int int_off = 0;    // index of NUM_REACT_ in Model::rxn_int (type slot is int_off-1)
+  int float_off = 0;  // first float parameter
+  int env_off = 0;    // first env parameter within a cell's rxn_env_data
+  int nr = 0, np = 0;
+  int n_int_prop = 2, n_float_prop = 0;
+};
+
+// Flat tables that drive the device code.  All indices are int32.
+struct Tables {
+  int n = 0;        // dependent variables
+  int n_state = 0;  // state variables per cell
+  int n_rxn = 0;
+  int n_part = 0;   // variable-reactant occurrences (rate partials)
+  int n_jac = 0;    // solver Jacobian entries
+  int n_lu = 0;     // L+U entries
+  int n_photo = 0;  // photolysis reactions
+  int n_flev = 0, n_blev = 0;
+  int max_fgather = 0;
+
+  // rate laws: type, number of reactants (incl. constants), packed float
+  // parameters (the type's head block), photolysis slot
+  std::vector<int> rx_type, rx_nreact, rx_fpar, rx_photo;
+  std::vector<double> fpar;
+  // constant reactants (state index), variable reactants (dependent index)
+  std::vector<int> rx_cptr, rx_cidx, rx_vptr, rx_vdep;
+  // f gather by dependent species: reaction, coefficient, product flag
+  std::vector<int> fg_ptr, fg_rxn, fg_prod;
+  std::vector<double> fg_coef;
+  // J gather by solver Jacobian entry (CSC order)
+  std::vector<int> jg_ptr, jg_part, jg_ind, jg_lupos, jg_row;
+  std::vector<double> jg_coef;
+  // LU structure in pivot order
+  std::vector<int> lu_perm, lu_iperm, lu_rowptr, lu_col, lu_diag;
+  std::vector<int> upd_ptr, upd_src, upd_dst;  // per L entry position
+  std::vector<int> fl_ptr, fl_rows;            // forward / factor row levels
+  std::vector<int> bl_ptr, bl_rows;            // backward row levels
+  std::vector<int> dep_state;                  // dependent index -> state index
+};
+
+class Model {
+ public:
+  Model(int n_state_var, int n_cells, const int* var_type, int n_rxn,
+        int n_rxn_int, int n_rxn_float, int n_rxn_env);
+
+  // rxn_add_condensed_data (src/rxn_solver.c:658-700)
+  bool add_rxn(int type, int n_int, int n_float, int n_env, const int* ints,
+               const double* floats, std::string* err);
+
+  // get_jac_init (src/camp_solver.c:1417-1712) for a gas-phase model:
+  // reaction Jacobian, DERIV_ID/JAC_ID, solver Jacobian; then the LU
+  // elimination order and the device tables.  Returns false on error.
+  bool build(std::string* err);
+
+  int n_state() const { return n_state_; }
+  int n_cells() const { return n_cells_; }
+  int n_dep() const { return n_dep_; }
+  int n_rxn() const { return n_rxn_; }
+  int n_added() const { return n_added_; }
+  int n_rxn_env() const { return n_env_; }
+  const std::vector<int>& var_type() const { return var_type_; }
+  const std::vector<int>& rxn_int() const { return rxn_int_; }
+  const std::vector<double>& rxn_float() const { return rxn_float_; }
+  const std::vector<Rxn>& rxns() const { return rxns_; }
+  const std::vector<int>& solver_colptr() const { return sj_colptr_; }
+  const std::vector<int>& solver_rowid() const { return sj_rowid_; }
+  const Tables& tables() const { return tab_; }
+  bool built() const { return built_; }
+
+  // photolysis: index of each photolysis reaction in mechanism order (-1 for
+  // other types), and its RXN_ID_ value
+  const std::vector<int>& photo_slot() const { return photo_slot_; }
+  int photo_id(int rxn) const;
+
+ private:
+  void build_rxn_jacobian();
+  void update_ids();
+  void build_solver_jacobian();
+  void build_lu();
+  void build_tables();
+  int rxn_elem_id(int dep, int ind) const;
+
+  int n_state_, n_cells_, n_dep_, n_rxn_;
+  int n_added_ = 0, n_env_ = 0;
+  std::vector<int> var_type_;
+  std::vector<int> rxn_int_;
+  std::vector<double> rxn_float_;
+  std::vector<Rxn> rxns_;
+  std::vector<int> photo_slot_;
+  std::vector<int> deriv_ids_;
+  std::vector<int> rj_colptr_, rj_rowid_;
+  std::vector<int> sj_colptr_, sj_rowid_;
+  Tables tab_;
+  bool built_ = false;
+};
+
+}  // namespace campb

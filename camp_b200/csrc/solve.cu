@@ -1,0 +1,1322 @@
+// Per-cell stiff chemistry solve on sm_100a.
+//
+// One warp integrates one grid cell over a whole host time step with its own
+// variable-order BDF (the CVODE algorithm: Nordsieck history, Newton
+// iteration on I - gamma*J, WRMS local error test, step and order control).
+// The kernel is persistent: each warp pulls the next cell index from a
+// global counter when its cell finishes, so cells with very different
+// stiffness keep every SM busy until the tail.
+//
+// Lane l of a warp owns the dependent variables l, l+32, l+64, ... for the
+// element-wise vector work; the rate, Jacobian and LU phases are spread over
+// the lanes by reaction, Jacobian entry and LU row, with row-level
+// schedules computed on the host so that no two lanes write the same word.
+// Everything a warp touches during the integration lives in its slice of
+// shared memory except the saved Jacobian, which sits in a per-warp global
+// slot (L2-resident: a few MB for all resident warps).
+//
+// Precision: the plain form is FP64 throughout.  The mixed form keeps the
+// saved Jacobian, the LU factors and the triangular solves in FP32 and
+// everything else (rates, residual, state, error test, step control) in
+// FP64; the Newton iteration then acts as iterative refinement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.hpp"
+
+namespace campb {
+
+#define FULLMASK 0xffffffffu
+
+constexpr double kSmall = 1.0e-30;
+constexpr double kTiny = 1.0e-60;
+
+// CVODE constants (Hindmarsh et al., ACM TOMS 31(3) 2005; CVODE docs)
+constexpr int QMAX = 5;
+constexpr int LMAX = QMAX + 1;
+constexpr double ETAMX1 = 10000.0, ETAMX2 = 10.0, ETAMX3 = 10.0;
+constexpr double ETAMXF = 0.2, ETAMIN = 0.1, ETACF = 0.25;
+constexpr double ADDON = 0.000001, BIAS1 = 6.0, BIAS2 = 6.0, BIAS3 = 10.0;
+constexpr double THRESH = 1.5;
+constexpr int SMALL_NST = 10, MXNEF1 = 3, SMALL_NEF = 2, LONG_WAIT = 10;
+constexpr int MAXCOR = 3;
+constexpr double CRDOWN = 0.3, DGMAX = 0.3, RDIV = 2.0;
+constexpr int MSBP = 20, MSBJ = 50;
+constexpr double DGMAX_J = 0.2, NLSCOEF = 0.1;
+constexpr double UROUND = 2.220446049250313e-16;
+
+// outcome codes (CVODE flags)
+constexpr int OK = 0, TOO_MUCH_WORK = -1, TOO_MUCH_ACC = -2, ERR_FAILURE = -3,
+              CONV_FAILURE = -4,
+              REPTD_RHSFUNC_ERR = -10, UNREC_RHSFUNC_ERR = -11, ILL_INPUT = -22;
+// nonlinear solver outcomes
+constexpr int NL_OK = 0, NL_CONV_FAIL = 1, NL_RHS_RECVR = 2, NL_TRY_AGAIN = 3,
+              NL_CONSTR_RECVR = 4;
+constexpr int NO_FAILURES = 0, FAIL_BAD_J = 1, FAIL_OTHER = 2;
+constexpr int FIRST_CALL = 0, PREV_CONV_FAIL = 1, PREV_ERR_FAIL = 2;
+constexpr int DO_ERROR_TEST = 100, PREDICT_AGAIN = 101, TRY_AGAIN = 102;
+
+// ---------------------------------------------------------------------------
+// Device tables
+// ---------------------------------------------------------------------------
+struct DevMech {
+  int n, n_state, n_rxn, n_part, n_jac, n_lu, n_photo, n_flev, n_blev;
+  int n_const;
+  const int *rx_type, *rx_nreact, *rx_fpar, *rx_photo;
+  const double* fpar;
+  const int *rx_cptr, *rx_cidx, *rx_vptr, *rx_vdep;
+  const int *fg_ptr, *fg_rxn, *fg_prod;
+  const double* fg_coef;
+  const int *jg_ptr, *jg_part, *jg_ind, *jg_lupos, *jg_row;
+  const double* jg_coef;
+  const int *lu_perm, *lu_rowptr, *lu_col, *lu_diag;
+  const int *upd_ptr, *upd_src, *upd_dst;
+  const int *fl_ptr, *fl_rows, *bl_ptr, *bl_rows;
+  const int *dep_state, *const_state;
+  const double* atol;  // per dependent variable
+};
+
+struct Layout {  // per-warp shared-memory slice (byte offsets)
+  int zn, ewt, acor, y, ftemp, tempv, rates, keff, lu, z, bytes;
+};
+
+struct SolveArgs {
+  DevMech m;
+  Layout lay;
+  double* state;
+  const double* env;
+  const double* photo;
+  const int* order;
+  int n_cells;
+  int* counter;
+  CellStats* stats;
+  void* jscratch;  // per-warp saved Jacobian slots
+  double t0, t1, rtol;
+  int max_steps, maxncf, maxnef;
+};
+
+// ---------------------------------------------------------------------------
+// Warp helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(FULLMASK, v, o));
+  return v;
+}
+__device__ __forceinline__ bool warp_any(bool p) { return __any_sync(FULLMASK, p) != 0; }
+
+// value the reference's f sees for a solver variable: y above -SMALL is used
+// as is, anything else (only exactly -SMALL reaches here) becomes TINY
+// (src/camp_solver.c:805-833)
+__device__ __forceinline__ double state_of(double y) { return y > -kSmall ? y : kTiny; }
+
+template <typename T>
+__device__ __forceinline__ T ldg(const T* p) {
+  return __ldg(p);
+}
+
+// ---------------------------------------------------------------------------
+// Rate constants (update_env_state of the gas types)
+// ---------------------------------------------------------------------------
+__device__ double rate_constant(const DevMech& m, int r, double T, double P,
+                                const double* photo_cell) {
+  const double* f = m.fpar + ldg(m.rx_fpar + r);
+  const int nr = ldg(m.rx_nreact + r);
+  switch (ldg(m.rx_type + r)) {
+    case RXN_ARRHENIUS:  // src/rxns/rxn_arrhenius.c:103-118
+      return f[0] * exp(f[2] / T) * (f[1] == 0.0 ? 1.0 : pow(T / f[3], f[1])) *
+             (f[4] == 0.0 ? 1.0 : (1.0 + f[4] * P)) * pow(f[5] * P / T, (double)(nr - 1));
+    case RXN_TROE: {  // src/rxns/rxn_troe.c:118-140
+      double conv = f[9] * P / T;
+      double k0 = f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
+                  (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) * conv;
+      double kinf = k0 / (f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
+                          (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4])));
+      double e = log10(kinf) / f[7];
+      return (k0 / (1.0 + kinf)) * pow(f[6], 1.0 / (1.0 + e * e)) *
+             pow(conv, (double)(nr - 1)) * f[8];
+    }
+    case RXN_CMAQ_H2O2: {  // src/rxns/rxn_CMAQ_H2O2.c:106-125
+      double conv = f[6] * P / T;
+      return (f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
+                  (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) +
+              f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
+                  (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4])) * conv) *
+             pow(conv, (double)(nr - 1));
+    }
+    case RXN_CMAQ_OH_HNO3: {  // src/rxns/rxn_CMAQ_OH_HNO3.c:110-133
+      double conv = f[10] * P / T;
+      double k2 = f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
+                  (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4]));
+      double k3 = f[6] * (f[8] == 0.0 ? 1.0 : exp(f[8] / T)) *
+                  (f[7] == 0.0 ? 1.0 : pow(T / 300.0, f[7])) * conv;
+      return (f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
+                  (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) +
+              k3 / (1.0 + k3 / k2)) *
+             pow(conv, (double)(nr - 1)) * f[9];
+    }
+    case RXN_PHOTOLYSIS:  // src/rxns/rxn_photolysis.c:137-148
+      return f[0] * (photo_cell ? photo_cell[ldg(m.rx_photo + r)] : 0.0);
+  }
+  return 0.0;
+}
+
+// k of every reaction times the (clamped) constant-species concentrations it
+// multiplies; constant species are clamped to TINY as solver_run does.
+__device__ void compute_keff(const DevMech& m, const double* cell_state,
+                             double T, double P, const double* photo_cell,
+                             double* keff, int lane) {
+  for (int r = lane; r < m.n_rxn; r += 32) {
+    double k = rate_constant(m, r, T, P, photo_cell);
+    for (int c = ldg(m.rx_cptr + r); c < ldg(m.rx_cptr + r + 1); ++c) {
+      double s = cell_state[ldg(m.rx_cidx + c)];
+      k *= s > kTiny ? s : kTiny;
+    }
+    keff[r] = k;
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Right-hand side f(y) and Jacobian
+// ---------------------------------------------------------------------------
+// Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
+// When rp/rl are given, the production and loss sums are written too.
+__device__ int dev_f(const DevMech& m, const double* y, double h,
+                     const double* keff, double* rates, double* out, int lane,
+                     double* rp = nullptr, double* rl = nullptr) {
+  bool bad = false;
+  for (int i = lane; i < m.n; i += 32) bad |= y[i] < -kSmall;
+  if (warp_any(bad)) return 1;
+  for (int r = lane; r < m.n_rxn; r += 32) {
+    double rate = keff[r];
+    for (int v = ldg(m.rx_vptr + r); v < ldg(m.rx_vptr + r + 1); ++v)
+      rate *= state_of(y[ldg(m.rx_vdep + v)]);
+    rates[r] = rate;
+  }
+  __syncwarp();
+  // gather per species: reaction loss and (guarded) product contributions,
+  // split by sign into production and loss (src/time_derivative.c:90-97)
+  for (int i = lane; i < m.n; i += 32) {
+    const double yi = state_of(y[i]);
+    double P = 0.0, L = 0.0;
+    const int e1 = ldg(m.fg_ptr + i + 1);
+    for (int e = ldg(m.fg_ptr + i); e < e1; ++e) {
+      const double rate = rates[ldg(m.fg_rxn + e)];
+      if (rate == 0.0) continue;
+      const double c = ldg(m.fg_coef + e);
+      // a negative yield may not drive the product negative within one step
+      // (src/rxns/rxn_arrhenius.c:153-160)
+      if (ldg(m.fg_prod + e) && !(-rate * c * h <= yi)) continue;
+      const double v = rate * c;
+      if (v > 0.0)
+        P += v;
+      else
+        L -= v;
+    }
+    out[i] = (P + L != 0.0) ? P - L : 0.0;
+    if (rp) rp[i] = P;
+    if (rl) rl[i] = L;
+  }
+  __syncwarp();
+  return 0;
+}
+
+// Solver Jacobian values (CSC order) into Jout; production and loss parts
+// into jp/jl when given (src/rxns/rxn_arrhenius.c:178-212).
+template <typename JT>
+__device__ int dev_jac(const DevMech& m, const double* y, double h,
+                       const double* keff, double* part, JT* Jout, int lane,
+                       double* jp = nullptr, double* jl = nullptr) {
+  bool bad = false;
+  for (int i = lane; i < m.n; i += 32) bad |= y[i] < -kSmall;
+  if (warp_any(bad)) return 1;
+  for (int r = lane; r < m.n_rxn; r += 32) {
+    const int v0 = ldg(m.rx_vptr + r), v1 = ldg(m.rx_vptr + r + 1);
+    for (int kv = v0; kv < v1; ++kv) {
+      double p = keff[r];
+      for (int v = v0; v < v1; ++v)
+        if (v != kv) p *= state_of(y[ldg(m.rx_vdep + v)]);
+      part[kv] = p;
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < m.n_jac; e += 32) {
+    const double yrow = state_of(y[ldg(m.jg_row + e)]);
+    double P = 0.0, L = 0.0;
+    const int g1 = ldg(m.jg_ptr + e + 1);
+    for (int g = ldg(m.jg_ptr + e); g < g1; ++g) {
+      const double p = part[ldg(m.jg_part + g)];
+      const int ind = ldg(m.jg_ind + g);
+      if (ind < 0) {
+        L += p;
+      } else {
+        const double c = ldg(m.jg_coef + g);
+        if (-p * state_of(y[ind]) * c * h <= yrow) P += c * p;
+      }
+    }
+    Jout[e] = (JT)(P - L);
+    if (jp) jp[e] = P;
+    if (jl) jl[e] = L;
+  }
+  __syncwarp();
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// LU of M = I - gamma*J on the fixed order, and the triangular solves
+// ---------------------------------------------------------------------------
+template <typename LT>
+__device__ bool dev_form_factor(const DevMech& m, const LT* J, double gamma, LT* LU,
+                                int lane) {
+  for (int q = lane; q < m.n_lu; q += 32) LU[q] = (LT)0;
+  __syncwarp();
+  for (int e = lane; e < m.n_jac; e += 32) LU[ldg(m.jg_lupos + e)] = (LT)(-gamma * (double)J[e]);
+  __syncwarp();
+  for (int i = lane; i < m.n; i += 32) LU[ldg(m.lu_diag + i)] += (LT)1;
+  __syncwarp();
+  bool bad = false;
+  for (int lv = 0; lv < m.n_flev; ++lv) {
+    const int r1 = ldg(m.fl_ptr + lv + 1);
+    for (int idx = ldg(m.fl_ptr + lv) + lane; idx < r1; idx += 32) {
+      const int i = ldg(m.fl_rows + idx);
+      const int d = ldg(m.lu_diag + i);
+      for (int q = ldg(m.lu_rowptr + i); q < d; ++q) {
+        const int k = ldg(m.lu_col + q);
+        const LT l = LU[q] / LU[ldg(m.lu_diag + k)];
+        LU[q] = l;
+        const int p1 = ldg(m.upd_ptr + q + 1);
+        for (int p = ldg(m.upd_ptr + q); p < p1; ++p)
+          LU[ldg(m.upd_dst + p)] -= l * LU[ldg(m.upd_src + p)];
+      }
+      const LT piv = LU[d];
+      bad |= (piv == (LT)0) || !isfinite((double)piv);
+    }
+    __syncwarp();
+  }
+  return !warp_any(bad);
+}
+
+// b (original variable order, FP64) <- M^{-1} b
+template <typename LT>
+__device__ void dev_lsolve(const DevMech& m, const LT* LU, double* b, LT* z, int lane) {
+  for (int k = lane; k < m.n; k += 32) z[k] = (LT)b[ldg(m.lu_perm + k)];
+  __syncwarp();
+  for (int lv = 0; lv < m.n_flev; ++lv) {
+    const int r1 = ldg(m.fl_ptr + lv + 1);
+    for (int idx = ldg(m.fl_ptr + lv) + lane; idx < r1; idx += 32) {
+      const int i = ldg(m.fl_rows + idx);
+      LT s = z[i];
+      const int d = ldg(m.lu_diag + i);
+      for (int q = ldg(m.lu_rowptr + i); q < d; ++q) s -= LU[q] * z[ldg(m.lu_col + q)];
+      z[i] = s;
+    }
+    __syncwarp();
+  }
+  for (int lv = 0; lv < m.n_blev; ++lv) {
+    const int r1 = ldg(m.bl_ptr + lv + 1);
+    for (int idx = ldg(m.bl_ptr + lv) + lane; idx < r1; idx += 32) {
+      const int i = ldg(m.bl_rows + idx);
+      LT s = z[i];
+      const int d = ldg(m.lu_diag + i);
+      const int q1 = ldg(m.lu_rowptr + i + 1);
+      for (int q = d + 1; q < q1; ++q) s -= LU[q] * z[ldg(m.lu_col + q)];
+      z[i] = s / LU[d];
+    }
+    __syncwarp();
+  }
+  for (int k = lane; k < m.n; k += 32) b[ldg(m.lu_perm + k)] = (double)z[k];
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// BDF integrator state of one cell (warp-uniform scalars)
+// ---------------------------------------------------------------------------
+template <typename LT>
+struct Cell {
+  const DevMech* m;
+  int lane, n;
+  double* zn[LMAX];
+  double *ewt, *acor, *y, *ftemp, *tempv, *rates, *keff;
+  LT *LU, *z, *J;
+  double rtol;
+  int max_steps, maxncf, maxnef;
+  double h0;
+  // method state
+  int q, qprime, qwait, L, jcur;
+  double h, hprime, hscale, eta, etamax, hu, next_h, tn;
+  double tau[LMAX + 1], tq[6], l[LMAX];
+  double rl1, gamma, gammap, gamrat, crate, acnrm, saved_tq5;
+  double etaqm1, etaq, etaqp1;
+  int nst, nfe, nsetups, netf, nni, ncfn, nje, nstlp, nstlj;
+
+  __device__ double wrms(const double* v) const {
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      double t = v[i] * ewt[i];
+      s += t * t;
+    }
+    return sqrt(warp_sum(s) / n);
+  }
+  __device__ int f(const double* yy, double* out) {
+    return dev_f(*m, yy, h > 0.0 ? h : h0, keff, rates, out, lane);
+  }
+  __device__ bool set_ewt(const double* yy) {
+    bool bad = false;
+    for (int i = lane; i < n; i += 32) {
+      double t = rtol * fabs(yy[i]) + m->atol[i];
+      bad |= !(t > 0.0);
+      ewt[i] = 1.0 / t;
+    }
+    __syncwarp();
+    return !warp_any(bad);
+  }
+  __device__ void rescale() {
+    double factor = eta;
+    for (int j = 1; j <= q; ++j) {
+      for (int i = lane; i < n; i += 32) zn[j][i] *= factor;
+      factor *= eta;
+    }
+    __syncwarp();
+    h = hscale * eta;
+    next_h = h;
+    hscale = h;
+  }
+  __device__ void predict() {
+    tn += h;
+    for (int i = lane; i < n; i += 32)
+      for (int k = 1; k <= q; ++k)
+        for (int j = q; j >= k; --j) zn[j - 1][i] += zn[j][i];
+    __syncwarp();
+  }
+  __device__ void restore(double saved_t) {
+    tn = saved_t;
+    for (int i = lane; i < n; i += 32)
+      for (int k = 1; k <= q; ++k)
+        for (int j = q; j >= k; --j) zn[j - 1][i] -= zn[j][i];
+    __syncwarp();
+  }
+  // l and tq of the fixed-leading-coefficient BDF formula
+  __device__ void set() {
+    double alpha0, alpha0_hat, xi_inv, xistar_inv, hsum;
+    l[0] = l[1] = xi_inv = xistar_inv = 1.0;
+    for (int i = 2; i <= q; ++i) l[i] = 0.0;
+    alpha0 = alpha0_hat = -1.0;
+    hsum = h;
+    if (q > 1) {
+      for (int j = 2; j < q; ++j) {
+        hsum += tau[j - 1];
+        xi_inv = h / hsum;
+        alpha0 -= 1.0 / j;
+        for (int i = j; i >= 1; --i) l[i] += l[i - 1] * xi_inv;
+      }
+      alpha0 -= 1.0 / q;
+      xistar_inv = -l[1] - alpha0;
+      hsum += tau[q - 1];
+      xi_inv = h / hsum;
+      alpha0_hat = -l[1] - xi_inv;
+      for (int i = q; i >= 1; --i) l[i] += l[i - 1] * xistar_inv;
+    }
+    double A1 = 1.0 - alpha0_hat + alpha0;
+    double A2 = 1.0 + q * A1;
+    tq[2] = fabs(A1 / (alpha0 * A2));
+    tq[5] = fabs(A2 * xistar_inv / (l[q] * xi_inv));
+    if (qwait == 1) {
+      if (q > 1) {
+        double C = xistar_inv / l[q];
+        double A3 = alpha0 + 1.0 / q;
+        double A4 = alpha0_hat + xi_inv;
+        double Cpinv = (1.0 - A4 + A3) / A3;
+        tq[1] = fabs(C * Cpinv);
+      } else {
+        tq[1] = 1.0;
+      }
+      hsum += tau[q];
+      xi_inv = h / hsum;
+      double A5 = alpha0 - 1.0 / (q + 1);
+      double A6 = alpha0_hat - xi_inv;
+      double Cppinv = (1.0 - A6 + A5) / A2;
+      tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+    }
+    tq[4] = NLSCOEF / tq[2];
+    rl1 = 1.0 / l[1];
+    gamma = h * rl1;
+    if (nst == 0) gammap = gamma;
+    gamrat = (nst > 0) ? gamma / gammap : 1.0;
+  }
+  __device__ void increase_order() {
+    for (int i = 0; i <= QMAX; ++i) l[i] = 0.0;
+    l[2] = 1.0;
+    double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = hscale;
+    if (q > 1) {
+      for (int j = 1; j < q; ++j) {
+        hsum += tau[j + 1];
+        double xi = hsum / hscale;
+        prod *= xi;
+        alpha0 -= 1.0 / (j + 1);
+        alpha1 += 1.0 / xi;
+        for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xiold + l[i - 1];
+        xiold = xi;
+      }
+    }
+    double A1 = (-alpha0 - alpha1) / prod;
+    for (int i = lane; i < n; i += 32) {
+      double top = A1 * zn[QMAX][i];
+      zn[q + 1][i] = top;
+      for (int j = 2; j <= q; ++j) zn[j][i] += l[j] * top;
+    }
+    __syncwarp();
+  }
+  __device__ void decrease_order() {
+    for (int i = 0; i <= QMAX; ++i) l[i] = 0.0;
+    l[2] = 1.0;
+    double hsum = 0.0;
+    for (int j = 1; j <= q - 2; ++j) {
+      hsum += tau[j];
+      double xi = hsum / hscale;
+      for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xi + l[i - 1];
+    }
+    for (int i = lane; i < n; i += 32)
+      for (int j = 2; j < q; ++j) zn[j][i] -= l[j] * zn[q][i];
+    __syncwarp();
+  }
+  __device__ void adjust_order(int dq) {
+    if (dq == 1)
+      increase_order();
+    else if (dq == -1)
+      decrease_order();
+  }
+  __device__ void adjust_params() {
+    if (qprime != q) {
+      adjust_order(qprime - q);
+      q = qprime;
+      L = q + 1;
+      qwait = L;
+    }
+    rescale();
+  }
+  // J reuse rule of the CVODE direct linear solver interface; returns 0, or
+  // >0 for a recoverable failure
+  __device__ int lsetup(int convfail, const double* ypred) {
+    double dgamma = fabs(gamma / gammap - 1.0);
+    bool jbad = (nst == 0) || (nst > nstlj + MSBJ) ||
+                ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_J)) || (convfail == FAIL_OTHER);
+    if (!jbad) {
+      jcur = 0;
+    } else {
+      nje++;
+      nstlj = nst;
+      jcur = 1;
+      if (dev_jac<LT>(*m, ypred, h > 0.0 ? h : h0, keff, rates, J, lane)) return 1;
+    }
+    return dev_form_factor<LT>(*m, J, gamma, LU, lane) ? 0 : 1;
+  }
+  __device__ int newton(bool projected) {
+    int mm = 0;
+    double del, delp = 0.0;
+    for (;;) {
+      for (int i = lane; i < n; i += 32)
+        tempv[i] = gamma * ftemp[i] - (rl1 * zn[1][i] + acor[i]);
+      __syncwarp();
+      dev_lsolve<LT>(*m, LU, tempv, z, lane);
+      if (gamrat != 1.0) {
+        double s = 2.0 / (1.0 + gamrat);
+        for (int i = lane; i < n; i += 32) tempv[i] *= s;
+      }
+      nni++;
+      del = wrms(tempv);
+      for (int i = lane; i < n; i += 32) {
+        acor[i] += tempv[i];
+        y[i] = zn[0][i] + acor[i];
+      }
+      __syncwarp();
+      if (mm > 0) crate = fmax(CRDOWN * crate, del / delp);
+      double dcon = del * fmin(1.0, crate) / tq[4];
+      if (dcon <= 1.0) {
+        acnrm = (mm == 0 && !projected) ? del : wrms(acor);
+        jcur = 0;
+        return NL_OK;
+      }
+      ++mm;
+      if ((mm == MAXCOR) || ((mm >= 2) && (del > RDIV * delp)))
+        return jcur ? NL_CONV_FAIL : NL_TRY_AGAIN;
+      delp = del;
+      int r = f(y, ftemp);
+      nfe++;
+      if (r > 0) return jcur ? NL_RHS_RECVR : NL_TRY_AGAIN;
+    }
+  }
+  // non-negativity of the converged iterate (CVODE's cvCheckConstraints
+  // with constraint >= 0 on every component)
+  __device__ int check_constraints() {
+    bool viol = false;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32)
+      if (y[i] < 0.0) {
+        viol = true;
+        double t = y[i] * ewt[i];
+        s += t * t;
+      }
+    if (!warp_any(viol)) return NL_OK;
+    double vnorm = sqrt(warp_sum(s) / n);
+    if (vnorm <= tq[4]) {
+      for (int i = lane; i < n; i += 32)
+        if (y[i] < 0.0) {
+          acor[i] -= y[i];
+          y[i] = 0.0;
+        }
+      __syncwarp();
+      acnrm = wrms(acor);
+      return NL_OK;
+    }
+    double e = 1.0e300;
+    for (int i = lane; i < n; i += 32)
+      if (y[i] < 0.0) {
+        double qv = zn[0][i] / (zn[0][i] - y[i]);
+        e = fmin(e, qv);
+      }
+    e = warp_min(e) * 0.9;
+    eta = e > 0.1 ? e : 0.1;
+    return NL_CONSTR_RECVR;
+  }
+  __device__ bool start_guess() {
+    bool proj = false;
+    for (int i = lane; i < n; i += 32) {
+      double a = zn[0][i] < 0.0 ? -zn[0][i] : 0.0;
+      proj |= a != 0.0;
+      acor[i] = a;
+      y[i] = zn[0][i] + a;
+    }
+    __syncwarp();
+    return warp_any(proj);
+  }
+  __device__ int nls(int nflag) {
+    int convfail = ((nflag == FIRST_CALL) || (nflag == PREV_ERR_FAIL)) ? NO_FAILURES : FAIL_OTHER;
+    bool call_setup = (nflag == PREV_CONV_FAIL) || (nflag == PREV_ERR_FAIL) || (nst == 0) ||
+                      (nst >= nstlp + MSBP) || (fabs(gamrat - 1.0) > DGMAX);
+    bool projected = start_guess();
+    for (;;) {
+      int r = f(y, ftemp);
+      nfe++;
+      if (r > 0) return NL_RHS_RECVR;
+      if (call_setup) {
+        int ier = lsetup(convfail, y);
+        nsetups++;
+        call_setup = false;
+        gamrat = crate = 1.0;
+        gammap = gamma;
+        nstlp = nst;
+        if (ier > 0) return NL_CONV_FAIL;
+      }
+      int ier = newton(projected);
+      if (ier == NL_OK) return check_constraints();
+      if (ier != NL_TRY_AGAIN) return ier;
+      call_setup = true;
+      convfail = FAIL_BAD_J;
+      projected = start_guess();
+    }
+  }
+  __device__ int handle_nflag(int* nflag, double saved_t, int* ncf) {
+    int nf = *nflag;
+    if (nf == NL_OK) return DO_ERROR_TEST;
+    ncfn++;
+    restore(saved_t);
+    (*ncf)++;
+    etamax = 1.0;
+    if (*ncf == maxncf) return nf == NL_RHS_RECVR ? REPTD_RHSFUNC_ERR : CONV_FAILURE;
+    if (nf != NL_CONSTR_RECVR) eta = ETACF;
+    *nflag = PREV_CONV_FAIL;
+    rescale();
+    return PREDICT_AGAIN;
+  }
+  __device__ int error_test(int* nflag, double saved_t, int* nef, double* dsm) {
+    *dsm = acnrm * tq[2];
+    if (*dsm <= 1.0) return OK;
+    (*nef)++;
+    netf++;
+    *nflag = PREV_ERR_FAIL;
+    restore(saved_t);
+    if (*nef == maxnef) return ERR_FAILURE;
+    etamax = 1.0;
+    if (*nef <= MXNEF1) {
+      eta = 1.0 / (pow(BIAS2 * *dsm, 1.0 / L) + ADDON);
+      eta = fmax(ETAMIN, eta);
+      if (*nef >= SMALL_NEF) eta = fmin(eta, ETAMXF);
+      rescale();
+      return TRY_AGAIN;
+    }
+    if (q > 1) {
+      eta = ETAMIN;
+      adjust_order(-1);
+      L = q;
+      q--;
+      qwait = L;
+      rescale();
+      return TRY_AGAIN;
+    }
+    eta = ETAMIN;
+    h *= eta;
+    next_h = h;
+    hscale = h;
+    qwait = LONG_WAIT;
+    int r = f(zn[0], tempv);
+    nfe++;
+    if (r > 0) return UNREC_RHSFUNC_ERR;
+    for (int i = lane; i < n; i += 32) zn[1][i] = h * tempv[i];
+    __syncwarp();
+    return TRY_AGAIN;
+  }
+  __device__ void complete_step() {
+    nst++;
+    hu = h;
+    for (int i = q; i >= 2; --i) tau[i] = tau[i - 1];
+    if ((q == 1) && (nst > 1)) tau[2] = tau[1];
+    tau[1] = h;
+    const bool save = (qwait - 1 == 1) && (q != QMAX);
+    for (int i = lane; i < n; i += 32) {
+      const double a = acor[i];
+      for (int j = 0; j <= q; ++j) zn[j][i] += l[j] * a;
+      if (save) zn[QMAX][i] = a;
+    }
+    __syncwarp();
+    qwait--;
+    if (save) {
+      saved_tq5 = tq[5];
+    }
+  }
+  __device__ void set_eta() {
+    if (eta < THRESH) {
+      eta = 1.0;
+      hprime = h;
+    } else {
+      eta = fmin(eta, etamax);
+      hprime = h * eta;
+    }
+  }
+  __device__ void prepare_next_step(double dsm) {
+    if (etamax == 1.0) {
+      qwait = qwait > 2 ? qwait : 2;
+      qprime = q;
+      hprime = h;
+      eta = 1.0;
+      return;
+    }
+    etaq = 1.0 / (pow(BIAS2 * dsm, 1.0 / L) + ADDON);
+    if (qwait != 0) {
+      eta = etaq;
+      qprime = q;
+      set_eta();
+      return;
+    }
+    qwait = 2;
+    etaqm1 = 0.0;
+    if (q > 1) {
+      double ddn = wrms(zn[q]) * tq[1];
+      etaqm1 = 1.0 / (pow(BIAS1 * ddn, 1.0 / q) + ADDON);
+    }
+    etaqp1 = 0.0;
+    if (q != QMAX && saved_tq5 != 0.0) {
+      double cquot = (tq[5] / saved_tq5) * pow(h / tau[2], (double)L);
+      for (int i = lane; i < n; i += 32) tempv[i] = acor[i] - cquot * zn[QMAX][i];
+      double dup = wrms(tempv) * tq[3];
+      etaqp1 = 1.0 / (pow(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
+    }
+    double etam = fmax(etaqm1, fmax(etaq, etaqp1));
+    if (etam < THRESH) {
+      eta = 1.0;
+      qprime = q;
+    } else if (etam == etaq) {
+      eta = etaq;
+      qprime = q;
+    } else if (etam == etaqm1) {
+      eta = etaqm1;
+      qprime = q - 1;
+    } else {
+      eta = etaqp1;
+      qprime = q + 1;
+      for (int i = lane; i < n; i += 32) zn[QMAX][i] = acor[i];
+      __syncwarp();
+    }
+    set_eta();
+  }
+  __device__ int step() {
+    double saved_t = tn, dsm = 0.0;
+    int ncf = 0, nef = 0, nflag = FIRST_CALL;
+    if ((nst > 0) && (hprime != h)) adjust_params();
+    for (;;) {
+      predict();
+      set();
+      nflag = nls(nflag);
+      int kflag = handle_nflag(&nflag, saved_t, &ncf);
+      if (kflag == PREDICT_AGAIN) continue;
+      if (kflag != DO_ERROR_TEST) return kflag;
+      int eflag = error_test(&nflag, saved_t, &nef, &dsm);
+      if (eflag == TRY_AGAIN) continue;
+      if (eflag != OK) return eflag;
+      break;
+    }
+    complete_step();
+    prepare_next_step(dsm);
+    etamax = (nst <= SMALL_NST) ? ETAMX2 : ETAMX3;
+    for (int i = lane; i < n; i += 32) acor[i] *= tq[2];
+    __syncwarp();
+    return OK;
+  }
+  // CVodeReInit + CVodeSetInitStep(h0) + CVode(tout, CV_NORMAL); y (shared)
+  // holds the initial values and receives the interpolated solution
+  __device__ int integrate(double t0, double tout) {
+    for (int i = 0; i <= LMAX; ++i) tau[i] = 0.0;
+    for (int i = 0; i < 6; ++i) tq[i] = 0.0;
+    q = 1;
+    L = 2;
+    qwait = L;
+    etamax = ETAMX1;
+    qprime = 1;
+    nst = nfe = nsetups = netf = nni = ncfn = nje = 0;
+    nstlp = nstlj = 0;
+    saved_tq5 = 0.0;
+    crate = 1.0;
+    jcur = 0;
+    hu = 0.0;
+    tn = t0;
+    gammap = gamma = 0.0;
+    h = 0.0;
+    h0 = tout - t0;
+    eta = 1.0;
+    for (int i = lane; i < n; i += 32) {
+      zn[0][i] = y[i];
+      for (int j = 1; j < LMAX; ++j) zn[j][i] = 0.0;
+    }
+    __syncwarp();
+    if (!set_ewt(zn[0])) return ILL_INPUT;
+    next_h = 0.0;
+    if (f(zn[0], zn[1])) return REPTD_RHSFUNC_ERR;
+    nfe++;
+    h = h0;
+    if ((tout - t0) * h < 0.0) return ILL_INPUT;
+    hscale = h;
+    hprime = h;
+    for (int i = lane; i < n; i += 32) zn[1][i] *= h;
+    __syncwarp();
+    int nstloc = 0;
+    for (;;) {
+      next_h = h;
+      if (nst > 0 && !set_ewt(zn[0])) return ILL_INPUT;
+      if (max_steps > 0 && nstloc >= max_steps) return TOO_MUCH_WORK;
+      double tolsf = UROUND * wrms(zn[0]);
+      if (tolsf > 1.0) return TOO_MUCH_ACC;
+      int kflag = step();
+      if (kflag != OK) return kflag;
+      nstloc++;
+      if ((tn - tout) * h >= 0.0) {
+        double s = (tout - tn) / h;
+        for (int i = lane; i < n; i += 32) {
+          double v = zn[q][i];
+          for (int j = q - 1; j >= 0; --j) v = zn[j][i] + s * v;
+          y[i] = v;
+        }
+        __syncwarp();
+        next_h = hprime;
+        return OK;
+      }
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+template <typename LT>
+__device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, char* base, int gwarp, int lane) {
+  c.m = &a.m;
+  c.lane = lane;
+  c.n = a.m.n;
+  double* zn = (double*)(base + a.lay.zn);
+  for (int j = 0; j < LMAX; ++j) c.zn[j] = zn + j * a.m.n;
+  c.ewt = (double*)(base + a.lay.ewt);
+  c.acor = (double*)(base + a.lay.acor);
+  c.y = (double*)(base + a.lay.y);
+  c.ftemp = (double*)(base + a.lay.ftemp);
+  c.tempv = (double*)(base + a.lay.tempv);
+  c.rates = (double*)(base + a.lay.rates);
+  c.keff = (double*)(base + a.lay.keff);
+  c.LU = (LT*)(base + a.lay.lu);
+  c.z = (LT*)(base + a.lay.z);
+  c.J = (LT*)a.jscratch + (size_t)gwarp * a.m.n_jac;
+  c.rtol = a.rtol;
+  c.max_steps = a.max_steps;
+  c.maxncf = a.maxncf;
+  c.maxnef = a.maxnef;
+}
+
+template <typename LT>
+__global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
+  extern __shared__ __align__(16) char smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int gwarp = blockIdx.x * (blockDim.x >> 5) + wib;
+  char* base = smem + (size_t)wib * a.lay.bytes;
+  Cell<LT> c;
+  bind_cell<LT>(c, a, base, gwarp, lane);
+  const DevMech& m = a.m;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(a.counter, 1);
+    idx = __shfl_sync(FULLMASK, idx, 0);
+    if (idx >= a.n_cells) break;
+    const int cell = a.order ? a.order[idx] : idx;
+    double* st = a.state + (size_t)cell * m.n_state;
+    // solver_run: dependent values clamped to >= TINY, constants clamped in
+    // place (src/camp_solver.c:554-567)
+    for (int i = lane; i < m.n; i += 32) {
+      double v = st[ldg(m.dep_state + i)];
+      c.y[i] = v > kTiny ? v : kTiny;
+    }
+    for (int j = lane; j < m.n_const; j += 32) {
+      int s = ldg(m.const_state + j);
+      double v = st[s];
+      st[s] = v > kTiny ? v : kTiny;
+    }
+    __syncwarp();
+    const double T = a.env[2 * (size_t)cell], P = a.env[2 * (size_t)cell + 1];
+    compute_keff(m, st, T, P, a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr,
+                 c.keff, lane);
+    int flag = c.integrate(a.t0, a.t1);
+    if (flag == OK)
+      for (int i = lane; i < m.n; i += 32) st[ldg(m.dep_state + i)] = c.y[i] > 0.0 ? c.y[i] : 0.0;
+    if (lane == 0) {
+      CellStats s;
+      s.status = flag;
+      s.nst = c.nst;
+      s.nfe = c.nfe;
+      s.nsetups = c.nsetups;
+      s.netf = c.netf;
+      s.nni = c.nni;
+      s.ncfn = c.ncfn;
+      s.nje = c.nje;
+      s.hu = c.hu;
+      s.hcur = c.next_h;
+      a.stats[cell] = s;
+    }
+    __syncwarp();
+  }
+}
+
+struct EvalArgs {
+  DevMech m;
+  Layout lay;
+  const double* state;
+  const double* env;
+  const double* photo;
+  int n_cells;
+  double h;
+  double *rp, *rl, *f, *jp, *jl, *jv;
+  int do_jac;
+};
+
+__global__ void eval_kernel(EvalArgs a) {
+  extern __shared__ __align__(16) char smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int cell = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (cell >= a.n_cells) return;
+  char* base = smem + (size_t)wib * a.lay.bytes;
+  const DevMech& m = a.m;
+  double* y = (double*)(base + a.lay.y);
+  double* rates = (double*)(base + a.lay.rates);
+  double* keff = (double*)(base + a.lay.keff);
+  const double* st = a.state + (size_t)cell * m.n_state;
+  for (int i = lane; i < m.n; i += 32) y[i] = st[ldg(m.dep_state + i)];
+  __syncwarp();
+  compute_keff(m, st, a.env[2 * cell], a.env[2 * cell + 1],
+               a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, keff, lane);
+  if (!a.do_jac) {
+    double* out = (double*)(base + a.lay.ftemp);
+    dev_f(m, y, a.h, keff, rates, out, lane, a.rp + (size_t)cell * m.n,
+          a.rl + (size_t)cell * m.n);
+    for (int i = lane; i < m.n; i += 32) a.f[(size_t)cell * m.n + i] = out[i];
+  } else {
+    dev_jac<double>(m, y, a.h, keff, rates, a.jv + (size_t)cell * m.n_jac, lane,
+                    a.jp + (size_t)cell * m.n_jac, a.jl + (size_t)cell * m.n_jac);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side of the engine
+// ---------------------------------------------------------------------------
+#define CK(call)                                                        \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) {                                            \
+      *err = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+      return false;                                                     \
+    }                                                                   \
+  } while (0)
+
+struct Engine::Impl {
+  DevMech m{};
+  void* d_tables = nullptr;
+  int capacity = 0;
+  int n_state = 0, n_photo = 0;
+  int sm_count = 0, max_smem = 0;
+  // buffers
+  void *d_state = nullptr, *d_env = nullptr, *d_photo = nullptr, *d_order = nullptr;
+  size_t c_state = 0, c_env = 0, c_photo = 0, c_order = 0;
+  void* d_stats = nullptr;
+  size_t c_stats = 0;
+  int* d_counter = nullptr;
+  void* d_jscratch = nullptr;
+  size_t c_jscratch = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool ev_pending = false;
+};
+
+Engine::Engine() : impl_(new Impl) {}
+
+Engine::~Engine() {
+  Impl* I = impl_;
+  cudaFree(I->d_tables);
+  cudaFree(I->d_state);
+  cudaFree(I->d_env);
+  cudaFree(I->d_photo);
+  cudaFree(I->d_order);
+  cudaFree(I->d_stats);
+  cudaFree(I->d_counter);
+  cudaFree(I->d_jscratch);
+  if (I->ev0) cudaEventDestroy(I->ev0);
+  if (I->ev1) cudaEventDestroy(I->ev1);
+  delete I;
+}
+
+bool Engine::ensure(void** p, size_t* cap, size_t bytes, std::string* err) {
+  if (*cap >= bytes && *p) return true;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  CK(cudaMalloc(p, bytes > 0 ? bytes : 16));
+  *cap = bytes;
+  return true;
+}
+
+namespace {
+// packs host vectors into one device blob; returns device pointers
+struct Packer {
+  std::vector<char> blob;
+  std::vector<std::pair<size_t, const void**>> fix;
+  template <typename T>
+  void add(const std::vector<T>& v, const T** dst) {
+    size_t off = (blob.size() + 15) & ~size_t(15);
+    blob.resize(off + std::max<size_t>(v.size(), 1) * sizeof(T), 0);
+    if (!v.empty()) memcpy(blob.data() + off, v.data(), v.size() * sizeof(T));
+    fix.push_back({off, (const void**)dst});
+  }
+};
+}  // namespace
+
+bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int capacity,
+                  std::string* err) {
+  Impl* I = impl_;
+  const Tables& t = model.tables();
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&I->sm_count, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaDeviceGetAttribute(&I->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  DevMech& m = I->m;
+  m.n = t.n;
+  m.n_state = t.n_state;
+  m.n_rxn = t.n_rxn;
+  m.n_part = t.n_part;
+  m.n_jac = t.n_jac;
+  m.n_lu = t.n_lu;
+  m.n_photo = t.n_photo;
+  m.n_flev = t.n_flev;
+  m.n_blev = t.n_blev;
+  std::vector<int> cst;
+  for (int i = 0; i < t.n_state; ++i)
+    if (model.var_type()[i] == VAR_CONSTANT) cst.push_back(i);
+  m.n_const = (int)cst.size();
+  Packer pk;
+  pk.add(t.rx_type, &m.rx_type);
+  pk.add(t.rx_nreact, &m.rx_nreact);
+  pk.add(t.rx_fpar, &m.rx_fpar);
+  pk.add(t.rx_photo, &m.rx_photo);
+  pk.add(t.fpar, &m.fpar);
+  pk.add(t.rx_cptr, &m.rx_cptr);
+  pk.add(t.rx_cidx, &m.rx_cidx);
+  pk.add(t.rx_vptr, &m.rx_vptr);
+  pk.add(t.rx_vdep, &m.rx_vdep);
+  pk.add(t.fg_ptr, &m.fg_ptr);
+  pk.add(t.fg_rxn, &m.fg_rxn);
+  pk.add(t.fg_prod, &m.fg_prod);
+  pk.add(t.fg_coef, &m.fg_coef);
+  pk.add(t.jg_ptr, &m.jg_ptr);
+  pk.add(t.jg_part, &m.jg_part);
+  pk.add(t.jg_ind, &m.jg_ind);
+  pk.add(t.jg_lupos, &m.jg_lupos);
+  pk.add(t.jg_row, &m.jg_row);
+  pk.add(t.jg_coef, &m.jg_coef);
+  pk.add(t.lu_perm, &m.lu_perm);
+  pk.add(t.lu_rowptr, &m.lu_rowptr);
+  pk.add(t.lu_col, &m.lu_col);
+  pk.add(t.lu_diag, &m.lu_diag);
+  pk.add(t.upd_ptr, &m.upd_ptr);
+  pk.add(t.upd_src, &m.upd_src);
+  pk.add(t.upd_dst, &m.upd_dst);
+  pk.add(t.fl_ptr, &m.fl_ptr);
+  pk.add(t.fl_rows, &m.fl_rows);
+  pk.add(t.bl_ptr, &m.bl_ptr);
+  pk.add(t.bl_rows, &m.bl_rows);
+  pk.add(t.dep_state, &m.dep_state);
+  pk.add(cst, &m.const_state);
+  pk.add(atol_dep, &m.atol);
+  if (I->d_tables) cudaFree(I->d_tables);
+  I->d_tables = nullptr;
+  CK(cudaMalloc(&I->d_tables, pk.blob.size()));
+  CK(cudaMemcpy(I->d_tables, pk.blob.data(), pk.blob.size(), cudaMemcpyHostToDevice));
+  for (auto& f : pk.fix) *f.second = (const void*)((char*)I->d_tables + f.first);
+  I->capacity = capacity;
+  I->n_state = t.n_state;
+  I->n_photo = t.n_photo;
+  if (!I->d_counter) CK(cudaMalloc((void**)&I->d_counter, sizeof(int) * 4));
+  if (!I->ev0) {
+    CK(cudaEventCreate(&I->ev0));
+    CK(cudaEventCreate(&I->ev1));
+  }
+  return true;
+}
+
+static Layout make_layout(const DevMech& m, int lt_size) {
+  Layout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = (off + bytes + 15) & ~size_t(15);
+    return (int)o;
+  };
+  const size_t vec = sizeof(double) * m.n;
+  L.zn = take(vec * LMAX);
+  L.ewt = take(vec);
+  L.acor = take(vec);
+  L.y = take(vec);
+  L.ftemp = take(vec);
+  L.tempv = take(vec);
+  L.rates = take(sizeof(double) * std::max(m.n_rxn, m.n_part));
+  L.keff = take(sizeof(double) * m.n_rxn);
+  L.lu = take((size_t)lt_size * m.n_lu);
+  L.z = take((size_t)lt_size * m.n);
+  L.bytes = (int)off;
+  return L;
+}
+
+bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_photo,
+                          const int* d_order, int n_cells, double t0, double t1,
+                          const SolveSettings& s, void* stream, std::string* err) {
+  Impl* I = impl_;
+  if (n_cells <= 0) return true;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int lt = s.precision == 1 ? 4 : 8;
+  Layout lay = make_layout(I->m, lt);
+  int max_warps = I->max_smem / lay.bytes;
+  if (max_warps < 1) {
+    *err = "mechanism too large for the shared-memory layout (" +
+           std::to_string(lay.bytes) + " bytes per cell)";
+    return false;
+  }
+  int warps = s.warps_per_block > 0 ? std::min(s.warps_per_block, max_warps) : max_warps;
+  warps = std::min(warps, 16);
+  int bps = std::max(1, s.blocks_per_sm);
+  while (bps > 1 && (size_t)bps * warps * lay.bytes > (size_t)I->max_smem) --bps;
+  int grid = I->sm_count * bps;
+  // no more warps than cells
+  long total_warps = (long)grid * warps;
+  if (total_warps > n_cells) grid = std::max(1, (int)((n_cells + warps - 1) / warps));
+  total_warps = (long)grid * warps;
+  if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
+  if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)lt * I->m.n_jac * total_warps, err))
+    return false;
+  CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
+  SolveArgs a;
+  a.m = I->m;
+  a.lay = lay;
+  a.state = d_state;
+  a.env = d_env;
+  a.photo = I->m.n_photo > 0 ? d_photo : nullptr;
+  a.order = d_order;
+  a.n_cells = n_cells;
+  a.counter = I->d_counter;
+  a.stats = (CellStats*)I->d_stats;
+  a.jscratch = I->d_jscratch;
+  a.t0 = t0;
+  a.t1 = t1;
+  a.rtol = s.rtol;
+  a.max_steps = s.max_steps;
+  a.maxncf = s.max_conv_fails;
+  a.maxnef = s.max_conv_fails;
+  size_t smem = (size_t)warps * lay.bytes;
+  CK(cudaEventRecord(I->ev0, st));
+  if (s.precision == 1) {
+    CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    solve_kernel<float><<<grid, warps * 32, smem, st>>>(a);
+  } else {
+    CK(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    solve_kernel<double><<<grid, warps * 32, smem, st>>>(a);
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(I->ev1, st));
+  I->ev_pending = true;
+  ++launches_;
+  return true;
+}
+
+bool Engine::read_last_ms(void* stream) {
+  (void)stream;
+  Impl* I = impl_;
+  if (!I->ev_pending) return true;
+  if (cudaEventSynchronize(I->ev1) != cudaSuccess) return false;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, I->ev0, I->ev1);
+  last_ms_ = ms;
+  I->ev_pending = false;
+  return true;
+}
+
+bool Engine::fetch_stats(std::vector<CellStats>* out, int n_cells, void* stream,
+                         std::string* err) {
+  Impl* I = impl_;
+  out->resize(n_cells);
+  if (n_cells <= 0) return true;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(out->data(), I->d_stats, sizeof(CellStats) * n_cells,
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  read_last_ms(stream);
+  return true;
+}
+
+bool Engine::sync(void* stream, std::string* err) {
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  read_last_ms(stream);
+  return true;
+}
+
+double* Engine::d_state_buf(int n_cells, std::string* err) {
+  if (!ensure(&impl_->d_state, &impl_->c_state, sizeof(double) * (size_t)n_cells * impl_->n_state,
+              err))
+    return nullptr;
+  return (double*)impl_->d_state;
+}
+double* Engine::d_env_buf(int n_cells, std::string* err) {
+  if (!ensure(&impl_->d_env, &impl_->c_env, sizeof(double) * 2 * (size_t)n_cells, err))
+    return nullptr;
+  return (double*)impl_->d_env;
+}
+double* Engine::d_photo_buf(int n_cells, std::string* err) {
+  if (!ensure(&impl_->d_photo, &impl_->c_photo,
+              sizeof(double) * (size_t)n_cells * std::max(1, impl_->n_photo), err))
+    return nullptr;
+  return (double*)impl_->d_photo;
+}
+int* Engine::d_order_buf(int n_cells, std::string* err) {
+  if (!ensure(&impl_->d_order, &impl_->c_order, sizeof(int) * (size_t)n_cells, err))
+    return nullptr;
+  return (int*)impl_->d_order;
+}
+
+bool Engine::eval_deriv(const double* h_state, const double* h_env, const double* h_photo,
+                        int n_cells, double h, double* r_p, double* r_l, double* f,
+                        std::string* err) {
+  Impl* I = impl_;
+  const DevMech& m = I->m;
+  size_t ns = (size_t)n_cells * m.n_state, nn = (size_t)n_cells * m.n;
+  double *ds = nullptr, *de = nullptr, *dp = nullptr, *dout = nullptr;
+  CK(cudaMalloc(&ds, sizeof(double) * ns));
+  CK(cudaMalloc(&de, sizeof(double) * 2 * n_cells));
+  CK(cudaMalloc(&dp, sizeof(double) * std::max<size_t>(1, (size_t)n_cells * m.n_photo)));
+  CK(cudaMalloc(&dout, sizeof(double) * 3 * nn));
+  CK(cudaMemcpy(ds, h_state, sizeof(double) * ns, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(de, h_env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice));
+  if (m.n_photo > 0 && h_photo)
+    CK(cudaMemcpy(dp, h_photo, sizeof(double) * n_cells * m.n_photo, cudaMemcpyHostToDevice));
+  EvalArgs a{};
+  a.m = m;
+  a.lay = make_layout(m, 8);
+  a.state = ds;
+  a.env = de;
+  a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
+  a.n_cells = n_cells;
+  a.h = h;
+  a.rp = dout;
+  a.rl = dout + nn;
+  a.f = dout + 2 * nn;
+  a.do_jac = 0;
+  int warps = std::max(1, std::min(8, I->max_smem / a.lay.bytes));
+  size_t smem = (size_t)warps * a.lay.bytes;
+  CK(cudaFuncSetAttribute(eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  eval_kernel<<<(n_cells + warps - 1) / warps, warps * 32, smem>>>(a);
+  CK(cudaGetLastError());
+  ++launches_;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(r_p, a.rp, sizeof(double) * nn, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(r_l, a.rl, sizeof(double) * nn, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(f, a.f, sizeof(double) * nn, cudaMemcpyDeviceToHost));
+  cudaFree(ds);
+  cudaFree(de);
+  cudaFree(dp);
+  cudaFree(dout);
+  return true;
+}
+
+bool Engine::eval_jac(const double* h_state, const double* h_env, const double* h_photo,
+                      int n_cells, double h, double* jp, double* jl, std::string* err) {
+  Impl* I = impl_;
+  const DevMech& m = I->m;
+  size_t ns = (size_t)n_cells * m.n_state, nj = (size_t)n_cells * m.n_jac;
+  double *ds = nullptr, *de = nullptr, *dp = nullptr, *dout = nullptr;
+  CK(cudaMalloc(&ds, sizeof(double) * ns));
+  CK(cudaMalloc(&de, sizeof(double) * 2 * n_cells));
+  CK(cudaMalloc(&dp, sizeof(double) * std::max<size_t>(1, (size_t)n_cells * m.n_photo)));
+  CK(cudaMalloc(&dout, sizeof(double) * 3 * nj));
+  CK(cudaMemcpy(ds, h_state, sizeof(double) * ns, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(de, h_env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice));
+  if (m.n_photo > 0 && h_photo)
+    CK(cudaMemcpy(dp, h_photo, sizeof(double) * n_cells * m.n_photo, cudaMemcpyHostToDevice));
+  EvalArgs a{};
+  a.m = m;
+  a.lay = make_layout(m, 8);
+  a.state = ds;
+  a.env = de;
+  a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
+  a.n_cells = n_cells;
+  a.h = h;
+  a.jp = dout;
+  a.jl = dout + nj;
+  a.jv = dout + 2 * nj;
+  a.do_jac = 1;
+  int warps = std::max(1, std::min(8, I->max_smem / a.lay.bytes));
+  size_t smem = (size_t)warps * a.lay.bytes;
+  CK(cudaFuncSetAttribute(eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  eval_kernel<<<(n_cells + warps - 1) / warps, warps * 32, smem>>>(a);
+  CK(cudaGetLastError());
+  ++launches_;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(jp, a.jp, sizeof(double) * nj, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(jl, a.jl, sizeof(double) * nj, cudaMemcpyDeviceToHost));
+  cudaFree(ds);
+  cudaFree(de);
+  cudaFree(dp);
+  cudaFree(dout);
+  return true;
+}
+
+}  // namespace campb

@@ -1,0 +1,247 @@
+"""Python host API over libcamp_b200 — the mirror of ``camp_solver_data_t``.
+
+The reference's Fortran ``camp_solver_data_t`` (src/camp_solver_data.F90)
+creates the C solver with ``solver_new``, feeds it every reaction's packed
+data with ``rxn_add_condensed_data``, calls ``solver_initialize`` and then
+``solver_run`` once per host time step, and pushes per-cell photolysis rates
+through ``rxn_update_data``.  :class:`Solver` makes the same calls, in the
+same order, through the C ABI of ``libcamp_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .mechanism import RXN_PHOTOLYSIS, Mechanism
+
+# solver defaults, src/camp_solver_data.F90:33-37
+DEFAULT_MAX_STEPS = 10000
+DEFAULT_MAX_CONV_FAILS = 1000
+
+FP64 = 0
+MIXED = 1
+
+
+class SolverError(RuntimeError):
+    pass
+
+
+class Solver:
+    """One CAMP solver instance for ``n_cells`` cells of ``mech``."""
+
+    def __init__(self, mech: Mechanism, n_cells: int):
+        self.lib = _lib.load()
+        self.mech = mech
+        self.n_cells = int(n_cells)
+        self._h = self.lib.solver_new(
+            mech.n_state_var, self.n_cells, np.ascontiguousarray(mech.var_type, np.int32),
+            mech.n_rxn, mech.n_rxn_int_param, mech.n_rxn_float_param, mech.n_rxn_env_param,
+            0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+        )
+        if not self._h:
+            raise SolverError(_lib.last_error())
+        for r in mech.rxns:
+            self.lib.rxn_add_condensed_data(
+                r.rxn_type, r.ints.size, r.floats.size, r.n_env,
+                np.ascontiguousarray(r.ints, np.int32), np.ascontiguousarray(r.floats, np.float64),
+                self._h,
+            )
+        self.ready = False
+
+    # ------------------------------------------------------------------
+    def initialize(self, abs_tol=None, rel_tol: float | None = None,
+                   max_steps: int = DEFAULT_MAX_STEPS,
+                   max_conv_fails: int = DEFAULT_MAX_CONV_FAILS) -> None:
+        """solver_initialize; abs_tol per state variable (default: mechanism's)."""
+        atol = np.ascontiguousarray(self.mech.abs_tol if abs_tol is None else abs_tol, np.float64)
+        if atol.size == 1:
+            atol = np.full(self.mech.n_state_var, float(atol))
+        rtol = self.mech.rel_tol if rel_tol is None else float(rel_tol)
+        self.rtol = rtol
+        self.atol = atol
+        self.lib.solver_initialize(self._h, atol, rtol, int(max_steps), int(max_conv_fails))
+        self.ready = bool(self.lib.camp_b200_is_ready(self._h))
+        if not self.ready:
+            raise SolverError(_lib.last_error())
+
+    def build_sparsity_only(self, abs_tol=None, rel_tol=None) -> None:
+        """solver_initialize without requiring a GPU: the host-side sparsity
+        and packed-data update are done before any device work, so they can be
+        inspected on a machine without CUDA devices."""
+        atol = np.ascontiguousarray(self.mech.abs_tol if abs_tol is None else abs_tol, np.float64)
+        rtol = self.mech.rel_tol if rel_tol is None else float(rel_tol)
+        self.lib.solver_initialize(self._h, atol, rtol, DEFAULT_MAX_STEPS, DEFAULT_MAX_CONV_FAILS)
+        self.ready = bool(self.lib.camp_b200_is_ready(self._h))
+
+    def set_precision(self, mode: int) -> None:
+        if self.lib.camp_b200_set_precision(self._h, int(mode)) != 0:
+            raise SolverError(_lib.last_error())
+
+    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 1) -> None:
+        self.lib.camp_b200_set_launch(self._h, int(warps_per_block), int(blocks_per_sm))
+
+    def set_cost_ordering(self, enable: bool = True) -> None:
+        self.lib.camp_b200_set_cost_ordering(self._h, 1 if enable else 0)
+
+    # ------------------------------------------------------------------
+    def solve(self, state: np.ndarray, env: np.ndarray, t_initial: float, t_final: float) -> int:
+        """solver_run on host arrays; state [n_cells, n_state_var] in place."""
+        if state.dtype != np.float64 or not state.flags.c_contiguous:
+            raise TypeError("state must be a C-contiguous float64 array")
+        env = np.ascontiguousarray(env, np.float64)
+        return int(self.lib.solver_run(self._h, state.reshape(-1), env.reshape(-1),
+                                       float(t_initial), float(t_final)))
+
+    def run_device(self, d_state, d_env, n_cells: int, t_initial: float, t_final: float,
+                   stream=None) -> int:
+        """Device-resident run; d_state/d_env are torch CUDA tensors or raw
+        device pointers (int)."""
+        ps = d_state.data_ptr() if hasattr(d_state, "data_ptr") else int(d_state)
+        pe = d_env.data_ptr() if hasattr(d_env, "data_ptr") else int(d_env)
+        st = None
+        if stream is not None:
+            st = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        rc = self.lib.camp_b200_run_device(self._h, ps, pe, int(n_cells), float(t_initial),
+                                           float(t_final), st)
+        if rc < 0:
+            raise SolverError(_lib.last_error())
+        return rc
+
+    def launch_device(self, d_state, d_env, n_cells: int, t_initial: float, t_final: float,
+                      stream=None) -> None:
+        ps = d_state.data_ptr() if hasattr(d_state, "data_ptr") else int(d_state)
+        pe = d_env.data_ptr() if hasattr(d_env, "data_ptr") else int(d_env)
+        st = None
+        if stream is not None:
+            st = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        if self.lib.camp_b200_launch_device(self._h, ps, pe, int(n_cells), float(t_initial),
+                                            float(t_final), st) < 0:
+            raise SolverError(_lib.last_error())
+
+    def sync_status(self, stream=None) -> int:
+        st = None
+        if stream is not None:
+            st = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        rc = self.lib.camp_b200_sync_status(self._h, st)
+        if rc < 0:
+            raise SolverError(_lib.last_error())
+        return rc
+
+    # ------------------------------------------------------------------
+    def set_photo_rate(self, cell: int, photo_id: int, base_rate: float) -> None:
+        """Photolysis update through the reference's rxn_update_data path."""
+        ud = self.lib.rxn_photolysis_create_rate_update_data()
+        self.lib.rxn_photolysis_set_rate_update_data(ud, int(photo_id), float(base_rate))
+        cursor = C.c_int(0)
+        self.lib.rxn_update_data(int(cell), C.byref(cursor), RXN_PHOTOLYSIS, ud, self._h)
+        self.lib.solver_free_update_data(ud)
+
+    @property
+    def n_photo(self) -> int:
+        return int(self.lib.camp_b200_n_photo(self._h))
+
+    def set_photo_rates(self, rates: np.ndarray) -> None:
+        """Base rates [n_cells, n_photo] for photolysis ids 1..n_photo.
+
+        Ids are assigned in mechanism order, so id j+1 is photolysis reaction
+        j; this sets the same values a loop of rxn_update_data calls would."""
+        rates = np.ascontiguousarray(rates, np.float64)
+        n = rates.shape[0]
+        if rates.shape[1] != self.n_photo:
+            raise ValueError("rates must have one column per photolysis reaction")
+        self.lib.camp_b200_set_photo_rates(self._h, rates.reshape(-1), n)
+
+    # ------------------------------------------------------------------
+    def statistics(self) -> dict:
+        ints = [C.c_int() for _ in range(9)]
+        dbl = [C.c_double() for _ in range(2)]
+        ints2 = [C.c_int() for _ in range(3)]
+        dbl2 = [C.c_double() for _ in range(3)]
+        self.lib.solver_get_statistics(self._h, *[C.byref(x) for x in ints],
+                                       *[C.byref(x) for x in dbl], *[C.byref(x) for x in ints2],
+                                       *[C.byref(x) for x in dbl2])
+        keys = ["solver_flag", "num_steps", "RHS_evals", "LS_setups", "error_test_fails",
+                "NLS_iters", "NLS_convergence_fails", "DLS_Jac_evals", "DLS_RHS_evals"]
+        out = {k: v.value for k, v in zip(keys, ints)}
+        out["last_time_step__s"] = dbl[0].value
+        out["next_time_step__s"] = dbl[1].value
+        out.update({k: v.value for k, v in zip(["Jac_eval_fails", "RHS_evals_total",
+                                                 "Jac_evals_total"], ints2)})
+        out.update({k: v.value for k, v in zip(["RHS_time__s", "Jac_time__s",
+                                                 "max_loss_precision"], dbl2)})
+        return out
+
+    def cell_stats(self, n_cells: int | None = None) -> np.ndarray:
+        n = self.n_cells if n_cells is None else int(n_cells)
+        arr = (_lib.CellStats * n)()
+        self.lib.camp_b200_get_cell_stats(self._h, arr, n)
+        dt = np.dtype([("status", np.int32), ("nst", np.int32), ("nfe", np.int32),
+                       ("nsetups", np.int32), ("netf", np.int32), ("nni", np.int32),
+                       ("ncfn", np.int32), ("nje", np.int32), ("hu", np.float64),
+                       ("hcur", np.float64)])
+        return np.frombuffer(bytes(arr), dtype=dt).copy()
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.camp_b200_kernel_launches(self._h))
+
+    def last_kernel_ms(self) -> float:
+        return float(self.lib.camp_b200_last_kernel_ms(self._h))
+
+    # ------------------------------------------------------------------
+    def solver_jac(self):
+        n = self.lib.camp_b200_n_dep_var(self._h)
+        nnz = self.lib.camp_b200_n_jac_elem(self._h)
+        cp = np.zeros(n + 1, np.int32)
+        ri = np.zeros(max(nnz, 1), np.int32)
+        if self.lib.camp_b200_get_solver_jac(self._h, cp, ri) != 0:
+            raise SolverError("sparsity not built")
+        return cp, ri[:nnz]
+
+    def rxn_int_data(self) -> np.ndarray:
+        out = np.zeros(self.lib.camp_b200_rxn_int_data_size(self._h), np.int32)
+        self.lib.camp_b200_get_rxn_int_data(self._h, out)
+        return out
+
+    def lu_order(self) -> np.ndarray:
+        out = np.zeros(self.lib.camp_b200_n_dep_var(self._h), np.int32)
+        self.lib.camp_b200_get_lu_order(self._h, out)
+        return out
+
+    def n_lu(self) -> int:
+        return int(self.lib.camp_b200_n_lu_elem(self._h))
+
+    def eval_deriv(self, state, env, h):
+        state = np.ascontiguousarray(state, np.float64)
+        nc = state.shape[0]
+        n = self.lib.camp_b200_n_dep_var(self._h)
+        rp, rl, f = (np.zeros(nc * n) for _ in range(3))
+        if self.lib.camp_b200_eval_deriv(self._h, state.reshape(-1),
+                                         np.ascontiguousarray(env, np.float64).reshape(-1),
+                                         nc, float(h), rp, rl, f) != 0:
+            raise SolverError(_lib.last_error())
+        return f.reshape(nc, n), rp.reshape(nc, n), rl.reshape(nc, n)
+
+    def eval_jac(self, state, env, h):
+        state = np.ascontiguousarray(state, np.float64)
+        nc = state.shape[0]
+        nnz = self.lib.camp_b200_n_jac_elem(self._h)
+        jp, jl = np.zeros(nc * nnz), np.zeros(nc * nnz)
+        if self.lib.camp_b200_eval_jac(self._h, state.reshape(-1),
+                                       np.ascontiguousarray(env, np.float64).reshape(-1),
+                                       nc, float(h), jp, jl) != 0:
+            raise SolverError(_lib.last_error())
+        jp, jl = jp.reshape(nc, nnz), jl.reshape(nc, nnz)
+        return jp - jl, jp, jl
+
+    def free(self) -> None:
+        if self._h:
+            self.lib.solver_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

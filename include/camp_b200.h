@@ -1,0 +1,205 @@
+/* libcamp_b200 — drop-in C ABI for CAMP's per-cell chemistry solve on B200.
+ *
+ * The first group of entry points keeps the names, argument meaning and
+ * error behaviour of the reference's C solver interface, so the reference's
+ * Fortran caller (src/camp_solver_data.F90:43-363, bind(c)) links against
+ * this library unchanged.  Each declaration cites the reference interface it
+ * replaces.  The second group (camp_b200_*) is this library's own extension
+ * API: device-resident runs, precision selection, per-cell status and the
+ * evaluation hooks the parity tests use.
+ *
+ * Per-cell semantics: every grid cell is integrated independently with its
+ * own BDF step size and order (the reference couples all cells of a call into
+ * one CVODE system, src/camp_solver.c:145).  solver_run returns 1 if any cell
+ * failed; failed cells keep their input state.
+ */
+#ifndef CAMP_B200_H
+#define CAMP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Reference-compatible entry points                                        */
+/* ---------------------------------------------------------------------- */
+
+/* replaces src/camp_solver.c:83 (declared src/camp_solver.h:16-24) */
+void *solver_new(int n_state_var, int n_cells, int *var_type, int n_rxn,
+                 int n_rxn_int_param, int n_rxn_float_param,
+                 int n_rxn_env_param, int n_aero_phase,
+                 int n_aero_phase_int_param, int n_aero_phase_float_param,
+                 int n_aero_rep, int n_aero_rep_int_param,
+                 int n_aero_rep_float_param, int n_aero_rep_env_param,
+                 int n_sub_model, int n_sub_model_int_param,
+                 int n_sub_model_float_param, int n_sub_model_env_param);
+
+/* replaces src/camp_solver.c:374 (src/camp_solver.h:25-26) */
+void solver_initialize(void *solver_data, double *abs_tol, double rel_tol,
+                       int max_steps, int max_conv_fails);
+
+/* replaces src/camp_solver.c:544 (src/camp_solver.h:31-32); 0 = success,
+ * 1 = at least one cell failed */
+int solver_run(void *solver_data, double *state, double *env, double t_initial,
+               double t_final);
+
+/* replaces src/camp_solver.c:725 (src/camp_solver.h:33-40).  Counters are the
+ * maximum over the cells of the last run (the per-cell analogue of the single
+ * coupled CVODE's counters); per-cell values come from
+ * camp_b200_get_cell_stats. */
+void solver_get_statistics(void *solver_data, int *solver_flag, int *num_steps,
+                           int *RHS_evals, int *LS_setups,
+                           int *error_test_fails, int *NLS_iters,
+                           int *NLS_convergence_fails, int *DLS_Jac_evals,
+                           int *DLS_RHS_evals, double *last_time_step__s,
+                           double *next_time_step__s, int *Jac_eval_fails,
+                           int *RHS_evals_total, int *Jac_evals_total,
+                           double *RHS_time__s, double *Jac_time__s,
+                           double *max_loss_precision);
+
+/* replaces src/camp_solver.c:1764 */
+void solver_reset_timers(void *solver_data);
+/* replaces src/camp_solver.c:1832 */
+void solver_free(void *solver_data);
+/* replaces src/camp_solver.c:1962 */
+void solver_free_update_data(void *update_data);
+
+/* replace src/camp_solver.c:502 and :522 (CAMP_DEBUG builds of the
+ * reference); accepted and recorded, they change nothing here */
+int solver_set_debug_out(void *solver_data, int do_output);
+int solver_set_eval_jac(void *solver_data, int eval_Jac);
+
+/* replaces src/rxn_solver.c:658 (src/rxn_solver.h) */
+void rxn_add_condensed_data(int rxn_type, int n_int_param, int n_float_param,
+                            int n_env_param, int *int_param,
+                            double *float_param, void *solver_data);
+/* replaces src/rxn_solver.c:708; rxn_id is the in/out cursor of the
+ * reference: the search starts at *rxn_id and stops at the first reaction
+ * that accepts the update */
+void rxn_update_data(int cell_id, int *rxn_id, int update_rxn_type,
+                     void *update_data, void *solver_data);
+/* replaces src/rxn_solver.c:769 */
+void rxn_print_data(void *solver_data);
+/* replaces src/rxn_solver.c:851 */
+void rxn_free_update_data(void *update_data);
+/* replace src/rxns/rxn_photolysis.c:262-283 (bound from
+ * src/rxns/rxn_photolysis.F90:135-152) */
+void *rxn_photolysis_create_rate_update_data(void);
+void rxn_photolysis_set_rate_update_data(void *update_data, int photo_id,
+                                         double base_rate);
+
+/* replace src/aero_phase_solver.c:175,210, src/aero_rep_solver.c:443,492,546
+ * and src/sub_model_solver.c:413,468,509.  Data is accepted; a model with
+ * aerosol phases, representations or sub-models is rejected at
+ * solver_initialize in this build (gas-phase chemistry only). */
+void aero_phase_add_condensed_data(int n_int_param, int n_float_param,
+                                   int *int_param, double *float_param,
+                                   void *solver_data);
+void aero_rep_add_condensed_data(int aero_rep_type, int n_int_param,
+                                 int n_float_param, int n_env_param,
+                                 int *int_param, double *float_param,
+                                 void *solver_data);
+void aero_rep_update_data(int cell_id, int *aero_rep_id, int update_aero_rep_type,
+                          void *update_data, void *solver_data);
+void sub_model_add_condensed_data(int sub_model_type, int n_int_param,
+                                  int n_float_param, int n_env_param,
+                                  int *int_param, double *float_param,
+                                  void *solver_data);
+void sub_model_update_data(int cell_id, int *sub_model_id,
+                           int update_sub_model_type, void *update_data,
+                           void *solver_data);
+void aero_phase_print_data(void *solver_data);
+void aero_rep_print_data(void *solver_data);
+void sub_model_print_data(void *solver_data);
+
+/* ---------------------------------------------------------------------- */
+/* Extension API                                                            */
+/* ---------------------------------------------------------------------- */
+
+/* precision modes */
+#define CAMP_B200_FP64 0  /* everything in FP64 */
+#define CAMP_B200_MIXED 1 /* FP32 Jacobian and LU, FP64 residual/state/error test */
+
+/* per-cell status codes (CVODE flag values) */
+#define CAMP_B200_OK 0
+#define CAMP_B200_TOO_MUCH_WORK (-1)
+#define CAMP_B200_TOO_MUCH_ACC (-2)
+#define CAMP_B200_ERR_FAILURE (-3)
+#define CAMP_B200_CONV_FAILURE (-4)
+#define CAMP_B200_LSETUP_FAIL (-6)
+#define CAMP_B200_RHSFUNC_FAIL (-8)
+#define CAMP_B200_REPTD_RHSFUNC_ERR (-10)
+#define CAMP_B200_UNREC_RHSFUNC_ERR (-11)
+#define CAMP_B200_ILL_INPUT (-22)
+#define CAMP_B200_NOT_RUN (-99)
+
+/* per-cell counters of the last run */
+typedef struct {
+  int status;
+  int nst, nfe, nsetups, netf, nni, ncfn, nje;
+  double hu, hcur;
+} camp_b200_cell_stats;
+
+/* Last error message of this thread ("" if none). */
+const char *camp_b200_last_error(void);
+/* 1 if the solver finished solver_initialize without error. */
+int camp_b200_is_ready(void *solver_data);
+
+int camp_b200_set_precision(void *solver_data, int mode);
+/* cells per block (warps per block); 0 = automatic */
+int camp_b200_set_launch(void *solver_data, int warps_per_block, int blocks_per_sm);
+/* Orders the cells of the next run by decreasing internal step count of the
+ * previous run (longest-first scheduling of the persistent kernel). */
+int camp_b200_set_cost_ordering(void *solver_data, int enable);
+
+/* Runs on caller-owned device buffers (state [n_cells*n_state_var], env
+ * [n_cells*2]) on the given cudaStream_t (NULL = default stream) without host
+ * copies; n_cells may be below the capacity given to solver_new.  Returns 0
+ * or 1 like solver_run after the stream has been synchronised, or -1 on a
+ * usage error. */
+int camp_b200_run_device(void *solver_data, double *d_state, const double *d_env,
+                         int n_cells, double t_initial, double t_final,
+                         void *stream);
+/* Same, but returns right after the launch (no synchronisation, status not
+ * read back).  Use camp_b200_sync_status afterwards. */
+int camp_b200_launch_device(void *solver_data, double *d_state,
+                            const double *d_env, int n_cells, double t_initial,
+                            double t_final, void *stream);
+int camp_b200_sync_status(void *solver_data, void *stream);
+
+/* Per-cell photolysis base rates: rates[c * n_photo + j] for photolysis
+ * reaction j (mechanism order) of cell c, as if rxn_update_data had been
+ * called for every cell and reaction. */
+int camp_b200_n_photo(void *solver_data);
+int camp_b200_set_photo_rates(void *solver_data, const double *rates, int n_cells);
+
+int camp_b200_get_cell_stats(void *solver_data, camp_b200_cell_stats *out, int n_cells);
+/* number of GPU kernel launches made by this solver since creation */
+long camp_b200_kernel_launches(void *solver_data);
+/* duration of the last solve kernel in ms (CUDA events on its stream) */
+double camp_b200_last_kernel_ms(void *solver_data);
+
+/* Sparsity and data after solver_initialize (for parity tests). */
+int camp_b200_n_dep_var(void *solver_data);
+int camp_b200_n_jac_elem(void *solver_data);
+int camp_b200_n_lu_elem(void *solver_data);
+int camp_b200_rxn_int_data_size(void *solver_data);
+int camp_b200_get_solver_jac(void *solver_data, int *col_ptrs, int *row_ids);
+int camp_b200_get_rxn_int_data(void *solver_data, int *out);
+int camp_b200_get_lu_order(void *solver_data, int *perm);
+
+/* Device evaluation of the derivative and Jacobian for n_cells states (host
+ * buffers), through the same device code the solver uses: rate constants
+ * from env and the photolysis rates set for those cells, then f (production,
+ * loss, net) and the solver Jacobian (CSC order of camp_b200_get_solver_jac,
+ * production and loss parts) at time step h. */
+int camp_b200_eval_deriv(void *solver_data, const double *state, const double *env,
+                         int n_cells, double h, double *r_p, double *r_l,
+                         double *deriv);
+int camp_b200_eval_jac(void *solver_data, const double *state, const double *env,
+                       int n_cells, double h, double *j_prod, double *j_loss);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1434 @@
+/* CPU oracle for the CAMP per-cell chemistry solve (TEST INFRASTRUCTURE).
+ * See camp_oracle.h for what is restated from where.  Nothing in the product
+ * links this file; it exists to check the CUDA path and to time the CPU
+ * baseline. */
+#include "camp_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* constants of src/camp_common.h:34-45 */
+#define VAR_VARIABLE 1
+#define SMALL 1.0e-30
+#define TINY 1.0e-60
+
+/* reaction type ids, src/rxn_solver.c:19-35 */
+#define T_ARRHENIUS 1
+#define T_TROE 2
+#define T_CMAQ_H2O2 3
+#define T_CMAQ_OH_HNO3 4
+#define T_PHOTOLYSIS 5
+
+static void *zalloc(size_t n) {
+  void *p = calloc(n ? n : 1, 1);
+  if (!p) {
+    fprintf(stderr, "camp_oracle: out of memory\n");
+    exit(EXIT_FAILURE);
+  }
+  return p;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Mechanism                                                                 */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int type;
+  int nr, np;
+  int n_int_prop;      /* 2, or 3 for photolysis (RXN_ID) */
+  int *ints;           /* points at NUM_REACT_ inside the packed int data */
+  const double *fl;    /* packed float data of this reaction */
+  int n_float_prop;
+  int env_off;
+} ORxn;
+
+#define R_REACT(r, x) ((r)->ints[(r)->n_int_prop + (x)] - 1)
+#define R_PROD(r, x) ((r)->ints[(r)->n_int_prop + (r)->nr + (x)] - 1)
+#define R_DERIV_ID(r, x) ((r)->ints[(r)->n_int_prop + (r)->nr + (r)->np + (x)])
+#define R_JAC_ID(r, x) \
+  ((r)->ints[(r)->n_int_prop + 2 * ((r)->nr + (r)->np) + (x)])
+#define R_YIELD(r, x) ((r)->fl[(r)->n_float_prop + (x)])
+
+typedef struct {
+  int n;          /* dimension (dependent variables) */
+  int nnz;        /* entries of L+U */
+  int *perm;      /* pivot k -> original index */
+  int *iperm;     /* original index -> pivot position */
+  int *rowptr;    /* n+1, rows in pivot order */
+  int *colidx;    /* column (pivot order), ascending within a row */
+  int *diag;      /* position of the diagonal in each row */
+  int *a_to_lu;   /* solver CSC element -> LU position */
+} LUSym;
+
+struct OracleMech {
+  int n_state, n_dep, n_rxn, n_added;
+  int *var_type;
+  int *int_data, int_size, int_cap;
+  double *float_data;
+  int float_size, float_cap;
+  int n_env;
+  ORxn *rx;
+  int built;
+  int *deriv_ids;
+  int n_rxn_jac;
+  int *rj_colptr, *rj_rowid;
+  int n_solver_jac;
+  int *sj_colptr, *sj_rowid;
+  int *rxn_to_solver;
+  LUSym lu;
+};
+
+OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn) {
+  OracleMech *m = (OracleMech *)zalloc(sizeof(OracleMech));
+  m->n_state = n_state_var;
+  m->n_rxn = n_rxn;
+  m->var_type = (int *)zalloc(sizeof(int) * n_state_var);
+  for (int i = 0; i < n_state_var; ++i) {
+    m->var_type[i] = var_type[i];
+    if (var_type[i] == VAR_VARIABLE) m->n_dep++;
+  }
+  m->rx = (ORxn *)zalloc(sizeof(ORxn) * (n_rxn + 1));
+  return m;
+}
+
+/* Mirrors rxn_add_condensed_data (src/rxn_solver.c:658-700): the type id is
+ * stored ahead of the reaction's ints, and the float and env offsets advance
+ * by the reaction's sizes. */
+int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
+               const int *ints, const double *floats) {
+  if (m->n_added >= m->n_rxn) return 1;
+  if (type < T_ARRHENIUS || type > T_PHOTOLYSIS) return 2;
+  if (m->int_size + n_int + 1 > m->int_cap) {
+    m->int_cap = 2 * (m->int_size + n_int + 1) + 64;
+    m->int_data = (int *)realloc(m->int_data, sizeof(int) * m->int_cap);
+  }
+  if (m->float_size + n_float > m->float_cap) {
+    m->float_cap = 2 * (m->float_size + n_float) + 64;
+    m->float_data =
+        (double *)realloc(m->float_data, sizeof(double) * m->float_cap);
+  }
+  ORxn *r = &m->rx[m->n_added];
+  r->type = type;
+  r->env_off = m->n_env;
+  /* offsets only for now: the arrays may still move on realloc */
+  r->ints = (int *)(size_t)(m->int_size + 1);
+  r->fl = (const double *)(size_t)m->float_size;
+  m->int_data[m->int_size] = type;
+  memcpy(m->int_data + m->int_size + 1, ints, sizeof(int) * n_int);
+  memcpy(m->float_data + m->float_size, floats, sizeof(double) * n_float);
+  m->int_size += n_int + 1;
+  m->float_size += n_float;
+  m->n_env += n_env;
+  m->n_added++;
+  return 0;
+}
+
+/* --- Jacobian element registry (restates src/Jacobian.c:105-214) -------- */
+typedef struct {
+  int n;
+  int *cnt, *cap;
+  int **rows;
+  int *colptr, *rowid, nnz;
+} JacReg;
+
+static void jr_init(JacReg *j, int n) {
+  j->n = n;
+  j->cnt = (int *)zalloc(sizeof(int) * n);
+  j->cap = (int *)zalloc(sizeof(int) * n);
+  j->rows = (int **)zalloc(sizeof(int *) * n);
+  j->colptr = NULL;
+  j->rowid = NULL;
+  j->nnz = 0;
+}
+/* a (dep, ind) pair is kept once per column */
+static void jr_register(JacReg *j, int dep, int ind) {
+  for (int i = 0; i < j->cnt[ind]; ++i)
+    if (j->rows[ind][i] == dep) return;
+  if (j->cnt[ind] == j->cap[ind]) {
+    j->cap[ind] = j->cap[ind] ? 2 * j->cap[ind] : 8;
+    j->rows[ind] = (int *)realloc(j->rows[ind], sizeof(int) * j->cap[ind]);
+  }
+  j->rows[ind][j->cnt[ind]++] = dep;
+}
+static int cmp_int(const void *a, const void *b) {
+  int x = *(const int *)a, y = *(const int *)b;
+  return (x > y) - (x < y);
+}
+/* rows sorted ascending within each column, columns in index order */
+static void jr_build(JacReg *j) {
+  j->nnz = 0;
+  for (int c = 0; c < j->n; ++c) {
+    qsort(j->rows[c], (size_t)j->cnt[c], sizeof(int), cmp_int);
+    j->nnz += j->cnt[c];
+  }
+  j->colptr = (int *)zalloc(sizeof(int) * (j->n + 1));
+  j->rowid = (int *)zalloc(sizeof(int) * (j->nnz + 1));
+  int e = 0;
+  for (int c = 0; c < j->n; ++c) {
+    j->colptr[c] = e;
+    for (int i = 0; i < j->cnt[c]; ++i) j->rowid[e++] = j->rows[c][i];
+    free(j->rows[c]);
+  }
+  j->colptr[j->n] = e;
+  free(j->rows);
+  free(j->cnt);
+  free(j->cap);
+  j->rows = NULL;
+  j->cnt = j->cap = NULL;
+}
+static int jr_elem_id(const int *colptr, const int *rowid, int dep, int ind) {
+  for (int e = colptr[ind]; e < colptr[ind + 1]; ++e)
+    if (rowid[e] == dep) return e;
+  return -1;
+}
+
+/* --- LU symbolic: Markowitz order over diagonal pivots ------------------- */
+static void lu_symbolic(LUSym *lu, int n, const int *colptr, const int *rowid) {
+  unsigned char *P = (unsigned char *)zalloc((size_t)n * n);
+  for (int c = 0; c < n; ++c)
+    for (int e = colptr[c]; e < colptr[c + 1]; ++e) P[rowid[e] * n + c] = 1;
+  for (int i = 0; i < n; ++i) P[i * n + i] = 1;
+  unsigned char *done = (unsigned char *)zalloc(n);
+  lu->n = n;
+  lu->perm = (int *)zalloc(sizeof(int) * n);
+  lu->iperm = (int *)zalloc(sizeof(int) * n);
+  for (int k = 0; k < n; ++k) {
+    long best = -1;
+    int bi = -1;
+    for (int i = 0; i < n; ++i) {
+      if (done[i]) continue;
+      long r = 0, c = 0;
+      for (int j = 0; j < n; ++j) {
+        if (done[j]) continue;
+        r += P[i * n + j];
+        c += P[j * n + i];
+      }
+      long score = (r - 1) * (c - 1);
+      if (best < 0 || score < best) {
+        best = score;
+        bi = i;
+      }
+    }
+    done[bi] = 1;
+    lu->perm[k] = bi;
+    lu->iperm[bi] = k;
+    /* eliminate bi: fill rows i with P[i][bi] in columns j with P[bi][j] */
+    for (int i = 0; i < n; ++i) {
+      if (done[i] || !P[i * n + bi]) continue;
+      for (int j = 0; j < n; ++j)
+        if (!done[j] && P[bi * n + j]) P[i * n + j] = 1;
+    }
+  }
+  /* P now holds the filled pattern in original indices */
+  lu->rowptr = (int *)zalloc(sizeof(int) * (n + 1));
+  int nnz = 0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) nnz += P[i * n + j];
+  lu->nnz = nnz;
+  lu->colidx = (int *)zalloc(sizeof(int) * nnz);
+  lu->diag = (int *)zalloc(sizeof(int) * n);
+  int e = 0;
+  for (int pi = 0; pi < n; ++pi) {
+    lu->rowptr[pi] = e;
+    int oi = lu->perm[pi];
+    for (int pj = 0; pj < n; ++pj) {
+      if (!P[oi * n + lu->perm[pj]]) continue;
+      if (pj == pi) lu->diag[pi] = e;
+      lu->colidx[e++] = pj;
+    }
+  }
+  lu->rowptr[n] = e;
+  int annz = colptr[n];
+  lu->a_to_lu = (int *)zalloc(sizeof(int) * (annz + 1));
+  for (int c = 0; c < n; ++c)
+    for (int a = colptr[c]; a < colptr[c + 1]; ++a) {
+      int pr = lu->iperm[rowid[a]], pc = lu->iperm[c];
+      for (int q = lu->rowptr[pr]; q < lu->rowptr[pr + 1]; ++q)
+        if (lu->colidx[q] == pc) {
+          lu->a_to_lu[a] = q;
+          break;
+        }
+    }
+  free(P);
+  free(done);
+}
+
+static void lu_free(LUSym *lu) {
+  free(lu->perm);
+  free(lu->iperm);
+  free(lu->rowptr);
+  free(lu->colidx);
+  free(lu->diag);
+  free(lu->a_to_lu);
+}
+
+/* Builds the sparsity as get_jac_init does for a gas-only model
+ * (src/camp_solver.c:1440-1683): diagonal plus the reaction elements of
+ * every reaction (src/rxns/rxn_arrhenius.c:44-60 and the same loop in the
+ * other gas types), then DERIV_ID/JAC_ID (src/rxns/rxn_arrhenius.c:71-91),
+ * then the var x var solver Jacobian with its map. */
+int om_build(OracleMech *m) {
+  if (m->n_added != m->n_rxn) return 1;
+  for (int i = 0; i < m->n_rxn; ++i) {
+    ORxn *r = &m->rx[i];
+    r->ints = m->int_data + (size_t)r->ints;
+    r->fl = m->float_data + (size_t)r->fl;
+    r->nr = r->ints[0];
+    r->np = r->ints[1];
+    r->n_int_prop = r->type == T_PHOTOLYSIS ? 3 : 2;
+    switch (r->type) {
+      case T_ARRHENIUS: r->n_float_prop = 6; break;
+      case T_TROE: r->n_float_prop = 10; break;
+      case T_CMAQ_H2O2: r->n_float_prop = 7; break;
+      case T_CMAQ_OH_HNO3: r->n_float_prop = 11; break;
+      default: r->n_float_prop = 1; break;
+    }
+  }
+  int n = m->n_state;
+  JacReg rj;
+  jr_init(&rj, n);
+  for (int i = 0; i < n; ++i) jr_register(&rj, i, i);
+  for (int i = 0; i < m->n_rxn; ++i) {
+    ORxn *r = &m->rx[i];
+    for (int ind = 0; ind < r->nr; ++ind) {
+      for (int d = 0; d < r->nr; ++d) jr_register(&rj, R_REACT(r, d), R_REACT(r, ind));
+      for (int d = 0; d < r->np; ++d) jr_register(&rj, R_PROD(r, d), R_REACT(r, ind));
+    }
+  }
+  jr_build(&rj);
+  m->n_rxn_jac = rj.nnz;
+  m->rj_colptr = rj.colptr;
+  m->rj_rowid = rj.rowid;
+
+  m->deriv_ids = (int *)zalloc(sizeof(int) * n);
+  for (int i = 0, d = 0; i < n; ++i)
+    m->deriv_ids[i] = m->var_type[i] == VAR_VARIABLE ? d++ : -1;
+  for (int i = 0; i < m->n_rxn; ++i) {
+    ORxn *r = &m->rx[i];
+    for (int k = 0; k < r->nr; ++k) R_DERIV_ID(r, k) = m->deriv_ids[R_REACT(r, k)];
+    for (int k = 0; k < r->np; ++k)
+      R_DERIV_ID(r, r->nr + k) = m->deriv_ids[R_PROD(r, k)];
+    int ij = 0;
+    for (int ind = 0; ind < r->nr; ++ind) {
+      for (int d = 0; d < r->nr; ++d)
+        R_JAC_ID(r, ij++) =
+            jr_elem_id(m->rj_colptr, m->rj_rowid, R_REACT(r, d), R_REACT(r, ind));
+      for (int d = 0; d < r->np; ++d)
+        R_JAC_ID(r, ij++) =
+            jr_elem_id(m->rj_colptr, m->rj_rowid, R_PROD(r, d), R_REACT(r, ind));
+    }
+  }
+
+  /* solver Jacobian: var x var elements of the reaction Jacobian */
+  JacReg sj;
+  jr_init(&sj, n);
+  for (int ind = 0; ind < n; ++ind)
+    for (int dep = 0; dep < n; ++dep) {
+      if (m->var_type[dep] != VAR_VARIABLE ||
+          jr_elem_id(m->rj_colptr, m->rj_rowid, dep, ind) == -1)
+        continue;
+      if (m->var_type[ind] == VAR_VARIABLE) jr_register(&sj, dep, ind);
+    }
+  jr_build(&sj);
+  m->n_solver_jac = sj.nnz;
+  m->sj_colptr = (int *)zalloc(sizeof(int) * (m->n_dep + 1));
+  m->sj_rowid = (int *)zalloc(sizeof(int) * (sj.nnz + 1));
+  for (int c = 0; c < n; ++c)
+    if (m->deriv_ids[c] >= 0) m->sj_colptr[m->deriv_ids[c]] = sj.colptr[c];
+  m->sj_colptr[m->n_dep] = sj.nnz;
+  for (int e = 0; e < sj.nnz; ++e) m->sj_rowid[e] = m->deriv_ids[sj.rowid[e]];
+  m->rxn_to_solver = (int *)zalloc(sizeof(int) * (m->n_rxn_jac + 1));
+  for (int ind = 0; ind < n; ++ind)
+    for (int e = m->rj_colptr[ind]; e < m->rj_colptr[ind + 1]; ++e) {
+      int dep = m->rj_rowid[e];
+      m->rxn_to_solver[e] =
+          (m->var_type[dep] == VAR_VARIABLE && m->var_type[ind] == VAR_VARIABLE)
+              ? jr_elem_id(sj.colptr, sj.rowid, dep, ind)
+              : -1;
+    }
+  free(sj.colptr);
+  free(sj.rowid);
+  lu_symbolic(&m->lu, m->n_dep, m->sj_colptr, m->sj_rowid);
+  m->built = 1;
+  return 0;
+}
+
+void om_free(OracleMech *m) {
+  if (!m) return;
+  free(m->var_type);
+  free(m->int_data);
+  free(m->float_data);
+  free(m->rx);
+  free(m->deriv_ids);
+  free(m->rj_colptr);
+  free(m->rj_rowid);
+  free(m->sj_colptr);
+  free(m->sj_rowid);
+  free(m->rxn_to_solver);
+  if (m->built) lu_free(&m->lu);
+  free(m);
+}
+
+int om_n_dep_var(const OracleMech *m) { return m->n_dep; }
+int om_n_rxn_env_data(const OracleMech *m) { return m->n_env; }
+int om_n_rxn_jac_elem(const OracleMech *m) { return m->n_rxn_jac; }
+int om_n_solver_jac_elem(const OracleMech *m) { return m->n_solver_jac; }
+int om_n_lu_elem(const OracleMech *m) { return m->lu.nnz; }
+int om_rxn_int_data_size(const OracleMech *m) { return m->int_size; }
+void om_get_rxn_jac(const OracleMech *m, int *colptr, int *rowid) {
+  memcpy(colptr, m->rj_colptr, sizeof(int) * (m->n_state + 1));
+  memcpy(rowid, m->rj_rowid, sizeof(int) * m->n_rxn_jac);
+}
+void om_get_solver_jac(const OracleMech *m, int *colptr, int *rowid) {
+  memcpy(colptr, m->sj_colptr, sizeof(int) * (m->n_dep + 1));
+  memcpy(rowid, m->sj_rowid, sizeof(int) * m->n_solver_jac);
+}
+void om_get_rxn_int_data(const OracleMech *m, int *out) {
+  memcpy(out, m->int_data, sizeof(int) * m->int_size);
+}
+void om_get_lu_order(const OracleMech *m, int *perm) {
+  memcpy(perm, m->lu.perm, sizeof(int) * m->n_dep);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Rate constants (update_env_state of each gas type)                        */
+/* ------------------------------------------------------------------------ */
+
+int om_set_photo_rate(const OracleMech *m, double *rxn_env, int photo_id,
+                      double base_rate) {
+  int found = 0;
+  for (int i = 0; i < m->n_rxn; ++i) {
+    const ORxn *r = &m->rx[i];
+    if (r->type != T_PHOTOLYSIS || r->ints[2] != photo_id || r->ints[2] <= 0)
+      continue;
+    rxn_env[r->env_off + 1] = base_rate;
+    rxn_env[r->env_off] = r->fl[0] * base_rate;
+    found = 1;
+  }
+  return found;
+}
+
+void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
+  const double T = env[0], P = env[1];
+  for (int i = 0; i < m->n_rxn; ++i) {
+    const ORxn *r = &m->rx[i];
+    const double *f = r->fl;
+    double *k = rxn_env + r->env_off;
+    switch (r->type) {
+      case T_ARRHENIUS: /* src/rxns/rxn_arrhenius.c:103-118 */
+        k[0] = f[0] * exp(f[2] / T) * (f[1] == 0.0 ? 1.0 : pow(T / f[3], f[1])) *
+               (f[4] == 0.0 ? 1.0 : (1.0 + f[4] * P)) *
+               pow(f[5] * P / T, r->nr - 1);
+        break;
+      case T_TROE: { /* src/rxns/rxn_troe.c:118-140 */
+        double conv = f[9] * P / T;
+        double k0 = f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
+                    (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) * conv;
+        double kinf = k0 / (f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
+                            (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4])));
+        k[0] = (k0 / (1.0 + kinf)) *
+               pow(f[6], (1.0 / (1.0 + pow(log10(kinf) / f[7], 2)))) *
+               pow(conv, r->nr - 1) * f[8];
+        break;
+      }
+      case T_CMAQ_H2O2: { /* src/rxns/rxn_CMAQ_H2O2.c:106-125 */
+        double conv = f[6] * P / T;
+        k[0] = (f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
+                    (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) +
+                f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
+                    (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4])) * conv) *
+               pow(conv, r->nr - 1);
+        break;
+      }
+      case T_CMAQ_OH_HNO3: { /* src/rxns/rxn_CMAQ_OH_HNO3.c:110-133 */
+        double conv = f[10] * P / T;
+        double k2 = f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
+                    (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4]));
+        double k3 = f[6] * (f[8] == 0.0 ? 1.0 : exp(f[8] / T)) *
+                    (f[7] == 0.0 ? 1.0 : pow(T / 300.0, f[7])) * conv;
+        k[0] = (f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
+                    (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) +
+                k3 / (1.0 + k3 / k2)) *
+               pow(conv, r->nr - 1) * f[9];
+        break;
+      }
+      case T_PHOTOLYSIS: /* src/rxns/rxn_photolysis.c:137-148 */
+        k[0] = f[0] * k[1];
+        break;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Derivative and Jacobian (calc_deriv_contrib / calc_jac_contrib)           */
+/* ------------------------------------------------------------------------ */
+
+/* The gas types share one mass-action form: rate = k * prod(y_react), loss of
+ * rate on each reactant, rate*yield on each product unless a negative yield
+ * would drive the product below zero within one step
+ * (src/rxns/rxn_arrhenius.c:131-165).  Contributions are split by sign into
+ * production and loss sums (src/time_derivative.c:90-97). */
+void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
+              double time_step, double *deriv, double *r_p, double *r_l) {
+  long double *P = (long double *)zalloc(sizeof(long double) * m->n_dep * 2);
+  long double *L = P + m->n_dep;
+  for (int i = 0; i < m->n_rxn; ++i) {
+    const ORxn *r = &m->rx[i];
+    long double rate = rxn_env[r->env_off];
+    for (int s = 0; s < r->nr; ++s) rate *= state[R_REACT(r, s)];
+    if (rate == 0.0) continue;
+    for (int s = 0; s < r->nr; ++s) {
+      int d = R_DERIV_ID(r, s);
+      if (d < 0) continue;
+      L[d] += rate; /* -rate is negative: a loss */
+    }
+    for (int s = 0; s < r->np; ++s) {
+      int d = R_DERIV_ID(r, r->nr + s);
+      if (d < 0) continue;
+      if (-rate * R_YIELD(r, s) * time_step <= state[R_PROD(r, s)]) {
+        long double c = rate * R_YIELD(r, s);
+        if (c > 0.0)
+          P[d] += c;
+        else
+          L[d] += -c;
+      }
+    }
+  }
+  for (int d = 0; d < m->n_dep; ++d) {
+    /* time_derivative_output without the estimate (src/time_derivative.c:46-88) */
+    deriv[d] = (P[d] + L[d] != 0.0) ? (double)(P[d] - L[d]) : 0.0;
+    if (r_p) r_p[d] = (double)P[d];
+    if (r_l) r_l[d] = (double)L[d];
+  }
+  free(P);
+}
+
+/* src/rxns/rxn_arrhenius.c:178-212 and src/Jacobian.c:223-241, then the
+ * jac_map fold with unit parameters (src/camp_solver.c:1096-1106). */
+void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
+            double time_step, double *jvals) {
+  long double *P = (long double *)zalloc(sizeof(long double) * m->n_rxn_jac * 2);
+  long double *L = P + m->n_rxn_jac;
+  for (int i = 0; i < m->n_rxn; ++i) {
+    const ORxn *r = &m->rx[i];
+    int e = 0;
+    for (int ind = 0; ind < r->nr; ++ind) {
+      double rate = rxn_env[r->env_off];
+      for (int s = 0; s < r->nr; ++s)
+        if (s != ind) rate *= state[R_REACT(r, s)];
+      for (int d = 0; d < r->nr; ++d, ++e) {
+        int id = R_JAC_ID(r, e);
+        if (id < 0) continue;
+        L[id] += rate;
+      }
+      for (int d = 0; d < r->np; ++d, ++e) {
+        int id = R_JAC_ID(r, e);
+        if (id < 0) continue;
+        if (-rate * state[R_REACT(r, ind)] * R_YIELD(r, d) * time_step <=
+            state[R_PROD(r, d)])
+          P[id] += R_YIELD(r, d) * rate;
+      }
+    }
+  }
+  for (int s = 0; s < m->n_solver_jac; ++s) jvals[s] = 0.0;
+  for (int e = 0; e < m->n_rxn_jac; ++e) {
+    int s = m->rxn_to_solver[e];
+    if (s >= 0) jvals[s] += (double)(P[e] - L[e]);
+  }
+  free(P);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sparse LU of M = I - gamma*J                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Forms M in LU storage, factors it row by row (IKJ order with a dense work
+ * row), returns 0, or 1 when a pivot is zero or not finite (the linear solver
+ * setup then fails recoverably, as a singular KLU factorization does). */
+static int lu_factor(const LUSym *lu, const double *jvals, int annz,
+                     double gamma, double *LU, double *w) {
+  int n = lu->n;
+  for (int q = 0; q < lu->nnz; ++q) LU[q] = 0.0;
+  for (int a = 0; a < annz; ++a) LU[lu->a_to_lu[a]] = -gamma * jvals[a];
+  for (int i = 0; i < n; ++i) LU[lu->diag[i]] += 1.0;
+  for (int i = 0; i < n; ++i) {
+    for (int q = lu->rowptr[i]; q < lu->rowptr[i + 1]; ++q) w[lu->colidx[q]] = LU[q];
+    for (int q = lu->rowptr[i]; q < lu->diag[i]; ++q) {
+      int k = lu->colidx[q];
+      double lik = w[k] / LU[lu->diag[k]];
+      w[k] = lik;
+      for (int p = lu->diag[k] + 1; p < lu->rowptr[k + 1]; ++p)
+        w[lu->colidx[p]] -= lik * LU[p];
+    }
+    for (int q = lu->rowptr[i]; q < lu->rowptr[i + 1]; ++q) LU[q] = w[lu->colidx[q]];
+    double piv = LU[lu->diag[i]];
+    if (piv == 0.0 || !isfinite(piv)) return 1;
+  }
+  return 0;
+}
+
+/* Solves M x = b in place (b in original variable order). */
+static void lu_solve(const LUSym *lu, const double *LU, double *b, double *z) {
+  int n = lu->n;
+  for (int i = 0; i < n; ++i) z[i] = b[lu->perm[i]];
+  for (int i = 0; i < n; ++i) {
+    double s = z[i];
+    for (int q = lu->rowptr[i]; q < lu->diag[i]; ++q) s -= LU[q] * z[lu->colidx[q]];
+    z[i] = s;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = z[i];
+    for (int q = lu->diag[i] + 1; q < lu->rowptr[i + 1]; ++q)
+      s -= LU[q] * z[lu->colidx[q]];
+    z[i] = s / LU[lu->diag[i]];
+  }
+  for (int i = 0; i < n; ++i) b[lu->perm[i]] = z[i];
+}
+
+/* ------------------------------------------------------------------------ */
+/* BDF integrator (restated CVODE algorithm, one cell)                       */
+/* ------------------------------------------------------------------------ */
+
+#define QMAX 5
+#define LMAX (QMAX + 1)
+#define ETAMX1 10000.0
+#define ETAMX2 10.0
+#define ETAMX3 10.0
+#define ETAMXF 0.2
+#define ETAMIN 0.1
+#define ETACF 0.25
+#define ADDON 0.000001
+#define BIAS1 6.0
+#define BIAS2 6.0
+#define BIAS3 10.0
+#define ONEPSM 1.000001
+#define THRESH 1.5
+#define SMALL_NST 10
+#define MXNEF1 3
+#define SMALL_NEF 2
+#define LONG_WAIT 10
+#define MAXCOR 3
+#define CRDOWN 0.3
+#define DGMAX 0.3
+#define RDIV 2.0
+#define MSBP 20
+#define MSBJ 50
+#define DGMAX_J 0.2
+#define NLSCOEF 0.1
+#define UROUND 2.220446049250313e-16
+
+/* nonlinear solver outcomes */
+#define NL_OK 0
+#define NL_CONV_FAIL 1
+#define NL_RHS_RECVR 2
+#define NL_TRY_AGAIN 3
+#define NL_CONSTR_RECVR 4
+/* convfail values passed to the linear solver setup */
+#define NO_FAILURES 0
+#define FAIL_BAD_J 1
+#define FAIL_OTHER 2
+/* nflag values */
+#define FIRST_CALL 0
+#define PREV_CONV_FAIL 1
+#define PREV_ERR_FAIL 2
+
+typedef struct {
+  const LUSym *lu;
+  int n, annz;
+  or_rhs_fn f;
+  or_jac_fn jac;
+  void *ctx;
+  double rtol;
+  const double *atol;
+  int max_steps, maxncf, maxnef;
+  /* work */
+  double *zn[LMAX];
+  double *ewt, *acor, *tempv, *ftemp, *y, *savedJ, *LU, *w, *z;
+  /* state of the method */
+  int q, qprime, qwait, L, indx_acor;
+  double h, hprime, hscale, eta, etamax, hu, next_h;
+  double tn, tau[LMAX + 1], tq[6], l[LMAX];
+  double rl1, gamma, gammap, gamrat, crate, acnrm, saved_tq5;
+  long nst, nfe, nsetups, netf, nni, ncfn, nje, nstlp, nstlj;
+  int jcur;
+  double etaqm1, etaq, etaqp1;
+} Bdf;
+
+static double wrms(const double *v, const double *w, int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double t = v[i] * w[i];
+    s += t * t;
+  }
+  return sqrt(s / n);
+}
+
+static int set_ewt(Bdf *b, const double *y) {
+  for (int i = 0; i < b->n; ++i) {
+    double t = b->rtol * fabs(y[i]) + b->atol[i];
+    if (t <= 0.0) return 1;
+    b->ewt[i] = 1.0 / t;
+  }
+  return 0;
+}
+
+static void bdf_rescale(Bdf *b) {
+  double factor = b->eta;
+  for (int j = 1; j <= b->q; ++j) {
+    for (int i = 0; i < b->n; ++i) b->zn[j][i] *= factor;
+    factor *= b->eta;
+  }
+  b->h = b->hscale * b->eta;
+  b->next_h = b->h;
+  b->hscale = b->h;
+}
+
+static void bdf_predict(Bdf *b) {
+  b->tn += b->h;
+  for (int k = 1; k <= b->q; ++k)
+    for (int j = b->q; j >= k; --j)
+      for (int i = 0; i < b->n; ++i) b->zn[j - 1][i] += b->zn[j][i];
+}
+
+static void bdf_restore(Bdf *b, double saved_t) {
+  b->tn = saved_t;
+  for (int k = 1; k <= b->q; ++k)
+    for (int j = b->q; j >= k; --j)
+      for (int i = 0; i < b->n; ++i) b->zn[j - 1][i] -= b->zn[j][i];
+}
+
+/* l and tq coefficients of the fixed-leading-coefficient BDF formula */
+static void bdf_set(Bdf *b) {
+  int q = b->q;
+  double *l = b->l, *tau = b->tau;
+  double alpha0, alpha0_hat, xi_inv, xistar_inv, hsum;
+  l[0] = l[1] = xi_inv = xistar_inv = 1.0;
+  for (int i = 2; i <= q; ++i) l[i] = 0.0;
+  alpha0 = alpha0_hat = -1.0;
+  hsum = b->h;
+  if (q > 1) {
+    for (int j = 2; j < q; ++j) {
+      hsum += tau[j - 1];
+      xi_inv = b->h / hsum;
+      alpha0 -= 1.0 / j;
+      for (int i = j; i >= 1; --i) l[i] += l[i - 1] * xi_inv;
+    }
+    alpha0 -= 1.0 / q;
+    xistar_inv = -l[1] - alpha0;
+    hsum += tau[q - 1];
+    xi_inv = b->h / hsum;
+    alpha0_hat = -l[1] - xi_inv;
+    for (int i = q; i >= 1; --i) l[i] += l[i - 1] * xistar_inv;
+  }
+  /* test quantities */
+  double A1 = 1.0 - alpha0_hat + alpha0;
+  double A2 = 1.0 + q * A1;
+  b->tq[2] = fabs(A1 / (alpha0 * A2));
+  b->tq[5] = fabs(A2 * xistar_inv / (l[q] * xi_inv));
+  if (b->qwait == 1) {
+    if (q > 1) {
+      double C = xistar_inv / l[q];
+      double A3 = alpha0 + 1.0 / q;
+      double A4 = alpha0_hat + xi_inv;
+      double Cpinv = (1.0 - A4 + A3) / A3;
+      b->tq[1] = fabs(C * Cpinv);
+    } else {
+      b->tq[1] = 1.0;
+    }
+    hsum += tau[q];
+    xi_inv = b->h / hsum;
+    double A5 = alpha0 - 1.0 / (q + 1);
+    double A6 = alpha0_hat - xi_inv;
+    double Cppinv = (1.0 - A6 + A5) / A2;
+    b->tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+  }
+  b->tq[4] = NLSCOEF / b->tq[2];
+  b->rl1 = 1.0 / l[1];
+  b->gamma = b->h * b->rl1;
+  if (b->nst == 0) b->gammap = b->gamma;
+  b->gamrat = (b->nst > 0) ? b->gamma / b->gammap : 1.0;
+}
+
+static void bdf_increase_order(Bdf *b) {
+  double *l = b->l;
+  int q = b->q;
+  for (int i = 0; i <= QMAX; ++i) l[i] = 0.0;
+  l[2] = 1.0;
+  double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0,
+         hsum = b->hscale;
+  if (q > 1) {
+    for (int j = 1; j < q; ++j) {
+      hsum += b->tau[j + 1];
+      double xi = hsum / b->hscale;
+      prod *= xi;
+      alpha0 -= 1.0 / (j + 1);
+      alpha1 += 1.0 / xi;
+      for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xiold + l[i - 1];
+      xiold = xi;
+    }
+  }
+  double A1 = (-alpha0 - alpha1) / prod;
+  int Lnew = q + 2; /* zn[L] with L = q+1 becomes the new top column */
+  (void)Lnew;
+  for (int i = 0; i < b->n; ++i) b->zn[q + 1][i] = A1 * b->zn[b->indx_acor][i];
+  for (int j = 2; j <= q; ++j)
+    for (int i = 0; i < b->n; ++i) b->zn[j][i] += l[j] * b->zn[q + 1][i];
+}
+
+static void bdf_decrease_order(Bdf *b) {
+  double *l = b->l;
+  int q = b->q;
+  for (int i = 0; i <= QMAX; ++i) l[i] = 0.0;
+  l[2] = 1.0;
+  double hsum = 0.0;
+  for (int j = 1; j <= q - 2; ++j) {
+    hsum += b->tau[j];
+    double xi = hsum / b->hscale;
+    for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xi + l[i - 1];
+  }
+  for (int j = 2; j < q; ++j)
+    for (int i = 0; i < b->n; ++i) b->zn[j][i] -= l[j] * b->zn[q][i];
+}
+
+static void bdf_adjust_order(Bdf *b, int deltaq) {
+  if (deltaq == 1)
+    bdf_increase_order(b);
+  else if (deltaq == -1)
+    bdf_decrease_order(b);
+}
+
+static void bdf_adjust_params(Bdf *b) {
+  if (b->qprime != b->q) {
+    bdf_adjust_order(b, b->qprime - b->q);
+    b->q = b->qprime;
+    b->L = b->q + 1;
+    b->qwait = b->L;
+  }
+  bdf_rescale(b);
+}
+
+/* Linear solver setup: J reuse rule of the CVODE direct interface, then
+ * M = I - gamma J factored. Returns 0, >0 recoverable, <0 fatal. */
+static int bdf_lsetup(Bdf *b, int convfail, const double *ypred) {
+  double dgamma = fabs(b->gamma / b->gammap - 1.0);
+  int jbad = (b->nst == 0) || (b->nst > b->nstlj + MSBJ) ||
+             ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_J)) ||
+             (convfail == FAIL_OTHER);
+  if (!jbad) {
+    b->jcur = 0;
+  } else {
+    b->nje++;
+    b->nstlj = b->nst;
+    b->jcur = 1;
+    int r = b->jac(b->ctx, b->tn, ypred, b->h, b->savedJ);
+    if (r < 0) return -1;
+    if (r > 0) return 1;
+  }
+  return lu_factor(b->lu, b->savedJ, b->annz, b->gamma, b->LU, b->w);
+}
+
+static int bdf_newton_iteration(Bdf *b, int projected) {
+  int n = b->n, m = 0;
+  double del, delp = 0.0;
+  for (;;) {
+    for (int i = 0; i < n; ++i)
+      b->tempv[i] = b->gamma * b->ftemp[i] - (b->rl1 * b->zn[1][i] + b->acor[i]);
+    lu_solve(b->lu, b->LU, b->tempv, b->z);
+    if (b->gamrat != 1.0) {
+      double s = 2.0 / (1.0 + b->gamrat);
+      for (int i = 0; i < n; ++i) b->tempv[i] *= s;
+    }
+    b->nni++;
+    del = wrms(b->tempv, b->ewt, n);
+    for (int i = 0; i < n; ++i) {
+      b->acor[i] += b->tempv[i];
+      b->y[i] = b->zn[0][i] + b->acor[i];
+    }
+    if (m > 0) b->crate = fmax(CRDOWN * b->crate, del / delp);
+    double dcon = del * fmin(1.0, b->crate) / b->tq[4];
+    if (dcon <= 1.0) {
+      b->acnrm = (m == 0 && !projected) ? del : wrms(b->acor, b->ewt, n);
+      b->jcur = 0;
+      return NL_OK;
+    }
+    ++m;
+    if ((m == MAXCOR) || ((m >= 2) && (del > RDIV * delp))) {
+      if (!b->jcur) return NL_TRY_AGAIN;
+      return NL_CONV_FAIL;
+    }
+    delp = del;
+    int r = b->f(b->ctx, b->tn, b->y, b->h, b->ftemp);
+    b->nfe++;
+    if (r < 0) return -1;
+    if (r > 0) {
+      if (!b->jcur) return NL_TRY_AGAIN;
+      return NL_RHS_RECVR;
+    }
+  }
+}
+
+/* Newton solve of one step; returns NL_OK, NL_CONV_FAIL, NL_RHS_RECVR,
+ * NL_CONSTR_RECVR or negative for an unrecoverable failure (OR_* codes).
+ *
+ * Positivity: the reference's f rejects any concentration below -1e-30
+ * (src/camp_solver.c:805-833) and its modified CVODE steers around negative
+ * predictions with a guess helper (src/camp_solver.c:1321-1408) whose call
+ * sites are in the missing CVODE source.  This restatement instead
+ *   (a) starts the Newton iteration from the predicted state with negative
+ *       components raised to zero (acor starts at that projection), and
+ *   (b) applies CVODE's published non-negativity constraint check to the
+ *       converged iterate (cvCheckConstraints, SUNDIALS >= 5.0): a violation
+ *       whose WRMS norm is within the Newton tolerance tq[4] is projected to
+ *       zero, a larger one rejects the step with eta = max(0.1, 0.9 * min over
+ *       violated i of zn0_i / (zn0_i - y_i)). */
+static int bdf_check_constraints(Bdf *b) {
+  int n = b->n, viol = 0;
+  for (int i = 0; i < n; ++i)
+    if (b->y[i] < 0.0) {
+      viol = 1;
+      break;
+    }
+  if (!viol) return NL_OK;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i)
+    if (b->y[i] < 0.0) {
+      double t = b->y[i] * b->ewt[i];
+      s += t * t;
+    }
+  double vnorm = sqrt(s / n);
+  if (vnorm <= b->tq[4]) {
+    for (int i = 0; i < n; ++i)
+      if (b->y[i] < 0.0) {
+        b->acor[i] -= b->y[i];
+        b->y[i] = 0.0;
+      }
+    b->acnrm = wrms(b->acor, b->ewt, n);
+    return NL_OK;
+  }
+  double eta = 1.0e300;
+  for (int i = 0; i < n; ++i)
+    if (b->y[i] < 0.0) {
+      double d = b->zn[0][i] - b->y[i];
+      double qv = b->zn[0][i] / d;
+      if (qv < eta) eta = qv;
+    }
+  eta *= 0.9;
+  b->eta = eta > 0.1 ? eta : 0.1;
+  return NL_CONSTR_RECVR;
+}
+
+static int bdf_nls(Bdf *b, int nflag) {
+  int convfail = ((nflag == FIRST_CALL) || (nflag == PREV_ERR_FAIL))
+                     ? NO_FAILURES
+                     : FAIL_OTHER;
+  int call_setup = (nflag == PREV_CONV_FAIL) || (nflag == PREV_ERR_FAIL) ||
+                   (b->nst == 0) || (b->nst >= b->nstlp + MSBP) ||
+                   (fabs(b->gamrat - 1.0) > DGMAX);
+  int projected = 0;
+  for (int i = 0; i < b->n; ++i) {
+    double a = b->zn[0][i] < 0.0 ? -b->zn[0][i] : 0.0;
+    if (a != 0.0) projected = 1;
+    b->acor[i] = a;
+    b->y[i] = b->zn[0][i] + a;
+  }
+  for (;;) {
+    int r = b->f(b->ctx, b->tn, b->y, b->h, b->ftemp);
+    b->nfe++;
+    if (r < 0) return OR_RHSFUNC_FAIL;
+    if (r > 0) return NL_RHS_RECVR;
+    if (call_setup) {
+      int ier = bdf_lsetup(b, convfail, b->y);
+      b->nsetups++;
+      call_setup = 0;
+      b->gamrat = b->crate = 1.0;
+      b->gammap = b->gamma;
+      b->nstlp = b->nst;
+      if (ier < 0) return OR_LSETUP_FAIL;
+      if (ier > 0) return NL_CONV_FAIL;
+    }
+    int ier = bdf_newton_iteration(b, projected);
+    if (ier < 0) return OR_RHSFUNC_FAIL;
+    if (ier == NL_OK) return bdf_check_constraints(b);
+    if (ier != NL_TRY_AGAIN) return ier;
+    call_setup = 1;
+    convfail = FAIL_BAD_J;
+    for (int i = 0; i < b->n; ++i) {
+      double a = b->zn[0][i] < 0.0 ? -b->zn[0][i] : 0.0;
+      b->acor[i] = a;
+      b->y[i] = b->zn[0][i] + a;
+    }
+  }
+}
+
+#define DO_ERROR_TEST 100
+#define PREDICT_AGAIN 101
+#define TRY_AGAIN 102
+
+static int bdf_handle_nflag(Bdf *b, int *nflag, double saved_t, int *ncf) {
+  int nf = *nflag;
+  if (nf == NL_OK) return DO_ERROR_TEST;
+  b->ncfn++;
+  bdf_restore(b, saved_t);
+  if (nf < 0) return nf;
+  (*ncf)++;
+  b->etamax = 1.0;
+  if (*ncf == b->maxncf)
+    return nf == NL_RHS_RECVR ? OR_REPTD_RHSFUNC_ERR : OR_CONV_FAILURE;
+  if (nf != NL_CONSTR_RECVR) b->eta = ETACF;
+  *nflag = PREV_CONV_FAIL;
+  bdf_rescale(b);
+  return PREDICT_AGAIN;
+}
+
+static int bdf_error_test(Bdf *b, int *nflag, double saved_t, int *nef,
+                          double *dsm) {
+  *dsm = b->acnrm * b->tq[2];
+  if (*dsm <= 1.0) return OR_SUCCESS;
+  (*nef)++;
+  b->netf++;
+  *nflag = PREV_ERR_FAIL;
+  bdf_restore(b, saved_t);
+  if (*nef == b->maxnef) return OR_ERR_FAILURE;
+  b->etamax = 1.0;
+  if (*nef <= MXNEF1) {
+    b->eta = 1.0 / (pow(BIAS2 * *dsm, 1.0 / b->L) + ADDON);
+    b->eta = fmax(ETAMIN, b->eta);
+    if (*nef >= SMALL_NEF) b->eta = fmin(b->eta, ETAMXF);
+    bdf_rescale(b);
+    return TRY_AGAIN;
+  }
+  if (b->q > 1) {
+    b->eta = ETAMIN;
+    bdf_adjust_order(b, -1);
+    b->L = b->q;
+    b->q--;
+    b->qwait = b->L;
+    bdf_rescale(b);
+    return TRY_AGAIN;
+  }
+  b->eta = ETAMIN;
+  b->h *= b->eta;
+  b->next_h = b->h;
+  b->hscale = b->h;
+  b->qwait = LONG_WAIT;
+  int r = b->f(b->ctx, b->tn, b->zn[0], b->h, b->tempv);
+  b->nfe++;
+  if (r < 0) return OR_RHSFUNC_FAIL;
+  if (r > 0) return OR_UNREC_RHSFUNC_ERR;
+  for (int i = 0; i < b->n; ++i) b->zn[1][i] = b->h * b->tempv[i];
+  return TRY_AGAIN;
+}
+
+static void bdf_complete_step(Bdf *b) {
+  b->nst++;
+  b->hu = b->h;
+  for (int i = b->q; i >= 2; --i) b->tau[i] = b->tau[i - 1];
+  if ((b->q == 1) && (b->nst > 1)) b->tau[2] = b->tau[1];
+  b->tau[1] = b->h;
+  for (int j = 0; j <= b->q; ++j)
+    for (int i = 0; i < b->n; ++i) b->zn[j][i] += b->l[j] * b->acor[i];
+  b->qwait--;
+  if ((b->qwait == 1) && (b->q != QMAX)) {
+    memcpy(b->zn[QMAX], b->acor, sizeof(double) * b->n);
+    b->saved_tq5 = b->tq[5];
+    b->indx_acor = QMAX;
+  }
+}
+
+static void bdf_set_eta(Bdf *b) {
+  if (b->eta < THRESH) {
+    b->eta = 1.0;
+    b->hprime = b->h;
+  } else {
+    b->eta = fmin(b->eta, b->etamax);
+    b->hprime = b->h * b->eta;
+  }
+}
+
+static void bdf_prepare_next_step(Bdf *b, double dsm) {
+  if (b->etamax == 1.0) {
+    b->qwait = b->qwait > 2 ? b->qwait : 2;
+    b->qprime = b->q;
+    b->hprime = b->h;
+    b->eta = 1.0;
+    return;
+  }
+  b->etaq = 1.0 / (pow(BIAS2 * dsm, 1.0 / b->L) + ADDON);
+  if (b->qwait != 0) {
+    b->eta = b->etaq;
+    b->qprime = b->q;
+    bdf_set_eta(b);
+    return;
+  }
+  b->qwait = 2;
+  /* eta for order q-1 */
+  b->etaqm1 = 0.0;
+  if (b->q > 1) {
+    double ddn = wrms(b->zn[b->q], b->ewt, b->n) * b->tq[1];
+    b->etaqm1 = 1.0 / (pow(BIAS1 * ddn, 1.0 / b->q) + ADDON);
+  }
+  /* eta for order q+1 */
+  b->etaqp1 = 0.0;
+  if (b->q != QMAX && b->saved_tq5 != 0.0) {
+    double cquot = (b->tq[5] / b->saved_tq5) * pow(b->h / b->tau[2], b->L);
+    for (int i = 0; i < b->n; ++i)
+      b->tempv[i] = b->acor[i] - cquot * b->zn[QMAX][i];
+    double dup = wrms(b->tempv, b->ewt, b->n) * b->tq[3];
+    b->etaqp1 = 1.0 / (pow(BIAS3 * dup, 1.0 / (b->L + 1)) + ADDON);
+  }
+  /* choose */
+  double etam = fmax(b->etaqm1, fmax(b->etaq, b->etaqp1));
+  if (etam < THRESH) {
+    b->eta = 1.0;
+    b->qprime = b->q;
+  } else if (etam == b->etaq) {
+    b->eta = b->etaq;
+    b->qprime = b->q;
+  } else if (etam == b->etaqm1) {
+    b->eta = b->etaqm1;
+    b->qprime = b->q - 1;
+  } else {
+    b->eta = b->etaqp1;
+    b->qprime = b->q + 1;
+    memcpy(b->zn[QMAX], b->acor, sizeof(double) * b->n);
+  }
+  bdf_set_eta(b);
+}
+
+static int bdf_step(Bdf *b) {
+  double saved_t = b->tn, dsm = 0.0;
+  int ncf = 0, nef = 0, nflag = FIRST_CALL;
+  if ((b->nst > 0) && (b->hprime != b->h)) bdf_adjust_params(b);
+  for (;;) {
+    bdf_predict(b);
+    bdf_set(b);
+    nflag = bdf_nls(b, nflag);
+    int kflag = bdf_handle_nflag(b, &nflag, saved_t, &ncf);
+    if (kflag == PREDICT_AGAIN) continue;
+    if (kflag != DO_ERROR_TEST) return kflag;
+    int eflag = bdf_error_test(b, &nflag, saved_t, &nef, &dsm);
+    if (eflag == TRY_AGAIN) continue;
+    if (eflag != OR_SUCCESS) return eflag;
+    break;
+  }
+  bdf_complete_step(b);
+  bdf_prepare_next_step(b, dsm);
+  b->etamax = (b->nst <= SMALL_NST) ? ETAMX2 : ETAMX3;
+  for (int i = 0; i < b->n; ++i) b->acor[i] *= b->tq[2];
+  return OR_SUCCESS;
+}
+
+/* Interpolated solution at t from the Nordsieck array (CVodeGetDky, k=0). */
+static void bdf_dky(const Bdf *b, double t, double *out) {
+  double s = (t - b->tn) / b->h;
+  for (int i = 0; i < b->n; ++i) {
+    double v = b->zn[b->q][i];
+    for (int j = b->q - 1; j >= 0; --j) v = b->zn[j][i] + s * v;
+    out[i] = v;
+  }
+}
+
+typedef struct {
+  double *mem;
+} BdfWork;
+
+static void bdf_alloc(Bdf *b, BdfWork *wk, int n, int annz, int lunnz) {
+  size_t tot = (size_t)n * (LMAX + 8) + (size_t)annz + (size_t)lunnz;
+  wk->mem = (double *)zalloc(sizeof(double) * (tot + 8));
+  double *p = wk->mem;
+  for (int j = 0; j < LMAX; ++j, p += n) b->zn[j] = p;
+  b->ewt = p; p += n;
+  b->acor = p; p += n;
+  b->tempv = p; p += n;
+  b->ftemp = p; p += n;
+  b->y = p; p += n;
+  b->w = p; p += n;
+  b->z = p; p += n;
+  b->savedJ = p; p += annz;
+  b->LU = p;
+}
+
+/* One cell from t0 to tout with initial step h0 (CVodeReInit + CVode in
+ * CV_NORMAL mode with CVodeSetInitStep(h0), src/camp_solver.c:619-633). */
+static int bdf_integrate(Bdf *b, double t0, double tout, double h0, double *y,
+                         OracleStats *st) {
+  int n = b->n;
+  memset(b->tau, 0, sizeof(b->tau));
+  memset(b->tq, 0, sizeof(b->tq));
+  b->q = 1;
+  b->L = 2;
+  b->qwait = b->L;
+  b->etamax = ETAMX1;
+  b->qprime = 1;
+  b->nst = b->nfe = b->nsetups = b->netf = b->nni = b->ncfn = b->nje = 0;
+  b->nstlp = b->nstlj = 0;
+  b->saved_tq5 = 0.0;
+  b->indx_acor = QMAX;
+  b->crate = 1.0;
+  b->jcur = 0;
+  b->hu = 0.0;
+  b->tn = t0;
+  b->gammap = b->gamma = 0.0;
+  memcpy(b->zn[0], y, sizeof(double) * n);
+  for (int j = 1; j < LMAX; ++j) memset(b->zn[j], 0, sizeof(double) * n);
+  int flag = OR_SUCCESS;
+  if (set_ewt(b, b->zn[0])) {
+    flag = OR_ILL_INPUT;
+    goto done;
+  }
+  b->next_h = 0.0;
+  {
+    int r = b->f(b->ctx, t0, b->zn[0], h0, b->zn[1]);
+    b->nfe++;
+    if (r != 0) {
+      flag = r < 0 ? OR_RHSFUNC_FAIL : OR_REPTD_RHSFUNC_ERR;
+      goto done;
+    }
+  }
+  b->h = h0;
+  if ((tout - t0) * b->h < 0.0) {
+    flag = OR_ILL_INPUT;
+    goto done;
+  }
+  b->hscale = b->h;
+  b->hprime = b->h;
+  for (int i = 0; i < n; ++i) b->zn[1][i] *= b->h;
+  long nstloc = 0;
+  for (;;) {
+    b->next_h = b->h;
+    if (b->nst > 0 && set_ewt(b, b->zn[0])) {
+      flag = OR_ILL_INPUT;
+      break;
+    }
+    if (b->max_steps > 0 && nstloc >= b->max_steps) {
+      flag = OR_TOO_MUCH_WORK;
+      break;
+    }
+    double tolsf = UROUND * wrms(b->zn[0], b->ewt, n);
+    if (tolsf > 1.0) {
+      flag = OR_TOO_MUCH_ACC;
+      break;
+    }
+    int kflag = bdf_step(b);
+    if (kflag != OR_SUCCESS) {
+      flag = kflag;
+      break;
+    }
+    nstloc++;
+    if ((b->tn - tout) * b->h >= 0.0) {
+      bdf_dky(b, tout, y);
+      b->next_h = b->hprime;
+      break;
+    }
+  }
+done:
+  if (st) {
+    st->nst = b->nst;
+    st->nfe = b->nfe;
+    st->nsetups = b->nsetups;
+    st->netf = b->netf;
+    st->nni = b->nni;
+    st->ncfn = b->ncfn;
+    st->nje = b->nje;
+    st->hu = b->hu;
+    st->hcur = b->next_h;
+    st->flag = flag;
+    st->qu = b->q;
+  }
+  return flag;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Oracle's own f/J as BDF callbacks                                         */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  const OracleMech *m;
+  double *state;         /* one cell's state (constants kept, deps overwritten) */
+  const double *rxn_env; /* one cell's rate constants */
+  double *scratch_rp;
+  double h0;
+} CellCtx;
+
+/* src/camp_solver.c:805-833: y < -SMALL is a recoverable failure; other
+ * values are copied (exactly -SMALL becomes TINY). */
+static int load_state(CellCtx *c, const double *y) {
+  const OracleMech *m = c->m;
+  for (int i = 0, d = 0; i < m->n_state; ++i) {
+    if (m->var_type[i] != VAR_VARIABLE) continue;
+    if (y[d] < -SMALL) return 1;
+    c->state[i] = y[d] > -SMALL ? y[d] : TINY;
+    ++d;
+  }
+  return 0;
+}
+
+static int cell_rhs(void *ctx, double t, const double *y, double h,
+                    double *ydot) {
+  (void)t;
+  CellCtx *c = (CellCtx *)ctx;
+  if (load_state(c, y)) return 1;
+  double ts = h > 0.0 ? h : c->h0;
+  om_deriv(c->m, c->state, c->rxn_env, ts, ydot, NULL, NULL);
+  return 0;
+}
+
+static int cell_jac(void *ctx, double t, const double *y, double h,
+                    double *jvals) {
+  (void)t;
+  CellCtx *c = (CellCtx *)ctx;
+  if (load_state(c, y)) return 1;
+  om_jac(c->m, c->state, c->rxn_env, h > 0.0 ? h : c->h0, jvals);
+  return 0;
+}
+
+typedef struct {
+  const OracleMech *m;
+  int c0, c1;
+  double *state;
+  const double *env;
+  double *rxn_env;
+  double t0, t1, rtol;
+  const double *abs_tol;
+  int max_steps, max_conv_fails;
+  int *status;
+  OracleStats *stats;
+  int n_fail;
+} SolveJob;
+
+static void *solve_job(void *arg) {
+  SolveJob *jb = (SolveJob *)arg;
+  const OracleMech *m = jb->m;
+  int n = m->n_dep, ns = m->n_state;
+  Bdf b;
+  memset(&b, 0, sizeof(b));
+  BdfWork wk;
+  bdf_alloc(&b, &wk, n, m->n_solver_jac, m->lu.nnz);
+  double *atol = (double *)zalloc(sizeof(double) * (n + 1));
+  for (int i = 0, d = 0; i < ns; ++i)
+    if (m->var_type[i] == VAR_VARIABLE) atol[d++] = jb->abs_tol[i];
+  double *y = (double *)zalloc(sizeof(double) * (n + 1));
+  b.lu = &m->lu;
+  b.n = n;
+  b.annz = m->n_solver_jac;
+  b.f = cell_rhs;
+  b.jac = cell_jac;
+  b.rtol = jb->rtol;
+  b.atol = atol;
+  b.max_steps = jb->max_steps;
+  b.maxncf = jb->max_conv_fails;
+  b.maxnef = jb->max_conv_fails;
+  CellCtx ctx;
+  ctx.m = m;
+  b.ctx = &ctx;
+  for (int c = jb->c0; c < jb->c1; ++c) {
+    double *st = jb->state + (size_t)c * ns;
+    double *re = jb->rxn_env + (size_t)c * m->n_env;
+    /* solver_run: dependent values clamped to >= TINY, constants too
+     * (src/camp_solver.c:554-567); rate constants from env (:587-603) */
+    for (int i = 0, d = 0; i < ns; ++i) {
+      if (m->var_type[i] == VAR_VARIABLE)
+        y[d++] = st[i] > TINY ? st[i] : TINY;
+      else if (m->var_type[i] == 2)
+        st[i] = st[i] > TINY ? st[i] : TINY;
+    }
+    om_update_env(m, jb->env + 2 * (size_t)c, re);
+    ctx.state = st;
+    ctx.rxn_env = re;
+    ctx.h0 = jb->t1 - jb->t0;
+    OracleStats s;
+    int flag = bdf_integrate(&b, jb->t0, jb->t1, jb->t1 - jb->t0, y, &s);
+    if (jb->status) jb->status[c] = flag;
+    if (jb->stats) jb->stats[c] = s;
+    if (flag != OR_SUCCESS) {
+      jb->n_fail++;
+      continue;
+    }
+    for (int i = 0, d = 0; i < ns; ++i)
+      if (m->var_type[i] == VAR_VARIABLE) {
+        st[i] = y[d] > 0.0 ? y[d] : 0.0;
+        ++d;
+      }
+  }
+  free(wk.mem);
+  free(atol);
+  free(y);
+  return NULL;
+}
+
+int om_solve(const OracleMech *m, int n_cells, double *state, const double *env,
+             double *rxn_env, double t0, double t1, double rtol,
+             const double *abs_tol, int max_steps, int max_conv_fails,
+             int n_threads, int *status, OracleStats *stats) {
+  if (!m->built) return -1;
+  if (n_threads < 1) n_threads = 1;
+  if (n_threads > n_cells) n_threads = n_cells > 0 ? n_cells : 1;
+  SolveJob *jobs = (SolveJob *)zalloc(sizeof(SolveJob) * n_threads);
+  pthread_t *th = (pthread_t *)zalloc(sizeof(pthread_t) * n_threads);
+  for (int t = 0; t < n_threads; ++t) {
+    SolveJob *jb = &jobs[t];
+    jb->m = m;
+    jb->c0 = (int)((long)n_cells * t / n_threads);
+    jb->c1 = (int)((long)n_cells * (t + 1) / n_threads);
+    jb->state = state;
+    jb->env = env;
+    jb->rxn_env = rxn_env;
+    jb->t0 = t0;
+    jb->t1 = t1;
+    jb->rtol = rtol;
+    jb->abs_tol = abs_tol;
+    jb->max_steps = max_steps;
+    jb->max_conv_fails = max_conv_fails;
+    jb->status = status;
+    jb->stats = stats;
+  }
+  if (n_threads == 1) {
+    solve_job(&jobs[0]);
+  } else {
+    for (int t = 0; t < n_threads; ++t)
+      pthread_create(&th[t], NULL, solve_job, &jobs[t]);
+    for (int t = 0; t < n_threads; ++t) pthread_join(th[t], NULL);
+  }
+  int nf = 0;
+  for (int t = 0; t < n_threads; ++t) nf += jobs[t].n_fail;
+  free(jobs);
+  free(th);
+  return nf;
+}
+
+int om_solve_cb(const OracleMech *m, int n_cells, double *y_dep, double t0,
+                double t1, double rtol, const double *abs_tol_dep,
+                int max_steps, int max_conv_fails, or_rhs_fn f, or_jac_fn jac,
+                void **ctxs, int *status, OracleStats *stats) {
+  if (!m->built) return -1;
+  int n = m->n_dep;
+  Bdf b;
+  memset(&b, 0, sizeof(b));
+  BdfWork wk;
+  bdf_alloc(&b, &wk, n, m->n_solver_jac, m->lu.nnz);
+  b.lu = &m->lu;
+  b.n = n;
+  b.annz = m->n_solver_jac;
+  b.f = f;
+  b.jac = jac;
+  b.rtol = rtol;
+  b.atol = abs_tol_dep;
+  b.max_steps = max_steps;
+  b.maxncf = max_conv_fails;
+  b.maxnef = max_conv_fails;
+  int nf = 0;
+  for (int c = 0; c < n_cells; ++c) {
+    b.ctx = ctxs[c];
+    double *y = y_dep + (size_t)c * n;
+    OracleStats s;
+    int flag = bdf_integrate(&b, t0, t1, t1 - t0, y, &s);
+    if (status) status[c] = flag;
+    if (stats) stats[c] = s;
+    if (flag != OR_SUCCESS) nf++;
+  }
+  free(wk.mem);
+  return nf;
+}

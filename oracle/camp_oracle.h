@@ -1,0 +1,109 @@
+/* CPU oracle for the CAMP per-cell chemistry solve (TEST INFRASTRUCTURE).
+ *
+ * Only tests/, the smoke check and bench.py's CPU-baseline leg use this
+ * library, as the checker.  The product (libcamp_b200) never links it.
+ *
+ * Contents, each restated from the reference and cited at its definition:
+ *   - gas-phase reaction rate constants, derivative and Jacobian
+ *     contributions for the ARRHENIUS, TROE, CMAQ_H2O2, CMAQ_OH_HNO3 and
+ *     PHOTOLYSIS types (src/rxns/rxn_*.c), with long double accumulators
+ *     as in src/time_derivative.c and src/Jacobian.c;
+ *   - the Jacobian sparsity build and DERIV_ID/JAC_ID update
+ *     (src/Jacobian.c, src/camp_solver.c:1417-1712);
+ *   - a sparse LU of I - gamma*J on a Markowitz diagonal-pivot order (the
+ *     reference uses SuiteSparse KLU, which is not in the reference tree);
+ *   - the variable-order BDF integrator of CVODE (Hindmarsh et al., ACM TOMS
+ *     31(3) 2005 and the CVODE documentation), restated per cell, because the
+ *     reference's modified CVODE 3.4-alpha source is not in the tree.
+ */
+#ifndef CAMP_ORACLE_H
+#define CAMP_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OracleMech OracleMech;
+
+/* Solver outcome codes (CVODE flag values) */
+#define OR_SUCCESS 0
+#define OR_TOO_MUCH_WORK (-1)
+#define OR_TOO_MUCH_ACC (-2)
+#define OR_ERR_FAILURE (-3)
+#define OR_CONV_FAILURE (-4)
+#define OR_LSETUP_FAIL (-6)
+#define OR_RHSFUNC_FAIL (-8)
+#define OR_REPTD_RHSFUNC_ERR (-10)
+#define OR_UNREC_RHSFUNC_ERR (-11)
+#define OR_ILL_INPUT (-22)
+
+/* per-cell statistics (CVODE counters) */
+typedef struct {
+  long nst, nfe, nsetups, netf, nni, ncfn, nje;
+  double hu, hcur;
+  int flag;
+  int qu;
+} OracleStats;
+
+/* Callback form of the right-hand side and Jacobian, so the same BDF can
+ * run on the oracle's own f/J or on the reference's (through ref_glue.c).
+ * f returns 0 on success, >0 for a recoverable failure, <0 unrecoverable.
+ * jac fills the solver Jacobian values in the CSC order of the pattern. */
+typedef int (*or_rhs_fn)(void *ctx, double t, const double *y, double h,
+                         double *ydot);
+typedef int (*or_jac_fn)(void *ctx, double t, const double *y, double h,
+                         double *jvals);
+
+OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn);
+int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
+               const int *ints, const double *floats);
+int om_build(OracleMech *m);
+void om_free(OracleMech *m);
+
+int om_n_dep_var(const OracleMech *m);
+int om_n_rxn_env_data(const OracleMech *m);
+int om_n_rxn_jac_elem(const OracleMech *m);
+int om_n_solver_jac_elem(const OracleMech *m);
+int om_n_lu_elem(const OracleMech *m);
+int om_rxn_int_data_size(const OracleMech *m);
+void om_get_rxn_jac(const OracleMech *m, int *col_ptrs, int *row_ids);
+void om_get_solver_jac(const OracleMech *m, int *col_ptrs, int *row_ids);
+void om_get_rxn_int_data(const OracleMech *m, int *out);
+void om_get_lu_order(const OracleMech *m, int *perm);
+
+/* Photolysis base rate of every reaction whose RXN_ID equals photo_id, in
+ * one cell's rxn_env_data (src/rxns/rxn_photolysis.c:109-124). */
+int om_set_photo_rate(const OracleMech *m, double *rxn_env_cell, int photo_id,
+                      double base_rate);
+/* Rate constants for one cell from env = {T [K], P [Pa]}. */
+void om_update_env(const OracleMech *m, const double *env, double *rxn_env_cell);
+/* One cell's derivative: production, loss and net over dependent vars. */
+void om_deriv(const OracleMech *m, const double *state, const double *rxn_env_cell,
+              double time_step, double *deriv, double *r_p, double *r_l);
+/* One cell's solver Jacobian values (solver CSC order). */
+void om_jac(const OracleMech *m, const double *state, const double *rxn_env_cell,
+            double time_step, double *jvals);
+
+/* Integrates n_cells independent cells from t0 to t1 (per-cell CVODE
+ * semantics), with the oracle's own f/J.  state is [n_cells*n_state_var] and
+ * is updated in place like solver_run; env is [n_cells*2]; rxn_env is
+ * [n_cells*n_rxn_env_data] and must hold the photolysis base rates.
+ * status[c] receives the per-cell flag; stats may be NULL.
+ * Returns the number of failed cells. */
+int om_solve(const OracleMech *m, int n_cells, double *state, const double *env,
+             double *rxn_env, double t0, double t1, double rtol,
+             const double *abs_tol, int max_steps, int max_conv_fails,
+             int n_threads, int *status, OracleStats *stats);
+
+/* The same integrator driven by external f/J callbacks.  ctxs[i] is the
+ * callback context for cell i; the callbacks see only dependent variables.
+ * abs_tol_dep has one entry per dependent variable. */
+int om_solve_cb(const OracleMech *m, int n_cells, double *y_dep, double t0,
+                double t1, double rtol, const double *abs_tol_dep,
+                int max_steps, int max_conv_fails, or_rhs_fn f, or_jac_fn jac,
+                void **ctxs, int *status, OracleStats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

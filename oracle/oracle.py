@@ -1,0 +1,330 @@
+"""ctypes front end of the oracle libraries (TEST INFRASTRUCTURE ONLY).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module, and only as the checker.  The product,
+``camp_b200``, never imports it.
+
+Two libraries live in ``oracle/_ref`` (built by ``oracle/Makefile``):
+
+* ``libcamp_oracle.so`` - the CPU restatement in ``camp_oracle.c``: gas-phase
+  f/J restated from the reference's ``src/rxns/rxn_*.c``, the sparsity build
+  of ``src/camp_solver.c:1417-1712``, a sparse LU, and the CVODE BDF
+  algorithm restated per cell.  Needs only gcc, so it builds anywhere.
+* ``libcamp_ref.so`` - the reference's own reaction/derivative/Jacobian C
+  sources compiled from the reference tree plus ``ref_glue.c``.  Present only
+  where the reference tree was available at build time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+ORACLE_SO = os.path.join(REF_DIR, "libcamp_oracle.so")
+REF_SO = os.path.join(REF_DIR, "libcamp_ref.so")
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+class OracleStats(C.Structure):
+    _fields_ = [
+        ("nst", C.c_long),
+        ("nfe", C.c_long),
+        ("nsetups", C.c_long),
+        ("netf", C.c_long),
+        ("nni", C.c_long),
+        ("ncfn", C.c_long),
+        ("nje", C.c_long),
+        ("hu", C.c_double),
+        ("hcur", C.c_double),
+        ("flag", C.c_int),
+        ("qu", C.c_int),
+    ]
+
+
+def build(with_ref: bool = True) -> None:
+    """Builds the oracle libraries (the reference part only if its tree exists)."""
+    target = "all" if with_ref else "oracle"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+_oracle_lib = None
+_ref_lib = None
+
+
+def oracle_lib():
+    global _oracle_lib
+    if _oracle_lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build(with_ref=False)
+        lib = C.CDLL(ORACLE_SO)
+        vp = C.c_void_p
+        lib.om_new.restype = vp
+        lib.om_new.argtypes = [C.c_int, _i32p, C.c_int]
+        lib.om_add_rxn.restype = C.c_int
+        lib.om_add_rxn.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p]
+        lib.om_build.restype = C.c_int
+        lib.om_build.argtypes = [vp]
+        lib.om_free.argtypes = [vp]
+        for name in (
+            "om_n_dep_var",
+            "om_n_rxn_env_data",
+            "om_n_rxn_jac_elem",
+            "om_n_solver_jac_elem",
+            "om_n_lu_elem",
+            "om_rxn_int_data_size",
+        ):
+            getattr(lib, name).restype = C.c_int
+            getattr(lib, name).argtypes = [vp]
+        lib.om_get_rxn_jac.argtypes = [vp, _i32p, _i32p]
+        lib.om_get_solver_jac.argtypes = [vp, _i32p, _i32p]
+        lib.om_get_rxn_int_data.argtypes = [vp, _i32p]
+        lib.om_get_lu_order.argtypes = [vp, _i32p]
+        lib.om_set_photo_rate.restype = C.c_int
+        lib.om_set_photo_rate.argtypes = [vp, _f64p, C.c_int, C.c_double]
+        lib.om_update_env.argtypes = [vp, _f64p, _f64p]
+        lib.om_deriv.argtypes = [vp, _f64p, _f64p, C.c_double, _f64p, _f64p, _f64p]
+        lib.om_jac.argtypes = [vp, _f64p, _f64p, C.c_double, _f64p]
+        lib.om_solve.restype = C.c_int
+        lib.om_solve.argtypes = [
+            vp, C.c_int, _f64p, _f64p, _f64p, C.c_double, C.c_double, C.c_double,
+            _f64p, C.c_int, C.c_int, C.c_int, _i32p, C.POINTER(OracleStats),
+        ]
+        lib.om_solve_cb.restype = C.c_int
+        lib.om_solve_cb.argtypes = [
+            vp, C.c_int, _f64p, C.c_double, C.c_double, C.c_double, _f64p,
+            C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
+            _i32p, C.POINTER(OracleStats),
+        ]
+        _oracle_lib = lib
+    return _oracle_lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(
+                "oracle/_ref/libcamp_ref.so is absent (it is built from the reference tree)"
+            )
+        lib = C.CDLL(REF_SO)
+        vp = C.c_void_p
+        lib.ref_new.restype = vp
+        lib.ref_new.argtypes = [C.c_int, C.c_int, _i32p] + [C.c_int] * 15
+        lib.rxn_add_condensed_data.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p, vp]
+        lib.ref_build.restype = C.c_int
+        lib.ref_build.argtypes = [vp]
+        for name in (
+            "ref_n_dep_var",
+            "ref_n_rxn_jac_elem",
+            "ref_n_solver_jac_elem",
+            "ref_n_mapped_values",
+            "ref_n_rxn_env_data",
+            "ref_rxn_int_data_size",
+        ):
+            getattr(lib, name).restype = C.c_int
+            getattr(lib, name).argtypes = [vp]
+        lib.ref_get_rxn_jac.argtypes = [vp, _i32p, _i32p]
+        lib.ref_get_solver_jac.argtypes = [vp, _i32p, _i32p]
+        lib.ref_get_jac_map.argtypes = [vp, _i32p]
+        lib.ref_get_rxn_int_data.argtypes = [vp, _i32p]
+        lib.ref_get_rxn_env_data.argtypes = [vp, C.c_int, _f64p]
+        lib.ref_set_rxn_env_data.argtypes = [vp, C.c_int, _f64p]
+        lib.ref_set_state.argtypes = [vp, _f64p, _f64p]
+        lib.ref_update_env.argtypes = [vp, C.c_int]
+        lib.ref_calc_deriv.argtypes = [vp, C.c_int, C.c_double, _f64p, _f64p, _f64p]
+        lib.ref_calc_jac.argtypes = [vp, C.c_int, C.c_double, _f64p, _f64p]
+        lib.ref_free.argtypes = [vp]
+        lib.rxn_update_data.argtypes = [C.c_int, C.POINTER(C.c_int), C.c_int, vp, vp]
+        lib.rxn_photolysis_create_rate_update_data.restype = vp
+        lib.rxn_photolysis_set_rate_update_data.argtypes = [vp, C.c_int, C.c_double]
+        _ref_lib = lib
+    return _ref_lib
+
+
+class OracleModel:
+    """The oracle's restated mechanism, built from packed reaction blocks."""
+
+    def __init__(self, mech):
+        self.lib = oracle_lib()
+        self.mech = mech
+        self.h = self.lib.om_new(mech.n_state_var, np.ascontiguousarray(mech.var_type, np.int32), mech.n_rxn)
+        for r in mech.rxns:
+            rc = self.lib.om_add_rxn(
+                self.h, r.rxn_type, r.ints.size, r.floats.size, r.n_env,
+                np.ascontiguousarray(r.ints, np.int32), np.ascontiguousarray(r.floats, np.float64),
+            )
+            if rc != 0:
+                raise ValueError(f"oracle rejected reaction type {r.rxn_type} (code {rc})")
+        if self.lib.om_build(self.h) != 0:
+            raise RuntimeError("oracle sparsity build failed")
+        self.n_dep = self.lib.om_n_dep_var(self.h)
+        self.n_env = self.lib.om_n_rxn_env_data(self.h)
+        self.n_rxn_jac = self.lib.om_n_rxn_jac_elem(self.h)
+        self.n_jac = self.lib.om_n_solver_jac_elem(self.h)
+        self.n_lu = self.lib.om_n_lu_elem(self.h)
+
+    def __del__(self):
+        try:
+            self.lib.om_free(self.h)
+        except Exception:
+            pass
+
+    def solver_jac(self):
+        cp = np.zeros(self.n_dep + 1, np.int32)
+        ri = np.zeros(max(self.n_jac, 1), np.int32)
+        self.lib.om_get_solver_jac(self.h, cp, ri)
+        return cp, ri[: self.n_jac]
+
+    def rxn_jac(self):
+        cp = np.zeros(self.mech.n_state_var + 1, np.int32)
+        ri = np.zeros(max(self.n_rxn_jac, 1), np.int32)
+        self.lib.om_get_rxn_jac(self.h, cp, ri)
+        return cp, ri[: self.n_rxn_jac]
+
+    def rxn_int_data(self):
+        out = np.zeros(self.lib.om_rxn_int_data_size(self.h), np.int32)
+        self.lib.om_get_rxn_int_data(self.h, out)
+        return out
+
+    def lu_order(self):
+        out = np.zeros(self.n_dep, np.int32)
+        self.lib.om_get_lu_order(self.h, out)
+        return out
+
+    def rxn_env(self, env, photo_rates: dict[int, float] | None = None):
+        """One cell's rate constants for env=(T, P) and photolysis base rates."""
+        re = np.zeros(max(self.n_env, 1), np.float64)
+        for pid, rate in (photo_rates or {}).items():
+            self.lib.om_set_photo_rate(self.h, re, int(pid), float(rate))
+        self.lib.om_update_env(self.h, np.asarray(env, np.float64), re)
+        return re
+
+    def deriv(self, state, rxn_env, time_step):
+        f = np.zeros(self.n_dep)
+        rp = np.zeros(self.n_dep)
+        rl = np.zeros(self.n_dep)
+        self.lib.om_deriv(self.h, np.ascontiguousarray(state, np.float64), rxn_env, float(time_step), f, rp, rl)
+        return f, rp, rl
+
+    def jac(self, state, rxn_env, time_step):
+        j = np.zeros(max(self.n_jac, 1))
+        self.lib.om_jac(self.h, np.ascontiguousarray(state, np.float64), rxn_env, float(time_step), j)
+        return j[: self.n_jac]
+
+    def solve(self, state, env, photo_rates, t0, t1, rtol, abs_tol, max_steps=10000,
+              max_conv_fails=1000, n_threads=1):
+        """Per-cell solve; state [n_cells, n_state_var] is updated in place.
+
+        photo_rates is [n_cells, n_photo] of base rates for photolysis ids
+        1..n_photo.  Returns (n_failed, status, stats)."""
+        state = np.ascontiguousarray(state, np.float64)
+        n_cells = state.shape[0]
+        env = np.ascontiguousarray(env, np.float64).reshape(n_cells, 2)
+        re = np.zeros((n_cells, max(self.n_env, 1)), np.float64)
+        photo_rates = np.asarray(photo_rates, np.float64).reshape(n_cells, -1)
+        for c in range(n_cells):
+            for pid in range(photo_rates.shape[1]):
+                self.lib.om_set_photo_rate(self.h, re[c], pid + 1, float(photo_rates[c, pid]))
+        status = np.zeros(n_cells, np.int32)
+        stats = (OracleStats * n_cells)()
+        nf = self.lib.om_solve(
+            self.h, n_cells, state, env, re, float(t0), float(t1), float(rtol),
+            np.ascontiguousarray(abs_tol, np.float64), int(max_steps), int(max_conv_fails),
+            int(n_threads), status, stats,
+        )
+        return nf, status, stats, state
+
+
+class RefModel:
+    """The reference's own C code for one or more cells (via ref_glue.c)."""
+
+    def __init__(self, mech, n_cells: int = 1):
+        self.lib = ref_lib()
+        self.mech = mech
+        self.n_cells = n_cells
+        self.h = self.lib.ref_new(
+            mech.n_state_var, n_cells, np.ascontiguousarray(mech.var_type, np.int32),
+            mech.n_rxn, mech.n_rxn_int_param, mech.n_rxn_float_param, mech.n_rxn_env_param,
+            0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+        )
+        for r in mech.rxns:
+            self.lib.rxn_add_condensed_data(
+                r.rxn_type, r.ints.size, r.floats.size, r.n_env,
+                np.ascontiguousarray(r.ints, np.int32), np.ascontiguousarray(r.floats, np.float64), self.h,
+            )
+        rc = self.lib.ref_build(self.h)
+        if rc != 0:
+            raise RuntimeError(f"reference sparsity build failed ({rc})")
+        self.n_dep = self.lib.ref_n_dep_var(self.h)
+        self.n_rxn_jac = self.lib.ref_n_rxn_jac_elem(self.h)
+        self.n_jac = self.lib.ref_n_solver_jac_elem(self.h)
+        self.n_env = self.lib.ref_n_rxn_env_data(self.h)
+        self.state = np.zeros((n_cells, mech.n_state_var))
+        self.env = np.zeros((n_cells, 2))
+        self.lib.ref_set_state(self.h, self.state.reshape(-1), self.env.reshape(-1))
+
+    def solver_jac(self):
+        cp = np.zeros(self.n_dep + 1, np.int32)
+        ri = np.zeros(max(self.n_jac, 1), np.int32)
+        self.lib.ref_get_solver_jac(self.h, cp, ri)
+        return cp, ri[: self.n_jac]
+
+    def rxn_jac(self):
+        cp = np.zeros(self.mech.n_state_var + 1, np.int32)
+        ri = np.zeros(max(self.n_rxn_jac, 1), np.int32)
+        self.lib.ref_get_rxn_jac(self.h, cp, ri)
+        return cp, ri[: self.n_rxn_jac]
+
+    def jac_map(self):
+        n = self.lib.ref_n_mapped_values(self.h)
+        out = np.zeros(3 * max(n, 1), np.int32)
+        self.lib.ref_get_jac_map(self.h, out)
+        return out[: 3 * n].reshape(n, 3)
+
+    def rxn_int_data(self):
+        """Packed reaction ints (with type slots) after rxn_update_ids."""
+        out = np.zeros(self.lib.ref_rxn_int_data_size(self.h), np.int32)
+        self.lib.ref_get_rxn_int_data(self.h, out)
+        return out
+
+    def set_photo_rate(self, cell: int, photo_id: int, rate: float) -> None:
+        """Goes through the reference's rxn_update_data path."""
+        ud = self.lib.rxn_photolysis_create_rate_update_data()
+        self.lib.rxn_photolysis_set_rate_update_data(ud, int(photo_id), float(rate))
+        rid = C.c_int(0)
+        self.lib.rxn_update_data(int(cell), C.byref(rid), 5, ud, self.h)
+
+    def set_cell(self, cell, state, env):
+        self.state[cell, :] = state
+        self.env[cell, :] = env
+
+    def update_env(self, cell):
+        self.lib.ref_update_env(self.h, int(cell))
+
+    def rxn_env(self, cell):
+        out = np.zeros(max(self.n_env, 1))
+        self.lib.ref_get_rxn_env_data(self.h, int(cell), out)
+        return out
+
+    def deriv(self, cell, time_step):
+        f = np.zeros(self.n_dep)
+        rp = np.zeros(self.n_dep)
+        rl = np.zeros(self.n_dep)
+        self.lib.ref_calc_deriv(self.h, int(cell), float(time_step), f, rp, rl)
+        return f, rp, rl
+
+    def jac(self, cell, time_step):
+        jr = np.zeros(max(self.n_rxn_jac, 1))
+        js = np.zeros(max(self.n_jac, 1))
+        self.lib.ref_calc_jac(self.h, int(cell), float(time_step), jr, js)
+        return js[: self.n_jac], jr[: self.n_rxn_jac]

@@ -1,0 +1,1 @@
+#include "../sundials_shim.h"

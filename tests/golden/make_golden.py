@@ -1,0 +1,115 @@
+"""Generates the committed golden fixtures from the reference (run here only).
+
+    python tests/golden/make_golden.py [REFERENCE_ROOT]
+
+Outputs (all small):
+  cb05cl_ae5.mech.json   packed cb05cl_ae5 mechanism as the Fortran caller
+                         would hand it to rxn_add_condensed_data (packer:
+                         camp_b200/mechanism.py), with the photolysis ids the
+                         reference's cb05 test assigns
+  cb05cl_ae5_ref.npz     outputs of the reference's own C code
+                         (oracle/_ref/libcamp_ref.so, compiled from the
+                         reference sources) on seeded cell states:
+                         sparsity (solver CSC, reaction CSC, jac_map, packed
+                         ints after rxn_update_ids), per-cell rate constants,
+                         production/loss/net derivative and solver Jacobian
+                         at several time steps
+
+The cell states follow the workload distribution (camp_b200/cells.py, seed
+20241203) plus a few edge-case cells: concentrations exactly at TINY, a dark
+cell (all photolysis rates zero) and a cell where PAR is nearly exhausted so
+the negative-yield guard of the reference switches contributions off.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from camp_b200.cells import make_cells  # noqa: E402
+from camp_b200.mechanism import load_mechanism  # noqa: E402
+
+SEED = 20241203
+H_VALUES = (1.0e-6, 1.0, 60.0)
+
+
+def cb05_files(ref_root: str) -> list[str]:
+    return [
+        os.path.join(ref_root, "mechanisms/cb05cl_ae5/cb05cl_ae5_mechanism.json"),
+        os.path.join(ref_root, "mechanisms/cb05cl_ae5/cb05cl_ae5_species.json"),
+        os.path.join(ref_root, "test/chemistry/cb05cl_ae5/cb05cl_ae5_init.json"),
+    ]
+
+
+def edge_cells(mech, cells):
+    """Appends edge-case cells to a seeded batch."""
+    st, env, ph = cells.state.copy(), cells.env.copy(), cells.photo_rates.copy()
+    extra_s, extra_e, extra_p = [], [], []
+    var = mech.var_type == 1
+    # concentrations at TINY
+    s = st[0].copy()
+    s[var] = 1.0e-60
+    extra_s.append(s); extra_e.append([298.0, 101325.0]); extra_p.append(ph[0])
+    # dark cell
+    extra_s.append(st[1].copy()); extra_e.append(env[1]); extra_p.append(np.zeros_like(ph[1]))
+    # PAR nearly exhausted while its negative-yield producers are abundant
+    s = st[2].copy()
+    s[mech.index("PAR")] = 1.0e-12
+    for name in ("ROR", "OLE", "IOLE", "ISOP", "TERP"):
+        if name in mech.species:
+            s[mech.index(name)] = 50.0
+    extra_s.append(s); extra_e.append([300.0, 1.0e5]); extra_p.append(ph[2])
+    return (np.vstack([st, np.asarray(extra_s)]), np.vstack([env, np.asarray(extra_e)]),
+            np.vstack([ph, np.asarray(extra_p)]))
+
+
+def main(ref_root: str) -> None:
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import RefModel, build  # noqa: E402
+
+    build(with_ref=True)
+    mech = load_mechanism(cb05_files(ref_root), name="cb05cl_ae5")
+    mech.rel_tol = 1.0e-4
+    mech.abs_tol[:] = 1.0e-8
+    mech.save(os.path.join(HERE, "cb05cl_ae5.mech.json"))
+
+    cells = make_cells(mech, 8, SEED)
+    state, env, photo = edge_cells(mech, cells)
+    nc = state.shape[0]
+    ref = RefModel(mech, nc)
+    out = {}
+    cp, ri = ref.solver_jac()
+    out["solver_colptr"], out["solver_rowid"] = cp, ri
+    rcp, rri = ref.rxn_jac()
+    out["rxn_colptr"], out["rxn_rowid"] = rcp, rri
+    out["jac_map"] = ref.jac_map()
+    out["rxn_int_data"] = ref.rxn_int_data()
+    out["state"], out["env"], out["photo"] = state, env, photo
+    out["h"] = np.asarray(H_VALUES)
+    rxn_env, F, RP, RL, J = [], [], [], [], []
+    for c in range(nc):
+        ref.set_cell(c, state[c], env[c])
+        for pid in range(photo.shape[1]):
+            ref.set_photo_rate(c, pid + 1, photo[c, pid])
+        ref.update_env(c)
+        rxn_env.append(ref.rxn_env(c))
+    for h in H_VALUES:
+        fs, rps, rls, js = [], [], [], []
+        for c in range(nc):
+            f, rp, rl = ref.deriv(c, h)
+            j, _ = ref.jac(c, h)
+            fs.append(f); rps.append(rp); rls.append(rl); js.append(j)
+        F.append(fs); RP.append(rps); RL.append(rls); J.append(js)
+    out["rxn_env"] = np.asarray(rxn_env)
+    out["f"], out["r_p"], out["r_l"], out["jac"] = (np.asarray(x) for x in (F, RP, RL, J))
+    np.savez_compressed(os.path.join(HERE, "cb05cl_ae5_ref.npz"), **out)
+    print("wrote", nc, "cells;", "jac nnz", len(ri), "rxn jac nnz", len(rri))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

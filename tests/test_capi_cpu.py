@@ -1,0 +1,100 @@
+"""The C-ABI library without a GPU: it loads, exports every declared entry
+point, and its host-side sparsity build is bit-exact with the reference's."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, gpu_available
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "camp_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    txt = "\n".join(l for l in txt.splitlines() if not l.lstrip().startswith("#"))
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", txt)
+    skip = {"extern", "if", "while", "sizeof"}
+    return sorted({n for n in names if n not in skip})
+
+
+def test_exports_every_declared_symbol(lib):
+    from camp_b200 import _lib
+
+    names = header_functions()
+    assert len(names) >= 40
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in include/camp_b200.h but not exported"
+    assert sorted(_lib.EXPORTED) == names
+
+
+def test_sparsity_via_c_abi(cb05, cb05_ref, lib):
+    from camp_b200.solver import Solver
+
+    s = Solver(cb05, 4)
+    s.build_sparsity_only()
+    if not gpu_available():
+        assert not s.ready
+    cp, ri = s.solver_jac()
+    assert np.array_equal(cp, cb05_ref["solver_colptr"])
+    assert np.array_equal(ri, cb05_ref["solver_rowid"])
+    # DERIV_ID_/JAC_ID_ of every reaction, bit for bit
+    assert np.array_equal(s.rxn_int_data(), cb05_ref["rxn_int_data"])
+    perm = s.lu_order()
+    assert sorted(perm.tolist()) == list(range(74))
+    assert s.n_lu() <= 748
+
+
+def test_photolysis_update_data_layout(lib):
+    """int photo id followed, unaligned, by the double base rate
+    (src/rxns/rxn_photolysis.c:262-283)."""
+    ud = lib.rxn_photolysis_create_rate_update_data()
+    lib.rxn_photolysis_set_rate_update_data(ud, 7, 2.5e-3)
+    raw = C.string_at(ud, 12)
+    assert int.from_bytes(raw[:4], "little", signed=True) == 7
+    assert np.frombuffer(raw[4:12], np.float64)[0] == 2.5e-3
+    lib.solver_free_update_data(ud)
+
+
+def test_rejects_unsupported(cb05, lib):
+    """Aerosol sub-models are refused at initialize with a readable error."""
+    from camp_b200 import _lib
+
+    m = cb05
+    h = lib.solver_new(m.n_state_var, 1, np.ascontiguousarray(m.var_type, np.int32), m.n_rxn,
+                       m.n_rxn_int_param, m.n_rxn_float_param, m.n_rxn_env_param,
+                       0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0)
+    for r in m.rxns:
+        lib.rxn_add_condensed_data(r.rxn_type, r.ints.size, r.floats.size, r.n_env,
+                                   np.ascontiguousarray(r.ints, np.int32),
+                                   np.ascontiguousarray(r.floats), h)
+    lib.solver_initialize(h, np.ascontiguousarray(m.abs_tol), 1e-4, 100, 10)
+    assert lib.camp_b200_is_ready(h) == 0
+    assert "sub-models" in _lib.last_error()
+    st = np.zeros(m.n_state_var)
+    env = np.array([298.0, 1e5])
+    assert lib.solver_run(h, st, env, 0.0, 1.0) == 1
+    lib.solver_free(h)
+
+
+def test_packer_matches_fixture(cb05):
+    """Re-packing the reference JSON reproduces the committed packed data."""
+    ref = "/root/reference"
+    if not os.path.isdir(ref):
+        pytest.skip("reference tree absent")
+    import sys
+
+    sys.path.insert(0, GOLDEN)
+    from make_golden import cb05_files
+
+    from camp_b200.mechanism import load_mechanism, reaction_summary
+
+    m = load_mechanism(cb05_files(ref), name="cb05cl_ae5")
+    assert m.n_rxn == 186 and m.n_dep_var == 74
+    summ = reaction_summary(m)
+    assert summ["by_type"] == {5: 25, 1: 142, 2: 15, 4: 1, 3: 3}
+    for a, b in zip(m.rxns, cb05.rxns):
+        assert a.rxn_type == b.rxn_type
+        assert np.array_equal(a.ints, b.ints)
+        assert np.array_equal(a.floats, b.floats)

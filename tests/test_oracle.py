@@ -1,0 +1,117 @@
+"""The CPU oracle pinned against the reference's own C code.
+
+The golden fixture (tests/golden/cb05cl_ae5_ref.npz) holds the reference's
+sparsity, rate constants, derivative and Jacobian on seeded cb05cl_ae5 cells,
+computed by the reference's C sources (tests/golden/make_golden.py).  The
+oracle's restatement must reproduce the sparsity bit-exactly and the
+numbers to 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleModel, ref_available
+
+
+@pytest.fixture(scope="module")
+def om(cb05):
+    return OracleModel(cb05)
+
+
+def test_sparsity_bit_exact(om, cb05_ref):
+    cp, ri = om.solver_jac()
+    assert np.array_equal(cp, cb05_ref["solver_colptr"])
+    assert np.array_equal(ri, cb05_ref["solver_rowid"])
+    rcp, rri = om.rxn_jac()
+    assert np.array_equal(rcp, cb05_ref["rxn_colptr"])
+    assert np.array_equal(rri, cb05_ref["rxn_rowid"])
+    # DERIV_ID_/JAC_ID_ written back into the packed ints
+    assert np.array_equal(om.rxn_int_data(), cb05_ref["rxn_int_data"])
+
+
+def test_sizes(om):
+    assert om.n_dep == 74
+    assert om.n_jac == 671
+    assert om.n_rxn_jac == 716
+
+
+def _photo_dict(row):
+    return {pid + 1: float(row[pid]) for pid in range(row.size)}
+
+
+def test_rate_constants(om, cb05_ref):
+    for c in range(cb05_ref["state"].shape[0]):
+        re = om.rxn_env(cb05_ref["env"][c], _photo_dict(cb05_ref["photo"][c]))
+        np.testing.assert_allclose(re, cb05_ref["rxn_env"][c], rtol=1e-15, atol=0)
+
+
+def test_deriv_and_jacobian(om, cb05_ref):
+    for ih, h in enumerate(cb05_ref["h"]):
+        for c in range(cb05_ref["state"].shape[0]):
+            re = cb05_ref["rxn_env"][c]
+            st = cb05_ref["state"][c]
+            f, rp, rl = om.deriv(st, re, h)
+            np.testing.assert_allclose(rp, cb05_ref["r_p"][ih][c], rtol=1e-12, atol=0)
+            np.testing.assert_allclose(rl, cb05_ref["r_l"][ih][c], rtol=1e-12, atol=0)
+            scale = cb05_ref["r_p"][ih][c] + cb05_ref["r_l"][ih][c]
+            assert np.all(np.abs(f - cb05_ref["f"][ih][c]) <= 1e-12 * scale)
+            j = om.jac(st, re, h)
+            jr = cb05_ref["jac"][ih][c]
+            assert np.all(np.abs(j - jr) <= 1e-12 * np.abs(jr) + 1e-300)
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference build absent")
+def test_live_against_reference_build(cb05, om):
+    """Fresh random states through the reference build and the oracle."""
+    from camp_b200.cells import make_cells
+    from oracle.oracle import RefModel
+
+    cells = make_cells(cb05, 5, 777)
+    ref = RefModel(cb05, 5)
+    for c in range(5):
+        ref.set_cell(c, cells.state[c], cells.env[c])
+        for pid in range(cells.photo_rates.shape[1]):
+            ref.set_photo_rate(c, pid + 1, cells.photo_rates[c, pid])
+        ref.update_env(c)
+        re = om.rxn_env(cells.env[c], _photo_dict(cells.photo_rates[c]))
+        assert np.array_equal(re, ref.rxn_env(c))
+        for h in (1e-3, 30.0):
+            f1, p1, l1 = ref.deriv(c, h)
+            f2, p2, l2 = om.deriv(cells.state[c], re, h)
+            np.testing.assert_allclose(p2, p1, rtol=1e-12, atol=0)
+            np.testing.assert_allclose(l2, l1, rtol=1e-12, atol=0)
+            j1, _ = ref.jac(c, h)
+            j2 = om.jac(cells.state[c], re, h)
+            assert np.all(np.abs(j2 - j1) <= 1e-12 * np.abs(j1) + 1e-300)
+
+
+def test_lu_fill_vs_kpp(om):
+    """Fill of the Markowitz order against KPP's generated cb05 LU
+    (LU_NONZERO = 748, test/chemistry/cb05cl_ae5/cb05cl_ae5_Parameters.f90)."""
+    assert om.n_lu <= 748
+
+
+def test_bdf_consecutive_first_order(cb05):
+    """A -> B -> C with first-order rates against the closed form, the check
+    the reference's per-reaction unit tests make
+    (test/unit_rxn_data/test_rxn_photolysis.F90:288-311)."""
+    from camp_b200.mechanism import Mechanism, PackedRxn
+
+    k1, k2 = 0.05, 0.3
+    # two photolysis reactions, base rates k1 and k2
+    rx = []
+    for (a, b) in ((1, 2), (2, 3)):
+        ints = np.zeros(3 + (1 + 2) * 2, np.int32)
+        ints[0], ints[1], ints[2], ints[3], ints[4] = 1, 1, len(rx) + 1, a, b
+        rx.append(PackedRxn(5, ints, np.array([1.0, 1.0]), 2))
+    mech = Mechanism("abc", ["A", "B", "C"], np.array([1, 1, 1], np.int32),
+                     np.full(3, 1e-12), 1e-10, rx, {1: 0, 2: 1})
+    om = OracleModel(mech)
+    t = 40.0
+    y0 = np.array([[1.0, 0.0, 0.0]])
+    nf, status, stats, out = om.solve(y0.copy(), np.array([[298.0, 1e5]]),
+                                      np.array([[k1, k2]]), 0.0, t, 1e-10, np.full(3, 1e-14))
+    assert nf == 0 and status[0] == 0
+    A = np.exp(-k1 * t)
+    B = k1 / (k2 - k1) * (np.exp(-k1 * t) - np.exp(-k2 * t))
+    C = 1.0 - A - B
+    np.testing.assert_allclose(out[0], [A, B, C], rtol=1e-7, atol=1e-12)
