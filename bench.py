@@ -1,0 +1,392 @@
+"""Benchmark: cell-steps/s of the per-cell chemistry solve on B200.
+
+Workload (default): the cb05cl_ae5 gas-phase mechanism (74 dependent species,
+186 reactions) on 100 000 seeded synthetic cells, host steps of 60 s, rtol
+1e-4, atol 1e-8 ppm, the reference's default limits (10 000 internal steps,
+1 000 convergence / error-test failures).  Cell states: T ~ U(260, 310) K,
+P ~ U(5e4, 1.013e5) Pa, photolysis = 1e-4 s^-1 base set (jo2 = 0) x U[0,1],
+variable species log-uniform 1e-6..1e2 ppm (seed 20241203).
+
+One bench "step" is one host time step: every cell advanced over 60 s by its
+own BDF integration.  The 10-step sequence of the workload restarts from the
+seeded initial state every 10 steps.  value = cells x steps / device time of
+the timed steps (CUDA events on the launch stream, L2 flushed between steps),
+max over ranks; e2e = the same through solver_run with pinned host buffers
+(host<->device copies inside the timed region, host clock).
+
+--impl reference times the reference's own C derivative/Jacobian code
+(compiled from the reference sources into oracle/_ref) driven by the restated
+CVODE BDF and sparse LU on all host cores, on a bounded sample of the same
+workload (the same 10-step sequence for a subset of the cells).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 20241203
+MECH_FILE = os.path.join(ROOT, "tests", "golden", "cb05cl_ae5.mech.json")
+# compulsory HBM bytes per cell-step of cb05cl_ae5: state read (80 x 8),
+# env (16), photolysis base rates (25 x 8), dependent state write (74 x 8)
+METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=100000)
+    ap.add_argument("--dt", type=float, default=60.0)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=128)
+    ap.add_argument("--max-steps", type=int, default=10000)
+    return ap.parse_args()
+
+
+def bytes_per_cell_step(mech) -> int:
+    n_photo = sum(1 for r in mech.rxns if r.rxn_type == 5)
+    return 8 * mech.n_state_var + 16 + 8 * n_photo + 8 * mech.n_dep_var
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference arm
+# ---------------------------------------------------------------------------
+def cpu_reference_run(mech, cells, steps, warmup, dt, sample, max_steps):
+    """Times the reference's C f/J + restated BDF on all host cores; each step
+    is the same host step of the 10-step sequence for `sample` cells."""
+    from oracle.oracle import ref_available, ref_solve, OracleModel
+
+    n_threads = os.cpu_count() or 1
+    atol = np.full(mech.n_state_var, 1e-8)
+    kind = "reference" if ref_available() else "port"
+    sub = cells.slice(0, sample)
+    state = sub.state.copy()
+    times = []
+    om = None if kind == "reference" else OracleModel(mech)
+    for it in range(warmup + steps):
+        if it % 10 == 0:
+            state = sub.state.copy()
+        t0 = time.perf_counter()
+        if kind == "reference":
+            ref_solve(mech, state, sub.env, sub.photo_rates, 0.0, dt, 1e-4, atol,
+                      max_steps=max_steps, n_threads=n_threads)
+        else:
+            om.solve(state, sub.env, sub.photo_rates, 0.0, dt, 1e-4, atol,
+                     max_steps=max_steps, n_threads=n_threads)
+        if it >= warmup:
+            times.append(time.perf_counter() - t0)
+    per_step = float(np.mean(times))
+    return {
+        "value": sample / per_step,
+        "unit": "cell-steps/s",
+        "cores": n_threads,
+        "kind": kind,
+        "sample": (f"{sample} cells x {steps} host steps of {dt:g} s (the workload's 10-step "
+                   f"sequence for the first {sample} seeded cells); "
+                   + ("reference C f/J compiled from the reference sources + restated "
+                      "CVODE BDF / sparse LU" if kind == "reference" else
+                      "oracle C restatement of the reference f/J + restated CVODE BDF / sparse LU")),
+        "ms_per_step": per_step * 1e3,
+    }
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_init()
+    if rank != 0:
+        return
+    from camp_b200.cells import make_cells
+    from camp_b200.mechanism import Mechanism
+
+    mech = Mechanism.load(MECH_FILE)
+    cells = make_cells(mech, args.cpu_sample, SEED)
+    cb = cpu_reference_run(mech, cells, args.steps, args.warmup, args.dt, args.cpu_sample,
+                           args.max_steps)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": cb["value"],
+        "unit": "cell-steps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": cb["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "cb05cl_ae5 cell states, host steps of 60 s, rtol 1e-4, atol 1e-8 ppm",
+                   "cells_per_step": args.cpu_sample, "dt_s": args.dt},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu_arm(args):
+    world, rank, local = dist_init()
+    import torch
+
+    torch.cuda.set_device(local)
+    from camp_b200.cells import make_cells
+    from camp_b200.mechanism import Mechanism
+    from camp_b200.solver import FP64, MIXED, Solver
+
+    mech = Mechanism.load(MECH_FILE)
+    n = args.cells
+    cells = make_cells(mech, n, SEED + 7919 * rank)
+    atol = np.full(mech.n_state_var, 1e-8)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def make_solver(prec):
+        s = Solver(mech, n)
+        s.initialize(abs_tol=atol, rel_tol=1e-4, max_steps=args.max_steps)
+        s.set_precision(prec)
+        s.set_photo_rates(cells.photo_rates)
+        return s
+
+    init_state = torch.from_numpy(cells.state).to(dev)
+    d_env = torch.from_numpy(cells.env).to(dev)
+
+    def device_run(s, steps, warmup):
+        """warmup + timed host steps on device-resident inputs."""
+        d_state = init_state.clone()
+        step_ms, ok_cells, launches0 = [], [], None
+        kernel_ms = []
+        for it in range(warmup + steps):
+            if it % 10 == 0:
+                d_state.copy_(init_state)
+            flush.zero_()
+            if it == warmup:
+                barrier(world)
+                torch.cuda.synchronize()
+                launches0 = s.kernel_launches()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.launch_device(d_state, d_env, n, 0.0, args.dt, stream)
+            e1.record(stream)
+            s.sync_status(stream)
+            if it >= warmup:
+                torch.cuda.synchronize()
+                step_ms.append(e0.elapsed_time(e1))
+                kernel_ms.append(s.last_kernel_ms())
+                st = s.cell_stats(n)
+                ok_cells.append(int(np.count_nonzero(st["status"] == 0)))
+        torch.cuda.synchronize()
+        barrier(world)
+        launches = s.kernel_launches() - launches0
+        return step_ms, kernel_ms, ok_cells, launches, s.cell_stats(n)
+
+    prec = MIXED if args.precision == "mixed" else FP64
+    solver = make_solver(prec)
+    with ClockSampler(local) as clk:
+        step_ms, kernel_ms, ok_cells, launches, last_stats = device_run(solver, args.steps, args.warmup)
+    total_s = max_over_ranks(sum(step_ms) / 1e3, world)
+    value = world * n * args.steps / total_s
+    fp64 = None
+    if not args.no_fp64_compare:
+        s64 = make_solver(FP64)
+        sm64, km64, ok64, _, _ = device_run(s64, args.steps, min(args.warmup, 3))
+        t64 = max_over_ranks(sum(sm64) / 1e3, world)
+        fp64 = {"value": world * n * args.steps / t64, "unit": "cell-steps/s",
+                "ms_per_step": 1e3 * t64 / args.steps,
+                "ok_cell_fraction": float(np.mean(ok64)) / n}
+        s64.free()
+    e2e = None
+    if not args.no_e2e:
+        # pinned host buffers; copies inside the timed region
+        h_state = torch.empty((n, mech.n_state_var), dtype=torch.float64, pin_memory=True)
+        h_env = torch.from_numpy(cells.env).pin_memory()
+        hs, he = h_state.numpy(), h_env.numpy()
+        times = []
+        for it in range(args.warmup + args.steps):
+            if it % 10 == 0:
+                hs[:] = cells.state
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            solver.solve(hs, he, 0.0, args.dt)
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        te = max_over_ranks(sum(times), world)
+        n_photo = solver.n_photo
+        e2e = {"value": world * n * args.steps / te, "unit": "cell-steps/s",
+               "h2d_bytes_per_step": int(8 * n * (mech.n_state_var + 2 + n_photo)),
+               "d2h_bytes_per_step": int(8 * n * mech.n_state_var + 56 * n)}
+    if rank != 0:
+        return
+    cb = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu_cells = make_cells(mech, args.cpu_sample, SEED)
+        cb = cpu_reference_run(mech, cpu_cells, min(args.steps, 10), 1, args.dt, args.cpu_sample,
+                               args.max_steps)
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    bpcs = bytes_per_cell_step(mech)
+    mean_kernel_s = float(np.mean(kernel_ms)) / 1e3
+    achieved = bpcs * n / mean_kernel_s / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64+f32 (mixed: FP32 Jacobian/LU, FP64 residual/state/error test)"
+                 if prec == MIXED else "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": "cb05cl_ae5, 1e5 cells per GPU, host steps of 60 s (10-step sequence), "
+                        "rtol 1e-4, atol 1e-8 ppm, max 10000 internal steps",
+            "cells_per_gpu": n, "dt_s": args.dt, "precision": args.precision,
+            "l2": "flushed (256 MB write) before every timed step",
+            "seed": SEED,
+        },
+        "ok_cell_fraction": float(np.mean(ok_cells)) / n,
+        "internal_steps_per_cell_step": float(np.mean(last_stats["nst"])),
+        "fp64": fp64,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": None,
+            "note": f"{bpcs} compulsory bytes per cell-step x cells / mean solve-kernel time "
+                    "(of measured peak); the kernel is FP64/issue-latency bound, not HBM bound",
+        },
+        "cpu_baseline": cb,
+    }
+    print(json.dumps(line), flush=True)
+    solver.free()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

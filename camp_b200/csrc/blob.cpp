@@ -1,0 +1,261 @@
+// Builds the compact shared-memory tables of the solve kernel (blob.hpp).
+#include "blob.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <numeric>
+
+#include "model.hpp"
+
+namespace campb {
+
+namespace {
+
+constexpr int kLanes = 32;
+constexpr uint16_t kNoSlot = 0xFFFF;
+
+struct Writer {
+  std::vector<uint8_t> buf;
+  template <typename T>
+  int put(const std::vector<T>& v) {
+    size_t off = (buf.size() + 15) & ~size_t(15);
+    buf.resize(off + std::max<size_t>(v.size(), 1) * sizeof(T), 0);
+    if (!v.empty()) memcpy(buf.data() + off, v.data(), v.size() * sizeof(T));
+    return (int)off;
+  }
+};
+
+// Longest-processing-time assignment of weighted items to the 32 lanes.
+std::vector<std::vector<int>> lpt(const std::vector<long>& weight) {
+  std::vector<int> idx(weight.size());
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return weight[a] > weight[b]; });
+  std::vector<long> load(kLanes, 0);
+  std::vector<std::vector<int>> lanes(kLanes);
+  for (int i : idx) {
+    int best = 0;
+    for (int l = 1; l < kLanes; ++l)
+      if (load[l] < load[best]) best = l;
+    lanes[best].push_back(i);
+    load[best] += weight[i];
+  }
+  return lanes;
+}
+
+}  // namespace
+
+bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vector<uint8_t>* blob,
+                BlobOff* off, std::string* err) {
+  const int n = t.n;
+  if (n > 1023) {
+    *err = "more than 1023 dependent variables";
+    return false;
+  }
+  if (t.n_rxn > 65535 || t.n_part > 65535 || t.n_lu > 65535 || t.n_jac > 65535 ||
+      (int)t.fg_rxn.size() > 65535 || (int)t.jg_part.size() > 65535 ||
+      (int)t.fa_pos.size() > 65535) {
+    *err = "mechanism exceeds the 16-bit table encodings";
+    return false;
+  }
+  // coefficient table
+  std::map<uint64_t, int> cid;
+  std::vector<double> coef;
+  auto coef_id = [&](double v) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    auto it = cid.find(b);
+    if (it != cid.end()) return it->second;
+    int id = (int)coef.size();
+    coef.push_back(v);
+    cid[b] = id;
+    return id;
+  };
+  // reactions
+  std::vector<uint32_t> rx_word(t.n_rxn);
+  std::vector<uint16_t> rx_vptr(t.n_rxn + 1);
+  for (int r = 0; r < t.n_rxn; ++r) {
+    int v0 = t.rx_vptr[r], v1 = t.rx_vptr[r + 1];
+    if (v1 - v0 > 3) {
+      *err = "reaction " + std::to_string(r) + " has more than 3 variable reactants";
+      return false;
+    }
+    uint32_t w = (uint32_t)(v1 - v0) << 30;
+    for (int k = 0; k < v1 - v0; ++k) w |= (uint32_t)t.rx_vdep[v0 + k] << (10 * k);
+    rx_word[r] = w;
+    rx_vptr[r] = (uint16_t)v0;
+  }
+  rx_vptr[t.n_rxn] = (uint16_t)t.n_part;
+  // f gather entries
+  std::vector<uint32_t> fg_ent(t.fg_rxn.size());
+  for (size_t e = 0; e < fg_ent.size(); ++e) {
+    int c = coef_id(t.fg_coef[e]);
+    fg_ent[e] = (uint32_t)t.fg_rxn[e] | ((uint32_t)c << 16) | ((uint32_t)(t.fg_prod[e] ? 1 : 0) << 31);
+  }
+  // balanced f units: species lists longer than the per-lane share are split
+  // into slots that a combine pass adds up
+  const int total = t.fg_ptr[n];
+  const int share = std::max(1, (total + kLanes - 1) / kLanes);
+  struct Unit {
+    int sp, b, e, slot;
+  };
+  std::vector<Unit> units;
+  std::vector<uint16_t> split;
+  int n_slots = 0;
+  for (int i = 0; i < n; ++i) {
+    int b = t.fg_ptr[i], e = t.fg_ptr[i + 1], c = e - b;
+    if (c <= share) {
+      units.push_back({i, b, e, kNoSlot});
+      continue;
+    }
+    int k = (c + share - 1) / share;
+    split.push_back((uint16_t)i);
+    split.push_back((uint16_t)n_slots);
+    split.push_back((uint16_t)k);
+    for (int j = 0; j < k; ++j) {
+      int ub = b + (int)((long)c * j / k), ue = b + (int)((long)c * (j + 1) / k);
+      units.push_back({i, ub, ue, n_slots++});
+    }
+  }
+  std::vector<long> uw(units.size());
+  for (size_t u = 0; u < units.size(); ++u) uw[u] = 2 + (units[u].e - units[u].b);
+  auto ulanes = lpt(uw);
+  std::vector<uint16_t> fg_unit, fg_lane(kLanes + 1, 0);
+  for (int l = 0; l < kLanes; ++l) {
+    fg_lane[l] = (uint16_t)(fg_unit.size() / 4);
+    for (int u : ulanes[l]) {
+      fg_unit.push_back((uint16_t)units[u].sp);
+      fg_unit.push_back((uint16_t)units[u].b);
+      fg_unit.push_back((uint16_t)units[u].e);
+      fg_unit.push_back((uint16_t)units[u].slot);
+    }
+  }
+  fg_lane[kLanes] = (uint16_t)(fg_unit.size() / 4);
+  // J gather
+  std::vector<uint32_t> jg_w0(t.jg_part.size());
+  std::vector<uint16_t> jg_w1(t.jg_part.size());
+  for (size_t g = 0; g < jg_w0.size(); ++g) {
+    int c = coef_id(t.jg_coef[g]);
+    jg_w0[g] = (uint32_t)t.jg_part[g] | ((uint32_t)c << 16);
+    jg_w1[g] = (uint16_t)(t.jg_ind[g] + 1);
+  }
+  if (coef.size() > 32767) {
+    *err = "too many distinct yields for the table encoding";
+    return false;
+  }
+  std::vector<uint16_t> jg_ptr(t.n_jac + 1), jg_lupos(t.n_jac), jg_row(t.n_jac);
+  for (int e = 0; e <= t.n_jac; ++e) jg_ptr[e] = (uint16_t)t.jg_ptr[e];
+  for (int e = 0; e < t.n_jac; ++e) {
+    jg_lupos[e] = (uint16_t)t.jg_lupos[e];
+    jg_row[e] = (uint16_t)t.jg_row[e];
+  }
+  std::vector<long> jw(t.n_jac);
+  for (int e = 0; e < t.n_jac; ++e) jw[e] = 2 + (t.jg_ptr[e + 1] - t.jg_ptr[e]);
+  auto jlanes = lpt(jw);
+  std::vector<uint16_t> jg_lane(kLanes + 1, 0), jg_slots;
+  for (int l = 0; l < kLanes; ++l) {
+    jg_lane[l] = (uint16_t)jg_slots.size();
+    std::vector<int> s = jlanes[l];
+    std::sort(s.begin(), s.end());
+    for (int e : s) jg_slots.push_back((uint16_t)e);
+  }
+  jg_lane[kLanes] = (uint16_t)jg_slots.size();
+  // LU
+  auto u16 = [](const std::vector<int>& v) {
+    std::vector<uint16_t> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = (uint16_t)v[i];
+    return o;
+  };
+  std::vector<uint32_t> fa(t.fa_pos.size());
+  for (size_t i = 0; i < fa.size(); ++i) fa[i] = (uint32_t)t.fa_pos[i] | ((uint32_t)t.fa_piv[i] << 16);
+  struct G {
+    std::vector<uint16_t> lane;
+    std::vector<uint32_t> unit, pair;
+  };
+  auto pack = [&](const Tables::Grouped& g, G* o) {
+    o->lane = u16(g.lane_ptr);
+    o->unit.resize(2 * g.unit_target.size());
+    for (size_t u = 0; u < g.unit_target.size(); ++u) {
+      o->unit[2 * u] = (uint32_t)g.unit_target[u] | ((uint32_t)g.unit_count[u] << 16);
+      o->unit[2 * u + 1] = (uint32_t)g.unit_begin[u] | ((uint32_t)g.unit_recip[u] << 16);
+    }
+    o->pair.resize(g.pair_a.size());
+    for (size_t p = 0; p < g.pair_a.size(); ++p)
+      o->pair[p] = (uint32_t)g.pair_a[p] | ((uint32_t)g.pair_b[p] << 16);
+    return g.unit_target.size() <= 65535 && g.pair_a.size() <= 65535 && g.lane_ptr.size() > 0;
+  };
+  G gfb, gfw, gbw;
+  if (!pack(t.fb, &gfb) || !pack(t.fwd, &gfw) || !pack(t.bwd, &gbw)) {
+    *err = "LU schedule exceeds the 16-bit table encodings";
+    return false;
+  }
+
+  Writer w;
+  // the offsets themselves lead the blob, so device code can rebuild its
+  // table pointers from shared memory alone
+  w.buf.resize(256, 0);
+  static_assert(sizeof(BlobOff) <= 256, "BlobOff must fit the blob header");
+  BlobOff o{};
+  o.n = n;
+  o.n_rxn = t.n_rxn;
+  o.n_part = t.n_part;
+  o.n_jac = t.n_jac;
+  o.n_lu = t.n_lu;
+  o.n_coef = (int)coef.size();
+  o.n_funits = (int)units.size();
+  o.n_fsplit = (int)split.size() / 3;
+  o.n_fscratch = n_slots;
+  o.n_flev = t.n_flev;
+  o.n_blev = t.n_blev;
+  o.rx_word = w.put(rx_word);
+  o.rx_vptr = w.put(rx_vptr);
+  o.coef = w.put(coef);
+  o.fg_ent = w.put(fg_ent);
+  o.fg_unit = w.put(fg_unit);
+  o.fg_lane = w.put(fg_lane);
+  o.fg_split = w.put(split);
+  o.jg_w0 = w.put(jg_w0);
+  o.jg_w1 = w.put(jg_w1);
+  o.jg_ptr = w.put(jg_ptr);
+  o.jg_lupos = w.put(jg_lupos);
+  o.jg_row = w.put(jg_row);
+  o.jg_lane = w.put(jg_lane);
+  o.jg_slots = w.put(jg_slots);
+  o.n_plev = t.n_plev;
+  o.lu_perm = w.put(u16(t.lu_perm));
+  o.lu_diag = w.put(u16(t.lu_diag));
+  o.fd_ptr = w.put(u16(t.fd_ptr));
+  o.fd_piv = w.put(u16(t.fd_piv));
+  o.fa_ptr = w.put(u16(t.fa_ptr));
+  o.fa = w.put(fa);
+  o.fb_lane = w.put(gfb.lane);
+  o.fb_unit = w.put(gfb.unit);
+  o.fb_pair = w.put(gfb.pair);
+  o.fw_lane = w.put(gfw.lane);
+  o.fw_unit = w.put(gfw.unit);
+  o.fw_pair = w.put(gfw.pair);
+  o.bf_ptr = w.put(u16(t.bf_ptr));
+  o.bf_piv = w.put(u16(t.bf_piv));
+  o.bw_lane = w.put(gbw.lane);
+  o.bw_unit = w.put(gbw.unit);
+  o.bw_pair = w.put(gbw.pair);
+  {
+    std::vector<uint32_t> up(t.upd_ptr.begin(), t.upd_ptr.end()), ud(t.upd_src.size());
+    for (size_t p = 0; p < ud.size(); ++p)
+      ud[p] = (uint32_t)t.upd_src[p] | ((uint32_t)t.upd_dst[p] << 16);
+    o.lu_rowptr = w.put(u16(t.lu_rowptr));
+    o.lu_col = w.put(u16(t.lu_col));
+    o.upd_ptr = w.put(up);
+    o.upd = w.put(ud);
+  }
+  o.dep_state = w.put(u16(t.dep_state));
+  o.atol = w.put(atol_dep);
+  w.buf.resize((w.buf.size() + 15) & ~size_t(15), 0);
+  o.bytes = (int)w.buf.size();
+  memcpy(w.buf.data(), &o, sizeof(o));
+  blob->swap(w.buf);
+  *off = o;
+  return true;
+}
+
+}  // namespace campb

@@ -1,0 +1,57 @@
+// Compact mechanism tables for the solve kernel.  The host packs them into one
+// 16-byte aligned blob; every block copies the blob into the front of its
+// shared memory with one bulk (TMA) copy, and all warps of the block read it
+// from there.  Offsets are in bytes from the start of the blob.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace campb {
+
+struct BlobOff {
+  int bytes;
+  // counts
+  int n, n_rxn, n_part, n_jac, n_lu, n_coef, n_funits, n_fsplit, n_fscratch;
+  int n_plev, n_flev, n_blev;
+  // reactions: variable reactants packed (nv<<30 | d2<<20 | d1<<10 | d0), partial base
+  int rx_word, rx_vptr;
+  // coefficient table (double)
+  int coef;
+  // f gather: entries (rxn | coef<<16 | prod<<31), units (species, begin, end,
+  // slot) as 4 x uint16, lane pointers (33 x uint16), split species (species,
+  // first slot, count) as 3 x uint16
+  int fg_ent, fg_unit, fg_lane, fg_split;
+  // J gather: w0 = part | coef<<16, w1 = independent species + 1 (0 = loss
+  // entry); per slot: entry pointer, LU position, row; lane slot lists
+  int jg_w0, jg_w1, jg_ptr, jg_lupos, jg_row, jg_lane, jg_slots;
+  // LU: perm, diag (uint16); factorization by pivot level: reciprocal
+  // pivots (fd_ptr, fd_piv: uint16), scaled L entries (fa_ptr uint16, fa =
+  // pos | pivot<<16), Schur updates grouped by target (fb); forward solve
+  // (fw); backward solve pivots finalised per level (bf_ptr, bf_piv) and
+  // updates (bw).  A grouped phase G has lane pointers (uint16, 33 per
+  // level), units (uint32 target | count<<16, uint32 first pair) and pairs
+  // (uint32 a | b<<16).
+  int lu_perm, lu_diag;
+  int fd_ptr, fd_piv, fa_ptr, fa;
+  int fb_lane, fb_unit, fb_pair;
+  int fw_lane, fw_unit, fw_pair;
+  int bf_ptr, bf_piv;
+  int bw_lane, bw_unit, bw_pair;
+  // row-wise LU for the sequential (one-lane) mode: rowptr, col (uint16),
+  // update pointer per L entry (uint32) and updates (src | dst<<16)
+  int lu_rowptr, lu_col, upd_ptr, upd;
+  // dependent index -> state index (uint16); absolute tolerances (double)
+  int dep_state, atol;
+};
+
+struct Tables;
+
+// Builds the blob; false (with a message) if the mechanism exceeds the
+// encodings (more than 3 variable reactants in a reaction, more than 1023
+// dependent variables, or index spaces beyond 16 bits).
+bool build_blob(const Tables& t, const std::vector<double>& atol_dep,
+                std::vector<uint8_t>* blob, BlobOff* off, std::string* err);
+
+}  // namespace campb

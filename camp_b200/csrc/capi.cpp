@@ -430,6 +430,15 @@ int camp_b200_set_launch(void* solver_data, int warps_per_block, int blocks_per_
   return 0;
 }
 
+int camp_b200_set_lu_mode(void* solver_data, int mode) {
+  if (mode != 0 && mode != 1) {
+    set_error("camp_b200_set_lu_mode: mode must be 0 or 1");
+    return -1;
+  }
+  S(solver_data)->settings.lu_mode = mode;
+  return 0;
+}
+
 int camp_b200_set_cost_ordering(void* solver_data, int enable) {
   S(solver_data)->cost_order = enable != 0;
   return 0;

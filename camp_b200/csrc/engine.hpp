@@ -23,6 +23,7 @@ struct SolveSettings {
   int precision = 0;       // 0 = FP64, 1 = mixed
   int warps_per_block = 0; // 0 = as many as fit
   int blocks_per_sm = 1;
+  int lu_mode = 0;         // 0 = level schedule over the warp, 1 = one lane
 };
 
 class Engine {

@@ -290,6 +290,188 @@ void Model::build_lu() {
   levels(blev, nbl, &t.bl_ptr, &t.bl_rows);
   t.n_flev = nfl;
   t.n_blev = nbl;
+  build_level_schedules(pos, flev, nfl, blev, nbl);
+}
+
+namespace {
+// Longest-processing-time split of weighted units over 32 lanes; returns the
+// units in lane order and fills lane_ptr (33 entries, offsets from base).
+std::vector<int> lane_order(const std::vector<long>& w, int base, std::vector<int>* lane_ptr) {
+  const int lanes = 32;
+  std::vector<int> idx(w.size());
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return w[a] > w[b]; });
+  std::vector<long> load(lanes, 0);
+  std::vector<std::vector<int>> per(lanes);
+  for (int i : idx) {
+    int best = 0;
+    for (int l = 1; l < lanes; ++l)
+      if (load[l] < load[best]) best = l;
+    per[best].push_back(i);
+    load[best] += w[i];
+  }
+  std::vector<int> out;
+  for (int l = 0; l < lanes; ++l) {
+    lane_ptr->push_back(base + (int)out.size());
+    out.insert(out.end(), per[l].begin(), per[l].end());
+  }
+  lane_ptr->push_back(base + (int)out.size());
+  return out;
+}
+
+// Appends one level of a grouped phase: targets with their pair lists.
+void add_grouped_level(Tables::Grouped* g, const std::vector<int>& targets,
+                       const std::vector<std::vector<std::pair<int, int>>>& pairs,
+                       const std::vector<int>* recip = nullptr) {
+  std::vector<long> w(targets.size());
+  for (size_t u = 0; u < targets.size(); ++u) w[u] = 2 + (long)pairs[u].size();
+  int base = (int)g->unit_target.size();
+  std::vector<int> order = lane_order(w, base, &g->lane_ptr);
+  for (int u : order) {
+    g->unit_target.push_back(targets[u]);
+    g->unit_begin.push_back((int)g->pair_a.size());
+    g->unit_count.push_back((int)pairs[u].size());
+    g->unit_recip.push_back(recip ? (*recip)[u] : 0);
+    for (auto& pr : pairs[u]) {
+      g->pair_a.push_back(pr.first);
+      g->pair_b.push_back(pr.second);
+    }
+  }
+  g->n_levels++;
+}
+}  // namespace
+
+// Level schedules of the factorization and the triangular solves.
+void Model::build_level_schedules(const std::vector<std::vector<int>>& pos,
+                                  const std::vector<int>& flev, int nfl,
+                                  const std::vector<int>& blev, int nbl) {
+  Tables& t = tab_;
+  const int n = n_dep_;
+  auto has = [&](int i, int j) { return pos[i][j] >= 0; };
+  // pivot k depends on k' < k when k' updates row k or column k
+  std::vector<int> plev(n, 0);
+  int npl = 0;
+  for (int k = 0; k < n; ++k) {
+    int lv = 0;
+    for (int kk = 0; kk < k; ++kk)
+      if (has(k, kk) || has(kk, k)) lv = std::max(lv, plev[kk] + 1);
+    plev[k] = lv;
+    npl = std::max(npl, lv + 1);
+  }
+  t.n_plev = npl;
+  t.fa_ptr.assign(1, 0);
+  t.fd_ptr.assign(1, 0);
+  t.fd_piv.clear();
+  t.fa_pos.clear();
+  t.fa_piv.clear();
+  t.fb = Tables::Grouped();
+  // Grouped factor phase g (0..npl): g = 0 holds the reciprocals of the
+  // level-0 pivots; g = l+1 holds the Schur updates of level l and the
+  // reciprocals of the level-(l+1) pivots.  A pivot's reciprocal is taken by
+  // the unit that last updates its diagonal in that phase, or by a unit of
+  // its own when the diagonal was already final.  Unit targets are LU
+  // positions; recip holds the pivot + 1 whose reciprocal the unit takes.
+  std::vector<int> last_upd_level(n, -1);  // last level that updates (k,k)
+  for (int k = 0; k < n; ++k)
+    for (int kk = 0; kk < k; ++kk)
+      if (has(k, kk) && has(kk, k)) last_upd_level[k] = std::max(last_upd_level[k], plev[kk]);
+  auto emit_phase = [&](int g) {
+    // Schur updates of level g-1
+    std::vector<int> targets, recip;
+    std::vector<std::vector<std::pair<int, int>>> pairs;
+    std::vector<std::vector<int>> slot(n, std::vector<int>(n, -1));
+    if (g > 0) {
+      const int l = g - 1;
+      for (int k = 0; k < n; ++k) {
+        if (plev[k] != l) continue;
+        for (int i = k + 1; i < n; ++i) {
+          if (!has(i, k)) continue;
+          for (int j = k + 1; j < n; ++j) {
+            if (!has(k, j)) continue;
+            int& sl = slot[i][j];
+            if (sl < 0) {
+              sl = (int)targets.size();
+              targets.push_back(pos[i][j]);
+              recip.push_back(0);
+              pairs.emplace_back();
+            }
+            pairs[sl].push_back({pos[i][k], pos[k][j]});
+          }
+        }
+      }
+    }
+    // reciprocals of the pivots of level g
+    for (int k = 0; k < n; ++k) {
+      if (plev[k] != g) continue;
+      int sl = slot[k][k];
+      if (sl >= 0) {
+        recip[sl] = k + 1;
+      } else {
+        targets.push_back(pos[k][k]);
+        recip.push_back(k + 1);
+        pairs.emplace_back();
+      }
+    }
+    add_grouped_level(&t.fb, targets, pairs, &recip);
+  };
+  for (int g = 0; g <= npl; ++g) {
+    emit_phase(g);
+    if (g == npl) break;
+    for (int k = 0; k < n; ++k)
+      if (plev[k] == g)
+        for (int i = k + 1; i < n; ++i)
+          if (has(i, k)) {
+            t.fa_pos.push_back(pos[i][k]);
+            t.fa_piv.push_back(k);
+          }
+    t.fa_ptr.push_back((int)t.fa_pos.size());
+  }
+  (void)last_upd_level;
+  // forward substitution by forward levels: z_i -= l_ik z_k, k in the level
+  t.fwd = Tables::Grouped();
+  for (int l = 0; l < nfl; ++l) {
+    std::vector<int> targets;
+    std::vector<std::vector<std::pair<int, int>>> pairs;
+    std::vector<int> slot(n, -1);
+    for (int k = 0; k < n; ++k) {
+      if (flev[k] != l) continue;
+      for (int i = k + 1; i < n; ++i) {
+        if (!has(i, k)) continue;
+        if (slot[i] < 0) {
+          slot[i] = (int)targets.size();
+          targets.push_back(i);
+          pairs.emplace_back();
+        }
+        pairs[slot[i]].push_back({pos[i][k], k});
+      }
+    }
+    add_grouped_level(&t.fwd, targets, pairs);
+  }
+  // backward substitution: level l finalises its pivots (z_k *= 1/u_kk),
+  // then z_i -= u_ik z_k for the rows above
+  t.bwd = Tables::Grouped();
+  t.bf_ptr.assign(1, 0);
+  t.bf_piv.clear();
+  for (int l = 0; l < nbl; ++l) {
+    std::vector<int> targets;
+    std::vector<std::vector<std::pair<int, int>>> pairs;
+    std::vector<int> slot(n, -1);
+    for (int k = 0; k < n; ++k) {
+      if (blev[k] != l) continue;
+      t.bf_piv.push_back(k);
+      for (int i = 0; i < k; ++i) {
+        if (!has(i, k)) continue;
+        if (slot[i] < 0) {
+          slot[i] = (int)targets.size();
+          targets.push_back(i);
+          pairs.emplace_back();
+        }
+        pairs[slot[i]].push_back({pos[i][k], k});
+      }
+    }
+    t.bf_ptr.push_back((int)t.bf_piv.size());
+    add_grouped_level(&t.bwd, targets, pairs);
+  }
 }
 
 void Model::build_tables() {

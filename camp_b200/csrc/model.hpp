@@ -61,6 +61,23 @@ struct Tables {
   std::vector<int> fl_ptr, fl_rows;            // forward / factor row levels
   std::vector<int> bl_ptr, bl_rows;            // backward row levels
   std::vector<int> dep_state;                  // dependent index -> state index
+  // Right-looking factorization by pivot levels (pivots whose rows and
+  // columns no other pivot of the level updates).  Per level: pivots whose
+  // reciprocal is taken (fd), L entries scaled by their pivot reciprocal
+  // (fa: position, pivot), and the Schur updates grouped by target (fb).
+  // Forward / backward solves by column levels, grouped by target.
+  // A grouped phase is: units (target, first pair, pair count) and pairs
+  // (two positions); units are spread over 32 lanes per level.
+  struct Grouped {
+    int n_levels = 0;
+    std::vector<int> lane_ptr;  // n_levels * 33 unit indices
+    std::vector<int> unit_target, unit_begin, unit_count, unit_recip;
+    std::vector<int> pair_a, pair_b;
+  };
+  int n_plev = 0;
+  std::vector<int> fd_ptr, fd_piv, fa_ptr, fa_pos, fa_piv;
+  Grouped fb, fwd, bwd;
+  std::vector<int> bf_ptr, bf_piv;  // backward: pivots finalised per level
 };
 
 class Model {
@@ -102,6 +119,9 @@ class Model {
   void update_ids();
   void build_solver_jacobian();
   void build_lu();
+  void build_level_schedules(const std::vector<std::vector<int>>& pos,
+                             const std::vector<int>& flev, int nfl,
+                             const std::vector<int>& blev, int nbl);
   void build_tables();
   int rxn_elem_id(int dep, int ind) const;
 

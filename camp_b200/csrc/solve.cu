@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "blob.hpp"
 #include "engine.hpp"
 
 namespace campb {
@@ -81,11 +82,15 @@ struct DevMech {
 };
 
 struct Layout {  // per-warp shared-memory slice (byte offsets)
-  int zn, ewt, acor, y, ftemp, tempv, rates, keff, lu, z, bytes;
+  int zn, ewt, acor, y, ftemp, tempv, rates, keff, fscr, lu, z, dinv, ctl, bytes;
 };
 
 struct SolveArgs {
   DevMech m;
+  BlobOff off;
+  const void* blob;  // table blob in global memory (copied to shared)
+  int tab_bytes;     // shared-memory bytes reserved for the tables
+  int* err;
   Layout lay;
   double* state;
   const double* env;
@@ -97,6 +102,7 @@ struct SolveArgs {
   void* jscratch;  // per-warp saved Jacobian slots
   double t0, t1, rtol;
   int max_steps, maxncf, maxnef;
+  int lu_mode;
 };
 
 // ---------------------------------------------------------------------------
@@ -118,6 +124,9 @@ __device__ __forceinline__ bool warp_any(bool p) { return __any_sync(FULLMASK, p
 // as is, anything else (only exactly -SMALL reaches here) becomes TINY
 // (src/camp_solver.c:805-833)
 __device__ __forceinline__ double state_of(double y) { return y > -kSmall ? y : kTiny; }
+
+// one out-of-line copy of pow for the step-size controller
+__device__ __noinline__ double dpow(double x, double y) { return pow(x, y); }
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) {
@@ -187,81 +196,253 @@ __device__ void compute_keff(const DevMech& m, const double* cell_state,
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory tables (blob.hpp) as typed pointers
+// ---------------------------------------------------------------------------
+struct Tab {
+  const uint32_t* rx_word;
+  const uint16_t* rx_vptr;
+  const double* coef;
+  const uint32_t* fg_ent;
+  const uint16_t *fg_unit, *fg_lane, *fg_split;
+  const uint32_t* jg_w0;
+  const uint16_t *jg_w1, *jg_ptr, *jg_lupos, *jg_row, *jg_lane, *jg_slots;
+  const uint16_t *lu_perm, *lu_diag, *fd_ptr, *fd_piv, *fa_ptr;
+  const uint32_t* fa;
+  const uint16_t* fb_lane;
+  const uint32_t *fb_unit, *fb_pair;
+  const uint16_t* fw_lane;
+  const uint32_t *fw_unit, *fw_pair;
+  const uint16_t *bf_ptr, *bf_piv, *bw_lane;
+  const uint32_t *bw_unit, *bw_pair;
+  const uint16_t* dep_state;
+  const double* atol;
+  const uint16_t *lu_rowptr, *lu_col;
+  const uint32_t *upd_ptr, *upd;
+  int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev;
+};
+
+__device__ __forceinline__ Tab make_tab(const char* b) {
+  const BlobOff& o = *reinterpret_cast<const BlobOff*>(b);
+  Tab t;
+  t.rx_word = (const uint32_t*)(b + o.rx_word);
+  t.rx_vptr = (const uint16_t*)(b + o.rx_vptr);
+  t.coef = (const double*)(b + o.coef);
+  t.fg_ent = (const uint32_t*)(b + o.fg_ent);
+  t.fg_unit = (const uint16_t*)(b + o.fg_unit);
+  t.fg_lane = (const uint16_t*)(b + o.fg_lane);
+  t.fg_split = (const uint16_t*)(b + o.fg_split);
+  t.jg_w0 = (const uint32_t*)(b + o.jg_w0);
+  t.jg_w1 = (const uint16_t*)(b + o.jg_w1);
+  t.jg_ptr = (const uint16_t*)(b + o.jg_ptr);
+  t.jg_lupos = (const uint16_t*)(b + o.jg_lupos);
+  t.jg_row = (const uint16_t*)(b + o.jg_row);
+  t.jg_lane = (const uint16_t*)(b + o.jg_lane);
+  t.jg_slots = (const uint16_t*)(b + o.jg_slots);
+  t.lu_perm = (const uint16_t*)(b + o.lu_perm);
+  t.lu_diag = (const uint16_t*)(b + o.lu_diag);
+  t.fd_ptr = (const uint16_t*)(b + o.fd_ptr);
+  t.fd_piv = (const uint16_t*)(b + o.fd_piv);
+  t.fa_ptr = (const uint16_t*)(b + o.fa_ptr);
+  t.fa = (const uint32_t*)(b + o.fa);
+  t.fb_lane = (const uint16_t*)(b + o.fb_lane);
+  t.fb_unit = (const uint32_t*)(b + o.fb_unit);
+  t.fb_pair = (const uint32_t*)(b + o.fb_pair);
+  t.fw_lane = (const uint16_t*)(b + o.fw_lane);
+  t.fw_unit = (const uint32_t*)(b + o.fw_unit);
+  t.fw_pair = (const uint32_t*)(b + o.fw_pair);
+  t.bf_ptr = (const uint16_t*)(b + o.bf_ptr);
+  t.bf_piv = (const uint16_t*)(b + o.bf_piv);
+  t.bw_lane = (const uint16_t*)(b + o.bw_lane);
+  t.bw_unit = (const uint32_t*)(b + o.bw_unit);
+  t.bw_pair = (const uint32_t*)(b + o.bw_pair);
+  t.dep_state = (const uint16_t*)(b + o.dep_state);
+  t.atol = (const double*)(b + o.atol);
+  t.lu_rowptr = (const uint16_t*)(b + o.lu_rowptr);
+  t.lu_col = (const uint16_t*)(b + o.lu_col);
+  t.upd_ptr = (const uint32_t*)(b + o.upd_ptr);
+  t.upd = (const uint32_t*)(b + o.upd);
+  t.n = o.n;
+  t.n_rxn = o.n_rxn;
+  t.n_jac = o.n_jac;
+  t.n_lu = o.n_lu;
+  t.n_fsplit = o.n_fsplit;
+  t.n_plev = o.n_plev;
+  t.n_flev = o.n_flev;
+  t.n_blev = o.n_blev;
+  return t;
+}
+
+// Copies the table blob into the front of the block's shared memory with one
+// bulk (TMA) copy completed on an mbarrier.  The wait is bounded; on timeout
+// the block records an error, waits once more (bounded) for its copy and
+// returns false.
+__device__ bool stage_tables(char* dst, const void* src, int bytes, unsigned long long* bar,
+                             int* err_flag) {
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            (unsigned)__cvta_generic_to_shared(dst)),
+        "l"(src), "r"(bytes), "r"(b)
+        : "memory");
+  }
+  auto wait = [&](long limit) {
+    unsigned done = 0;
+    for (long it = 0; it < limit && !done; ++it)
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+          : "=r"(done)
+          : "r"(b)
+          : "memory");
+    return done != 0;
+  };
+  bool ok = wait(1L << 24);
+  if (!ok) {
+    atomicExch(err_flag, 1);
+    wait(1L << 24);
+  }
+  return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// ---------------------------------------------------------------------------
 // Right-hand side f(y) and Jacobian
 // ---------------------------------------------------------------------------
-// Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
-// When rp/rl are given, the production and loss sums are written too.
-__device__ int dev_f(const DevMech& m, const double* y, double h,
-                     const double* keff, double* rates, double* out, int lane,
-                     double* rp = nullptr, double* rl = nullptr) {
-  bool bad = false;
-  for (int i = lane; i < m.n; i += 32) bad |= y[i] < -kSmall;
-  if (warp_any(bad)) return 1;
-  for (int r = lane; r < m.n_rxn; r += 32) {
+__device__ __forceinline__ void rates_of(const Tab& t, const double* y, const double* keff,
+                                         double* rates, int lane) {
+  for (int r = lane; r < t.n_rxn; r += 32) {
+    const uint32_t w = t.rx_word[r];
+    const int nv = w >> 30;
     double rate = keff[r];
-    for (int v = ldg(m.rx_vptr + r); v < ldg(m.rx_vptr + r + 1); ++v)
-      rate *= state_of(y[ldg(m.rx_vdep + v)]);
+    if (nv > 0) rate *= state_of(y[w & 1023u]);
+    if (nv > 1) rate *= state_of(y[(w >> 10) & 1023u]);
+    if (nv > 2) rate *= state_of(y[(w >> 20) & 1023u]);
     rates[r] = rate;
   }
+}
+
+// Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
+// When rp/rl are given, the production and loss sums are written too.
+// Species lists are processed in lane-balanced units; lists split over
+// several units are added up in a combine pass (fscr holds their partials).
+__device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
+                                  const double* keff, double* rates, double* fscr,
+                                  double* out, int lane, double* rp = nullptr,
+                                  double* rl = nullptr) {
+  const Tab t = make_tab(tb);
+  bool bad = false;
+  for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
+  if (warp_any(bad)) return 1;
+  rates_of(t, y, keff, rates, lane);
   __syncwarp();
-  // gather per species: reaction loss and (guarded) product contributions,
-  // split by sign into production and loss (src/time_derivative.c:90-97)
-  for (int i = lane; i < m.n; i += 32) {
-    const double yi = state_of(y[i]);
-    double P = 0.0, L = 0.0;
-    const int e1 = ldg(m.fg_ptr + i + 1);
-    for (int e = ldg(m.fg_ptr + i); e < e1; ++e) {
-      const double rate = rates[ldg(m.fg_rxn + e)];
-      if (rate == 0.0) continue;
-      const double c = ldg(m.fg_coef + e);
+  const int u1 = t.fg_lane[lane + 1];
+  for (int u = t.fg_lane[lane]; u < u1; ++u) {
+    const int sp = t.fg_unit[4 * u], b = t.fg_unit[4 * u + 1], e = t.fg_unit[4 * u + 2];
+    const int slot = t.fg_unit[4 * u + 3];
+    const double yi = state_of(y[sp]);
+    // branch-free accumulation, two entries per iteration: a guarded product
+    // term that may not apply, and a zero rate, contribute 0 to both sums
+    double P0 = 0.0, L0 = 0.0, P1 = 0.0, L1 = 0.0;
+    int k = b;
+    for (; k + 1 < e; k += 2) {
+      const uint32_t w0 = t.fg_ent[k], w1 = t.fg_ent[k + 1];
+      const double r0 = rates[w0 & 0xFFFFu], r1 = rates[w1 & 0xFFFFu];
+      const double c0 = t.coef[(w0 >> 16) & 0x7FFFu], c1 = t.coef[(w1 >> 16) & 0x7FFFu];
       // a negative yield may not drive the product negative within one step
       // (src/rxns/rxn_arrhenius.c:153-160)
-      if (ldg(m.fg_prod + e) && !(-rate * c * h <= yi)) continue;
-      const double v = rate * c;
-      if (v > 0.0)
-        P += v;
-      else
-        L -= v;
+      const double v0 = ((w0 >> 31) && !(-r0 * c0 * h <= yi)) ? 0.0 : r0 * c0;
+      const double v1 = ((w1 >> 31) && !(-r1 * c1 * h <= yi)) ? 0.0 : r1 * c1;
+      P0 += fmax(v0, 0.0);
+      L0 += fmax(-v0, 0.0);
+      P1 += fmax(v1, 0.0);
+      L1 += fmax(-v1, 0.0);
     }
-    out[i] = (P + L != 0.0) ? P - L : 0.0;
-    if (rp) rp[i] = P;
-    if (rl) rl[i] = L;
+    if (k < e) {
+      const uint32_t w0 = t.fg_ent[k];
+      const double r0 = rates[w0 & 0xFFFFu];
+      const double c0 = t.coef[(w0 >> 16) & 0x7FFFu];
+      const double v0 = ((w0 >> 31) && !(-r0 * c0 * h <= yi)) ? 0.0 : r0 * c0;
+      P0 += fmax(v0, 0.0);
+      L0 += fmax(-v0, 0.0);
+    }
+    const double P = P0 + P1, L = L0 + L1;
+    if (slot == 0xFFFF) {
+      out[sp] = (P + L != 0.0) ? P - L : 0.0;
+      if (rp) rp[sp] = P;
+      if (rl) rl[sp] = L;
+    } else {
+      fscr[2 * slot] = P;
+      fscr[2 * slot + 1] = L;
+    }
+  }
+  __syncwarp();
+  for (int s = lane; s < t.n_fsplit; s += 32) {
+    const int sp = t.fg_split[3 * s], first = t.fg_split[3 * s + 1], cnt = t.fg_split[3 * s + 2];
+    double P = 0.0, L = 0.0;
+    for (int j = 0; j < cnt; ++j) {
+      P += fscr[2 * (first + j)];
+      L += fscr[2 * (first + j) + 1];
+    }
+    out[sp] = (P + L != 0.0) ? P - L : 0.0;
+    if (rp) rp[sp] = P;
+    if (rl) rl[sp] = L;
   }
   __syncwarp();
   return 0;
 }
 
-// Solver Jacobian values (CSC order) into Jout; production and loss parts
-// into jp/jl when given (src/rxns/rxn_arrhenius.c:178-212).
+// Solver Jacobian values into Jout (indexed by CSC entry; each lane writes the
+// entries of its balanced slot list); production and loss parts into jp/jl
+// when given (src/rxns/rxn_arrhenius.c:178-212).
 template <typename JT>
-__device__ int dev_jac(const DevMech& m, const double* y, double h,
-                       const double* keff, double* part, JT* Jout, int lane,
-                       double* jp = nullptr, double* jl = nullptr) {
+__device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
+                                    const double* keff, double* part, JT* Jout, int lane,
+                                    double* jp = nullptr, double* jl = nullptr) {
+  const Tab t = make_tab(tb);
   bool bad = false;
-  for (int i = lane; i < m.n; i += 32) bad |= y[i] < -kSmall;
+  for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
   if (warp_any(bad)) return 1;
-  for (int r = lane; r < m.n_rxn; r += 32) {
-    const int v0 = ldg(m.rx_vptr + r), v1 = ldg(m.rx_vptr + r + 1);
-    for (int kv = v0; kv < v1; ++kv) {
-      double p = keff[r];
-      for (int v = v0; v < v1; ++v)
-        if (v != kv) p *= state_of(y[ldg(m.rx_vdep + v)]);
-      part[kv] = p;
+  // d rate / d y_k for every variable reactant occurrence k
+  for (int r = lane; r < t.n_rxn; r += 32) {
+    const uint32_t w = t.rx_word[r];
+    const int nv = w >> 30, base = t.rx_vptr[r];
+    const double k = keff[r];
+    if (nv == 1) {
+      part[base] = k;
+    } else if (nv == 2) {
+      const double y0 = state_of(y[w & 1023u]), y1 = state_of(y[(w >> 10) & 1023u]);
+      part[base] = k * y1;
+      part[base + 1] = k * y0;
+    } else if (nv == 3) {
+      const double y0 = state_of(y[w & 1023u]), y1 = state_of(y[(w >> 10) & 1023u]);
+      const double y2 = state_of(y[(w >> 20) & 1023u]);
+      part[base] = k * y1 * y2;
+      part[base + 1] = k * y0 * y2;
+      part[base + 2] = k * y0 * y1;
     }
   }
   __syncwarp();
-  for (int e = lane; e < m.n_jac; e += 32) {
-    const double yrow = state_of(y[ldg(m.jg_row + e)]);
+  const int s1 = t.jg_lane[lane + 1];
+  for (int s = t.jg_lane[lane]; s < s1; ++s) {
+    const int e = t.jg_slots[s];
+    const double yrow = state_of(y[t.jg_row[e]]);
     double P = 0.0, L = 0.0;
-    const int g1 = ldg(m.jg_ptr + e + 1);
-    for (int g = ldg(m.jg_ptr + e); g < g1; ++g) {
-      const double p = part[ldg(m.jg_part + g)];
-      const int ind = ldg(m.jg_ind + g);
-      if (ind < 0) {
+    const int g1 = t.jg_ptr[e + 1];
+    for (int g = t.jg_ptr[e]; g < g1; ++g) {
+      const uint32_t w0 = t.jg_w0[g];
+      const double p = part[w0 & 0xFFFFu];
+      const int ind1 = t.jg_w1[g];
+      if (ind1 == 0) {
         L += p;
       } else {
-        const double c = ldg(m.jg_coef + g);
-        if (-p * state_of(y[ind]) * c * h <= yrow) P += c * p;
+        const double c = t.coef[w0 >> 16];
+        if (-p * state_of(y[ind1 - 1]) * c * h <= yrow) P += c * p;
       }
     }
     Jout[e] = (JT)(P - L);
@@ -275,32 +456,71 @@ __device__ int dev_jac(const DevMech& m, const double* y, double h,
 // ---------------------------------------------------------------------------
 // LU of M = I - gamma*J on the fixed order, and the triangular solves
 // ---------------------------------------------------------------------------
-template <typename LT>
-__device__ bool dev_form_factor(const DevMech& m, const LT* J, double gamma, LT* LU,
-                                int lane) {
-  for (int q = lane; q < m.n_lu; q += 32) LU[q] = (LT)0;
-  __syncwarp();
-  for (int e = lane; e < m.n_jac; e += 32) LU[ldg(m.jg_lupos + e)] = (LT)(-gamma * (double)J[e]);
-  __syncwarp();
-  for (int i = lane; i < m.n; i += 32) LU[ldg(m.lu_diag + i)] += (LT)1;
-  __syncwarp();
+// One level of a grouped phase: every unit of this lane subtracts its pair
+// products from its target, acc[target] -= sum a[pa] * x[pb].  A unit that
+// carries a pivot (factorization only) then stores the reciprocal of its
+// final value, the pivot, in dinv; the return value flags a zero or
+// non-finite pivot.
+template <typename LT, typename XT>
+__device__ __forceinline__ bool grouped_level(const uint16_t* lane_ptr, const uint32_t* unit,
+                                              const uint32_t* pair, int level, LT* acc,
+                                              const LT* a, const XT* x, LT* dinv, int lane) {
   bool bad = false;
-  for (int lv = 0; lv < m.n_flev; ++lv) {
-    const int r1 = ldg(m.fl_ptr + lv + 1);
-    for (int idx = ldg(m.fl_ptr + lv) + lane; idx < r1; idx += 32) {
-      const int i = ldg(m.fl_rows + idx);
-      const int d = ldg(m.lu_diag + i);
-      for (int q = ldg(m.lu_rowptr + i); q < d; ++q) {
-        const int k = ldg(m.lu_col + q);
-        const LT l = LU[q] / LU[ldg(m.lu_diag + k)];
-        LU[q] = l;
-        const int p1 = ldg(m.upd_ptr + q + 1);
-        for (int p = ldg(m.upd_ptr + q); p < p1; ++p)
-          LU[ldg(m.upd_dst + p)] -= l * LU[ldg(m.upd_src + p)];
-      }
-      const LT piv = LU[d];
-      bad |= (piv == (LT)0) || !isfinite((double)piv);
+  const int u1 = lane_ptr[33 * level + lane + 1];
+  for (int u = lane_ptr[33 * level + lane]; u < u1; ++u) {
+    const uint32_t w = unit[2 * u], w2 = unit[2 * u + 1];
+    const int tgt = w & 0xFFFFu, cnt = w >> 16;
+    const int p0 = w2 & 0xFFFFu, piv = w2 >> 16;
+    LT s0 = acc[tgt], s1 = (LT)0;
+    int p = p0;
+    for (; p + 1 < p0 + cnt; p += 2) {
+      const uint32_t q0 = pair[p], q1 = pair[p + 1];
+      s0 -= a[q0 & 0xFFFFu] * (LT)x[q0 >> 16];
+      s1 -= a[q1 & 0xFFFFu] * (LT)x[q1 >> 16];
     }
+    if (p < p0 + cnt) {
+      const uint32_t q0 = pair[p];
+      s0 -= a[q0 & 0xFFFFu] * (LT)x[q0 >> 16];
+    }
+    const LT s = s0 + s1;
+    acc[tgt] = s;
+    if (piv) {
+      const bool pbad = (s == (LT)0) || !isfinite((double)s);
+      bad |= pbad;
+      dinv[piv - 1] = pbad ? (LT)0 : (LT)1 / s;
+    }
+  }
+  return bad;
+}
+
+// M = I - gamma*J scattered into the LU pattern, then a right-looking
+// factorization level by level: reciprocal pivots of the level, scaled L
+// columns, Schur updates grouped by target.  Returns false on a zero or
+// non-finite pivot.
+template <typename LT>
+__device__ __noinline__ bool dev_form_factor(const char* tb, const LT* J, double gamma,
+                                             LT* LU, LT* dinv, int lane) {
+  const Tab t = make_tab(tb);
+  for (int q = lane; q < t.n_lu; q += 32) LU[q] = (LT)0;
+  __syncwarp();
+  const int s1 = t.jg_lane[lane + 1];
+  for (int s = t.jg_lane[lane]; s < s1; ++s) {
+    const int e = t.jg_slots[s];
+    LU[t.jg_lupos[e]] = (LT)(-gamma * (double)J[e]);
+  }
+  __syncwarp();
+  for (int i = lane; i < t.n; i += 32) LU[t.lu_diag[i]] += (LT)1;
+  __syncwarp();
+  bool bad = grouped_level<LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, 0, LU, LU, LU, dinv, lane);
+  __syncwarp();
+  for (int lv = 0; lv < t.n_plev; ++lv) {
+    const int a1 = t.fa_ptr[lv + 1];
+    for (int i = t.fa_ptr[lv] + lane; i < a1; i += 32) {
+      const uint32_t w = t.fa[i];
+      LU[w & 0xFFFFu] *= dinv[w >> 16];
+    }
+    __syncwarp();
+    bad |= grouped_level<LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, lv + 1, LU, LU, LU, dinv, lane);
     __syncwarp();
   }
   return !warp_any(bad);
@@ -308,33 +528,110 @@ __device__ bool dev_form_factor(const DevMech& m, const LT* J, double gamma, LT*
 
 // b (original variable order, FP64) <- M^{-1} b
 template <typename LT>
-__device__ void dev_lsolve(const DevMech& m, const LT* LU, double* b, LT* z, int lane) {
-  for (int k = lane; k < m.n; k += 32) z[k] = (LT)b[ldg(m.lu_perm + k)];
+__device__ __noinline__ void dev_lsolve(const char* tb, const LT* LU, const LT* dinv,
+                                        double* b, LT* z, int lane) {
+  const Tab t = make_tab(tb);
+  for (int k = lane; k < t.n; k += 32) z[k] = (LT)b[t.lu_perm[k]];
   __syncwarp();
-  for (int lv = 0; lv < m.n_flev; ++lv) {
-    const int r1 = ldg(m.fl_ptr + lv + 1);
-    for (int idx = ldg(m.fl_ptr + lv) + lane; idx < r1; idx += 32) {
-      const int i = ldg(m.fl_rows + idx);
-      LT s = z[i];
-      const int d = ldg(m.lu_diag + i);
-      for (int q = ldg(m.lu_rowptr + i); q < d; ++q) s -= LU[q] * z[ldg(m.lu_col + q)];
-      z[i] = s;
-    }
+  for (int lv = 0; lv < t.n_flev; ++lv) {
+    grouped_level<LT, LT>(t.fw_lane, t.fw_unit, t.fw_pair, lv, z, LU, z, (LT*)nullptr, lane);
     __syncwarp();
   }
-  for (int lv = 0; lv < m.n_blev; ++lv) {
-    const int r1 = ldg(m.bl_ptr + lv + 1);
-    for (int idx = ldg(m.bl_ptr + lv) + lane; idx < r1; idx += 32) {
-      const int i = ldg(m.bl_rows + idx);
-      LT s = z[i];
-      const int d = ldg(m.lu_diag + i);
-      const int q1 = ldg(m.lu_rowptr + i + 1);
-      for (int q = d + 1; q < q1; ++q) s -= LU[q] * z[ldg(m.lu_col + q)];
-      z[i] = s / LU[d];
+  for (int lv = 0; lv < t.n_blev; ++lv) {
+    const int f1 = t.bf_ptr[lv + 1];
+    for (int i = t.bf_ptr[lv] + lane; i < f1; i += 32) {
+      const int k = t.bf_piv[i];
+      z[k] *= dinv[k];
     }
     __syncwarp();
+    grouped_level<LT, LT>(t.bw_lane, t.bw_unit, t.bw_pair, lv, z, LU, z, (LT*)nullptr, lane);
+    __syncwarp();
   }
-  for (int k = lane; k < m.n; k += 32) b[ldg(m.lu_perm + k)] = (double)z[k];
+  for (int k = lane; k < t.n; k += 32) b[t.lu_perm[k]] = (double)z[k];
+  __syncwarp();
+}
+
+// Sequential mode: lane 0 factors row by row (IKJ order, the same update
+// lists the oracle's dense-row elimination follows) and runs both triangular
+// solves; the other lanes wait at the closing __syncwarp.  Fewer phases and
+// higher instruction-level parallelism than the level schedule, at the price
+// of issue slots.
+template <typename LT>
+__device__ __noinline__ bool dev_form_factor_seq(const char* tb, const LT* J, double gamma,
+                                                 LT* LU, LT* dinv, int lane) {
+  const Tab t = make_tab(tb);
+  for (int q = lane; q < t.n_lu; q += 32) LU[q] = (LT)0;
+  __syncwarp();
+  const int s1 = t.jg_lane[lane + 1];
+  for (int s = t.jg_lane[lane]; s < s1; ++s) {
+    const int e = t.jg_slots[s];
+    LU[t.jg_lupos[e]] = (LT)(-gamma * (double)J[e]);
+  }
+  __syncwarp();
+  for (int i = lane; i < t.n; i += 32) LU[t.lu_diag[i]] += (LT)1;
+  __syncwarp();
+  bool bad = false;
+  if (lane == 0) {
+    for (int i = 0; i < t.n; ++i) {
+      const int d = t.lu_diag[i];
+      for (int q = t.lu_rowptr[i]; q < d; ++q) {
+        const LT l = LU[q] * dinv[t.lu_col[q]];
+        LU[q] = l;
+        const uint32_t p1 = t.upd_ptr[q + 1];
+        uint32_t p = t.upd_ptr[q];
+        for (; p + 1 < p1; p += 2) {
+          const uint32_t u0 = t.upd[p], u1 = t.upd[p + 1];
+          const LT a0 = LU[u0 & 0xFFFFu], a1 = LU[u1 & 0xFFFFu];
+          LU[u0 >> 16] -= l * a0;
+          LU[u1 >> 16] -= l * a1;
+        }
+        if (p < p1) {
+          const uint32_t u0 = t.upd[p];
+          LU[u0 >> 16] -= l * LU[u0 & 0xFFFFu];
+        }
+      }
+      const LT piv = LU[d];
+      const bool pbad = (piv == (LT)0) || !isfinite((double)piv);
+      bad |= pbad;
+      dinv[i] = pbad ? (LT)0 : (LT)1 / piv;
+    }
+  }
+  __syncwarp();
+  return !warp_any(bad);
+}
+
+template <typename LT>
+__device__ __noinline__ void dev_lsolve_seq(const char* tb, const LT* LU, const LT* dinv,
+                                            double* b, LT* z, int lane) {
+  const Tab t = make_tab(tb);
+  for (int k = lane; k < t.n; k += 32) z[k] = (LT)b[t.lu_perm[k]];
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < t.n; ++i) {
+      LT s0 = z[i], s1 = (LT)0;
+      const int d = t.lu_diag[i];
+      int q = t.lu_rowptr[i];
+      for (; q + 1 < d; q += 2) {
+        s0 -= LU[q] * z[t.lu_col[q]];
+        s1 -= LU[q + 1] * z[t.lu_col[q + 1]];
+      }
+      if (q < d) s0 -= LU[q] * z[t.lu_col[q]];
+      z[i] = s0 + s1;
+    }
+    for (int i = t.n - 1; i >= 0; --i) {
+      LT s0 = z[i], s1 = (LT)0;
+      const int d = t.lu_diag[i], q1 = t.lu_rowptr[i + 1];
+      int q = d + 1;
+      for (; q + 1 < q1; q += 2) {
+        s0 -= LU[q] * z[t.lu_col[q]];
+        s1 -= LU[q + 1] * z[t.lu_col[q + 1]];
+      }
+      if (q < q1) s0 -= LU[q] * z[t.lu_col[q]];
+      z[i] = (s0 + s1) * dinv[i];
+    }
+  }
+  __syncwarp();
+  for (int k = lane; k < t.n; k += 32) b[t.lu_perm[k]] = (double)z[k];
   __syncwarp();
 }
 
@@ -343,18 +640,20 @@ __device__ void dev_lsolve(const DevMech& m, const LT* LU, double* b, LT* z, int
 // ---------------------------------------------------------------------------
 template <typename LT>
 struct Cell {
-  const DevMech* m;
+  const char* tb;     // shared-memory tables
+  const double* atol;
+  int lu_mode;        // 0 = level schedule over the lanes, 1 = one lane
   int lane, n;
-  double* zn[LMAX];
-  double *ewt, *acor, *y, *ftemp, *tempv, *rates, *keff;
-  LT *LU, *z, *J;
+  double* zb;  // Nordsieck history: column j at zb + j*n
+  double *ewt, *acor, *y, *ftemp, *tempv, *rates, *keff, *fscr;
+  LT *LU, *z, *J, *dinv;
   double rtol;
   int max_steps, maxncf, maxnef;
   double h0;
   // method state
   int q, qprime, qwait, L, jcur;
   double h, hprime, hscale, eta, etamax, hu, next_h, tn;
-  double tau[LMAX + 1], tq[6], l[LMAX];
+  double *tau, *tq, *l;  // per-warp shared scalars (all lanes hold equal values)
   double rl1, gamma, gammap, gamrat, crate, acnrm, saved_tq5;
   double etaqm1, etaq, etaqp1;
   int nst, nfe, nsetups, netf, nni, ncfn, nje, nstlp, nstlj;
@@ -368,14 +667,14 @@ struct Cell {
     return sqrt(warp_sum(s) / n);
   }
   __device__ int f(const double* yy, double* out) {
-    return dev_f(*m, yy, h > 0.0 ? h : h0, keff, rates, out, lane);
+    return dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
   }
   __device__ bool set_ewt(const double* yy) {
     bool bad = false;
     for (int i = lane; i < n; i += 32) {
-      double t = rtol * fabs(yy[i]) + m->atol[i];
-      bad |= !(t > 0.0);
-      ewt[i] = 1.0 / t;
+      double w = rtol * fabs(yy[i]) + atol[i];
+      bad |= !(w > 0.0);
+      ewt[i] = 1.0 / w;
     }
     __syncwarp();
     return !warp_any(bad);
@@ -383,7 +682,7 @@ struct Cell {
   __device__ void rescale() {
     double factor = eta;
     for (int j = 1; j <= q; ++j) {
-      for (int i = lane; i < n; i += 32) zn[j][i] *= factor;
+      for (int i = lane; i < n; i += 32) (zb + (j) * n)[i] *= factor;
       factor *= eta;
     }
     __syncwarp();
@@ -395,14 +694,14 @@ struct Cell {
     tn += h;
     for (int i = lane; i < n; i += 32)
       for (int k = 1; k <= q; ++k)
-        for (int j = q; j >= k; --j) zn[j - 1][i] += zn[j][i];
+        for (int j = q; j >= k; --j) (zb + (j - 1) * n)[i] += (zb + (j) * n)[i];
     __syncwarp();
   }
   __device__ void restore(double saved_t) {
     tn = saved_t;
     for (int i = lane; i < n; i += 32)
       for (int k = 1; k <= q; ++k)
-        for (int j = q; j >= k; --j) zn[j - 1][i] -= zn[j][i];
+        for (int j = q; j >= k; --j) (zb + (j - 1) * n)[i] -= (zb + (j) * n)[i];
     __syncwarp();
   }
   // l and tq of the fixed-leading-coefficient BDF formula
@@ -470,9 +769,9 @@ struct Cell {
     }
     double A1 = (-alpha0 - alpha1) / prod;
     for (int i = lane; i < n; i += 32) {
-      double top = A1 * zn[QMAX][i];
-      zn[q + 1][i] = top;
-      for (int j = 2; j <= q; ++j) zn[j][i] += l[j] * top;
+      double top = A1 * (zb + (QMAX) * n)[i];
+      (zb + (q + 1) * n)[i] = top;
+      for (int j = 2; j <= q; ++j) (zb + (j) * n)[i] += l[j] * top;
     }
     __syncwarp();
   }
@@ -486,7 +785,7 @@ struct Cell {
       for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xi + l[i - 1];
     }
     for (int i = lane; i < n; i += 32)
-      for (int j = 2; j < q; ++j) zn[j][i] -= l[j] * zn[q][i];
+      for (int j = 2; j < q; ++j) (zb + (j) * n)[i] -= l[j] * (zb + (q) * n)[i];
     __syncwarp();
   }
   __device__ void adjust_order(int dq) {
@@ -516,18 +815,23 @@ struct Cell {
       nje++;
       nstlj = nst;
       jcur = 1;
-      if (dev_jac<LT>(*m, ypred, h > 0.0 ? h : h0, keff, rates, J, lane)) return 1;
+      if (dev_jac<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane)) return 1;
     }
-    return dev_form_factor<LT>(*m, J, gamma, LU, lane) ? 0 : 1;
+    const bool ok = lu_mode ? dev_form_factor_seq<LT>(tb, J, gamma, LU, dinv, lane)
+                            : dev_form_factor<LT>(tb, J, gamma, LU, dinv, lane);
+    return ok ? 0 : 1;
   }
   __device__ int newton(bool projected) {
     int mm = 0;
     double del, delp = 0.0;
     for (;;) {
       for (int i = lane; i < n; i += 32)
-        tempv[i] = gamma * ftemp[i] - (rl1 * zn[1][i] + acor[i]);
+        tempv[i] = gamma * ftemp[i] - (rl1 * (zb + (1) * n)[i] + acor[i]);
       __syncwarp();
-      dev_lsolve<LT>(*m, LU, tempv, z, lane);
+      if (lu_mode)
+        dev_lsolve_seq<LT>(tb, LU, dinv, tempv, z, lane);
+      else
+        dev_lsolve<LT>(tb, LU, dinv, tempv, z, lane);
       if (gamrat != 1.0) {
         double s = 2.0 / (1.0 + gamrat);
         for (int i = lane; i < n; i += 32) tempv[i] *= s;
@@ -536,7 +840,7 @@ struct Cell {
       del = wrms(tempv);
       for (int i = lane; i < n; i += 32) {
         acor[i] += tempv[i];
-        y[i] = zn[0][i] + acor[i];
+        y[i] = (zb + (0) * n)[i] + acor[i];
       }
       __syncwarp();
       if (mm > 0) crate = fmax(CRDOWN * crate, del / delp);
@@ -581,7 +885,7 @@ struct Cell {
     double e = 1.0e300;
     for (int i = lane; i < n; i += 32)
       if (y[i] < 0.0) {
-        double qv = zn[0][i] / (zn[0][i] - y[i]);
+        double qv = (zb + (0) * n)[i] / ((zb + (0) * n)[i] - y[i]);
         e = fmin(e, qv);
       }
     e = warp_min(e) * 0.9;
@@ -591,10 +895,10 @@ struct Cell {
   __device__ bool start_guess() {
     bool proj = false;
     for (int i = lane; i < n; i += 32) {
-      double a = zn[0][i] < 0.0 ? -zn[0][i] : 0.0;
+      double a = (zb + (0) * n)[i] < 0.0 ? -(zb + (0) * n)[i] : 0.0;
       proj |= a != 0.0;
       acor[i] = a;
-      y[i] = zn[0][i] + a;
+      y[i] = (zb + (0) * n)[i] + a;
     }
     __syncwarp();
     return warp_any(proj);
@@ -648,7 +952,7 @@ struct Cell {
     if (*nef == maxnef) return ERR_FAILURE;
     etamax = 1.0;
     if (*nef <= MXNEF1) {
-      eta = 1.0 / (pow(BIAS2 * *dsm, 1.0 / L) + ADDON);
+      eta = 1.0 / (dpow(BIAS2 * *dsm, 1.0 / L) + ADDON);
       eta = fmax(ETAMIN, eta);
       if (*nef >= SMALL_NEF) eta = fmin(eta, ETAMXF);
       rescale();
@@ -668,10 +972,10 @@ struct Cell {
     next_h = h;
     hscale = h;
     qwait = LONG_WAIT;
-    int r = f(zn[0], tempv);
+    int r = f((zb + (0) * n), tempv);
     nfe++;
     if (r > 0) return UNREC_RHSFUNC_ERR;
-    for (int i = lane; i < n; i += 32) zn[1][i] = h * tempv[i];
+    for (int i = lane; i < n; i += 32) (zb + (1) * n)[i] = h * tempv[i];
     __syncwarp();
     return TRY_AGAIN;
   }
@@ -684,8 +988,8 @@ struct Cell {
     const bool save = (qwait - 1 == 1) && (q != QMAX);
     for (int i = lane; i < n; i += 32) {
       const double a = acor[i];
-      for (int j = 0; j <= q; ++j) zn[j][i] += l[j] * a;
-      if (save) zn[QMAX][i] = a;
+      for (int j = 0; j <= q; ++j) (zb + (j) * n)[i] += l[j] * a;
+      if (save) (zb + (QMAX) * n)[i] = a;
     }
     __syncwarp();
     qwait--;
@@ -710,7 +1014,7 @@ struct Cell {
       eta = 1.0;
       return;
     }
-    etaq = 1.0 / (pow(BIAS2 * dsm, 1.0 / L) + ADDON);
+    etaq = 1.0 / (dpow(BIAS2 * dsm, 1.0 / L) + ADDON);
     if (qwait != 0) {
       eta = etaq;
       qprime = q;
@@ -720,15 +1024,15 @@ struct Cell {
     qwait = 2;
     etaqm1 = 0.0;
     if (q > 1) {
-      double ddn = wrms(zn[q]) * tq[1];
-      etaqm1 = 1.0 / (pow(BIAS1 * ddn, 1.0 / q) + ADDON);
+      double ddn = wrms((zb + (q) * n)) * tq[1];
+      etaqm1 = 1.0 / (dpow(BIAS1 * ddn, 1.0 / q) + ADDON);
     }
     etaqp1 = 0.0;
     if (q != QMAX && saved_tq5 != 0.0) {
-      double cquot = (tq[5] / saved_tq5) * pow(h / tau[2], (double)L);
-      for (int i = lane; i < n; i += 32) tempv[i] = acor[i] - cquot * zn[QMAX][i];
+      double cquot = (tq[5] / saved_tq5) * dpow(h / tau[2], (double)L);
+      for (int i = lane; i < n; i += 32) tempv[i] = acor[i] - cquot * (zb + (QMAX) * n)[i];
       double dup = wrms(tempv) * tq[3];
-      etaqp1 = 1.0 / (pow(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
+      etaqp1 = 1.0 / (dpow(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
     }
     double etam = fmax(etaqm1, fmax(etaq, etaqp1));
     if (etam < THRESH) {
@@ -743,7 +1047,7 @@ struct Cell {
     } else {
       eta = etaqp1;
       qprime = q + 1;
-      for (int i = lane; i < n; i += 32) zn[QMAX][i] = acor[i];
+      for (int i = lane; i < n; i += 32) (zb + (QMAX) * n)[i] = acor[i];
       __syncwarp();
     }
     set_eta();
@@ -793,26 +1097,26 @@ struct Cell {
     h0 = tout - t0;
     eta = 1.0;
     for (int i = lane; i < n; i += 32) {
-      zn[0][i] = y[i];
-      for (int j = 1; j < LMAX; ++j) zn[j][i] = 0.0;
+      (zb + (0) * n)[i] = y[i];
+      for (int j = 1; j < LMAX; ++j) (zb + (j) * n)[i] = 0.0;
     }
     __syncwarp();
-    if (!set_ewt(zn[0])) return ILL_INPUT;
+    if (!set_ewt((zb + (0) * n))) return ILL_INPUT;
     next_h = 0.0;
-    if (f(zn[0], zn[1])) return REPTD_RHSFUNC_ERR;
+    if (f((zb + (0) * n), (zb + (1) * n))) return REPTD_RHSFUNC_ERR;
     nfe++;
     h = h0;
     if ((tout - t0) * h < 0.0) return ILL_INPUT;
     hscale = h;
     hprime = h;
-    for (int i = lane; i < n; i += 32) zn[1][i] *= h;
+    for (int i = lane; i < n; i += 32) (zb + (1) * n)[i] *= h;
     __syncwarp();
     int nstloc = 0;
     for (;;) {
       next_h = h;
-      if (nst > 0 && !set_ewt(zn[0])) return ILL_INPUT;
+      if (nst > 0 && !set_ewt((zb + (0) * n))) return ILL_INPUT;
       if (max_steps > 0 && nstloc >= max_steps) return TOO_MUCH_WORK;
-      double tolsf = UROUND * wrms(zn[0]);
+      double tolsf = UROUND * wrms((zb + (0) * n));
       if (tolsf > 1.0) return TOO_MUCH_ACC;
       int kflag = step();
       if (kflag != OK) return kflag;
@@ -820,8 +1124,8 @@ struct Cell {
       if ((tn - tout) * h >= 0.0) {
         double s = (tout - tn) / h;
         for (int i = lane; i < n; i += 32) {
-          double v = zn[q][i];
-          for (int j = q - 1; j >= 0; --j) v = zn[j][i] + s * v;
+          double v = (zb + (q) * n)[i];
+          for (int j = q - 1; j >= 0; --j) v = (zb + (j) * n)[i] + s * v;
           y[i] = v;
         }
         __syncwarp();
@@ -836,12 +1140,17 @@ struct Cell {
 // Kernels
 // ---------------------------------------------------------------------------
 template <typename LT>
-__device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, char* base, int gwarp, int lane) {
-  c.m = &a.m;
+__device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char* base,
+                          int gwarp, int lane) {
+  c.tb = tab;
+  c.atol = make_tab(tab).atol;
   c.lane = lane;
-  c.n = a.m.n;
-  double* zn = (double*)(base + a.lay.zn);
-  for (int j = 0; j < LMAX; ++j) c.zn[j] = zn + j * a.m.n;
+  c.n = a.off.n;
+  c.zb = (double*)(base + a.lay.zn);
+  double* ctl = (double*)(base + a.lay.ctl);
+  c.tau = ctl;
+  c.tq = ctl + (LMAX + 2);
+  c.l = ctl + (LMAX + 2) + 8;
   c.ewt = (double*)(base + a.lay.ewt);
   c.acor = (double*)(base + a.lay.acor);
   c.y = (double*)(base + a.lay.y);
@@ -849,25 +1158,31 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, char* base, int gwarp
   c.tempv = (double*)(base + a.lay.tempv);
   c.rates = (double*)(base + a.lay.rates);
   c.keff = (double*)(base + a.lay.keff);
+  c.fscr = (double*)(base + a.lay.fscr);
   c.LU = (LT*)(base + a.lay.lu);
   c.z = (LT*)(base + a.lay.z);
-  c.J = (LT*)a.jscratch + (size_t)gwarp * a.m.n_jac;
+  c.dinv = (LT*)(base + a.lay.dinv);
+  c.J = (LT*)a.jscratch + (size_t)gwarp * a.off.n_jac;
   c.rtol = a.rtol;
   c.max_steps = a.max_steps;
   c.maxncf = a.maxncf;
   c.maxnef = a.maxnef;
+  c.lu_mode = a.lu_mode;
 }
 
 template <typename LT>
 __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
   extern __shared__ __align__(16) char smem[];
+  __shared__ unsigned long long tma_bar;
+  if (!stage_tables(smem, a.blob, a.off.bytes, &tma_bar, a.err)) return;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * (blockDim.x >> 5) + wib;
-  char* base = smem + (size_t)wib * a.lay.bytes;
+  char* base = smem + a.tab_bytes + (size_t)wib * a.lay.bytes;
   Cell<LT> c;
-  bind_cell<LT>(c, a, base, gwarp, lane);
+  bind_cell<LT>(c, a, smem, base, gwarp, lane);
   const DevMech& m = a.m;
+  const uint16_t* dep_state = make_tab(smem).dep_state;
   for (;;) {
     int idx = 0;
     if (lane == 0) idx = atomicAdd(a.counter, 1);
@@ -877,8 +1192,8 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
     double* st = a.state + (size_t)cell * m.n_state;
     // solver_run: dependent values clamped to >= TINY, constants clamped in
     // place (src/camp_solver.c:554-567)
-    for (int i = lane; i < m.n; i += 32) {
-      double v = st[ldg(m.dep_state + i)];
+    for (int i = lane; i < c.n; i += 32) {
+      double v = st[dep_state[i]];
       c.y[i] = v > kTiny ? v : kTiny;
     }
     for (int j = lane; j < m.n_const; j += 32) {
@@ -892,7 +1207,7 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
                  c.keff, lane);
     int flag = c.integrate(a.t0, a.t1);
     if (flag == OK)
-      for (int i = lane; i < m.n; i += 32) st[ldg(m.dep_state + i)] = c.y[i] > 0.0 ? c.y[i] : 0.0;
+      for (int i = lane; i < c.n; i += 32) st[dep_state[i]] = c.y[i] > 0.0 ? c.y[i] : 0.0;
     if (lane == 0) {
       CellStats s;
       s.status = flag;
@@ -913,6 +1228,10 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
 
 struct EvalArgs {
   DevMech m;
+  BlobOff off;
+  const void* blob;
+  int tab_bytes;
+  int* err;
   Layout lay;
   const double* state;
   const double* env;
@@ -925,28 +1244,32 @@ struct EvalArgs {
 
 __global__ void eval_kernel(EvalArgs a) {
   extern __shared__ __align__(16) char smem[];
+  __shared__ unsigned long long tma_bar;
+  if (!stage_tables(smem, a.blob, a.off.bytes, &tma_bar, a.err)) return;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int cell = blockIdx.x * (blockDim.x >> 5) + wib;
   if (cell >= a.n_cells) return;
-  char* base = smem + (size_t)wib * a.lay.bytes;
+  char* base = smem + a.tab_bytes + (size_t)wib * a.lay.bytes;
+  const Tab t = make_tab(smem);
   const DevMech& m = a.m;
   double* y = (double*)(base + a.lay.y);
   double* rates = (double*)(base + a.lay.rates);
   double* keff = (double*)(base + a.lay.keff);
+  double* fscr = (double*)(base + a.lay.fscr);
   const double* st = a.state + (size_t)cell * m.n_state;
-  for (int i = lane; i < m.n; i += 32) y[i] = st[ldg(m.dep_state + i)];
+  for (int i = lane; i < t.n; i += 32) y[i] = st[t.dep_state[i]];
   __syncwarp();
   compute_keff(m, st, a.env[2 * cell], a.env[2 * cell + 1],
                a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, keff, lane);
   if (!a.do_jac) {
     double* out = (double*)(base + a.lay.ftemp);
-    dev_f(m, y, a.h, keff, rates, out, lane, a.rp + (size_t)cell * m.n,
-          a.rl + (size_t)cell * m.n);
-    for (int i = lane; i < m.n; i += 32) a.f[(size_t)cell * m.n + i] = out[i];
+    dev_f(smem, y, a.h, keff, rates, fscr, out, lane, a.rp + (size_t)cell * t.n,
+          a.rl + (size_t)cell * t.n);
+    for (int i = lane; i < t.n; i += 32) a.f[(size_t)cell * t.n + i] = out[i];
   } else {
-    dev_jac<double>(m, y, a.h, keff, rates, a.jv + (size_t)cell * m.n_jac, lane,
-                    a.jp + (size_t)cell * m.n_jac, a.jl + (size_t)cell * m.n_jac);
+    dev_jac<double>(smem, y, a.h, keff, rates, a.jv + (size_t)cell * t.n_jac, lane,
+                    a.jp + (size_t)cell * t.n_jac, a.jl + (size_t)cell * t.n_jac);
   }
 }
 
@@ -964,6 +1287,8 @@ __global__ void eval_kernel(EvalArgs a) {
 
 struct Engine::Impl {
   DevMech m{};
+  BlobOff off{};
+  void* d_blob = nullptr;
   void* d_tables = nullptr;
   int capacity = 0;
   int n_state = 0, n_photo = 0;
@@ -985,6 +1310,7 @@ Engine::Engine() : impl_(new Impl) {}
 Engine::~Engine() {
   Impl* I = impl_;
   cudaFree(I->d_tables);
+  cudaFree(I->d_blob);
   cudaFree(I->d_state);
   cudaFree(I->d_env);
   cudaFree(I->d_photo);
@@ -1083,6 +1409,12 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   CK(cudaMalloc(&I->d_tables, pk.blob.size()));
   CK(cudaMemcpy(I->d_tables, pk.blob.data(), pk.blob.size(), cudaMemcpyHostToDevice));
   for (auto& f : pk.fix) *f.second = (const void*)((char*)I->d_tables + f.first);
+  std::vector<uint8_t> blob;
+  if (!build_blob(t, atol_dep, &blob, &I->off, err)) return false;
+  if (I->d_blob) cudaFree(I->d_blob);
+  I->d_blob = nullptr;
+  CK(cudaMalloc(&I->d_blob, blob.size()));
+  CK(cudaMemcpy(I->d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
   I->capacity = capacity;
   I->n_state = t.n_state;
   I->n_photo = t.n_photo;
@@ -1094,28 +1426,33 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   return true;
 }
 
-static Layout make_layout(const DevMech& m, int lt_size) {
+static Layout make_layout(const BlobOff& o, int lt_size) {
   Layout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
-    size_t o = off;
+    size_t r = off;
     off = (off + bytes + 15) & ~size_t(15);
-    return (int)o;
+    return (int)r;
   };
-  const size_t vec = sizeof(double) * m.n;
+  const size_t vec = sizeof(double) * o.n;
   L.zn = take(vec * LMAX);
   L.ewt = take(vec);
   L.acor = take(vec);
   L.y = take(vec);
   L.ftemp = take(vec);
   L.tempv = take(vec);
-  L.rates = take(sizeof(double) * std::max(m.n_rxn, m.n_part));
-  L.keff = take(sizeof(double) * m.n_rxn);
-  L.lu = take((size_t)lt_size * m.n_lu);
-  L.z = take((size_t)lt_size * m.n);
+  L.rates = take(sizeof(double) * std::max(o.n_rxn, o.n_part));
+  L.keff = take(sizeof(double) * o.n_rxn);
+  L.fscr = take(sizeof(double) * 2 * std::max(1, o.n_fscratch));
+  L.lu = take((size_t)lt_size * o.n_lu);
+  L.z = take((size_t)lt_size * o.n);
+  L.dinv = take((size_t)lt_size * o.n);
+  L.ctl = take(sizeof(double) * 32);
   L.bytes = (int)off;
   return L;
 }
+
+static int tab_bytes_of(const BlobOff& o) { return (o.bytes + 127) & ~127; }
 
 bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_photo,
                           const int* d_order, int n_cells, double t0, double t1,
@@ -1124,8 +1461,9 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   if (n_cells <= 0) return true;
   cudaStream_t st = (cudaStream_t)stream;
   const int lt = s.precision == 1 ? 4 : 8;
-  Layout lay = make_layout(I->m, lt);
-  int max_warps = I->max_smem / lay.bytes;
+  Layout lay = make_layout(I->off, lt);
+  const int tab = tab_bytes_of(I->off);
+  int max_warps = (I->max_smem - tab) / lay.bytes;
   if (max_warps < 1) {
     *err = "mechanism too large for the shared-memory layout (" +
            std::to_string(lay.bytes) + " bytes per cell)";
@@ -1134,7 +1472,7 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   int warps = s.warps_per_block > 0 ? std::min(s.warps_per_block, max_warps) : max_warps;
   warps = std::min(warps, 16);
   int bps = std::max(1, s.blocks_per_sm);
-  while (bps > 1 && (size_t)bps * warps * lay.bytes > (size_t)I->max_smem) --bps;
+  while (bps > 1 && (size_t)bps * (tab + warps * lay.bytes) > (size_t)I->max_smem) --bps;
   int grid = I->sm_count * bps;
   // no more warps than cells
   long total_warps = (long)grid * warps;
@@ -1146,6 +1484,10 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
   SolveArgs a;
   a.m = I->m;
+  a.off = I->off;
+  a.blob = I->d_blob;
+  a.tab_bytes = tab;
+  a.err = I->d_counter + 1;
   a.lay = lay;
   a.state = d_state;
   a.env = d_env;
@@ -1161,7 +1503,8 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   a.max_steps = s.max_steps;
   a.maxncf = s.max_conv_fails;
   a.maxnef = s.max_conv_fails;
-  size_t smem = (size_t)warps * lay.bytes;
+  a.lu_mode = s.lu_mode;
+  size_t smem = (size_t)tab + (size_t)warps * lay.bytes;
   CK(cudaEventRecord(I->ev0, st));
   if (s.precision == 1) {
     CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1250,7 +1593,11 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
     CK(cudaMemcpy(dp, h_photo, sizeof(double) * n_cells * m.n_photo, cudaMemcpyHostToDevice));
   EvalArgs a{};
   a.m = m;
-  a.lay = make_layout(m, 8);
+  a.off = I->off;
+  a.blob = I->d_blob;
+  a.tab_bytes = tab_bytes_of(I->off);
+  a.err = I->d_counter + 1;
+  a.lay = make_layout(I->off, 8);
   a.state = ds;
   a.env = de;
   a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
@@ -1260,8 +1607,8 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
   a.rl = dout + nn;
   a.f = dout + 2 * nn;
   a.do_jac = 0;
-  int warps = std::max(1, std::min(8, I->max_smem / a.lay.bytes));
-  size_t smem = (size_t)warps * a.lay.bytes;
+  int warps = std::max(1, std::min(8, (I->max_smem - a.tab_bytes) / a.lay.bytes));
+  size_t smem = (size_t)a.tab_bytes + (size_t)warps * a.lay.bytes;
   CK(cudaFuncSetAttribute(eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   eval_kernel<<<(n_cells + warps - 1) / warps, warps * 32, smem>>>(a);
   CK(cudaGetLastError());
@@ -1293,7 +1640,11 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
     CK(cudaMemcpy(dp, h_photo, sizeof(double) * n_cells * m.n_photo, cudaMemcpyHostToDevice));
   EvalArgs a{};
   a.m = m;
-  a.lay = make_layout(m, 8);
+  a.off = I->off;
+  a.blob = I->d_blob;
+  a.tab_bytes = tab_bytes_of(I->off);
+  a.err = I->d_counter + 1;
+  a.lay = make_layout(I->off, 8);
   a.state = ds;
   a.env = de;
   a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
@@ -1303,8 +1654,8 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   a.jl = dout + nj;
   a.jv = dout + 2 * nj;
   a.do_jac = 1;
-  int warps = std::max(1, std::min(8, I->max_smem / a.lay.bytes));
-  size_t smem = (size_t)warps * a.lay.bytes;
+  int warps = std::max(1, std::min(8, (I->max_smem - a.tab_bytes) / a.lay.bytes));
+  size_t smem = (size_t)a.tab_bytes + (size_t)warps * a.lay.bytes;
   CK(cudaFuncSetAttribute(eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   eval_kernel<<<(n_cells + warps - 1) / warps, warps * 32, smem>>>(a);
   CK(cudaGetLastError());

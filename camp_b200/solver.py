@@ -82,6 +82,10 @@ class Solver:
     def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 1) -> None:
         self.lib.camp_b200_set_launch(self._h, int(warps_per_block), int(blocks_per_sm))
 
+    def set_lu_mode(self, mode: int) -> None:
+        if self.lib.camp_b200_set_lu_mode(self._h, int(mode)) != 0:
+            raise SolverError(_lib.last_error())
+
     def set_cost_ordering(self, enable: bool = True) -> None:
         self.lib.camp_b200_set_cost_ordering(self._h, 1 if enable else 0)
 

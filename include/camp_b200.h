@@ -148,6 +148,10 @@ int camp_b200_is_ready(void *solver_data);
 int camp_b200_set_precision(void *solver_data, int mode);
 /* cells per block (warps per block); 0 = automatic */
 int camp_b200_set_launch(void *solver_data, int warps_per_block, int blocks_per_sm);
+/* LU strategy of the per-cell linear algebra: 0 = level schedules spread over
+ * the 32 lanes of a cell's warp, 1 = one lane factors and solves row by row
+ * (fewer warp synchronisations).  The autotuner picks per mechanism. */
+int camp_b200_set_lu_mode(void *solver_data, int mode);
 /* Orders the cells of the next run by decreasing internal step count of the
  * previous run (longest-first scheduling of the persistent kernel). */
 int camp_b200_set_cost_ordering(void *solver_data, int enable);

@@ -328,3 +328,70 @@ class RefModel:
         js = np.zeros(max(self.n_jac, 1))
         self.lib.ref_calc_jac(self.h, int(cell), float(time_step), jr, js)
         return js[: self.n_jac], jr[: self.n_rxn_jac]
+
+
+def _ref_cb_setup(lib):
+    vp = C.c_void_p
+    lib.ref_cell_ctx_new.restype = vp
+    lib.ref_cell_ctx_new.argtypes = [vp, C.c_int, C.c_double]
+    lib.ref_cell_ctx_free.argtypes = [vp]
+
+
+def ref_solve(mech, state, env, photo_rates, t0, t1, rtol, abs_tol, max_steps=10000,
+              max_conv_fails=1000, n_threads=None):
+    """Per-cell solve with the reference's own f/J (compiled reference C code)
+    driven by the restated BDF and sparse LU.  Cells are split over threads,
+    each with its own reference model object.  state is updated in place
+    (dependent variables of successful cells, as solver_run does).
+
+    Returns (status, stats) arrays."""
+    import os
+    import threading
+
+    rlib = ref_lib()
+    _ref_cb_setup(rlib)
+    olib = oracle_lib()
+    om = OracleModel(mech)
+    n_cells = state.shape[0]
+    n_threads = n_threads or os.cpu_count() or 1
+    n_threads = max(1, min(n_threads, n_cells))
+    dep = mech.dep_index()
+    atol_dep = np.ascontiguousarray(np.asarray(abs_tol, np.float64)[dep])
+    status = np.zeros(n_cells, np.int32)
+    stats = (OracleStats * n_cells)()
+    f_ptr = C.cast(rlib.ref_cb_rhs, C.c_void_p)
+    j_ptr = C.cast(rlib.ref_cb_jac, C.c_void_p)
+    TINY = 1.0e-60
+
+    def work(c0, c1):
+        nc = c1 - c0
+        rm = RefModel(mech, nc)
+        for c in range(nc):
+            st = state[c0 + c].copy()
+            for i, vt in enumerate(mech.var_type):
+                if vt == 2:
+                    st[i] = max(st[i], TINY)
+            rm.set_cell(c, st, env[c0 + c])
+            for pid in range(photo_rates.shape[1]):
+                rm.set_photo_rate(c, pid + 1, photo_rates[c0 + c, pid])
+            rm.update_env(c)
+        y = np.ascontiguousarray(np.maximum(state[c0:c1][:, dep], TINY))
+        ctxs = (C.c_void_p * nc)(*[rlib.ref_cell_ctx_new(rm.h, c, t1 - t0) for c in range(nc)])
+        st_out = np.zeros(nc, np.int32)
+        sub = (OracleStats * nc)()
+        olib.om_solve_cb(om.h, nc, y, float(t0), float(t1), float(rtol), atol_dep,
+                         int(max_steps), int(max_conv_fails), f_ptr, j_ptr, ctxs, st_out, sub)
+        for c in range(nc):
+            rlib.ref_cell_ctx_free(ctxs[c])
+            status[c0 + c] = st_out[c]
+            stats[c0 + c] = sub[c]
+            if st_out[c] == 0:
+                state[c0 + c, dep] = np.maximum(y[c], 0.0)
+
+    bounds = [int(n_cells * t / n_threads) for t in range(n_threads + 1)]
+    th = [threading.Thread(target=work, args=(bounds[t], bounds[t + 1])) for t in range(n_threads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    return status, stats

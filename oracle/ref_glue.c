@@ -376,3 +376,51 @@ void ref_free(void *h) {
   free(rs->solver_row_ids);
   free(rs);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Callback form for the oracle's restated BDF (oracle/camp_oracle.c): one  */
+/* cell's f and Jac through the reference code, over dependent variables.   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  RefSolver *rs;
+  int cell;
+  double h0;
+} RefCellCtx;
+
+void *ref_cell_ctx_new(void *h, int cell, double h0) {
+  RefCellCtx *c = (RefCellCtx *)xmalloc(sizeof(RefCellCtx));
+  c->rs = (RefSolver *)h;
+  c->cell = cell;
+  c->h0 = h0;
+  return c;
+}
+void ref_cell_ctx_free(void *c) { free(c); }
+
+/* camp_solver_update_model_state (src/camp_solver.c:805-833) for one cell */
+static int ref_load_y(RefCellCtx *c, const double *y) {
+  ModelData *md = &c->rs->sd.model_data;
+  double *st = md->total_state + (size_t)c->cell * md->n_per_cell_state_var;
+  for (int i = 0, d = 0; i < md->n_per_cell_state_var; ++i) {
+    if (md->var_type[i] != CHEM_SPEC_VARIABLE) continue;
+    if (y[d] < -SMALL) return 1;
+    st[i] = y[d] > -SMALL ? y[d] : TINY;
+    ++d;
+  }
+  return 0;
+}
+
+int ref_cb_rhs(void *ctx, double t, const double *y, double h, double *ydot) {
+  (void)t;
+  RefCellCtx *c = (RefCellCtx *)ctx;
+  if (ref_load_y(c, y)) return 1;
+  ref_calc_deriv(c->rs, c->cell, h > 0.0 ? h : c->h0, ydot, NULL, NULL);
+  return 0;
+}
+
+int ref_cb_jac(void *ctx, double t, const double *y, double h, double *jvals) {
+  (void)t;
+  RefCellCtx *c = (RefCellCtx *)ctx;
+  if (ref_load_y(c, y)) return 1;
+  ref_calc_jac(c->rs, c->cell, h > 0.0 ? h : c->h0, NULL, jvals);
+  return 0;
+}
