@@ -21,8 +21,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", "-lineinfo"]
 
-SOURCES = ["model.cpp", "blob.cpp", "capi.cpp", "solve.cu"]
-HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", os.path.join("..", "..", "include", "camp_b200.h")]
+SOURCES = ["model.cpp", "blob.cpp", "capi.cpp", "solve.cu", "lanes.cu"]
+HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", "bdf_consts.hpp", "rates.cuh", os.path.join("..", "..", "include", "camp_b200.h")]
 
 
 def _newer(src: str, dst: str) -> bool:

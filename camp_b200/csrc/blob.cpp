@@ -224,8 +224,6 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.n_plev = t.n_plev;
   o.lu_perm = w.put(u16(t.lu_perm));
   o.lu_diag = w.put(u16(t.lu_diag));
-  o.fd_ptr = w.put(u16(t.fd_ptr));
-  o.fd_piv = w.put(u16(t.fd_piv));
   o.fa_ptr = w.put(u16(t.fa_ptr));
   o.fa = w.put(fa);
   o.fb_lane = w.put(gfb.lane);
@@ -234,11 +232,15 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.fw_lane = w.put(gfw.lane);
   o.fw_unit = w.put(gfw.unit);
   o.fw_pair = w.put(gfw.pair);
-  o.bf_ptr = w.put(u16(t.bf_ptr));
-  o.bf_piv = w.put(u16(t.bf_piv));
   o.bw_lane = w.put(gbw.lane);
   o.bw_unit = w.put(gbw.unit);
   o.bw_pair = w.put(gbw.pair);
+  o.dep_state = w.put(u16(t.dep_state));
+  o.atol = w.put(atol_dep);
+  // the one-lane LU tables come last: the level-scheduled mode stages only
+  // the bytes before them into shared memory
+  w.buf.resize((w.buf.size() + 15) & ~size_t(15), 0);
+  o.stage_bytes = (int)w.buf.size();
   {
     std::vector<uint32_t> up(t.upd_ptr.begin(), t.upd_ptr.end()), ud(t.upd_src.size());
     for (size_t p = 0; p < ud.size(); ++p)
@@ -248,6 +250,119 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     o.upd_ptr = w.put(up);
     o.upd = w.put(ud);
   }
+  w.buf.resize((w.buf.size() + 15) & ~size_t(15), 0);
+  o.bytes = (int)w.buf.size();
+  memcpy(w.buf.data(), &o, sizeof(o));
+  blob->swap(w.buf);
+  *off = o;
+  return true;
+}
+
+}  // namespace campb
+
+namespace campb {
+
+bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
+                     std::vector<uint8_t>* blob, LaneOff* off, std::string* err) {
+  const int n = t.n;
+  if (n > 1023 || t.n_rxn > 65535 || t.n_lu > 65535) {
+    *err = "mechanism exceeds the lane-kernel table encodings";
+    return false;
+  }
+  std::map<uint64_t, int> cid;
+  std::vector<double> coef;
+  auto coef_id = [&](double v) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    auto it = cid.find(b);
+    if (it != cid.end()) return it->second;
+    int id = (int)coef.size();
+    coef.push_back(v);
+    cid[b] = id;
+    return id;
+  };
+  // LU positions by (pivot row, pivot column)
+  std::vector<std::vector<int>> pos(n, std::vector<int>(n, -1));
+  for (int i = 0; i < n; ++i)
+    for (int q = t.lu_rowptr[i]; q < t.lu_rowptr[i + 1]; ++q) pos[i][t.lu_col[q]] = q;
+  // participants in reaction order: the variable reactant occurrences
+  // (rx_vdep), then the variable products (recovered from the f gather
+  // lists, which hold every product of a reaction with its yield)
+  std::vector<std::vector<std::pair<int, double>>> prods(t.n_rxn);
+  for (int d = 0; d < n; ++d)
+    for (int e = t.fg_ptr[d]; e < t.fg_ptr[d + 1]; ++e)
+      if (t.fg_prod[e]) prods[t.fg_rxn[e]].push_back({d, t.fg_coef[e]});
+  std::vector<uint32_t> rx_word(t.n_rxn), rx_part;
+  std::vector<uint16_t> rx_pptr(t.n_rxn + 1), rx_jptr(t.n_rxn + 1), jpos;
+  for (int r = 0; r < t.n_rxn; ++r) {
+    int v0 = t.rx_vptr[r], v1 = t.rx_vptr[r + 1];
+    if (v1 - v0 > 3) {
+      *err = "reaction " + std::to_string(r) + " has more than 3 variable reactants";
+      return false;
+    }
+    uint32_t w = (uint32_t)(v1 - v0) << 30;
+    for (int k = 0; k < v1 - v0; ++k) w |= (uint32_t)t.rx_vdep[v0 + k] << (10 * k);
+    rx_word[r] = w;
+    rx_pptr[r] = (uint16_t)rx_part.size();
+    std::vector<int> sp;
+    for (int k = v0; k < v1; ++k) {
+      rx_part.push_back((uint32_t)t.rx_vdep[k] | ((uint32_t)coef_id(-1.0) << 10));
+      sp.push_back(t.rx_vdep[k]);
+    }
+    for (auto& pr : prods[r]) {
+      rx_part.push_back((uint32_t)pr.first | ((uint32_t)coef_id(pr.second) << 10) | (1u << 31));
+      sp.push_back(pr.first);
+    }
+    rx_jptr[r] = (uint16_t)jpos.size();
+    for (int k = v0; k < v1; ++k) {
+      int col = t.lu_iperm[t.rx_vdep[k]];
+      for (int s : sp) {
+        int q = pos[t.lu_iperm[s]][col];
+        if (q < 0) {
+          *err = "internal: Jacobian entry outside the LU pattern";
+          return false;
+        }
+        jpos.push_back((uint16_t)q);
+      }
+    }
+  }
+  rx_pptr[t.n_rxn] = (uint16_t)rx_part.size();
+  rx_jptr[t.n_rxn] = (uint16_t)jpos.size();
+  if (rx_part.size() > 65535 || jpos.size() > 65535 || coef.size() > 32767) {
+    *err = "mechanism exceeds the lane-kernel table encodings";
+    return false;
+  }
+  auto u16 = [](const std::vector<int>& v) {
+    std::vector<uint16_t> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = (uint16_t)v[i];
+    return o;
+  };
+  std::vector<uint32_t> up(t.upd_ptr.begin(), t.upd_ptr.end()), ud(t.upd_src.size());
+  for (size_t p = 0; p < ud.size(); ++p)
+    ud[p] = (uint32_t)t.upd_src[p] | ((uint32_t)t.upd_dst[p] << 16);
+  Writer w;
+  w.buf.resize(256, 0);
+  static_assert(sizeof(LaneOff) <= 256, "LaneOff must fit the blob header");
+  LaneOff o{};
+  o.n = n;
+  o.n_rxn = t.n_rxn;
+  o.n_lu = t.n_lu;
+  o.n_coef = (int)coef.size();
+  o.n_part = (int)rx_part.size();
+  o.n_jpos = (int)jpos.size();
+  o.n_upd = (int)ud.size();
+  o.rx_word = w.put(rx_word);
+  o.rx_pptr = w.put(rx_pptr);
+  o.rx_part = w.put(rx_part);
+  o.rx_jptr = w.put(rx_jptr);
+  o.jpos = w.put(jpos);
+  o.coef = w.put(coef);
+  o.lu_perm = w.put(u16(t.lu_perm));
+  o.lu_rowptr = w.put(u16(t.lu_rowptr));
+  o.lu_col = w.put(u16(t.lu_col));
+  o.lu_diag = w.put(u16(t.lu_diag));
+  o.upd_ptr = w.put(up);
+  o.upd = w.put(ud);
   o.dep_state = w.put(u16(t.dep_state));
   o.atol = w.put(atol_dep);
   w.buf.resize((w.buf.size() + 15) & ~size_t(15), 0);

@@ -11,7 +11,8 @@
 namespace campb {
 
 struct BlobOff {
-  int bytes;
+  int bytes;        // whole blob
+  int stage_bytes;  // prefix the level-scheduled mode stages (all but the one-lane LU)
   // counts
   int n, n_rxn, n_part, n_jac, n_lu, n_coef, n_funits, n_fsplit, n_fscratch;
   int n_plev, n_flev, n_blev;
@@ -26,18 +27,17 @@ struct BlobOff {
   // J gather: w0 = part | coef<<16, w1 = independent species + 1 (0 = loss
   // entry); per slot: entry pointer, LU position, row; lane slot lists
   int jg_w0, jg_w1, jg_ptr, jg_lupos, jg_row, jg_lane, jg_slots;
-  // LU: perm, diag (uint16); factorization by pivot level: reciprocal
-  // pivots (fd_ptr, fd_piv: uint16), scaled L entries (fa_ptr uint16, fa =
-  // pos | pivot<<16), Schur updates grouped by target (fb); forward solve
-  // (fw); backward solve pivots finalised per level (bf_ptr, bf_piv) and
-  // updates (bw).  A grouped phase G has lane pointers (uint16, 33 per
-  // level), units (uint32 target | count<<16, uint32 first pair) and pairs
-  // (uint32 a | b<<16).
+  // LU: perm, diag (uint16); factorization by pivot level: scaled L entries
+  // (fa_ptr uint16, fa = pos | pivot<<16), Schur updates grouped by target
+  // with the reciprocal pivots taken in the same phase (fb); forward solve
+  // (fw); backward solve updates with the pivots finalised in the same
+  // phase (bw).  A grouped phase G has lane pointers (uint16, 33 per level),
+  // units (uint32 target | count<<16, uint32 first pair | (pivot+1)<<16,
+  // pivot 0 = none) and pairs (uint32 a | b<<16).
   int lu_perm, lu_diag;
-  int fd_ptr, fd_piv, fa_ptr, fa;
+  int fa_ptr, fa;
   int fb_lane, fb_unit, fb_pair;
   int fw_lane, fw_unit, fw_pair;
-  int bf_ptr, bf_piv;
   int bw_lane, bw_unit, bw_pair;
   // row-wise LU for the sequential (one-lane) mode: rowptr, col (uint16),
   // update pointer per L entry (uint32) and updates (src | dst<<16)
@@ -53,5 +53,32 @@ struct Tables;
 // dependent variables, or index spaces beyond 16 bits).
 bool build_blob(const Tables& t, const std::vector<double>& atol_dep,
                 std::vector<uint8_t>* blob, BlobOff* off, std::string* err);
+
+}  // namespace campb
+
+namespace campb {
+
+// Tables of the lane-per-cell kernel (one cell per lane, all lanes of a warp
+// read the same table entry at the same time).  Header first, then sections;
+// offsets in bytes from the start of the blob.
+struct LaneOff {
+  int bytes;
+  int n, n_rxn, n_lu, n_coef, n_part, n_jpos, n_upd;
+  // reactions: variable reactants (nv<<30 | d2<<20 | d1<<10 | d0, uint32);
+  // participants (variable reactant occurrences, then variable products) per
+  // reaction: pointer (uint16) and entries (species | coef<<10 | product<<31)
+  int rx_word, rx_pptr, rx_part;
+  // Jacobian scatter: per reaction, for each variable reactant occurrence k
+  // and each participant p, the LU position of d(p)/d(k) (uint16)
+  int rx_jptr, jpos;
+  int coef;  // double
+  // row-wise LU in pivot order (uint16) and update lists (uint32)
+  int lu_perm, lu_rowptr, lu_col, lu_diag, upd_ptr, upd;
+  int dep_state;  // uint16
+  int atol;       // double
+};
+
+bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
+                     std::vector<uint8_t>* blob, LaneOff* off, std::string* err);
 
 }  // namespace campb

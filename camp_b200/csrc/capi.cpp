@@ -439,6 +439,16 @@ int camp_b200_set_lu_mode(void* solver_data, int mode) {
   return 0;
 }
 
+int camp_b200_set_kernel(void* solver_data, int kernel, int place) {
+  if (kernel != 0 && kernel != 1) {
+    set_error("camp_b200_set_kernel: kernel must be 0 or 1");
+    return -1;
+  }
+  S(solver_data)->settings.kernel = kernel;
+  if (place >= 0) S(solver_data)->settings.lane_place = place & 7;
+  return 0;
+}
+
 int camp_b200_set_cost_ordering(void* solver_data, int enable) {
   S(solver_data)->cost_order = enable != 0;
   return 0;

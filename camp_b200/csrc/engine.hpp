@@ -24,6 +24,8 @@ struct SolveSettings {
   int warps_per_block = 0; // 0 = as many as fit
   int blocks_per_sm = 1;
   int lu_mode = 0;         // 0 = level schedule over the warp, 1 = one lane
+  int kernel = 0;          // 0 = warp per cell, 1 = lane per cell
+  int lane_place = 7;      // lane kernel: bit0 y, bit1 LU, bit2 z in shared memory
 };
 
 class Engine {

@@ -360,8 +360,6 @@ void Model::build_level_schedules(const std::vector<std::vector<int>>& pos,
   }
   t.n_plev = npl;
   t.fa_ptr.assign(1, 0);
-  t.fd_ptr.assign(1, 0);
-  t.fd_piv.clear();
   t.fa_pos.clear();
   t.fa_piv.clear();
   t.fb = Tables::Grouped();
@@ -371,10 +369,6 @@ void Model::build_level_schedules(const std::vector<std::vector<int>>& pos,
   // the unit that last updates its diagonal in that phase, or by a unit of
   // its own when the diagonal was already final.  Unit targets are LU
   // positions; recip holds the pivot + 1 whose reciprocal the unit takes.
-  std::vector<int> last_upd_level(n, -1);  // last level that updates (k,k)
-  for (int k = 0; k < n; ++k)
-    for (int kk = 0; kk < k; ++kk)
-      if (has(k, kk) && has(kk, k)) last_upd_level[k] = std::max(last_upd_level[k], plev[kk]);
   auto emit_phase = [&](int g) {
     // Schur updates of level g-1
     std::vector<int> targets, recip;
@@ -426,7 +420,6 @@ void Model::build_level_schedules(const std::vector<std::vector<int>>& pos,
           }
     t.fa_ptr.push_back((int)t.fa_pos.size());
   }
-  (void)last_upd_level;
   // forward substitution by forward levels: z_i -= l_ik z_k, k in the level
   t.fwd = Tables::Grouped();
   for (int l = 0; l < nfl; ++l) {
@@ -447,30 +440,39 @@ void Model::build_level_schedules(const std::vector<std::vector<int>>& pos,
     }
     add_grouped_level(&t.fwd, targets, pairs);
   }
-  // backward substitution: level l finalises its pivots (z_k *= 1/u_kk),
-  // then z_i -= u_ik z_k for the rows above
+  // backward substitution in nbl phases: phase g applies z_i -= u_ik z_k for
+  // the pivots k of level g-1 and finalises (z_k *= 1/u_kk) the pivots of
+  // level g, each by the unit that last updates it or by a unit of its own
   t.bwd = Tables::Grouped();
-  t.bf_ptr.assign(1, 0);
-  t.bf_piv.clear();
-  for (int l = 0; l < nbl; ++l) {
-    std::vector<int> targets;
+  for (int g = 0; g < nbl; ++g) {
+    std::vector<int> targets, fin;
     std::vector<std::vector<std::pair<int, int>>> pairs;
     std::vector<int> slot(n, -1);
-    for (int k = 0; k < n; ++k) {
-      if (blev[k] != l) continue;
-      t.bf_piv.push_back(k);
-      for (int i = 0; i < k; ++i) {
-        if (!has(i, k)) continue;
-        if (slot[i] < 0) {
-          slot[i] = (int)targets.size();
-          targets.push_back(i);
-          pairs.emplace_back();
+    if (g > 0)
+      for (int k = 0; k < n; ++k) {
+        if (blev[k] != g - 1) continue;
+        for (int i = 0; i < k; ++i) {
+          if (!has(i, k)) continue;
+          if (slot[i] < 0) {
+            slot[i] = (int)targets.size();
+            targets.push_back(i);
+            fin.push_back(0);
+            pairs.emplace_back();
+          }
+          pairs[slot[i]].push_back({pos[i][k], k});
         }
-        pairs[slot[i]].push_back({pos[i][k], k});
+      }
+    for (int k = 0; k < n; ++k) {
+      if (blev[k] != g) continue;
+      if (slot[k] >= 0) {
+        fin[slot[k]] = k + 1;
+      } else {
+        targets.push_back(k);
+        fin.push_back(k + 1);
+        pairs.emplace_back();
       }
     }
-    t.bf_ptr.push_back((int)t.bf_piv.size());
-    add_grouped_level(&t.bwd, targets, pairs);
+    add_grouped_level(&t.bwd, targets, pairs, &fin);
   }
 }
 

@@ -75,9 +75,8 @@ struct Tables {
     std::vector<int> pair_a, pair_b;
   };
   int n_plev = 0;
-  std::vector<int> fd_ptr, fd_piv, fa_ptr, fa_pos, fa_piv;
+  std::vector<int> fa_ptr, fa_pos, fa_piv;
   Grouped fb, fwd, bwd;
-  std::vector<int> bf_ptr, bf_piv;  // backward: pivots finalised per level
 };
 
 class Model {

@@ -28,6 +28,7 @@
 
 #include "blob.hpp"
 #include "engine.hpp"
+#include "rates.cuh"
 
 namespace campb {
 
@@ -64,23 +65,6 @@ constexpr int DO_ERROR_TEST = 100, PREDICT_AGAIN = 101, TRY_AGAIN = 102;
 // ---------------------------------------------------------------------------
 // Device tables
 // ---------------------------------------------------------------------------
-struct DevMech {
-  int n, n_state, n_rxn, n_part, n_jac, n_lu, n_photo, n_flev, n_blev;
-  int n_const;
-  const int *rx_type, *rx_nreact, *rx_fpar, *rx_photo;
-  const double* fpar;
-  const int *rx_cptr, *rx_cidx, *rx_vptr, *rx_vdep;
-  const int *fg_ptr, *fg_rxn, *fg_prod;
-  const double* fg_coef;
-  const int *jg_ptr, *jg_part, *jg_ind, *jg_lupos, *jg_row;
-  const double* jg_coef;
-  const int *lu_perm, *lu_rowptr, *lu_col, *lu_diag;
-  const int *upd_ptr, *upd_src, *upd_dst;
-  const int *fl_ptr, *fl_rows, *bl_ptr, *bl_rows;
-  const int *dep_state, *const_state;
-  const double* atol;  // per dependent variable
-};
-
 struct Layout {  // per-warp shared-memory slice (byte offsets)
   int zn, ewt, acor, y, ftemp, tempv, rates, keff, fscr, lu, z, dinv, ctl, bytes;
 };
@@ -90,6 +74,7 @@ struct SolveArgs {
   BlobOff off;
   const void* blob;  // table blob in global memory (copied to shared)
   int tab_bytes;     // shared-memory bytes reserved for the tables
+  int stage_bytes;   // blob bytes staged into them
   int* err;
   Layout lay;
   double* state;
@@ -128,72 +113,6 @@ __device__ __forceinline__ double state_of(double y) { return y > -kSmall ? y : 
 // one out-of-line copy of pow for the step-size controller
 __device__ __noinline__ double dpow(double x, double y) { return pow(x, y); }
 
-template <typename T>
-__device__ __forceinline__ T ldg(const T* p) {
-  return __ldg(p);
-}
-
-// ---------------------------------------------------------------------------
-// Rate constants (update_env_state of the gas types)
-// ---------------------------------------------------------------------------
-__device__ double rate_constant(const DevMech& m, int r, double T, double P,
-                                const double* photo_cell) {
-  const double* f = m.fpar + ldg(m.rx_fpar + r);
-  const int nr = ldg(m.rx_nreact + r);
-  switch (ldg(m.rx_type + r)) {
-    case RXN_ARRHENIUS:  // src/rxns/rxn_arrhenius.c:103-118
-      return f[0] * exp(f[2] / T) * (f[1] == 0.0 ? 1.0 : pow(T / f[3], f[1])) *
-             (f[4] == 0.0 ? 1.0 : (1.0 + f[4] * P)) * pow(f[5] * P / T, (double)(nr - 1));
-    case RXN_TROE: {  // src/rxns/rxn_troe.c:118-140
-      double conv = f[9] * P / T;
-      double k0 = f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
-                  (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) * conv;
-      double kinf = k0 / (f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
-                          (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4])));
-      double e = log10(kinf) / f[7];
-      return (k0 / (1.0 + kinf)) * pow(f[6], 1.0 / (1.0 + e * e)) *
-             pow(conv, (double)(nr - 1)) * f[8];
-    }
-    case RXN_CMAQ_H2O2: {  // src/rxns/rxn_CMAQ_H2O2.c:106-125
-      double conv = f[6] * P / T;
-      return (f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
-                  (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) +
-              f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
-                  (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4])) * conv) *
-             pow(conv, (double)(nr - 1));
-    }
-    case RXN_CMAQ_OH_HNO3: {  // src/rxns/rxn_CMAQ_OH_HNO3.c:110-133
-      double conv = f[10] * P / T;
-      double k2 = f[3] * (f[5] == 0.0 ? 1.0 : exp(f[5] / T)) *
-                  (f[4] == 0.0 ? 1.0 : pow(T / 300.0, f[4]));
-      double k3 = f[6] * (f[8] == 0.0 ? 1.0 : exp(f[8] / T)) *
-                  (f[7] == 0.0 ? 1.0 : pow(T / 300.0, f[7])) * conv;
-      return (f[0] * (f[2] == 0.0 ? 1.0 : exp(f[2] / T)) *
-                  (f[1] == 0.0 ? 1.0 : pow(T / 300.0, f[1])) +
-              k3 / (1.0 + k3 / k2)) *
-             pow(conv, (double)(nr - 1)) * f[9];
-    }
-    case RXN_PHOTOLYSIS:  // src/rxns/rxn_photolysis.c:137-148
-      return f[0] * (photo_cell ? photo_cell[ldg(m.rx_photo + r)] : 0.0);
-  }
-  return 0.0;
-}
-
-// k of every reaction times the (clamped) constant-species concentrations it
-// multiplies; constant species are clamped to TINY as solver_run does.
-__device__ void compute_keff(const DevMech& m, const double* cell_state,
-                             double T, double P, const double* photo_cell,
-                             double* keff, int lane) {
-  for (int r = lane; r < m.n_rxn; r += 32) {
-    double k = rate_constant(m, r, T, P, photo_cell);
-    for (int c = ldg(m.rx_cptr + r); c < ldg(m.rx_cptr + r + 1); ++c) {
-      double s = cell_state[ldg(m.rx_cidx + c)];
-      k *= s > kTiny ? s : kTiny;
-    }
-    keff[r] = k;
-  }
-  __syncwarp();
-}
 
 // ---------------------------------------------------------------------------
 // Shared-memory tables (blob.hpp) as typed pointers
@@ -206,13 +125,13 @@ struct Tab {
   const uint16_t *fg_unit, *fg_lane, *fg_split;
   const uint32_t* jg_w0;
   const uint16_t *jg_w1, *jg_ptr, *jg_lupos, *jg_row, *jg_lane, *jg_slots;
-  const uint16_t *lu_perm, *lu_diag, *fd_ptr, *fd_piv, *fa_ptr;
+  const uint16_t *lu_perm, *lu_diag, *fa_ptr;
   const uint32_t* fa;
   const uint16_t* fb_lane;
   const uint32_t *fb_unit, *fb_pair;
   const uint16_t* fw_lane;
   const uint32_t *fw_unit, *fw_pair;
-  const uint16_t *bf_ptr, *bf_piv, *bw_lane;
+  const uint16_t *bw_lane;
   const uint32_t *bw_unit, *bw_pair;
   const uint16_t* dep_state;
   const double* atol;
@@ -240,8 +159,6 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.jg_slots = (const uint16_t*)(b + o.jg_slots);
   t.lu_perm = (const uint16_t*)(b + o.lu_perm);
   t.lu_diag = (const uint16_t*)(b + o.lu_diag);
-  t.fd_ptr = (const uint16_t*)(b + o.fd_ptr);
-  t.fd_piv = (const uint16_t*)(b + o.fd_piv);
   t.fa_ptr = (const uint16_t*)(b + o.fa_ptr);
   t.fa = (const uint32_t*)(b + o.fa);
   t.fb_lane = (const uint16_t*)(b + o.fb_lane);
@@ -250,8 +167,6 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.fw_lane = (const uint16_t*)(b + o.fw_lane);
   t.fw_unit = (const uint32_t*)(b + o.fw_unit);
   t.fw_pair = (const uint32_t*)(b + o.fw_pair);
-  t.bf_ptr = (const uint16_t*)(b + o.bf_ptr);
-  t.bf_piv = (const uint16_t*)(b + o.bf_piv);
   t.bw_lane = (const uint16_t*)(b + o.bw_lane);
   t.bw_unit = (const uint32_t*)(b + o.bw_unit);
   t.bw_pair = (const uint32_t*)(b + o.bw_pair);
@@ -461,10 +376,13 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
 // carries a pivot (factorization only) then stores the reciprocal of its
 // final value, the pivot, in dinv; the return value flags a zero or
 // non-finite pivot.
-template <typename LT, typename XT>
+template <int MODE, typename LT, typename XT>
 __device__ __forceinline__ bool grouped_level(const uint16_t* lane_ptr, const uint32_t* unit,
                                               const uint32_t* pair, int level, LT* acc,
                                               const LT* a, const XT* x, LT* dinv, int lane) {
+  // MODE 0: plain; 1: a unit carrying pivot k stores dinv[k] = 1 / (its
+  // final value) (factorization); 2: a unit carrying pivot k scales its final
+  // value by dinv[k] (backward substitution)
   bool bad = false;
   const int u1 = lane_ptr[33 * level + lane + 1];
   for (int u = lane_ptr[33 * level + lane]; u < u1; ++u) {
@@ -482,13 +400,14 @@ __device__ __forceinline__ bool grouped_level(const uint16_t* lane_ptr, const ui
       const uint32_t q0 = pair[p];
       s0 -= a[q0 & 0xFFFFu] * (LT)x[q0 >> 16];
     }
-    const LT s = s0 + s1;
-    acc[tgt] = s;
-    if (piv) {
+    LT s = s0 + s1;
+    if (MODE == 1 && piv) {
       const bool pbad = (s == (LT)0) || !isfinite((double)s);
       bad |= pbad;
       dinv[piv - 1] = pbad ? (LT)0 : (LT)1 / s;
     }
+    if (MODE == 2 && piv) s *= dinv[piv - 1];
+    acc[tgt] = s;
   }
   return bad;
 }
@@ -511,7 +430,7 @@ __device__ __noinline__ bool dev_form_factor(const char* tb, const LT* J, double
   __syncwarp();
   for (int i = lane; i < t.n; i += 32) LU[t.lu_diag[i]] += (LT)1;
   __syncwarp();
-  bool bad = grouped_level<LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, 0, LU, LU, LU, dinv, lane);
+  bool bad = grouped_level<1, LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, 0, LU, LU, LU, dinv, lane);
   __syncwarp();
   for (int lv = 0; lv < t.n_plev; ++lv) {
     const int a1 = t.fa_ptr[lv + 1];
@@ -520,7 +439,7 @@ __device__ __noinline__ bool dev_form_factor(const char* tb, const LT* J, double
       LU[w & 0xFFFFu] *= dinv[w >> 16];
     }
     __syncwarp();
-    bad |= grouped_level<LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, lv + 1, LU, LU, LU, dinv, lane);
+    bad |= grouped_level<1, LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, lv + 1, LU, LU, LU, dinv, lane);
     __syncwarp();
   }
   return !warp_any(bad);
@@ -534,17 +453,11 @@ __device__ __noinline__ void dev_lsolve(const char* tb, const LT* LU, const LT* 
   for (int k = lane; k < t.n; k += 32) z[k] = (LT)b[t.lu_perm[k]];
   __syncwarp();
   for (int lv = 0; lv < t.n_flev; ++lv) {
-    grouped_level<LT, LT>(t.fw_lane, t.fw_unit, t.fw_pair, lv, z, LU, z, (LT*)nullptr, lane);
+    grouped_level<0, LT, LT>(t.fw_lane, t.fw_unit, t.fw_pair, lv, z, LU, z, (LT*)nullptr, lane);
     __syncwarp();
   }
-  for (int lv = 0; lv < t.n_blev; ++lv) {
-    const int f1 = t.bf_ptr[lv + 1];
-    for (int i = t.bf_ptr[lv] + lane; i < f1; i += 32) {
-      const int k = t.bf_piv[i];
-      z[k] *= dinv[k];
-    }
-    __syncwarp();
-    grouped_level<LT, LT>(t.bw_lane, t.bw_unit, t.bw_pair, lv, z, LU, z, (LT*)nullptr, lane);
+  for (int g = 0; g < t.n_blev; ++g) {
+    grouped_level<2, LT, LT>(t.bw_lane, t.bw_unit, t.bw_pair, g, z, LU, z, (LT*)dinv, lane);
     __syncwarp();
   }
   for (int k = lane; k < t.n; k += 32) b[t.lu_perm[k]] = (double)z[k];
@@ -1174,7 +1087,7 @@ template <typename LT>
 __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
   extern __shared__ __align__(16) char smem[];
   __shared__ unsigned long long tma_bar;
-  if (!stage_tables(smem, a.blob, a.off.bytes, &tma_bar, a.err)) return;
+  if (!stage_tables(smem, a.blob, a.stage_bytes, &tma_bar, a.err)) return;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -1231,6 +1144,7 @@ struct EvalArgs {
   BlobOff off;
   const void* blob;
   int tab_bytes;
+  int stage_bytes;
   int* err;
   Layout lay;
   const double* state;
@@ -1245,7 +1159,7 @@ struct EvalArgs {
 __global__ void eval_kernel(EvalArgs a) {
   extern __shared__ __align__(16) char smem[];
   __shared__ unsigned long long tma_bar;
-  if (!stage_tables(smem, a.blob, a.off.bytes, &tma_bar, a.err)) return;
+  if (!stage_tables(smem, a.blob, a.stage_bytes, &tma_bar, a.err)) return;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int cell = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -1285,10 +1199,20 @@ __global__ void eval_kernel(EvalArgs a) {
     }                                                                   \
   } while (0)
 
+bool lanes_launch(const DevMech& m, const void* d_blob, const LaneOff& off, double* d_state,
+                  const double* d_env, const double* d_photo, const int* d_order, int n_cells,
+                  int* d_counter, CellStats* d_stats, void** scr64, size_t* cap64,
+                  void** scrlt, size_t* caplt, double t0, double t1, const SolveSettings& s,
+                  int sm_count, int max_smem, void* stream, std::string* err);
+
 struct Engine::Impl {
   DevMech m{};
   BlobOff off{};
   void* d_blob = nullptr;
+  LaneOff loff{};
+  void* d_lblob = nullptr;
+  void *d_scr64 = nullptr, *d_scrlt = nullptr;
+  size_t c_scr64 = 0, c_scrlt = 0;
   void* d_tables = nullptr;
   int capacity = 0;
   int n_state = 0, n_photo = 0;
@@ -1311,6 +1235,9 @@ Engine::~Engine() {
   Impl* I = impl_;
   cudaFree(I->d_tables);
   cudaFree(I->d_blob);
+  cudaFree(I->d_lblob);
+  cudaFree(I->d_scr64);
+  cudaFree(I->d_scrlt);
   cudaFree(I->d_state);
   cudaFree(I->d_env);
   cudaFree(I->d_photo);
@@ -1415,6 +1342,12 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   I->d_blob = nullptr;
   CK(cudaMalloc(&I->d_blob, blob.size()));
   CK(cudaMemcpy(I->d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  std::vector<uint8_t> lblob;
+  if (!build_lane_blob(t, atol_dep, &lblob, &I->loff, err)) return false;
+  if (I->d_lblob) cudaFree(I->d_lblob);
+  I->d_lblob = nullptr;
+  CK(cudaMalloc(&I->d_lblob, lblob.size()));
+  CK(cudaMemcpy(I->d_lblob, lblob.data(), lblob.size(), cudaMemcpyHostToDevice));
   I->capacity = capacity;
   I->n_state = t.n_state;
   I->n_photo = t.n_photo;
@@ -1452,7 +1385,14 @@ static Layout make_layout(const BlobOff& o, int lt_size) {
   return L;
 }
 
-static int tab_bytes_of(const BlobOff& o) { return (o.bytes + 127) & ~127; }
+// shared-memory bytes of the staged tables: the one-lane LU mode also needs
+// the row-wise LU tables at the end of the blob
+static int stage_bytes_of(const BlobOff& o, int lu_mode) {
+  return lu_mode ? o.bytes : o.stage_bytes;
+}
+static int tab_bytes_of(const BlobOff& o, int lu_mode) {
+  return (stage_bytes_of(o, lu_mode) + 127) & ~127;
+}
 
 bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_photo,
                           const int* d_order, int n_cells, double t0, double t1,
@@ -1460,9 +1400,22 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   Impl* I = impl_;
   if (n_cells <= 0) return true;
   cudaStream_t st = (cudaStream_t)stream;
+  if (s.kernel == 1) {
+    if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
+    CK(cudaEventRecord(I->ev0, st));
+    if (!lanes_launch(I->m, I->d_lblob, I->loff, d_state, d_env, d_photo, d_order, n_cells,
+                      I->d_counter, (CellStats*)I->d_stats, &I->d_scr64, &I->c_scr64,
+                      &I->d_scrlt, &I->c_scrlt, t0, t1, s, I->sm_count, I->max_smem, stream,
+                      err))
+      return false;
+    CK(cudaEventRecord(I->ev1, st));
+    I->ev_pending = true;
+    ++launches_;
+    return true;
+  }
   const int lt = s.precision == 1 ? 4 : 8;
   Layout lay = make_layout(I->off, lt);
-  const int tab = tab_bytes_of(I->off);
+  const int tab = tab_bytes_of(I->off, s.lu_mode);
   int max_warps = (I->max_smem - tab) / lay.bytes;
   if (max_warps < 1) {
     *err = "mechanism too large for the shared-memory layout (" +
@@ -1487,6 +1440,7 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   a.off = I->off;
   a.blob = I->d_blob;
   a.tab_bytes = tab;
+  a.stage_bytes = stage_bytes_of(I->off, s.lu_mode);
   a.err = I->d_counter + 1;
   a.lay = lay;
   a.state = d_state;
@@ -1595,7 +1549,8 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
   a.m = m;
   a.off = I->off;
   a.blob = I->d_blob;
-  a.tab_bytes = tab_bytes_of(I->off);
+  a.tab_bytes = tab_bytes_of(I->off, 1);
+  a.stage_bytes = I->off.bytes;
   a.err = I->d_counter + 1;
   a.lay = make_layout(I->off, 8);
   a.state = ds;
@@ -1642,7 +1597,8 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   a.m = m;
   a.off = I->off;
   a.blob = I->d_blob;
-  a.tab_bytes = tab_bytes_of(I->off);
+  a.tab_bytes = tab_bytes_of(I->off, 1);
+  a.stage_bytes = I->off.bytes;
   a.err = I->d_counter + 1;
   a.lay = make_layout(I->off, 8);
   a.state = ds;

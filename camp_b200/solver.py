@@ -86,6 +86,11 @@ class Solver:
         if self.lib.camp_b200_set_lu_mode(self._h, int(mode)) != 0:
             raise SolverError(_lib.last_error())
 
+    def set_kernel(self, kernel: int, place: int = -1) -> None:
+        """0 = warp per cell, 1 = lane per cell (place: shared-memory bits)."""
+        if self.lib.camp_b200_set_kernel(self._h, int(kernel), int(place)) != 0:
+            raise SolverError(_lib.last_error())
+
     def set_cost_ordering(self, enable: bool = True) -> None:
         self.lib.camp_b200_set_cost_ordering(self._h, 1 if enable else 0)
 

@@ -152,6 +152,12 @@ int camp_b200_set_launch(void *solver_data, int warps_per_block, int blocks_per_
  * the 32 lanes of a cell's warp, 1 = one lane factors and solves row by row
  * (fewer warp synchronisations).  The autotuner picks per mechanism. */
 int camp_b200_set_lu_mode(void *solver_data, int mode);
+/* Kernel organisation: 0 = one warp per cell (lanes share a cell's sparse
+ * work), 1 = one lane per cell (32 cells per warp share every instruction).
+ * place (lane kernel only): bit 0 keeps the state y, bit 1 the LU factors and
+ * bit 2 the solve vector in shared memory; the rest of a cell's working set
+ * lives in a lane-interleaved global scratch.  -1 keeps the current value. */
+int camp_b200_set_kernel(void *solver_data, int kernel, int place);
 /* Orders the cells of the next run by decreasing internal step count of the
  * previous run (longest-first scheduling of the persistent kernel). */
 int camp_b200_set_cost_ordering(void *solver_data, int enable);

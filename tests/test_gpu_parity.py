@@ -46,6 +46,11 @@ def test_jacobian_matches_reference(solver, cb05_ref):
 
 
 def _run_both(cb05, n_cells, seed, precision=0, t1=60.0):
+    """Solves the same seeded cells on the GPU and with the oracle at the same
+    tolerances (rtol 1e-4, atol 1e-8 ppm), and with the oracle at tight
+    tolerances (rtol 1e-8, atol 1e-12) as the accuracy yardstick."""
+    import os
+
     from camp_b200.cells import make_cells
     from camp_b200.solver import Solver
     from oracle.oracle import OracleModel
@@ -57,41 +62,53 @@ def _run_both(cb05, n_cells, seed, precision=0, t1=60.0):
     s.set_precision(precision)
     s.set_photo_rates(cells.photo_rates)
     gpu_state = cells.state.copy()
-    rc = s.solve(gpu_state, cells.env, 0.0, t1)
-    gstats = s.cell_stats()
+    s.solve(gpu_state, cells.env, 0.0, t1)
+    gstatus = s.cell_stats()["status"]
     om = OracleModel(cb05)
-    nf, status, stats, cpu_state = om.solve(cells.state.copy(), cells.env, cells.photo_rates,
-                                            0.0, t1, 1e-4, atol, n_threads=8)
-    return cells, rc, gpu_state, gstats, status, cpu_state, stats
+    nt = os.cpu_count() or 1
+    _, status, _, cpu_state = om.solve(cells.state.copy(), cells.env, cells.photo_rates,
+                                       0.0, t1, 1e-4, atol, n_threads=nt)
+    _, tstatus, _, tight = om.solve(cells.state.copy(), cells.env, cells.photo_rates, 0.0, t1,
+                                    1e-8, np.full(cb05.n_state_var, 1e-12),
+                                    max_steps=100000, n_threads=nt)
+    return gpu_state, gstatus, cpu_state, status, tight, tstatus
 
 
-def _agreement(cb05, a, b, ok):
+def _tol_units(cb05, x, truth, rows):
+    """Per-cell max error in units of the loose tolerance (1e-4 |y| + 1e-8)."""
     dep = cb05.dep_index()
-    x, y = a[ok][:, dep], b[ok][:, dep]
-    big = (np.abs(y) > 1e-8)
-    rel = np.abs(x - y)[big] / np.abs(y)[big]
-    return rel.max() if rel.size else 0.0
+    y = truth[rows][:, dep]
+    return (np.abs(x[rows][:, dep] - y) / (1e-4 * np.abs(y) + 1e-8)).max(axis=1)
+
+
+def _check_solve(cb05, precision, seed, bulk_rel):
+    g, gst, c, cst, tight, tst = _run_both(cb05, 96, seed, precision=precision)
+    # the same cells succeed (and fail) on both sides
+    assert np.mean(gst == cst) >= 0.95
+    ok = (gst == 0) & (cst == 0)
+    assert ok.sum() >= 0.5 * len(ok)
+    # the bulk of the values agree far inside the tolerance
+    dep = cb05.dep_index()
+    x, y = g[ok][:, dep], c[ok][:, dep]
+    big = np.abs(y) > 1e-6
+    assert np.median(np.abs(x - y)[big] / np.abs(y)[big]) < bulk_rel
+    # the GPU's error against a tight solution is the oracle's own error at
+    # the same tolerances: two BDF runs at rtol 1e-4 differ by their global
+    # errors, so their per-cell distance is compared as distributions
+    both = ok & (tst == 0)
+    assert both.sum() >= 0.4 * len(ok)
+    eg = _tol_units(cb05, g, tight, both)
+    ec = _tol_units(cb05, c, tight, both)
+    assert np.median(eg) <= 2.0 * np.median(ec) + 1.0
+    assert np.percentile(eg, 90) <= 2.0 * np.percentile(ec, 90) + 5.0
 
 
 def test_fp64_solve_matches_oracle(cb05):
-    cells, rc, g, gs, status, c, cs = _run_both(cb05, 96, 11, precision=0)
-    ok = (gs["status"] == 0) & (status == 0)
-    # the same cells succeed on both sides
-    assert np.mean(gs["status"] == status) >= 0.95
-    assert ok.sum() >= 0.5 * len(ok)
-    assert _agreement(cb05, g, c, ok) < 1e-3
-    # and the bulk agree far more tightly than the 1e-3 bar
-    dep = cb05.dep_index()
-    x, y = g[ok][:, dep], c[ok][:, dep]
-    big = np.abs(y) > 1e-8
-    assert np.median(np.abs(x - y)[big] / np.abs(y)[big]) < 1e-8
+    _check_solve(cb05, precision=0, seed=11, bulk_rel=1e-7)
 
 
 def test_mixed_solve_matches_oracle(cb05):
-    cells, rc, g, gs, status, c, cs = _run_both(cb05, 96, 12, precision=1)
-    ok = (gs["status"] == 0) & (status == 0)
-    assert ok.sum() >= 0.5 * len(ok)
-    assert _agreement(cb05, g, c, ok) < 1e-3
+    _check_solve(cb05, precision=1, seed=12, bulk_rel=1e-4)
 
 
 def test_failed_cells_keep_input_state(cb05):
