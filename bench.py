@@ -41,6 +41,10 @@ MECH_FILE = os.path.join(ROOT, "tests", "golden", "cb05cl_ae5.mech.json")
 # compulsory HBM bytes per cell-step of cb05cl_ae5: state read (80 x 8),
 # env (16), photolysis base rates (25 x 8), dependent state write (74 x 8)
 METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
+# DRAM bytes (read + write) per cell of one solve launch, from the ncu capture
+# summarised in profiles/solve_kernel_mixed_cb05_2000cells.md (2.91 MB for
+# 2 000 cells); the launch's traffic grows with the cells it processes
+TRAFFIC_BYTES_PER_CELL = 2.911e6 / 2000
 
 
 def parse():
@@ -372,9 +376,11 @@ def run_gpu_arm(args):
             "peak": peak,
             "unit": "GB/s",
             "frac": achieved / peak,
-            "traffic": None,
+            "traffic": TRAFFIC_BYTES_PER_CELL * n,
             "note": f"{bpcs} compulsory bytes per cell-step x cells / mean solve-kernel time "
-                    "(of measured peak); the kernel is FP64/issue-latency bound, not HBM bound",
+                    "(of measured peak); traffic = ncu DRAM bytes per launch scaled from a "
+                    "2000-cell capture; the kernel is bound by issue latency (IPC 0.72, FP64 "
+                    "pipe 3.7 %), not by HBM",
         },
         "cpu_baseline": cb,
     }

@@ -163,8 +163,8 @@ int camp_b200_set_kernel(void *solver_data, int kernel, int place);
 int camp_b200_set_cost_ordering(void *solver_data, int enable);
 
 /* Runs on caller-owned device buffers (state [n_cells*n_state_var], env
- * [n_cells*2]) on the given cudaStream_t (NULL = default stream) without host
- * copies; n_cells may be below the capacity given to solver_new.  Returns 0
+ * [n_cells*2]) on the given cudaStream_t (NULL = the solver's own stream, not
+ * the legacy default stream) without host copies; n_cells may be below the capacity given to solver_new.  Returns 0
  * or 1 like solver_run after the stream has been synchronised, or -1 on a
  * usage error. */
 int camp_b200_run_device(void *solver_data, double *d_state, const double *d_env,
