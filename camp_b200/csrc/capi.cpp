@@ -439,6 +439,15 @@ int camp_b200_set_lu_mode(void* solver_data, int mode) {
   return 0;
 }
 
+int camp_b200_set_layout(void* solver_data, int hist_global) {
+  if (hist_global != 0 && hist_global != 1) {
+    set_error("camp_b200_set_layout: hist_global must be 0 or 1");
+    return -1;
+  }
+  S(solver_data)->settings.hist_global = hist_global;
+  return 0;
+}
+
 int camp_b200_set_kernel(void* solver_data, int kernel, int place) {
   if (kernel != 0 && kernel != 1) {
     set_error("camp_b200_set_kernel: kernel must be 0 or 1");

@@ -26,6 +26,8 @@ struct SolveSettings {
   int lu_mode = 0;         // 0 = level schedule over the warp, 1 = one lane
   int kernel = 0;          // 0 = warp per cell, 1 = lane per cell
   int lane_place = 7;      // lane kernel: bit0 y, bit1 LU, bit2 z in shared memory
+  int hist_global = 0;     // warp kernel: Nordsieck history + rate constants in
+                           // global memory (1) or shared memory (0)
 };
 
 class Engine {

@@ -65,7 +65,7 @@ constexpr int DO_ERROR_TEST = 100, PREDICT_AGAIN = 101, TRY_AGAIN = 102;
 // ---------------------------------------------------------------------------
 // Device tables
 // ---------------------------------------------------------------------------
-struct Layout {  // per-warp shared-memory slice (byte offsets)
+struct Layout {  // per-warp shared-memory slice (byte offsets; -1 = not in it)
   int zn, ewt, acor, y, ftemp, tempv, rates, keff, fscr, lu, z, dinv, ctl, bytes;
 };
 
@@ -85,6 +85,8 @@ struct SolveArgs {
   int* counter;
   CellStats* stats;
   void* jscratch;  // per-warp saved Jacobian slots
+  double* hist;    // per-warp Nordsieck history zn[LMAX][n] + rate constants
+  int hist_stride; // doubles per warp in hist
   double t0, t1, rtol;
   int max_steps, maxncf, maxnef;
   int lu_mode;
@@ -110,8 +112,15 @@ __device__ __forceinline__ bool warp_any(bool p) { return __any_sync(FULLMASK, p
 // (src/camp_solver.c:805-833)
 __device__ __forceinline__ double state_of(double y) { return y > -kSmall ? y : kTiny; }
 
-// one out-of-line copy of pow for the step-size controller
+// Device loops carry `#pragma unroll 1` unless unrolling is wanted: the
+// solve kernel is bound by instruction fetch (a warp per cell, each at its own
+// point of the BDF control flow), so compact code beats unrolled code here.
+
+// one out-of-line copy each of pow, division and square root for the BDF
+// control code (IEEE results, identical to the inline forms)
 __device__ __noinline__ double dpow(double x, double y) { return pow(x, y); }
+__device__ __noinline__ double ddiv(double a, double b) { return a / b; }
+__device__ __noinline__ double dsqrt(double a) { return sqrt(a); }
 
 
 // ---------------------------------------------------------------------------
@@ -210,6 +219,7 @@ __device__ bool stage_tables(char* dst, const void* src, int bytes, unsigned lon
   }
   auto wait = [&](long limit) {
     unsigned done = 0;
+    #pragma unroll 1
     for (long it = 0; it < limit && !done; ++it)
       asm volatile(
           "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -231,6 +241,7 @@ __device__ bool stage_tables(char* dst, const void* src, int bytes, unsigned lon
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void rates_of(const Tab& t, const double* y, const double* keff,
                                          double* rates, int lane) {
+  #pragma unroll 1
   for (int r = lane; r < t.n_rxn; r += 32) {
     const uint32_t w = t.rx_word[r];
     const int nv = w >> 30;
@@ -252,11 +263,13 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
                                   double* rl = nullptr) {
   const Tab t = make_tab(tb);
   bool bad = false;
+  #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
   if (warp_any(bad)) return 1;
   rates_of(t, y, keff, rates, lane);
   __syncwarp();
   const int u1 = t.fg_lane[lane + 1];
+  #pragma unroll 1
   for (int u = t.fg_lane[lane]; u < u1; ++u) {
     const int sp = t.fg_unit[4 * u], b = t.fg_unit[4 * u + 1], e = t.fg_unit[4 * u + 2];
     const int slot = t.fg_unit[4 * u + 3];
@@ -265,6 +278,7 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
     // term that may not apply, and a zero rate, contribute 0 to both sums
     double P0 = 0.0, L0 = 0.0, P1 = 0.0, L1 = 0.0;
     int k = b;
+    #pragma unroll 1
     for (; k + 1 < e; k += 2) {
       const uint32_t w0 = t.fg_ent[k], w1 = t.fg_ent[k + 1];
       const double r0 = rates[w0 & 0xFFFFu], r1 = rates[w1 & 0xFFFFu];
@@ -297,9 +311,11 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
     }
   }
   __syncwarp();
+  #pragma unroll 1
   for (int s = lane; s < t.n_fsplit; s += 32) {
     const int sp = t.fg_split[3 * s], first = t.fg_split[3 * s + 1], cnt = t.fg_split[3 * s + 2];
     double P = 0.0, L = 0.0;
+    #pragma unroll 1
     for (int j = 0; j < cnt; ++j) {
       P += fscr[2 * (first + j)];
       L += fscr[2 * (first + j) + 1];
@@ -321,9 +337,11 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
                                     double* jp = nullptr, double* jl = nullptr) {
   const Tab t = make_tab(tb);
   bool bad = false;
+  #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
   if (warp_any(bad)) return 1;
   // d rate / d y_k for every variable reactant occurrence k
+  #pragma unroll 1
   for (int r = lane; r < t.n_rxn; r += 32) {
     const uint32_t w = t.rx_word[r];
     const int nv = w >> 30, base = t.rx_vptr[r];
@@ -344,11 +362,13 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
   }
   __syncwarp();
   const int s1 = t.jg_lane[lane + 1];
+  #pragma unroll 1
   for (int s = t.jg_lane[lane]; s < s1; ++s) {
     const int e = t.jg_slots[s];
     const double yrow = state_of(y[t.jg_row[e]]);
     double P = 0.0, L = 0.0;
     const int g1 = t.jg_ptr[e + 1];
+    #pragma unroll 1
     for (int g = t.jg_ptr[e]; g < g1; ++g) {
       const uint32_t w0 = t.jg_w0[g];
       const double p = part[w0 & 0xFFFFu];
@@ -385,12 +405,14 @@ __device__ __forceinline__ bool grouped_level(const uint16_t* lane_ptr, const ui
   // value by dinv[k] (backward substitution)
   bool bad = false;
   const int u1 = lane_ptr[33 * level + lane + 1];
+  #pragma unroll 1
   for (int u = lane_ptr[33 * level + lane]; u < u1; ++u) {
     const uint32_t w = unit[2 * u], w2 = unit[2 * u + 1];
     const int tgt = w & 0xFFFFu, cnt = w >> 16;
     const int p0 = w2 & 0xFFFFu, piv = w2 >> 16;
     LT s0 = acc[tgt], s1 = (LT)0;
     int p = p0;
+    #pragma unroll 1
     for (; p + 1 < p0 + cnt; p += 2) {
       const uint32_t q0 = pair[p], q1 = pair[p + 1];
       s0 -= a[q0 & 0xFFFFu] * (LT)x[q0 >> 16];
@@ -420,20 +442,25 @@ template <typename LT>
 __device__ __noinline__ bool dev_form_factor(const char* tb, const LT* J, double gamma,
                                              LT* LU, LT* dinv, int lane) {
   const Tab t = make_tab(tb);
+  #pragma unroll 1
   for (int q = lane; q < t.n_lu; q += 32) LU[q] = (LT)0;
   __syncwarp();
   const int s1 = t.jg_lane[lane + 1];
+  #pragma unroll 1
   for (int s = t.jg_lane[lane]; s < s1; ++s) {
     const int e = t.jg_slots[s];
     LU[t.jg_lupos[e]] = (LT)(-gamma * (double)J[e]);
   }
   __syncwarp();
+  #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) LU[t.lu_diag[i]] += (LT)1;
   __syncwarp();
   bool bad = grouped_level<1, LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, 0, LU, LU, LU, dinv, lane);
   __syncwarp();
+  #pragma unroll 1
   for (int lv = 0; lv < t.n_plev; ++lv) {
     const int a1 = t.fa_ptr[lv + 1];
+    #pragma unroll 1
     for (int i = t.fa_ptr[lv] + lane; i < a1; i += 32) {
       const uint32_t w = t.fa[i];
       LU[w & 0xFFFFu] *= dinv[w >> 16];
@@ -450,16 +477,20 @@ template <typename LT>
 __device__ __noinline__ void dev_lsolve(const char* tb, const LT* LU, const LT* dinv,
                                         double* b, LT* z, int lane) {
   const Tab t = make_tab(tb);
+  #pragma unroll 1
   for (int k = lane; k < t.n; k += 32) z[k] = (LT)b[t.lu_perm[k]];
   __syncwarp();
+  #pragma unroll 1
   for (int lv = 0; lv < t.n_flev; ++lv) {
     grouped_level<0, LT, LT>(t.fw_lane, t.fw_unit, t.fw_pair, lv, z, LU, z, (LT*)nullptr, lane);
     __syncwarp();
   }
+  #pragma unroll 1
   for (int g = 0; g < t.n_blev; ++g) {
     grouped_level<2, LT, LT>(t.bw_lane, t.bw_unit, t.bw_pair, g, z, LU, z, (LT*)dinv, lane);
     __syncwarp();
   }
+  #pragma unroll 1
   for (int k = lane; k < t.n; k += 32) b[t.lu_perm[k]] = (double)z[k];
   __syncwarp();
 }
@@ -473,25 +504,31 @@ template <typename LT>
 __device__ __noinline__ bool dev_form_factor_seq(const char* tb, const LT* J, double gamma,
                                                  LT* LU, LT* dinv, int lane) {
   const Tab t = make_tab(tb);
+  #pragma unroll 1
   for (int q = lane; q < t.n_lu; q += 32) LU[q] = (LT)0;
   __syncwarp();
   const int s1 = t.jg_lane[lane + 1];
+  #pragma unroll 1
   for (int s = t.jg_lane[lane]; s < s1; ++s) {
     const int e = t.jg_slots[s];
     LU[t.jg_lupos[e]] = (LT)(-gamma * (double)J[e]);
   }
   __syncwarp();
+  #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) LU[t.lu_diag[i]] += (LT)1;
   __syncwarp();
   bool bad = false;
   if (lane == 0) {
+    #pragma unroll 1
     for (int i = 0; i < t.n; ++i) {
       const int d = t.lu_diag[i];
+      #pragma unroll 1
       for (int q = t.lu_rowptr[i]; q < d; ++q) {
         const LT l = LU[q] * dinv[t.lu_col[q]];
         LU[q] = l;
         const uint32_t p1 = t.upd_ptr[q + 1];
         uint32_t p = t.upd_ptr[q];
+        #pragma unroll 1
         for (; p + 1 < p1; p += 2) {
           const uint32_t u0 = t.upd[p], u1 = t.upd[p + 1];
           const LT a0 = LU[u0 & 0xFFFFu], a1 = LU[u1 & 0xFFFFu];
@@ -517,13 +554,16 @@ template <typename LT>
 __device__ __noinline__ void dev_lsolve_seq(const char* tb, const LT* LU, const LT* dinv,
                                             double* b, LT* z, int lane) {
   const Tab t = make_tab(tb);
+  #pragma unroll 1
   for (int k = lane; k < t.n; k += 32) z[k] = (LT)b[t.lu_perm[k]];
   __syncwarp();
   if (lane == 0) {
+    #pragma unroll 1
     for (int i = 0; i < t.n; ++i) {
       LT s0 = z[i], s1 = (LT)0;
       const int d = t.lu_diag[i];
       int q = t.lu_rowptr[i];
+      #pragma unroll 1
       for (; q + 1 < d; q += 2) {
         s0 -= LU[q] * z[t.lu_col[q]];
         s1 -= LU[q + 1] * z[t.lu_col[q + 1]];
@@ -531,10 +571,12 @@ __device__ __noinline__ void dev_lsolve_seq(const char* tb, const LT* LU, const 
       if (q < d) s0 -= LU[q] * z[t.lu_col[q]];
       z[i] = s0 + s1;
     }
+    #pragma unroll 1
     for (int i = t.n - 1; i >= 0; --i) {
       LT s0 = z[i], s1 = (LT)0;
       const int d = t.lu_diag[i], q1 = t.lu_rowptr[i + 1];
       int q = d + 1;
+      #pragma unroll 1
       for (; q + 1 < q1; q += 2) {
         s0 -= LU[q] * z[t.lu_col[q]];
         s1 -= LU[q + 1] * z[t.lu_col[q + 1]];
@@ -544,6 +586,7 @@ __device__ __noinline__ void dev_lsolve_seq(const char* tb, const LT* LU, const 
     }
   }
   __syncwarp();
+  #pragma unroll 1
   for (int k = lane; k < t.n; k += 32) b[t.lu_perm[k]] = (double)z[k];
   __syncwarp();
 }
@@ -573,28 +616,32 @@ struct Cell {
 
   __device__ double wrms(const double* v) const {
     double s = 0.0;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
       double t = v[i] * ewt[i];
       s += t * t;
     }
-    return sqrt(warp_sum(s) / n);
+    return dsqrt(ddiv(warp_sum(s), (double)n));
   }
   __device__ int f(const double* yy, double* out) {
     return dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
   }
   __device__ bool set_ewt(const double* yy) {
     bool bad = false;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
       double w = rtol * fabs(yy[i]) + atol[i];
       bad |= !(w > 0.0);
-      ewt[i] = 1.0 / w;
+      ewt[i] = ddiv(1.0, w);
     }
     __syncwarp();
     return !warp_any(bad);
   }
   __device__ void rescale() {
     double factor = eta;
+    #pragma unroll 1
     for (int j = 1; j <= q; ++j) {
+      #pragma unroll 1
       for (int i = lane; i < n; i += 32) (zb + (j) * n)[i] *= factor;
       factor *= eta;
     }
@@ -603,101 +650,129 @@ struct Cell {
     next_h = h;
     hscale = h;
   }
+  // zn <- zn * Pascal(q) (sign +1) or its inverse (sign -1), one element's
+  // q+1 history values at a time in registers: for k = 1..q, j = q..k,
+  // zn[j-1] += sign * zn[j]
+  __device__ void pascal(double sign) {
+    #pragma unroll 1
+    for (int i = lane; i < n; i += 32) {
+      double v[LMAX];
+#pragma unroll
+      for (int j = 0; j < LMAX; ++j) v[j] = (j <= q) ? zb[j * n + i] : 0.0;
+#pragma unroll
+      for (int k = 1; k <= QMAX; ++k)
+#pragma unroll
+        for (int j = QMAX; j >= 1; --j)
+          if (k <= q && j >= k && j <= q) v[j - 1] += sign * v[j];
+#pragma unroll
+      for (int j = 0; j < QMAX; ++j)
+        if (j < q) zb[j * n + i] = v[j];
+    }
+    __syncwarp();
+  }
   __device__ void predict() {
     tn += h;
-    for (int i = lane; i < n; i += 32)
-      for (int k = 1; k <= q; ++k)
-        for (int j = q; j >= k; --j) (zb + (j - 1) * n)[i] += (zb + (j) * n)[i];
-    __syncwarp();
+    pascal(1.0);
   }
   __device__ void restore(double saved_t) {
     tn = saved_t;
-    for (int i = lane; i < n; i += 32)
-      for (int k = 1; k <= q; ++k)
-        for (int j = q; j >= k; --j) (zb + (j - 1) * n)[i] -= (zb + (j) * n)[i];
-    __syncwarp();
+    pascal(-1.0);
   }
   // l and tq of the fixed-leading-coefficient BDF formula
   __device__ void set() {
     double alpha0, alpha0_hat, xi_inv, xistar_inv, hsum;
     l[0] = l[1] = xi_inv = xistar_inv = 1.0;
+    #pragma unroll 1
     for (int i = 2; i <= q; ++i) l[i] = 0.0;
     alpha0 = alpha0_hat = -1.0;
     hsum = h;
     if (q > 1) {
+      #pragma unroll 1
       for (int j = 2; j < q; ++j) {
         hsum += tau[j - 1];
-        xi_inv = h / hsum;
-        alpha0 -= 1.0 / j;
+        xi_inv = ddiv(h, hsum);
+        alpha0 -= ddiv(1.0, (double)j);
+        #pragma unroll 1
         for (int i = j; i >= 1; --i) l[i] += l[i - 1] * xi_inv;
       }
-      alpha0 -= 1.0 / q;
+      alpha0 -= ddiv(1.0, (double)q);
       xistar_inv = -l[1] - alpha0;
       hsum += tau[q - 1];
-      xi_inv = h / hsum;
+      xi_inv = ddiv(h, hsum);
       alpha0_hat = -l[1] - xi_inv;
+      #pragma unroll 1
       for (int i = q; i >= 1; --i) l[i] += l[i - 1] * xistar_inv;
     }
     double A1 = 1.0 - alpha0_hat + alpha0;
     double A2 = 1.0 + q * A1;
-    tq[2] = fabs(A1 / (alpha0 * A2));
-    tq[5] = fabs(A2 * xistar_inv / (l[q] * xi_inv));
+    tq[2] = fabs(ddiv(A1, alpha0 * A2));
+    tq[5] = fabs(ddiv(A2 * xistar_inv, l[q] * xi_inv));
     if (qwait == 1) {
       if (q > 1) {
-        double C = xistar_inv / l[q];
-        double A3 = alpha0 + 1.0 / q;
+        double C = ddiv(xistar_inv, l[q]);
+        double A3 = alpha0 + ddiv(1.0, (double)q);
         double A4 = alpha0_hat + xi_inv;
-        double Cpinv = (1.0 - A4 + A3) / A3;
+        double Cpinv = ddiv(1.0 - A4 + A3, A3);
         tq[1] = fabs(C * Cpinv);
       } else {
         tq[1] = 1.0;
       }
       hsum += tau[q];
-      xi_inv = h / hsum;
-      double A5 = alpha0 - 1.0 / (q + 1);
+      xi_inv = ddiv(h, hsum);
+      double A5 = alpha0 - ddiv(1.0, (double)(q + 1));
       double A6 = alpha0_hat - xi_inv;
-      double Cppinv = (1.0 - A6 + A5) / A2;
-      tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+      double Cppinv = ddiv(1.0 - A6 + A5, A2);
+      tq[3] = fabs(ddiv(Cppinv, xi_inv * (q + 2) * A5));
     }
-    tq[4] = NLSCOEF / tq[2];
-    rl1 = 1.0 / l[1];
+    tq[4] = ddiv(NLSCOEF, tq[2]);
+    rl1 = ddiv(1.0, l[1]);
     gamma = h * rl1;
     if (nst == 0) gammap = gamma;
-    gamrat = (nst > 0) ? gamma / gammap : 1.0;
+    gamrat = (nst > 0) ? ddiv(gamma, gammap) : 1.0;
   }
   __device__ void increase_order() {
+    #pragma unroll 1
     for (int i = 0; i <= QMAX; ++i) l[i] = 0.0;
     l[2] = 1.0;
     double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = hscale;
     if (q > 1) {
+      #pragma unroll 1
       for (int j = 1; j < q; ++j) {
         hsum += tau[j + 1];
-        double xi = hsum / hscale;
+        double xi = ddiv(hsum, hscale);
         prod *= xi;
-        alpha0 -= 1.0 / (j + 1);
-        alpha1 += 1.0 / xi;
+        alpha0 -= ddiv(1.0, (double)(j + 1));
+        alpha1 += ddiv(1.0, xi);
+        #pragma unroll 1
         for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xiold + l[i - 1];
         xiold = xi;
       }
     }
-    double A1 = (-alpha0 - alpha1) / prod;
+    double A1 = ddiv(-alpha0 - alpha1, prod);
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
       double top = A1 * (zb + (QMAX) * n)[i];
       (zb + (q + 1) * n)[i] = top;
+      #pragma unroll 1
       for (int j = 2; j <= q; ++j) (zb + (j) * n)[i] += l[j] * top;
     }
     __syncwarp();
   }
   __device__ void decrease_order() {
+    #pragma unroll 1
     for (int i = 0; i <= QMAX; ++i) l[i] = 0.0;
     l[2] = 1.0;
     double hsum = 0.0;
+    #pragma unroll 1
     for (int j = 1; j <= q - 2; ++j) {
       hsum += tau[j];
-      double xi = hsum / hscale;
+      double xi = ddiv(hsum, hscale);
+      #pragma unroll 1
       for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xi + l[i - 1];
     }
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32)
+      #pragma unroll 1
       for (int j = 2; j < q; ++j) (zb + (j) * n)[i] -= l[j] * (zb + (q) * n)[i];
     __syncwarp();
   }
@@ -719,7 +794,7 @@ struct Cell {
   // J reuse rule of the CVODE direct linear solver interface; returns 0, or
   // >0 for a recoverable failure
   __device__ int lsetup(int convfail, const double* ypred) {
-    double dgamma = fabs(gamma / gammap - 1.0);
+    double dgamma = fabs(ddiv(gamma, gammap) - 1.0);
     bool jbad = (nst == 0) || (nst > nstlj + MSBJ) ||
                 ((convfail == FAIL_BAD_J) && (dgamma < DGMAX_J)) || (convfail == FAIL_OTHER);
     if (!jbad) {
@@ -737,7 +812,9 @@ struct Cell {
   __device__ int newton(bool projected) {
     int mm = 0;
     double del, delp = 0.0;
+    #pragma unroll 1
     for (;;) {
+      #pragma unroll 1
       for (int i = lane; i < n; i += 32)
         tempv[i] = gamma * ftemp[i] - (rl1 * (zb + (1) * n)[i] + acor[i]);
       __syncwarp();
@@ -746,18 +823,20 @@ struct Cell {
       else
         dev_lsolve<LT>(tb, LU, dinv, tempv, z, lane);
       if (gamrat != 1.0) {
-        double s = 2.0 / (1.0 + gamrat);
+        double s = ddiv(2.0, 1.0 + gamrat);
+        #pragma unroll 1
         for (int i = lane; i < n; i += 32) tempv[i] *= s;
       }
       nni++;
       del = wrms(tempv);
+      #pragma unroll 1
       for (int i = lane; i < n; i += 32) {
         acor[i] += tempv[i];
         y[i] = (zb + (0) * n)[i] + acor[i];
       }
       __syncwarp();
-      if (mm > 0) crate = fmax(CRDOWN * crate, del / delp);
-      double dcon = del * fmin(1.0, crate) / tq[4];
+      if (mm > 0) crate = fmax(CRDOWN * crate, ddiv(del, delp));
+      double dcon = ddiv(del * fmin(1.0, crate), tq[4]);
       if (dcon <= 1.0) {
         acnrm = (mm == 0 && !projected) ? del : wrms(acor);
         jcur = 0;
@@ -777,6 +856,7 @@ struct Cell {
   __device__ int check_constraints() {
     bool viol = false;
     double s = 0.0;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32)
       if (y[i] < 0.0) {
         viol = true;
@@ -784,8 +864,9 @@ struct Cell {
         s += t * t;
       }
     if (!warp_any(viol)) return NL_OK;
-    double vnorm = sqrt(warp_sum(s) / n);
+    double vnorm = dsqrt(ddiv(warp_sum(s), (double)n));
     if (vnorm <= tq[4]) {
+      #pragma unroll 1
       for (int i = lane; i < n; i += 32)
         if (y[i] < 0.0) {
           acor[i] -= y[i];
@@ -796,9 +877,10 @@ struct Cell {
       return NL_OK;
     }
     double e = 1.0e300;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32)
       if (y[i] < 0.0) {
-        double qv = (zb + (0) * n)[i] / ((zb + (0) * n)[i] - y[i]);
+        double qv = ddiv(zb[i], zb[i] - y[i]);
         e = fmin(e, qv);
       }
     e = warp_min(e) * 0.9;
@@ -807,6 +889,7 @@ struct Cell {
   }
   __device__ bool start_guess() {
     bool proj = false;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
       double a = (zb + (0) * n)[i] < 0.0 ? -(zb + (0) * n)[i] : 0.0;
       proj |= a != 0.0;
@@ -821,6 +904,7 @@ struct Cell {
     bool call_setup = (nflag == PREV_CONV_FAIL) || (nflag == PREV_ERR_FAIL) || (nst == 0) ||
                       (nst >= nstlp + MSBP) || (fabs(gamrat - 1.0) > DGMAX);
     bool projected = start_guess();
+    #pragma unroll 1
     for (;;) {
       int r = f(y, ftemp);
       nfe++;
@@ -865,7 +949,7 @@ struct Cell {
     if (*nef == maxnef) return ERR_FAILURE;
     etamax = 1.0;
     if (*nef <= MXNEF1) {
-      eta = 1.0 / (dpow(BIAS2 * *dsm, 1.0 / L) + ADDON);
+      eta = ddiv(1.0, dpow(BIAS2 * *dsm, ddiv(1.0, (double)L)) + ADDON);
       eta = fmax(ETAMIN, eta);
       if (*nef >= SMALL_NEF) eta = fmin(eta, ETAMXF);
       rescale();
@@ -885,9 +969,13 @@ struct Cell {
     next_h = h;
     hscale = h;
     qwait = LONG_WAIT;
-    int r = f((zb + (0) * n), tempv);
+    #pragma unroll 1
+    for (int i = lane; i < n; i += 32) y[i] = zb[i];
+    __syncwarp();
+    int r = f(y, tempv);
     nfe++;
     if (r > 0) return UNREC_RHSFUNC_ERR;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) (zb + (1) * n)[i] = h * tempv[i];
     __syncwarp();
     return TRY_AGAIN;
@@ -895,12 +983,15 @@ struct Cell {
   __device__ void complete_step() {
     nst++;
     hu = h;
+    #pragma unroll 1
     for (int i = q; i >= 2; --i) tau[i] = tau[i - 1];
     if ((q == 1) && (nst > 1)) tau[2] = tau[1];
     tau[1] = h;
     const bool save = (qwait - 1 == 1) && (q != QMAX);
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
       const double a = acor[i];
+      #pragma unroll 1
       for (int j = 0; j <= q; ++j) (zb + (j) * n)[i] += l[j] * a;
       if (save) (zb + (QMAX) * n)[i] = a;
     }
@@ -927,7 +1018,7 @@ struct Cell {
       eta = 1.0;
       return;
     }
-    etaq = 1.0 / (dpow(BIAS2 * dsm, 1.0 / L) + ADDON);
+    etaq = ddiv(1.0, dpow(BIAS2 * dsm, ddiv(1.0, (double)L)) + ADDON);
     if (qwait != 0) {
       eta = etaq;
       qprime = q;
@@ -938,14 +1029,15 @@ struct Cell {
     etaqm1 = 0.0;
     if (q > 1) {
       double ddn = wrms((zb + (q) * n)) * tq[1];
-      etaqm1 = 1.0 / (dpow(BIAS1 * ddn, 1.0 / q) + ADDON);
+      etaqm1 = ddiv(1.0, dpow(BIAS1 * ddn, ddiv(1.0, (double)q)) + ADDON);
     }
     etaqp1 = 0.0;
     if (q != QMAX && saved_tq5 != 0.0) {
-      double cquot = (tq[5] / saved_tq5) * dpow(h / tau[2], (double)L);
+      double cquot = ddiv(tq[5], saved_tq5) * dpow(ddiv(h, tau[2]), (double)L);
+      #pragma unroll 1
       for (int i = lane; i < n; i += 32) tempv[i] = acor[i] - cquot * (zb + (QMAX) * n)[i];
       double dup = wrms(tempv) * tq[3];
-      etaqp1 = 1.0 / (dpow(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
+      etaqp1 = ddiv(1.0, dpow(BIAS3 * dup, ddiv(1.0, (double)(L + 1))) + ADDON);
     }
     double etam = fmax(etaqm1, fmax(etaq, etaqp1));
     if (etam < THRESH) {
@@ -960,6 +1052,7 @@ struct Cell {
     } else {
       eta = etaqp1;
       qprime = q + 1;
+      #pragma unroll 1
       for (int i = lane; i < n; i += 32) (zb + (QMAX) * n)[i] = acor[i];
       __syncwarp();
     }
@@ -969,6 +1062,7 @@ struct Cell {
     double saved_t = tn, dsm = 0.0;
     int ncf = 0, nef = 0, nflag = FIRST_CALL;
     if ((nst > 0) && (hprime != h)) adjust_params();
+    #pragma unroll 1
     for (;;) {
       predict();
       set();
@@ -984,6 +1078,7 @@ struct Cell {
     complete_step();
     prepare_next_step(dsm);
     etamax = (nst <= SMALL_NST) ? ETAMX2 : ETAMX3;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) acor[i] *= tq[2];
     __syncwarp();
     return OK;
@@ -991,7 +1086,9 @@ struct Cell {
   // CVodeReInit + CVodeSetInitStep(h0) + CVode(tout, CV_NORMAL); y (shared)
   // holds the initial values and receives the interpolated solution
   __device__ int integrate(double t0, double tout) {
+    #pragma unroll 1
     for (int i = 0; i <= LMAX; ++i) tau[i] = 0.0;
+    #pragma unroll 1
     for (int i = 0; i < 6; ++i) tq[i] = 0.0;
     q = 1;
     L = 2;
@@ -1009,22 +1106,26 @@ struct Cell {
     h = 0.0;
     h0 = tout - t0;
     eta = 1.0;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
       (zb + (0) * n)[i] = y[i];
+      #pragma unroll 1
       for (int j = 1; j < LMAX; ++j) (zb + (j) * n)[i] = 0.0;
     }
     __syncwarp();
     if (!set_ewt((zb + (0) * n))) return ILL_INPUT;
     next_h = 0.0;
-    if (f((zb + (0) * n), (zb + (1) * n))) return REPTD_RHSFUNC_ERR;
+    if (f(y, (zb + (1) * n))) return REPTD_RHSFUNC_ERR;
     nfe++;
     h = h0;
     if ((tout - t0) * h < 0.0) return ILL_INPUT;
     hscale = h;
     hprime = h;
+    #pragma unroll 1
     for (int i = lane; i < n; i += 32) (zb + (1) * n)[i] *= h;
     __syncwarp();
     int nstloc = 0;
+    #pragma unroll 1
     for (;;) {
       next_h = h;
       if (nst > 0 && !set_ewt((zb + (0) * n))) return ILL_INPUT;
@@ -1036,8 +1137,10 @@ struct Cell {
       nstloc++;
       if ((tn - tout) * h >= 0.0) {
         double s = (tout - tn) / h;
+        #pragma unroll 1
         for (int i = lane; i < n; i += 32) {
           double v = (zb + (q) * n)[i];
+          #pragma unroll 1
           for (int j = q - 1; j >= 0; --j) v = (zb + (j) * n)[i] + s * v;
           y[i] = v;
         }
@@ -1059,7 +1162,7 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char
   c.atol = make_tab(tab).atol;
   c.lane = lane;
   c.n = a.off.n;
-  c.zb = (double*)(base + a.lay.zn);
+  c.zb = a.lay.zn >= 0 ? (double*)(base + a.lay.zn) : a.hist + (size_t)gwarp * a.hist_stride;
   double* ctl = (double*)(base + a.lay.ctl);
   c.tau = ctl;
   c.tq = ctl + (LMAX + 2);
@@ -1070,7 +1173,7 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char
   c.ftemp = (double*)(base + a.lay.ftemp);
   c.tempv = (double*)(base + a.lay.tempv);
   c.rates = (double*)(base + a.lay.rates);
-  c.keff = (double*)(base + a.lay.keff);
+  c.keff = a.lay.keff >= 0 ? (double*)(base + a.lay.keff) : c.zb + (size_t)LMAX * a.off.n;
   c.fscr = (double*)(base + a.lay.fscr);
   c.LU = (LT*)(base + a.lay.lu);
   c.z = (LT*)(base + a.lay.z);
@@ -1096,6 +1199,7 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
   bind_cell<LT>(c, a, smem, base, gwarp, lane);
   const DevMech& m = a.m;
   const uint16_t* dep_state = make_tab(smem).dep_state;
+  #pragma unroll 1
   for (;;) {
     int idx = 0;
     if (lane == 0) idx = atomicAdd(a.counter, 1);
@@ -1105,10 +1209,12 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
     double* st = a.state + (size_t)cell * m.n_state;
     // solver_run: dependent values clamped to >= TINY, constants clamped in
     // place (src/camp_solver.c:554-567)
+    #pragma unroll 1
     for (int i = lane; i < c.n; i += 32) {
       double v = st[dep_state[i]];
       c.y[i] = v > kTiny ? v : kTiny;
     }
+    #pragma unroll 1
     for (int j = lane; j < m.n_const; j += 32) {
       int s = ldg(m.const_state + j);
       double v = st[s];
@@ -1120,6 +1226,7 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
                  c.keff, lane);
     int flag = c.integrate(a.t0, a.t1);
     if (flag == OK)
+      #pragma unroll 1
       for (int i = lane; i < c.n; i += 32) st[dep_state[i]] = c.y[i] > 0.0 ? c.y[i] : 0.0;
     if (lane == 0) {
       CellStats s;
@@ -1172,6 +1279,7 @@ __global__ void eval_kernel(EvalArgs a) {
   double* keff = (double*)(base + a.lay.keff);
   double* fscr = (double*)(base + a.lay.fscr);
   const double* st = a.state + (size_t)cell * m.n_state;
+  #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) y[i] = st[t.dep_state[i]];
   __syncwarp();
   compute_keff(m, st, a.env[2 * cell], a.env[2 * cell + 1],
@@ -1180,6 +1288,7 @@ __global__ void eval_kernel(EvalArgs a) {
     double* out = (double*)(base + a.lay.ftemp);
     dev_f(smem, y, a.h, keff, rates, fscr, out, lane, a.rp + (size_t)cell * t.n,
           a.rl + (size_t)cell * t.n);
+    #pragma unroll 1
     for (int i = lane; i < t.n; i += 32) a.f[(size_t)cell * t.n + i] = out[i];
   } else {
     dev_jac<double>(smem, y, a.h, keff, rates, a.jv + (size_t)cell * t.n_jac, lane,
@@ -1225,6 +1334,8 @@ struct Engine::Impl {
   int* d_counter = nullptr;
   void* d_jscratch = nullptr;
   size_t c_jscratch = 0;
+  void* d_hist = nullptr;
+  size_t c_hist = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool ev_pending = false;
 };
@@ -1245,6 +1356,7 @@ Engine::~Engine() {
   cudaFree(I->d_stats);
   cudaFree(I->d_counter);
   cudaFree(I->d_jscratch);
+  cudaFree(I->d_hist);
   if (I->ev0) cudaEventDestroy(I->ev0);
   if (I->ev1) cudaEventDestroy(I->ev1);
   delete I;
@@ -1359,7 +1471,10 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   return true;
 }
 
-static Layout make_layout(const BlobOff& o, int lt_size) {
+// per-warp shared-memory slice; the solve kernel keeps the Nordsieck history
+// and the rate constants in global memory (with_hist = false), which leaves
+// room for more resident cells
+static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist) {
   Layout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -1368,14 +1483,14 @@ static Layout make_layout(const BlobOff& o, int lt_size) {
     return (int)r;
   };
   const size_t vec = sizeof(double) * o.n;
-  L.zn = take(vec * LMAX);
+  L.zn = with_hist ? take(vec * LMAX) : -1;
   L.ewt = take(vec);
   L.acor = take(vec);
   L.y = take(vec);
   L.ftemp = take(vec);
   L.tempv = take(vec);
   L.rates = take(sizeof(double) * std::max(o.n_rxn, o.n_part));
-  L.keff = take(sizeof(double) * o.n_rxn);
+  L.keff = with_hist ? take(sizeof(double) * o.n_rxn) : -1;
   L.fscr = take(sizeof(double) * 2 * std::max(1, o.n_fscratch));
   L.lu = take((size_t)lt_size * o.n_lu);
   L.z = take((size_t)lt_size * o.n);
@@ -1414,7 +1529,7 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
     return true;
   }
   const int lt = s.precision == 1 ? 4 : 8;
-  Layout lay = make_layout(I->off, lt);
+  Layout lay = make_layout(I->off, lt, s.hist_global == 0);
   const int tab = tab_bytes_of(I->off, s.lu_mode);
   int max_warps = (I->max_smem - tab) / lay.bytes;
   if (max_warps < 1) {
@@ -1434,6 +1549,11 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
   if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)lt * I->m.n_jac * total_warps, err))
     return false;
+  // history + rate constants per warp, rounded to 256-byte rows
+  const int hist_stride = s.hist_global ? ((LMAX * I->off.n + I->off.n_rxn) + 31) & ~31 : 0;
+  if (s.hist_global &&
+      !ensure(&I->d_hist, &I->c_hist, sizeof(double) * (size_t)hist_stride * total_warps, err))
+    return false;
   CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
   SolveArgs a;
   a.m = I->m;
@@ -1451,6 +1571,8 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   a.counter = I->d_counter;
   a.stats = (CellStats*)I->d_stats;
   a.jscratch = I->d_jscratch;
+  a.hist = (double*)I->d_hist;
+  a.hist_stride = hist_stride;
   a.t0 = t0;
   a.t1 = t1;
   a.rtol = s.rtol;
@@ -1552,7 +1674,7 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
   a.tab_bytes = tab_bytes_of(I->off, 1);
   a.stage_bytes = I->off.bytes;
   a.err = I->d_counter + 1;
-  a.lay = make_layout(I->off, 8);
+  a.lay = make_layout(I->off, 8, true);
   a.state = ds;
   a.env = de;
   a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
@@ -1600,7 +1722,7 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   a.tab_bytes = tab_bytes_of(I->off, 1);
   a.stage_bytes = I->off.bytes;
   a.err = I->d_counter + 1;
-  a.lay = make_layout(I->off, 8);
+  a.lay = make_layout(I->off, 8, true);
   a.state = ds;
   a.env = de;
   a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;

@@ -82,6 +82,12 @@ class Solver:
     def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 1) -> None:
         self.lib.camp_b200_set_launch(self._h, int(warps_per_block), int(blocks_per_sm))
 
+    def set_layout(self, hist_global: int) -> None:
+        """0: Nordsieck history and rate constants in shared memory; 1: in
+        global memory (more resident cells per SM)."""
+        if self.lib.camp_b200_set_layout(self._h, int(hist_global)) != 0:
+            raise SolverError(_lib.last_error())
+
     def set_lu_mode(self, mode: int) -> None:
         if self.lib.camp_b200_set_lu_mode(self._h, int(mode)) != 0:
             raise SolverError(_lib.last_error())

@@ -158,6 +158,10 @@ int camp_b200_set_lu_mode(void *solver_data, int mode);
  * bit 2 the solve vector in shared memory; the rest of a cell's working set
  * lives in a lane-interleaved global scratch.  -1 keeps the current value. */
 int camp_b200_set_kernel(void *solver_data, int kernel, int place);
+/* Where the warp-per-cell kernel keeps each cell's Nordsieck history and rate
+ * constants: 0 = shared memory (default), 1 = global memory (L1/L2 cached),
+ * which leaves shared memory for more resident cells.  The autotuner picks. */
+int camp_b200_set_layout(void *solver_data, int hist_global);
 /* Orders the cells of the next run by decreasing internal step count of the
  * previous run (longest-first scheduling of the persistent kernel). */
 int camp_b200_set_cost_ordering(void *solver_data, int enable);
