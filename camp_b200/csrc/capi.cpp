@@ -475,6 +475,27 @@ int camp_b200_run_device(void* solver_data, double* d_state, const double* d_env
   return status_of(s, n_cells);
 }
 
+static_assert(sizeof(camp_b200_cell_stats) == sizeof(campb::CellStats),
+              "camp_b200_cell_stats must mirror the device CellStats");
+
+int camp_b200_run_device_noalloc(void* solver_data, double* d_state, const double* d_env,
+                                 const double* d_photo, camp_b200_cell_stats* d_stats,
+                                 int n_cells, double t_initial, double t_final, void* stream) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0) {
+    set_error("camp_b200_run_device_noalloc: solver not ready or n_cells <= 0");
+    return -1;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+  std::string err;
+  if (!s->engine->run_solve_static(d_state, d_env, d_photo, (campb::CellStats*)d_stats, n_cells,
+                                   t_initial, t_final, s->settings, st, &err)) {
+    set_error("camp_b200_run_device_noalloc: " + err);
+    return -1;
+  }
+  return 0;
+}
+
 int camp_b200_launch_device(void* solver_data, double* d_state, const double* d_env,
                             int n_cells, double t_initial, double t_final, void* stream) {
   Solver* s = S(solver_data);

@@ -44,6 +44,14 @@ class Engine {
   bool launch_solve(double* d_state, const double* d_env, const double* d_photo,
                     const int* d_order, int n_cells, double t0, double t1,
                     const SolveSettings& s, void* stream, std::string* err);
+  // The same solve without any device allocation: its scratch lives in a
+  // fixed static device array (solve.cu), per-cell stats go to the caller's
+  // d_stats, the Nordsieck history stays in shared memory.  Waits for the
+  // stream; false with a message on a usage error, on a scratch need above
+  // the static size, or on a kernel error.
+  bool run_solve_static(double* d_state, const double* d_env, const double* d_photo,
+                        CellStats* d_stats, int n_cells, double t0, double t1,
+                        const SolveSettings& s, void* stream, std::string* err);
   // Copies per-cell stats of the last launch to the host (synchronising).
   bool fetch_stats(std::vector<CellStats>* out, int n_cells, void* stream,
                    std::string* err);

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "blob.hpp"
 #include "engine.hpp"
@@ -1745,6 +1746,138 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   cudaFree(de);
   cudaFree(dp);
   cudaFree(dout);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Solve without device allocation
+//
+// Some callers cannot allocate device memory while they run: a host model
+// that hands the whole device heap to its own pool allocator up front, or a
+// code that runs this solve inside a region where cudaMalloc is not allowed.
+// For them the solve's scratch (the cell counter, the error flag and each
+// resident cell's saved Jacobian) lives in one fixed static device array of
+// kStaticScratchBytes that every GPU loading this library holds until the
+// process exits.  Calls share the array and it keeps the last call's
+// contents; the counter and flag are cleared by every call, the Jacobian
+// slots are always written before they are read.  Two such calls that
+// overlap on the GPU (different streams, or different solvers on one device)
+// race on the array.
+// ---------------------------------------------------------------------------
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;  // 8 MiB
+constexpr size_t kStaticHeadBytes = 256;                 // counter, error flag
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of the static scratch on the current device.  The host-side
+// name g_static_scratch is only a stand-in, so the address is looked up once
+// per device (with that device current) and kept.
+static bool static_scratch_address(char** out, std::string* err) {
+  static std::mutex mu;
+  static void* addr[64] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    *err = "device index out of range for the static scratch table";
+    return false;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_static_scratch));
+    addr[dev] = p;
+  }
+  *out = (char*)addr[dev];
+  return true;
+}
+
+bool Engine::run_solve_static(double* d_state, const double* d_env, const double* d_photo,
+                              CellStats* d_stats, int n_cells, double t0, double t1,
+                              const SolveSettings& s, void* stream, std::string* err) {
+  Impl* I = impl_;
+  if (n_cells <= 0) return true;
+  if (!d_state || !d_env || !d_stats || (I->m.n_photo > 0 && !d_photo)) {
+    *err = "state, env, stats (and photolysis rates, when the mechanism has photolysis) "
+           "must be device buffers";
+    return false;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int lt = s.precision == 1 ? 4 : 8;
+  Layout lay = make_layout(I->off, lt, true);
+  const int tab = tab_bytes_of(I->off, s.lu_mode);
+  int warps = (I->max_smem - tab) / lay.bytes;
+  if (warps < 1) {
+    *err = "mechanism too large for the shared-memory layout (" + std::to_string(lay.bytes) +
+           " bytes per cell)";
+    return false;
+  }
+  if (s.warps_per_block > 0) warps = std::min(warps, s.warps_per_block);
+  warps = std::min(warps, 16);
+  // one resident cell keeps n_jac Jacobian values (the kernel indexes them
+  // by warp); the static array bounds the number of resident cells
+  const size_t per_warp = (size_t)lt * I->m.n_jac;
+  const size_t fit = (kStaticScratchBytes - kStaticHeadBytes) / per_warp;
+  if (fit < (size_t)I->sm_count) {
+    *err = "the mechanism needs " + std::to_string(per_warp) +
+           " bytes of scratch per resident cell; the static scratch of " +
+           std::to_string(kStaticScratchBytes) + " bytes holds " + std::to_string(fit) +
+           ", fewer than one per SM (" + std::to_string(I->sm_count) + ")";
+    return false;
+  }
+  warps = std::min(warps, (int)(fit / (size_t)I->sm_count));
+  int grid = I->sm_count;
+  if ((long)grid * warps > n_cells) grid = std::max(1, (n_cells + warps - 1) / warps);
+  char* base = nullptr;
+  if (!static_scratch_address(&base, err)) return false;
+  int* counter = (int*)base;
+  CK(cudaMemsetAsync(counter, 0, kStaticHeadBytes, st));
+  SolveArgs a;
+  a.m = I->m;
+  a.off = I->off;
+  a.blob = I->d_blob;
+  a.tab_bytes = tab;
+  a.stage_bytes = stage_bytes_of(I->off, s.lu_mode);
+  a.err = counter + 1;
+  a.lay = lay;
+  a.state = d_state;
+  a.env = d_env;
+  a.photo = I->m.n_photo > 0 ? d_photo : nullptr;
+  a.order = nullptr;
+  a.n_cells = n_cells;
+  a.counter = counter;
+  a.stats = d_stats;
+  a.jscratch = base + kStaticHeadBytes;
+  a.hist = nullptr;
+  a.hist_stride = 0;
+  a.t0 = t0;
+  a.t1 = t1;
+  a.rtol = s.rtol;
+  a.max_steps = s.max_steps;
+  a.maxncf = s.max_conv_fails;
+  a.maxnef = s.max_conv_fails;
+  a.lu_mode = s.lu_mode;
+  const size_t smem = (size_t)tab + (size_t)warps * lay.bytes;
+  CK(cudaEventRecord(I->ev0, st));
+  if (s.precision == 1) {
+    CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    solve_kernel<float><<<grid, warps * 32, smem, st>>>(a);
+  } else {
+    CK(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)smem));
+    solve_kernel<double><<<grid, warps * 32, smem, st>>>(a);
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(I->ev1, st));
+  ++launches_;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, I->ev0, I->ev1) == cudaSuccess) last_ms_ = ms;
+  if (flag) {
+    *err = "solve kernel: the table stage into shared memory did not complete";
+    return false;
+  }
   return true;
 }
 

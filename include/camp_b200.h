@@ -181,6 +181,26 @@ int camp_b200_launch_device(void *solver_data, double *d_state,
                             double t_final, void *stream);
 int camp_b200_sync_status(void *solver_data, void *stream);
 
+/* No counterpart in the reference: a device-resident solve that allocates no
+ * device memory, for callers that cannot call cudaMalloc while they run (a
+ * host model whose pool allocator owns the device heap, or code running where
+ * allocation is not allowed).  All buffers are the caller's: state
+ * [n_cells*n_state_var] (updated in place), env [n_cells*2], photolysis base
+ * rates [n_cells*n_photo] (may be NULL without photolysis reactions) and the
+ * per-cell results d_stats [n_cells], all in device memory.  The solve's
+ * scratch lives in one static 8 MiB device array that every GPU loading this
+ * library holds until exit; a mechanism needing more than that for one
+ * resident cell per SM is rejected with an error, fewer resident cells are
+ * used when it needs less.  The first call on a device looks up the array's
+ * address; make that first call before any stream capture.  Calls share the
+ * array, so two calls that overlap on the GPU race.  Waits for the stream;
+ * returns 0 when the solve ran (per-cell status in d_stats) or -1 with
+ * camp_b200_last_error() set. */
+int camp_b200_run_device_noalloc(void *solver_data, double *d_state,
+                                 const double *d_env, const double *d_photo,
+                                 camp_b200_cell_stats *d_stats, int n_cells,
+                                 double t_initial, double t_final, void *stream);
+
 /* Per-cell photolysis base rates: rates[c * n_photo + j] for photolysis
  * reaction j (mechanism order) of cell c, as if rxn_update_data had been
  * called for every cell and reaction. */
