@@ -43,13 +43,15 @@ EXPORTED = [
     "sub_model_add_condensed_data", "sub_model_update_data", "aero_phase_print_data",
     "aero_rep_print_data", "sub_model_print_data",
     "camp_b200_last_error", "camp_b200_is_ready", "camp_b200_set_precision",
-    "camp_b200_set_launch", "camp_b200_set_lu_mode", "camp_b200_set_kernel", "camp_b200_set_layout", "camp_b200_set_cost_ordering", "camp_b200_run_device",
+    "camp_b200_set_launch", "camp_b200_set_lu_mode", "camp_b200_set_kernel", "camp_b200_set_layout", "camp_b200_autotune", "camp_b200_get_tuning", "camp_b200_set_cost_ordering", "camp_b200_run_device",
     "camp_b200_launch_device", "camp_b200_sync_status", "camp_b200_run_device_noalloc", "camp_b200_n_photo",
     "camp_b200_set_photo_rates", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
     "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
-    "camp_b200_eval_jac",
+    "camp_b200_eval_jac", "camp_b200_server_new", "camp_b200_server_add_solver",
+    "camp_b200_server_submit", "camp_b200_server_wait", "camp_b200_server_pending",
+    "camp_b200_server_free",
 ]
 
 _lib = None
@@ -87,6 +89,11 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_set_cost_ordering.argtypes = [vp, ip]
     lib.camp_b200_set_lu_mode.restype = ip
     lib.camp_b200_set_lu_mode.argtypes = [vp, ip]
+    lib.camp_b200_autotune.restype = ip
+    lib.camp_b200_autotune.argtypes = [vp, _f64p, _f64p, ip, dp, dp]
+    lib.camp_b200_get_tuning.restype = ip
+    lib.camp_b200_get_tuning.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.camp_b200_set_layout.restype = ip
     lib.camp_b200_set_layout.argtypes = [vp, ip]
     lib.camp_b200_set_kernel.restype = ip
@@ -119,6 +126,17 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_eval_deriv.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p, _f64p]
     lib.camp_b200_eval_jac.restype = ip
     lib.camp_b200_eval_jac.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p]
+    lib.camp_b200_server_new.restype = vp
+    lib.camp_b200_server_new.argtypes = [ip, dp, dp]
+    lib.camp_b200_server_add_solver.restype = ip
+    lib.camp_b200_server_add_solver.argtypes = [vp, vp]
+    lib.camp_b200_server_submit.restype = C.c_long
+    lib.camp_b200_server_submit.argtypes = [vp, ip, vp, vp, vp, ip, dp, dp]
+    lib.camp_b200_server_wait.restype = ip
+    lib.camp_b200_server_wait.argtypes = [vp, C.c_long, C.POINTER(C.c_double), vp, ip]
+    lib.camp_b200_server_pending.restype = ip
+    lib.camp_b200_server_pending.argtypes = [vp]
+    lib.camp_b200_server_free.argtypes = [vp]
     _lib = lib
     return lib
 

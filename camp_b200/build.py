@@ -21,8 +21,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", "-lineinfo"]
 
-SOURCES = ["model.cpp", "blob.cpp", "capi.cpp", "solve.cu", "lanes.cu"]
-HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", "bdf_consts.hpp", "rates.cuh", os.path.join("..", "..", "include", "camp_b200.h")]
+SOURCES = ["model.cpp", "blob.cpp", "capi.cpp", "serve.cpp", "solve.cu", "lanes.cu"]
+HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", "serve.hpp", "bdf_consts.hpp", "rates.cuh",
+           os.path.join("..", "..", "include", "camp_b200.h")]
 
 
 def _newer(src: str, dst: str) -> bool:
@@ -43,7 +44,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"] if verbose else []
             else:
-                cmd += ["-x", "cu"] if src == "capi.cpp" else []
+                cmd += ["-x", "cu"] if src in ("capi.cpp", "serve.cpp") else []
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

@@ -15,6 +15,7 @@
 
 #include "engine.hpp"
 #include "model.hpp"
+#include "serve.hpp"
 
 using campb::CellStats;
 using campb::Engine;
@@ -54,6 +55,7 @@ struct Solver {
   std::vector<CellStats> stats;
   int last_n = 0;
   bool cost_order = false;
+  double tuned_ms = -1.0;  // sample kernel time of the autotuned settings
   std::vector<int> order;
 
   int photo_count() const {
@@ -448,6 +450,77 @@ int camp_b200_set_layout(void* solver_data, int hist_global) {
   return 0;
 }
 
+int camp_b200_autotune(void* solver_data, const double* state, const double* env, int n_cells,
+                       double t_initial, double t_final) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells || !state || !env) {
+    set_error("camp_b200_autotune: solver not ready, or sample empty or above capacity");
+    return -1;
+  }
+  std::string err;
+  double* ds = s->engine->d_state_buf(n_cells, &err);
+  double* de = ds ? s->engine->d_env_buf(n_cells, &err) : nullptr;
+  if (!ds || !de) {
+    set_error("camp_b200_autotune: " + err);
+    return -1;
+  }
+  cudaStream_t st = s->stream;
+  const size_t bytes = sizeof(double) * (size_t)n_cells * s->n_state;
+  if (cudaMemcpyAsync(de, env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice, st) !=
+      cudaSuccess) {
+    set_error("camp_b200_autotune: host to device copy failed");
+    return -1;
+  }
+  // candidates: resident cells per block, where the Nordsieck history lives,
+  // and the LU strategy; the precision and kernel organisation stay as set
+  campb::SolveSettings base = s->settings, best = s->settings;
+  double best_ms = -1.0;
+  const bool cost_order = s->cost_order;
+  s->cost_order = false;
+  for (int lu = 0; lu <= 1; ++lu)
+    for (int hg = 0; hg <= 1; ++hg) {
+      campb::SolveSettings c = base;
+      c.kernel = 0;
+      c.lu_mode = lu;
+      c.hist_global = hg;
+      const int mx = s->engine->max_cells_per_block(c);
+      std::vector<int> ws;
+      for (int w : {mx, mx - 1, mx - 2, (2 * mx) / 3, mx / 2, 8, 11})
+        if (w >= 2 && w <= mx && std::find(ws.begin(), ws.end(), w) == ws.end()) ws.push_back(w);
+      for (int w : ws) {
+        c.warps_per_block = w;
+        c.blocks_per_sm = 1;
+        s->settings = c;
+        if (cudaMemcpyAsync(ds, state, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            !run_common(s, ds, de, n_cells, t_initial, t_final, st, true)) {
+          s->settings = base;
+          s->cost_order = cost_order;
+          set_error("camp_b200_autotune: trial run failed: " + std::string(camp_b200_last_error()));
+          return -1;
+        }
+        const double ms = s->engine->last_kernel_ms();
+        if (best_ms < 0.0 || ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
+      }
+    }
+  s->settings = best;
+  s->tuned_ms = best_ms;
+  s->cost_order = cost_order;
+  return 0;
+}
+
+int camp_b200_get_tuning(void* solver_data, int* warps_per_block, int* hist_global,
+                         int* lu_mode, double* sample_ms) {
+  Solver* s = S(solver_data);
+  if (warps_per_block) *warps_per_block = s->settings.warps_per_block;
+  if (hist_global) *hist_global = s->settings.hist_global;
+  if (lu_mode) *lu_mode = s->settings.lu_mode;
+  if (sample_ms) *sample_ms = s->tuned_ms;
+  return 0;
+}
+
 int camp_b200_set_kernel(void* solver_data, int kernel, int place) {
   if (kernel != 0 && kernel != 1) {
     set_error("camp_b200_set_kernel: kernel must be 0 or 1");
@@ -621,5 +694,68 @@ int camp_b200_eval_jac(void* solver_data, const double* state, const double* env
   }
   return 0;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving loop
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void* camp_b200_server_new(int n_slots, double device_mb, double host_mb) {
+  auto* sv = new campb::Server;
+  std::string err;
+  if (!sv->init(n_slots, (size_t)(device_mb * 1048576.0), (size_t)(host_mb * 1048576.0), &err)) {
+    set_error("camp_b200_server_new: " + err);
+    delete sv;
+    return nullptr;
+  }
+  return sv;
+}
+
+int camp_b200_server_add_solver(void* server, void* solver_data) {
+  Solver* s = S(solver_data);
+  if (!server || !s->ready) {
+    set_error("camp_b200_server_add_solver: no server, or the solver is not initialised");
+    return -1;
+  }
+  s->ensure_photo();
+  std::string err;
+  int id = static_cast<campb::Server*>(server)->add_mechanism(s->engine.get(), s->settings,
+                                                              s->n_state, s->n_photo, &err);
+  if (id < 0) set_error("camp_b200_server_add_solver: " + err);
+  return id;
+}
+
+long camp_b200_server_submit(void* server, int mech, double* state, const double* env,
+                             const double* photo, int n_cells, double t_initial,
+                             double t_final) {
+  std::string err;
+  long id = static_cast<campb::Server*>(server)->submit(mech, state, env, photo, n_cells,
+                                                        t_initial, t_final, &err);
+  if (id < 0) set_error("camp_b200_server_submit: " + err);
+  return id;
+}
+
+int camp_b200_server_wait(void* server, long request, double* latency_ms,
+                          camp_b200_cell_stats* stats, int n_cells) {
+  std::string err;
+  std::vector<campb::CellStats> st;
+  int rc = static_cast<campb::Server*>(server)->wait(request, latency_ms, &st, &err);
+  if (rc < 0) {
+    set_error("camp_b200_server_wait: " + err);
+    return rc;
+  }
+  if (stats)
+    for (int c = 0; c < n_cells && c < (int)st.size(); ++c)
+      std::memcpy(&stats[c], &st[c], sizeof(camp_b200_cell_stats));
+  return rc;
+}
+
+int camp_b200_server_pending(void* server) {
+  return static_cast<campb::Server*>(server)->pending();
+}
+
+void camp_b200_server_free(void* server) { delete static_cast<campb::Server*>(server); }
 
 }  // extern "C"

@@ -2,6 +2,8 @@
 // per-cell solve and evaluation kernels.
 #pragma once
 
+#include <atomic>
+
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -66,15 +68,29 @@ class Engine {
   double* d_photo_buf(int n_cells, std::string* err);
   int* d_order_buf(int n_cells, std::string* err);
   bool sync(void* stream, std::string* err);
+  // cells (warps) per block that fit the shared memory for these settings
+  int max_cells_per_block(const SolveSettings& s) const;
+  // Serving slots: a launch on caller-provided buffers and scratch (from
+  // slot_scratch_bytes for at most max_blocks blocks), so several launches
+  // can be in flight on different streams.  No allocation, no sync.
+  size_t slot_scratch_bytes(const SolveSettings& s, int max_blocks) const;
+  bool launch_solve_slot(double* d_state, const double* d_env, const double* d_photo,
+                         CellStats* d_stats, int n_cells, double t0, double t1,
+                         const SolveSettings& s, char* scratch, size_t scratch_bytes,
+                         int max_blocks, void* stream, std::string* err);
+  int sm_count() const;
   long launches() const { return launches_; }
   double last_kernel_ms() const { return last_ms_; }
   bool read_last_ms(void* stream);
 
  private:
   bool ensure(void** p, size_t* cap, size_t bytes, std::string* err);
+  void fill_args(struct SolveArgs* a, const struct WarpLaunch& w, const SolveSettings& s,
+                 double* d_state, const double* d_env, const double* d_photo,
+                 const int* d_order, int n_cells, double t0, double t1) const;
   struct Impl;
   Impl* impl_;
-  long launches_ = 0;
+  std::atomic<long> launches_{0};
   double last_ms_ = 0.0;
 };
 

@@ -1510,6 +1510,83 @@ static int tab_bytes_of(const BlobOff& o, int lu_mode) {
   return (stage_bytes_of(o, lu_mode) + 127) & ~127;
 }
 
+// Geometry and launch of the warp-per-cell kernel shared by the solver's own
+// launches and the serving slots.  Scratch pointers come from the caller.
+struct WarpLaunch {
+  int grid = 0, warps = 0, tab = 0, lt = 8;
+  Layout lay{};
+  size_t smem = 0;
+};
+
+static bool plan_warp_launch(const BlobOff& off, int sm_count, int max_smem,
+                             const SolveSettings& s, int n_cells, int max_blocks,
+                             WarpLaunch* w, std::string* err) {
+  w->lt = s.precision == 1 ? 4 : 8;
+  w->lay = make_layout(off, w->lt, s.hist_global == 0);
+  w->tab = tab_bytes_of(off, s.lu_mode);
+  int max_warps = (max_smem - w->tab) / w->lay.bytes;
+  if (max_warps < 1) {
+    *err = "mechanism too large for the shared-memory layout (" +
+           std::to_string(w->lay.bytes) + " bytes per cell)";
+    return false;
+  }
+  int warps = s.warps_per_block > 0 ? std::min(s.warps_per_block, max_warps) : max_warps;
+  warps = std::min(warps, 16);
+  int bps = std::max(1, s.blocks_per_sm);
+  while (bps > 1 && (size_t)bps * (w->tab + warps * w->lay.bytes) > (size_t)max_smem) --bps;
+  int grid = std::min(sm_count * bps, std::max(1, max_blocks));
+  // no more warps than cells
+  if ((long)grid * warps > n_cells) grid = std::max(1, (int)((n_cells + warps - 1) / warps));
+  w->grid = grid;
+  w->warps = warps;
+  w->smem = (size_t)w->tab + (size_t)warps * w->lay.bytes;
+  return true;
+}
+
+static int hist_stride_of(const BlobOff& off, const SolveSettings& s) {
+  // history + rate constants per warp, rounded to 256-byte rows
+  return s.hist_global ? ((LMAX * off.n + off.n_rxn) + 31) & ~31 : 0;
+}
+
+static bool launch_warp_kernel(SolveArgs& a, const WarpLaunch& w, int precision,
+                               cudaStream_t st, std::string* err) {
+  if (precision == 1) {
+    CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)w.smem));
+    solve_kernel<float><<<w.grid, w.warps * 32, w.smem, st>>>(a);
+  } else {
+    CK(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)w.smem));
+    solve_kernel<double><<<w.grid, w.warps * 32, w.smem, st>>>(a);
+  }
+  CK(cudaGetLastError());
+  return true;
+}
+
+void Engine::fill_args(SolveArgs* a, const WarpLaunch& w, const SolveSettings& s, double* d_state,
+                       const double* d_env, const double* d_photo, const int* d_order,
+                       int n_cells, double t0, double t1) const {
+  const Impl* I = impl_;
+  a->m = I->m;
+  a->off = I->off;
+  a->blob = I->d_blob;
+  a->tab_bytes = w.tab;
+  a->stage_bytes = stage_bytes_of(I->off, s.lu_mode);
+  a->lay = w.lay;
+  a->state = d_state;
+  a->env = d_env;
+  a->photo = I->m.n_photo > 0 ? d_photo : nullptr;
+  a->order = d_order;
+  a->n_cells = n_cells;
+  a->t0 = t0;
+  a->t1 = t1;
+  a->rtol = s.rtol;
+  a->max_steps = s.max_steps;
+  a->maxncf = s.max_conv_fails;
+  a->maxnef = s.max_conv_fails;
+  a->lu_mode = s.lu_mode;
+}
+
 bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_photo,
                           const int* d_order, int n_cells, double t0, double t1,
                           const SolveSettings& s, void* stream, std::string* err) {
@@ -1529,74 +1606,90 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
     ++launches_;
     return true;
   }
-  const int lt = s.precision == 1 ? 4 : 8;
-  Layout lay = make_layout(I->off, lt, s.hist_global == 0);
-  const int tab = tab_bytes_of(I->off, s.lu_mode);
-  int max_warps = (I->max_smem - tab) / lay.bytes;
-  if (max_warps < 1) {
-    *err = "mechanism too large for the shared-memory layout (" +
-           std::to_string(lay.bytes) + " bytes per cell)";
+  WarpLaunch w;
+  if (!plan_warp_launch(I->off, I->sm_count, I->max_smem, s, n_cells, I->sm_count * 64, &w, err))
     return false;
-  }
-  int warps = s.warps_per_block > 0 ? std::min(s.warps_per_block, max_warps) : max_warps;
-  warps = std::min(warps, 16);
-  int bps = std::max(1, s.blocks_per_sm);
-  while (bps > 1 && (size_t)bps * (tab + warps * lay.bytes) > (size_t)I->max_smem) --bps;
-  int grid = I->sm_count * bps;
-  // no more warps than cells
-  long total_warps = (long)grid * warps;
-  if (total_warps > n_cells) grid = std::max(1, (int)((n_cells + warps - 1) / warps));
-  total_warps = (long)grid * warps;
+  const long total_warps = (long)w.grid * w.warps;
   if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
-  if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)lt * I->m.n_jac * total_warps, err))
+  if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)w.lt * I->m.n_jac * total_warps, err))
     return false;
-  // history + rate constants per warp, rounded to 256-byte rows
-  const int hist_stride = s.hist_global ? ((LMAX * I->off.n + I->off.n_rxn) + 31) & ~31 : 0;
+  const int hist_stride = hist_stride_of(I->off, s);
   if (s.hist_global &&
       !ensure(&I->d_hist, &I->c_hist, sizeof(double) * (size_t)hist_stride * total_warps, err))
     return false;
   CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
   SolveArgs a;
-  a.m = I->m;
-  a.off = I->off;
-  a.blob = I->d_blob;
-  a.tab_bytes = tab;
-  a.stage_bytes = stage_bytes_of(I->off, s.lu_mode);
+  fill_args(&a, w, s, d_state, d_env, d_photo, d_order, n_cells, t0, t1);
   a.err = I->d_counter + 1;
-  a.lay = lay;
-  a.state = d_state;
-  a.env = d_env;
-  a.photo = I->m.n_photo > 0 ? d_photo : nullptr;
-  a.order = d_order;
-  a.n_cells = n_cells;
   a.counter = I->d_counter;
   a.stats = (CellStats*)I->d_stats;
   a.jscratch = I->d_jscratch;
   a.hist = (double*)I->d_hist;
   a.hist_stride = hist_stride;
-  a.t0 = t0;
-  a.t1 = t1;
-  a.rtol = s.rtol;
-  a.max_steps = s.max_steps;
-  a.maxncf = s.max_conv_fails;
-  a.maxnef = s.max_conv_fails;
-  a.lu_mode = s.lu_mode;
-  size_t smem = (size_t)tab + (size_t)warps * lay.bytes;
   CK(cudaEventRecord(I->ev0, st));
-  if (s.precision == 1) {
-    CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem));
-    solve_kernel<float><<<grid, warps * 32, smem, st>>>(a);
-  } else {
-    CK(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem));
-    solve_kernel<double><<<grid, warps * 32, smem, st>>>(a);
-  }
-  CK(cudaGetLastError());
+  if (!launch_warp_kernel(a, w, s.precision, st, err)) return false;
   CK(cudaEventRecord(I->ev1, st));
   I->ev_pending = true;
   ++launches_;
   return true;
+}
+
+size_t Engine::slot_scratch_bytes(const SolveSettings& s, int max_blocks) const {
+  const Impl* I = impl_;
+  WarpLaunch w;
+  std::string err;
+  if (!plan_warp_launch(I->off, I->sm_count, I->max_smem, s, 1 << 30, max_blocks, &w, &err))
+    return 0;
+  const size_t warps = (size_t)w.grid * w.warps;
+  const size_t j = ((size_t)w.lt * I->m.n_jac * warps + 255) & ~size_t(255);
+  const size_t h = sizeof(double) * (size_t)hist_stride_of(I->off, s) * warps;
+  return 256 + j + h;
+}
+
+bool Engine::launch_solve_slot(double* d_state, const double* d_env, const double* d_photo,
+                               CellStats* d_stats, int n_cells, double t0, double t1,
+                               const SolveSettings& s, char* scratch, size_t scratch_bytes,
+                               int max_blocks, void* stream, std::string* err) {
+  Impl* I = impl_;
+  if (n_cells <= 0) return true;
+  if (s.kernel != 0) {
+    *err = "serving slots run the warp-per-cell kernel only";
+    return false;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  WarpLaunch w;
+  if (!plan_warp_launch(I->off, I->sm_count, I->max_smem, s, n_cells, max_blocks, &w, err))
+    return false;
+  const size_t warps = (size_t)w.grid * w.warps;
+  const size_t jb = ((size_t)w.lt * I->m.n_jac * warps + 255) & ~size_t(255);
+  const int hist_stride = hist_stride_of(I->off, s);
+  if (256 + jb + sizeof(double) * (size_t)hist_stride * warps > scratch_bytes) {
+    *err = "slot scratch too small for this launch";
+    return false;
+  }
+  int* counter = (int*)scratch;
+  CK(cudaMemsetAsync(counter, 0, 2 * sizeof(int), st));
+  SolveArgs a;
+  fill_args(&a, w, s, d_state, d_env, d_photo, nullptr, n_cells, t0, t1);
+  a.err = counter + 1;
+  a.counter = counter;
+  a.stats = d_stats;
+  a.jscratch = scratch + 256;
+  a.hist = hist_stride ? (double*)(scratch + 256 + jb) : nullptr;
+  a.hist_stride = hist_stride;
+  if (!launch_warp_kernel(a, w, s.precision, st, err)) return false;
+  ++launches_;
+  return true;
+}
+
+int Engine::sm_count() const { return impl_->sm_count; }
+
+int Engine::max_cells_per_block(const SolveSettings& s) const {
+  const Impl* I = impl_;
+  if (s.kernel != 0) return 0;
+  const int lt = s.precision == 1 ? 4 : 8;
+  const Layout lay = make_layout(I->off, lt, s.hist_global == 0);
+  return std::min(16, std::max(0, (I->max_smem - tab_bytes_of(I->off, s.lu_mode)) / lay.bytes));
 }
 
 bool Engine::read_last_ms(void* stream) {

@@ -82,6 +82,24 @@ class Solver:
     def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 1) -> None:
         self.lib.camp_b200_set_launch(self._h, int(warps_per_block), int(blocks_per_sm))
 
+    def autotune(self, state, env, t_initial: float, t_final: float) -> dict:
+        """Times the candidate launch configurations on a sample of cells
+        (host arrays; state is not modified) and keeps the fastest."""
+        st = np.ascontiguousarray(state, np.float64)
+        ev = np.ascontiguousarray(env, np.float64).reshape(-1, 2)
+        n = st.shape[0]
+        if self.lib.camp_b200_autotune(self._h, st.reshape(-1), ev.reshape(-1), n,
+                                       float(t_initial), float(t_final)) != 0:
+            raise SolverError(_lib.last_error())
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        w, hg, lu, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        self.lib.camp_b200_get_tuning(self._h, C.byref(w), C.byref(hg), C.byref(lu),
+                                      C.byref(ms))
+        return {"warps_per_block": w.value, "hist_global": hg.value, "lu_mode": lu.value,
+                "sample_ms": ms.value}
+
     def set_layout(self, hist_global: int) -> None:
         """0: Nordsieck history and rate constants in shared memory; 1: in
         global memory (more resident cells per SM)."""
@@ -105,7 +123,12 @@ class Solver:
         """solver_run on host arrays; state [n_cells, n_state_var] in place."""
         if state.dtype != np.float64 or not state.flags.c_contiguous:
             raise TypeError("state must be a C-contiguous float64 array")
+        # solver_run advances every cell the solver was created for
+        if state.shape != (self.n_cells, self.mech.n_state_var):
+            raise ValueError(f"state must be [{self.n_cells}, {self.mech.n_state_var}]")
         env = np.ascontiguousarray(env, np.float64)
+        if env.size != 2 * self.n_cells:
+            raise ValueError(f"env must hold {self.n_cells} (T, P) pairs")
         return int(self.lib.solver_run(self._h, state.reshape(-1), env.reshape(-1),
                                        float(t_initial), float(t_final)))
 

@@ -162,6 +162,18 @@ int camp_b200_set_kernel(void *solver_data, int kernel, int place);
  * constants: 0 = shared memory (default), 1 = global memory (L1/L2 cached),
  * which leaves shared memory for more resident cells.  The autotuner picks. */
 int camp_b200_set_layout(void *solver_data, int hist_global);
+/* Autotuner: solves the given sample of cells (host buffers, state is not
+ * modified) once per candidate launch configuration -- cells per block, the
+ * history layout of camp_b200_set_layout and the LU mode of
+ * camp_b200_set_lu_mode -- for the current precision, and keeps the fastest
+ * by kernel time.  Use a sample representative of the cells to be solved
+ * (a few thousand cells, the host step of the run).  0 or -1. */
+int camp_b200_autotune(void *solver_data, const double *state, const double *env,
+                       int n_cells, double t_initial, double t_final);
+/* The launch configuration in use and the autotuner's sample time (ms, -1
+ * when not tuned). */
+int camp_b200_get_tuning(void *solver_data, int *warps_per_block, int *hist_global,
+                         int *lu_mode, double *sample_ms);
 /* Orders the cells of the next run by decreasing internal step count of the
  * previous run (longest-first scheduling of the persistent kernel). */
 int camp_b200_set_cost_ordering(void *solver_data, int enable);
@@ -232,6 +244,37 @@ int camp_b200_eval_deriv(void *solver_data, const double *state, const double *e
                          double *deriv);
 int camp_b200_eval_jac(void *solver_data, const double *state, const double *env,
                        int n_cells, double h, double *j_prod, double *j_loss);
+
+/* ---------------------------------------------------------------------- */
+/* Serving loop (continuous batching of column solves)                      */
+/* ---------------------------------------------------------------------- */
+
+/* A request is one column: n_cells cells of one mechanism (an initialised
+ * solver registered with the server) over one host step.  Requests are
+ * admitted in arrival order as soon as one of n_slots slots is free and their
+ * buffers fit the device and pinned-host budgets (MiB); admitted requests run
+ * concurrently on the GPU.  Each cell's result does not depend on what else
+ * runs. */
+void *camp_b200_server_new(int n_slots, double device_mb, double host_mb);
+/* Registers an initialised solver (its tables and current settings); returns
+ * the mechanism index, or -1.  Register every mechanism before submitting. */
+int camp_b200_server_add_solver(void *server, void *solver_data);
+/* Queues a request; state [n_cells*n_state_var], env [n_cells*2] and photo
+ * [n_cells*n_photo] (NULL without photolysis) are host arrays that must stay
+ * valid until camp_b200_server_wait returns, which writes the new state.
+ * Returns the request id (>= 0) or -1. */
+long camp_b200_server_submit(void *server, int mech, double *state,
+                             const double *env, const double *photo, int n_cells,
+                             double t_initial, double t_final);
+/* Blocks until the request is done; 0 = every cell succeeded, 1 = some cell
+ * failed (its state is left as submitted), -1 = error.  latency_ms (may be
+ * NULL) receives submit-to-completion time; stats (may be NULL) n_cells
+ * per-cell counters. */
+int camp_b200_server_wait(void *server, long request, double *latency_ms,
+                          camp_b200_cell_stats *stats, int n_cells);
+/* Requests submitted and not yet waited for. */
+int camp_b200_server_pending(void *server);
+void camp_b200_server_free(void *server);
 
 #ifdef __cplusplus
 }

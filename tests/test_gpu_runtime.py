@@ -1,0 +1,83 @@
+"""Runtime around the solve kernel on the GPU: the autotuner and the serving
+loop (continuous batching).  Both must leave every cell's result unchanged:
+a cell's integration does not depend on the launch configuration or on what
+else runs on the GPU."""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="no CUDA device")]
+
+RTOL = 1e-12  # same kernel, same cell: equal to round-off
+
+
+def _solver(mech, n, precision=1, max_steps=3000):
+    from camp_b200.solver import Solver
+
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4, max_steps=max_steps)
+    s.set_precision(precision)
+    return s
+
+
+def test_autotune_keeps_results(cb05):
+    from camp_b200.cells import make_cells
+
+    n = 400
+    cells = make_cells(cb05, n, 31)
+    s = _solver(cb05, n, max_steps=1500)
+    s.set_photo_rates(cells.photo_rates)
+    ref = cells.state.copy()
+    s.solve(ref, cells.env, 0.0, 60.0)
+    ref_status = s.cell_stats()["status"]
+    tuned = s.autotune(cells.state, cells.env, 0.0, 60.0)
+    assert 1 <= tuned["warps_per_block"] <= 16
+    assert tuned["hist_global"] in (0, 1) and tuned["lu_mode"] in (0, 1)
+    assert tuned["sample_ms"] > 0
+    out = cells.state.copy()
+    s.solve(out, cells.env, 0.0, 60.0)
+    np.testing.assert_array_equal(s.cell_stats()["status"], ref_status)
+    np.testing.assert_allclose(out, ref, rtol=RTOL, atol=0)
+
+
+def test_serving_mix_equals_alone(cb05, tmp_path):
+    """Columns of two mechanisms, 10-200 cells and host steps of 60/300/900 s
+    submitted back to back; each result equals the same column solved alone
+    through solver_run."""
+    from camp_b200.cells import make_cells, photo_base_rates
+    from camp_b200.serve import Server
+    from camp_b200.synth import load_synthetic
+
+    syn, syn_base = load_synthetic(str(tmp_path), 40, 100, 7)
+    mechs = [(cb05, photo_base_rates(cb05)), (syn, syn_base)]
+    solvers = [_solver(m, 200) for m, _ in mechs]
+    server = Server(n_slots=6, device_mb=512, host_mb=128)
+    ids = [server.add_solver(s) for s in solvers]
+    rng = np.random.Generator(np.random.PCG64(5))
+    reqs = []
+    for k in range(14):
+        mi = 0 if rng.uniform() < 0.7 else 1
+        n = int(rng.integers(10, 201))
+        dt = float(rng.choice([60.0, 300.0, 900.0]))
+        mech, base = mechs[mi]
+        c = make_cells(mech, n, 100 + k, photo_base=base)
+        st = c.state.copy()
+        rid = server.submit(ids[mi], st, c.env, c.photo_rates, 0.0, dt)
+        reqs.append((rid, mi, c, dt, st))
+    assert server.pending() == len(reqs)
+    lat = []
+    for rid, mi, c, dt, st in reqs:
+        rc, ms, out, stats = server.wait(rid)
+        lat.append(ms)
+        s = _solver(mechs[mi][0], c.n_cells)
+        s.set_photo_rates(c.photo_rates)
+        alone = c.state.copy()
+        rc_alone = s.solve(alone, c.env, 0.0, dt)
+        assert rc == rc_alone
+        np.testing.assert_array_equal(stats["status"], s.cell_stats()["status"])
+        np.testing.assert_allclose(out, alone, rtol=RTOL, atol=0)
+    assert server.pending() == 0
+    assert all(x > 0 for x in lat)
+    server.close()
