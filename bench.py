@@ -61,6 +61,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--max-steps", type=int, default=10000)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch the device step directly instead of as a CUDA graph")
+    ap.add_argument("--serve-rates", default="5,10,20,40",
+                    help="Poisson arrival rates (requests/s) of the serving sweep")
+    ap.add_argument("--serve-seconds", type=float, default=8.0)
     return ap.parse_args()
 
 
@@ -227,6 +233,91 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# Serving sweep
+# ---------------------------------------------------------------------------
+def serving_run(args, precision):
+    """Open-loop Poisson arrivals of column requests at each rate: 10-200
+    cells per column, 70 % cb05cl_ae5 and 30 % a 40-species / 100-reaction
+    synthetic gas-phase mechanism (standing in for the aerosol mechanism,
+    which this solver does not support), host steps of 60, 300 or 900 s.
+    Latency is submit-to-completion inside the library."""
+    import tempfile
+
+    from camp_b200.cells import make_cells, photo_base_rates
+    from camp_b200.mechanism import Mechanism
+    from camp_b200.serve import Server
+    from camp_b200.solver import Solver
+    from camp_b200.synth import load_synthetic
+
+    cb05 = Mechanism.load(MECH_FILE)
+    with tempfile.TemporaryDirectory() as td:
+        syn, syn_base = load_synthetic(td, 40, 100, 7)
+    mechs = [(cb05, photo_base_rates(cb05)), (syn, syn_base)]
+    solvers = []
+    for m, _ in mechs:
+        s = Solver(m, 200)
+        s.initialize(abs_tol=np.full(m.n_state_var, 1e-8), rel_tol=1e-4,
+                     max_steps=args.max_steps)
+        s.set_precision(precision)
+        solvers.append(s)
+    server = Server(n_slots=8, device_mb=4096, host_mb=1024)
+    ids = [server.add_solver(s) for s in solvers]
+    rng = np.random.Generator(np.random.PCG64(SEED + 1))
+    out = []
+    for rate in [float(x) for x in args.serve_rates.split(",")]:
+        arrivals = []
+        t = 0.0
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t > args.serve_seconds:
+                break
+            mi = 0 if rng.uniform() < 0.7 else 1
+            n = int(rng.integers(10, 201))
+            dt = float(rng.choice([60.0, 300.0, 900.0]))
+            c = make_cells(mechs[mi][0], n, int(rng.integers(1 << 30)), photo_base=mechs[mi][1])
+            arrivals.append((t, mi, c, dt))
+        results = []
+
+        def collect(q):
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                rid, n = item
+                rc, ms, _, _ = server.wait(rid)
+                results.append((ms, n, time.perf_counter()))
+
+        import queue
+
+        q = queue.Queue()
+        th = threading.Thread(target=collect, args=(q,), daemon=True)
+        th.start()
+        t0 = time.perf_counter()
+        for (ta, mi, c, dt) in arrivals:
+            delay = t0 + ta - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            rid = server.submit(ids[mi], c.state, c.env, c.photo_rates, 0.0, dt)
+            q.put((rid, c.n_cells))
+        q.put(None)
+        th.join()
+        lat = np.array([r[0] for r in results])
+        cells = sum(r[1] for r in results)
+        span = max(r[2] for r in results) - t0
+        out.append({"offered_rps": rate, "requests": len(results),
+                    "achieved_rps": len(results) / span, "cells_per_s": cells / span,
+                    "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99))})
+    server.close()
+    for s in solvers:
+        s.free()
+    return {"mix": "70% cb05cl_ae5 / 30% synthetic 40 species 100 reactions; 10-200 cells; "
+                   "host steps 60/300/900 s; Poisson arrivals",
+            "precision": "mixed" if precision == 1 else "fp64", "slots": 8,
+            "seconds_per_rate": args.serve_seconds, "rates": out}
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args):
@@ -254,6 +345,8 @@ def run_gpu_arm(args):
         s.initialize(abs_tol=atol, rel_tol=1e-4, max_steps=args.max_steps)
         s.set_precision(prec)
         s.set_photo_rates(cells.photo_rates)
+        # device step (counter reset + solve kernel) as one CUDA graph
+        s.set_graph(not args.no_graph)
         return s
 
     init_state = torch.from_numpy(cells.state).to(dev)
@@ -325,6 +418,9 @@ def run_gpu_arm(args):
         e2e = {"value": world * n * args.steps / te, "unit": "cell-steps/s",
                "h2d_bytes_per_step": int(8 * n * (mech.n_state_var + 2 + n_photo)),
                "d2h_bytes_per_step": int(8 * n * mech.n_state_var + 56 * n)}
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = serving_run(args, prec)
     if rank != 0:
         return
     cb = None
@@ -383,6 +479,7 @@ def run_gpu_arm(args):
                     "pipe 3.7 %), not by HBM",
         },
         "cpu_baseline": cb,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
     solver.free()

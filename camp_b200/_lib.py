@@ -43,7 +43,7 @@ EXPORTED = [
     "sub_model_add_condensed_data", "sub_model_update_data", "aero_phase_print_data",
     "aero_rep_print_data", "sub_model_print_data",
     "camp_b200_last_error", "camp_b200_is_ready", "camp_b200_set_precision",
-    "camp_b200_set_launch", "camp_b200_set_lu_mode", "camp_b200_set_kernel", "camp_b200_set_layout", "camp_b200_autotune", "camp_b200_get_tuning", "camp_b200_set_cost_ordering", "camp_b200_run_device",
+    "camp_b200_set_launch", "camp_b200_set_lu_mode", "camp_b200_set_kernel", "camp_b200_set_layout", "camp_b200_set_graph", "camp_b200_autotune", "camp_b200_get_tuning", "camp_b200_set_cost_ordering", "camp_b200_run_device",
     "camp_b200_launch_device", "camp_b200_sync_status", "camp_b200_run_device_noalloc", "camp_b200_n_photo",
     "camp_b200_set_photo_rates", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
@@ -94,6 +94,8 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_get_tuning.restype = ip
     lib.camp_b200_get_tuning.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    lib.camp_b200_set_graph.restype = ip
+    lib.camp_b200_set_graph.argtypes = [vp, ip]
     lib.camp_b200_set_layout.restype = ip
     lib.camp_b200_set_layout.argtypes = [vp, ip]
     lib.camp_b200_set_kernel.restype = ip

@@ -441,6 +441,11 @@ int camp_b200_set_lu_mode(void* solver_data, int mode) {
   return 0;
 }
 
+int camp_b200_set_graph(void* solver_data, int enable) {
+  S(solver_data)->settings.use_graph = enable ? 1 : 0;
+  return 0;
+}
+
 int camp_b200_set_layout(void* solver_data, int hist_global) {
   if (hist_global != 0 && hist_global != 1) {
     set_error("camp_b200_set_layout: hist_global must be 0 or 1");

@@ -28,6 +28,7 @@ struct SolveSettings {
   int lu_mode = 0;         // 0 = level schedule over the warp, 1 = one lane
   int kernel = 0;          // 0 = warp per cell, 1 = lane per cell
   int lane_place = 7;      // lane kernel: bit0 y, bit1 LU, bit2 z in shared memory
+  int use_graph = 0;       // warp kernel: launch the device step as a CUDA graph
   int hist_global = 0;     // warp kernel: Nordsieck history + rate constants in
                            // global memory (1) or shared memory (0)
 };
@@ -72,10 +73,11 @@ class Engine {
   int max_cells_per_block(const SolveSettings& s) const;
   // Serving slots: a launch on caller-provided buffers and scratch (from
   // slot_scratch_bytes for at most max_blocks blocks), so several launches
-  // can be in flight on different streams.  No allocation, no sync.
+  // can be in flight on different streams; d_tspan holds each cell's
+  // (t0, t1).  No allocation, no sync.
   size_t slot_scratch_bytes(const SolveSettings& s, int max_blocks) const;
   bool launch_solve_slot(double* d_state, const double* d_env, const double* d_photo,
-                         CellStats* d_stats, int n_cells, double t0, double t1,
+                         CellStats* d_stats, const double* d_tspan, int n_cells,
                          const SolveSettings& s, char* scratch, size_t scratch_bytes,
                          int max_blocks, void* stream, std::string* err);
   int sm_count() const;
@@ -85,6 +87,8 @@ class Engine {
 
  private:
   bool ensure(void** p, size_t* cap, size_t bytes, std::string* err);
+  bool launch_graph(struct SolveArgs& a, const struct WarpLaunch& w, int precision,
+                    void* stream, std::string* err);
   void fill_args(struct SolveArgs* a, const struct WarpLaunch& w, const SolveSettings& s,
                  double* d_state, const double* d_env, const double* d_photo,
                  const int* d_order, int n_cells, double t0, double t1) const;

@@ -2,19 +2,24 @@
 // submitted as they arrive and solved with continuous batching.
 //
 // A request is one column (a set of cells) of one mechanism over one host
-// time step.  A dispatcher thread admits queued requests in arrival order as
-// soon as a slot (a CUDA stream with its own kernel scratch) is free and the
-// request's buffers fit the device and pinned-host budgets; admitted requests
-// run concurrently, each kernel spreading over as many SMs as its cells fill,
-// so a request that arrives while others are on the GPU starts on the SMs
-// they leave free.  Completion is detected per request with an event; the
-// results are copied back into the caller's arrays and the memory returned to
-// the budgets.  Each cell's integration is independent of which request,
-// slot or SM runs it, so a result is the same alone and in the mix.
+// time step.  A dispatcher thread turns the queue into batches: whenever a
+// slot (a CUDA stream with its own kernel scratch) is free, the oldest
+// request and every later queued request of the same mechanism that fits the
+// device and pinned-host budgets are merged into one launch whose cells each
+// carry their own (t0, t1).  The persistent kernel's warps take the cells of
+// all merged requests from one counter, so a long (stiff) cell of one request
+// does not leave the warps of that launch idle while other requests wait;
+// batches on different slots run concurrently, the next one filling the SMs
+// the previous one's tail leaves free.  Completion is detected per batch with
+// an event; results are copied back into the callers' arrays and memory is
+// returned to the budgets.  Each cell's integration is independent of which
+// request, batch, slot or SM runs it, so a result is the same alone and in
+// the mix.
 #include <cuda_runtime.h>
 
 #include <chrono>
 #include <condition_variable>
+#include <algorithm>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -46,13 +51,23 @@ struct Server::Req {
   int n = 0;
   double t0 = 0, t1 = 0;
   double t_submit = 0, t_start = 0, t_done = 0;
-  int slot = -1;
-  char *d_buf = nullptr, *h_buf = nullptr;
-  size_t off_env = 0, off_photo = 0, off_stats = 0, off_flag = 0;
   bool done = false;
   int rc = 0;  // 0 every cell ok, 1 some cell failed, -1 error
   std::string err;
   std::vector<CellStats> stats;
+};
+
+// Requests of one mechanism merged into one launch: their cells are laid out
+// back to back (same offsets on the device and in pinned host memory), each
+// with its own (t0, t1), so the kernel's warps share the cells of every
+// request in the batch.
+struct Server::Batch {
+  int mech = 0;
+  std::vector<long> reqs;
+  std::vector<int> first;  // first cell of each request
+  int n = 0;
+  char *d_buf = nullptr, *h_buf = nullptr;
+  size_t off_env = 0, off_photo = 0, off_tspan = 0, off_stats = 0, off_flag = 0, bytes = 0;
 };
 
 struct Server::Slot {
@@ -60,7 +75,7 @@ struct Server::Slot {
   cudaEvent_t done = nullptr;
   char* scratch = nullptr;
   size_t scratch_bytes = 0;
-  long req = -1;
+  std::unique_ptr<Batch> batch;
 };
 
 Server::Server() {}
@@ -162,26 +177,24 @@ long Server::submit(int mech, double* state, const double* env, const double* ph
   r->t0 = t0;
   r->t1 = t1;
   r->t_submit = now_s();
-  // buffer layout (same offsets on the device and in pinned host memory)
-  size_t off = align256(sizeof(double) * (size_t)n * m.n_state);
-  r->off_env = off;
-  off += align256(sizeof(double) * 2 * (size_t)n);
-  r->off_photo = off;
-  off += align256(sizeof(double) * (size_t)n * m.n_photo);
-  r->off_stats = off;
-  off += align256(sizeof(CellStats) * (size_t)n);
-  r->off_flag = off;  // the kernel's error flag, read back into pinned memory
-  off += 256;
-  if (off > device_bytes_ || off > host_bytes_) {
+  if (batch_bytes(m, n) > device_bytes_ || batch_bytes(m, n) > host_bytes_) {
     *err = "request larger than the memory budget";
     return -1;
   }
-  bytes_[r->id] = off;
   const long id = r->id;
   queue_.push_back(id);
   requests_[id] = std::move(r);
   cv_.notify_all();
   return id;
+}
+
+size_t Server::batch_bytes(const Mech& m, int n) const {
+  size_t off = align256(sizeof(double) * (size_t)n * m.n_state);
+  off += align256(sizeof(double) * 2 * (size_t)n);                // env
+  off += align256(sizeof(double) * (size_t)n * m.n_photo);        // photolysis
+  off += align256(sizeof(double) * 2 * (size_t)n);                // (t0, t1)
+  off += align256(sizeof(CellStats) * (size_t)n);                 // stats
+  return off + 256;                                               // error flag
 }
 
 void Server::loop() {
@@ -190,40 +203,66 @@ void Server::loop() {
   while (!stop_) {
     bool progress = false;
     // completions
-    for (size_t k = 0; k < slots_.size(); ++k) {
-      Slot& s = slots_[k];
-      if (s.req < 0) continue;
+    for (auto& s : slots_) {
+      if (!s.batch) continue;
       if (cudaEventQuery(s.done) != cudaSuccess) continue;
-      finish(*requests_[s.req]);
-      s.req = -1;
+      finish(*s.batch);
+      s.batch.reset();
       progress = true;
     }
-    // admissions in arrival order; the head waits until it fits
+    // admissions: the oldest request and every later queued request of its
+    // mechanism (up to max_batch_cells_) form the next batch
     while (!queue_.empty()) {
       int free_slot = -1;
       for (size_t k = 0; k < slots_.size(); ++k)
-        if (slots_[k].req < 0) {
+        if (!slots_[k].batch) {
           free_slot = (int)k;
           break;
         }
       if (free_slot < 0) break;
-      Req& r = *requests_[queue_.front()];
-      const size_t bytes = bytes_[r.id];
-      char* d = dev_.alloc(bytes);
-      char* h = d ? host_.alloc(bytes) : nullptr;
-      if (!d || !h) {
-        dev_.release(d);
-        break;
+      const int mech = requests_[queue_.front()]->mech;
+      std::vector<long> take;
+      int cells = 0;
+      for (long id : queue_) {
+        const Req& r = *requests_[id];
+        if (r.mech != mech) continue;
+        if (!take.empty() && cells + r.n > max_batch_cells_) break;
+        take.push_back(id);
+        cells += r.n;
       }
-      queue_.pop_front();
-      r.d_buf = d;
-      r.h_buf = h;
-      start(r, free_slot);
+      // shrink the batch until its buffers fit what the budgets have free
+      char *d = nullptr, *h = nullptr;
+      size_t bytes = 0;
+      while (!take.empty()) {
+        bytes = batch_bytes(mechs_[mech], cells);
+        d = dev_.alloc(bytes);
+        h = d ? host_.alloc(bytes) : nullptr;
+        if (d && h) break;
+        dev_.release(d);
+        d = nullptr;
+        if (take.size() == 1) {
+          take.clear();
+          break;
+        }
+        const size_t keep = take.size() / 2;
+        for (size_t k = keep; k < take.size(); ++k) cells -= requests_[take[k]]->n;
+        take.resize(keep);
+      }
+      if (take.empty()) break;  // the head waits until memory frees up
+      auto b = std::make_unique<Batch>();
+      b->mech = mech;
+      b->reqs = take;
+      b->n = cells;
+      b->d_buf = d;
+      b->h_buf = h;
+      b->bytes = bytes;
+      for (long id : take) queue_.erase(std::find(queue_.begin(), queue_.end(), id));
+      start(std::move(b), free_slot);
       progress = true;
     }
     if (progress) cv_.notify_all();
     bool busy = false;
-    for (auto& s : slots_) busy |= s.req >= 0;
+    for (auto& s : slots_) busy |= (bool)s.batch;
     if (busy)
       cv_.wait_for(lk, std::chrono::microseconds(50));
     else
@@ -231,61 +270,88 @@ void Server::loop() {
   }
 }
 
-void Server::start(Req& r, int slot) {
+void Server::start(std::unique_ptr<Batch> bp, int slot) {
   Slot& s = slots_[slot];
-  const Mech& m = mechs_[r.mech];
-  r.slot = slot;
-  r.t_start = now_s();
-  const size_t sb = sizeof(double) * (size_t)r.n * m.n_state;
-  std::memcpy(r.h_buf, r.state, sb);
-  std::memcpy(r.h_buf + r.off_env, r.env, sizeof(double) * 2 * (size_t)r.n);
-  if (m.n_photo > 0)
-    std::memcpy(r.h_buf + r.off_photo, r.photo, sizeof(double) * (size_t)r.n * m.n_photo);
-  const size_t in_bytes = r.off_stats;
+  Batch& b = *bp;
+  const Mech& m = mechs_[b.mech];
+  const int n = b.n;
+  const size_t sb = align256(sizeof(double) * (size_t)n * m.n_state);
+  b.off_env = sb;
+  b.off_photo = b.off_env + align256(sizeof(double) * 2 * (size_t)n);
+  b.off_tspan = b.off_photo + align256(sizeof(double) * (size_t)n * m.n_photo);
+  b.off_stats = b.off_tspan + align256(sizeof(double) * 2 * (size_t)n);
+  b.off_flag = b.off_stats + align256(sizeof(CellStats) * (size_t)n);
+  const double now = now_s();
+  int c0 = 0;
+  for (long id : b.reqs) {
+    Req& r = *requests_[id];
+    r.t_start = now;
+    b.first.push_back(c0);
+    std::memcpy(b.h_buf + sizeof(double) * (size_t)c0 * m.n_state, r.state,
+                sizeof(double) * (size_t)r.n * m.n_state);
+    std::memcpy(b.h_buf + b.off_env + sizeof(double) * 2 * (size_t)c0, r.env,
+                sizeof(double) * 2 * (size_t)r.n);
+    if (m.n_photo > 0)
+      std::memcpy(b.h_buf + b.off_photo + sizeof(double) * (size_t)c0 * m.n_photo, r.photo,
+                  sizeof(double) * (size_t)r.n * m.n_photo);
+    double* ts = (double*)(b.h_buf + b.off_tspan) + 2 * (size_t)c0;
+    for (int c = 0; c < r.n; ++c) {
+      ts[2 * c] = r.t0;
+      ts[2 * c + 1] = r.t1;
+    }
+    c0 += r.n;
+  }
   std::string err;
-  bool ok = cudaMemcpyAsync(r.d_buf, r.h_buf, in_bytes, cudaMemcpyHostToDevice, s.stream) ==
+  bool ok = cudaMemcpyAsync(b.d_buf, b.h_buf, b.off_stats, cudaMemcpyHostToDevice, s.stream) ==
             cudaSuccess;
   ok = ok && m.engine->launch_solve_slot(
-                 (double*)r.d_buf, (const double*)(r.d_buf + r.off_env),
-                 (const double*)(r.d_buf + r.off_photo), (CellStats*)(r.d_buf + r.off_stats),
-                 r.n, r.t0, r.t1, m.settings, s.scratch, s.scratch_bytes,
-                 m.engine->sm_count(), s.stream, &err);
-  ok = ok && cudaMemcpyAsync(r.h_buf, r.d_buf, sb, cudaMemcpyDeviceToHost, s.stream) ==
-                 cudaSuccess;
-  ok = ok && cudaMemcpyAsync(r.h_buf + r.off_stats, r.d_buf + r.off_stats,
-                             sizeof(CellStats) * (size_t)r.n, cudaMemcpyDeviceToHost,
+                 (double*)b.d_buf, (const double*)(b.d_buf + b.off_env),
+                 (const double*)(b.d_buf + b.off_photo), (CellStats*)(b.d_buf + b.off_stats),
+                 (const double*)(b.d_buf + b.off_tspan), n, m.settings, s.scratch,
+                 s.scratch_bytes, m.engine->sm_count(), s.stream, &err);
+  ok = ok && cudaMemcpyAsync(b.h_buf, b.d_buf, sizeof(double) * (size_t)n * m.n_state,
+                             cudaMemcpyDeviceToHost, s.stream) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(b.h_buf + b.off_stats, b.d_buf + b.off_stats,
+                             sizeof(CellStats) * (size_t)n, cudaMemcpyDeviceToHost,
                              s.stream) == cudaSuccess;
-  ok = ok && cudaMemcpyAsync(r.h_buf + r.off_flag, s.scratch + sizeof(int), sizeof(int),
+  ok = ok && cudaMemcpyAsync(b.h_buf + b.off_flag, s.scratch + sizeof(int), sizeof(int),
                              cudaMemcpyDeviceToHost, s.stream) == cudaSuccess;
   if (!ok && err.empty()) err = "copy failed";
   cudaEventRecord(s.done, s.stream);
-  s.req = r.id;
-  if (!ok) {
-    r.rc = -1;
-    r.err = err;
-  }
+  if (!ok)
+    for (long id : b.reqs) {
+      requests_[id]->rc = -1;
+      requests_[id]->err = err;
+    }
+  s.batch = std::move(bp);
 }
 
-void Server::finish(Req& r) {
-  const Mech& m = mechs_[r.mech];
+void Server::finish(Batch& b) {
+  const Mech& m = mechs_[b.mech];
   int flag = 0;
-  std::memcpy(&flag, r.h_buf + r.off_flag, sizeof(int));
-  if (r.rc == 0 && flag) {
-    r.rc = -1;
-    r.err = "solve kernel: the table stage into shared memory did not complete";
+  std::memcpy(&flag, b.h_buf + b.off_flag, sizeof(int));
+  const double now = now_s();
+  for (size_t k = 0; k < b.reqs.size(); ++k) {
+    Req& r = *requests_[b.reqs[k]];
+    const int c0 = b.first[k];
+    if (r.rc == 0 && flag) {
+      r.rc = -1;
+      r.err = "solve kernel: the table stage into shared memory did not complete";
+    }
+    if (r.rc == 0) {
+      r.stats.resize(r.n);
+      std::memcpy(r.stats.data(), b.h_buf + b.off_stats + sizeof(CellStats) * (size_t)c0,
+                  sizeof(CellStats) * (size_t)r.n);
+      std::memcpy(r.state, b.h_buf + sizeof(double) * (size_t)c0 * m.n_state,
+                  sizeof(double) * (size_t)r.n * m.n_state);
+      for (const auto& c : r.stats)
+        if (c.status != 0) r.rc = 1;
+    }
+    r.t_done = now;
+    r.done = true;
   }
-  if (r.rc == 0) {
-    r.stats.resize(r.n);
-    std::memcpy(r.stats.data(), r.h_buf + r.off_stats, sizeof(CellStats) * (size_t)r.n);
-    std::memcpy(r.state, r.h_buf, sizeof(double) * (size_t)r.n * m.n_state);
-    for (const auto& c : r.stats)
-      if (c.status != 0) r.rc = 1;
-  }
-  dev_.release(r.d_buf);
-  host_.release(r.h_buf);
-  r.d_buf = r.h_buf = nullptr;
-  r.t_done = now_s();
-  r.done = true;
+  dev_.release(b.d_buf);
+  host_.release(b.h_buf);
 }
 
 int Server::wait(long id, double* latency_ms, std::vector<CellStats>* stats, std::string* err) {
@@ -302,7 +368,6 @@ int Server::wait(long id, double* latency_ms, std::vector<CellStats>* stats, std
   const int rc = r.rc;
   if (rc < 0) *err = r.err;
   requests_.erase(it);
-  bytes_.erase(id);
   return rc;
 }
 

@@ -84,6 +84,7 @@ class Server {
 
  private:
   struct Req;
+  struct Batch;
   struct Slot;
   struct Mech {
     Engine* engine;
@@ -91,8 +92,9 @@ class Server {
     int n_state, n_photo;
   };
   void loop();
-  void start(Req& r, int slot);
-  void finish(Req& r);
+  size_t batch_bytes(const Mech& m, int n) const;
+  void start(std::unique_ptr<Batch> b, int slot);
+  void finish(Batch& b);
 
   int device_ = 0;
   void* d_base_ = nullptr;
@@ -102,7 +104,7 @@ class Server {
   std::vector<Mech> mechs_;
   std::vector<Slot> slots_;
   std::map<long, std::unique_ptr<Req>> requests_;
-  std::map<long, size_t> bytes_;
+  int max_batch_cells_ = 16384;
   std::deque<long> queue_;
   long next_id_ = 0;
   bool stop_ = false;

@@ -88,6 +88,7 @@ struct SolveArgs {
   void* jscratch;  // per-warp saved Jacobian slots
   double* hist;    // per-warp Nordsieck history zn[LMAX][n] + rate constants
   int hist_stride; // doubles per warp in hist
+  const double* tspan = nullptr;  // per-cell (t0, t1); null: t0, t1 for all
   double t0, t1, rtol;
   int max_steps, maxncf, maxnef;
   int lu_mode;
@@ -1225,7 +1226,9 @@ __global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
     const double T = a.env[2 * (size_t)cell], P = a.env[2 * (size_t)cell + 1];
     compute_keff(m, st, T, P, a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr,
                  c.keff, lane);
-    int flag = c.integrate(a.t0, a.t1);
+    const double t0 = a.tspan ? a.tspan[2 * (size_t)cell] : a.t0;
+    const double t1 = a.tspan ? a.tspan[2 * (size_t)cell + 1] : a.t1;
+    int flag = c.integrate(t0, t1);
     if (flag == OK)
       #pragma unroll 1
       for (int i = lane; i < c.n; i += 32) st[dep_state[i]] = c.y[i] > 0.0 ? c.y[i] : 0.0;
@@ -1339,6 +1342,13 @@ struct Engine::Impl {
   size_t c_hist = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool ev_pending = false;
+  // the device step (counter reset + solve kernel) as an instantiated graph;
+  // its kernel node's launch shape and arguments are updated per launch
+  cudaGraph_t graph = nullptr;  // kept: its node handles address the exec's nodes
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraphNode_t gkernel = nullptr;
+  int gprecision = -1, ggrid = 0, gblock = 0;
+  size_t gsmem = 0;
 };
 
 Engine::Engine() : impl_(new Impl) {}
@@ -1360,6 +1370,8 @@ Engine::~Engine() {
   cudaFree(I->d_hist);
   if (I->ev0) cudaEventDestroy(I->ev0);
   if (I->ev1) cudaEventDestroy(I->ev1);
+  if (I->gexec) cudaGraphExecDestroy(I->gexec);
+  if (I->graph) cudaGraphDestroy(I->graph);
   delete I;
 }
 
@@ -1617,7 +1629,6 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   if (s.hist_global &&
       !ensure(&I->d_hist, &I->c_hist, sizeof(double) * (size_t)hist_stride * total_warps, err))
     return false;
-  CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
   SolveArgs a;
   fill_args(&a, w, s, d_state, d_env, d_photo, d_order, n_cells, t0, t1);
   a.err = I->d_counter + 1;
@@ -1627,10 +1638,66 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   a.hist = (double*)I->d_hist;
   a.hist_stride = hist_stride;
   CK(cudaEventRecord(I->ev0, st));
-  if (!launch_warp_kernel(a, w, s.precision, st, err)) return false;
+  if (s.use_graph) {
+    if (!launch_graph(a, w, s.precision, st, err)) return false;
+  } else {
+    CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
+    if (!launch_warp_kernel(a, w, s.precision, st, err)) return false;
+  }
   CK(cudaEventRecord(I->ev1, st));
   I->ev_pending = true;
   ++launches_;
+  return true;
+}
+
+bool Engine::launch_graph(SolveArgs& a, const WarpLaunch& w, int precision, void* stream,
+                          std::string* err) {
+  Impl* I = impl_;
+  cudaStream_t st = (cudaStream_t)stream;
+  void* func = precision == 1 ? (void*)solve_kernel<float> : (void*)solve_kernel<double>;
+  CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.smem));
+  void* args[] = {&a};
+  cudaKernelNodeParams kp{};
+  kp.func = func;
+  kp.gridDim = dim3(w.grid);
+  kp.blockDim = dim3(w.warps * 32);
+  kp.sharedMemBytes = (unsigned)w.smem;
+  kp.kernelParams = args;
+  // an instantiated kernel node takes new arguments but keeps its launch
+  // shape: a new shape (fewer cells than resident warps, other settings)
+  // instantiates the graph again
+  if (!I->gexec || I->gprecision != precision || I->ggrid != w.grid ||
+      I->gblock != w.warps * 32 || I->gsmem != w.smem) {
+    if (I->gexec) cudaGraphExecDestroy(I->gexec);
+    if (I->graph) cudaGraphDestroy(I->graph);
+    I->gexec = nullptr;
+    I->graph = nullptr;
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    I->graph = g;
+    cudaMemsetParams mp{};
+    mp.dst = I->d_counter;
+    mp.value = 0;
+    mp.elementSize = sizeof(int);
+    mp.width = 1;
+    mp.height = 1;
+    cudaGraphNode_t mset = nullptr;
+    cudaError_t e = cudaGraphAddMemsetNode(&mset, g, nullptr, 0, &mp);
+    if (e == cudaSuccess) e = cudaGraphAddKernelNode(&I->gkernel, g, &mset, 1, &kp);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&I->gexec, g, 0);
+    if (e != cudaSuccess) {
+      *err = std::string("solve graph: ") + cudaGetErrorString(e);
+      I->gexec = nullptr;
+      return false;
+    }
+    I->gprecision = precision;
+    I->ggrid = w.grid;
+    I->gblock = w.warps * 32;
+    I->gsmem = w.smem;
+  } else {
+    CK(cudaGraphExecKernelNodeSetParams(I->gexec, I->gkernel, &kp));
+  }
+  CK(cudaGraphLaunch(I->gexec, st));
   return true;
 }
 
@@ -1647,7 +1714,7 @@ size_t Engine::slot_scratch_bytes(const SolveSettings& s, int max_blocks) const 
 }
 
 bool Engine::launch_solve_slot(double* d_state, const double* d_env, const double* d_photo,
-                               CellStats* d_stats, int n_cells, double t0, double t1,
+                               CellStats* d_stats, const double* d_tspan, int n_cells,
                                const SolveSettings& s, char* scratch, size_t scratch_bytes,
                                int max_blocks, void* stream, std::string* err) {
   Impl* I = impl_;
@@ -1670,7 +1737,8 @@ bool Engine::launch_solve_slot(double* d_state, const double* d_env, const doubl
   int* counter = (int*)scratch;
   CK(cudaMemsetAsync(counter, 0, 2 * sizeof(int), st));
   SolveArgs a;
-  fill_args(&a, w, s, d_state, d_env, d_photo, nullptr, n_cells, t0, t1);
+  fill_args(&a, w, s, d_state, d_env, d_photo, nullptr, n_cells, 0.0, 0.0);
+  a.tspan = d_tspan;
   a.err = counter + 1;
   a.counter = counter;
   a.stats = d_stats;

@@ -100,6 +100,10 @@ class Solver:
         return {"warps_per_block": w.value, "hist_global": hg.value, "lu_mode": lu.value,
                 "sample_ms": ms.value}
 
+    def set_graph(self, enable: bool) -> None:
+        """Launch each run's device step as one CUDA graph."""
+        self.lib.camp_b200_set_graph(self._h, int(bool(enable)))
+
     def set_layout(self, hist_global: int) -> None:
         """0: Nordsieck history and rate constants in shared memory; 1: in
         global memory (more resident cells per SM)."""

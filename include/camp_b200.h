@@ -158,6 +158,11 @@ int camp_b200_set_lu_mode(void *solver_data, int mode);
  * bit 2 the solve vector in shared memory; the rest of a cell's working set
  * lives in a lane-interleaved global scratch.  -1 keeps the current value. */
 int camp_b200_set_kernel(void *solver_data, int kernel, int place);
+/* 1: the device step of each run (cell-counter reset + solve kernel) is
+ * launched as one instantiated CUDA graph whose kernel node is updated with
+ * the run's arguments, instead of as separate launches.  Results are the
+ * same either way.  Default 0. */
+int camp_b200_set_graph(void *solver_data, int enable);
 /* Where the warp-per-cell kernel keeps each cell's Nordsieck history and rate
  * constants: 0 = shared memory (default), 1 = global memory (L1/L2 cached),
  * which leaves shared memory for more resident cells.  The autotuner picks. */
@@ -250,11 +255,12 @@ int camp_b200_eval_jac(void *solver_data, const double *state, const double *env
 /* ---------------------------------------------------------------------- */
 
 /* A request is one column: n_cells cells of one mechanism (an initialised
- * solver registered with the server) over one host step.  Requests are
- * admitted in arrival order as soon as one of n_slots slots is free and their
- * buffers fit the device and pinned-host budgets (MiB); admitted requests run
- * concurrently on the GPU.  Each cell's result does not depend on what else
- * runs. */
+ * solver registered with the server) over its own host step.  Whenever one of
+ * n_slots slots is free, the oldest queued request and the later queued
+ * requests of the same mechanism that fit the device and pinned-host budgets
+ * (MiB) are merged into one launch whose warps share all their cells;
+ * launches on different slots run concurrently.  Each cell's result does not
+ * depend on what else runs. */
 void *camp_b200_server_new(int n_slots, double device_mb, double host_mb);
 /* Registers an initialised solver (its tables and current settings); returns
  * the mechanism index, or -1.  Register every mechanism before submitting. */

@@ -81,3 +81,31 @@ def test_serving_mix_equals_alone(cb05, tmp_path):
     assert server.pending() == 0
     assert all(x > 0 for x in lat)
     server.close()
+
+
+def test_graph_launch_keeps_results(cb05):
+    """The device step launched as a CUDA graph (updated per run) gives the
+    results of the plain launches, over runs with changing arguments."""
+    import torch
+
+    from camp_b200.cells import make_cells
+
+    n = 256
+    cells = make_cells(cb05, n, 41)
+    dev = torch.device("cuda", 0)
+    env = torch.from_numpy(cells.env).to(dev)
+    outs = []
+    for graph in (False, True):
+        s = _solver(cb05, n, max_steps=1500)
+        s.set_photo_rates(cells.photo_rates)
+        s.set_graph(graph)
+        st = torch.from_numpy(cells.state).to(dev)
+        res = []
+        # same launch shape with new arguments (node update), then other shapes
+        for dt in (60.0, 120.0, 300.0, 60.0):
+            s.run_device(st, env, n if dt != 300.0 else n // 2, 0.0, dt)
+            res.append((st.cpu().numpy().copy(), s.cell_stats(n // 2)["status"].copy()))
+        outs.append(res)
+    for (a, sa), (b, sb) in zip(*outs):
+        np.testing.assert_array_equal(sa, sb)
+        np.testing.assert_allclose(b, a, rtol=RTOL, atol=0)
