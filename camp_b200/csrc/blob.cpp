@@ -149,6 +149,15 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     jg_lupos[e] = (uint16_t)t.jg_lupos[e];
     jg_row[e] = (uint16_t)t.jg_row[e];
   }
+  // per LU position: the solver-J slot that fills it (+1, 0 = none) and, in
+  // bit 15, whether it is a diagonal (M = I - gamma*J in one pass)
+  if (t.n_jac >= 32767) {
+    *err = "too many Jacobian elements for the table encoding";
+    return false;
+  }
+  std::vector<uint16_t> lu_src(t.n_lu, 0);
+  for (int e = 0; e < t.n_jac; ++e) lu_src[t.jg_lupos[e]] = (uint16_t)(e + 1);
+  for (int i = 0; i < n; ++i) lu_src[t.lu_diag[i]] |= 0x8000u;
   std::vector<long> jw(t.n_jac);
   for (int e = 0; e < t.n_jac; ++e) jw[e] = 2 + (t.jg_ptr[e + 1] - t.jg_ptr[e]);
   auto jlanes = lpt(jw);
@@ -224,6 +233,7 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.n_plev = t.n_plev;
   o.lu_perm = w.put(u16(t.lu_perm));
   o.lu_diag = w.put(u16(t.lu_diag));
+  o.lu_src = w.put(lu_src);
   o.fa_ptr = w.put(u16(t.fa_ptr));
   o.fa = w.put(fa);
   o.fb_lane = w.put(gfb.lane);

@@ -34,7 +34,7 @@ struct BlobOff {
   // phase (bw).  A grouped phase G has lane pointers (uint16, 33 per level),
   // units (uint32 target | count<<16, uint32 first pair | (pivot+1)<<16,
   // pivot 0 = none) and pairs (uint32 a | b<<16).
-  int lu_perm, lu_diag;
+  int lu_perm, lu_diag, lu_src;
   int fa_ptr, fa;
   int fb_lane, fb_unit, fb_pair;
   int fw_lane, fw_unit, fw_pair;

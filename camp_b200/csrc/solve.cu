@@ -66,6 +66,10 @@ constexpr int DO_ERROR_TEST = 100, PREDICT_AGAIN = 101, TRY_AGAIN = 102;
 // ---------------------------------------------------------------------------
 // Device tables
 // ---------------------------------------------------------------------------
+// Cells (warps) per block of the solve kernel: its launch bound leaves 168
+// registers per thread, enough to keep the BDF state without spilling.
+constexpr int kMaxCellsPerBlock = 12;
+
 struct Layout {  // per-warp shared-memory slice (byte offsets; -1 = not in it)
   int zn, ewt, acor, y, ftemp, tempv, rates, keff, fscr, lu, z, dinv, ctl, bytes;
 };
@@ -136,7 +140,7 @@ struct Tab {
   const uint16_t *fg_unit, *fg_lane, *fg_split;
   const uint32_t* jg_w0;
   const uint16_t *jg_w1, *jg_ptr, *jg_lupos, *jg_row, *jg_lane, *jg_slots;
-  const uint16_t *lu_perm, *lu_diag, *fa_ptr;
+  const uint16_t *lu_perm, *lu_diag, *lu_src, *fa_ptr;
   const uint32_t* fa;
   const uint16_t* fb_lane;
   const uint32_t *fb_unit, *fb_pair;
@@ -170,6 +174,7 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.jg_slots = (const uint16_t*)(b + o.jg_slots);
   t.lu_perm = (const uint16_t*)(b + o.lu_perm);
   t.lu_diag = (const uint16_t*)(b + o.lu_diag);
+  t.lu_src = (const uint16_t*)(b + o.lu_src);
   t.fa_ptr = (const uint16_t*)(b + o.fa_ptr);
   t.fa = (const uint32_t*)(b + o.fa);
   t.fb_lane = (const uint16_t*)(b + o.fb_lane);
@@ -333,6 +338,23 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
 // Solver Jacobian values into Jout (indexed by CSC entry; each lane writes the
 // entries of its balanced slot list); production and loss parts into jp/jl
 // when given (src/rxns/rxn_arrhenius.c:178-212).
+// One entry of a solver-Jacobian slot: a loss partial (independent species
+// index 0) adds to L; a product partial times its yield adds to P when the
+// negative-yield guard lets the product term apply (src/rxns/rxn_arrhenius.c
+// :201-207).
+__device__ __forceinline__ void jac_term(const Tab& t, const double* part, const double* y,
+                                         double yrow, double h, int g, double* P, double* L) {
+  const uint32_t w0 = t.jg_w0[g];
+  const int ind1 = t.jg_w1[g];
+  const double p = part[w0 & 0xFFFFu];
+  const double c = t.coef[w0 >> 16];
+  const double yi = state_of(y[ind1 > 0 ? ind1 - 1 : 0]);
+  const bool prod = ind1 != 0;
+  const bool apply = -p * yi * c * h <= yrow;
+  *P += (prod && apply) ? c * p : 0.0;
+  *L += prod ? 0.0 : p;
+}
+
 template <typename JT>
 __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
                                     const double* keff, double* part, JT* Jout, int lane,
@@ -368,20 +390,17 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
   for (int s = t.jg_lane[lane]; s < s1; ++s) {
     const int e = t.jg_slots[s];
     const double yrow = state_of(y[t.jg_row[e]]);
-    double P = 0.0, L = 0.0;
+    // branch-free, two entries per iteration into alternating sums
+    double P0 = 0.0, L0 = 0.0, P1 = 0.0, L1 = 0.0;
     const int g1 = t.jg_ptr[e + 1];
+    int g = t.jg_ptr[e];
     #pragma unroll 1
-    for (int g = t.jg_ptr[e]; g < g1; ++g) {
-      const uint32_t w0 = t.jg_w0[g];
-      const double p = part[w0 & 0xFFFFu];
-      const int ind1 = t.jg_w1[g];
-      if (ind1 == 0) {
-        L += p;
-      } else {
-        const double c = t.coef[w0 >> 16];
-        if (-p * state_of(y[ind1 - 1]) * c * h <= yrow) P += c * p;
-      }
+    for (; g + 1 < g1; g += 2) {
+      jac_term(t, part, y, yrow, h, g, &P0, &L0);
+      jac_term(t, part, y, yrow, h, g + 1, &P1, &L1);
     }
+    if (g < g1) jac_term(t, part, y, yrow, h, g, &P0, &L0);
+    const double P = P0 + P1, L = L0 + L1;
     Jout[e] = (JT)(P - L);
     if (jp) jp[e] = P;
     if (jl) jl[e] = L;
@@ -444,18 +463,15 @@ template <typename LT>
 __device__ __noinline__ bool dev_form_factor(const char* tb, const LT* J, double gamma,
                                              LT* LU, LT* dinv, int lane) {
   const Tab t = make_tab(tb);
+  // M = I - gamma*J in one pass over the LU positions (fill-in starts at 0)
   #pragma unroll 1
-  for (int q = lane; q < t.n_lu; q += 32) LU[q] = (LT)0;
-  __syncwarp();
-  const int s1 = t.jg_lane[lane + 1];
-  #pragma unroll 1
-  for (int s = t.jg_lane[lane]; s < s1; ++s) {
-    const int e = t.jg_slots[s];
-    LU[t.jg_lupos[e]] = (LT)(-gamma * (double)J[e]);
+  for (int q = lane; q < t.n_lu; q += 32) {
+    const uint32_t src = t.lu_src[q];
+    const int e = (int)(src & 0x7FFFu) - 1;
+    LT v = e >= 0 ? (LT)(-gamma * (double)J[e]) : (LT)0;
+    if (src & 0x8000u) v += (LT)1;
+    LU[q] = v;
   }
-  __syncwarp();
-  #pragma unroll 1
-  for (int i = lane; i < t.n; i += 32) LU[t.lu_diag[i]] += (LT)1;
   __syncwarp();
   bool bad = grouped_level<1, LT, LT>(t.fb_lane, t.fb_unit, t.fb_pair, 0, LU, LU, LU, dinv, lane);
   __syncwarp();
@@ -1189,7 +1205,7 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char
 }
 
 template <typename LT>
-__global__ void __launch_bounds__(512, 1) solve_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(32 * kMaxCellsPerBlock, 1) solve_kernel(SolveArgs a) {
   extern __shared__ __align__(16) char smem[];
   __shared__ unsigned long long tma_bar;
   if (!stage_tables(smem, a.blob, a.stage_bytes, &tma_bar, a.err)) return;
@@ -1543,7 +1559,7 @@ static bool plan_warp_launch(const BlobOff& off, int sm_count, int max_smem,
     return false;
   }
   int warps = s.warps_per_block > 0 ? std::min(s.warps_per_block, max_warps) : max_warps;
-  warps = std::min(warps, 16);
+  warps = std::min(warps, kMaxCellsPerBlock);
   int bps = std::max(1, s.blocks_per_sm);
   while (bps > 1 && (size_t)bps * (w->tab + warps * w->lay.bytes) > (size_t)max_smem) --bps;
   int grid = std::min(sm_count * bps, std::max(1, max_blocks));
@@ -1757,7 +1773,8 @@ int Engine::max_cells_per_block(const SolveSettings& s) const {
   if (s.kernel != 0) return 0;
   const int lt = s.precision == 1 ? 4 : 8;
   const Layout lay = make_layout(I->off, lt, s.hist_global == 0);
-  return std::min(16, std::max(0, (I->max_smem - tab_bytes_of(I->off, s.lu_mode)) / lay.bytes));
+  return std::min(kMaxCellsPerBlock,
+                  std::max(0, (I->max_smem - tab_bytes_of(I->off, s.lu_mode)) / lay.bytes));
 }
 
 bool Engine::read_last_ms(void* stream) {
@@ -1972,7 +1989,7 @@ bool Engine::run_solve_static(double* d_state, const double* d_env, const double
     return false;
   }
   if (s.warps_per_block > 0) warps = std::min(warps, s.warps_per_block);
-  warps = std::min(warps, 16);
+  warps = std::min(warps, kMaxCellsPerBlock);
   // one resident cell keeps n_jac Jacobian values (the kernel indexes them
   // by warp); the static array bounds the number of resident cells
   const size_t per_warp = (size_t)lt * I->m.n_jac;
