@@ -226,13 +226,11 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.jg_w0 = w.put(jg_w0);
   o.jg_w1 = w.put(jg_w1);
   o.jg_ptr = w.put(jg_ptr);
-  o.jg_lupos = w.put(jg_lupos);
   o.jg_row = w.put(jg_row);
   o.jg_lane = w.put(jg_lane);
   o.jg_slots = w.put(jg_slots);
   o.n_plev = t.n_plev;
   o.lu_perm = w.put(u16(t.lu_perm));
-  o.lu_diag = w.put(u16(t.lu_diag));
   o.lu_src = w.put(lu_src);
   o.fa_ptr = w.put(u16(t.fa_ptr));
   o.fa = w.put(fa);
@@ -255,6 +253,8 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     std::vector<uint32_t> up(t.upd_ptr.begin(), t.upd_ptr.end()), ud(t.upd_src.size());
     for (size_t p = 0; p < ud.size(); ++p)
       ud[p] = (uint32_t)t.upd_src[p] | ((uint32_t)t.upd_dst[p] << 16);
+    o.jg_lupos = w.put(jg_lupos);
+    o.lu_diag = w.put(u16(t.lu_diag));
     o.lu_rowptr = w.put(u16(t.lu_rowptr));
     o.lu_col = w.put(u16(t.lu_col));
     o.upd_ptr = w.put(up);

@@ -39,8 +39,9 @@ struct BlobOff {
   int fb_lane, fb_unit, fb_pair;
   int fw_lane, fw_unit, fw_pair;
   int bw_lane, bw_unit, bw_pair;
-  // row-wise LU for the sequential (one-lane) mode: rowptr, col (uint16),
-  // update pointer per L entry (uint32) and updates (src | dst<<16)
+  // row-wise LU for the sequential (one-lane) mode: J slot -> LU position
+  // (jg_lupos), diagonal positions, rowptr, col (uint16), update pointer per
+  // L entry (uint32) and updates (src | dst<<16); staged only in that mode
   int lu_rowptr, lu_col, upd_ptr, upd;
   // dependent index -> state index (uint16); absolute tolerances (double)
   int dep_state, atol;

@@ -1524,7 +1524,8 @@ static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist) {
   L.lu = take((size_t)lt_size * o.n_lu);
   L.z = take((size_t)lt_size * o.n);
   L.dinv = take((size_t)lt_size * o.n);
-  L.ctl = take(sizeof(double) * 32);
+  // control block: tau[LMAX + 2], tq[8], l[LMAX + 1]
+  L.ctl = take(sizeof(double) * (LMAX + 2 + 8 + LMAX + 1));
   L.bytes = (int)off;
   return L;
 }
