@@ -42,9 +42,9 @@ MECH_FILE = os.path.join(ROOT, "tests", "golden", "cb05cl_ae5.mech.json")
 # env (16), photolysis base rates (25 x 8), dependent state write (74 x 8)
 METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
 # DRAM bytes (read + write) per cell of one solve launch, from the ncu capture
-# summarised in profiles/solve_kernel_mixed_cb05_2000cells.md (2.91 MB for
+# summarised in profiles/solve_kernel_mixed_cb05_2000cells.md (3.45 MB for
 # 2 000 cells); the launch's traffic grows with the cells it processes
-TRAFFIC_BYTES_PER_CELL = 2.911e6 / 2000
+TRAFFIC_BYTES_PER_CELL = 3.445e6 / 2000
 
 
 def parse():
@@ -127,33 +127,21 @@ class ClockSampler:
 
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
+    from camp_b200 import replicas
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    return world, rank, local
+    return replicas.init("nccl")
 
 
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from camp_b200 import replicas
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(x, world)
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from camp_b200 import replicas
 
-        dist.barrier()
+    replicas.barrier(world)
 
 
 # ---------------------------------------------------------------------------
@@ -199,7 +187,8 @@ def cpu_reference_run(mech, cells, steps, warmup, dt, sample, max_steps):
 
 
 def run_reference_arm(args):
-    world, rank, local = dist_init()
+    # the CPU arm needs no process group: rank 0 runs, the other ranks exit
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from camp_b200.cells import make_cells
@@ -331,7 +320,9 @@ def run_gpu_arm(args):
 
     mech = Mechanism.load(MECH_FILE)
     n = args.cells
-    cells = make_cells(mech, n, SEED + 7919 * rank)
+    from camp_b200 import replicas
+
+    cells = make_cells(mech, n, replicas.rank_seed(SEED, rank))
     atol = np.full(mech.n_state_var, 1e-8)
     dev = torch.device("cuda", local)
     # a created stream: the legacy default stream (handle 0) would read as
@@ -387,13 +378,14 @@ def run_gpu_arm(args):
     with ClockSampler(local) as clk:
         step_ms, kernel_ms, ok_cells, launches, last_stats = device_run(solver, args.steps, args.warmup)
     total_s = max_over_ranks(sum(step_ms) / 1e3, world)
-    value = world * n * args.steps / total_s
+    value = replicas.aggregate_throughput(n, args.steps, world, total_s)
     fp64 = None
     if not args.no_fp64_compare:
         s64 = make_solver(FP64)
         sm64, km64, ok64, _, _ = device_run(s64, args.steps, min(args.warmup, 3))
         t64 = max_over_ranks(sum(sm64) / 1e3, world)
-        fp64 = {"value": world * n * args.steps / t64, "unit": "cell-steps/s",
+        fp64 = {"value": replicas.aggregate_throughput(n, args.steps, world, t64),
+                "unit": "cell-steps/s",
                 "ms_per_step": 1e3 * t64 / args.steps,
                 "ok_cell_fraction": float(np.mean(ok64)) / n}
         s64.free()
@@ -415,13 +407,16 @@ def run_gpu_arm(args):
                 times.append(time.perf_counter() - t0)
         te = max_over_ranks(sum(times), world)
         n_photo = solver.n_photo
-        e2e = {"value": world * n * args.steps / te, "unit": "cell-steps/s",
+        e2e = {"value": replicas.aggregate_throughput(n, args.steps, world, te),
+               "unit": "cell-steps/s",
                "h2d_bytes_per_step": int(8 * n * (mech.n_state_var + 2 + n_photo)),
                "d2h_bytes_per_step": int(8 * n * mech.n_state_var + 56 * n)}
     serving = None
     if world == 1 and not args.no_serving:
         serving = serving_run(args, prec)
     if rank != 0:
+        solver.free()
+        replicas.finalize(world)
         return
     cb = None
     if world == 1 and not args.no_cpu_baseline:
@@ -475,18 +470,16 @@ def run_gpu_arm(args):
             "traffic": TRAFFIC_BYTES_PER_CELL * n,
             "note": f"{bpcs} compulsory bytes per cell-step x cells / mean solve-kernel time "
                     "(of measured peak); traffic = ncu DRAM bytes per launch scaled from a "
-                    "2000-cell capture; the kernel is bound by issue latency (IPC 0.72, FP64 "
-                    "pipe 3.7 %), not by HBM",
+                    "2000-cell capture; the kernel is bound by dependent-issue latency (IPC "
+                    "1.14, FP64 pipe 6.8 %, profiles/solve_kernel_mixed_cb05_2000cells.md), "
+                    "not by HBM",
         },
         "cpu_baseline": cb,
         "serving": serving,
     }
     print(json.dumps(line), flush=True)
     solver.free()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    replicas.finalize(world)
 
 
 def main():
