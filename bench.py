@@ -342,10 +342,13 @@ def run_gpu_arm(args):
 
     init_state = torch.from_numpy(cells.state).to(dev)
     d_env = torch.from_numpy(cells.env).to(dev)
+    d_photo = torch.from_numpy(np.ascontiguousarray(cells.photo_rates)).to(dev)
 
     def device_run(s, steps, warmup):
         """warmup + timed host steps on device-resident inputs."""
         d_state = init_state.clone()
+        # every input resident in HBM: photolysis rates from device memory too
+        s.set_photo_rates_device(d_photo, n)
         step_ms, ok_cells, launches0 = [], [], None
         kernel_ms = []
         for it in range(warmup + steps):
@@ -395,6 +398,8 @@ def run_gpu_arm(args):
         h_state = torch.empty((n, mech.n_state_var), dtype=torch.float64, pin_memory=True)
         h_env = torch.from_numpy(cells.env).pin_memory()
         hs, he = h_state.numpy(), h_env.numpy()
+        # end to end: photolysis rates travel from the host with each run
+        solver.set_photo_rates_device(None)
         times = []
         for it in range(args.warmup + args.steps):
             if it % 10 == 0:

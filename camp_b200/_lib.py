@@ -45,7 +45,7 @@ EXPORTED = [
     "camp_b200_last_error", "camp_b200_is_ready", "camp_b200_set_precision",
     "camp_b200_set_launch", "camp_b200_set_lu_mode", "camp_b200_set_kernel", "camp_b200_set_layout", "camp_b200_set_graph", "camp_b200_autotune", "camp_b200_get_tuning", "camp_b200_set_cost_ordering", "camp_b200_run_device",
     "camp_b200_launch_device", "camp_b200_sync_status", "camp_b200_run_device_noalloc", "camp_b200_n_photo",
-    "camp_b200_set_photo_rates", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
+    "camp_b200_set_photo_rates", "camp_b200_set_photo_rates_device", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
     "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
@@ -111,6 +111,8 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_n_photo.restype = ip
     lib.camp_b200_n_photo.argtypes = [vp]
     lib.camp_b200_set_photo_rates.argtypes = [vp, _f64p, ip]
+    lib.camp_b200_set_photo_rates_device.restype = ip
+    lib.camp_b200_set_photo_rates_device.argtypes = [vp, vp, ip]
     lib.camp_b200_get_cell_stats.restype = ip
     lib.camp_b200_get_cell_stats.argtypes = [vp, C.POINTER(CellStats), ip]
     lib.camp_b200_kernel_launches.restype = C.c_long

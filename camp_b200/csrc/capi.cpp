@@ -47,6 +47,10 @@ struct Solver {
   // per-cell photolysis base rates [n_cells * n_photo]
   std::vector<double> photo;
   int n_photo = 0;
+  // device-resident photolysis rates set by camp_b200_set_photo_rates_device
+  // (used instead of the host copy while set)
+  const double* d_photo_user = nullptr;
+  int d_photo_cells = 0;
   SolveSettings settings;
   std::vector<double> atol_dep;
   bool ready = false;
@@ -80,7 +84,13 @@ bool run_common(Solver* s, double* d_state, const double* d_env, int n_cells,
                 double t0, double t1, cudaStream_t st, bool sync) {
   std::string err;
   const double* d_photo = nullptr;
-  if (s->n_photo > 0) {
+  if (s->n_photo > 0 && s->d_photo_user) {
+    if (n_cells > s->d_photo_cells) {
+      set_error("device photolysis rates cover fewer cells than the run");
+      return false;
+    }
+    d_photo = s->d_photo_user;
+  } else if (s->n_photo > 0) {
     double* dp = s->engine->d_photo_buf(n_cells, &err);
     if (!dp) {
       set_error(err);
@@ -611,6 +621,15 @@ int camp_b200_set_photo_rates(void* solver_data, const double* rates, int n_cell
   s->ensure_photo();
   if (n_cells < 0 || n_cells > s->n_cells) return -1;
   std::copy(rates, rates + (size_t)n_cells * s->n_photo, s->photo.begin());
+  return 0;
+}
+
+int camp_b200_set_photo_rates_device(void* solver_data, const double* d_rates, int n_cells) {
+  Solver* s = S(solver_data);
+  s->ensure_photo();
+  if (n_cells < 0) return -1;
+  s->d_photo_user = n_cells > 0 ? d_rates : nullptr;
+  s->d_photo_cells = d_rates ? n_cells : 0;
   return 0;
 }
 

@@ -180,6 +180,19 @@ class Solver:
         self.lib.rxn_update_data(int(cell), C.byref(cursor), RXN_PHOTOLYSIS, ud, self._h)
         self.lib.solver_free_update_data(ud)
 
+    def set_photo_rates_device(self, d_rates, n_cells: int | None = None) -> None:
+        """Photolysis rates already in device memory (torch CUDA tensor or
+        pointer; None returns to the host rates)."""
+        if d_rates is None:
+            self.lib.camp_b200_set_photo_rates_device(self._h, None, 0)
+            self._d_photo_ref = None
+            return
+        ptr = d_rates.data_ptr() if hasattr(d_rates, "data_ptr") else int(d_rates)
+        n = self.n_cells if n_cells is None else int(n_cells)
+        self._d_photo_ref = d_rates  # keep the buffer alive while in use
+        if self.lib.camp_b200_set_photo_rates_device(self._h, ptr, n) != 0:
+            raise SolverError(_lib.last_error())
+
     @property
     def n_photo(self) -> int:
         return int(self.lib.camp_b200_n_photo(self._h))

@@ -223,6 +223,10 @@ int camp_b200_run_device_noalloc(void *solver_data, double *d_state,
  * called for every cell and reaction. */
 int camp_b200_n_photo(void *solver_data);
 int camp_b200_set_photo_rates(void *solver_data, const double *rates, int n_cells);
+/* Device-resident form: rates [n_cells * n_photo] in device memory, read by
+ * every following run (no per-run upload) until called with NULL, which
+ * returns to the host rates.  The buffer must stay valid meanwhile. */
+int camp_b200_set_photo_rates_device(void *solver_data, const double *d_rates, int n_cells);
 
 int camp_b200_get_cell_stats(void *solver_data, camp_b200_cell_stats *out, int n_cells);
 /* number of GPU kernel launches made by this solver since creation */

@@ -109,3 +109,26 @@ def test_graph_launch_keeps_results(cb05):
     for (a, sa), (b, sb) in zip(*outs):
         np.testing.assert_array_equal(sa, sb)
         np.testing.assert_allclose(b, a, rtol=RTOL, atol=0)
+
+
+def test_device_photolysis_rates(cb05):
+    """Rates handed over in device memory give the results of host rates."""
+    import torch
+
+    from camp_b200.cells import make_cells
+
+    n = 128
+    cells = make_cells(cb05, n, 51)
+    dev = torch.device("cuda", 0)
+    env = torch.from_numpy(cells.env).to(dev)
+    s = _solver(cb05, n, max_steps=1500)
+    s.set_photo_rates(cells.photo_rates)
+    a = torch.from_numpy(cells.state).to(dev)
+    s.run_device(a, env, n, 0.0, 60.0)
+    sa = s.cell_stats()["status"].copy()
+    s.set_photo_rates(np.zeros_like(cells.photo_rates))  # host copy no longer matches
+    s.set_photo_rates_device(torch.from_numpy(np.ascontiguousarray(cells.photo_rates)).to(dev))
+    b = torch.from_numpy(cells.state).to(dev)
+    s.run_device(b, env, n, 0.0, 60.0)
+    np.testing.assert_array_equal(s.cell_stats()["status"], sa)
+    np.testing.assert_allclose(b.cpu().numpy(), a.cpu().numpy(), rtol=RTOL, atol=0)
