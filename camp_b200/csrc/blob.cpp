@@ -164,8 +164,13 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   std::vector<uint16_t> jg_lane(kLanes + 1, 0), jg_slots;
   for (int l = 0; l < kLanes; ++l) {
     jg_lane[l] = (uint16_t)jg_slots.size();
+    // longest slots first on every lane: the lanes of a warp step through
+    // their k-th slots together, so slots of similar length line up and the
+    // warp runs sum_k max_lane(len) ~ the per-lane total instead of far more
     std::vector<int> s = jlanes[l];
-    std::sort(s.begin(), s.end());
+    std::stable_sort(s.begin(), s.end(), [&](int a, int b) {
+      return t.jg_ptr[a + 1] - t.jg_ptr[a] > t.jg_ptr[b + 1] - t.jg_ptr[b];
+    });
     for (int e : s) jg_slots.push_back((uint16_t)e);
   }
   jg_lane[kLanes] = (uint16_t)jg_slots.size();
