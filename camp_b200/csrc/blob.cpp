@@ -86,11 +86,25 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     rx_vptr[r] = (uint16_t)v0;
   }
   rx_vptr[t.n_rxn] = (uint16_t)t.n_part;
-  // f gather entries
-  std::vector<uint32_t> fg_ent(t.fg_rxn.size());
-  for (size_t e = 0; e < fg_ent.size(); ++e) {
-    int c = coef_id(t.fg_coef[e]);
-    fg_ent[e] = (uint32_t)t.fg_rxn[e] | ((uint32_t)c << 16) | ((uint32_t)(t.fg_prod[e] ? 1 : 0) << 31);
+  // f gather entries.  Each species list is regrouped, keeping reaction
+  // order within a group: reactant occurrences (loss, coefficient -1), then
+  // products with a non-negative yield, then products with a negative yield,
+  // so that the device's common path adds each group without classifying
+  // every term.  grp_end[2 * i + g] is the end of group g of species i.
+  std::vector<uint32_t> fg_ent;
+  fg_ent.reserve(t.fg_rxn.size());
+  std::vector<int> grp_end(2 * n);
+  for (int i = 0; i < n; ++i) {
+    for (int g = 0; g < 3; ++g) {
+      for (int e = t.fg_ptr[i]; e < t.fg_ptr[i + 1]; ++e) {
+        const int eg = !t.fg_prod[e] ? 0 : (t.fg_coef[e] >= 0.0 ? 1 : 2);
+        if (eg != g) continue;
+        int c = coef_id(t.fg_coef[e]);
+        fg_ent.push_back((uint32_t)t.fg_rxn[e] | ((uint32_t)c << 16) |
+                         ((uint32_t)(t.fg_prod[e] ? 1 : 0) << 31));
+      }
+      if (g < 2) grp_end[2 * i + g] = (int)fg_ent.size();
+    }
   }
   // balanced f units: species lists longer than the per-lane share are split
   // into slots that a combine pass adds up
@@ -99,6 +113,7 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   struct Unit {
     int sp, b, e, slot;
   };
+  auto clampi = [](int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); };
   std::vector<Unit> units;
   std::vector<uint16_t> split;
   int n_slots = 0;
@@ -120,24 +135,41 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   std::vector<long> uw(units.size());
   for (size_t u = 0; u < units.size(); ++u) uw[u] = 2 + (units[u].e - units[u].b);
   auto ulanes = lpt(uw);
+  // unit record (8 x uint16, one 16-byte load): species, first entry, end
+  // of its loss entries, end of its non-negative-yield products, end, slot
   std::vector<uint16_t> fg_unit, fg_lane(kLanes + 1, 0);
   for (int l = 0; l < kLanes; ++l) {
-    fg_lane[l] = (uint16_t)(fg_unit.size() / 4);
+    fg_lane[l] = (uint16_t)(fg_unit.size() / 8);
     for (int u : ulanes[l]) {
-      fg_unit.push_back((uint16_t)units[u].sp);
-      fg_unit.push_back((uint16_t)units[u].b);
-      fg_unit.push_back((uint16_t)units[u].e);
-      fg_unit.push_back((uint16_t)units[u].slot);
+      const Unit& x = units[u];
+      fg_unit.push_back((uint16_t)x.sp);
+      fg_unit.push_back((uint16_t)x.b);
+      fg_unit.push_back((uint16_t)clampi(grp_end[2 * x.sp], x.b, x.e));
+      fg_unit.push_back((uint16_t)clampi(grp_end[2 * x.sp + 1], x.b, x.e));
+      fg_unit.push_back((uint16_t)x.e);
+      fg_unit.push_back((uint16_t)x.slot);
+      fg_unit.push_back(0);
+      fg_unit.push_back(0);
     }
   }
-  fg_lane[kLanes] = (uint16_t)(fg_unit.size() / 4);
-  // J gather
-  std::vector<uint32_t> jg_w0(t.jg_part.size());
-  std::vector<uint16_t> jg_w1(t.jg_part.size());
-  for (size_t g = 0; g < jg_w0.size(); ++g) {
-    int c = coef_id(t.jg_coef[g]);
-    jg_w0[g] = (uint32_t)t.jg_part[g] | ((uint32_t)c << 16);
-    jg_w1[g] = (uint16_t)(t.jg_ind[g] + 1);
+  fg_lane[kLanes] = (uint16_t)(fg_unit.size() / 8);
+  // J gather: each slot's partials regrouped, losses first (they add to the
+  // loss part unguarded) and then products (guarded, into the production
+  // part); jg_mid[e] is the first product entry of slot e
+  std::vector<uint32_t> jg_w0;
+  std::vector<uint16_t> jg_w1, jg_mid(t.n_jac);
+  jg_w0.reserve(t.jg_part.size());
+  jg_w1.reserve(t.jg_part.size());
+  for (int e = 0; e < t.n_jac; ++e) {
+    for (int pass = 0; pass < 2; ++pass) {
+      if (pass == 1) jg_mid[e] = (uint16_t)jg_w0.size();
+      for (int g = t.jg_ptr[e]; g < t.jg_ptr[e + 1]; ++g) {
+        if ((t.jg_ind[g] >= 0) != (pass == 1)) continue;
+        int c = coef_id(t.jg_coef[g]);
+        jg_w0.push_back((uint32_t)t.jg_part[g] | ((uint32_t)c << 16));
+        jg_w1.push_back((uint16_t)(t.jg_ind[g] + 1));
+      }
+    }
   }
   if (coef.size() > 32767) {
     *err = "too many distinct yields for the table encoding";
@@ -231,6 +263,7 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.jg_w0 = w.put(jg_w0);
   o.jg_w1 = w.put(jg_w1);
   o.jg_ptr = w.put(jg_ptr);
+  o.jg_mid = w.put(jg_mid);
   o.jg_row = w.put(jg_row);
   o.jg_lane = w.put(jg_lane);
   o.jg_slots = w.put(jg_slots);

@@ -26,7 +26,7 @@ struct BlobOff {
   int fg_ent, fg_unit, fg_lane, fg_split;
   // J gather: w0 = part | coef<<16, w1 = independent species + 1 (0 = loss
   // entry); per slot: entry pointer, LU position, row; lane slot lists
-  int jg_w0, jg_w1, jg_ptr, jg_lupos, jg_row, jg_lane, jg_slots;
+  int jg_w0, jg_w1, jg_ptr, jg_mid, jg_lupos, jg_row, jg_lane, jg_slots;
   // LU: perm, diag (uint16); factorization by pivot level: scaled L entries
   // (fa_ptr uint16, fa = pos | pivot<<16), Schur updates grouped by target
   // with the reciprocal pivots taken in the same phase (fb); forward solve

@@ -139,7 +139,7 @@ struct Tab {
   const uint32_t* fg_ent;
   const uint16_t *fg_unit, *fg_lane, *fg_split;
   const uint32_t* jg_w0;
-  const uint16_t *jg_w1, *jg_ptr, *jg_lupos, *jg_row, *jg_lane, *jg_slots;
+  const uint16_t *jg_w1, *jg_ptr, *jg_mid, *jg_lupos, *jg_row, *jg_lane, *jg_slots;
   const uint16_t *lu_perm, *lu_diag, *lu_src, *fa_ptr;
   const uint32_t* fa;
   const uint16_t* fb_lane;
@@ -168,6 +168,7 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.jg_w0 = (const uint32_t*)(b + o.jg_w0);
   t.jg_w1 = (const uint16_t*)(b + o.jg_w1);
   t.jg_ptr = (const uint16_t*)(b + o.jg_ptr);
+  t.jg_mid = (const uint16_t*)(b + o.jg_mid);
   t.jg_lupos = (const uint16_t*)(b + o.jg_lupos);
   t.jg_row = (const uint16_t*)(b + o.jg_row);
   t.jg_lane = (const uint16_t*)(b + o.jg_lane);
@@ -246,8 +247,11 @@ __device__ bool stage_tables(char* dst, const void* src, int bytes, unsigned lon
 // ---------------------------------------------------------------------------
 // Right-hand side f(y) and Jacobian
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void rates_of(const Tab& t, const double* y, const double* keff,
+// Reaction rates k * prod(y) into rates[]; returns (warp-uniform) whether
+// any rate is negative, which only a reactant in (-SMALL, 0) can cause.
+__device__ __forceinline__ bool rates_of(const Tab& t, const double* y, const double* keff,
                                          double* rates, int lane) {
+  bool neg = false;
   #pragma unroll 1
   for (int r = lane; r < t.n_rxn; r += 32) {
     const uint32_t w = t.rx_word[r];
@@ -257,7 +261,9 @@ __device__ __forceinline__ void rates_of(const Tab& t, const double* y, const do
     if (nv > 1) rate *= state_of(y[(w >> 10) & 1023u]);
     if (nv > 2) rate *= state_of(y[(w >> 20) & 1023u]);
     rates[r] = rate;
+    neg |= rate < 0.0;
   }
+  return warp_any(neg);
 }
 
 // Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
@@ -273,39 +279,70 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
   #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
   if (warp_any(bad)) return 1;
-  rates_of(t, y, keff, rates, lane);
+  const bool negrate = rates_of(t, y, keff, rates, lane);
   __syncwarp();
+  const uint4* fg_unit = (const uint4*)t.fg_unit;
   const int u1 = t.fg_lane[lane + 1];
   #pragma unroll 1
   for (int u = t.fg_lane[lane]; u < u1; ++u) {
-    const int sp = t.fg_unit[4 * u], b = t.fg_unit[4 * u + 1], e = t.fg_unit[4 * u + 2];
-    const int slot = t.fg_unit[4 * u + 3];
+    // unit record: species | first entry, end of losses | end of
+    // non-negative-yield products, end | slot
+    const uint4 rec = fg_unit[u];
+    const int sp = rec.x & 0xFFFFu, b = rec.x >> 16;
+    const int m1 = rec.y & 0xFFFFu, m2 = rec.y >> 16;
+    const int e = rec.z & 0xFFFFu, slot = rec.z >> 16;
     const double yi = state_of(y[sp]);
-    // branch-free accumulation, two entries per iteration: a guarded product
-    // term that may not apply, and a zero rate, contribute 0 to both sums
     double P0 = 0.0, L0 = 0.0, P1 = 0.0, L1 = 0.0;
-    int k = b;
-    #pragma unroll 1
-    for (; k + 1 < e; k += 2) {
-      const uint32_t w0 = t.fg_ent[k], w1 = t.fg_ent[k + 1];
-      const double r0 = rates[w0 & 0xFFFFu], r1 = rates[w1 & 0xFFFFu];
-      const double c0 = t.coef[(w0 >> 16) & 0x7FFFu], c1 = t.coef[(w1 >> 16) & 0x7FFFu];
-      // a negative yield may not drive the product negative within one step
-      // (src/rxns/rxn_arrhenius.c:153-160)
-      const double v0 = ((w0 >> 31) && !(-r0 * c0 * h <= yi)) ? 0.0 : r0 * c0;
-      const double v1 = ((w1 >> 31) && !(-r1 * c1 * h <= yi)) ? 0.0 : r1 * c1;
-      P0 += fmax(v0, 0.0);
-      L0 += fmax(-v0, 0.0);
-      P1 += fmax(v1, 0.0);
-      L1 += fmax(-v1, 0.0);
-    }
-    if (k < e) {
-      const uint32_t w0 = t.fg_ent[k];
-      const double r0 = rates[w0 & 0xFFFFu];
-      const double c0 = t.coef[(w0 >> 16) & 0x7FFFu];
-      const double v0 = ((w0 >> 31) && !(-r0 * c0 * h <= yi)) ? 0.0 : r0 * c0;
-      P0 += fmax(v0, 0.0);
-      L0 += fmax(-v0, 0.0);
+    if (!negrate && yi >= 0.0 && h >= 0.0) {
+      // common path: every rate >= 0 and the product concentration >= 0, so
+      // each group's sign is known and the negative-yield guard
+      // (src/rxns/rxn_arrhenius.c:153-160) can only fail for negative yields
+      int k = b;
+      #pragma unroll 1
+      for (; k + 1 < m1; k += 2) {
+        L0 += rates[t.fg_ent[k] & 0xFFFFu];
+        L1 += rates[t.fg_ent[k + 1] & 0xFFFFu];
+      }
+      if (k < m1) L0 += rates[t.fg_ent[k] & 0xFFFFu];
+      #pragma unroll 1
+      for (k = m1; k + 1 < m2; k += 2) {
+        const uint32_t w0 = t.fg_ent[k], w1 = t.fg_ent[k + 1];
+        P0 += __dmul_rn(rates[w0 & 0xFFFFu], t.coef[(w0 >> 16) & 0x7FFFu]);
+        P1 += __dmul_rn(rates[w1 & 0xFFFFu], t.coef[(w1 >> 16) & 0x7FFFu]);
+      }
+      if (k < m2) {
+        const uint32_t w0 = t.fg_ent[k];
+        P0 += __dmul_rn(rates[w0 & 0xFFFFu], t.coef[(w0 >> 16) & 0x7FFFu]);
+      }
+      #pragma unroll 1
+      for (k = m2; k < e; ++k) {
+        const uint32_t w0 = t.fg_ent[k];
+        const double v = __dmul_rn(rates[w0 & 0xFFFFu], -t.coef[(w0 >> 16) & 0x7FFFu]);
+        L1 += v * h <= yi ? v : 0.0;
+      }
+    } else {
+      // any sign: classify every term, guard every product term
+      int k = b;
+      #pragma unroll 1
+      for (; k + 1 < e; k += 2) {
+        const uint32_t w0 = t.fg_ent[k], w1 = t.fg_ent[k + 1];
+        const double r0 = rates[w0 & 0xFFFFu], r1 = rates[w1 & 0xFFFFu];
+        const double c0 = t.coef[(w0 >> 16) & 0x7FFFu], c1 = t.coef[(w1 >> 16) & 0x7FFFu];
+        const double v0 = ((w0 >> 31) && !(-r0 * c0 * h <= yi)) ? 0.0 : r0 * c0;
+        const double v1 = ((w1 >> 31) && !(-r1 * c1 * h <= yi)) ? 0.0 : r1 * c1;
+        P0 += v0 > 0.0 ? v0 : 0.0;
+        L0 += v0 < 0.0 ? -v0 : 0.0;
+        P1 += v1 > 0.0 ? v1 : 0.0;
+        L1 += v1 < 0.0 ? -v1 : 0.0;
+      }
+      if (k < e) {
+        const uint32_t w0 = t.fg_ent[k];
+        const double r0 = rates[w0 & 0xFFFFu];
+        const double c0 = t.coef[(w0 >> 16) & 0x7FFFu];
+        const double v0 = ((w0 >> 31) && !(-r0 * c0 * h <= yi)) ? 0.0 : r0 * c0;
+        P0 += v0 > 0.0 ? v0 : 0.0;
+        L0 += v0 < 0.0 ? -v0 : 0.0;
+      }
     }
     const double P = P0 + P1, L = L0 + L1;
     if (slot == 0xFFFF) {
@@ -338,21 +375,16 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
 // Solver Jacobian values into Jout (indexed by CSC entry; each lane writes the
 // entries of its balanced slot list); production and loss parts into jp/jl
 // when given (src/rxns/rxn_arrhenius.c:178-212).
-// One entry of a solver-Jacobian slot: a loss partial (independent species
-// index 0) adds to L; a product partial times its yield adds to P when the
-// negative-yield guard lets the product term apply (src/rxns/rxn_arrhenius.c
-// :201-207).
-__device__ __forceinline__ void jac_term(const Tab& t, const double* part, const double* y,
-                                         double yrow, double h, int g, double* P, double* L) {
+// One product entry of a solver-Jacobian slot: the partial times its yield
+// adds to the production part when the negative-yield guard lets the product
+// term apply (src/rxns/rxn_arrhenius.c:201-207).
+__device__ __forceinline__ double jac_prod(const Tab& t, const double* part, const double* y,
+                                           double yrow, double h, int g) {
   const uint32_t w0 = t.jg_w0[g];
-  const int ind1 = t.jg_w1[g];
   const double p = part[w0 & 0xFFFFu];
   const double c = t.coef[w0 >> 16];
-  const double yi = state_of(y[ind1 > 0 ? ind1 - 1 : 0]);
-  const bool prod = ind1 != 0;
-  const bool apply = -p * yi * c * h <= yrow;
-  *P += (prod && apply) ? c * p : 0.0;
-  *L += prod ? 0.0 : p;
+  const double yi = state_of(y[t.jg_w1[g] - 1]);
+  return -p * yi * c * h <= yrow ? __dmul_rn(c, p) : 0.0;
 }
 
 template <typename JT>
@@ -390,16 +422,23 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
   for (int s = t.jg_lane[lane]; s < s1; ++s) {
     const int e = t.jg_slots[s];
     const double yrow = state_of(y[t.jg_row[e]]);
-    // branch-free, two entries per iteration into alternating sums
+    // loss partials [g0, gm) add to L as they are; product partials
+    // [gm, g1) are guarded; two entries per iteration into alternating sums
     double P0 = 0.0, L0 = 0.0, P1 = 0.0, L1 = 0.0;
-    const int g1 = t.jg_ptr[e + 1];
+    const int gm = t.jg_mid[e], g1 = t.jg_ptr[e + 1];
     int g = t.jg_ptr[e];
     #pragma unroll 1
-    for (; g + 1 < g1; g += 2) {
-      jac_term(t, part, y, yrow, h, g, &P0, &L0);
-      jac_term(t, part, y, yrow, h, g + 1, &P1, &L1);
+    for (; g + 1 < gm; g += 2) {
+      L0 += part[t.jg_w0[g] & 0xFFFFu];
+      L1 += part[t.jg_w0[g + 1] & 0xFFFFu];
     }
-    if (g < g1) jac_term(t, part, y, yrow, h, g, &P0, &L0);
+    if (g < gm) L0 += part[t.jg_w0[g] & 0xFFFFu];
+    #pragma unroll 1
+    for (g = gm; g + 1 < g1; g += 2) {
+      P0 += jac_prod(t, part, y, yrow, h, g);
+      P1 += jac_prod(t, part, y, yrow, h, g + 1);
+    }
+    if (g < g1) P0 += jac_prod(t, part, y, yrow, h, g);
     const double P = P0 + P1, L = L0 + L1;
     Jout[e] = (JT)(P - L);
     if (jp) jp[e] = P;
@@ -1180,7 +1219,10 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char
   c.atol = make_tab(tab).atol;
   c.lane = lane;
   c.n = a.off.n;
-  c.zb = a.lay.zn >= 0 ? (double*)(base + a.lay.zn) : a.hist + (size_t)gwarp * a.hist_stride;
+  // per-warp global slab: [Nordsieck history when it is not in shared
+  // memory] [rate constants when they are not in shared memory]
+  double* slab = a.hist ? a.hist + (size_t)gwarp * a.hist_stride : nullptr;
+  c.zb = a.lay.zn >= 0 ? (double*)(base + a.lay.zn) : slab;
   double* ctl = (double*)(base + a.lay.ctl);
   c.tau = ctl;
   c.tq = ctl + (LMAX + 2);
@@ -1191,7 +1233,8 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char
   c.ftemp = (double*)(base + a.lay.ftemp);
   c.tempv = (double*)(base + a.lay.tempv);
   c.rates = (double*)(base + a.lay.rates);
-  c.keff = a.lay.keff >= 0 ? (double*)(base + a.lay.keff) : c.zb + (size_t)LMAX * a.off.n;
+  c.keff = a.lay.keff >= 0 ? (double*)(base + a.lay.keff)
+                           : slab + (a.lay.zn >= 0 ? 0 : (size_t)LMAX * a.off.n);
   c.fscr = (double*)(base + a.lay.fscr);
   c.LU = (LT*)(base + a.lay.lu);
   c.z = (LT*)(base + a.lay.z);
@@ -1503,7 +1546,8 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
 // per-warp shared-memory slice; the solve kernel keeps the Nordsieck history
 // and the rate constants in global memory (with_hist = false), which leaves
 // room for more resident cells
-static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist) {
+static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist,
+                          bool keff_in_smem) {
   Layout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -1519,7 +1563,7 @@ static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist) {
   L.ftemp = take(vec);
   L.tempv = take(vec);
   L.rates = take(sizeof(double) * std::max(o.n_rxn, o.n_part));
-  L.keff = with_hist ? take(sizeof(double) * o.n_rxn) : -1;
+  L.keff = keff_in_smem ? take(sizeof(double) * o.n_rxn) : -1;
   L.fscr = take(sizeof(double) * 2 * std::max(1, o.n_fscratch));
   L.lu = take((size_t)lt_size * o.n_lu);
   L.z = take((size_t)lt_size * o.n);
@@ -1551,7 +1595,7 @@ static bool plan_warp_launch(const BlobOff& off, int sm_count, int max_smem,
                              const SolveSettings& s, int n_cells, int max_blocks,
                              WarpLaunch* w, std::string* err) {
   w->lt = s.precision == 1 ? 4 : 8;
-  w->lay = make_layout(off, w->lt, s.hist_global == 0);
+  w->lay = make_layout(off, w->lt, s.hist_global == 0, true);
   w->tab = tab_bytes_of(off, s.lu_mode);
   int max_warps = (max_smem - w->tab) / w->lay.bytes;
   if (max_warps < 1) {
@@ -1573,8 +1617,10 @@ static bool plan_warp_launch(const BlobOff& off, int sm_count, int max_smem,
 }
 
 static int hist_stride_of(const BlobOff& off, const SolveSettings& s) {
-  // history + rate constants per warp, rounded to 256-byte rows
-  return s.hist_global ? ((LMAX * off.n + off.n_rxn) + 31) & ~31 : 0;
+  // global slab per warp for the Nordsieck history when it is not in shared
+  // memory, rounded to 256-byte rows (the rate constants stay in shared
+  // memory: they sit on the dependent path of every f and J evaluation)
+  return s.hist_global ? (LMAX * off.n + 31) & ~31 : 0;
 }
 
 static bool launch_warp_kernel(SolveArgs& a, const WarpLaunch& w, int precision,
@@ -1643,7 +1689,7 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)w.lt * I->m.n_jac * total_warps, err))
     return false;
   const int hist_stride = hist_stride_of(I->off, s);
-  if (s.hist_global &&
+  if (hist_stride &&
       !ensure(&I->d_hist, &I->c_hist, sizeof(double) * (size_t)hist_stride * total_warps, err))
     return false;
   SolveArgs a;
@@ -1773,7 +1819,7 @@ int Engine::max_cells_per_block(const SolveSettings& s) const {
   const Impl* I = impl_;
   if (s.kernel != 0) return 0;
   const int lt = s.precision == 1 ? 4 : 8;
-  const Layout lay = make_layout(I->off, lt, s.hist_global == 0);
+  const Layout lay = make_layout(I->off, lt, s.hist_global == 0, true);
   return std::min(kMaxCellsPerBlock,
                   std::max(0, (I->max_smem - tab_bytes_of(I->off, s.lu_mode)) / lay.bytes));
 }
@@ -1854,7 +1900,7 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
   a.tab_bytes = tab_bytes_of(I->off, 1);
   a.stage_bytes = I->off.bytes;
   a.err = I->d_counter + 1;
-  a.lay = make_layout(I->off, 8, true);
+  a.lay = make_layout(I->off, 8, true, true);
   a.state = ds;
   a.env = de;
   a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
@@ -1902,7 +1948,7 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   a.tab_bytes = tab_bytes_of(I->off, 1);
   a.stage_bytes = I->off.bytes;
   a.err = I->d_counter + 1;
-  a.lay = make_layout(I->off, 8, true);
+  a.lay = make_layout(I->off, 8, true, true);
   a.state = ds;
   a.env = de;
   a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
@@ -1981,7 +2027,7 @@ bool Engine::run_solve_static(double* d_state, const double* d_env, const double
   }
   cudaStream_t st = (cudaStream_t)stream;
   const int lt = s.precision == 1 ? 4 : 8;
-  Layout lay = make_layout(I->off, lt, true);
+  Layout lay = make_layout(I->off, lt, true, true);
   const int tab = tab_bytes_of(I->off, s.lu_mode);
   int warps = (I->max_smem - tab) / lay.bytes;
   if (warps < 1) {
