@@ -25,7 +25,7 @@ constexpr double UROUND = 2.220446049250313e-16;
 // outcome codes (CVODE flags)
 constexpr int OK = 0, TOO_MUCH_WORK = -1, TOO_MUCH_ACC = -2, ERR_FAILURE = -3,
               CONV_FAILURE = -4, REPTD_RHSFUNC_ERR = -10, UNREC_RHSFUNC_ERR = -11,
-              ILL_INPUT = -22;
+              ILL_INPUT = -22, TOO_CLOSE = -27;
 // nonlinear solver outcomes
 constexpr int NL_OK = 0, NL_CONV_FAIL = 1, NL_RHS_RECVR = 2, NL_TRY_AGAIN = 3,
               NL_CONSTR_RECVR = 4;

@@ -605,6 +605,10 @@ L_INIT_F:
   }
   s->nfe++;
   s->h = s->h0;
+  if (s->h0 == 0.0) {  // CVODE's cvHin refuses tout == t0
+    s->flag = TOO_CLOSE;
+    goto L_DONE;
+  }
   if ((s->tout - s->t0) * s->h < 0.0) {
     s->flag = ILL_INPUT;
     goto L_DONE;

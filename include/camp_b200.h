@@ -131,6 +131,7 @@ void sub_model_print_data(void *solver_data);
 #define CAMP_B200_REPTD_RHSFUNC_ERR (-10)
 #define CAMP_B200_UNREC_RHSFUNC_ERR (-11)
 #define CAMP_B200_ILL_INPUT (-22)
+#define CAMP_B200_TOO_CLOSE (-27)
 #define CAMP_B200_NOT_RUN (-99)
 
 /* per-cell counters of the last run */

@@ -1189,6 +1189,12 @@ static int bdf_integrate(Bdf *b, double t0, double tout, double h0, double *y,
     }
   }
   b->h = h0;
+  /* CVODE with a zero initial step estimates one (cvHin), which refuses an
+   * output time at the initial time: CV_TOO_CLOSE */
+  if (h0 == 0.0) {
+    flag = OR_TOO_CLOSE;
+    goto done;
+  }
   if ((tout - t0) * b->h < 0.0) {
     flag = OR_ILL_INPUT;
     goto done;

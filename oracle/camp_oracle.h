@@ -36,6 +36,7 @@ typedef struct OracleMech OracleMech;
 #define OR_REPTD_RHSFUNC_ERR (-10)
 #define OR_UNREC_RHSFUNC_ERR (-11)
 #define OR_ILL_INPUT (-22)
+#define OR_TOO_CLOSE (-27)
 
 /* per-cell statistics (CVODE counters) */
 typedef struct {

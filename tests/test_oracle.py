@@ -115,3 +115,17 @@ def test_bdf_consecutive_first_order(cb05):
     B = k1 / (k2 - k1) * (np.exp(-k1 * t) - np.exp(-k2 * t))
     C = 1.0 - A - B
     np.testing.assert_allclose(out[0], [A, B, C], rtol=1e-7, atol=1e-12)
+
+
+def test_zero_length_step_is_too_close(cb05):
+    """CVODE refuses tout == t0 when it must estimate the initial step
+    (cvHin: CV_TOO_CLOSE, -27); the cell keeps its input."""
+    from camp_b200.cells import make_cells
+    from oracle.oracle import OracleModel
+
+    cells = make_cells(cb05, 2, 4)
+    nf, status, _, out = OracleModel(cb05).solve(cells.state.copy(), cells.env,
+                                                 cells.photo_rates, 5.0, 5.0, 1e-4,
+                                                 np.full(cb05.n_state_var, 1e-8))
+    assert nf == 2 and list(status) == [-27, -27]
+    np.testing.assert_array_equal(out, cells.state)
