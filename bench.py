@@ -42,9 +42,9 @@ MECH_FILE = os.path.join(ROOT, "tests", "golden", "cb05cl_ae5.mech.json")
 # env (16), photolysis base rates (25 x 8), dependent state write (74 x 8)
 METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
 # DRAM bytes (read + write) per cell of one solve launch, from the ncu capture
-# summarised in profiles/solve_kernel_mixed_cb05_2000cells.md (3.45 MB for
+# summarised in profiles/solve_kernel_mixed_cb05_2000cells.md (3.19 MB for
 # 2 000 cells); the launch's traffic grows with the cells it processes
-TRAFFIC_BYTES_PER_CELL = 3.445e6 / 2000
+TRAFFIC_BYTES_PER_CELL = 3.187e6 / 2000
 
 
 def parse():
@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--max-steps", type=int, default=10000)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-cost-order", action="store_true",
+                    help="fetch cells in index order instead of longest-first")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch the device step directly instead of as a CUDA graph")
     ap.add_argument("--serve-rates", default="5,10,20,40",
@@ -338,6 +340,9 @@ def run_gpu_arm(args):
         s.set_photo_rates(cells.photo_rates)
         # device step (counter reset + solve kernel) as one CUDA graph
         s.set_graph(not args.no_graph)
+        # persistent-kernel schedule: cells in decreasing order of their
+        # internal step count in the previous host step (longest first)
+        s.set_cost_ordering(not args.no_cost_order)
         return s
 
     init_state = torch.from_numpy(cells.state).to(dev)
@@ -476,7 +481,7 @@ def run_gpu_arm(args):
             "note": f"{bpcs} compulsory bytes per cell-step x cells / mean solve-kernel time "
                     "(of measured peak); traffic = ncu DRAM bytes per launch scaled from a "
                     "2000-cell capture; the kernel is bound by dependent-issue latency (IPC "
-                    "1.14, FP64 pipe 6.8 %, profiles/solve_kernel_mixed_cb05_2000cells.md), "
+                    "1.0, FP64 pipe 4.4 %, profiles/solve_kernel_mixed_cb05_2000cells.md), "
                     "not by HBM",
         },
         "cpu_baseline": cb,
