@@ -214,24 +214,44 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   };
   std::vector<uint32_t> fa(t.fa_pos.size());
   for (size_t i = 0; i < fa.size(); ++i) fa[i] = (uint32_t)t.fa_pos[i] | ((uint32_t)t.fa_piv[i] << 16);
+  // A grouped phase is stored as rounds: level l runs rounds
+  // [rnd[l], rnd[l + 1]); round r gives lane k the record rec[32 r + k] of
+  // its r-th unit (units of a lane in decreasing size) or, when the lane has
+  // fewer units, a no-op record whose target is the spare slot `dummy` past
+  // the end of the accumulator.  Records: target | count<<16, first pair |
+  // (pivot+1)<<16.
   struct G {
-    std::vector<uint16_t> lane;
-    std::vector<uint32_t> unit, pair;
+    std::vector<uint16_t> rnd;
+    std::vector<uint32_t> rec, pair;
   };
-  auto pack = [&](const Tables::Grouped& g, G* o) {
-    o->lane = u16(g.lane_ptr);
-    o->unit.resize(2 * g.unit_target.size());
-    for (size_t u = 0; u < g.unit_target.size(); ++u) {
-      o->unit[2 * u] = (uint32_t)g.unit_target[u] | ((uint32_t)g.unit_count[u] << 16);
-      o->unit[2 * u + 1] = (uint32_t)g.unit_begin[u] | ((uint32_t)g.unit_recip[u] << 16);
+  auto pack = [&](const Tables::Grouped& g, G* o, int dummy) {
+    o->rnd.assign(1, 0);
+    o->rec.clear();
+    for (int l = 0; l < g.n_levels; ++l) {
+      int rounds = 0;
+      for (int k = 0; k < kLanes; ++k)
+        rounds = std::max(rounds, g.lane_ptr[33 * l + k + 1] - g.lane_ptr[33 * l + k]);
+      for (int r = 0; r < rounds; ++r)
+        for (int k = 0; k < kLanes; ++k) {
+          const int u = g.lane_ptr[33 * l + k] + r;
+          if (u < g.lane_ptr[33 * l + k + 1]) {
+            o->rec.push_back((uint32_t)g.unit_target[u] | ((uint32_t)g.unit_count[u] << 16));
+            o->rec.push_back((uint32_t)g.unit_begin[u] | ((uint32_t)g.unit_recip[u] << 16));
+          } else {
+            o->rec.push_back((uint32_t)dummy);
+            o->rec.push_back(0u);
+          }
+        }
+      o->rnd.push_back((uint16_t)(o->rnd.back() + rounds));
     }
     o->pair.resize(g.pair_a.size());
     for (size_t p = 0; p < g.pair_a.size(); ++p)
       o->pair[p] = (uint32_t)g.pair_a[p] | ((uint32_t)g.pair_b[p] << 16);
-    return g.unit_target.size() <= 65535 && g.pair_a.size() <= 65535 && g.lane_ptr.size() > 0;
+    return g.unit_target.size() <= 65535 && g.pair_a.size() <= 65535 && dummy <= 65535 &&
+           o->rec.size() / 2 / kLanes <= 65535;
   };
   G gfb, gfw, gbw;
-  if (!pack(t.fb, &gfb) || !pack(t.fwd, &gfw) || !pack(t.bwd, &gbw)) {
+  if (!pack(t.fb, &gfb, t.n_lu) || !pack(t.fwd, &gfw, n) || !pack(t.bwd, &gbw, n)) {
     *err = "LU schedule exceeds the 16-bit table encodings";
     return false;
   }
@@ -272,14 +292,14 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.lu_src = w.put(lu_src);
   o.fa_ptr = w.put(u16(t.fa_ptr));
   o.fa = w.put(fa);
-  o.fb_lane = w.put(gfb.lane);
-  o.fb_unit = w.put(gfb.unit);
+  o.fb_lane = w.put(gfb.rnd);
+  o.fb_unit = w.put(gfb.rec);
   o.fb_pair = w.put(gfb.pair);
-  o.fw_lane = w.put(gfw.lane);
-  o.fw_unit = w.put(gfw.unit);
+  o.fw_lane = w.put(gfw.rnd);
+  o.fw_unit = w.put(gfw.rec);
   o.fw_pair = w.put(gfw.pair);
-  o.bw_lane = w.put(gbw.lane);
-  o.bw_unit = w.put(gbw.unit);
+  o.bw_lane = w.put(gbw.rnd);
+  o.bw_unit = w.put(gbw.rec);
   o.bw_pair = w.put(gbw.pair);
   o.dep_state = w.put(u16(t.dep_state));
   o.atol = w.put(atol_dep);

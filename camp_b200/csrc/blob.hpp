@@ -31,9 +31,11 @@ struct BlobOff {
   // (fa_ptr uint16, fa = pos | pivot<<16), Schur updates grouped by target
   // with the reciprocal pivots taken in the same phase (fb); forward solve
   // (fw); backward solve updates with the pivots finalised in the same
-  // phase (bw).  A grouped phase G has lane pointers (uint16, 33 per level),
-  // units (uint32 target | count<<16, uint32 first pair | (pivot+1)<<16,
-  // pivot 0 = none) and pairs (uint32 a | b<<16).
+  // phase (bw).  A grouped phase G has round pointers per level (uint16,
+  // levels + 1; the *_lane fields), one record per lane and round (the
+  // *_unit fields: uint32 target | count<<16, uint32 first pair |
+  // (pivot+1)<<16, pivot 0 = none; a no-op record targets the spare slot
+  // past the accumulator) and pairs (uint32 a | b<<16).
   int lu_perm, lu_diag, lu_src;
   int fa_ptr, fa;
   int fb_lane, fb_unit, fb_pair;

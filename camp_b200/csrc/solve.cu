@@ -435,19 +435,22 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
 // final value, the pivot, in dinv; the return value flags a zero or
 // non-finite pivot.
 template <int MODE, typename LT, typename XT>
-__device__ __forceinline__ bool grouped_level(const uint16_t* lane_ptr, const uint32_t* unit,
+__device__ __forceinline__ bool grouped_level(const uint16_t* rnd, const uint32_t* rec,
                                               const uint32_t* pair, int level, LT* acc,
                                               const LT* a, const XT* x, LT* dinv, int lane) {
   // MODE 0: plain; 1: a unit carrying pivot k stores dinv[k] = 1 / (its
   // final value) (factorization); 2: a unit carrying pivot k scales its final
-  // value by dinv[k] (backward substitution)
+  // value by dinv[k] (backward substitution).  Round r hands this lane the
+  // record rec[32 r + lane]; a no-op record targets the spare accumulator
+  // slot with no pairs and no pivot, so every lane runs the same code.
   bool bad = false;
-  const int u1 = lane_ptr[33 * level + lane + 1];
+  const uint2* rec2 = (const uint2*)rec;
+  const int r1 = rnd[level + 1];
   #pragma unroll 1
-  for (int u = lane_ptr[33 * level + lane]; u < u1; ++u) {
-    const uint32_t w = unit[2 * u], w2 = unit[2 * u + 1];
-    const int tgt = w & 0xFFFFu, cnt = w >> 16;
-    const int p0 = w2 & 0xFFFFu, piv = w2 >> 16;
+  for (int r = rnd[level]; r < r1; ++r) {
+    const uint2 w = rec2[32 * r + lane];
+    const int tgt = w.x & 0xFFFFu, cnt = w.x >> 16;
+    const int p0 = w.y & 0xFFFFu, piv = w.y >> 16;
     LT s0 = acc[tgt], s1 = (LT)0;
     int p = p0;
     #pragma unroll 1
@@ -1546,8 +1549,9 @@ static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist,
   L.rates = take(sizeof(double) * std::max(o.n_rxn, o.n_part));
   L.keff = keff_in_smem ? take(sizeof(double) * o.n_rxn) : -1;
   L.fscr = take(sizeof(double) * 2 * std::max(1, o.n_fscratch));
-  L.lu = take((size_t)lt_size * o.n_lu);
-  L.z = take((size_t)lt_size * o.n);
+  // one spare slot each: the target of the grouped phases' no-op records
+  L.lu = take((size_t)lt_size * (o.n_lu + 1));
+  L.z = take((size_t)lt_size * (o.n + 1));
   L.dinv = take((size_t)lt_size * o.n);
   // control block: tau[LMAX + 2], tq[8], l[LMAX + 1]
   L.ctl = take(sizeof(double) * (LMAX + 2 + 8 + LMAX + 1));
