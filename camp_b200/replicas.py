@@ -23,6 +23,11 @@ def init(backend: str = "nccl", timeout_s: float = 300.0):
     if world > 1:
         import torch.distributed as dist
 
+        if backend == "nccl":
+            import torch
+
+            # each rank owns its GPU before NCCL binds a communicator to it
+            torch.cuda.set_device(local)
         if not dist.is_initialized():
             dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
     return world, rank, local
