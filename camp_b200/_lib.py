@@ -49,7 +49,7 @@ EXPORTED = [
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
     "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
-    "camp_b200_eval_jac", "camp_b200_server_new", "camp_b200_server_add_solver",
+    "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_server_new", "camp_b200_server_add_solver",
     "camp_b200_server_submit", "camp_b200_server_wait", "camp_b200_server_pending",
     "camp_b200_server_free",
 ]
@@ -130,6 +130,8 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_eval_deriv.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p, _f64p]
     lib.camp_b200_eval_jac.restype = ip
     lib.camp_b200_eval_jac.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p]
+    lib.camp_b200_check_jac.restype = ip
+    lib.camp_b200_check_jac.argtypes = [vp, _f64p, _f64p, ip, dp, dp, dp, _f64p, _i32p]
     lib.camp_b200_server_new.restype = vp
     lib.camp_b200_server_new.argtypes = [ip, dp, dp]
     lib.camp_b200_server_add_solver.restype = ip

@@ -719,6 +719,26 @@ int camp_b200_eval_jac(void* solver_data, const double* state, const double* env
   return 0;
 }
 
+int camp_b200_check_jac(void* solver_data, const double* state, const double* env, int n_cells,
+                        double h, double rel_tol, double abs_tol, double* worst_rel,
+                        int* n_failed) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells || !worst_rel || !n_failed) {
+    set_error("camp_b200_check_jac: solver not ready, bad sizes or missing outputs");
+    return -1;
+  }
+  s->ensure_photo();
+  std::string err;
+  if (!s->engine->check_jac(state, env, s->n_photo ? s->photo.data() : nullptr, n_cells, h,
+                            rel_tol, abs_tol, worst_rel, n_failed, &err)) {
+    set_error(err);
+    return -1;
+  }
+  int total = 0;
+  for (int c = 0; c < n_cells; ++c) total += n_failed[c] > 0 ? n_failed[c] : 0;
+  return total;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

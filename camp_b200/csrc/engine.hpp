@@ -63,6 +63,12 @@ class Engine {
                   std::string* err);
   bool eval_jac(const double* h_state, const double* h_env, const double* h_photo,
                 int n_cells, double h, double* jp, double* jl, std::string* err);
+  // Finite-difference audit of the analytic Jacobian (debug tool): per cell,
+  // elements that fail at every step size and the worst best-step relative
+  // difference (-1: f or J could not be evaluated at this state).
+  bool check_jac(const double* h_state, const double* h_env, const double* h_photo,
+                 int n_cells, double h, double rel_tol, double abs_tol, double* worst,
+                 int* nfail, std::string* err);
 
   double* d_state_buf(int n_cells, std::string* err);
   double* d_env_buf(int n_cells, std::string* err);

@@ -19,6 +19,7 @@ struct DevMech {
   const int *fg_ptr, *fg_rxn, *fg_prod;
   const double* fg_coef;
   const int *jg_ptr, *jg_part, *jg_ind, *jg_lupos, *jg_row;
+  const int* jac_colptr;  // solver Jacobian CSC column pointers
   const double* jg_coef;
   const int *lu_perm, *lu_rowptr, *lu_col, *lu_diag;
   const int *upd_ptr, *upd_src, *upd_dst;

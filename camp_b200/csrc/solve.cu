@@ -90,6 +90,17 @@ __device__ __forceinline__ double warp_min(double v) {
   return v;
 }
 __device__ __forceinline__ bool warp_any(bool p) { return __any_sync(FULLMASK, p) != 0; }
+__device__ __forceinline__ bool warp_all(bool p) { return __all_sync(FULLMASK, p) != 0; }
+__device__ __forceinline__ int warp_isum(int v) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULLMASK, v, o));
+  return v;
+}
 
 // value the reference's f sees for a solver variable: y above -SMALL is used
 // as is, anything else (only exactly -SMALL reaches here) becomes TINY
@@ -1344,6 +1355,122 @@ __global__ void eval_kernel(EvalArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Finite-difference audit of the analytic Jacobian (debug tool)
+// ---------------------------------------------------------------------------
+// The counterpart of the reference's check_Jac (src/camp_solver.c:1146-1257)
+// for one warp per cell: every element of column j of the solver Jacobian is
+// compared with a forward-difference estimate over steps dx = x_j * 10^-12
+// ... 10^0, as the reference's GSL forward derivative does: the differences
+// at dx and dx/2 give the Richardson estimate 2 D(dx/2) - D(dx) and an error
+// estimate (their difference plus the rounding of f, 4 eps (P + L) / (dx/2)
+// from the production and loss sums).  An element passes at the first step
+// where |J - estimate| < max(abs_tol, 1.2 error estimate) or the relative
+// difference is below rel_tol.  Columns whose concentration is below SMALL
+// are skipped, as in the reference.  Per cell: the number of elements that
+// never passed and the largest best-step relative difference among them.
+struct CheckArgs {
+  EvalArgs e;        // tables, layout, state, env, photo, h; e.jv: J scratch
+  double rel_tol, abs_tol;
+  double* best;      // [n_cells * n_jac] best relative difference per element
+  double* worst;     // [n_cells]
+  int* nfail;        // [n_cells]
+};
+
+__global__ void jac_check_kernel(CheckArgs c) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ unsigned long long tma_bar;
+  const EvalArgs& a = c.e;
+  if (!stage_tables(smem, a.blob, a.stage_bytes, &tma_bar, a.err)) return;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int cell = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (cell >= a.n_cells) return;
+  char* base = smem + a.tab_bytes + (size_t)wib * a.lay.bytes;
+  const Tab t = make_tab(smem);
+  const DevMech& m = a.m;
+  double* y = (double*)(base + a.lay.y);
+  double* f0 = (double*)(base + a.lay.ftemp);
+  double* f1 = (double*)(base + a.lay.tempv);
+  double* f2 = (double*)(base + a.lay.zn);
+  double* rp0 = (double*)(base + a.lay.acor);
+  double* rl0 = (double*)(base + a.lay.ewt);
+  double* rates = (double*)(base + a.lay.rates);
+  double* keff = (double*)(base + a.lay.keff);
+  double* fscr = (double*)(base + a.lay.fscr);
+  double* J = a.jv + (size_t)cell * t.n_jac;
+  double* best = c.best + (size_t)cell * t.n_jac;
+  const double* st = a.state + (size_t)cell * m.n_state;
+  #pragma unroll 1
+  for (int i = lane; i < t.n; i += 32) y[i] = st[t.dep_state[i]];
+  __syncwarp();
+  compute_keff(m, st, a.env[2 * cell], a.env[2 * cell + 1],
+               a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, keff, lane);
+  if (dev_f(smem, y, a.h, keff, rates, fscr, f0, lane, rp0, rl0) ||
+      dev_jac<double>(smem, y, a.h, keff, rates, J, lane)) {
+    if (lane == 0) {
+      c.nfail[cell] = -1;
+      c.worst[cell] = -1.0;
+    }
+    return;
+  }
+  #pragma unroll 1
+  for (int e = lane; e < t.n_jac; e += 32) best[e] = -1.0;  // -1: not checked
+  __syncwarp();
+  #pragma unroll 1
+  for (int j = 0; j < t.n; ++j) {
+    const double x = y[j];
+    if (x < kSmall) continue;
+    const int e0 = ldg(m.jac_colptr + j), e1 = ldg(m.jac_colptr + j + 1);
+    #pragma unroll 1
+    for (int e = e0 + lane; e < e1; e += 32) best[e] = 1.0e300;
+    __syncwarp();
+    #pragma unroll 1
+    for (double scale = 1.0e-12; scale <= 1.0; scale *= 10.0) {
+      const double dx = x * scale;
+      if (lane == 0) y[j] = x + dx;
+      __syncwarp();
+      int r = dev_f(smem, y, a.h, keff, rates, fscr, f1, lane);
+      if (lane == 0) y[j] = x + 0.5 * dx;
+      __syncwarp();
+      r |= dev_f(smem, y, a.h, keff, rates, fscr, f2, lane);
+      if (lane == 0) y[j] = x;
+      __syncwarp();
+      if (r) continue;
+      bool all = true;
+      #pragma unroll 1
+      for (int e = e0 + lane; e < e1; e += 32) {
+        const int i = ldg(m.jg_row + e);
+        const double d1 = (f1[i] - f0[i]) / dx, d2 = (f2[i] - f0[i]) / (0.5 * dx);
+        const double est = 2.0 * d2 - d1;
+        const double err = fabs(d1 - d2) + 4.0 * UROUND * (rp0[i] + rl0[i]) / (0.5 * dx);
+        const double diff = fabs(J[e] - est);
+        const double rel = est != 0.0 ? diff / fabs(est) : (diff == 0.0 ? 0.0 : 1.0);
+        const bool pass = diff < fmax(c.abs_tol, 1.2 * err) || rel < c.rel_tol;
+        best[e] = pass ? 0.0 : fmin(best[e], rel);
+        all &= best[e] == 0.0;
+      }
+      __syncwarp();
+      if (warp_all(all)) break;
+    }
+  }
+  int fails = 0;
+  double worst = 0.0;
+  #pragma unroll 1
+  for (int e = lane; e < t.n_jac; e += 32) {
+    if (best[e] > 0.0) {
+      ++fails;
+      worst = fmax(worst, best[e]);
+    }
+  }
+  fails = warp_isum(fails);
+  worst = warp_max(worst);
+  if (lane == 0) {
+    c.nfail[cell] = fails;
+    c.worst[cell] = worst;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side of the engine
 // ---------------------------------------------------------------------------
 #define CK(call)                                                        \
@@ -1484,6 +1611,7 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   pk.add(t.jg_ind, &m.jg_ind);
   pk.add(t.jg_lupos, &m.jg_lupos);
   pk.add(t.jg_row, &m.jg_row);
+  pk.add(model.solver_colptr(), &m.jac_colptr);
   pk.add(t.jg_coef, &m.jg_coef);
   pk.add(t.lu_perm, &m.lu_perm);
   pk.add(t.lu_rowptr, &m.lu_rowptr);
@@ -1957,6 +2085,81 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   cudaFree(dp);
   cudaFree(dout);
   return true;
+}
+
+bool Engine::check_jac(const double* h_state, const double* h_env, const double* h_photo,
+                       int n_cells, double h, double rel_tol, double abs_tol, double* worst,
+                       int* nfail, std::string* err) {
+  Impl* I = impl_;
+  const DevMech& m = I->m;
+  const size_t ns = (size_t)n_cells * m.n_state, nj = (size_t)n_cells * m.n_jac;
+  double *ds = nullptr, *de = nullptr, *dp = nullptr, *dj = nullptr, *db = nullptr,
+         *dw = nullptr;
+  int* dn = nullptr;
+  bool ok = false;
+  do {
+    if (cudaMalloc(&ds, sizeof(double) * ns) != cudaSuccess ||
+        cudaMalloc(&de, sizeof(double) * 2 * n_cells) != cudaSuccess ||
+        cudaMalloc(&dp, sizeof(double) * std::max<size_t>(1, (size_t)n_cells * m.n_photo)) !=
+            cudaSuccess ||
+        cudaMalloc(&dj, sizeof(double) * nj) != cudaSuccess ||
+        cudaMalloc(&db, sizeof(double) * nj) != cudaSuccess ||
+        cudaMalloc(&dw, sizeof(double) * n_cells) != cudaSuccess ||
+        cudaMalloc(&dn, sizeof(int) * n_cells) != cudaSuccess) {
+      *err = "check_jac: device allocation failed";
+      break;
+    }
+    cudaMemcpy(ds, h_state, sizeof(double) * ns, cudaMemcpyHostToDevice);
+    cudaMemcpy(de, h_env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice);
+    if (m.n_photo > 0 && h_photo)
+      cudaMemcpy(dp, h_photo, sizeof(double) * n_cells * m.n_photo, cudaMemcpyHostToDevice);
+    CheckArgs c{};
+    EvalArgs& a = c.e;
+    a.m = m;
+    a.off = I->off;
+    a.blob = I->d_blob;
+    a.tab_bytes = tab_bytes_of(I->off, 1);
+    a.stage_bytes = I->off.bytes;
+    a.err = I->d_counter + 1;
+    a.lay = make_layout(I->off, 8, true, true);
+    a.state = ds;
+    a.env = de;
+    a.photo = (m.n_photo > 0 && h_photo) ? dp : nullptr;
+    a.n_cells = n_cells;
+    a.h = h;
+    a.jv = dj;
+    c.rel_tol = rel_tol;
+    c.abs_tol = abs_tol;
+    c.best = db;
+    c.worst = dw;
+    c.nfail = dn;
+    const int warps = std::max(1, std::min(8, (I->max_smem - a.tab_bytes) / a.lay.bytes));
+    const size_t smem = (size_t)a.tab_bytes + (size_t)warps * a.lay.bytes;
+    if (cudaFuncSetAttribute(jac_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess) {
+      *err = "check_jac: shared memory attribute";
+      break;
+    }
+    jac_check_kernel<<<(n_cells + warps - 1) / warps, warps * 32, smem>>>(c);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      *err = std::string("check_jac: ") + cudaGetErrorString(e);
+      break;
+    }
+    ++launches_;
+    cudaMemcpy(worst, dw, sizeof(double) * n_cells, cudaMemcpyDeviceToHost);
+    cudaMemcpy(nfail, dn, sizeof(int) * n_cells, cudaMemcpyDeviceToHost);
+    ok = true;
+  } while (false);
+  cudaFree(ds);
+  cudaFree(de);
+  cudaFree(dp);
+  cudaFree(dj);
+  cudaFree(db);
+  cudaFree(dw);
+  cudaFree(dn);
+  return ok;
 }
 
 // ---------------------------------------------------------------------------

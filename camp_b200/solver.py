@@ -267,6 +267,20 @@ class Solver:
     def n_lu(self) -> int:
         return int(self.lib.camp_b200_n_lu_elem(self._h))
 
+    def check_jac(self, state, env, h: float, rel_tol: float = 1e-4, abs_tol: float = 1e-9):
+        """Finite-difference audit of the device Jacobian at these states;
+        returns (n_failed per cell, worst relative difference per cell)."""
+        state = np.ascontiguousarray(state, np.float64)
+        env = np.ascontiguousarray(env, np.float64)
+        nc = state.shape[0]
+        worst = np.zeros(nc, np.float64)
+        nfail = np.zeros(nc, np.int32)
+        if self.lib.camp_b200_check_jac(self._h, state.reshape(-1), env.reshape(-1), nc,
+                                        float(h), float(rel_tol), float(abs_tol), worst,
+                                        nfail) < 0:
+            raise SolverError(_lib.last_error())
+        return nfail, worst
+
     def eval_deriv(self, state, env, h):
         state = np.ascontiguousarray(state, np.float64)
         nc = state.shape[0]

@@ -287,6 +287,24 @@ int camp_b200_server_wait(void *server, long request, double *latency_ms,
 int camp_b200_server_pending(void *server);
 void camp_b200_server_free(void *server);
 
+/* ---------------------------------------------------------------------- */
+/* Debug: finite-difference audit of the analytic Jacobian                  */
+/* ---------------------------------------------------------------------- */
+
+/* replaces check_Jac (src/camp_solver.c:1146-1257, CAMP_DEBUG builds): for
+ * n_cells states (host buffers) and the photolysis rates set for those cells,
+ * compares every solver-Jacobian element at step size h with forward
+ * differences of f over steps x_j * 10^-12 .. 10^0 of its column's
+ * concentration (columns below 1e-30 skipped); an element passes at the
+ * first step where |J - FD| < abs_tol or the relative difference < rel_tol
+ * (the reference uses 1e-9 and 1e-4).  Per cell: n_failed = elements that
+ * never passed (-1 when f or J fails at the state), worst_rel = their
+ * largest best-step relative difference.  Returns the total of failed
+ * elements, or -1. */
+int camp_b200_check_jac(void *solver_data, const double *state, const double *env,
+                        int n_cells, double h, double rel_tol, double abs_tol,
+                        double *worst_rel, int *n_failed);
+
 #ifdef __cplusplus
 }
 #endif
