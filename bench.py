@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--max-steps", type=int, default=10000)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-1e5", action="store_true",
+                    help="skip the 1e5-cell single-host-step measurement")
     ap.add_argument("--no-cost-order", action="store_true",
                     help="fetch cells in index order instead of longest-first")
     ap.add_argument("--no-graph", action="store_true",
@@ -309,6 +311,54 @@ def serving_run(args, precision):
 
 
 # ---------------------------------------------------------------------------
+# 1e5 cells, one host step
+# ---------------------------------------------------------------------------
+def run_1e5(mech, args, dev, stream):
+    """The metric's cell count: 1e5 seeded cells over the first host step of
+    the sequence (the most expensive one: every cell starts from its seeded
+    state), mixed and FP64, device-resident, longest-first order from a
+    previous identical run; device time of the second run."""
+    import torch
+
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import FP64, MIXED, Solver
+
+    n = 100000
+    cells = make_cells(mech, n, SEED)
+    init = torch.from_numpy(cells.state).to(dev)
+    env = torch.from_numpy(cells.env).to(dev)
+    photo = torch.from_numpy(np.ascontiguousarray(cells.photo_rates)).to(dev)
+    out = {"cells": n, "host_step_s": args.dt,
+           "note": "first host step of the sequence, cells ordered longest-first from an "
+                   "identical previous run; device time (CUDA events)"}
+    for name, p in (("mixed", MIXED), ("fp64", FP64)):
+        s = Solver(mech, n)
+        s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4,
+                     max_steps=args.max_steps)
+        s.set_precision(p)
+        s.set_photo_rates_device(photo, n)
+        s.set_cost_ordering(True)
+        s.set_graph(not args.no_graph)
+        for rep in range(2):
+            st = init.clone()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.launch_device(st, env, n, 0.0, args.dt, stream)
+            e1.record(stream)
+            s.sync_status(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        nst = int(s.cell_stats(n)["nst"].sum())
+        out[name] = {"cell_steps_per_s": n / (ms / 1e3), "internal_steps_per_s": nst / (ms / 1e3),
+                     "ms": ms}
+        s.free()
+    out["mixed_over_fp64"] = out["mixed"]["cell_steps_per_s"] / out["fp64"]["cell_steps_per_s"]
+    return out
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args):
@@ -424,6 +474,9 @@ def run_gpu_arm(args):
     serving = None
     if world == 1 and not args.no_serving:
         serving = serving_run(args, prec)
+    at_1e5 = None
+    if world == 1 and not args.no_1e5:
+        at_1e5 = run_1e5(mech, args, dev, stream)
     if rank != 0:
         solver.free()
         replicas.finalize(world)
@@ -486,6 +539,7 @@ def run_gpu_arm(args):
         },
         "cpu_baseline": cb,
         "serving": serving,
+        "cells_1e5": at_1e5,
     }
     print(json.dumps(line), flush=True)
     solver.free()
