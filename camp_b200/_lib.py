@@ -49,7 +49,10 @@ EXPORTED = [
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
     "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
-    "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_server_new", "camp_b200_server_add_solver",
+    "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_solver_from_json",
+    "camp_b200_n_state_var", "camp_b200_state_name", "camp_b200_json_tolerances",
+    "camp_b200_get_var_type", "camp_b200_rxn_float_data_size", "camp_b200_get_rxn_float_data",
+    "camp_b200_server_new", "camp_b200_server_add_solver",
     "camp_b200_server_submit", "camp_b200_server_wait", "camp_b200_server_pending",
     "camp_b200_server_free",
 ]
@@ -130,6 +133,19 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_eval_deriv.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p, _f64p]
     lib.camp_b200_eval_jac.restype = ip
     lib.camp_b200_eval_jac.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p]
+    lib.camp_b200_solver_from_json.restype = vp
+    lib.camp_b200_solver_from_json.argtypes = [C.POINTER(C.c_char_p), ip, ip]
+    for name in ("camp_b200_n_state_var", "camp_b200_rxn_float_data_size"):
+        getattr(lib, name).restype = ip
+        getattr(lib, name).argtypes = [vp]
+    lib.camp_b200_state_name.restype = ip
+    lib.camp_b200_state_name.argtypes = [vp, ip, C.c_char_p, ip]
+    lib.camp_b200_json_tolerances.restype = ip
+    lib.camp_b200_json_tolerances.argtypes = [vp, _f64p, C.POINTER(C.c_double)]
+    lib.camp_b200_get_var_type.restype = ip
+    lib.camp_b200_get_var_type.argtypes = [vp, _i32p]
+    lib.camp_b200_get_rxn_float_data.restype = ip
+    lib.camp_b200_get_rxn_float_data.argtypes = [vp, _f64p]
     lib.camp_b200_check_jac.restype = ip
     lib.camp_b200_check_jac.argtypes = [vp, _f64p, _f64p, ip, dp, dp, dp, _f64p, _i32p]
     lib.camp_b200_server_new.restype = vp

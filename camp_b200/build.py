@@ -21,8 +21,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", "-lineinfo"]
 
-SOURCES = ["model.cpp", "blob.cpp", "capi.cpp", "serve.cpp", "solve.cu", "lanes.cu"]
-HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", "serve.hpp", "bdf_consts.hpp", "rates.cuh",
+SOURCES = ["model.cpp", "blob.cpp", "json.cpp", "loader.cpp", "capi.cpp", "serve.cpp", "solve.cu",
+           "lanes.cu"]
+HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", "json.hpp", "loader.hpp", "serve.hpp",
+           "bdf_consts.hpp", "rates.cuh",
            os.path.join("..", "..", "include", "camp_b200.h")]
 
 

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "loader.hpp"
 #include "model.hpp"
 #include "serve.hpp"
 
@@ -61,6 +62,10 @@ struct Solver {
   bool cost_order = false;
   double tuned_ms = -1.0;  // sample kernel time of the autotuned settings
   std::vector<int> order;
+  // state layout and tolerances of a solver created from CAMP JSON files
+  std::vector<std::string> state_names;
+  std::vector<double> json_abs_tol;
+  double json_rel_tol = 0.0;
 
   int photo_count() const {
     int c = 0;
@@ -801,5 +806,81 @@ int camp_b200_server_pending(void* server) {
 }
 
 void camp_b200_server_free(void* server) { delete static_cast<campb::Server*>(server); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// CAMP JSON input without the Fortran camp_core
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void* camp_b200_solver_from_json(const char* const* files, int n_files, int n_cells) {
+  if (!files || n_files <= 0 || n_cells <= 0) {
+    set_error("camp_b200_solver_from_json: no files or no cells");
+    return nullptr;
+  }
+  std::vector<std::string> paths;
+  for (int k = 0; k < n_files; ++k) paths.emplace_back(files[k] ? files[k] : "");
+  campb::LoadedMechanism lm;
+  std::string err;
+  if (!campb::load_mechanism_json(paths, &lm, &err)) {
+    set_error("camp_b200_solver_from_json: " + err);
+    return nullptr;
+  }
+  void* sd = solver_new((int)lm.species.size(), n_cells, lm.var_type.data(), (int)lm.rxns.size(),
+                        lm.n_int(), lm.n_float(), lm.n_env(), 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+  if (!sd) return nullptr;
+  for (auto& r : lm.rxns)
+    rxn_add_condensed_data(r.type, (int)r.ints.size(), (int)r.floats.size(), r.n_env,
+                           r.ints.data(), r.floats.data(), sd);
+  Solver* s = S(sd);
+  if (s->add_error) {
+    set_error("camp_b200_solver_from_json: " + s->add_error_msg);
+    solver_free(sd);
+    return nullptr;
+  }
+  s->state_names = lm.species;
+  s->json_abs_tol = lm.abs_tol;
+  s->json_rel_tol = lm.rel_tol;
+  return sd;
+}
+
+int camp_b200_n_state_var(void* solver_data) { return S(solver_data)->n_state; }
+
+int camp_b200_state_name(void* solver_data, int i, char* buf, int buf_len) {
+  Solver* s = S(solver_data);
+  if (i < 0 || i >= (int)s->state_names.size()) return -1;
+  const std::string& n = s->state_names[i];
+  if (buf && buf_len > 0) {
+    const int k = std::min<int>((int)n.size(), buf_len - 1);
+    std::memcpy(buf, n.data(), k);
+    buf[k] = '\0';
+  }
+  return (int)n.size();
+}
+
+int camp_b200_json_tolerances(void* solver_data, double* abs_tol, double* rel_tol) {
+  Solver* s = S(solver_data);
+  if (s->json_abs_tol.empty()) return -1;
+  if (abs_tol) std::copy(s->json_abs_tol.begin(), s->json_abs_tol.end(), abs_tol);
+  if (rel_tol) *rel_tol = s->json_rel_tol;
+  return 0;
+}
+
+int camp_b200_get_var_type(void* solver_data, int* out) {
+  Solver* s = S(solver_data);
+  std::copy(s->var_type.begin(), s->var_type.end(), out);
+  return 0;
+}
+
+int camp_b200_rxn_float_data_size(void* solver_data) {
+  return (int)S(solver_data)->model->rxn_float().size();
+}
+
+int camp_b200_get_rxn_float_data(void* solver_data, double* out) {
+  const Model& m = *S(solver_data)->model;
+  std::copy(m.rxn_float().begin(), m.rxn_float().end(), out);
+  return 0;
+}
 
 }  // extern "C"

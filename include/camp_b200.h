@@ -288,6 +288,30 @@ int camp_b200_server_pending(void *server);
 void camp_b200_server_free(void *server);
 
 /* ---------------------------------------------------------------------- */
+/* CAMP JSON input without the Fortran camp_core                            */
+/* ---------------------------------------------------------------------- */
+
+/* replaces the Fortran camp_core's input reading and reaction packing
+ * (src/camp_core.F90:303-798, src/chem_spec_data.F90, src/rxns/rxn_*.F90
+ * initialize) for gas-phase mechanisms: reads CAMP JSON files (CHEM_SPEC,
+ * MECHANISM and RELATIVE_TOLERANCE objects), orders the state (gas species
+ * in order of first appearance), packs every reaction and calls solver_new
+ * and rxn_add_condensed_data.  Photolysis reactions get the photolysis ids
+ * 1, 2, ... in mechanism order.  Then call solver_initialize (tolerances
+ * from camp_b200_json_tolerances) and solver_run.  NULL on error. */
+void *camp_b200_solver_from_json(const char *const *files, int n_files, int n_cells);
+int camp_b200_n_state_var(void *solver_data);
+/* name of state variable i into buf (NUL-terminated, truncated to buf_len);
+ * returns the full length, or -1 (no JSON layout or i out of range) */
+int camp_b200_state_name(void *solver_data, int i, char *buf, int buf_len);
+/* per-state-variable absolute tolerances and the relative tolerance read
+ * from the JSON files (defaults 1e-14 and 1e-8); -1 without a JSON layout */
+int camp_b200_json_tolerances(void *solver_data, double *abs_tol, double *rel_tol);
+int camp_b200_get_var_type(void *solver_data, int *out);
+int camp_b200_rxn_float_data_size(void *solver_data);
+int camp_b200_get_rxn_float_data(void *solver_data, double *out);
+
+/* ---------------------------------------------------------------------- */
 /* Debug: finite-difference audit of the analytic Jacobian                  */
 /* ---------------------------------------------------------------------- */
 

@@ -1,0 +1,128 @@
+"""The C++ reader/packer of CAMP JSON input (camp_b200_solver_from_json)
+against the Python packer: the same state layout, tolerances and packed
+reaction data, bit for bit (CPU only; no kernel runs)."""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from camp_b200 import _lib
+
+REF_CB05 = "/root/reference/mechanisms/cb05cl_ae5"
+
+
+def _cpp_solver(files, n_cells=2):
+    lib = _lib.load()
+    arr = (C.c_char_p * len(files))(*[f.encode() for f in files])
+    h = lib.camp_b200_solver_from_json(arr, len(files), n_cells)
+    assert h, _lib.last_error()
+    return lib, h
+
+
+def _compare(files):
+    from camp_b200.mechanism import load_mechanism
+    from camp_b200.solver import Solver
+
+    mech = load_mechanism(files)
+    lib, h = _cpp_solver(files)
+    try:
+        ns = lib.camp_b200_n_state_var(h)
+        assert ns == mech.n_state_var
+        buf = C.create_string_buffer(256)
+        names = []
+        for i in range(ns):
+            lib.camp_b200_state_name(h, i, buf, 256)
+            names.append(buf.value.decode())
+        assert names == mech.species
+        vt = np.zeros(ns, np.int32)
+        lib.camp_b200_get_var_type(h, vt)
+        np.testing.assert_array_equal(vt, mech.var_type)
+        at = np.zeros(ns)
+        rt = C.c_double()
+        assert lib.camp_b200_json_tolerances(h, at, C.byref(rt)) == 0
+        np.testing.assert_array_equal(at, mech.abs_tol)
+        assert rt.value == mech.rel_tol
+        # packed reaction data as added (before solver_initialize)
+        py = Solver(mech, 2)
+        ni = lib.camp_b200_rxn_int_data_size(h)
+        assert ni == py.lib.camp_b200_rxn_int_data_size(py._h)
+        a, b = np.zeros(ni, np.int32), np.zeros(ni, np.int32)
+        lib.camp_b200_get_rxn_int_data(h, a)
+        py.lib.camp_b200_get_rxn_int_data(py._h, b)
+        np.testing.assert_array_equal(a, b)
+        nf = lib.camp_b200_rxn_float_data_size(h)
+        fa, fb = np.zeros(nf), np.zeros(nf)
+        lib.camp_b200_get_rxn_float_data(h, fa)
+        py.lib.camp_b200_get_rxn_float_data(py._h, fb)
+        np.testing.assert_array_equal(fa, fb)
+        py.free()
+    finally:
+        lib.solver_free(h)
+
+
+def test_synthetic_mechanism(tmp_path):
+    from camp_b200.synth import write_synthetic
+
+    files, _ = write_synthetic(str(tmp_path), 60, 150, 3)
+    _compare(files)
+
+
+def test_every_gas_type_and_option(tmp_path):
+    """CMAQ types, Ea instead of C, minute time units, repeated reactants,
+    constant species, per-species tolerances, a relative tolerance, species
+    merged across files, mechanisms merged by name."""
+    sp1 = {"camp-data": [
+        {"name": "A", "type": "CHEM_SPEC", "absolute integration tolerance": 1e-6},
+        {"name": "B", "type": "CHEM_SPEC"},
+        {"name": "M", "type": "CHEM_SPEC", "tracer type": "CONSTANT"},
+        {"name": "RELTOL", "type": "RELATIVE_TOLERANCE", "value": 1e-5},
+    ]}
+    sp2 = {"camp-data": [
+        {"name": "C", "type": "CHEM_SPEC"},
+        {"name": "B", "type": "CHEM_SPEC", "description": "merged"},
+    ]}
+    mech = {"camp-data": [
+        {"name": "m", "type": "MECHANISM", "reactions": [
+            {"type": "ARRHENIUS", "reactants": {"A": {}, "B": {}}, "products": {"C": {"yield": 0.7}},
+             "Ea": 2.0e-20, "B": -1.5, "D": 250.0, "E": 1.0e-6, "rxn id": "r1"},
+            {"type": "ARRHENIUS", "reactants": {"B": {"qty": 2}}, "products": {"A": {}},
+             "A": 3.0, "time unit": "MIN"},
+            {"type": "TROE", "reactants": {"A": {}, "M": {}}, "products": {"B": {}},
+             "k0_A": 5e-30, "k0_B": -2.0, "kinf_A": 1e-11, "Fc": 0.5, "N": 1.2},
+        ]},
+        {"name": "m", "type": "MECHANISM", "reactions": [
+            {"type": "CMAQ_H2O2", "reactants": {"B": {"qty": 2}}, "products": {"C": {}},
+             "k1_A": 2.3e-13, "k1_C": 600.0, "k2_A": 1.7e-33, "k2_C": 1000.0},
+            {"type": "CMAQ_OH_HNO3", "reactants": {"A": {}, "C": {}}, "products": {"B": {}},
+             "k0_A": 2.4e-14, "k0_C": 460.0, "k2_A": 2.7e-17, "k2_C": 2199.0,
+             "k3_A": 6.5e-34, "k3_C": 1335.0},
+            {"type": "PHOTOLYSIS", "reactants": {"C": {}}, "products": {"A": {}, "B": {"yield": -0.5}},
+             "scaling factor": 2.0},
+        ]},
+    ]}
+    paths = []
+    for name, obj in (("sp1.json", sp1), ("sp2.json", sp2), ("mech.json", mech)):
+        p = os.path.join(tmp_path, name)
+        with open(p, "w") as fh:
+            json.dump(obj, fh)
+        paths.append(p)
+    _compare(paths)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_CB05), reason="reference tree not present")
+def test_cb05_from_reference_files():
+    _compare([os.path.join(REF_CB05, "cb05cl_ae5_species.json"),
+              os.path.join(REF_CB05, "cb05cl_ae5_mechanism.json")])
+
+
+def test_errors_are_reported(tmp_path):
+    p = os.path.join(tmp_path, "bad.json")
+    with open(p, "w") as fh:
+        fh.write('{"camp-data": [{"name": "m", "type": "MECHANISM", "reactions": '
+                 '[{"type": "ARRHENIUS", "reactants": {"X": {}}, "products": {}}]}]}')
+    lib = _lib.load()
+    arr = (C.c_char_p * 1)(p.encode())
+    assert not lib.camp_b200_solver_from_json(arr, 1, 1)
+    assert "Missing species: X" in _lib.last_error()
