@@ -1991,17 +1991,30 @@ int* Engine::d_order_buf(int n_cells, std::string* err) {
   return (int*)impl_->d_order;
 }
 
+// temporary device buffer of the evaluation hooks, freed on every return
+struct DevBuf {
+  double* p = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t n) { return cudaMalloc((void**)&p, sizeof(double) * std::max<size_t>(1, n)); }
+};
+
 bool Engine::eval_deriv(const double* h_state, const double* h_env, const double* h_photo,
                         int n_cells, double h, double* r_p, double* r_l, double* f,
                         std::string* err) {
   Impl* I = impl_;
   const DevMech& m = I->m;
   size_t ns = (size_t)n_cells * m.n_state, nn = (size_t)n_cells * m.n;
-  double *ds = nullptr, *de = nullptr, *dp = nullptr, *dout = nullptr;
-  CK(cudaMalloc(&ds, sizeof(double) * ns));
-  CK(cudaMalloc(&de, sizeof(double) * 2 * n_cells));
-  CK(cudaMalloc(&dp, sizeof(double) * std::max<size_t>(1, (size_t)n_cells * m.n_photo)));
-  CK(cudaMalloc(&dout, sizeof(double) * 3 * nn));
+  DevBuf bs, be, bp, bo;
+  CK(bs.alloc(ns));
+  CK(be.alloc(2 * (size_t)n_cells));
+  CK(bp.alloc((size_t)n_cells * m.n_photo));
+  CK(bo.alloc(3 * nn));
+  double *ds = bs.p, *de = be.p, *dp = bp.p, *dout = bo.p;
   CK(cudaMemcpy(ds, h_state, sizeof(double) * ns, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(de, h_env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice));
   if (m.n_photo > 0 && h_photo)
@@ -2033,10 +2046,6 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
   CK(cudaMemcpy(r_p, a.rp, sizeof(double) * nn, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(r_l, a.rl, sizeof(double) * nn, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(f, a.f, sizeof(double) * nn, cudaMemcpyDeviceToHost));
-  cudaFree(ds);
-  cudaFree(de);
-  cudaFree(dp);
-  cudaFree(dout);
   return true;
 }
 
@@ -2045,11 +2054,12 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   Impl* I = impl_;
   const DevMech& m = I->m;
   size_t ns = (size_t)n_cells * m.n_state, nj = (size_t)n_cells * m.n_jac;
-  double *ds = nullptr, *de = nullptr, *dp = nullptr, *dout = nullptr;
-  CK(cudaMalloc(&ds, sizeof(double) * ns));
-  CK(cudaMalloc(&de, sizeof(double) * 2 * n_cells));
-  CK(cudaMalloc(&dp, sizeof(double) * std::max<size_t>(1, (size_t)n_cells * m.n_photo)));
-  CK(cudaMalloc(&dout, sizeof(double) * 3 * nj));
+  DevBuf bs, be, bp, bo;
+  CK(bs.alloc(ns));
+  CK(be.alloc(2 * (size_t)n_cells));
+  CK(bp.alloc((size_t)n_cells * m.n_photo));
+  CK(bo.alloc(3 * nj));
+  double *ds = bs.p, *de = be.p, *dp = bp.p, *dout = bo.p;
   CK(cudaMemcpy(ds, h_state, sizeof(double) * ns, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(de, h_env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice));
   if (m.n_photo > 0 && h_photo)
@@ -2080,10 +2090,6 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   CK(cudaDeviceSynchronize());
   CK(cudaMemcpy(jp, a.jp, sizeof(double) * nj, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(jl, a.jl, sizeof(double) * nj, cudaMemcpyDeviceToHost));
-  cudaFree(ds);
-  cudaFree(de);
-  cudaFree(dp);
-  cudaFree(dout);
   return true;
 }
 
