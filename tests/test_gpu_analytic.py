@@ -1,0 +1,75 @@
+"""Each gas-phase reaction type on the GPU against a closed-form solution.
+
+The reference's per-reaction tests integrate A -> B -> C with two reactions
+of one type and compare with the analytic solution
+(test/unit_rxn_data/test_rxn_troe.F90, test_rxn_CMAQ_H2O2.F90,
+test_rxn_CMAQ_OH_HNO3.F90, test_rxn_photolysis.F90,
+test/unit_tests/rxns/unit_test_rxn_arrhenius.F90).  Here the same chain runs
+through the C ABI in both precision forms.  The rate constants come from the
+oracle's rate-constant code, which is pinned to the reference's C by the
+golden fixture, so the comparison checks the device integrator:
+
+    A = exp(-k1 t),  B = k1 / (k2 - k1) (exp(-k1 t) - exp(-k2 t)),  C = 1 - A - B.
+"""
+import numpy as np
+import pytest
+
+from conftest import (CHAIN_CASES, CHAIN_ENV, CHAIN_PHOTO, chain_closed_form, chain_mechanism,
+                      chain_rates, gpu_available)
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="no CUDA device")]
+
+TIMES = (5.0, 20.0, 60.0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("rtype", list(CHAIN_CASES))
+def test_two_step_chain_matches_closed_form(tmp_path, rtype, precision):
+    from camp_b200.solver import Solver
+
+    mech, _ = chain_mechanism(tmp_path, rtype)
+    k1, k2 = chain_rates(mech, rtype)
+    n = len(TIMES)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.full(3, 1e-14), rel_tol=1e-9, max_steps=100000)
+    s.set_precision(precision)
+    if rtype == "PHOTOLYSIS":
+        s.set_photo_rates(np.tile(np.array(CHAIN_PHOTO), (n, 1)))
+    env = np.tile(np.array(CHAIN_ENV), (n, 1))
+    out = np.zeros((n, 3))
+    for c, t in enumerate(TIMES):  # one run per end time; cell c is kept from run c
+        x = np.tile(np.array([1.0, 0.0, 0.0]), (n, 1))
+        assert s.solve(x, env, 0.0, t) == 0, s.cell_stats()["status"]
+        out[c] = x[c]
+    np.testing.assert_allclose(out, chain_closed_form(k1, k2, TIMES), rtol=1e-6, atol=1e-12)
+
+
+@pytest.mark.parametrize("rtype", ["ARRHENIUS", "PHOTOLYSIS"])
+def test_chain_through_json_entry_point(tmp_path, rtype):
+    """The same chain built by the C++ JSON reader (camp_b200_solver_from_json)
+    instead of the Python packer."""
+    import ctypes as C
+
+    from camp_b200 import _lib
+
+    mech, files = chain_mechanism(tmp_path, rtype)
+    k1, k2 = chain_rates(mech, rtype)
+    lib = _lib.load()
+    paths = (C.c_char_p * len(files))(*[f.encode() for f in files])
+    n = 2
+    h = lib.camp_b200_solver_from_json(paths, len(files), n)
+    assert h, _lib.last_error()
+    try:
+        lib.solver_initialize(h, np.full(3, 1e-14), 1e-9, 100000, 1000)
+        assert lib.camp_b200_is_ready(h), _lib.last_error()
+        if rtype == "PHOTOLYSIS":
+            rates = np.ascontiguousarray(np.tile(np.array(CHAIN_PHOTO), (n, 1)).reshape(-1))
+            lib.camp_b200_set_photo_rates(h, rates, n)
+        state = np.ascontiguousarray(np.tile(np.array([1.0, 0.0, 0.0]), (n, 1)))
+        env = np.ascontiguousarray(np.tile(np.array(CHAIN_ENV), (n, 1)))
+        assert lib.solver_run(h, state.reshape(-1), env.reshape(-1), 0.0, 30.0) == 0
+    finally:
+        lib.solver_free(h)
+    np.testing.assert_allclose(state, np.tile(chain_closed_form(k1, k2, [30.0]), (n, 1)),
+                               rtol=1e-6, atol=1e-12)

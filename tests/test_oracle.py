@@ -117,6 +117,28 @@ def test_bdf_consecutive_first_order(cb05):
     np.testing.assert_allclose(out[0], [A, B, C], rtol=1e-7, atol=1e-12)
 
 
+@pytest.mark.parametrize("rtype", ["ARRHENIUS", "TROE", "CMAQ_H2O2", "CMAQ_OH_HNO3",
+                                   "PHOTOLYSIS"])
+def test_bdf_chain_per_reaction_type(tmp_path, rtype):
+    """The A -> B -> C chain of every gas-phase type, read from CAMP JSON,
+    against the closed form; the GPU counterpart runs the same chains."""
+    from conftest import CHAIN_ENV, CHAIN_PHOTO, chain_closed_form, chain_mechanism, chain_rates
+
+    mech, _ = chain_mechanism(tmp_path, rtype)
+    k1, k2 = chain_rates(mech, rtype)
+    assert 1e-2 < k1 < 1.0 and 1e-2 < k2 < 1.0 and abs(k1 - k2) > 1e-2
+    photo = np.array([CHAIN_PHOTO]) if rtype == "PHOTOLYSIS" else np.zeros((1, 0))
+    out = []
+    for t in (5.0, 60.0):
+        nf, status, _, x = OracleModel(mech).solve(np.array([[1.0, 0.0, 0.0]]),
+                                                   np.array([CHAIN_ENV]), photo, 0.0, t, 1e-9,
+                                                   np.full(3, 1e-14), max_steps=100000)
+        assert nf == 0
+        out.append(x[0])
+    np.testing.assert_allclose(out, chain_closed_form(k1, k2, [5.0, 60.0]), rtol=1e-7,
+                               atol=1e-12)
+
+
 def test_zero_length_step_is_too_close(cb05):
     """CVODE refuses tout == t0 when it must estimate the initial step
     (cvHin: CV_TOO_CLOSE, -27); the cell keeps its input."""
