@@ -39,12 +39,15 @@ EXPORTED = [
     "solver_set_debug_out", "solver_set_eval_jac", "rxn_add_condensed_data",
     "rxn_update_data", "rxn_print_data", "rxn_free_update_data",
     "rxn_photolysis_create_rate_update_data", "rxn_photolysis_set_rate_update_data",
+    "rxn_emission_create_rate_update_data", "rxn_emission_set_rate_update_data",
+    "rxn_first_order_loss_create_rate_update_data", "rxn_first_order_loss_set_rate_update_data",
+    "rxn_wet_deposition_create_rate_update_data", "rxn_wet_deposition_set_rate_update_data",
     "aero_phase_add_condensed_data", "aero_rep_add_condensed_data", "aero_rep_update_data",
     "sub_model_add_condensed_data", "sub_model_update_data", "aero_phase_print_data",
     "aero_rep_print_data", "sub_model_print_data",
     "camp_b200_last_error", "camp_b200_is_ready", "camp_b200_set_precision",
     "camp_b200_set_launch", "camp_b200_set_lu_mode", "camp_b200_set_kernel", "camp_b200_set_layout", "camp_b200_set_graph", "camp_b200_autotune", "camp_b200_get_tuning", "camp_b200_set_cost_ordering", "camp_b200_run_device",
-    "camp_b200_launch_device", "camp_b200_sync_status", "camp_b200_run_device_noalloc", "camp_b200_n_photo",
+    "camp_b200_launch_device", "camp_b200_sync_status", "camp_b200_run_device_noalloc", "camp_b200_n_photo", "camp_b200_rate_column",
     "camp_b200_set_photo_rates", "camp_b200_set_photo_rates_device", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
@@ -82,8 +85,9 @@ def load(path: str = LIB_PATH):
     lib.solver_free_update_data.argtypes = [vp]
     lib.rxn_add_condensed_data.argtypes = [ip, ip, ip, ip, _i32p, _f64p, vp]
     lib.rxn_update_data.argtypes = [ip, C.POINTER(C.c_int), ip, vp, vp]
-    lib.rxn_photolysis_create_rate_update_data.restype = vp
-    lib.rxn_photolysis_set_rate_update_data.argtypes = [vp, ip, dp]
+    for kind in ("photolysis", "emission", "first_order_loss", "wet_deposition"):
+        getattr(lib, f"rxn_{kind}_create_rate_update_data").restype = vp
+        getattr(lib, f"rxn_{kind}_set_rate_update_data").argtypes = [vp, ip, dp]
     lib.camp_b200_last_error.restype = C.c_char_p
     lib.camp_b200_is_ready.restype = ip
     lib.camp_b200_is_ready.argtypes = [vp]
@@ -113,6 +117,8 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_sync_status.argtypes = [vp, vp]
     lib.camp_b200_n_photo.restype = ip
     lib.camp_b200_n_photo.argtypes = [vp]
+    lib.camp_b200_rate_column.restype = ip
+    lib.camp_b200_rate_column.argtypes = [vp, ip] + [C.POINTER(C.c_int)] * 3
     lib.camp_b200_set_photo_rates.argtypes = [vp, _f64p, ip]
     lib.camp_b200_set_photo_rates_device.restype = ip
     lib.camp_b200_set_photo_rates_device.argtypes = [vp, vp, ip]

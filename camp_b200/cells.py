@@ -7,6 +7,10 @@ Per-cell inputs follow the documented workload distributions:
   [0, 1] (the day/night stiffness spread).  The cb05cl_ae5 base set is the
   reference cb05 test's 1e-4 s^-1 for every photolysis reaction except jo2,
   which is 0 (``test/chemistry/cb05cl_ae5/test_cb05cl_ae5.F90:349-362``);
+* the other host-set rates (emission in ppm s^-1, first-order loss and wet
+  deposition in s^-1) = a fixed base set x a second per-cell factor uniform
+  in [0.5, 1.5], drawn after everything else so that mechanisms without such
+  reactions keep their streams;
 * initial concentrations of variable species log-uniform in
   [conc_lo, conc_hi] ppm; constant species keep their "init conc" value.
 
@@ -18,14 +22,22 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .mechanism import CHEM_SPEC_VARIABLE, RXN_PHOTOLYSIS, Mechanism
+from .mechanism import (CHEM_SPEC_VARIABLE, RXN_EMISSION, RXN_FIRST_ORDER_LOSS, RXN_PHOTOLYSIS,
+                        RXN_WET_DEPOSITION, Mechanism)
+
+# base rates of the non-photolysis host-rate types: a surface emission
+# tendency (ppm s^-1) and dry / wet deposition rate constants (s^-1)
+EMISSION_BASE = 1.0e-8
+FIRST_ORDER_LOSS_BASE = 2.0e-5
+WET_DEPOSITION_BASE = 1.0e-4
 
 
 @dataclass
 class CellBatch:
     state: np.ndarray  # [n_cells, n_state_var] float64
     env: np.ndarray  # [n_cells, 2] (T K, P Pa)
-    photo_rates: np.ndarray  # [n_cells, n_photo] base rates for ids 1..n_photo
+    photo_rates: np.ndarray  # [n_cells, n_photo] host-set base rates, one column per
+    #                          host-rate reaction (Mechanism.rate_rxns order)
     seed: int
 
     @property
@@ -37,13 +49,25 @@ class CellBatch:
 
 
 def photo_base_rates(mech: Mechanism, base: float = 1.0e-4, zero_labels=("jo2",)) -> np.ndarray:
-    """Base rate per photolysis id (index id-1), 0 for the listed reactions."""
-    n_photo = len(mech.photo_ids)
-    out = np.full(n_photo, base, dtype=np.float64)
-    for pid, ridx in mech.photo_ids.items():
-        if mech.rxns[ridx].label in zero_labels:
-            out[pid - 1] = 0.0
+    """Base rate per host-rate column: ``base`` for photolysis (0 for the
+    listed reactions), the module's emission / deposition bases otherwise."""
+    other = {RXN_EMISSION: EMISSION_BASE, RXN_FIRST_ORDER_LOSS: FIRST_ORDER_LOSS_BASE,
+             RXN_WET_DEPOSITION: WET_DEPOSITION_BASE}
+    cols = mech.rate_rxns()
+    out = np.zeros(len(cols), dtype=np.float64)
+    for j, ridx in enumerate(cols):
+        r = mech.rxns[ridx]
+        if r.rxn_type == RXN_PHOTOLYSIS:
+            out[j] = 0.0 if r.label in zero_labels else base
+        else:
+            out[j] = other[r.rxn_type]
     return out
+
+
+def photolysis_columns(mech: Mechanism) -> np.ndarray:
+    """Mask of the host-rate columns that are photolysis reactions."""
+    return np.asarray([mech.rxns[i].rxn_type == RXN_PHOTOLYSIS for i in mech.rate_rxns()],
+                      dtype=bool)
 
 
 def make_cells(
@@ -78,6 +102,10 @@ def make_cells(
             v = float(mech.species_props[name]["init conc"])
         state[:, i] = 0.0 if v is None else v
     env = np.stack([T, P], axis=1)
+    is_photo = photolysis_columns(mech)
+    if photo.shape[1] and not is_photo.all():
+        other = rng.uniform(0.5, 1.5, n_cells)
+        photo[:, ~is_photo] = other[:, None] * np.asarray(photo_base)[None, ~is_photo]
     return CellBatch(state=state, env=env, photo_rates=photo, seed=seed)
 
 
@@ -93,4 +121,5 @@ def constant_values(mech: Mechanism) -> dict[str, float]:
 
 
 def n_photo(mech: Mechanism) -> int:
-    return sum(1 for r in mech.rxns if r.rxn_type == RXN_PHOTOLYSIS)
+    """Host-rate columns of a mechanism."""
+    return len(mech.rate_rxns())

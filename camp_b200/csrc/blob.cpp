@@ -97,11 +97,12 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   for (int i = 0; i < n; ++i) {
     for (int g = 0; g < 3; ++g) {
       for (int e = t.fg_ptr[i]; e < t.fg_ptr[i + 1]; ++e) {
-        const int eg = !t.fg_prod[e] ? 0 : (t.fg_coef[e] >= 0.0 ? 1 : 2);
+        const int eg = t.fg_prod[e] == FG_LOSS ? 0 : (t.fg_coef[e] >= 0.0 ? 1 : 2);
         if (eg != g) continue;
         int c = coef_id(t.fg_coef[e]);
+        // bit 31: the term is guarded (a product; not a loss or a source)
         fg_ent.push_back((uint32_t)t.fg_rxn[e] | ((uint32_t)c << 16) |
-                         ((uint32_t)(t.fg_prod[e] ? 1 : 0) << 31));
+                         ((uint32_t)(t.fg_prod[e] == FG_PRODUCT ? 1 : 0) << 31));
       }
       if (g < 2) grp_end[2 * i + g] = (int)fg_ent.size();
     }
@@ -353,13 +354,19 @@ bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
   std::vector<std::vector<int>> pos(n, std::vector<int>(n, -1));
   for (int i = 0; i < n; ++i)
     for (int q = t.lu_rowptr[i]; q < t.lu_rowptr[i + 1]; ++q) pos[i][t.lu_col[q]] = q;
-  // participants in reaction order: the variable reactant occurrences
-  // (rx_vdep), then the variable products (recovered from the f gather
-  // lists, which hold every product of a reaction with its yield)
-  std::vector<std::vector<std::pair<int, double>>> prods(t.n_rxn);
+  // participants in term order: the variable reactant occurrences
+  // (rx_vdep), then the variable products and sources (recovered from the f
+  // gather lists, which hold every product of a term with its yield)
+  struct Gain {
+    int d;
+    double c;
+    bool guarded;
+  };
+  std::vector<std::vector<Gain>> prods(t.n_rxn);
   for (int d = 0; d < n; ++d)
     for (int e = t.fg_ptr[d]; e < t.fg_ptr[d + 1]; ++e)
-      if (t.fg_prod[e]) prods[t.fg_rxn[e]].push_back({d, t.fg_coef[e]});
+      if (t.fg_prod[e] != FG_LOSS)
+        prods[t.fg_rxn[e]].push_back({d, t.fg_coef[e], t.fg_prod[e] == FG_PRODUCT});
   std::vector<uint32_t> rx_word(t.n_rxn), rx_part;
   std::vector<uint16_t> rx_pptr(t.n_rxn + 1), rx_jptr(t.n_rxn + 1), jpos;
   for (int r = 0; r < t.n_rxn; ++r) {
@@ -377,9 +384,10 @@ bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
       rx_part.push_back((uint32_t)t.rx_vdep[k] | ((uint32_t)coef_id(-1.0) << 10));
       sp.push_back(t.rx_vdep[k]);
     }
-    for (auto& pr : prods[r]) {
-      rx_part.push_back((uint32_t)pr.first | ((uint32_t)coef_id(pr.second) << 10) | (1u << 31));
-      sp.push_back(pr.first);
+    for (const Gain& pr : prods[r]) {
+      rx_part.push_back((uint32_t)pr.d | ((uint32_t)coef_id(pr.c) << 10) |
+                        ((pr.guarded ? 1u : 0u) << 31));
+      sp.push_back(pr.d);
     }
     rx_jptr[r] = (uint16_t)jpos.size();
     for (int k = v0; k < v1; ++k) {

@@ -45,7 +45,9 @@ struct Solver {
   int n_aero_phase_added = 0, n_aero_rep_added = 0, n_sub_model_added = 0;
   bool add_error = false;
   std::string add_error_msg;
-  // per-cell photolysis base rates [n_cells * n_photo]
+  // per-cell host-set base rates [n_cells * n_photo]: one column per
+  // reaction of a host-rate type (PHOTOLYSIS, FIRST_ORDER_LOSS, EMISSION,
+  // WET_DEPOSITION) in mechanism order
   std::vector<double> photo;
   int n_photo = 0;
   // device-resident photolysis rates set by camp_b200_set_photo_rates_device
@@ -67,12 +69,7 @@ struct Solver {
   std::vector<double> json_abs_tol;
   double json_rel_tol = 0.0;
 
-  int photo_count() const {
-    int c = 0;
-    for (const auto& r : model->rxns())
-      if (r.type == campb::RXN_PHOTOLYSIS) ++c;
-    return c;
-  }
+  int photo_count() const { return model->n_host_rate(); }
   void ensure_photo() {
     int np = photo_count();
     if (np != n_photo || photo.size() != (size_t)np * n_cells) {
@@ -357,48 +354,75 @@ void solver_free(void* solver_data) {
 void solver_free_update_data(void* update_data) { free(update_data); }
 void rxn_free_update_data(void* update_data) { free(update_data); }
 
-void* rxn_photolysis_create_rate_update_data(void) {
+namespace {
+// Update data of the host-rate types: an int reaction id followed, unaligned,
+// by the double base rate (src/rxns/rxn_photolysis.c:262-283,
+// rxn_emission.c:192-213, rxn_first_order_loss.c:208-229,
+// rxn_wet_deposition.c:218-239).
+void* create_rate_update_data(const char* what) {
   void* p = malloc(sizeof(int) + sizeof(double));
   if (!p) {
-    set_error("out of memory allocating photolysis update data");
+    set_error(std::string("out of memory allocating ") + what + " update data");
     exit(1);
   }
   return p;
 }
-
-// layout of src/rxns/rxn_photolysis.c:262-283: an int photo id followed,
-// unaligned, by the double base rate
-void rxn_photolysis_set_rate_update_data(void* update_data, int photo_id, double base_rate) {
-  memcpy(update_data, &photo_id, sizeof(int));
+void set_rate_update_data(void* update_data, int rxn_id, double base_rate) {
+  memcpy(update_data, &rxn_id, sizeof(int));
   memcpy((char*)update_data + sizeof(int), &base_rate, sizeof(double));
 }
+}  // namespace
 
+void* rxn_photolysis_create_rate_update_data(void) {
+  return create_rate_update_data("photolysis");
+}
+void rxn_photolysis_set_rate_update_data(void* update_data, int photo_id, double base_rate) {
+  set_rate_update_data(update_data, photo_id, base_rate);
+}
+void* rxn_emission_create_rate_update_data(void) { return create_rate_update_data("emission"); }
+void rxn_emission_set_rate_update_data(void* update_data, int rxn_id, double base_rate) {
+  set_rate_update_data(update_data, rxn_id, base_rate);
+}
+void* rxn_first_order_loss_create_rate_update_data(void) {
+  return create_rate_update_data("first-order loss");
+}
+void rxn_first_order_loss_set_rate_update_data(void* update_data, int rxn_id,
+                                               double base_rate) {
+  set_rate_update_data(update_data, rxn_id, base_rate);
+}
+void* rxn_wet_deposition_create_rate_update_data(void) {
+  return create_rate_update_data("wet deposition");
+}
+void rxn_wet_deposition_set_rate_update_data(void* update_data, int rxn_id, double base_rate) {
+  set_rate_update_data(update_data, rxn_id, base_rate);
+}
+
+// The reference walks the reactions from *rxn_id and stops at the first one
+// of update_rxn_type whose RXN_ID_ matches (> 0), leaving *rxn_id on it
+// (src/rxn_solver.c:700-760).  Here the match sets that reaction's column of
+// the cell's host-set base rates.
 void rxn_update_data(int cell_id, int* rxn_id, int update_rxn_type, void* update_data,
                      void* solver_data) {
   Solver* s = S(solver_data);
   if (cell_id < 0 || cell_id >= s->n_cells) return;
   const auto& rx = s->model->rxns();
   const int n_rxn = (int)rx.size();
-  if (update_rxn_type != campb::RXN_PHOTOLYSIS) {
-    // emission, first-order loss, wet deposition and condensed-phase
-    // photolysis updates have no reaction of that type here
+  if (!campb::host_rate_type(update_rxn_type)) {
+    // condensed-phase photolysis updates have no reaction of that type here
     *rxn_id = n_rxn;
     return;
   }
   s->ensure_photo();
-  int photo_id;
+  int id;
   double base;
-  memcpy(&photo_id, update_data, sizeof(int));
+  memcpy(&id, update_data, sizeof(int));
   memcpy(&base, (char*)update_data + sizeof(int), sizeof(double));
+  const auto& slot = s->model->photo_slot();
   for (; *rxn_id < n_rxn; (*rxn_id)++) {
-    const auto& r = rx[*rxn_id];
-    if (r.type != update_rxn_type) continue;
-    int rid = s->model->rxn_int()[r.int_off + 2];
-    if (photo_id == rid && rid > 0) {
-      int slot = 0;
-      for (int i = 0; i < *rxn_id; ++i)
-        if (rx[i].type == campb::RXN_PHOTOLYSIS) ++slot;
-      s->photo[(size_t)cell_id * s->n_photo + slot] = base;
+    if (rx[*rxn_id].type != update_rxn_type) continue;
+    const int rid = s->model->photo_id(*rxn_id);
+    if (id == rid && rid > 0) {
+      s->photo[(size_t)cell_id * s->n_photo + slot[*rxn_id]] = base;
       return;
     }
   }
@@ -407,10 +431,20 @@ void rxn_update_data(int cell_id, int* rxn_id, int update_rxn_type, void* update
 void rxn_print_data(void* solver_data) {
   Solver* s = S(solver_data);
   printf("\n\nReaction data\n\nnumber of reactions: %d\n\n", s->n_rxn);
-  static const char* names[] = {"", "Arrhenius", "Troe", "CMAQ_H2O2", "CMAQ_OH_HNO3",
-                                "Photolysis"};
-  for (const auto& r : s->model->rxns())
-    printf("\n\n%s reaction\n", (r.type >= 1 && r.type <= 5) ? names[r.type] : "Unknown");
+  for (const auto& r : s->model->rxns()) {
+    const char* name = "Unknown";
+    switch (r.type) {
+      case campb::RXN_ARRHENIUS: name = "Arrhenius"; break;
+      case campb::RXN_TROE: name = "Troe"; break;
+      case campb::RXN_CMAQ_H2O2: name = "CMAQ_H2O2"; break;
+      case campb::RXN_CMAQ_OH_HNO3: name = "CMAQ_OH_HNO3"; break;
+      case campb::RXN_PHOTOLYSIS: name = "Photolysis"; break;
+      case campb::RXN_FIRST_ORDER_LOSS: name = "First-Order loss"; break;
+      case campb::RXN_EMISSION: name = "Emission"; break;
+      case campb::RXN_WET_DEPOSITION: name = "Wet Deposition"; break;
+    }
+    printf("\n\n%s reaction\n", name);
+  }
   fflush(stdout);
 }
 void aero_phase_print_data(void* solver_data) {
@@ -619,6 +653,23 @@ int camp_b200_n_photo(void* solver_data) {
   Solver* s = S(solver_data);
   s->ensure_photo();
   return s->n_photo;
+}
+
+int camp_b200_rate_column(void* solver_data, int column, int* rxn_index, int* rxn_type,
+                          int* rxn_id) {
+  Solver* s = S(solver_data);
+  if (!s || !s->model) return -1;
+  const auto& slot = s->model->photo_slot();
+  const auto& rx = s->model->rxns();
+  for (int i = 0; i < (int)rx.size(); ++i)
+    if (slot[i] == column && column >= 0) {
+      if (rxn_index) *rxn_index = i;
+      if (rxn_type) *rxn_type = rx[i].type;
+      if (rxn_id) *rxn_id = s->model->photo_id(i);
+      return 0;
+    }
+  set_error("no host-rate column " + std::to_string(column));
+  return -1;
 }
 
 int camp_b200_set_photo_rates(void* solver_data, const double* rates, int n_cells) {

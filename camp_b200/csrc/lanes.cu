@@ -210,7 +210,7 @@ __device__ __noinline__ int op_jac(const char* tb, LS<LT>* s, const double* y, d
       for (int p = 0; p < np; ++p, ++jp) {
         const uint32_t pe = t.rx_part[p0 + p];
         const int pos = t.jpos[jp];
-        if (!(pe >> 31)) {
+        if (!(pe >> 31)) {  // a loss (sources have no reactants, so never reach here)
           AT(J, pos) -= part;
         } else {
           const double c = t.coef[(pe >> 10) & 0x7FFFu];

@@ -15,6 +15,7 @@ namespace {
 constexpr int kUnknown = 0, kVariable = 1, kConstant = 2, kPssa = 3, kActivity = 4;
 // reaction type ids, src/rxn_solver.c:19-35
 constexpr int kArrhenius = 1, kTroe = 2, kCmaqH2O2 = 3, kCmaqOHHNO3 = 4, kPhotolysis = 5;
+constexpr int kFirstOrderLoss = 12, kEmission = 13, kWetDeposition = 14;
 // physical constants, src/constants.F90:37-41
 constexpr double kBoltzmann = 1.3806505e-23;
 constexpr double kAvogadro = 6.02214179e23;
@@ -218,6 +219,26 @@ bool pack_reaction(const Json& r, const std::map<std::string, int>& gas_index, L
     out->type = kPhotolysis;
     out->ints = int_block(3, {-1}, react, prod);
     out->n_env = 2;
+  } else if (type == "FIRST_ORDER_LOSS" || type == "EMISSION") {
+    // src/rxns/rxn_first_order_loss.F90:169-220, rxn_emission.F90:166-217:
+    // one gas species, RXN_ID_ = -1 until the host creates update data
+    const bool loss = type == "FIRST_ORDER_LOSS";
+    const Json* js = r.get("species");
+    if (!js || js->kind != Json::String) {
+      *err = std::string(loss ? "First-Order Loss" : "Emission") +
+             " reaction is missing species name";
+      return false;
+    }
+    int id;
+    if (!gas_id(js->str, &id)) return false;
+    f = {num("scaling factor", 1.0)};
+    out->type = loss ? kFirstOrderLoss : kEmission;
+    out->ints = loss ? std::vector<int>{-1, id, 0, 0} : std::vector<int>{-1, id, 0};
+    out->n_env = 2;
+  } else if (type == "WET_DEPOSITION") {
+    *err = "WET_DEPOSITION removes the species of an aerosol phase, and aerosol phases are "
+           "not read from JSON here; add it as packed data (rxn_add_condensed_data)";
+    return false;
   } else {
     *err = "reaction type " + type + " is not supported";
     return false;
@@ -311,9 +332,15 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
       if (!pack_reaction(*r, gas_index, &lr, err)) return false;
       out->rxns.push_back(std::move(lr));
     }
+  // reaction ids of the host-rate types: one sequence in mechanism order, as
+  // generate_int_id (src/rand.F90:644-656) hands them out when the host
+  // creates one update object per such reaction in that order
   int next_id = 1;
-  for (auto& r : out->rxns)
+  for (auto& r : out->rxns) {
     if (r.type == kPhotolysis) r.ints[2] = next_id++;
+    if (r.type == kFirstOrderLoss || r.type == kEmission || r.type == kWetDeposition)
+      r.ints[0] = next_id++;
+  }
   out->name = mechs.empty() ? "mechanism" : mechs[0].first;
   return true;
 }

@@ -31,7 +31,8 @@ struct LoadedMechanism {
 
 // Reads CAMP JSON files ({"camp-data": [...]} with CHEM_SPEC, MECHANISM and
 // RELATIVE_TOLERANCE objects) and packs the gas-phase reactions.
-// Photolysis reactions get ids 1, 2, ... in mechanism order.
+// Reactions whose rate the host sets (PHOTOLYSIS, FIRST_ORDER_LOSS,
+// EMISSION) get ids 1, 2, ... in mechanism order.
 bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism* out,
                          std::string* err);
 

@@ -8,7 +8,8 @@
 namespace campb {
 
 namespace {
-// NUM_INT_PROP_ / NUM_FLOAT_PROP_ of the gas types (src/rxns/rxn_*.c headers)
+// NUM_INT_PROP_ / NUM_FLOAT_PROP_ of the supported types (src/rxns/rxn_*.c
+// headers)
 bool type_layout(int type, int* n_int_prop, int* n_float_prop) {
   switch (type) {
     case RXN_ARRHENIUS: *n_int_prop = 2; *n_float_prop = 6; return true;
@@ -16,6 +17,9 @@ bool type_layout(int type, int* n_int_prop, int* n_float_prop) {
     case RXN_CMAQ_H2O2: *n_int_prop = 2; *n_float_prop = 7; return true;
     case RXN_CMAQ_OH_HNO3: *n_int_prop = 2; *n_float_prop = 11; return true;
     case RXN_PHOTOLYSIS: *n_int_prop = 3; *n_float_prop = 1; return true;
+    case RXN_FIRST_ORDER_LOSS: *n_int_prop = 4; *n_float_prop = 1; return true;
+    case RXN_EMISSION: *n_int_prop = 3; *n_float_prop = 1; return true;
+    case RXN_WET_DEPOSITION: *n_int_prop = 2; *n_float_prop = 1; return true;
     default: return false;
   }
 }
@@ -69,37 +73,87 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
   rxn_float_.insert(rxn_float_.end(), floats, floats + n_float);
   r.env_off = n_env_;
   n_env_ += n_env;
-  if (!type_layout(type, &r.n_int_prop, &r.n_float_prop)) {
-    *err = "reaction type " + std::to_string(type) +
-           " is not supported (gas-phase ARRHENIUS, TROE, CMAQ_H2O2, "
-           "CMAQ_OH_HNO3 and PHOTOLYSIS only)";
+  const int idx = n_added_++;
+  // host-rate column, in mechanism order (known before solver_initialize so
+  // that rxn_update_data can be called as soon as the reaction is added)
+  photo_slot_.push_back(host_rate_type(type) ? n_host_rate_++ : -1);
+  auto fail = [&](const std::string& msg) {
+    *err = msg;
     rxns_.push_back(r);
-    ++n_added_;
     return false;
-  }
-  r.nr = n_int > 0 ? ints[0] : 0;
-  r.np = n_int > 1 ? ints[1] : 0;
-  int need_int = r.n_int_prop + (r.nr + 2) * (r.nr + r.np);
-  int need_float = r.n_float_prop + r.np;
-  rxns_.push_back(r);
-  ++n_added_;
-  if (r.nr < 1 || r.np < 0 || n_int < need_int || n_float < need_float) {
-    *err = "malformed packed data for reaction " + std::to_string(n_added_ - 1);
-    return false;
-  }
-  for (int k = 0; k < r.nr + r.np; ++k) {
-    int s = ints[r.n_int_prop + k] - 1;
-    if (s < 0 || s >= n_state_) {
-      *err = "species index out of range in reaction " + std::to_string(n_added_ - 1);
-      return false;
+  };
+  if (!type_layout(type, &r.n_int_prop, &r.n_float_prop))
+    return fail("reaction type " + std::to_string(type) +
+                " is not supported (ARRHENIUS, TROE, CMAQ_H2O2, CMAQ_OH_HNO3, PHOTOLYSIS, "
+                "FIRST_ORDER_LOSS, EMISSION and WET_DEPOSITION only)");
+  const std::string malformed = "malformed packed data for reaction " + std::to_string(idx);
+  if (n_int < r.n_int_prop || n_float < r.n_float_prop) return fail(malformed);
+  const int o = r.int_off;  // rxn_int_ position of ints[0]
+  switch (type) {
+    case RXN_FIRST_ORDER_LOSS: {  // RXN_ID_ REACT_ DERIV_ID_ JAC_ID_ (rxn_first_order_loss.c:20-23)
+      Term t;
+      t.react = {ints[1] - 1};
+      t.deriv_at = {o + 2};
+      t.jac_at = {o + 3};
+      r.terms.push_back(t);
+      r.rid_at = o;
+      break;
+    }
+    case RXN_EMISSION: {  // RXN_ID_ SPECIES_ DERIV_ID_ (rxn_emission.c:20-22)
+      Term t;
+      t.prod = {ints[1] - 1};
+      t.yield = {1.0};
+      t.source = true;
+      t.deriv_at = {o + 2};
+      r.terms.push_back(t);
+      r.rid_at = o;
+      break;
+    }
+    case RXN_WET_DEPOSITION: {  // RXN_ID_ NUM_SPEC_ REACT_(s) DERIV_ID_(s) JAC_ID_(s)
+      const int ns = ints[1];  // (rxn_wet_deposition.c:20-30)
+      if (ns < 0 || n_int < 2 + 3 * ns) return fail(malformed);
+      for (int k = 0; k < ns; ++k) {
+        Term t;
+        t.react = {ints[2 + k] - 1};
+        t.deriv_at = {o + 2 + ns + k};
+        t.jac_at = {o + 2 + 2 * ns + k};
+        r.terms.push_back(t);
+      }
+      r.rid_at = o;
+      break;
+    }
+    default: {  // NUM_REACT_ NUM_PROD_ [RXN_ID_] REACT_ PROD_ DERIV_ID_ JAC_ID_, yields
+      const int nr = ints[0], np = ints[1];
+      if (nr < 1 || np < 0 || n_int < r.n_int_prop + (nr + 2) * (nr + np) ||
+          n_float < r.n_float_prop + np)
+        return fail(malformed);
+      Term t;
+      const int p = r.n_int_prop;
+      for (int k = 0; k < nr; ++k) t.react.push_back(ints[p + k] - 1);
+      for (int k = 0; k < np; ++k) {
+        t.prod.push_back(ints[p + nr + k] - 1);
+        t.yield.push_back(floats[r.n_float_prop + k]);
+      }
+      for (int k = 0; k < nr + np; ++k) t.deriv_at.push_back(o + p + nr + np + k);
+      for (int e = 0; e < nr * (nr + np); ++e) t.jac_at.push_back(o + p + 2 * (nr + np) + e);
+      r.terms.push_back(t);
+      if (type == RXN_PHOTOLYSIS) r.rid_at = o + 2;
     }
   }
+  for (const Term& t : r.terms) {
+    for (int sp : t.react)
+      if (sp < 0 || sp >= n_state_) return fail("species index out of range in reaction " + std::to_string(idx));
+    for (int sp : t.prod)
+      if (sp < 0 || sp >= n_state_) return fail("species index out of range in reaction " + std::to_string(idx));
+  }
+  n_terms_ += (int)r.terms.size();
+  rxns_.push_back(r);
   return true;
 }
 
 int Model::photo_id(int rxn) const {
   const Rxn& r = rxns_[rxn];
-  return r.type == RXN_PHOTOLYSIS ? rxn_int_[r.int_off + 2] : 0;
+  return host_rate_type(r.type) && r.rid_at >= 0 ? rxn_int_[r.rid_at] : 0;
 }
 
 int Model::rxn_elem_id(int dep, int ind) const {
@@ -108,41 +162,41 @@ int Model::rxn_elem_id(int dep, int ind) const {
   return -1;
 }
 
-#define REACT(r, x) (rxn_int_[(r).int_off + (r).n_int_prop + (x)] - 1)
-#define PROD(r, x) (rxn_int_[(r).int_off + (r).n_int_prop + (r).nr + (x)] - 1)
-#define DERIV_ID(r, x) rxn_int_[(r).int_off + (r).n_int_prop + (r).nr + (r).np + (x)]
-#define JAC_ID(r, x) rxn_int_[(r).int_off + (r).n_int_prop + 2 * ((r).nr + (r).np) + (x)]
-#define YIELD(r, x) rxn_float_[(r).float_off + (r).n_float_prop + (x)]
-
-// Diagonal of every state variable plus, per reaction, each (reactant,
-// reactant) and (product, reactant) pair (src/camp_solver.c:1445-1460 and
-// the get_used_jac_elem functions, e.g. src/rxns/rxn_arrhenius.c:44-60).
+// Diagonal of every state variable plus, per mass-action term, each
+// (reactant, reactant) and (product, reactant) pair (src/camp_solver.c:
+// 1445-1460 and the get_used_jac_elem functions, e.g.
+// src/rxns/rxn_arrhenius.c:44-60, rxn_first_order_loss.c:37-46,
+// rxn_wet_deposition.c:38-49; EMISSION registers none).
 void Model::build_rxn_jacobian() {
   Registry reg(n_state_);
   for (int i = 0; i < n_state_; ++i) reg.add(i, i);
   for (const Rxn& r : rxns_)
-    for (int ind = 0; ind < r.nr; ++ind) {
-      for (int d = 0; d < r.nr; ++d) reg.add(REACT(r, d), REACT(r, ind));
-      for (int d = 0; d < r.np; ++d) reg.add(PROD(r, d), REACT(r, ind));
-    }
+    for (const Term& t : r.terms)
+      for (int ind : t.react) {
+        for (int d : t.react) reg.add(d, ind);
+        for (int d : t.prod) reg.add(d, ind);
+      }
   reg.to_csc(&rj_colptr_, &rj_rowid_);
 }
 
 // DERIV_ID and JAC_ID written back into the packed ints, as rxn_update_ids
-// does (src/camp_solver.c:1491-1503, src/rxns/rxn_arrhenius.c:71-91).
+// does (src/camp_solver.c:1491-1503, src/rxns/rxn_arrhenius.c:71-91,
+// rxn_first_order_loss.c:56-69, rxn_emission.c:52-62).
 void Model::update_ids() {
   deriv_ids_.assign(n_state_, -1);
   for (int i = 0, d = 0; i < n_state_; ++i)
     if (var_type_[i] == VAR_VARIABLE) deriv_ids_[i] = d++;
-  for (const Rxn& r : rxns_) {
-    for (int k = 0; k < r.nr; ++k) DERIV_ID(r, k) = deriv_ids_[REACT(r, k)];
-    for (int k = 0; k < r.np; ++k) DERIV_ID(r, r.nr + k) = deriv_ids_[PROD(r, k)];
-    int e = 0;
-    for (int ind = 0; ind < r.nr; ++ind) {
-      for (int d = 0; d < r.nr; ++d) JAC_ID(r, e++) = rxn_elem_id(REACT(r, d), REACT(r, ind));
-      for (int d = 0; d < r.np; ++d) JAC_ID(r, e++) = rxn_elem_id(PROD(r, d), REACT(r, ind));
+  for (const Rxn& r : rxns_)
+    for (const Term& t : r.terms) {
+      int k = 0;
+      for (int s : t.react) rxn_int_[t.deriv_at[k++]] = deriv_ids_[s];
+      for (int s : t.prod) rxn_int_[t.deriv_at[k++]] = deriv_ids_[s];
+      int e = 0;
+      for (int ind : t.react) {
+        for (int d : t.react) rxn_int_[t.jac_at[e++]] = rxn_elem_id(d, ind);
+        for (int d : t.prod) rxn_int_[t.jac_at[e++]] = rxn_elem_id(d, ind);
+      }
     }
-  }
 }
 
 // Solver Jacobian: the variable x variable entries of the reaction Jacobian
@@ -480,54 +534,60 @@ void Model::build_tables() {
   Tables& t = tab_;
   t.n = n_dep_;
   t.n_state = n_state_;
-  t.n_rxn = n_rxn_;
+  t.n_rxn = n_terms_;
   t.n_jac = (int)sj_rowid_.size();
   t.dep_state.clear();
   for (int i = 0; i < n_state_; ++i)
     if (var_type_[i] == VAR_VARIABLE) t.dep_state.push_back(i);
-  // rate laws and reactants
+  // rate laws and reactants, one entry per mass-action term; a reaction's
+  // terms share its float head block and host-rate column
   t.rx_type.clear(); t.rx_nreact.clear(); t.rx_fpar.clear(); t.rx_photo.clear();
   t.fpar.clear();
   t.rx_cptr.assign(1, 0); t.rx_cidx.clear();
   t.rx_vptr.assign(1, 0); t.rx_vdep.clear();
-  photo_slot_.assign(n_rxn_, -1);
-  int n_photo = 0;
   for (int ri = 0; ri < n_rxn_; ++ri) {
     const Rxn& r = rxns_[ri];
-    t.rx_type.push_back(r.type);
-    t.rx_nreact.push_back(r.nr);
-    t.rx_fpar.push_back((int)t.fpar.size());
+    const int fpar0 = (int)t.fpar.size();
     for (int k = 0; k < r.n_float_prop; ++k) t.fpar.push_back(rxn_float_[r.float_off + k]);
-    if (r.type == RXN_PHOTOLYSIS) photo_slot_[ri] = n_photo++;
-    t.rx_photo.push_back(photo_slot_[ri]);
-    for (int k = 0; k < r.nr; ++k) {
-      int s = REACT(r, k);
-      if (var_type_[s] == VAR_VARIABLE)
-        t.rx_vdep.push_back(deriv_ids_[s]);
-      else
-        t.rx_cidx.push_back(s);
+    for (const Term& tm : r.terms) {
+      t.rx_type.push_back(r.type);
+      t.rx_nreact.push_back((int)tm.react.size());
+      t.rx_fpar.push_back(fpar0);
+      t.rx_photo.push_back(photo_slot_[ri]);
+      for (int s : tm.react) {
+        if (var_type_[s] == VAR_VARIABLE)
+          t.rx_vdep.push_back(deriv_ids_[s]);
+        else
+          t.rx_cidx.push_back(s);
+      }
+      t.rx_cptr.push_back((int)t.rx_cidx.size());
+      t.rx_vptr.push_back((int)t.rx_vdep.size());
     }
-    t.rx_cptr.push_back((int)t.rx_cidx.size());
-    t.rx_vptr.push_back((int)t.rx_vdep.size());
   }
-  t.n_photo = n_photo;
+  t.n_photo = n_host_rate_;
   t.n_part = (int)t.rx_vdep.size();
-  // f gather: per dependent species, in reaction order, reactant
-  // occurrences (loss, coefficient -1) before products (coefficient yield)
+  // f gather: per dependent species, in term order, reactant occurrences
+  // (loss, coefficient -1) before products (coefficient yield)
   std::vector<std::vector<int>> frx(n_dep_), fpr(n_dep_);
   std::vector<std::vector<double>> fco(n_dep_);
-  for (int ri = 0; ri < n_rxn_; ++ri) {
-    const Rxn& r = rxns_[ri];
-    for (int k = 0; k < r.nr; ++k) {
-      int d = DERIV_ID(r, k);
-      if (d < 0) continue;
-      frx[d].push_back(ri); fco[d].push_back(-1.0); fpr[d].push_back(0);
-    }
-    for (int k = 0; k < r.np; ++k) {
-      int d = DERIV_ID(r, r.nr + k);
-      if (d < 0) continue;
-      frx[d].push_back(ri); fco[d].push_back(YIELD(r, k)); fpr[d].push_back(1);
-    }
+  {
+    int ti = 0;
+    for (const Rxn& r : rxns_)
+      for (const Term& tm : r.terms) {
+        int k = 0;
+        for (size_t j = 0; j < tm.react.size(); ++j) {
+          const int d = rxn_int_[tm.deriv_at[k++]];
+          if (d < 0) continue;
+          frx[d].push_back(ti); fco[d].push_back(-1.0); fpr[d].push_back(FG_LOSS);
+        }
+        for (size_t j = 0; j < tm.prod.size(); ++j) {
+          const int d = rxn_int_[tm.deriv_at[k++]];
+          if (d < 0) continue;
+          frx[d].push_back(ti); fco[d].push_back(tm.yield[j]);
+          fpr[d].push_back(tm.source ? FG_SOURCE : FG_PRODUCT);
+        }
+        ++ti;
+      }
   }
   t.fg_ptr.assign(n_dep_ + 1, 0);
   t.fg_rxn.clear(); t.fg_coef.clear(); t.fg_prod.clear();
@@ -541,8 +601,8 @@ void Model::build_tables() {
   }
   t.fg_ptr[n_dep_] = (int)t.fg_rxn.size();
   // J gather: per solver Jacobian entry (column = independent species,
-  // row = dependent species), in reaction order, for each variable
-  // independent reactant occurrence: reactant rows (loss) then product rows
+  // row = dependent species), in term order, for each variable independent
+  // reactant occurrence: reactant rows (loss) then product rows
   std::vector<std::vector<int>> jpart(t.n_jac), jind(t.n_jac);
   std::vector<std::vector<double>> jco(t.n_jac);
   auto slot_of = [&](int row, int col) {
@@ -550,27 +610,29 @@ void Model::build_tables() {
       if (sj_rowid_[e] == row) return e;
     return -1;
   };
-  for (int ri = 0; ri < n_rxn_; ++ri) {
-    const Rxn& r = rxns_[ri];
-    int kv = 0;
-    for (int ind = 0; ind < r.nr; ++ind) {
-      int sind = REACT(r, ind);
-      if (var_type_[sind] != VAR_VARIABLE) continue;
-      int part = t.rx_vptr[ri] + kv++;
-      int cind = deriv_ids_[sind];
-      for (int d = 0; d < r.nr; ++d) {
-        int sd = REACT(r, d);
-        if (var_type_[sd] != VAR_VARIABLE) continue;
-        int e = slot_of(deriv_ids_[sd], cind);
-        jpart[e].push_back(part); jco[e].push_back(-1.0); jind[e].push_back(-1);
+  {
+    int ti = 0;
+    for (const Rxn& r : rxns_)
+      for (const Term& tm : r.terms) {
+        int kv = 0;
+        for (int sind : tm.react) {
+          if (var_type_[sind] != VAR_VARIABLE) continue;
+          const int part = t.rx_vptr[ti] + kv++;
+          const int cind = deriv_ids_[sind];
+          for (int sd : tm.react) {
+            if (var_type_[sd] != VAR_VARIABLE) continue;
+            int e = slot_of(deriv_ids_[sd], cind);
+            jpart[e].push_back(part); jco[e].push_back(-1.0); jind[e].push_back(-1);
+          }
+          for (size_t d = 0; d < tm.prod.size(); ++d) {
+            const int sd = tm.prod[d];
+            if (var_type_[sd] != VAR_VARIABLE) continue;
+            int e = slot_of(deriv_ids_[sd], cind);
+            jpart[e].push_back(part); jco[e].push_back(tm.yield[d]); jind[e].push_back(cind);
+          }
+        }
+        ++ti;
       }
-      for (int d = 0; d < r.np; ++d) {
-        int sd = PROD(r, d);
-        if (var_type_[sd] != VAR_VARIABLE) continue;
-        int e = slot_of(deriv_ids_[sd], cind);
-        jpart[e].push_back(part); jco[e].push_back(YIELD(r, d)); jind[e].push_back(cind);
-      }
-    }
   }
   t.jg_ptr.assign(t.n_jac + 1, 0);
   t.jg_part.clear(); t.jg_coef.clear(); t.jg_ind.clear();

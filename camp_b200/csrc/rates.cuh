@@ -73,7 +73,11 @@ static __device__ double rate_constant(const DevMech& m, int r, double T, double
               k3 / (1.0 + k3 / k2)) *
              pow(conv, (double)(nr - 1)) * f[9];
     }
-    case RXN_PHOTOLYSIS:  // src/rxns/rxn_photolysis.c:137-148
+    case RXN_PHOTOLYSIS:        // src/rxns/rxn_photolysis.c:137-148
+    case RXN_FIRST_ORDER_LOSS:  // src/rxns/rxn_first_order_loss.c:118-130
+    case RXN_EMISSION:          // src/rxns/rxn_emission.c:109-120
+    case RXN_WET_DEPOSITION:    // src/rxns/rxn_wet_deposition.c:124-136
+      // SCALING_ * BASE_RATE_, the base rate being the cell's host-set value
       return f[0] * (photo_cell ? photo_cell[ldg(m.rx_photo + r)] : 0.0);
   }
   return 0.0;

@@ -50,6 +50,7 @@ RXN_CMAQ_OH_HNO3 = 4
 RXN_PHOTOLYSIS = 5
 RXN_FIRST_ORDER_LOSS = 12
 RXN_EMISSION = 13
+RXN_WET_DEPOSITION = 14
 
 RXN_TYPE_IDS = {
     "ARRHENIUS": RXN_ARRHENIUS,
@@ -57,7 +58,15 @@ RXN_TYPE_IDS = {
     "CMAQ_H2O2": RXN_CMAQ_H2O2,
     "CMAQ_OH_HNO3": RXN_CMAQ_OH_HNO3,
     "PHOTOLYSIS": RXN_PHOTOLYSIS,
+    "FIRST_ORDER_LOSS": RXN_FIRST_ORDER_LOSS,
+    "EMISSION": RXN_EMISSION,
+    "WET_DEPOSITION": RXN_WET_DEPOSITION,
 }
+
+# Types whose rate the host sets per cell through rxn_update_data
+# (src/rxn_solver.c:735-760); each such reaction is one column of the
+# per-cell base rates, in mechanism order.
+HOST_RATE_TYPES = (RXN_PHOTOLYSIS, RXN_FIRST_ORDER_LOSS, RXN_EMISSION, RXN_WET_DEPOSITION)
 
 # Physical constants, src/constants.F90:37-41
 BOLTZMANN = 1.3806505e-23
@@ -90,8 +99,8 @@ class Mechanism:
     abs_tol: np.ndarray  # float64 [n_state_var]
     rel_tol: float
     rxns: list[PackedRxn]
-    # photolysis id (RXN_ID_) -> index of the reaction in ``rxns``
-    photo_ids: dict[int, int] = field(default_factory=dict)
+    # RXN_ID_ of each reaction of a host-rate type -> its index in ``rxns``
+    rate_ids: dict[int, int] = field(default_factory=dict)
     species_props: dict[str, dict] = field(default_factory=dict)
 
     @property
@@ -143,7 +152,7 @@ class Mechanism:
                 }
                 for r in self.rxns
             ],
-            "photo_ids": {str(k): int(v) for k, v in self.photo_ids.items()},
+            "rate_ids": {str(k): int(v) for k, v in self.rate_ids.items()},
             "init_conc": {
                 n: float(p["init conc"]) for n, p in self.species_props.items() if "init conc" in p
             },
@@ -168,7 +177,8 @@ class Mechanism:
             abs_tol=np.asarray(d["abs_tol"], dtype=np.float64),
             rel_tol=float(d["rel_tol"]),
             rxns=rxns,
-            photo_ids={int(k): int(v) for k, v in d.get("photo_ids", {}).items()},
+            rate_ids={int(k): int(v)
+                      for k, v in d.get("rate_ids", d.get("photo_ids", {})).items()},
             species_props={n: {"init conc": v} for n, v in d.get("init_conc", {}).items()},
         )
 
@@ -183,6 +193,16 @@ class Mechanism:
 
     def photolysis_rxns(self) -> list[int]:
         return [i for i, r in enumerate(self.rxns) if r.rxn_type == RXN_PHOTOLYSIS]
+
+    def rate_rxns(self) -> list[int]:
+        """Reactions of a host-rate type in mechanism order: column j of the
+        per-cell base rates belongs to reaction rate_rxns()[j]."""
+        return [i for i, r in enumerate(self.rxns) if r.rxn_type in HOST_RATE_TYPES]
+
+    def rate_id(self, rxn: int) -> int:
+        """RXN_ID_ of a host-rate reaction (the id its update data carries)."""
+        r = self.rxns[rxn]
+        return int(r.ints[2] if r.rxn_type == RXN_PHOTOLYSIS else r.ints[0])
 
 
 # ---------------------------------------------------------------------------
@@ -307,11 +327,45 @@ def _int_block(n_int_prop: int, head: list[int], react: list[int], prod: list[in
     return ints
 
 
+def pack_species_rate(rtype: int, species: int, scaling: float = 1.0, label: str = "") -> PackedRxn:
+    """FIRST_ORDER_LOSS or EMISSION of one state variable (1-based index),
+    packed as src/rxns/rxn_first_order_loss.F90:169-220 and
+    rxn_emission.F90:166-217 do: RXN_ID_ (-1 until the host assigns one),
+    the species, then the DERIV_ID_ (and JAC_ID_) slots; SCALING_."""
+    n_int = 4 if rtype == RXN_FIRST_ORDER_LOSS else 3
+    ints = np.zeros(n_int, np.int32)
+    ints[0], ints[1] = -1, species
+    return PackedRxn(rtype, ints, np.asarray([scaling]), 2, label)
+
+
+def pack_wet_deposition(species: list[int], scaling: float = 1.0, label: str = "") -> PackedRxn:
+    """WET_DEPOSITION of the given state variables (1-based indices; the
+    Fortran packer lists every species of the named aerosol phase in every
+    instance of it, src/rxns/rxn_wet_deposition.F90:172-254): RXN_ID_,
+    NUM_SPEC_, REACT_(s), DERIV_ID_(s), JAC_ID_(s); SCALING_."""
+    ns = len(species)
+    ints = np.zeros(2 + 3 * ns, np.int32)
+    ints[0], ints[1] = -1, ns
+    ints[2 : 2 + ns] = species
+    return PackedRxn(RXN_WET_DEPOSITION, ints, np.asarray([scaling]), 2, label)
+
+
 def pack_reaction(rxn: dict, gas_id: Callable[[str], int]) -> PackedRxn:
     """Packs one gas-phase reaction as its Fortran ``initialize`` does."""
     rtype = rxn["type"]
     if rtype not in RXN_TYPE_IDS:
         raise NotImplementedError(f"reaction type {rtype} is not supported")
+    if rtype in ("FIRST_ORDER_LOSS", "EMISSION"):
+        if "species" not in rxn:
+            kind = "First-Order Loss" if rtype == "FIRST_ORDER_LOSS" else "Emission"
+            raise ValueError(f"{kind} reaction is missing species name")
+        return pack_species_rate(RXN_TYPE_IDS[rtype], gas_id(rxn["species"]),
+                                 float(rxn.get("scaling factor", 1.0)),
+                                 str(rxn.get("rxn id", "")))
+    if rtype == "WET_DEPOSITION":
+        raise NotImplementedError(
+            "WET_DEPOSITION removes the species of an aerosol phase, and aerosol phases are "
+            "not read from JSON here; build it with pack_wet_deposition")
     react = _expand_reactants(rxn["reactants"], gas_id)
     prod, ylds = _products(rxn.get("products", {}), gas_id)
     label = str(rxn.get("rxn id", ""))
@@ -383,10 +437,11 @@ def pack_reaction(rxn: dict, gas_id: Callable[[str], int]) -> PackedRxn:
 def load_mechanism(files: Iterable[str], name: str | None = None) -> Mechanism:
     """Loads CAMP JSON input files and packs the gas-phase mechanism.
 
-    Photolysis reactions receive sequential ids (1, 2, ...) in mechanism order,
-    which is what the reference's ``generate_int_id`` hands out when a host
-    model creates one update object per photolysis reaction in that order
-    (``test/chemistry/cb05cl_ae5/test_cb05cl_ae5.F90:293-310``).
+    Reactions whose rate the host sets (PHOTOLYSIS, FIRST_ORDER_LOSS,
+    EMISSION) receive sequential ids (1, 2, ...) in mechanism order, which is
+    what the reference's ``generate_int_id`` (src/rand.F90:644-656) hands out
+    when a host model creates one update object per such reaction in that
+    order (``test/chemistry/cb05cl_ae5/test_cb05cl_ae5.F90:293-310``).
     """
     db = _SpeciesDB()
     mechs: list[tuple[str, list[dict]]] = []
@@ -421,13 +476,7 @@ def load_mechanism(files: Iterable[str], name: str | None = None) -> Mechanism:
     for _, rx in mechs:
         for r in rx:
             rxns.append(pack_reaction(r, gas_id))
-    photo_ids = {}
-    next_id = 1
-    for i, r in enumerate(rxns):
-        if r.rxn_type == RXN_PHOTOLYSIS:
-            r.ints[2] = next_id
-            photo_ids[next_id] = i
-            next_id += 1
+    rate_ids = assign_rate_ids(rxns)
     var_type = np.asarray([db.var_type_of(n) for n in gas], dtype=np.int32)
     abs_tol = np.asarray([db.abs_tol_of(n) for n in gas], dtype=np.float64)
     mech = Mechanism(
@@ -437,10 +486,24 @@ def load_mechanism(files: Iterable[str], name: str | None = None) -> Mechanism:
         abs_tol=abs_tol,
         rel_tol=rel_tol if rel_tol is not None else 1.0e-8,
         rxns=rxns,
-        photo_ids=photo_ids,
+        rate_ids=rate_ids,
         species_props={n: dict(db.props[n]) for n in gas},
     )
     return mech
+
+
+def assign_rate_ids(rxns: list[PackedRxn]) -> dict[int, int]:
+    """Gives every reaction of a host-rate type the next id of one sequence,
+    in order, as a host creating one update object per such reaction does;
+    returns id -> reaction index."""
+    ids = {}
+    for i, r in enumerate(rxns):
+        if r.rxn_type not in HOST_RATE_TYPES:
+            continue
+        rid = len(ids) + 1
+        r.ints[2 if r.rxn_type == RXN_PHOTOLYSIS else 0] = rid
+        ids[rid] = i
+    return ids
 
 
 def reaction_summary(mech: Mechanism) -> dict:
@@ -449,5 +512,11 @@ def reaction_summary(mech: Mechanism) -> dict:
     by_nr: dict[int, int] = {}
     for r in mech.rxns:
         by_type[r.rxn_type] = by_type.get(r.rxn_type, 0) + 1
-        by_nr[int(r.ints[0])] = by_nr.get(int(r.ints[0]), 0) + 1
+        if r.rxn_type in (RXN_FIRST_ORDER_LOSS, RXN_WET_DEPOSITION):
+            nr = 1
+        elif r.rxn_type == RXN_EMISSION:
+            nr = 0
+        else:
+            nr = int(r.ints[0])
+        by_nr[nr] = by_nr.get(nr, 0) + 1
     return {"by_type": by_type, "by_n_react": by_nr}

@@ -3,8 +3,9 @@
 The reference's Fortran ``camp_solver_data_t`` (src/camp_solver_data.F90)
 creates the C solver with ``solver_new``, feeds it every reaction's packed
 data with ``rxn_add_condensed_data``, calls ``solver_initialize`` and then
-``solver_run`` once per host time step, and pushes per-cell photolysis rates
-through ``rxn_update_data``.  :class:`Solver` makes the same calls, in the
+``solver_run`` once per host time step, and pushes per-cell host-set rates
+(photolysis, emission, first-order loss, wet deposition) through
+``rxn_update_data``.  :class:`Solver` makes the same calls, in the
 same order, through the C ABI of ``libcamp_b200.so``.
 """
 from __future__ import annotations
@@ -14,7 +15,11 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .mechanism import RXN_PHOTOLYSIS, Mechanism
+from .mechanism import (RXN_EMISSION, RXN_FIRST_ORDER_LOSS, RXN_PHOTOLYSIS, RXN_WET_DEPOSITION,
+                        Mechanism)
+
+_UPDATE_KIND = {RXN_PHOTOLYSIS: "photolysis", RXN_EMISSION: "emission",
+                RXN_FIRST_ORDER_LOSS: "first_order_loss", RXN_WET_DEPOSITION: "wet_deposition"}
 
 # solver defaults, src/camp_solver_data.F90:33-37
 DEFAULT_MAX_STEPS = 10000
@@ -174,11 +179,24 @@ class Solver:
     # ------------------------------------------------------------------
     def set_photo_rate(self, cell: int, photo_id: int, base_rate: float) -> None:
         """Photolysis update through the reference's rxn_update_data path."""
-        ud = self.lib.rxn_photolysis_create_rate_update_data()
-        self.lib.rxn_photolysis_set_rate_update_data(ud, int(photo_id), float(base_rate))
+        self.set_rate(cell, RXN_PHOTOLYSIS, photo_id, base_rate)
+
+    def set_rate(self, cell: int, rxn_type: int, rxn_id: int, base_rate: float) -> None:
+        """Base rate of the reaction of a host-rate type with RXN_ID_ rxn_id,
+        through the update-data functions of that type and rxn_update_data."""
+        kind = _UPDATE_KIND[rxn_type]
+        ud = getattr(self.lib, f"rxn_{kind}_create_rate_update_data")()
+        getattr(self.lib, f"rxn_{kind}_set_rate_update_data")(ud, int(rxn_id), float(base_rate))
         cursor = C.c_int(0)
-        self.lib.rxn_update_data(int(cell), C.byref(cursor), RXN_PHOTOLYSIS, ud, self._h)
+        self.lib.rxn_update_data(int(cell), C.byref(cursor), int(rxn_type), ud, self._h)
         self.lib.solver_free_update_data(ud)
+
+    def rate_column(self, column: int) -> tuple[int, int, int]:
+        """(reaction index, type, RXN_ID_) of a host-rate column."""
+        vals = [C.c_int() for _ in range(3)]
+        if self.lib.camp_b200_rate_column(self._h, int(column), *[C.byref(v) for v in vals]):
+            raise SolverError(_lib.last_error())
+        return tuple(int(v.value) for v in vals)
 
     def set_photo_rates_device(self, d_rates, n_cells: int | None = None) -> None:
         """Photolysis rates already in device memory (torch CUDA tensor or
@@ -198,14 +216,14 @@ class Solver:
         return int(self.lib.camp_b200_n_photo(self._h))
 
     def set_photo_rates(self, rates: np.ndarray) -> None:
-        """Base rates [n_cells, n_photo] for photolysis ids 1..n_photo.
-
-        Ids are assigned in mechanism order, so id j+1 is photolysis reaction
-        j; this sets the same values a loop of rxn_update_data calls would."""
+        """Host-set base rates [n_cells, n_photo]: one column per reaction of
+        a host-rate type (photolysis, first-order loss, emission, wet
+        deposition) in mechanism order; this sets the same values a loop of
+        rxn_update_data calls would (see rate_column for a column's id)."""
         rates = np.ascontiguousarray(rates, np.float64)
         n = rates.shape[0]
-        if rates.shape[1] != self.n_photo:
-            raise ValueError("rates must have one column per photolysis reaction")
+        if rates.ndim != 2 or rates.shape[1] != self.n_photo:
+            raise ValueError("rates must have one column per host-rate reaction")
         self.lib.camp_b200_set_photo_rates(self._h, rates.reshape(-1), n)
 
     # ------------------------------------------------------------------

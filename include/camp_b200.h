@@ -87,6 +87,21 @@ void rxn_free_update_data(void *update_data);
 void *rxn_photolysis_create_rate_update_data(void);
 void rxn_photolysis_set_rate_update_data(void *update_data, int photo_id,
                                          double base_rate);
+/* replace src/rxns/rxn_emission.c:192-213 (bound from
+ * src/rxns/rxn_emission.F90:118-135) */
+void *rxn_emission_create_rate_update_data(void);
+void rxn_emission_set_rate_update_data(void *update_data, int rxn_id,
+                                       double base_rate);
+/* replace src/rxns/rxn_first_order_loss.c:208-229 (bound from
+ * src/rxns/rxn_first_order_loss.F90:121-138) */
+void *rxn_first_order_loss_create_rate_update_data(void);
+void rxn_first_order_loss_set_rate_update_data(void *update_data, int rxn_id,
+                                               double base_rate);
+/* replace src/rxns/rxn_wet_deposition.c:218-239 (bound from
+ * src/rxns/rxn_wet_deposition.F90:124-141) */
+void *rxn_wet_deposition_create_rate_update_data(void);
+void rxn_wet_deposition_set_rate_update_data(void *update_data, int rxn_id,
+                                             double base_rate);
 
 /* replace src/aero_phase_solver.c:175,210, src/aero_rep_solver.c:443,492,546
  * and src/sub_model_solver.c:413,468,509.  Data is accepted; a model with
@@ -203,8 +218,8 @@ int camp_b200_sync_status(void *solver_data, void *stream);
  * device memory, for callers that cannot call cudaMalloc while they run (a
  * host model whose pool allocator owns the device heap, or code running where
  * allocation is not allowed).  All buffers are the caller's: state
- * [n_cells*n_state_var] (updated in place), env [n_cells*2], photolysis base
- * rates [n_cells*n_photo] (may be NULL without photolysis reactions) and the
+ * [n_cells*n_state_var] (updated in place), env [n_cells*2], host-set base
+ * rates [n_cells*n_photo] (may be NULL without host-rate reactions) and the
  * per-cell results d_stats [n_cells], all in device memory.  The solve's
  * scratch lives in one static 8 MiB device array that every GPU loading this
  * library holds until exit; a mechanism needing more than that for one
@@ -219,11 +234,19 @@ int camp_b200_run_device_noalloc(void *solver_data, double *d_state,
                                  camp_b200_cell_stats *d_stats, int n_cells,
                                  double t_initial, double t_final, void *stream);
 
-/* Per-cell photolysis base rates: rates[c * n_photo + j] for photolysis
- * reaction j (mechanism order) of cell c, as if rxn_update_data had been
- * called for every cell and reaction. */
+/* Per-cell host-set base rates: rates[c * n_photo + j] for column j of cell
+ * c, as if rxn_update_data had been called for every cell and reaction.
+ * There is one column per reaction whose rate the host sets (PHOTOLYSIS,
+ * FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION), in mechanism order; for a
+ * mechanism whose only such reactions are photolysis, column j is photolysis
+ * reaction j. */
 int camp_b200_n_photo(void *solver_data);
 int camp_b200_set_photo_rates(void *solver_data, const double *rates, int n_cells);
+/* Which reaction column `column` of the base rates belongs to: its index in
+ * mechanism order, its type and its RXN_ID_ (the id update data carries).
+ * Any pointer may be NULL.  0, or -1 when there is no such column. */
+int camp_b200_rate_column(void *solver_data, int column, int *rxn_index, int *rxn_type,
+                          int *rxn_id);
 /* Device-resident form: rates [n_cells * n_photo] in device memory, read by
  * every following run (no per-run upload) until called with NULL, which
  * returns to the host rates.  The buffer must stay valid meanwhile. */
@@ -296,8 +319,9 @@ void camp_b200_server_free(void *server);
  * initialize) for gas-phase mechanisms: reads CAMP JSON files (CHEM_SPEC,
  * MECHANISM and RELATIVE_TOLERANCE objects), orders the state (gas species
  * in order of first appearance), packs every reaction and calls solver_new
- * and rxn_add_condensed_data.  Photolysis reactions get the photolysis ids
- * 1, 2, ... in mechanism order.  Then call solver_initialize (tolerances
+ * and rxn_add_condensed_data.  Reactions whose rate the host sets
+ * (PHOTOLYSIS, FIRST_ORDER_LOSS, EMISSION) get the ids 1, 2, ... in
+ * mechanism order.  WET_DEPOSITION needs aerosol phases and is rejected.  Then call solver_initialize (tolerances
  * from camp_b200_json_tolerances) and solver_run.  NULL on error. */
 void *camp_b200_solver_from_json(const char *const *files, int n_files, int n_cells);
 int camp_b200_n_state_var(void *solver_data);

@@ -21,6 +21,14 @@
 #define T_CMAQ_H2O2 3
 #define T_CMAQ_OH_HNO3 4
 #define T_PHOTOLYSIS 5
+#define T_FIRST_ORDER_LOSS 12
+#define T_EMISSION 13
+#define T_WET_DEPOSITION 14
+
+/* types whose packed data is not the NUM_REACT_/NUM_PROD_ layout */
+static int species_rate_type(int t) {
+  return t == T_FIRST_ORDER_LOSS || t == T_EMISSION || t == T_WET_DEPOSITION;
+}
 
 static void *zalloc(size_t n) {
   void *p = calloc(n ? n : 1, 1);
@@ -100,7 +108,7 @@ OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn) {
 int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
                const int *ints, const double *floats) {
   if (m->n_added >= m->n_rxn) return 1;
-  if (type < T_ARRHENIUS || type > T_PHOTOLYSIS) return 2;
+  if ((type < T_ARRHENIUS || type > T_PHOTOLYSIS) && !species_rate_type(type)) return 2;
   if (m->int_size + n_int + 1 > m->int_cap) {
     m->int_cap = 2 * (m->int_size + n_int + 1) + 64;
     m->int_data = (int *)realloc(m->int_data, sizeof(int) * m->int_cap);
@@ -276,6 +284,13 @@ int om_build(OracleMech *m) {
     ORxn *r = &m->rx[i];
     r->ints = m->int_data + (size_t)r->ints;
     r->fl = m->float_data + (size_t)r->fl;
+    if (species_rate_type(r->type)) {
+      /* RXN_ID_ first; the reactant / product fields stay unused */
+      r->nr = r->np = 0;
+      r->n_int_prop = 0;
+      r->n_float_prop = 1;
+      continue;
+    }
     r->nr = r->ints[0];
     r->np = r->ints[1];
     r->n_int_prop = r->type == T_PHOTOLYSIS ? 3 : 2;
@@ -293,6 +308,17 @@ int om_build(OracleMech *m) {
   for (int i = 0; i < n; ++i) jr_register(&rj, i, i);
   for (int i = 0; i < m->n_rxn; ++i) {
     ORxn *r = &m->rx[i];
+    const int *I = r->ints;
+    switch (r->type) {
+      case T_FIRST_ORDER_LOSS: /* src/rxns/rxn_first_order_loss.c:37-46 */
+        jr_register(&rj, I[1] - 1, I[1] - 1);
+        continue;
+      case T_EMISSION: /* src/rxns/rxn_emission.c:36-42: none */
+        continue;
+      case T_WET_DEPOSITION: /* src/rxns/rxn_wet_deposition.c:38-49 */
+        for (int s = 0; s < I[1]; ++s) jr_register(&rj, I[2 + s] - 1, I[2 + s] - 1);
+        continue;
+    }
     for (int ind = 0; ind < r->nr; ++ind) {
       for (int d = 0; d < r->nr; ++d) jr_register(&rj, R_REACT(r, d), R_REACT(r, ind));
       for (int d = 0; d < r->np; ++d) jr_register(&rj, R_PROD(r, d), R_REACT(r, ind));
@@ -308,6 +334,25 @@ int om_build(OracleMech *m) {
     m->deriv_ids[i] = m->var_type[i] == VAR_VARIABLE ? d++ : -1;
   for (int i = 0; i < m->n_rxn; ++i) {
     ORxn *r = &m->rx[i];
+    int *I = r->ints;
+    switch (r->type) {
+      case T_FIRST_ORDER_LOSS: /* src/rxns/rxn_first_order_loss.c:56-69 */
+        I[2] = m->deriv_ids[I[1] - 1];
+        I[3] = jr_elem_id(m->rj_colptr, m->rj_rowid, I[1] - 1, I[1] - 1);
+        continue;
+      case T_EMISSION: /* src/rxns/rxn_emission.c:52-62 */
+        I[2] = m->deriv_ids[I[1] - 1];
+        continue;
+      case T_WET_DEPOSITION: { /* src/rxns/rxn_wet_deposition.c:59-75 */
+        const int ns = I[1];
+        for (int s = 0; s < ns; ++s) {
+          I[2 + ns + s] = m->deriv_ids[I[2 + s] - 1];
+          I[2 + 2 * ns + s] =
+              jr_elem_id(m->rj_colptr, m->rj_rowid, I[2 + s] - 1, I[2 + s] - 1);
+        }
+        continue;
+      }
+    }
     for (int k = 0; k < r->nr; ++k) R_DERIV_ID(r, k) = m->deriv_ids[R_REACT(r, k)];
     for (int k = 0; k < r->np; ++k)
       R_DERIV_ID(r, r->nr + k) = m->deriv_ids[R_PROD(r, k)];
@@ -397,18 +442,34 @@ void om_get_lu_order(const OracleMech *m, int *perm) {
 /* Rate constants (update_env_state of each gas type)                        */
 /* ------------------------------------------------------------------------ */
 
-int om_set_photo_rate(const OracleMech *m, double *rxn_env, int photo_id,
-                      double base_rate) {
-  int found = 0;
+/* rxn_update_data (src/rxn_solver.c:700-760) with the update_data function
+ * of each host-rate type (src/rxns/rxn_photolysis.c:109-125,
+ * rxn_emission.c:82-98, rxn_first_order_loss.c:89-106,
+ * rxn_wet_deposition.c:95-112): the first reaction of the type whose RXN_ID_
+ * (> 0) matches takes BASE_RATE_ and RATE_ = SCALING_ * BASE_RATE_. */
+int om_set_rate(const OracleMech *m, double *rxn_env, int type, int rxn_id,
+                double base_rate) {
   for (int i = 0; i < m->n_rxn; ++i) {
     const ORxn *r = &m->rx[i];
-    if (r->type != T_PHOTOLYSIS || r->ints[2] != photo_id || r->ints[2] <= 0)
-      continue;
+    if (r->type != type) continue;
+    int rid;
+    if (type == T_PHOTOLYSIS)
+      rid = r->ints[2];
+    else if (species_rate_type(type))
+      rid = r->ints[0];
+    else
+      return 0;
+    if (rid != rxn_id || rid <= 0) continue;
     rxn_env[r->env_off + 1] = base_rate;
     rxn_env[r->env_off] = r->fl[0] * base_rate;
-    found = 1;
+    return 1;
   }
-  return found;
+  return 0;
+}
+
+int om_set_photo_rate(const OracleMech *m, double *rxn_env, int photo_id,
+                      double base_rate) {
+  return om_set_rate(m, rxn_env, T_PHOTOLYSIS, photo_id, base_rate);
 }
 
 void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
@@ -455,7 +516,10 @@ void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
                pow(conv, r->nr - 1) * f[9];
         break;
       }
-      case T_PHOTOLYSIS: /* src/rxns/rxn_photolysis.c:137-148 */
+      case T_PHOTOLYSIS:         /* src/rxns/rxn_photolysis.c:137-148 */
+      case T_FIRST_ORDER_LOSS:   /* src/rxns/rxn_first_order_loss.c:118-130 */
+      case T_EMISSION:           /* src/rxns/rxn_emission.c:109-120 */
+      case T_WET_DEPOSITION:     /* src/rxns/rxn_wet_deposition.c:124-136 */
         k[0] = f[0] * k[1];
         break;
     }
@@ -465,6 +529,14 @@ void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
 /* ------------------------------------------------------------------------ */
 /* Derivative and Jacobian (calc_deriv_contrib / calc_jac_contrib)           */
 /* ------------------------------------------------------------------------ */
+
+/* time_derivative_add_value (src/time_derivative.c:90-97) */
+static void add_value(long double *P, long double *L, int d, long double v) {
+  if (v > 0.0)
+    P[d] += v;
+  else
+    L[d] += -v;
+}
 
 /* The gas types share one mass-action form: rate = k * prod(y_react), loss of
  * rate on each reactant, rate*yield on each product unless a negative yield
@@ -477,6 +549,23 @@ void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
   long double *L = P + m->n_dep;
   for (int i = 0; i < m->n_rxn; ++i) {
     const ORxn *r = &m->rx[i];
+    const int *I = r->ints;
+    const double k = rxn_env[r->env_off];
+    switch (r->type) {
+      case T_FIRST_ORDER_LOSS: /* src/rxns/rxn_first_order_loss.c:143-158 */
+        if (I[2] >= 0) add_value(P, L, I[2], -(k * (long double)state[I[1] - 1]));
+        continue;
+      case T_EMISSION: /* src/rxns/rxn_emission.c:133-147 */
+        if (I[2] >= 0) add_value(P, L, I[2], (long double)k);
+        continue;
+      case T_WET_DEPOSITION: { /* src/rxns/rxn_wet_deposition.c:149-166 */
+        const int ns = I[1];
+        for (int s = 0; s < ns; ++s)
+          if (I[2 + ns + s] >= 0)
+            add_value(P, L, I[2 + ns + s], -(k * (long double)state[I[2 + s] - 1]));
+        continue;
+      }
+    }
     long double rate = rxn_env[r->env_off];
     for (int s = 0; s < r->nr; ++s) rate *= state[R_REACT(r, s)];
     if (rate == 0.0) continue;
@@ -514,6 +603,20 @@ void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
   long double *L = P + m->n_rxn_jac;
   for (int i = 0; i < m->n_rxn; ++i) {
     const ORxn *r = &m->rx[i];
+    const int *I = r->ints;
+    switch (r->type) {
+      case T_FIRST_ORDER_LOSS: /* src/rxns/rxn_first_order_loss.c:171-187 */
+        if (I[3] >= 0) L[I[3]] += rxn_env[r->env_off];
+        continue;
+      case T_EMISSION: /* src/rxns/rxn_emission.c:160-171: none */
+        continue;
+      case T_WET_DEPOSITION: { /* src/rxns/rxn_wet_deposition.c:179-197 */
+        const int ns = I[1];
+        for (int s = 0; s < ns; ++s)
+          if (I[2 + 2 * ns + s] >= 0) L[I[2 + 2 * ns + s]] += rxn_env[r->env_off];
+        continue;
+      }
+    }
     int e = 0;
     for (int ind = 0; ind < r->nr; ++ind) {
       double rate = rxn_env[r->env_off];

@@ -72,8 +72,12 @@ void om_get_solver_jac(const OracleMech *m, int *col_ptrs, int *row_ids);
 void om_get_rxn_int_data(const OracleMech *m, int *out);
 void om_get_lu_order(const OracleMech *m, int *perm);
 
-/* Photolysis base rate of every reaction whose RXN_ID equals photo_id, in
- * one cell's rxn_env_data (src/rxns/rxn_photolysis.c:109-124). */
+/* Base rate of the first reaction of rxn_type (PHOTOLYSIS, FIRST_ORDER_LOSS,
+ * EMISSION, WET_DEPOSITION) whose RXN_ID_ equals rxn_id, in one cell's
+ * rxn_env_data, as rxn_update_data does (src/rxn_solver.c:700-760); returns
+ * whether one matched.  om_set_photo_rate is the PHOTOLYSIS case. */
+int om_set_rate(const OracleMech *m, double *rxn_env_cell, int rxn_type, int rxn_id,
+                double base_rate);
 int om_set_photo_rate(const OracleMech *m, double *rxn_env_cell, int photo_id,
                       double base_rate);
 /* Rate constants for one cell from env = {T [K], P [Pa]}. */

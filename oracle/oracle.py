@@ -87,6 +87,8 @@ def oracle_lib():
         lib.om_get_lu_order.argtypes = [vp, _i32p]
         lib.om_set_photo_rate.restype = C.c_int
         lib.om_set_photo_rate.argtypes = [vp, _f64p, C.c_int, C.c_double]
+        lib.om_set_rate.restype = C.c_int
+        lib.om_set_rate.argtypes = [vp, _f64p, C.c_int, C.c_int, C.c_double]
         lib.om_update_env.argtypes = [vp, _f64p, _f64p]
         lib.om_deriv.argtypes = [vp, _f64p, _f64p, C.c_double, _f64p, _f64p, _f64p]
         lib.om_jac.argtypes = [vp, _f64p, _f64p, C.c_double, _f64p]
@@ -145,8 +147,9 @@ def ref_lib():
         lib.ref_calc_jac.argtypes = [vp, C.c_int, C.c_double, _f64p, _f64p]
         lib.ref_free.argtypes = [vp]
         lib.rxn_update_data.argtypes = [C.c_int, C.POINTER(C.c_int), C.c_int, vp, vp]
-        lib.rxn_photolysis_create_rate_update_data.restype = vp
-        lib.rxn_photolysis_set_rate_update_data.argtypes = [vp, C.c_int, C.c_double]
+        for kind in ("photolysis", "emission", "first_order_loss", "wet_deposition"):
+            getattr(lib, f"rxn_{kind}_create_rate_update_data").restype = vp
+            getattr(lib, f"rxn_{kind}_set_rate_update_data").argtypes = [vp, C.c_int, C.c_double]
         _ref_lib = lib
     return _ref_lib
 
@@ -201,11 +204,18 @@ class OracleModel:
         self.lib.om_get_lu_order(self.h, out)
         return out
 
+    def _set_rates(self, re, rates: dict[int, float]) -> None:
+        """Host-set base rates by RXN_ID_ (the reaction's type is looked up)."""
+        for rid, rate in rates.items():
+            rtype = self.mech.rxns[self.mech.rate_ids[int(rid)]].rxn_type
+            self.lib.om_set_rate(self.h, re, int(rtype), int(rid), float(rate))
+
     def rxn_env(self, env, photo_rates: dict[int, float] | None = None):
-        """One cell's rate constants for env=(T, P) and photolysis base rates."""
+        """One cell's rate constants for env=(T, P) and host-set base rates
+        keyed by RXN_ID_ (photolysis, first-order loss, emission, wet
+        deposition)."""
         re = np.zeros(max(self.n_env, 1), np.float64)
-        for pid, rate in (photo_rates or {}).items():
-            self.lib.om_set_photo_rate(self.h, re, int(pid), float(rate))
+        self._set_rates(re, photo_rates or {})
         self.lib.om_update_env(self.h, np.asarray(env, np.float64), re)
         return re
 
@@ -225,16 +235,20 @@ class OracleModel:
               max_conv_fails=1000, n_threads=1):
         """Per-cell solve; state [n_cells, n_state_var] is updated in place.
 
-        photo_rates is [n_cells, n_photo] of base rates for photolysis ids
-        1..n_photo.  Returns (n_failed, status, stats)."""
+        photo_rates is [n_cells, n_photo] of host-set base rates, one column
+        per host-rate reaction in mechanism order (``Mechanism.rate_rxns``).
+        Returns (n_failed, status, stats, state)."""
         state = np.ascontiguousarray(state, np.float64)
         n_cells = state.shape[0]
         env = np.ascontiguousarray(env, np.float64).reshape(n_cells, 2)
         re = np.zeros((n_cells, max(self.n_env, 1)), np.float64)
         photo_rates = np.asarray(photo_rates, np.float64).reshape(n_cells, -1)
+        cols = [(self.mech.rxns[i].rxn_type, self.mech.rate_id(i)) for i in self.mech.rate_rxns()]
+        if photo_rates.shape[1] != len(cols):
+            raise ValueError("photo_rates must have one column per host-rate reaction")
         for c in range(n_cells):
-            for pid in range(photo_rates.shape[1]):
-                self.lib.om_set_photo_rate(self.h, re[c], pid + 1, float(photo_rates[c, pid]))
+            for j, (rtype, rid) in enumerate(cols):
+                self.lib.om_set_rate(self.h, re[c], rtype, rid, float(photo_rates[c, j]))
         status = np.zeros(n_cells, np.int32)
         stats = (OracleStats * n_cells)()
         nf = self.lib.om_solve(
@@ -299,10 +313,22 @@ class RefModel:
 
     def set_photo_rate(self, cell: int, photo_id: int, rate: float) -> None:
         """Goes through the reference's rxn_update_data path."""
-        ud = self.lib.rxn_photolysis_create_rate_update_data()
-        self.lib.rxn_photolysis_set_rate_update_data(ud, int(photo_id), float(rate))
-        rid = C.c_int(0)
-        self.lib.rxn_update_data(int(cell), C.byref(rid), 5, ud, self.h)
+        self.set_rate(cell, 5, photo_id, rate)
+
+    def set_rate(self, cell: int, rxn_type: int, rxn_id: int, rate: float) -> None:
+        """A host-rate update through the reference's own update-data
+        functions of that type and its rxn_update_data."""
+        kind = {5: "photolysis", 12: "first_order_loss", 13: "emission",
+                14: "wet_deposition"}[int(rxn_type)]
+        ud = getattr(self.lib, f"rxn_{kind}_create_rate_update_data")()
+        getattr(self.lib, f"rxn_{kind}_set_rate_update_data")(ud, int(rxn_id), float(rate))
+        cursor = C.c_int(0)
+        self.lib.rxn_update_data(int(cell), C.byref(cursor), int(rxn_type), ud, self.h)
+
+    def set_rates(self, cell: int, row) -> None:
+        """One cell's host-rate columns (``Mechanism.rate_rxns`` order)."""
+        for j, i in enumerate(self.mech.rate_rxns()):
+            self.set_rate(cell, self.mech.rxns[i].rxn_type, self.mech.rate_id(i), float(row[j]))
 
     def set_cell(self, cell, state, env):
         self.state[cell, :] = state
@@ -372,8 +398,7 @@ def ref_solve(mech, state, env, photo_rates, t0, t1, rtol, abs_tol, max_steps=10
                 if vt == 2:
                     st[i] = max(st[i], TINY)
             rm.set_cell(c, st, env[c0 + c])
-            for pid in range(photo_rates.shape[1]):
-                rm.set_photo_rate(c, pid + 1, photo_rates[c0 + c, pid])
+            rm.set_rates(c, photo_rates[c0 + c])
             rm.update_env(c)
         y = np.ascontiguousarray(np.maximum(state[c0:c1][:, dep], TINY))
         ctxs = (C.c_void_p * nc)(*[rlib.ref_cell_ctx_new(rm.h, c, t1 - t0) for c in range(nc)])

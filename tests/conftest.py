@@ -36,6 +36,29 @@ def cb05_ref():
     return dict(np.load(os.path.join(GOLDEN, "cb05cl_ae5_ref.npz")))
 
 
+# golden fixtures made by tests/golden/make_golden.py from the reference's C
+# code: cb05cl_ae5, and the gas phase of MONARCH mod37 (cb05 with dry
+# deposition, emissions and the wet deposition of one aqueous phase)
+GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas")
+
+
+@pytest.fixture(scope="session")
+def mod37():
+    from camp_b200.mechanism import Mechanism
+
+    return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_gas.mech.json"))
+
+
+@pytest.fixture(scope="session", params=GOLDEN_MECHS)
+def golden(request):
+    """(mechanism, reference outputs) of each golden fixture."""
+    from camp_b200.mechanism import Mechanism
+
+    tag = request.param
+    return (Mechanism.load(os.path.join(GOLDEN, f"{tag}.mech.json")),
+            dict(np.load(os.path.join(GOLDEN, f"{tag}_ref.npz"))))
+
+
 @pytest.fixture(scope="session")
 def lib():
     from camp_b200 import build, _lib
@@ -99,3 +122,48 @@ def chain_closed_form(k1, k2, times):
     a = np.exp(-k1 * times)
     b = k1 / (k2 - k1) * (np.exp(-k1 * times) - np.exp(-k2 * times))
     return np.stack([a, b, 1.0 - a - b], axis=1)
+
+
+def species_rate_case(kind):
+    """The systems of the reference's EMISSION, FIRST_ORDER_LOSS and
+    WET_DEPOSITION unit tests (test/unit_rxn_data/test_rxn_emission.F90:
+    112-121,245-286, test_rxn_first_order_loss.F90:112-121,245-286,
+    test_rxn_wet_deposition.F90:119-128,314-367), packed directly.
+
+    Returns (mechanism, y0, first_rates, rates, truth): the second reaction's
+    base rate is first set to first_rates and then reset to rates, as those
+    tests do; truth(t) is the closed form at times t, [len(t), n_state]."""
+    from camp_b200.mechanism import (RXN_EMISSION, RXN_FIRST_ORDER_LOSS, Mechanism,
+                                     assign_rate_ids, pack_species_rate, pack_wet_deposition)
+
+    if kind in ("EMISSION", "FIRST_ORDER_LOSS"):
+        rtype = RXN_EMISSION if kind == "EMISSION" else RXN_FIRST_ORDER_LOSS
+        rxns = [pack_species_rate(rtype, 1, 1.0, "rxn A"), pack_species_rate(rtype, 2, 12.3, "rxn B")]
+        names, y0 = ["A", "B"], np.array([1.0, 1.0])
+        first = np.array([0.954, 42.11 if kind == "EMISSION" else 432.3])
+        rates = np.array([0.954, 1.0e-2])
+        k = np.array([0.954, 1.0e-2 * 12.3])
+        if kind == "EMISSION":
+            def truth(t):
+                return y0[None, :] + k[None, :] * np.asarray(t, float)[:, None]
+        else:
+            def truth(t):
+                return y0[None, :] * np.exp(-k[None, :] * np.asarray(t, float)[:, None])
+    else:
+        # two instances (1, 2) of phases rain (A, B) and cloud (B, C)
+        names = ["1.rain.A", "1.rain.B", "1.cloud.B", "1.cloud.C",
+                 "2.rain.A", "2.rain.B", "2.cloud.B", "2.cloud.C"]
+        y0 = np.array([1.0, 2.2, 1.7, 2.4, 2.5, 0.7, 1.6, 1.9])
+        rxns = [pack_wet_deposition([1, 2, 5, 6], 1.0, "rxn rain"),
+                pack_wet_deposition([3, 4, 7, 8], 12.3, "rxn cloud")]
+        first = np.array([0.954, 43912.5])
+        rates = np.array([0.954, 1.0e-2])
+        krow = np.array([0.954, 0.954, 0.123, 0.123, 0.954, 0.954, 0.123, 0.123])
+
+        def truth(t):
+            return y0[None, :] * np.exp(-krow[None, :] * np.asarray(t, float)[:, None])
+    ids = assign_rate_ids(rxns)
+    n = len(names)
+    mech = Mechanism(kind.lower(), names, np.ones(n, np.int32), np.full(n, 1.0e-12), 1.0e-10,
+                     rxns, ids)
+    return mech, y0, first, rates, truth

@@ -7,7 +7,17 @@ Outputs (all small):
                          would hand it to rxn_add_condensed_data (packer:
                          camp_b200/mechanism.py), with the photolysis ids the
                          reference's cb05 test assigns
-  cb05cl_ae5_ref.npz     outputs of the reference's own C code
+  monarch_mod37_gas.mech.json
+                         the gas-phase part of the shipped MONARCH mod37
+                         configuration (mechanisms/monarch_mod37: cb05, 45
+                         FIRST_ORDER_LOSS dry-deposition and 36 EMISSION
+                         reactions) plus its WET_DEPOSITION of the "cloud and
+                         rain water" phase, whose 49 species are appended as
+                         state variables (no aerosol representation is read;
+                         the packed wet-deposition data lists their indices as
+                         the Fortran packer would)
+  cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz
+                         outputs of the reference's own C code
                          (oracle/_ref/libcamp_ref.so, compiled from the
                          reference sources) on seeded cell states:
                          sparsity (solver CSC, reaction CSC, jac_map, packed
@@ -32,7 +42,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from camp_b200.cells import make_cells  # noqa: E402
-from camp_b200.mechanism import load_mechanism  # noqa: E402
+from camp_b200.mechanism import (CHEM_SPEC_VARIABLE, assign_rate_ids, load_mechanism,  # noqa: E402
+                                 pack_wet_deposition)
 
 SEED = 20241203
 H_VALUES = (1.0e-6, 1.0, 60.0)
@@ -44,6 +55,33 @@ def cb05_files(ref_root: str) -> list[str]:
         os.path.join(ref_root, "mechanisms/cb05cl_ae5/cb05cl_ae5_species.json"),
         os.path.join(ref_root, "test/chemistry/cb05cl_ae5/cb05cl_ae5_init.json"),
     ]
+
+
+MOD37_GAS_FILES = ("cb05_species.json", "cb05_abs_tol.json", "cb05_mechanism.json",
+                   "custom_species.json", "dry_deposition.json", "HERMES_emissions_rxns.json",
+                   "MEGAN_emissions_rxns.json")
+RAIN_PHASE = "cloud and rain water"
+
+
+def mod37_gas(ref_root: str):
+    import json
+
+    base = os.path.join(ref_root, "mechanisms/monarch_mod37")
+    mech = load_mechanism([os.path.join(base, f) for f in MOD37_GAS_FILES],
+                          name="monarch_mod37_gas")
+    with open(os.path.join(base, "aerosol_phases.json")) as fh:
+        phases = {o["name"]: o["species"] for o in json.load(fh)["camp-data"]
+                  if o.get("type") == "AERO_PHASE"}
+    first = mech.n_state_var
+    names = [f"{RAIN_PHASE}.{sp}" for sp in phases[RAIN_PHASE]]
+    mech.species = mech.species + names
+    mech.var_type = np.concatenate([mech.var_type,
+                                    np.full(len(names), CHEM_SPEC_VARIABLE, np.int32)])
+    mech.abs_tol = np.concatenate([mech.abs_tol, np.full(len(names), 1.0e-8)])
+    mech.rxns.append(pack_wet_deposition(list(range(first + 1, first + len(names) + 1)),
+                                         1.0, "rain loss"))
+    mech.rate_ids = assign_rate_ids(mech.rxns)
+    return mech
 
 
 def edge_cells(mech, cells):
@@ -70,13 +108,19 @@ def edge_cells(mech, cells):
 
 def main(ref_root: str) -> None:
     sys.path.insert(0, ROOT)
-    from oracle.oracle import RefModel, build  # noqa: E402
+    from oracle.oracle import build  # noqa: E402
 
     build(with_ref=True)
-    mech = load_mechanism(cb05_files(ref_root), name="cb05cl_ae5")
+    write_fixture(load_mechanism(cb05_files(ref_root), name="cb05cl_ae5"), "cb05cl_ae5")
+    write_fixture(mod37_gas(ref_root), "monarch_mod37_gas")
+
+
+def write_fixture(mech, tag: str) -> None:
+    from oracle.oracle import RefModel  # noqa: E402
+
     mech.rel_tol = 1.0e-4
     mech.abs_tol[:] = 1.0e-8
-    mech.save(os.path.join(HERE, "cb05cl_ae5.mech.json"))
+    mech.save(os.path.join(HERE, f"{tag}.mech.json"))
 
     cells = make_cells(mech, 8, SEED)
     state, env, photo = edge_cells(mech, cells)
@@ -94,8 +138,7 @@ def main(ref_root: str) -> None:
     rxn_env, F, RP, RL, J = [], [], [], [], []
     for c in range(nc):
         ref.set_cell(c, state[c], env[c])
-        for pid in range(photo.shape[1]):
-            ref.set_photo_rate(c, pid + 1, photo[c, pid])
+        ref.set_rates(c, photo[c])
         ref.update_env(c)
         rxn_env.append(ref.rxn_env(c))
     for h in H_VALUES:
@@ -107,8 +150,8 @@ def main(ref_root: str) -> None:
         F.append(fs); RP.append(rps); RL.append(rls); J.append(js)
     out["rxn_env"] = np.asarray(rxn_env)
     out["f"], out["r_p"], out["r_l"], out["jac"] = (np.asarray(x) for x in (F, RP, RL, J))
-    np.savez_compressed(os.path.join(HERE, "cb05cl_ae5_ref.npz"), **out)
-    print("wrote", nc, "cells;", "jac nnz", len(ri), "rxn jac nnz", len(rri))
+    np.savez_compressed(os.path.join(HERE, f"{tag}_ref.npz"), **out)
+    print(tag, "wrote", nc, "cells;", "jac nnz", len(ri), "rxn jac nnz", len(rri))
 
 
 if __name__ == "__main__":

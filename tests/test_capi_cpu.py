@@ -29,28 +29,47 @@ def test_exports_every_declared_symbol(lib):
     assert sorted(_lib.EXPORTED) == names
 
 
-def test_sparsity_via_c_abi(cb05, cb05_ref, lib):
+def test_sparsity_via_c_abi(golden, lib):
     from camp_b200.solver import Solver
 
-    s = Solver(cb05, 4)
+    mech, ref = golden
+    s = Solver(mech, 4)
     s.build_sparsity_only()
     if not gpu_available():
         assert not s.ready
     cp, ri = s.solver_jac()
-    assert np.array_equal(cp, cb05_ref["solver_colptr"])
-    assert np.array_equal(ri, cb05_ref["solver_rowid"])
+    assert np.array_equal(cp, ref["solver_colptr"])
+    assert np.array_equal(ri, ref["solver_rowid"])
     # DERIV_ID_/JAC_ID_ of every reaction, bit for bit
-    assert np.array_equal(s.rxn_int_data(), cb05_ref["rxn_int_data"])
+    assert np.array_equal(s.rxn_int_data(), ref["rxn_int_data"])
     perm = s.lu_order()
-    assert sorted(perm.tolist()) == list(range(74))
-    assert s.n_lu() <= 748
+    assert sorted(perm.tolist()) == list(range(mech.n_dep_var))
+    if mech.name == "cb05cl_ae5":
+        assert s.n_lu() <= 748
 
 
-def test_photolysis_update_data_layout(lib):
-    """int photo id followed, unaligned, by the double base rate
-    (src/rxns/rxn_photolysis.c:262-283)."""
-    ud = lib.rxn_photolysis_create_rate_update_data()
-    lib.rxn_photolysis_set_rate_update_data(ud, 7, 2.5e-3)
+def test_host_rate_columns(mod37, lib):
+    """One base-rate column per PHOTOLYSIS / FIRST_ORDER_LOSS / EMISSION /
+    WET_DEPOSITION reaction in mechanism order, each with its type and id,
+    known as soon as the reactions are added."""
+    from camp_b200.solver import Solver
+
+    s = Solver(mech := mod37, 2)
+    cols = mech.rate_rxns()
+    assert s.n_photo == len(cols) == 107
+    for j, i in enumerate(cols):
+        assert s.rate_column(j) == (i, mech.rxns[i].rxn_type, mech.rate_id(i))
+    assert lib.camp_b200_rate_column(s._h, len(cols), None, None, None) == -1
+
+
+@pytest.mark.parametrize("kind", ["photolysis", "emission", "first_order_loss",
+                                  "wet_deposition"])
+def test_rate_update_data_layout(lib, kind):
+    """int reaction id followed, unaligned, by the double base rate
+    (src/rxns/rxn_photolysis.c:262-283, rxn_emission.c:192-213,
+    rxn_first_order_loss.c:208-229, rxn_wet_deposition.c:218-239)."""
+    ud = getattr(lib, f"rxn_{kind}_create_rate_update_data")()
+    getattr(lib, f"rxn_{kind}_set_rate_update_data")(ud, 7, 2.5e-3)
     raw = C.string_at(ud, 12)
     assert int.from_bytes(raw[:4], "little", signed=True) == 7
     assert np.frombuffer(raw[4:12], np.float64)[0] == 2.5e-3
@@ -95,6 +114,24 @@ def test_packer_matches_fixture(cb05):
     summ = reaction_summary(m)
     assert summ["by_type"] == {5: 25, 1: 142, 2: 15, 4: 1, 3: 3}
     for a, b in zip(m.rxns, cb05.rxns):
+        assert a.rxn_type == b.rxn_type
+        assert np.array_equal(a.ints, b.ints)
+        assert np.array_equal(a.floats, b.floats)
+
+
+def test_mod37_packer_matches_fixture(mod37):
+    ref = "/root/reference"
+    if not os.path.isdir(ref):
+        pytest.skip("reference tree absent")
+    import sys
+
+    sys.path.insert(0, GOLDEN)
+    from make_golden import mod37_gas
+
+    m = mod37_gas(ref)
+    assert m.species == mod37.species
+    assert len(m.rxns) == len(mod37.rxns) == 268
+    for a, b in zip(m.rxns, mod37.rxns):
         assert a.rxn_type == b.rxn_type
         assert np.array_equal(a.ints, b.ints)
         assert np.array_equal(a.floats, b.floats)

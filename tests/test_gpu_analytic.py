@@ -73,3 +73,36 @@ def test_chain_through_json_entry_point(tmp_path, rtype):
         lib.solver_free(h)
     np.testing.assert_allclose(state, np.tile(chain_closed_form(k1, k2, [30.0]), (n, 1)),
                                rtol=1e-6, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("kind", ["EMISSION", "FIRST_ORDER_LOSS", "WET_DEPOSITION"])
+def test_host_rate_types_known_answer(kind, precision):
+    """The reference's EMISSION, FIRST_ORDER_LOSS and WET_DEPOSITION unit
+    tests: rates set per cell through the update-data functions and
+    rxn_update_data (the second one set, then reset), ten 1-s host steps
+    through solver_run, against the closed forms."""
+    from conftest import species_rate_case
+
+    from camp_b200.solver import Solver
+
+    mech, y0, first, rates, truth = species_rate_case(kind)
+    n = 4
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.full(y0.size, 1e-14), rel_tol=1e-10, max_steps=100000)
+    s.set_precision(precision)
+    cols = mech.rate_rxns()
+    for c in range(n):
+        for vals in (first, rates):
+            for j, i in enumerate(cols):
+                s.set_rate(c, mech.rxns[i].rxn_type, mech.rate_id(i), float(vals[j]))
+    y = np.tile(y0, (n, 1))
+    env = np.tile(np.array([298.0, 1.0e5]), (n, 1))
+    out = []
+    for step in range(10):
+        assert s.solve(y, env, float(step), float(step + 1)) == 0, s.cell_stats()["status"]
+        out.append(y.copy())
+    out = np.stack(out)  # [step, cell, species]
+    expect = truth(np.arange(1, 11))
+    for c in range(n):
+        np.testing.assert_allclose(out[:, c], expect, rtol=1e-7, atol=1e-14)

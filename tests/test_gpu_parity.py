@@ -1,5 +1,7 @@
 """GPU parity: the CUDA path through the C ABI against the reference's C
-derivative/Jacobian (golden fixture) and against the CPU oracle's solve."""
+derivative/Jacobian (golden fixtures: cb05cl_ae5 and the gas phase of MONARCH
+mod37 with its deposition and emission reactions) and against the CPU
+oracle's solve."""
 import numpy as np
 import pytest
 
@@ -12,16 +14,18 @@ RTOL_FJ = 1e-12  # derivative / Jacobian parity with the reference's FP64 C code
 
 
 @pytest.fixture(scope="module")
-def solver(cb05, cb05_ref):
+def solver_ref(golden):
     from camp_b200.solver import Solver
 
-    nc = cb05_ref["state"].shape[0]
-    s = Solver(cb05, max(nc, 256))
-    s.initialize(abs_tol=np.full(cb05.n_state_var, 1e-8), rel_tol=1e-4)
-    return s
+    mech, ref = golden
+    nc = ref["state"].shape[0]
+    s = Solver(mech, max(nc, 256))
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4)
+    return s, ref
 
 
-def test_deriv_matches_reference(solver, cb05_ref):
+def test_deriv_matches_reference(solver_ref):
+    solver, cb05_ref = solver_ref
     nc = cb05_ref["state"].shape[0]
     photo = np.zeros((solver.n_cells, solver.n_photo))
     photo[:nc] = cb05_ref["photo"]
@@ -34,7 +38,8 @@ def test_deriv_matches_reference(solver, cb05_ref):
         assert np.all(np.abs(f - cb05_ref["f"][ih]) <= RTOL_FJ * scale)
 
 
-def test_jacobian_matches_reference(solver, cb05_ref):
+def test_jacobian_matches_reference(solver_ref):
+    solver, cb05_ref = solver_ref
     nc = cb05_ref["state"].shape[0]
     photo = np.zeros((solver.n_cells, solver.n_photo))
     photo[:nc] = cb05_ref["photo"]
@@ -109,6 +114,14 @@ def test_fp64_solve_matches_oracle(cb05):
 
 def test_mixed_solve_matches_oracle(cb05):
     _check_solve(cb05, precision=1, seed=12, bulk_rel=1e-4)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mod37_gas_solve_matches_oracle(mod37, precision):
+    """cb05 with dry deposition, emissions and wet deposition: the same
+    outcome per cell and the oracle's accuracy at equal tolerances."""
+    _check_solve(mod37, precision=precision, seed=13 + precision,
+                 bulk_rel=1e-7 if precision == 0 else 1e-4)
 
 
 def test_failed_cells_keep_input_state(cb05):

@@ -100,6 +100,10 @@ def test_every_gas_type_and_option(tmp_path):
              "k3_A": 6.5e-34, "k3_C": 1335.0},
             {"type": "PHOTOLYSIS", "reactants": {"C": {}}, "products": {"A": {}, "B": {"yield": -0.5}},
              "scaling factor": 2.0},
+            {"type": "FIRST_ORDER_LOSS", "species": "A", "scaling factor": 0.5,
+             "rxn id": "dep A"},
+            {"type": "EMISSION", "species": "C", "rxn id": "emis C"},
+            {"type": "PHOTOLYSIS", "reactants": {"A": {}}, "products": {"C": {}}},
         ]},
     ]}
     paths = []
@@ -109,6 +113,39 @@ def test_every_gas_type_and_option(tmp_path):
             json.dump(obj, fh)
         paths.append(p)
     _compare(paths)
+
+
+REF_MOD37 = "/root/reference/mechanisms/monarch_mod37"
+REF_UNIT = "/root/reference/test/unit_rxn_data"
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_MOD37), reason="reference tree not present")
+def test_mod37_gas_from_reference_files():
+    """cb05 with dry deposition (FIRST_ORDER_LOSS) and emissions (EMISSION),
+    the gas-phase files of the shipped MONARCH mod37 configuration."""
+    files = ["cb05_species.json", "cb05_abs_tol.json", "cb05_mechanism.json",
+             "custom_species.json", "dry_deposition.json", "HERMES_emissions_rxns.json",
+             "MEGAN_emissions_rxns.json"]
+    _compare([os.path.join(REF_MOD37, f) for f in files])
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_UNIT), reason="reference tree not present")
+@pytest.mark.parametrize("name", ["test_emission.json", "test_first_order_loss.json"])
+def test_reference_unit_test_inputs(name):
+    _compare([os.path.join(REF_UNIT, name)])
+
+
+def test_wet_deposition_needs_packed_data(tmp_path):
+    p = os.path.join(tmp_path, "wet.json")
+    with open(p, "w") as fh:
+        json.dump({"camp-data": [
+            {"name": "A", "type": "CHEM_SPEC"},
+            {"name": "m", "type": "MECHANISM", "reactions": [
+                {"type": "WET_DEPOSITION", "aerosol phase": "rain"}]}]}, fh)
+    lib = _lib.load()
+    arr = (C.c_char_p * 1)(p.encode())
+    assert not lib.camp_b200_solver_from_json(arr, 1, 1)
+    assert "WET_DEPOSITION" in _lib.last_error()
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_CB05), reason="reference tree not present")

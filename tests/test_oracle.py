@@ -1,10 +1,11 @@
 """The CPU oracle pinned against the reference's own C code.
 
-The golden fixture (tests/golden/cb05cl_ae5_ref.npz) holds the reference's
-sparsity, rate constants, derivative and Jacobian on seeded cb05cl_ae5 cells,
-computed by the reference's C sources (tests/golden/make_golden.py).  The
-oracle's restatement must reproduce the sparsity bit-exactly and the
-numbers to 1e-12 relative.
+The golden fixtures (tests/golden/*_ref.npz) hold the reference's sparsity,
+rate constants, derivative and Jacobian on seeded cells of cb05cl_ae5 and of
+the gas phase of MONARCH mod37 (cb05 plus FIRST_ORDER_LOSS dry deposition,
+EMISSION and WET_DEPOSITION), computed by the reference's C sources
+(tests/golden/make_golden.py).  The oracle's restatement must reproduce the
+sparsity and packed ints bit-exactly and the numbers to 1e-12 relative.
 """
 import numpy as np
 import pytest
@@ -17,15 +18,22 @@ def om(cb05):
     return OracleModel(cb05)
 
 
-def test_sparsity_bit_exact(om, cb05_ref):
+@pytest.fixture(scope="module")
+def gom(golden):
+    mech, ref = golden
+    return OracleModel(mech), ref
+
+
+def test_sparsity_bit_exact(gom):
+    om, ref = gom
     cp, ri = om.solver_jac()
-    assert np.array_equal(cp, cb05_ref["solver_colptr"])
-    assert np.array_equal(ri, cb05_ref["solver_rowid"])
+    assert np.array_equal(cp, ref["solver_colptr"])
+    assert np.array_equal(ri, ref["solver_rowid"])
     rcp, rri = om.rxn_jac()
-    assert np.array_equal(rcp, cb05_ref["rxn_colptr"])
-    assert np.array_equal(rri, cb05_ref["rxn_rowid"])
+    assert np.array_equal(rcp, ref["rxn_colptr"])
+    assert np.array_equal(rri, ref["rxn_rowid"])
     # DERIV_ID_/JAC_ID_ written back into the packed ints
-    assert np.array_equal(om.rxn_int_data(), cb05_ref["rxn_int_data"])
+    assert np.array_equal(om.rxn_int_data(), ref["rxn_int_data"])
 
 
 def test_sizes(om):
@@ -38,39 +46,56 @@ def _photo_dict(row):
     return {pid + 1: float(row[pid]) for pid in range(row.size)}
 
 
-def test_rate_constants(om, cb05_ref):
-    for c in range(cb05_ref["state"].shape[0]):
-        re = om.rxn_env(cb05_ref["env"][c], _photo_dict(cb05_ref["photo"][c]))
-        np.testing.assert_allclose(re, cb05_ref["rxn_env"][c], rtol=1e-15, atol=0)
+def test_rate_constants(gom):
+    om, ref = gom
+    for c in range(ref["state"].shape[0]):
+        re = om.rxn_env(ref["env"][c], _photo_dict(ref["photo"][c]))
+        np.testing.assert_allclose(re, ref["rxn_env"][c], rtol=1e-15, atol=0)
 
 
-def test_deriv_and_jacobian(om, cb05_ref):
-    for ih, h in enumerate(cb05_ref["h"]):
-        for c in range(cb05_ref["state"].shape[0]):
-            re = cb05_ref["rxn_env"][c]
-            st = cb05_ref["state"][c]
+def test_deriv_and_jacobian(gom):
+    om, ref = gom
+    for ih, h in enumerate(ref["h"]):
+        for c in range(ref["state"].shape[0]):
+            re = ref["rxn_env"][c]
+            st = ref["state"][c]
             f, rp, rl = om.deriv(st, re, h)
-            np.testing.assert_allclose(rp, cb05_ref["r_p"][ih][c], rtol=1e-12, atol=0)
-            np.testing.assert_allclose(rl, cb05_ref["r_l"][ih][c], rtol=1e-12, atol=0)
-            scale = cb05_ref["r_p"][ih][c] + cb05_ref["r_l"][ih][c]
-            assert np.all(np.abs(f - cb05_ref["f"][ih][c]) <= 1e-12 * scale)
+            np.testing.assert_allclose(rp, ref["r_p"][ih][c], rtol=1e-12, atol=0)
+            np.testing.assert_allclose(rl, ref["r_l"][ih][c], rtol=1e-12, atol=0)
+            scale = ref["r_p"][ih][c] + ref["r_l"][ih][c]
+            assert np.all(np.abs(f - ref["f"][ih][c]) <= 1e-12 * scale)
             j = om.jac(st, re, h)
-            jr = cb05_ref["jac"][ih][c]
+            jr = ref["jac"][ih][c]
             assert np.all(np.abs(j - jr) <= 1e-12 * np.abs(jr) + 1e-300)
 
 
+def test_mod37_gas_composition(mod37):
+    """The mod37 gas-phase fixture holds every host-rate type: its rate
+    columns are photolysis, dry deposition, emissions and the wet
+    deposition, with ids 1..n in mechanism order."""
+    from camp_b200.mechanism import reaction_summary
+
+    by_type = reaction_summary(mod37)["by_type"]
+    assert by_type[12] == 45 and by_type[13] == 36 and by_type[14] == 1 and by_type[5] == 25
+    cols = mod37.rate_rxns()
+    assert [mod37.rate_id(i) for i in cols] == list(range(1, len(cols) + 1))
+    assert sorted(mod37.rate_ids) == list(range(1, len(cols) + 1))
+
+
 @pytest.mark.skipif(not ref_available(), reason="reference build absent")
-def test_live_against_reference_build(cb05, om):
+@pytest.mark.parametrize("which", ["cb05", "mod37"])
+def test_live_against_reference_build(request, which):
     """Fresh random states through the reference build and the oracle."""
     from camp_b200.cells import make_cells
     from oracle.oracle import RefModel
 
-    cells = make_cells(cb05, 5, 777)
-    ref = RefModel(cb05, 5)
+    mech = request.getfixturevalue(which)
+    om = OracleModel(mech)
+    cells = make_cells(mech, 5, 777)
+    ref = RefModel(mech, 5)
     for c in range(5):
         ref.set_cell(c, cells.state[c], cells.env[c])
-        for pid in range(cells.photo_rates.shape[1]):
-            ref.set_photo_rate(c, pid + 1, cells.photo_rates[c, pid])
+        ref.set_rates(c, cells.photo_rates[c])
         ref.update_env(c)
         re = om.rxn_env(cells.env[c], _photo_dict(cells.photo_rates[c]))
         assert np.array_equal(re, ref.rxn_env(c))
@@ -151,3 +176,48 @@ def test_zero_length_step_is_too_close(cb05):
                                                  np.full(cb05.n_state_var, 1e-8))
     assert nf == 2 and list(status) == [-27, -27]
     np.testing.assert_array_equal(out, cells.state)
+
+
+@pytest.mark.parametrize("kind", ["EMISSION", "FIRST_ORDER_LOSS", "WET_DEPOSITION"])
+def test_host_rate_types_known_answer(kind):
+    """The reference's unit-test systems for the host-rate types, integrated
+    over ten 1-s host steps, against their closed forms."""
+    from conftest import species_rate_case
+
+    mech, y0, _, rates, truth = species_rate_case(kind)
+    om = OracleModel(mech)
+    y = y0[None, :].copy()
+    out = []
+    for step in range(10):
+        nf, status, _, y = om.solve(y, np.array([[298.0, 1.0e5]]), rates[None, :], float(step),
+                                    float(step + 1), 1e-10, np.full(y0.size, 1e-14),
+                                    max_steps=100000)
+        assert nf == 0, status
+        out.append(y[0].copy())
+    np.testing.assert_allclose(out, truth(np.arange(1, 11)), rtol=1e-7, atol=1e-14)
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("kind", ["EMISSION", "FIRST_ORDER_LOSS", "WET_DEPOSITION"])
+def test_host_rate_updates_match_reference(kind):
+    """Rate updates through the reference's own update-data functions (a
+    value, then a reset) give the oracle's rate constants, f and J."""
+    from conftest import species_rate_case
+    from oracle.oracle import RefModel
+
+    mech, y0, first, rates, _ = species_rate_case(kind)
+    om = OracleModel(mech)
+    ref = RefModel(mech, 1)
+    ref.set_cell(0, y0, np.array([298.0, 1.0e5]))
+    ref.set_rates(0, first)
+    ref.set_rates(0, rates)
+    ref.update_env(0)
+    re = om.rxn_env([298.0, 1.0e5], {i + 1: float(r) for i, r in enumerate(rates)})
+    assert np.array_equal(re, ref.rxn_env(0))
+    assert np.array_equal(om.rxn_int_data(), ref.rxn_int_data())
+    f1, p1, l1 = ref.deriv(0, 1.0)
+    f2, p2, l2 = om.deriv(y0, re, 1.0)
+    np.testing.assert_allclose(p2, p1, rtol=1e-15, atol=0)
+    np.testing.assert_allclose(l2, l1, rtol=1e-15, atol=0)
+    j1, _ = ref.jac(0, 1.0)
+    np.testing.assert_allclose(om.jac(y0, re, 1.0), j1, rtol=1e-15, atol=0)
