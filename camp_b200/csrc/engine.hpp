@@ -77,6 +77,9 @@ class Engine {
   bool sync(void* stream, std::string* err);
   // cells (warps) per block that fit the shared memory for these settings
   int max_cells_per_block(const SolveSettings& s) const;
+  // false (with the reason) when the mechanism exceeds the warp-per-cell
+  // tables, so that only the lane-per-cell kernel can run it
+  bool warp_tables(std::string* err) const;
   // Serving slots: a launch on caller-provided buffers and scratch (from
   // slot_scratch_bytes for at most max_blocks blocks), so several launches
   // can be in flight on different streams; d_tspan holds each cell's

@@ -89,7 +89,8 @@ struct LaneLayout {
 struct LaneArgs {
   DevMech m;
   const void* blob;
-  int tab_bytes;
+  int tab_bytes;   // shared-memory bytes of the staged tables (0 when global)
+  int tab_global;  // 1: tables too large for shared memory, read from global
   LaneLayout lay;
   double* state;
   const double* env;
@@ -238,8 +239,25 @@ __device__ __noinline__ int op_factor(const char* tb, LS<LT>* s) {
     for (int q = t.lu_rowptr[i]; q < d; ++q) {
       const LT l = AT(LU, q) * (LT)AT(dinv, t.lu_col[q]);
       AT(LU, q) = l;
+      // the update list of L entry (i, k) targets distinct entries of row i
+      // and reads row k, so a group's loads can all be issued before its
+      // stores: eight updates wait for one memory latency instead of eight
       const uint32_t p1 = t.upd_ptr[q + 1];
-      for (uint32_t p = t.upd_ptr[q]; p < p1; ++p) {
+      uint32_t p = t.upd_ptr[q];
+      for (; p + 8 <= p1; p += 8) {
+        uint32_t u[8];
+        LT a[8], b[8];
+        #pragma unroll
+        for (int j = 0; j < 8; ++j) u[j] = t.upd[p + j];
+        #pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          a[j] = AT(LU, u[j] >> 16);
+          b[j] = AT(LU, u[j] & 0xFFFFu);
+        }
+        #pragma unroll
+        for (int j = 0; j < 8; ++j) AT(LU, u[j] >> 16) = a[j] - l * b[j];
+      }
+      for (; p < p1; ++p) {
         const uint32_t u = t.upd[p];
         AT(LU, u >> 16) -= l * AT(LU, u & 0xFFFFu);
       }
@@ -935,8 +953,10 @@ template <typename LT>
 __global__ void __launch_bounds__(512, 1) lane_kernel(LaneArgs a) {
   extern __shared__ __align__(16) char smem[];
   __shared__ unsigned long long tma_bar;
-  // stage the tables (bulk copy, bounded wait)
-  {
+  // stage the tables (bulk copy, bounded wait); tables larger than shared
+  // memory stay in global memory, where every read is warp-uniform (one
+  // broadcast line through L1, the lines shared by all warps in L2)
+  if (!a.tab_global) {
     const unsigned b = (unsigned)__cvta_generic_to_shared(&tma_bar);
     if (threadIdx.x == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
@@ -971,7 +991,7 @@ __global__ void __launch_bounds__(512, 1) lane_kernel(LaneArgs a) {
     }
     if (!__syncthreads_and(done ? 1 : 0)) return;
   }
-  const char* tb = smem;
+  const char* tb = a.tab_global ? (const char*)a.blob : smem;
   const Tab t = make_tab(tb);
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -1083,6 +1103,7 @@ static bool lane_layout(const LaneOff& o, int lt_size, int max_smem_block, int t
   L.wlt = std::max(elt, 1);
   int w = warps_per_block;
   const int avail = max_smem_block - tab_bytes;
+  if (avail < 0) return false;
   const int fit = L.smem_bytes_per_warp > 0 ? avail / std::max(1, L.smem_bytes_per_warp) : 16;
   if (fit < 1) return false;
   if (w <= 0) w = std::min(fit, 16);
@@ -1121,12 +1142,22 @@ bool lanes_launch(const DevMech& m, const void* d_blob, const LaneOff& off, doub
                   int sm_count, int max_smem, void* stream, std::string* err) {
   cudaStream_t st = (cudaStream_t)stream;
   const int lt = s.precision == 1 ? 4 : 8;
-  const int tab = (off.bytes + 127) & ~127;
+  int tab = (off.bytes + 127) & ~127;
+  int tab_global = 0;
   lanes::LaneLayout L;
   int warps = 0;
-  if (!lane_layout(off, lt, max_smem, tab, s.warps_per_block, s.lane_place, &L, &warps)) {
-    *err = "lane layout does not fit shared memory (try another placement)";
-    return false;
+  // the requested placement with the tables staged, else everything per lane
+  // in global memory, else the tables in global memory too (mechanisms whose
+  // LU schedule alone exceeds shared memory)
+  if (!lane_layout(off, lt, max_smem, tab, s.warps_per_block, s.lane_place, &L, &warps) &&
+      !lane_layout(off, lt, max_smem, tab, s.warps_per_block, 0, &L, &warps)) {
+    tab = 0;
+    tab_global = 1;
+    if (!lane_layout(off, lt, max_smem, 0, s.warps_per_block, s.lane_place, &L, &warps) &&
+        !lane_layout(off, lt, max_smem, 0, s.warps_per_block, 0, &L, &warps)) {
+      *err = "lane layout does not fit shared memory";
+      return false;
+    }
   }
   int grid = sm_count * std::max(1, s.blocks_per_sm);
   const long lanes_total = (long)grid * warps * 32;
@@ -1139,6 +1170,7 @@ bool lanes_launch(const DevMech& m, const void* d_blob, const LaneOff& off, doub
   a.m = m;
   a.blob = d_blob;
   a.tab_bytes = tab;
+  a.tab_global = tab_global;
   a.lay = L;
   a.state = d_state;
   a.env = d_env;

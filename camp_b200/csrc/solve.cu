@@ -1492,6 +1492,11 @@ struct Engine::Impl {
   DevMech m{};
   BlobOff off{};
   void* d_blob = nullptr;
+  // the warp-per-cell tables use 16-bit encodings; a mechanism beyond them
+  // (e.g. an LU with hundreds of thousands of Schur updates) runs on the
+  // lane-per-cell kernel only, and warp_why says why
+  bool warp_ok = true;
+  std::string warp_why;
   LaneOff loff{};
   void* d_lblob = nullptr;
   void *d_scr64 = nullptr, *d_scrlt = nullptr;
@@ -1633,11 +1638,14 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   CK(cudaMemcpy(I->d_tables, pk.blob.data(), pk.blob.size(), cudaMemcpyHostToDevice));
   for (auto& f : pk.fix) *f.second = (const void*)((char*)I->d_tables + f.first);
   std::vector<uint8_t> blob;
-  if (!build_blob(t, atol_dep, &blob, &I->off, err)) return false;
   if (I->d_blob) cudaFree(I->d_blob);
   I->d_blob = nullptr;
-  CK(cudaMalloc(&I->d_blob, blob.size()));
-  CK(cudaMemcpy(I->d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  I->warp_why.clear();
+  I->warp_ok = build_blob(t, atol_dep, &blob, &I->off, &I->warp_why);
+  if (I->warp_ok) {
+    CK(cudaMalloc(&I->d_blob, blob.size()));
+    CK(cudaMemcpy(I->d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  }
   std::vector<uint8_t> lblob;
   if (!build_lane_blob(t, atol_dep, &lblob, &I->loff, err)) return false;
   if (I->d_lblob) cudaFree(I->d_lblob);
@@ -1781,7 +1789,7 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   Impl* I = impl_;
   if (n_cells <= 0) return true;
   cudaStream_t st = (cudaStream_t)stream;
-  if (s.kernel == 1) {
+  if (s.kernel == 1 || !I->warp_ok) {
     if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
     CK(cudaEventRecord(I->ev0, st));
     if (!lanes_launch(I->m, I->d_lblob, I->loff, d_state, d_env, d_photo, d_order, n_cells,
@@ -1877,8 +1885,17 @@ bool Engine::launch_graph(SolveArgs& a, const WarpLaunch& w, int precision, void
   return true;
 }
 
+bool Engine::warp_tables(std::string* err) const {
+  if (impl_->warp_ok) return true;
+  *err = "this entry point runs the warp-per-cell kernel, whose tables this mechanism "
+         "exceeds (" + impl_->warp_why + "); solver_run and the device runs use the "
+         "lane-per-cell kernel for it";
+  return false;
+}
+
 size_t Engine::slot_scratch_bytes(const SolveSettings& s, int max_blocks) const {
   const Impl* I = impl_;
+  if (!I->warp_ok) return 0;
   WarpLaunch w;
   std::string err;
   if (!plan_warp_launch(I->off, I->sm_count, I->max_smem, s, 1 << 30, max_blocks, &w, &err))
@@ -1899,6 +1916,7 @@ bool Engine::launch_solve_slot(double* d_state, const double* d_env, const doubl
     *err = "serving slots run the warp-per-cell kernel only";
     return false;
   }
+  if (!warp_tables(err)) return false;
   cudaStream_t st = (cudaStream_t)stream;
   WarpLaunch w;
   if (!plan_warp_launch(I->off, I->sm_count, I->max_smem, s, n_cells, max_blocks, &w, err))
@@ -1930,7 +1948,7 @@ int Engine::sm_count() const { return impl_->sm_count; }
 
 int Engine::max_cells_per_block(const SolveSettings& s) const {
   const Impl* I = impl_;
-  if (s.kernel != 0) return 0;
+  if (s.kernel != 0 || !I->warp_ok) return 0;
   const int lt = s.precision == 1 ? 4 : 8;
   const Layout lay = make_layout(I->off, lt, s.hist_global == 0, true);
   return std::min(kMaxCellsPerBlock,
@@ -2007,6 +2025,7 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
                         int n_cells, double h, double* r_p, double* r_l, double* f,
                         std::string* err) {
   Impl* I = impl_;
+  if (!warp_tables(err)) return false;
   const DevMech& m = I->m;
   size_t ns = (size_t)n_cells * m.n_state, nn = (size_t)n_cells * m.n;
   DevBuf bs, be, bp, bo;
@@ -2052,6 +2071,7 @@ bool Engine::eval_deriv(const double* h_state, const double* h_env, const double
 bool Engine::eval_jac(const double* h_state, const double* h_env, const double* h_photo,
                       int n_cells, double h, double* jp, double* jl, std::string* err) {
   Impl* I = impl_;
+  if (!warp_tables(err)) return false;
   const DevMech& m = I->m;
   size_t ns = (size_t)n_cells * m.n_state, nj = (size_t)n_cells * m.n_jac;
   DevBuf bs, be, bp, bo;
@@ -2097,6 +2117,7 @@ bool Engine::check_jac(const double* h_state, const double* h_env, const double*
                        int n_cells, double h, double rel_tol, double abs_tol, double* worst,
                        int* nfail, std::string* err) {
   Impl* I = impl_;
+  if (!warp_tables(err)) return false;
   const DevMech& m = I->m;
   const size_t ns = (size_t)n_cells * m.n_state, nj = (size_t)n_cells * m.n_jac;
   double *ds = nullptr, *de = nullptr, *dp = nullptr, *dj = nullptr, *db = nullptr,
@@ -2213,6 +2234,7 @@ bool Engine::run_solve_static(double* d_state, const double* d_env, const double
                               CellStats* d_stats, int n_cells, double t0, double t1,
                               const SolveSettings& s, void* stream, std::string* err) {
   Impl* I = impl_;
+  if (!warp_tables(err)) return false;
   if (n_cells <= 0) return true;
   if (!d_state || !d_env || !d_stats || (I->m.n_photo > 0 && !d_photo)) {
     *err = "state, env, stats (and photolysis rates, when the mechanism has photolysis) "

@@ -1,0 +1,129 @@
+"""The lane-per-cell kernel, and the large synthetic mechanism that only it
+runs.
+
+The lane kernel (one lane per cell, 32 cells of a warp sharing every table
+read) is a second CUDA implementation of the same per-cell BDF solve; on
+cb05cl_ae5 and the mod37 gas phase it must reach the warp kernel's outcomes
+and values.  The synthetic 200-species / 600-reaction mechanism has an LU of
+18 681 entries with 622 765 Schur updates, beyond the warp kernel's 16-bit
+schedules: solver_initialize keeps only the lane kernel for it (tables read
+from global memory), solver_run uses it, and the warp-only entry points say
+why they refuse.
+
+The synthetic mechanism gains molecules in every reaction (1-4 unit-yield
+products from 1-2 reactants), so its concentrations grow quickly: at a 300 s
+host step the oracle's cells all stop at the 10 000-step limit (and at
+200 000), so the parity case uses a 0.5 s host step, which every cell
+finishes in a few hundred internal steps.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="no CUDA device")]
+
+T_LARGE = 0.5  # host step of the large-mechanism parity case (s)
+
+
+def _solve(mech, cells, precision, kernel, t1, max_steps):
+    from camp_b200.solver import Solver
+
+    s = Solver(mech, cells.n_cells)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4, max_steps=max_steps)
+    s.set_precision(precision)
+    if kernel is not None:
+        s.set_kernel(kernel)
+    s.set_photo_rates(cells.photo_rates)
+    x = cells.state.copy()
+    s.solve(x, cells.env, 0.0, t1)
+    return s, x, s.cell_stats()["status"].copy()
+
+
+def _tol_units(mech, x, truth, rows):
+    """Per-cell max difference in units of the tolerance (1e-4 |y| + 1e-8)."""
+    dep = mech.dep_index()
+    y = truth[rows][:, dep]
+    return (np.abs(x[rows][:, dep] - y) / (1e-4 * np.abs(y) + 1e-8)).max(axis=1)
+
+
+def _tight(mech, cells, t1):
+    """The oracle's BDF at rtol 1e-8, atol 1e-12: the accuracy yardstick."""
+    from oracle.oracle import OracleModel
+
+    _, st, _, y = OracleModel(mech).solve(cells.state.copy(), cells.env, cells.photo_rates, 0.0,
+                                          t1, 1e-8, np.full(mech.n_state_var, 1e-12),
+                                          max_steps=200000, n_threads=os.cpu_count() or 1)
+    return y, st
+
+
+def _same_accuracy(mech, a, b, tight, rows):
+    """Two BDF runs at rtol 1e-4 differ by their global errors, so each is
+    measured against the tight solution and their per-cell errors are
+    compared as distributions (median and 90th percentile)."""
+    ea = _tol_units(mech, a, tight, rows)
+    eb = _tol_units(mech, b, tight, rows)
+    assert np.median(ea) <= 2.0 * np.median(eb) + 1.0, (np.median(ea), np.median(eb))
+    assert np.percentile(ea, 90) <= 2.0 * np.percentile(eb, 90) + 5.0, (
+        np.percentile(ea, 90), np.percentile(eb, 90))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("which", ["cb05", "mod37"])
+def test_lane_kernel_matches_warp_kernel(request, which, precision):
+    from camp_b200.cells import make_cells
+
+    mech = request.getfixturevalue(which)
+    cells = make_cells(mech, 40, 23)
+    _, xw, sw = _solve(mech, cells, precision, 0, 60.0, 1500)
+    _, xl, sl = _solve(mech, cells, precision, 1, 60.0, 1500)
+    assert np.mean(sw == sl) >= 0.9
+    tight, tst = _tight(mech, cells, 60.0)
+    ok = (sw == 0) & (sl == 0) & (tst == 0)
+    assert ok.sum() >= 16
+    _same_accuracy(mech, xl, xw, tight, ok)
+
+
+@pytest.fixture(scope="module")
+def large():
+    import tempfile
+
+    from camp_b200.synth import load_synthetic
+
+    with tempfile.TemporaryDirectory() as td:
+        return load_synthetic(td, 200, 600)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_large_mechanism_matches_oracle(large, precision):
+    from camp_b200.cells import make_cells
+    from oracle.oracle import OracleModel
+
+    mech, base = large
+    cells = make_cells(mech, 32, 29, conc_lo=1e-8, photo_base=base)
+    s, x, st = _solve(mech, cells, precision, None, T_LARGE, 10000)
+    nf, ost, _, y = OracleModel(mech).solve(cells.state.copy(), cells.env, cells.photo_rates,
+                                            0.0, T_LARGE, 1e-4, np.full(mech.n_state_var, 1e-8),
+                                            n_threads=os.cpu_count() or 1)
+    assert np.mean(st == ost) >= 0.9
+    tight, tst = _tight(mech, cells, T_LARGE)
+    ok = (st == 0) & (ost == 0) & (tst == 0)
+    assert ok.sum() >= 24
+    _same_accuracy(mech, x, y, tight, ok)
+
+
+def test_large_mechanism_warp_entry_points_refuse(large):
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import Solver, SolverError
+
+    mech, base = large
+    cells = make_cells(mech, 4, 31, conc_lo=1e-8, photo_base=base)
+    s = Solver(mech, 4)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4)
+    assert s.ready
+    s.set_photo_rates(cells.photo_rates)
+    with pytest.raises(SolverError, match="warp-per-cell"):
+        s.eval_deriv(cells.state, cells.env, 1.0)
