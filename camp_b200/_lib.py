@@ -42,6 +42,10 @@ EXPORTED = [
     "rxn_emission_create_rate_update_data", "rxn_emission_set_rate_update_data",
     "rxn_first_order_loss_create_rate_update_data", "rxn_first_order_loss_set_rate_update_data",
     "rxn_wet_deposition_create_rate_update_data", "rxn_wet_deposition_set_rate_update_data",
+    "aero_rep_modal_binned_mass_create_gmd_update_data",
+    "aero_rep_modal_binned_mass_set_gmd_update_data",
+    "aero_rep_modal_binned_mass_create_gsd_update_data",
+    "aero_rep_modal_binned_mass_set_gsd_update_data",
     "aero_phase_add_condensed_data", "aero_rep_add_condensed_data", "aero_rep_update_data",
     "sub_model_add_condensed_data", "sub_model_update_data", "aero_phase_print_data",
     "aero_rep_print_data", "sub_model_print_data",
@@ -85,9 +89,16 @@ def load(path: str = LIB_PATH):
     lib.solver_free_update_data.argtypes = [vp]
     lib.rxn_add_condensed_data.argtypes = [ip, ip, ip, ip, _i32p, _f64p, vp]
     lib.rxn_update_data.argtypes = [ip, C.POINTER(C.c_int), ip, vp, vp]
+    lib.aero_phase_add_condensed_data.argtypes = [ip, ip, _i32p, _f64p, vp]
+    lib.aero_rep_add_condensed_data.argtypes = [ip, ip, ip, ip, _i32p, _f64p, vp]
+    lib.aero_rep_update_data.argtypes = [ip, C.POINTER(C.c_int), ip, vp, vp]
     for kind in ("photolysis", "emission", "first_order_loss", "wet_deposition"):
         getattr(lib, f"rxn_{kind}_create_rate_update_data").restype = vp
         getattr(lib, f"rxn_{kind}_set_rate_update_data").argtypes = [vp, ip, dp]
+    for what in ("gmd", "gsd"):
+        getattr(lib, f"aero_rep_modal_binned_mass_create_{what}_update_data").restype = vp
+        getattr(lib, f"aero_rep_modal_binned_mass_set_{what}_update_data").argtypes = [
+            vp, ip, ip, dp]
     lib.camp_b200_last_error.restype = C.c_char_p
     lib.camp_b200_is_ready.restype = ip
     lib.camp_b200_is_ready.argtypes = [vp]

@@ -11,6 +11,12 @@ Per-cell inputs follow the documented workload distributions:
   deposition in s^-1) = a fixed base set x a second per-cell factor uniform
   in [0.5, 1.5], drawn after everything else so that mechanisms without such
   reactions keep their streams;
+* aerosol (mechanisms with a modal/binned representation, drawn last): per
+  mode a geometric mean diameter log-uniform in 20-500 nm (the GSD is the
+  representation's) and a number concentration log-uniform in 1e7-1e10 m^-3,
+  per bin a number concentration log-uniform in 1e3-1e6 m^-3 (bins reach
+  15 um); the mode's or bin's volume is split over its mass species with
+  uniform random weights into kg m^-3; activity coefficients are 1;
 * initial concentrations of variable species log-uniform in
   [conc_lo, conc_hi] ppm; constant species keep their "init conc" value.
 
@@ -53,10 +59,14 @@ def photo_base_rates(mech: Mechanism, base: float = 1.0e-4, zero_labels=("jo2",)
     listed reactions), the module's emission / deposition bases otherwise."""
     other = {RXN_EMISSION: EMISSION_BASE, RXN_FIRST_ORDER_LOSS: FIRST_ORDER_LOSS_BASE,
              RXN_WET_DEPOSITION: WET_DEPOSITION_BASE}
-    cols = mech.rate_rxns()
+    cols = mech.rate_columns()
     out = np.zeros(len(cols), dtype=np.float64)
-    for j, ridx in enumerate(cols):
-        r = mech.rxns[ridx]
+    for j, col in enumerate(cols):
+        if col[0] != "rxn":
+            sec = mech.aero_reps[col[1]].sections[col[2]]
+            out[j] = sec.gmd if col[0] == "gmd" else sec.gsd
+            continue
+        r = mech.rxns[col[1]]
         if r.rxn_type == RXN_PHOTOLYSIS:
             out[j] = 0.0 if r.label in zero_labels else base
         else:
@@ -65,9 +75,51 @@ def photo_base_rates(mech: Mechanism, base: float = 1.0e-4, zero_labels=("jo2",)
 
 
 def photolysis_columns(mech: Mechanism) -> np.ndarray:
-    """Mask of the host-rate columns that are photolysis reactions."""
-    return np.asarray([mech.rxns[i].rxn_type == RXN_PHOTOLYSIS for i in mech.rate_rxns()],
-                      dtype=bool)
+    """Mask of the host-set columns that are photolysis reactions."""
+    return np.asarray([c[0] == "rxn" and mech.rxns[c[1]].rxn_type == RXN_PHOTOLYSIS
+                       for c in mech.rate_columns()], dtype=bool)
+
+
+def _aerosol_cells(mech: Mechanism, rng, state: np.ndarray, photo: np.ndarray) -> None:
+    """Per-cell aerosol state and mode GMD/GSD columns (module docstring)."""
+    from .aerosol import MODAL
+
+    n_cells = state.shape[0]
+    cols = mech.rate_columns()
+    col_of = {c: j for j, c in enumerate(cols)}
+    for ri, rep in enumerate(mech.aero_reps):
+        inst = 0
+        for si, sec in enumerate(rep.sections):
+            nb = sec.n_bins
+            if sec.kind == MODAL:
+                gmd = np.exp(rng.uniform(np.log(20e-9), np.log(500e-9), n_cells))
+                gsd = np.full(n_cells, sec.gsd)
+                photo[:, col_of[("gmd", ri, si)]] = gmd
+                photo[:, col_of[("gsd", ri, si)]] = gsd
+                number = np.exp(rng.uniform(np.log(1e7), np.log(1e10), (n_cells, 1)))
+                vol = number * (np.pi / 6.0 * gmd[:, None] ** 3 *
+                                np.exp(4.5 * np.log(gsd[:, None]) ** 2))
+            else:
+                dp = rep.floats[rep.ints[4 + len(rep.sections) + si] - 1 + 3 * np.arange(nb)]
+                number = np.exp(rng.uniform(np.log(1e3), np.log(1e6), (n_cells, nb)))
+                vol = number * (4.0 / 3.0 * np.pi * (dp[None, :] / 2.0) ** 3)
+            # instances of this section, Fortran order (phase, bin)
+            for pi in sec.phases:
+                ph = mech.aero_phases[pi]
+                mass_idx = [k for k, t in enumerate(ph.types) if t in (1, 2, 3)]
+                w = rng.uniform(0.0, 1.0, (n_cells, nb, len(mech.aero_phases[pi].species)))
+                for b in range(nb):
+                    first = rep.first_state + sum(
+                        len(mech.aero_phases[q].species) for q in rep.instances[:inst])
+                    wsum = w[:, b, mass_idx].sum(axis=1) if mass_idx else np.ones(n_cells)
+                    for k, t in enumerate(ph.types):
+                        if t in (1, 2, 3):
+                            dens = ph.floats[len(ph.species) + k]
+                            state[:, first + k] = (vol[:, b] / len(sec.phases) * w[:, b, k] /
+                                                   wsum * dens)
+                        else:
+                            state[:, first + k] = 1.0
+                    inst += 1
 
 
 def make_cells(
@@ -106,6 +158,8 @@ def make_cells(
     if photo.shape[1] and not is_photo.all():
         other = rng.uniform(0.5, 1.5, n_cells)
         photo[:, ~is_photo] = other[:, None] * np.asarray(photo_base)[None, ~is_photo]
+    if mech.aero_reps:
+        _aerosol_cells(mech, rng, state, photo)
     return CellBatch(state=state, env=env, photo_rates=photo, seed=seed)
 
 
@@ -121,5 +175,5 @@ def constant_values(mech: Mechanism) -> dict[str, float]:
 
 
 def n_photo(mech: Mechanism) -> int:
-    """Host-rate columns of a mechanism."""
-    return len(mech.rate_rxns())
+    """Host-set columns of a mechanism."""
+    return len(mech.rate_columns())

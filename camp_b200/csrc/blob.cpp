@@ -52,7 +52,7 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     *err = "more than 1023 dependent variables";
     return false;
   }
-  if (t.n_rxn > 65535 || t.n_part > 65535 || t.n_lu > 65535 || t.n_jac > 65535 ||
+  if (t.n_rates > 65535 || t.n_part_all > 65535 || t.n_lu > 65535 || t.n_jac > 65535 ||
       (int)t.fg_rxn.size() > 65535 || (int)t.jg_part.size() > 65535 ||
       (int)t.fa_pos.size() > 65535) {
     *err = "mechanism exceeds the 16-bit table encodings";
@@ -154,21 +154,26 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     }
   }
   fg_lane[kLanes] = (uint16_t)(fg_unit.size() / 8);
-  // J gather: each slot's partials regrouped, losses first (they add to the
-  // loss part unguarded) and then products (guarded, into the production
-  // part); jg_mid[e] is the first product entry of slot e
+  // J gather: each slot's partials regrouped: unguarded products (SIMPOL,
+  // into the production part), losses (into the loss part) and guarded
+  // products (into the production part); jg_umid[e] / jg_mid[e] are the
+  // first loss / guarded product entry of slot e
   std::vector<uint32_t> jg_w0;
-  std::vector<uint16_t> jg_w1, jg_mid(t.n_jac);
+  std::vector<uint16_t> jg_w1, jg_mid(t.n_jac), jg_umid(t.n_jac);
   jg_w0.reserve(t.jg_part.size());
   jg_w1.reserve(t.jg_part.size());
+  bool has_ug = false;
   for (int e = 0; e < t.n_jac; ++e) {
-    for (int pass = 0; pass < 2; ++pass) {
-      if (pass == 1) jg_mid[e] = (uint16_t)jg_w0.size();
+    for (int pass = 0; pass < 3; ++pass) {
+      if (pass == 1) jg_umid[e] = (uint16_t)jg_w0.size();
+      if (pass == 2) jg_mid[e] = (uint16_t)jg_w0.size();
       for (int g = t.jg_ptr[e]; g < t.jg_ptr[e + 1]; ++g) {
-        if ((t.jg_ind[g] >= 0) != (pass == 1)) continue;
+        const int kind = t.jg_ind[g] == -2 ? 0 : (t.jg_ind[g] == -1 ? 1 : 2);
+        if (kind != pass) continue;
+        has_ug |= kind == 0;
         int c = coef_id(t.jg_coef[g]);
         jg_w0.push_back((uint32_t)t.jg_part[g] | ((uint32_t)c << 16));
-        jg_w1.push_back((uint16_t)(t.jg_ind[g] + 1));
+        jg_w1.push_back((uint16_t)(t.jg_ind[g] >= 0 ? t.jg_ind[g] + 1 : 0));
       }
     }
   }
@@ -178,6 +183,33 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   }
   std::vector<uint16_t> jg_ptr(t.n_jac + 1), jg_lupos(t.n_jac), jg_row(t.n_jac);
   for (int e = 0; e <= t.n_jac; ++e) jg_ptr[e] = (uint16_t)t.jg_ptr[e];
+  // SIMPOL instance tables (dependent elements only: the constant ones are
+  // folded into the per-cell constants)
+  std::vector<uint16_t> si_rec, si_elem;
+  std::vector<double> si_ef;
+  for (int k = 0; k < t.n_simpol; ++k) {
+    const SimpolInst& si = t.simpol[k];
+    const int first = (int)si_elem.size();
+    int nd = 0;
+    for (size_t j = 0; j < si.elem.size(); ++j) {
+      const int d = std::lower_bound(t.dep_state.begin(), t.dep_state.end(), si.elem[j]) -
+                    t.dep_state.begin();
+      if (d >= n || t.dep_state[d] != si.elem[j]) continue;  // not a dependent variable
+      si_elem.push_back((uint16_t)d);
+      si_ef.push_back(si.inv_rho[j]);
+      si_ef.push_back(si.inv_mw[j]);
+      si_ef.push_back(si.in_phase[j] ? 1.0 : 0.0);
+      ++nd;
+    }
+    const auto dep_of = [&](int st) {
+      return (int)(std::lower_bound(t.dep_state.begin(), t.dep_state.end(), st) -
+                   t.dep_state.begin());
+    };
+    const uint16_t rec[8] = {(uint16_t)dep_of(si.gas), (uint16_t)dep_of(si.aero),
+                             (uint16_t)nd,                (uint16_t)first,
+                             (uint16_t)t.si_part0[k],     0, 0, 0};
+    si_rec.insert(si_rec.end(), rec, rec + 8);
+  }
   for (int e = 0; e < t.n_jac; ++e) {
     jg_lupos[e] = (uint16_t)t.jg_lupos[e];
     jg_row[e] = (uint16_t)t.jg_row[e];
@@ -288,6 +320,15 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.jg_row = w.put(jg_row);
   o.jg_lane = w.put(jg_lane);
   o.jg_slots = w.put(jg_slots);
+  o.has_ug = has_ug ? 1 : 0;
+  o.jg_umid = w.put(jg_umid);
+  o.n_simpol = t.n_simpol;
+  o.n_keff = t.n_keff;
+  o.n_rates = t.n_rates;
+  o.n_part_all = t.n_part_all;
+  o.si_rec = w.put(si_rec);
+  o.si_elem = w.put(si_elem);
+  o.si_ef = w.put(si_ef);
   o.n_plev = t.n_plev;
   o.lu_perm = w.put(u16(t.lu_perm));
   o.lu_src = w.put(lu_src);
@@ -333,6 +374,10 @@ namespace campb {
 
 bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
                      std::vector<uint8_t>* blob, LaneOff* off, std::string* err) {
+  if (t.n_simpol > 0) {
+    *err = "the lane-per-cell kernel does not evaluate SIMPOL phase transfer";
+    return false;
+  }
   const int n = t.n;
   if (n > 1023 || t.n_rxn > 65535 || t.n_lu > 65535) {
     *err = "mechanism exceeds the lane-kernel table encodings";

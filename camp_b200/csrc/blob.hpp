@@ -47,6 +47,17 @@ struct BlobOff {
   int lu_rowptr, lu_col, upd_ptr, upd;
   // dependent index -> state index (uint16); absolute tolerances (double)
   int dep_state, atol;
+  // SIMPOL phase transfer: per instance a record of 8 x uint16 (gas and
+  // aerosol dependent indices, dependent element count, first element, first
+  // Jacobian partial), per dependent element its index (uint16) and factors
+  // (1/density, 1/MW when in the instance's phase else 0, in-phase flag;
+  // 3 x double).  Its 4 pseudo-rates per instance follow the terms' rates,
+  // its 8 per-cell constants the terms' rate constants.
+  int n_simpol, n_keff, n_rates, n_part_all;
+  int si_rec, si_elem, si_ef;
+  // J gather with unguarded products (SIMPOL): they lead each slot, and
+  // jg_umid (uint16 per slot) is the slot's first loss entry
+  int has_ug, jg_umid;
 };
 
 struct Tables;

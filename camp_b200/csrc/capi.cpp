@@ -190,16 +190,91 @@ void rxn_add_condensed_data(int rxn_type, int n_int_param, int n_float_param,
   }
 }
 
-void aero_phase_add_condensed_data(int, int, int*, double*, void* solver_data) {
-  S(solver_data)->n_aero_phase_added++;
+void aero_phase_add_condensed_data(int n_int_param, int n_float_param, int* int_param,
+                                   double* float_param, void* solver_data) {
+  Solver* s = S(solver_data);
+  s->n_aero_phase_added++;
+  std::string err;
+  if (!s->model->add_aero_phase(n_int_param, n_float_param, int_param, float_param, &err) &&
+      !s->add_error) {
+    s->add_error = true;
+    s->add_error_msg = err;
+  }
 }
-void aero_rep_add_condensed_data(int, int, int, int, int*, double*, void* solver_data) {
-  S(solver_data)->n_aero_rep_added++;
+void aero_rep_add_condensed_data(int aero_rep_type, int n_int_param, int n_float_param,
+                                 int n_env_param, int* int_param, double* float_param,
+                                 void* solver_data) {
+  Solver* s = S(solver_data);
+  s->n_aero_rep_added++;
+  std::string err;
+  if (!s->model->add_aero_rep(aero_rep_type, n_int_param, n_float_param, n_env_param, int_param,
+                              float_param, &err) &&
+      !s->add_error) {
+    s->add_error = true;
+    s->add_error_msg = err;
+  }
 }
 void sub_model_add_condensed_data(int, int, int, int, int*, double*, void* solver_data) {
   S(solver_data)->n_sub_model_added++;
 }
-void aero_rep_update_data(int, int*, int, void*, void*) {}
+// GMD / GSD updates of the modal/binned representation
+// (src/aero_rep_solver.c:492-545,
+// src/aero_reps/aero_rep_modal_binned_mass.c:602-650): the update data is
+// {int rep id, int update type (0 GMD, 1 GSD), int section, double value};
+// the value becomes the cell's column of that mode.  The search starts at
+// *aero_rep_id and leaves it on the representation that took the update.
+void aero_rep_update_data(int cell_id, int* aero_rep_id, int update_aero_rep_type,
+                          void* update_data, void* solver_data) {
+  Solver* s = S(solver_data);
+  if (cell_id < 0 || cell_id >= s->n_cells) return;
+  const int n_rep = s->model->n_aero_rep();
+  if (update_aero_rep_type != campb::AERO_REP_MODAL_BINNED_MASS) {
+    *aero_rep_id = n_rep;
+    return;
+  }
+  s->ensure_photo();
+  int head[3];
+  double value;
+  memcpy(head, update_data, sizeof(head));
+  memcpy(&value, (char*)update_data + sizeof(head), sizeof(double));
+  for (; *aero_rep_id < n_rep; (*aero_rep_id)++) {
+    const int col = s->model->aero_column(head[0], head[2], head[1]);
+    if (col < 0) continue;
+    s->photo[(size_t)cell_id * s->n_photo + col] = value;
+    return;
+  }
+}
+
+namespace {
+void* create_aero_update_data(const char* what) {
+  void* p = malloc(3 * sizeof(int) + sizeof(double));
+  if (!p) {
+    set_error(std::string("out of memory allocating ") + what + " update data");
+    exit(1);
+  }
+  return p;
+}
+void set_aero_update_data(void* update_data, int rep_id, int type, int section, double v) {
+  const int head[3] = {rep_id, type, section};
+  memcpy(update_data, head, sizeof(head));
+  memcpy((char*)update_data + sizeof(head), &v, sizeof(double));
+}
+}  // namespace
+
+void* aero_rep_modal_binned_mass_create_gmd_update_data(void) {
+  return create_aero_update_data("GMD");
+}
+void aero_rep_modal_binned_mass_set_gmd_update_data(void* update_data, int aero_rep_id,
+                                                    int section_id, double gmd) {
+  set_aero_update_data(update_data, aero_rep_id, 0, section_id, gmd);
+}
+void* aero_rep_modal_binned_mass_create_gsd_update_data(void) {
+  return create_aero_update_data("GSD");
+}
+void aero_rep_modal_binned_mass_set_gsd_update_data(void* update_data, int aero_rep_id,
+                                                    int section_id, double gsd) {
+  set_aero_update_data(update_data, aero_rep_id, 1, section_id, gsd);
+}
 void sub_model_update_data(int, int*, int, void*, void*) {}
 
 void solver_initialize(void* solver_data, double* abs_tol, double rel_tol, int max_steps,
@@ -210,10 +285,13 @@ void solver_initialize(void* solver_data, double* abs_tol, double rel_tol, int m
     set_error("solver_initialize: " + s->add_error_msg);
     return;
   }
-  if (s->n_aero_phase + s->n_aero_rep + s->n_sub_model > 0) {
-    set_error(
-        "solver_initialize: aerosol phases, aerosol representations and "
-        "sub-models are not supported by this build (gas-phase mechanisms only)");
+  if (s->n_sub_model > 0) {
+    set_error("solver_initialize: sub-models are not supported by this build");
+    return;
+  }
+  if (s->n_aero_phase_added != s->n_aero_phase || s->n_aero_rep_added != s->n_aero_rep) {
+    set_error("solver_initialize: fewer aerosol phases or representations were added than "
+              "declared in solver_new");
     return;
   }
   std::string err;
@@ -668,6 +746,16 @@ int camp_b200_rate_column(void* solver_data, int column, int* rxn_index, int* rx
       if (rxn_id) *rxn_id = s->model->photo_id(i);
       return 0;
     }
+  // the GMD / GSD columns of the modes follow the reaction columns
+  const auto& modes = s->model->modes();
+  const int first = s->model->n_host_rate() - 2 * (int)modes.size();
+  if (column >= first && column < s->model->n_host_rate()) {
+    const int k = (column - first) / 2, what = (column - first) % 2;
+    if (rxn_index) *rxn_index = -1 - modes[k].first;
+    if (rxn_type) *rxn_type = what == 0 ? CAMP_B200_COLUMN_GMD : CAMP_B200_COLUMN_GSD;
+    if (rxn_id) *rxn_id = modes[k].second;
+    return 0;
+  }
   set_error("no host-rate column " + std::to_string(column));
   return -1;
 }

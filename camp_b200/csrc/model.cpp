@@ -20,6 +20,7 @@ bool type_layout(int type, int* n_int_prop, int* n_float_prop) {
     case RXN_FIRST_ORDER_LOSS: *n_int_prop = 4; *n_float_prop = 1; return true;
     case RXN_EMISSION: *n_int_prop = 3; *n_float_prop = 1; return true;
     case RXN_WET_DEPOSITION: *n_int_prop = 2; *n_float_prop = 1; return true;
+    case RXN_SIMPOL_PHASE_TRANSFER: *n_int_prop = 2; *n_float_prop = 10; return true;
     default: return false;
   }
 }
@@ -85,7 +86,7 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
   if (!type_layout(type, &r.n_int_prop, &r.n_float_prop))
     return fail("reaction type " + std::to_string(type) +
                 " is not supported (ARRHENIUS, TROE, CMAQ_H2O2, CMAQ_OH_HNO3, PHOTOLYSIS, "
-                "FIRST_ORDER_LOSS, EMISSION and WET_DEPOSITION only)");
+                "FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION and SIMPOL_PHASE_TRANSFER only)");
   const std::string malformed = "malformed packed data for reaction " + std::to_string(idx);
   if (n_int < r.n_int_prop || n_float < r.n_float_prop) return fail(malformed);
   const int o = r.int_off;  // rxn_int_ position of ints[0]
@@ -122,6 +123,15 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
       r.rid_at = o;
       break;
     }
+    case RXN_SIMPOL_PHASE_TRANSFER: {  // src/rxns/rxn_SIMPOL_phase_transfer.c:37-78
+      // no mass-action terms: its instances are resolved against the
+      // aerosol representation at solver_initialize
+      const int na = ints[0];
+      if (na < 1 || n_int < 4 + 13 * na) return fail(malformed);
+      if (ints[1] < 1 || ints[1] > n_state_)
+        return fail("species index out of range in reaction " + std::to_string(idx));
+      break;
+    }
     default: {  // NUM_REACT_ NUM_PROD_ [RXN_ID_] REACT_ PROD_ DERIV_ID_ JAC_ID_, yields
       const int nr = ints[0], np = ints[1];
       if (nr < 1 || np < 0 || n_int < r.n_int_prop + (nr + 2) * (nr + np) ||
@@ -156,6 +166,190 @@ int Model::photo_id(int rxn) const {
   return host_rate_type(r.type) && r.rid_at >= 0 ? rxn_int_[r.rid_at] : 0;
 }
 
+bool Model::add_aero_phase(int n_int, int n_float, const int* ints, const double* floats,
+                           std::string* err) {
+  // [NUM_STATE_VAR, SPEC_TYPE(x)], floats [MW(x), DENSITY(x)]
+  // (src/aero_phase_solver.c:25-32)
+  if (n_int < 1 || ints[0] < 0 || n_int < 1 + ints[0] || n_float < 2 * ints[0]) {
+    *err = "malformed aerosol phase data";
+    return false;
+  }
+  aph_int_.emplace_back(ints, ints + n_int);
+  aph_flt_.emplace_back(floats, floats + n_float);
+  return true;
+}
+
+bool Model::add_aero_rep(int type, int n_int, int n_float, int n_env, const int* ints,
+                         const double* floats, std::string* err) {
+  if (type != AERO_REP_MODAL_BINNED_MASS) {
+    *err = "aerosol representation type " + std::to_string(type) +
+           " is not supported (modal/binned mass only)";
+    return false;
+  }
+  // NUM_SECTION_ INT_DATA_SIZE_ FLOAT_DATA_SIZE_ AERO_REP_ID_, section
+  // locations, then per section its type, bins, phases and phase ids
+  // (src/aero_reps/aero_rep_modal_binned_mass.c:28-84)
+  if (n_int < 4 || ints[0] < 1 || n_int < 4 + 2 * ints[0] || n_env != 2 * ints[0]) {
+    *err = "malformed aerosol representation data";
+    return false;
+  }
+  const int ns = ints[0];
+  for (int x = 0; x < ns; ++x) {
+    const int li = ints[4 + x] - 1, lf = ints[4 + ns + x] - 1;
+    if (li < 0 || li + 3 > n_int || lf < 0) {
+      *err = "malformed aerosol representation data";
+      return false;
+    }
+    const int nb = ints[li + 1], np = ints[li + 2];
+    if (nb < 1 || np < 1 || li + 3 + 3 * nb * np > n_int || lf + 3 * nb > n_float) {
+      *err = "malformed aerosol representation data";
+      return false;
+    }
+    if (ints[li] == SECTION_MODAL) modes_.push_back({(int)arep_int_.size(), x});
+  }
+  arep_int_.emplace_back(ints, ints + n_int);
+  arep_flt_.emplace_back(floats, floats + n_float);
+  arep_type_.push_back(type);
+  return true;
+}
+
+int Model::aero_column(int rep_id, int section, int what) const {
+  if (what != 0 && what != 1) return -1;
+  for (size_t k = 0; k < modes_.size(); ++k) {
+    const auto& I = arep_int_[modes_[k].first];
+    if (I[3] == rep_id && rep_id != 0 && modes_[k].second == section)
+      return n_host_rate_ + 2 * (int)k + what;
+  }
+  return -1;
+}
+
+namespace {
+// views of the packed SIMPOL data, 0-based within the reaction's ints
+// (src/rxns/rxn_SIMPOL_phase_transfer.c:37-78)
+struct SimpolView {
+  int* I;
+  int n;
+  int gas() const { return I[1] - 1; }
+  int aero(int x) const { return I[2 + x] - 1; }
+  int act(int x) const { return I[2 + n + x] - 1; }
+  int phase(int x) const { return I[2 + 2 * n + x] - 1; }
+  int rep(int x) const { return I[2 + 3 * n + x] - 1; }
+  int& deriv(int x) const { return I[2 + 4 * n + x]; }
+  int& gas_act_jac(int x) const { return I[3 + 5 * n + x]; }
+  int& aero_act_jac(int x) const { return I[3 + 6 * n + x]; }
+  int& jac(int x) const { return I[3 + 7 * n + x]; }
+  int iloc(int x) const { return I[4 + 10 * n + x] - 1; }
+  int nelem(int x) const { return I[iloc(x)]; }
+  int& phase_jac(int x, int set, int e) const { return I[iloc(x) + 1 + set * nelem(x) + e]; }
+};
+}  // namespace
+
+// The instances of every SIMPOL reaction against its representation: the
+// mode or bin of the instance found the way the representation's C
+// functions walk it (sections, then bins, then the phases of a bin,
+// src/aero_reps/aero_rep_modal_binned_mass.c:300-330), the element list,
+// the element counts written into the representation and the state indices
+// written into PHASE_JAC_ID_ as get_used_jac_elem does
+// (src/rxns/rxn_SIMPOL_phase_transfer.c:86-151).
+bool Model::resolve_simpol(std::string* err) {
+  simpol_.clear();
+  for (size_t ri = 0; ri < rxns_.size(); ++ri) {
+    const Rxn& r = rxns_[ri];
+    if (r.type != RXN_SIMPOL_PHASE_TRANSFER) continue;
+    SimpolView v{&rxn_int_[r.int_off], rxn_int_[r.int_off]};
+    for (int x = 0; x < v.n; ++x) {
+      SimpolInst si;
+      si.rxn = (int)ri;
+      si.x = x;
+      for (int q = 0; q < 10; ++q) si.prm[q] = rxn_float_[r.float_off + q];
+      si.gas = v.gas();
+      si.aero = v.aero(x);
+      si.act = v.act(x);
+      si.rep = v.rep(x);
+      if (si.rep < 0 || si.rep >= (int)arep_int_.size()) {
+        *err = "SIMPOL reaction " + std::to_string(ri) + " names a missing aerosol representation";
+        return false;
+      }
+      std::vector<int>& R = arep_int_[si.rep];
+      const std::vector<double>& RF = arep_flt_[si.rep];
+      const int ns = R[0];
+      int idx = v.phase(x), found = 0;
+      for (int s = 0; s < ns && !found; ++s) {
+        const int li = R[4 + s] - 1;
+        for (int b = 0; b < R[li + 1] && !found; ++b) {
+          if (idx < R[li + 2]) {
+            si.section = s;
+            si.bin = b;
+            si.phase = idx;
+            found = 1;
+          } else {
+            idx -= R[li + 2];
+          }
+        }
+      }
+      if (!found) {
+        *err = "SIMPOL reaction " + std::to_string(ri) + " names a missing phase instance";
+        return false;
+      }
+      const int li = R[4 + si.section] - 1, lf = R[4 + ns + si.section] - 1;
+      const int nb = R[li + 1], np = R[li + 2];
+      si.kind = R[li];
+      si.n_phases = np;
+      si.bin_dp = RF[lf + 3 * si.bin];
+      if (si.kind == SECTION_MODAL) {
+        int k = 0;
+        for (; k < (int)modes_.size(); ++k)
+          if (modes_[k].first == si.rep && modes_[k].second == si.section) break;
+        si.gmd_col = n_host_rate_ + 2 * k;
+        si.gsd_col = si.gmd_col + 1;
+      }
+      for (int y = 0; y < np; ++y) {
+        const int st0 = R[li + 3 + si.bin * np + y] - 1;
+        const int ph = R[li + 3 + nb * np + si.bin * np + y] - 1;
+        if (ph < 0 || ph >= (int)aph_int_.size()) {
+          *err = "aerosol representation names a missing phase";
+          return false;
+        }
+        const std::vector<int>& P = aph_int_[ph];
+        const std::vector<double>& PF = aph_flt_[ph];
+        int cnt = 0;
+        for (int i = 0; i < P[0]; ++i) {
+          const int t = P[1 + i];
+          if (t != VAR_VARIABLE && t != VAR_CONSTANT && t != 3) continue;
+          si.elem.push_back(st0 + i);
+          si.inv_rho.push_back(1.0 / PF[P[0] + i]);
+          si.inv_mw.push_back(y == si.phase ? 1.0 / PF[i] : 0.0);
+          si.in_phase.push_back(y == si.phase ? 1 : 0);
+          ++cnt;
+        }
+        R[li + 3 + 2 * nb * np + si.bin * np + y] = cnt;  // PHASE_NUM_JAC_ELEM_
+      }
+      if ((int)si.elem.size() > v.nelem(x)) {
+        *err = "SIMPOL reaction " + std::to_string(ri) + ": more Jacobian elements than packed";
+        return false;
+      }
+      for (int e = 0; e < v.nelem(x); ++e) {
+        const int val = e < (int)si.elem.size() ? si.elem[e] : -1;
+        v.phase_jac(x, 0, e) = val;
+        v.phase_jac(x, 1, e) = val;
+      }
+      for (int sp : {si.gas, si.aero})
+        if (sp < 0 || sp >= n_state_ || var_type_[sp] != VAR_VARIABLE) {
+          *err = "SIMPOL reaction " + std::to_string(ri) +
+                 ": the gas and aerosol species must be variable state variables";
+          return false;
+        }
+      if (si.act >= 0 && (si.act >= n_state_ || var_type_[si.act] == VAR_VARIABLE)) {
+        *err = "SIMPOL reaction " + std::to_string(ri) +
+               ": a variable activity coefficient is not supported";
+        return false;
+      }
+      simpol_.push_back(si);
+    }
+  }
+  return true;
+}
+
 int Model::rxn_elem_id(int dep, int ind) const {
   for (int e = rj_colptr_[ind]; e < rj_colptr_[ind + 1]; ++e)
     if (rj_rowid_[e] == dep) return e;
@@ -176,6 +370,22 @@ void Model::build_rxn_jacobian() {
         for (int d : t.react) reg.add(d, ind);
         for (int d : t.prod) reg.add(d, ind);
       }
+  // SIMPOL (src/rxns/rxn_SIMPOL_phase_transfer.c:86-151): gas and aerosol
+  // species against each other, the activity coefficient and the elements
+  for (const SimpolInst& si : simpol_) {
+    reg.add(si.gas, si.gas);
+    reg.add(si.aero, si.gas);
+    reg.add(si.gas, si.aero);
+    reg.add(si.aero, si.aero);
+    if (si.act > 0) {
+      reg.add(si.gas, si.act);
+      reg.add(si.aero, si.act);
+    }
+    for (int e : si.elem) {
+      reg.add(si.gas, e);
+      reg.add(si.aero, e);
+    }
+  }
   reg.to_csc(&rj_colptr_, &rj_rowid_);
 }
 
@@ -197,6 +407,33 @@ void Model::update_ids() {
         for (int d : t.prod) rxn_int_[t.jac_at[e++]] = rxn_elem_id(d, ind);
       }
     }
+  // SIMPOL (src/rxns/rxn_SIMPOL_phase_transfer.c:160-205)
+  for (const Rxn& r : rxns_) {
+    if (r.type != RXN_SIMPOL_PHASE_TRANSFER) continue;
+    SimpolView v{&rxn_int_[r.int_off], rxn_int_[r.int_off]};
+    const int g = v.gas();
+    v.deriv(0) = deriv_ids_[g];
+    for (int x = 0; x < v.n; ++x) v.deriv(x + 1) = deriv_ids_[v.aero(x)];
+    int ij = 0;
+    v.jac(ij++) = rxn_elem_id(g, g);
+    for (int x = 0; x < v.n; ++x) {
+      const int a = v.aero(x);
+      v.jac(ij++) = rxn_elem_id(a, g);
+      v.jac(ij++) = rxn_elem_id(g, a);
+      v.jac(ij++) = rxn_elem_id(a, a);
+      if (v.act(x) > 0) {
+        v.gas_act_jac(x) = rxn_elem_id(g, v.act(x));
+        v.aero_act_jac(x) = rxn_elem_id(a, v.act(x));
+      } else {
+        v.gas_act_jac(x) = -1;
+        v.aero_act_jac(x) = -1;
+      }
+      for (int e = 0; e < v.nelem(x); ++e) {
+        if (v.phase_jac(x, 0, e) > 0) v.phase_jac(x, 0, e) = rxn_elem_id(g, v.phase_jac(x, 0, e));
+        if (v.phase_jac(x, 1, e) > 0) v.phase_jac(x, 1, e) = rxn_elem_id(a, v.phase_jac(x, 1, e));
+      }
+    }
+  }
 }
 
 // Solver Jacobian: the variable x variable entries of the reaction Jacobian
@@ -564,15 +801,32 @@ void Model::build_tables() {
       t.rx_vptr.push_back((int)t.rx_vdep.size());
     }
   }
-  t.n_photo = n_host_rate_;
+  t.n_photo = n_host_rate();
   t.n_part = (int)t.rx_vdep.size();
+  // SIMPOL instances: 4 pseudo-rates each after the terms' rates, 8 per-cell
+  // constants after the terms' rate constants, and their Jacobian partials
+  // (4 + 4 per dependent element) after the terms' partials
+  t.simpol = simpol_;
+  t.n_simpol = (int)simpol_.size();
+  t.n_rates = t.n_rxn + 4 * t.n_simpol;
+  t.n_keff = t.n_rxn + 8 * t.n_simpol;
+  t.si_part0.clear();
+  int n_part_all = t.n_part;
+  for (const SimpolInst& si : simpol_) {
+    t.si_part0.push_back(n_part_all);
+    int nd = 0;
+    for (int e : si.elem) nd += var_type_[e] == VAR_VARIABLE;
+    n_part_all += 4 + 4 * nd;
+  }
+  t.n_part_all = n_part_all;
   // f gather: per dependent species, in term order, reactant occurrences
   // (loss, coefficient -1) before products (coefficient yield)
   std::vector<std::vector<int>> frx(n_dep_), fpr(n_dep_);
   std::vector<std::vector<double>> fco(n_dep_);
   {
-    int ti = 0;
-    for (const Rxn& r : rxns_)
+    int ti = 0, ks = 0;
+    for (size_t ri = 0; ri < rxns_.size(); ++ri) {
+      const Rxn& r = rxns_[ri];
       for (const Term& tm : r.terms) {
         int k = 0;
         for (size_t j = 0; j < tm.react.size(); ++j) {
@@ -588,6 +842,18 @@ void Model::build_tables() {
         }
         ++ti;
       }
+      // SIMPOL at its place in the mechanism: the gas gains evaporation and
+      // loses condensation, the aerosol species the reverse
+      // (src/rxns/rxn_SIMPOL_phase_transfer.c:414-446)
+      for (; ks < t.n_simpol && simpol_[ks].rxn == (int)ri; ++ks) {
+        const int base = t.n_rxn + 4 * ks;
+        const int dg = deriv_ids_[simpol_[ks].gas], da = deriv_ids_[simpol_[ks].aero];
+        frx[dg].push_back(base); fco[dg].push_back(1.0); fpr[dg].push_back(FG_SOURCE);
+        frx[dg].push_back(base + 1); fco[dg].push_back(-1.0); fpr[dg].push_back(FG_LOSS);
+        frx[da].push_back(base + 2); fco[da].push_back(-1.0); fpr[da].push_back(FG_LOSS);
+        frx[da].push_back(base + 3); fco[da].push_back(1.0); fpr[da].push_back(FG_SOURCE);
+      }
+    }
   }
   t.fg_ptr.assign(n_dep_ + 1, 0);
   t.fg_rxn.clear(); t.fg_coef.clear(); t.fg_prod.clear();
@@ -634,6 +900,34 @@ void Model::build_tables() {
         ++ti;
       }
   }
+  // SIMPOL partials: losses (jg_ind -1) and unguarded productions (-2) of
+  // the gas and aerosol rows against each other and every dependent element
+  // (src/rxns/rxn_SIMPOL_phase_transfer.c:615-744, total-mass branch)
+  for (int k = 0; k < t.n_simpol; ++k) {
+    const SimpolInst& si = simpol_[k];
+    const int p0 = t.si_part0[k];
+    const int dg = deriv_ids_[si.gas], da = deriv_ids_[si.aero];
+    auto add = [&](int row, int col, int part, bool loss) {
+      int e = slot_of(row, col);
+      jpart[e].push_back(part);
+      jco[e].push_back(loss ? -1.0 : 1.0);
+      jind[e].push_back(loss ? -1 : -2);
+    };
+    add(dg, dg, p0 + 0, true);
+    add(da, dg, p0 + 1, false);
+    add(dg, da, p0 + 2, false);
+    add(da, da, p0 + 3, true);
+    int j = 0;
+    for (int es : si.elem) {
+      if (var_type_[es] != VAR_VARIABLE) continue;
+      const int de = deriv_ids_[es];
+      add(dg, de, p0 + 4 + 4 * j, false);
+      add(dg, de, p0 + 5 + 4 * j, true);
+      add(da, de, p0 + 6 + 4 * j, true);
+      add(da, de, p0 + 7 + 4 * j, false);
+      ++j;
+    }
+  }
   t.jg_ptr.assign(t.n_jac + 1, 0);
   t.jg_part.clear(); t.jg_coef.clear(); t.jg_ind.clear();
   t.jg_lupos.assign(t.n_jac, 0);
@@ -664,6 +958,7 @@ bool Model::build(std::string* err) {
     *err = "no dependent (VARIABLE) state variables";
     return false;
   }
+  if (!resolve_simpol(err)) return false;
   build_rxn_jacobian();
   update_ids();
   build_solver_jacobian();

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace campb {
@@ -19,7 +20,13 @@ enum : int {
   RXN_FIRST_ORDER_LOSS = 12,
   RXN_EMISSION = 13,
   RXN_WET_DEPOSITION = 14,
+  RXN_SIMPOL_PHASE_TRANSFER = 10,
 };
+
+// aerosol representation types, src/aero_rep_solver.c:19-20; section types
+// of the modal/binned mass representation
+enum : int { AERO_REP_MODAL_BINNED_MASS = 2 };
+enum : int { SECTION_BINNED = 1, SECTION_MODAL = 2 };
 
 // Types whose rate the host sets per cell through rxn_update_data
 // (src/rxn_solver.c:735-760): k = SCALING_ * BASE_RATE_.
@@ -27,6 +34,28 @@ inline bool host_rate_type(int type) {
   return type == RXN_PHOTOLYSIS || type == RXN_FIRST_ORDER_LOSS || type == RXN_EMISSION ||
          type == RXN_WET_DEPOSITION;
 }
+
+// One SIMPOL phase instance (a reaction's partitioning into one phase of
+// one mode or bin).  Elements are the mass species (variable, constant,
+// PSSA) of every phase of the mode or bin in state order: the number
+// concentration depends on all of them, the phase mass and mean molecular
+// weight on those of the instance's phase
+// (src/aero_reps/aero_rep_modal_binned_mass.c:86-125).
+struct SimpolInst {
+  int rxn = 0, x = 0;              // reaction, instance within it
+  int gas = 0, aero = 0, act = -1;  // state indices (act: -1 when none)
+  int rep = 0, section = 0, bin = 0, phase = 0;
+  int kind = SECTION_MODAL;
+  int gmd_col = -1, gsd_col = -1;   // host-set columns of a mode's GMD / GSD
+  double bin_dp = 0.0;              // bin diameter [m] (bins)
+  int n_phases = 0;                 // phases of the mode or bin (volume floors)
+  // the reaction's float parameters: DELTA_H DELTA_S DIFF_COEFF PRE_C_AVG
+  // B1..B4 CONV MW (src/rxns/rxn_SIMPOL_phase_transfer.c:31-40)
+  double prm[10] = {0.0};
+  std::vector<int> elem;            // state indices
+  std::vector<double> inv_rho, inv_mw;  // 1/density; 1/MW in the phase, else 0
+  std::vector<char> in_phase;
+};
 
 // kinds of f gather entries (Tables::fg_prod)
 enum : int { FG_LOSS = 0, FG_PRODUCT = 1, FG_SOURCE = 2 };
@@ -80,10 +109,21 @@ struct Tables {
   // constant reactants (state index), variable reactants (dependent index)
   std::vector<int> rx_cptr, rx_cidx, rx_vptr, rx_vdep;
   // f gather by dependent species: term, coefficient, kind (FG_LOSS,
-  // FG_PRODUCT: guarded, FG_SOURCE: unguarded gain of a zero-order term)
+  // FG_PRODUCT: guarded, FG_SOURCE: unguarded gain of a zero-order term).
+  // Terms n_rxn + 4 k + (0..3) are the SIMPOL pseudo-rates of instance k:
+  // gas gain (evaporation), gas loss (condensation), aerosol loss, gain.
   std::vector<int> fg_ptr, fg_rxn, fg_prod;
+  // SIMPOL: instances, their per-cell constants (keff slots n_rxn + 8 k ..),
+  // and their Jacobian partials (part slots from si_part0[k])
+  int n_simpol = 0;
+  std::vector<SimpolInst> simpol;
+  std::vector<int> si_part0;
+  int n_part_all = 0;  // n_part + SIMPOL partials
+  int n_keff = 0;      // n_rxn + 8 n_simpol
+  int n_rates = 0;     // n_rxn + 4 n_simpol
   std::vector<double> fg_coef;
-  // J gather by solver Jacobian entry (CSC order)
+  // J gather by solver Jacobian entry (CSC order); jg_ind: -1 loss, -2
+  // unguarded product (SIMPOL), else the guard's independent species
   std::vector<int> jg_ptr, jg_part, jg_ind, jg_lupos, jg_row;
   std::vector<double> jg_coef;
   // LU structure in pivot order
@@ -118,6 +158,21 @@ class Model {
   // rxn_add_condensed_data (src/rxn_solver.c:658-700)
   bool add_rxn(int type, int n_int, int n_float, int n_env, const int* ints,
                const double* floats, std::string* err);
+  // aero_phase_add_condensed_data (src/aero_phase_solver.c:175-202) and
+  // aero_rep_add_condensed_data (src/aero_rep_solver.c:443-484); the
+  // modal/binned mass representation only
+  bool add_aero_phase(int n_int, int n_float, const int* ints, const double* floats,
+                      std::string* err);
+  bool add_aero_rep(int type, int n_int, int n_float, int n_env, const int* ints,
+                    const double* floats, std::string* err);
+  int n_aero_phase() const { return (int)aph_int_.size(); }
+  int n_aero_rep() const { return (int)arep_int_.size(); }
+  // modes of every representation, (representation, section) in order: the
+  // GMD / GSD host-set columns after the reaction columns
+  const std::vector<std::pair<int, int>>& modes() const { return modes_; }
+  // aero_rep_update_data for the modal/binned representation: the id and
+  // the section of a GMD (what 0) / GSD (what 1) update -> its column, or -1
+  int aero_column(int rep_id, int section, int what) const;
 
   // get_jac_init (src/camp_solver.c:1417-1712) for a gas-phase model:
   // reaction Jacobian, DERIV_ID/JAC_ID, solver Jacobian; then the LU
@@ -144,7 +199,8 @@ class Model {
   const std::vector<int>& photo_slot() const { return photo_slot_; }
   int photo_id(int rxn) const;
   int n_terms() const { return n_terms_; }
-  int n_host_rate() const { return n_host_rate_; }
+  // host-set columns: reaction rates, then the GMD and GSD of every mode
+  int n_host_rate() const { return n_host_rate_ + 2 * (int)modes_.size(); }
 
  private:
   void build_rxn_jacobian();
@@ -155,6 +211,7 @@ class Model {
                              const std::vector<int>& flev, int nfl,
                              const std::vector<int>& blev, int nbl);
   void build_tables();
+  bool resolve_simpol(std::string* err);
   int rxn_elem_id(int dep, int ind) const;
 
   int n_state_, n_cells_, n_dep_, n_rxn_;
@@ -164,6 +221,11 @@ class Model {
   std::vector<double> rxn_float_;
   std::vector<Rxn> rxns_;
   std::vector<int> photo_slot_;
+  std::vector<std::vector<int>> aph_int_, arep_int_;
+  std::vector<std::vector<double>> aph_flt_, arep_flt_;
+  std::vector<int> arep_type_;
+  std::vector<std::pair<int, int>> modes_;
+  std::vector<SimpolInst> simpol_;
   std::vector<int> deriv_ids_;
   std::vector<int> rj_colptr_, rj_rowid_;
   std::vector<int> sj_colptr_, sj_rowid_;

@@ -26,6 +26,14 @@ struct DevMech {
   const int *fl_ptr, *fl_rows, *bl_ptr, *bl_rows;
   const int *dep_state, *const_state;
   const double* atol;  // per dependent variable
+  // SIMPOL instances: the reaction's 10 float parameters, section kind,
+  // GMD / GSD columns (modes) or bin diameter, activity coefficient state
+  // index (-1: none), phases of the mode or bin, and its constant (not
+  // dependent) mass species: state index, 1/density, 1/MW and in-phase flag
+  int n_simpol;
+  const double* si_prm;
+  const int *si_kind, *si_gmd_col, *si_gsd_col, *si_act, *si_nph, *si_cptr, *si_cidx;
+  const double *si_dp, *si_cinv_rho, *si_cinv_mw, *si_cin;
 };
 
 template <typename T>
@@ -83,8 +91,67 @@ static __device__ double rate_constant(const DevMech& m, int r, double T, double
   return 0.0;
 }
 
+// Per-cell constants of SIMPOL instance k into c[0..7]: the transition-
+// regime condensation rate constant k_c = 4 pi r D f(Kn, alpha) (src/util.h:
+// 50-135), K_eq, 1 / (kg m-3 -> ppm), the number factor of the mode or bin,
+// the activity coefficient, and the volume floors (one minimum mass per
+// phase of the mode or bin) plus the constant species' volume, mass and
+// moles (src/rxns/rxn_SIMPOL_phase_transfer.c:220-262,
+// src/aero_reps/aero_rep_modal_binned_mass.c:176-236,
+// src/aero_phase_solver.c:14-19,88-147).  A mode's radius and number factor
+// follow from the cell's GMD / GSD columns.
+static __device__ void simpol_constants(const DevMech& m, int k,
+                                                     const double* cell_state, double T,
+                                                     double P, const double* photo_cell,
+                                                     double* c) {
+  constexpr double R = 8.314472, PI = 3.14159265358979323846;
+  const double* f = m.si_prm + 10 * k;
+  double alpha = 0.1;
+  if (f[0] != 0.0 || f[1] != 0.0) {
+    const double del_g = f[0] - T * f[1];
+    alpha = exp(-del_g / (R * T));
+    alpha = alpha / (1.0 + alpha);
+  }
+  const double mfp = 3.0 * f[2] / sqrt(8.0 * R * T / (PI * f[9]));
+  double vp = f[4] / T + f[5] + f[6] * T + f[7] * log(T);
+  vp = 101325.0 * pow(10.0, vp);
+  double radius, nfac;
+  if (ldg(m.si_kind + k) == SECTION_MODAL) {
+    const double gmd = photo_cell ? photo_cell[ldg(m.si_gmd_col + k)] : 0.0;
+    const double gsd = photo_cell ? photo_cell[ldg(m.si_gsd_col + k)] : 0.0;
+    const double lg = log(gsd);
+    radius = gmd / 2.0 * exp(5.0 * lg * lg / 2.0);
+    nfac = 6.0 / (PI * pow(gmd, 3.0) * exp(9.0 / 2.0 * pow(lg, 2.0)));
+  } else {
+    const double dp = ldg(m.si_dp + k);
+    radius = dp / 2.0;
+    nfac = 3.0 / (4.0 * PI) / pow(dp / 2.0, 3.0);
+  }
+  const double kn = mfp / radius;
+  const double fs = (0.75 * alpha * (1.0 + kn)) /
+                    (kn * kn + (1.0 + 0.283 * alpha) * kn + 0.75 * alpha);
+  c[0] = 4.0 * PI * radius * f[2] * fs;
+  c[1] = vp / P / f[9] * 1.0e6;
+  c[2] = 1.0 / (f[8] * T / P);
+  c[3] = nfac;
+  const int act = ldg(m.si_act + k);
+  c[4] = act >= 0 ? cell_state[act] : 1.0;
+  double vol = ldg(m.si_nph + k) * (1.0e-25 / 1800.0), mass = 1.0e-25, mol = 1.0e-25 / 0.1;
+  for (int j = ldg(m.si_cptr + k); j < ldg(m.si_cptr + k + 1); ++j) {
+    double v = cell_state[ldg(m.si_cidx + j)];
+    v = v > bdf::kTiny ? v : bdf::kTiny;
+    vol += v * ldg(m.si_cinv_rho + j);
+    mass += v * ldg(m.si_cin + j);
+    mol += v * ldg(m.si_cinv_mw + j);
+  }
+  c[5] = vol;
+  c[6] = mass;
+  c[7] = mol;
+}
+
 // k of every reaction times the (clamped) constant-species concentrations it
-// multiplies; constant species are clamped to TINY as solver_run does.
+// multiplies; constant species are clamped to TINY as solver_run does.  The
+// SIMPOL constants follow the terms' (keff[n_rxn + 8 k ..]).
 static __device__ void compute_keff(const DevMech& m, const double* cell_state,
                              double T, double P, const double* photo_cell,
                              double* keff, int lane) {
@@ -96,6 +163,8 @@ static __device__ void compute_keff(const DevMech& m, const double* cell_state,
     }
     keff[r] = k;
   }
+  for (int k = lane; k < m.n_simpol; k += 32)
+    simpol_constants(m, k, cell_state, T, P, photo_cell, keff + m.n_rxn + 8 * k);
   __syncwarp();
 }
 

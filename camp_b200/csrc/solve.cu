@@ -141,7 +141,9 @@ struct Tab {
   const double* atol;
   const uint16_t *lu_rowptr, *lu_col;
   const uint32_t *upd_ptr, *upd;
-  int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev;
+  const uint16_t *si_rec, *si_elem, *jg_umid;
+  const double* si_ef;
+  int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev, n_simpol, has_ug;
 };
 
 __device__ __forceinline__ Tab make_tab(const char* b) {
@@ -167,6 +169,12 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.lu_src = (const uint16_t*)(b + o.lu_src);
   t.fa_ptr = (const uint16_t*)(b + o.fa_ptr);
   t.fa = (const uint32_t*)(b + o.fa);
+  t.si_rec = (const uint16_t*)(b + o.si_rec);
+  t.si_elem = (const uint16_t*)(b + o.si_elem);
+  t.si_ef = (const double*)(b + o.si_ef);
+  t.jg_umid = (const uint16_t*)(b + o.jg_umid);
+  t.n_simpol = o.n_simpol;
+  t.has_ug = o.has_ug;
   t.fb_lane = (const uint16_t*)(b + o.fb_lane);
   t.fb_unit = (const uint32_t*)(b + o.fb_unit);
   t.fb_pair = (const uint32_t*)(b + o.fb_pair);
@@ -255,6 +263,100 @@ __device__ __forceinline__ bool rates_of(const Tab& t, const double* y, const do
   return warp_any(neg);
 }
 
+// SIMPOL phase transfer, one lane per instance
+// (src/rxns/rxn_SIMPOL_phase_transfer.c:337-450 and 463-744, the total-mass
+// branch of the modal/binned representation): the mode's or bin's number
+// concentration from its volume, the phase's mass and mean molecular weight,
+// and the condensation and evaporation rates.  Per-cell constants c (keff
+// slots n_rxn + 8 k): condensation rate constant, K_eq, 1/(kg m-3 -> ppm),
+// number factor, activity coefficient, and the volume, mass and moles of the
+// floors and constant species.  The representation's radius partials are
+// zero (its radii do not depend on the state) and are left out.
+struct SimpolState {
+  double N, cond, evap, evap_rate, m, mol, inv_k;
+};
+__device__ __forceinline__ SimpolState simpol_state(const Tab& t, int k, const double* y,
+                                                    const double* keff) {
+  const uint16_t* rec = t.si_rec + 8 * k;
+  const double* c = keff + t.n_rxn + 8 * k;
+  double V = c[5], m = c[6], mol = c[7];
+  const int e0 = rec[3], e1 = e0 + rec[2];
+  #pragma unroll 1
+  for (int e = e0; e < e1; ++e) {
+    const double ye = state_of(y[t.si_elem[e]]);
+    const double* f = t.si_ef + 3 * e;
+    V += ye * f[0];
+    mol += ye * f[1];
+    m += ye * f[2];
+  }
+  SimpolState s;
+  s.N = V * c[3];
+  s.m = m;
+  s.mol = mol;
+  s.inv_k = c[2];
+  // k_c K_eq MW / m = k_c K_eq / moles
+  s.evap_rate = ddiv(c[0] * c[1], mol) * c[4];
+  s.cond = c[0] * state_of(y[rec[0]]);
+  s.evap = s.evap_rate * state_of(y[rec[1]]);
+  return s;
+}
+
+// the four pseudo-rates per instance; returns (warp-uniform) whether any is
+// negative
+__device__ __noinline__ bool simpol_rates(const char* tb, const double* y, const double* keff,
+                                          double* rates, int lane) {
+  const Tab t = make_tab(tb);
+  bool neg = false;
+  #pragma unroll 1
+  for (int k = lane; k < t.n_simpol; k += 32) {
+    const SimpolState s = simpol_state(t, k, y, keff);
+    double* r = rates + t.n_rxn + 4 * k;
+    r[0] = s.N * s.evap;            // gas gain
+    r[1] = s.N * s.cond;            // gas loss
+    r[2] = s.N * s.evap * s.inv_k;  // aerosol loss
+    r[3] = s.N * s.cond * s.inv_k;  // aerosol gain
+    neg |= r[0] < 0.0 || r[1] < 0.0 || r[2] < 0.0 || r[3] < 0.0;
+  }
+  return warp_any(neg);
+}
+
+// Jacobian partials per instance: gas-gas loss, aerosol-gas and gas-aerosol
+// productions, aerosol-aerosol loss, then per dependent element the gas
+// row's production and loss and the aerosol row's loss and production
+__device__ __noinline__ void simpol_partials(const char* tb, const double* y, const double* keff,
+                                             double* part, int lane) {
+  const Tab t = make_tab(tb);
+  #pragma unroll 1
+  for (int k = lane; k < t.n_simpol; k += 32) {
+    const uint16_t* rec = t.si_rec + 8 * k;
+    const double* c = keff + t.n_rxn + 8 * k;
+    const SimpolState s = simpol_state(t, k, y, keff);
+    double* p = part + rec[4];
+    p[0] = s.N * c[0];
+    p[1] = s.N * c[0] * s.inv_k;
+    p[2] = s.N * s.evap_rate;
+    p[3] = s.N * s.evap_rate * s.inv_k;
+    // d evap / d mass = -evap / m, d evap / d MW = evap / MW = evap mol / m
+    const double dedm = -ddiv(s.evap, s.m);
+    const double dedw = dedm * -s.mol;
+    const double inv_mol2 = ddiv(1.0, s.mol * s.mol);
+    const int e0 = rec[3], nd = rec[2];
+    #pragma unroll 1
+    for (int j = 0; j < nd; ++j) {
+      const double* f = t.si_ef + 3 * (e0 + j);
+      const double num = c[3] * f[0];
+      const double dm = f[2];
+      const double dw = f[2] != 0.0 ? (s.mol - f[1] * s.m) * inv_mol2 : 0.0;
+      const double gp = s.evap * num + s.N * dedm * dm + s.N * dedw * dw;
+      const double gl = s.cond * num;
+      p[4 + 4 * j] = gp;
+      p[5 + 4 * j] = gl;
+      p[6 + 4 * j] = s.evap * s.inv_k * num + (s.N * dedm * dm + s.N * dedw * dw) * s.inv_k;
+      p[7 + 4 * j] = gl * s.inv_k;
+    }
+  }
+}
+
 // Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
 // When rp/rl are given, the production and loss sums are written too.
 // Species lists are processed in lane-balanced units; lists split over
@@ -268,7 +370,8 @@ __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
   #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
   if (warp_any(bad)) return 1;
-  const bool negrate = rates_of(t, y, keff, rates, lane);
+  bool negrate = rates_of(t, y, keff, rates, lane);
+  if (t.n_simpol) negrate |= simpol_rates(tb, y, keff, rates, lane);
   __syncwarp();
   const uint4* fg_unit = (const uint4*)t.fg_unit;
   const int u1 = t.fg_lane[lane + 1];
@@ -405,6 +508,7 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
       part[base + 2] = k * y0 * y1;
     }
   }
+  if (t.n_simpol) simpol_partials(tb, y, keff, part, lane);
   __syncwarp();
   const int s1 = t.jg_lane[lane + 1];
   #pragma unroll 1
@@ -416,6 +520,12 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
     double P0 = 0.0, L0 = 0.0, P1 = 0.0, L1 = 0.0;
     const int gm = t.jg_mid[e], g1 = t.jg_ptr[e + 1];
     int g = t.jg_ptr[e];
+    if (t.has_ug) {
+      // unguarded productions (SIMPOL) lead the slot
+      const int gu = t.jg_umid[e];
+      #pragma unroll 1
+      for (; g < gu; ++g) P0 += part[t.jg_w0[g] & 0xFFFFu];
+    }
     #pragma unroll 1
     for (; g + 1 < gm; g += 2) {
       L0 += part[t.jg_w0[g] & 0xFFFFu];
@@ -1495,8 +1605,8 @@ struct Engine::Impl {
   // the warp-per-cell tables use 16-bit encodings; a mechanism beyond them
   // (e.g. an LU with hundreds of thousands of Schur updates) runs on the
   // lane-per-cell kernel only, and warp_why says why
-  bool warp_ok = true;
-  std::string warp_why;
+  bool warp_ok = true, lanes_ok = true;
+  std::string warp_why, lanes_why;
   LaneOff loff{};
   void* d_lblob = nullptr;
   void *d_scr64 = nullptr, *d_scrlt = nullptr;
@@ -1597,7 +1707,40 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   for (int i = 0; i < t.n_state; ++i)
     if (model.var_type()[i] == VAR_CONSTANT) cst.push_back(i);
   m.n_const = (int)cst.size();
+  // SIMPOL instances (device-side constants; see rates.cuh)
+  std::vector<double> si_prm, si_dp, si_cinv_rho, si_cinv_mw, si_cin;
+  std::vector<int> si_kind, si_gmd, si_gsd, si_act, si_nph, si_cptr(1, 0), si_cidx;
+  for (const SimpolInst& si : t.simpol) {
+    si_prm.insert(si_prm.end(), si.prm, si.prm + 10);
+    si_kind.push_back(si.kind);
+    si_gmd.push_back(si.gmd_col);
+    si_gsd.push_back(si.gsd_col);
+    si_dp.push_back(si.bin_dp);
+    si_act.push_back(si.act);
+    si_nph.push_back(si.n_phases);
+    for (size_t j = 0; j < si.elem.size(); ++j) {
+      if (model.var_type()[si.elem[j]] == VAR_VARIABLE) continue;
+      si_cidx.push_back(si.elem[j]);
+      si_cinv_rho.push_back(si.inv_rho[j]);
+      si_cinv_mw.push_back(si.inv_mw[j]);
+      si_cin.push_back(si.in_phase[j] ? 1.0 : 0.0);
+    }
+    si_cptr.push_back((int)si_cidx.size());
+  }
+  m.n_simpol = t.n_simpol;
   Packer pk;
+  pk.add(si_prm, &m.si_prm);
+  pk.add(si_kind, &m.si_kind);
+  pk.add(si_gmd, &m.si_gmd_col);
+  pk.add(si_gsd, &m.si_gsd_col);
+  pk.add(si_act, &m.si_act);
+  pk.add(si_nph, &m.si_nph);
+  pk.add(si_cptr, &m.si_cptr);
+  pk.add(si_cidx, &m.si_cidx);
+  pk.add(si_dp, &m.si_dp);
+  pk.add(si_cinv_rho, &m.si_cinv_rho);
+  pk.add(si_cinv_mw, &m.si_cinv_mw);
+  pk.add(si_cin, &m.si_cin);
   pk.add(t.rx_type, &m.rx_type);
   pk.add(t.rx_nreact, &m.rx_nreact);
   pk.add(t.rx_fpar, &m.rx_fpar);
@@ -1647,11 +1790,18 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
     CK(cudaMemcpy(I->d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
   }
   std::vector<uint8_t> lblob;
-  if (!build_lane_blob(t, atol_dep, &lblob, &I->loff, err)) return false;
   if (I->d_lblob) cudaFree(I->d_lblob);
   I->d_lblob = nullptr;
-  CK(cudaMalloc(&I->d_lblob, lblob.size()));
-  CK(cudaMemcpy(I->d_lblob, lblob.data(), lblob.size(), cudaMemcpyHostToDevice));
+  I->lanes_why.clear();
+  I->lanes_ok = build_lane_blob(t, atol_dep, &lblob, &I->loff, &I->lanes_why);
+  if (!I->warp_ok && !I->lanes_ok) {
+    *err = "mechanism fits neither kernel: " + I->warp_why + "; " + I->lanes_why;
+    return false;
+  }
+  if (I->lanes_ok) {
+    CK(cudaMalloc(&I->d_lblob, lblob.size()));
+    CK(cudaMemcpy(I->d_lblob, lblob.data(), lblob.size(), cudaMemcpyHostToDevice));
+  }
   I->capacity = capacity;
   I->n_state = t.n_state;
   I->n_photo = t.n_photo;
@@ -1682,8 +1832,8 @@ static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist,
   L.y = take(vec);
   L.ftemp = take(vec);
   L.tempv = take(vec);
-  L.rates = take(sizeof(double) * std::max(o.n_rxn, o.n_part));
-  L.keff = keff_in_smem ? take(sizeof(double) * o.n_rxn) : -1;
+  L.rates = take(sizeof(double) * std::max(o.n_rates, o.n_part_all));
+  L.keff = keff_in_smem ? take(sizeof(double) * o.n_keff) : -1;
   L.fscr = take(sizeof(double) * 2 * std::max(1, o.n_fscratch));
   // one spare slot each: the target of the grouped phases' no-op records
   L.lu = take((size_t)lt_size * (o.n_lu + 1));
@@ -1790,6 +1940,10 @@ bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_
   if (n_cells <= 0) return true;
   cudaStream_t st = (cudaStream_t)stream;
   if (s.kernel == 1 || !I->warp_ok) {
+    if (!I->lanes_ok) {
+      *err = "the lane-per-cell kernel cannot run this mechanism: " + I->lanes_why;
+      return false;
+    }
     if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
     CK(cudaEventRecord(I->ev0, st));
     if (!lanes_launch(I->m, I->d_lblob, I->loff, d_state, d_env, d_photo, d_order, n_cells,

@@ -102,6 +102,10 @@ class Mechanism:
     # RXN_ID_ of each reaction of a host-rate type -> its index in ``rxns``
     rate_ids: dict[int, int] = field(default_factory=dict)
     species_props: dict[str, dict] = field(default_factory=dict)
+    # aerosol phases and representations as aero_phase_add_condensed_data /
+    # aero_rep_add_condensed_data receive them (camp_b200.aerosol)
+    aero_phases: list = field(default_factory=list)
+    aero_reps: list = field(default_factory=list)
 
     @property
     def n_state_var(self) -> int:
@@ -126,6 +130,14 @@ class Mechanism:
     @property
     def n_rxn_env_param(self) -> int:
         return int(sum(r.n_env for r in self.rxns))
+
+    def aero_sizes(self) -> list[int]:
+        """solver_new's aerosol counts: phases (count, ints, floats) and
+        representations (count, ints, floats, env parameters)."""
+        ph, rp = self.aero_phases, self.aero_reps
+        return [len(ph), int(sum(p.ints.size for p in ph)), int(sum(p.floats.size for p in ph)),
+                len(rp), int(sum(r.ints.size for r in rp)), int(sum(r.floats.size for r in rp)),
+                int(sum(r.n_env for r in rp))]
 
     def index(self, name: str) -> int:
         return self.species.index(name)
@@ -156,10 +168,14 @@ class Mechanism:
             "init_conc": {
                 n: float(p["init conc"]) for n, p in self.species_props.items() if "init conc" in p
             },
+            "aero_phases": [p.to_dict() for p in self.aero_phases],
+            "aero_reps": [r.to_dict() for r in self.aero_reps],
         }
 
     @classmethod
     def from_dict(cls, d: dict) -> "Mechanism":
+        from .aerosol import AeroPhase, AeroRep
+
         rxns = [
             PackedRxn(
                 int(r["type"]),
@@ -180,6 +196,8 @@ class Mechanism:
             rate_ids={int(k): int(v)
                       for k, v in d.get("rate_ids", d.get("photo_ids", {})).items()},
             species_props={n: {"init conc": v} for n, v in d.get("init_conc", {}).items()},
+            aero_phases=[AeroPhase.from_dict(p) for p in d.get("aero_phases", [])],
+            aero_reps=[AeroRep.from_dict(r) for r in d.get("aero_reps", [])],
         )
 
     def save(self, path: str) -> None:
@@ -198,6 +216,18 @@ class Mechanism:
         """Reactions of a host-rate type in mechanism order: column j of the
         per-cell base rates belongs to reaction rate_rxns()[j]."""
         return [i for i, r in enumerate(self.rxns) if r.rxn_type in HOST_RATE_TYPES]
+
+    def rate_columns(self) -> list[tuple]:
+        """Columns of the per-cell host-set values, in order: ("rxn", i) for
+        every host-rate reaction (``rate_rxns``), then ("gmd", rep, section)
+        and ("gsd", rep, section) for every mode of every aerosol
+        representation (the targets of its GMD / GSD update data)."""
+        cols: list[tuple] = [("rxn", i) for i in self.rate_rxns()]
+        for ri, rep in enumerate(self.aero_reps):
+            for si, sec in enumerate(rep.sections):
+                if sec.kind == 2:  # MODAL
+                    cols += [("gmd", ri, si), ("gsd", ri, si)]
+        return cols
 
     def rate_id(self, rxn: int) -> int:
         """RXN_ID_ of a host-rate reaction (the id its update data carries)."""

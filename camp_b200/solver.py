@@ -43,16 +43,27 @@ class Solver:
         self._h = self.lib.solver_new(
             mech.n_state_var, self.n_cells, np.ascontiguousarray(mech.var_type, np.int32),
             mech.n_rxn, mech.n_rxn_int_param, mech.n_rxn_float_param, mech.n_rxn_env_param,
-            0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+            *mech.aero_sizes(), 0, 0, 0, 0,
         )
         if not self._h:
             raise SolverError(_lib.last_error())
+        # reactions, then aerosol phases and representations, the order of
+        # camp_solver_data%initialize (src/camp_solver_data.F90:635-700)
         for r in mech.rxns:
             self.lib.rxn_add_condensed_data(
                 r.rxn_type, r.ints.size, r.floats.size, r.n_env,
                 np.ascontiguousarray(r.ints, np.int32), np.ascontiguousarray(r.floats, np.float64),
                 self._h,
             )
+        for p in mech.aero_phases:
+            self.lib.aero_phase_add_condensed_data(
+                p.ints.size, p.floats.size, np.ascontiguousarray(p.ints, np.int32),
+                np.ascontiguousarray(p.floats, np.float64), self._h)
+        for a in mech.aero_reps:
+            self.lib.aero_rep_add_condensed_data(
+                a.rep_type, a.ints.size, a.floats.size, a.n_env,
+                np.ascontiguousarray(a.ints, np.int32), np.ascontiguousarray(a.floats, np.float64),
+                self._h)
         self.ready = False
 
     # ------------------------------------------------------------------
@@ -189,6 +200,17 @@ class Solver:
         getattr(self.lib, f"rxn_{kind}_set_rate_update_data")(ud, int(rxn_id), float(base_rate))
         cursor = C.c_int(0)
         self.lib.rxn_update_data(int(cell), C.byref(cursor), int(rxn_type), ud, self._h)
+        self.lib.solver_free_update_data(ud)
+
+    def set_aero(self, cell: int, rep_id: int, section: int, what: str, value: float) -> None:
+        """GMD [m] (what "gmd") or GSD ("gsd") of a mode of the modal/binned
+        representation with that id, through its update data and
+        aero_rep_update_data."""
+        ud = getattr(self.lib, f"aero_rep_modal_binned_mass_create_{what}_update_data")()
+        getattr(self.lib, f"aero_rep_modal_binned_mass_set_{what}_update_data")(
+            ud, int(rep_id), int(section), float(value))
+        cursor = C.c_int(0)
+        self.lib.aero_rep_update_data(int(cell), C.byref(cursor), 2, ud, self._h)
         self.lib.solver_free_update_data(ud)
 
     def rate_column(self, column: int) -> tuple[int, int, int]:

@@ -87,6 +87,15 @@ void rxn_free_update_data(void *update_data);
 void *rxn_photolysis_create_rate_update_data(void);
 void rxn_photolysis_set_rate_update_data(void *update_data, int photo_id,
                                          double base_rate);
+/* replace src/aero_reps/aero_rep_modal_binned_mass.c:677-739 (bound from
+ * src/aero_reps/aero_rep_modal_binned_mass.F90:258-263): GMD [m] and GSD
+ * update data of one mode (section) of the representation with that id */
+void *aero_rep_modal_binned_mass_create_gmd_update_data(void);
+void aero_rep_modal_binned_mass_set_gmd_update_data(void *update_data, int aero_rep_id,
+                                                    int section_id, double gmd);
+void *aero_rep_modal_binned_mass_create_gsd_update_data(void);
+void aero_rep_modal_binned_mass_set_gsd_update_data(void *update_data, int aero_rep_id,
+                                                    int section_id, double gsd);
 /* replace src/rxns/rxn_emission.c:192-213 (bound from
  * src/rxns/rxn_emission.F90:118-135) */
 void *rxn_emission_create_rate_update_data(void);
@@ -104,9 +113,10 @@ void rxn_wet_deposition_set_rate_update_data(void *update_data, int rxn_id,
                                              double base_rate);
 
 /* replace src/aero_phase_solver.c:175,210, src/aero_rep_solver.c:443,492,546
- * and src/sub_model_solver.c:413,468,509.  Data is accepted; a model with
- * aerosol phases, representations or sub-models is rejected at
- * solver_initialize in this build (gas-phase chemistry only). */
+ * and src/sub_model_solver.c:413,468,509.  Aerosol phases and the
+ * modal/binned mass representation (type 2) are solved with SIMPOL
+ * partitioning (reaction type 10); other representation types and any
+ * sub-model are rejected at solver_initialize. */
 void aero_phase_add_condensed_data(int n_int_param, int n_float_param,
                                    int *int_param, double *float_param,
                                    void *solver_data);
@@ -244,7 +254,14 @@ int camp_b200_n_photo(void *solver_data);
 int camp_b200_set_photo_rates(void *solver_data, const double *rates, int n_cells);
 /* Which reaction column `column` of the base rates belongs to: its index in
  * mechanism order, its type and its RXN_ID_ (the id update data carries).
+ * The columns after the reaction columns hold the geometric mean diameter
+ * [m] and standard deviation of every mode of the modal/binned aerosol
+ * representations (their update data sets them per cell); for those the
+ * reaction index is -1 - (representation index), the type
+ * CAMP_B200_COLUMN_GMD or _GSD and the id the section (mode) index.
  * Any pointer may be NULL.  0, or -1 when there is no such column. */
+#define CAMP_B200_COLUMN_GMD (-1)
+#define CAMP_B200_COLUMN_GSD (-2)
 int camp_b200_rate_column(void *solver_data, int column, int *rxn_index, int *rxn_type,
                           int *rxn_id);
 /* Device-resident form: rates [n_cells * n_photo] in device memory, read by

@@ -24,6 +24,7 @@
 #define T_FIRST_ORDER_LOSS 12
 #define T_EMISSION 13
 #define T_WET_DEPOSITION 14
+#define T_SIMPOL 10
 
 /* types whose packed data is not the NUM_REACT_/NUM_PROD_ layout */
 static int species_rate_type(int t) {
@@ -87,6 +88,14 @@ struct OracleMech {
   int *sj_colptr, *sj_rowid;
   int *rxn_to_solver;
   LUSym lu;
+  /* aerosol phases and representations, condensed data as added; a cell's
+   * representation env parameters (GMD, GSD per section) follow its
+   * reaction env parameters in the rxn_env buffer */
+  int n_aphase, n_arep, n_aero_env;
+  int *aph_int, *aph_ioff, *aph_foff, aph_ilen, aph_flen;
+  double *aph_flt;
+  int *arep_int, *arep_ioff, *arep_foff, *arep_eoff, *arep_type, arep_ilen, arep_flen;
+  double *arep_flt;
 };
 
 OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn) {
@@ -108,7 +117,9 @@ OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn) {
 int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
                const int *ints, const double *floats) {
   if (m->n_added >= m->n_rxn) return 1;
-  if ((type < T_ARRHENIUS || type > T_PHOTOLYSIS) && !species_rate_type(type)) return 2;
+  if ((type < T_ARRHENIUS || type > T_PHOTOLYSIS) && !species_rate_type(type) &&
+      type != T_SIMPOL)
+    return 2;
   if (m->int_size + n_int + 1 > m->int_cap) {
     m->int_cap = 2 * (m->int_size + n_int + 1) + 64;
     m->int_data = (int *)realloc(m->int_data, sizeof(int) * m->int_cap);
@@ -132,6 +143,316 @@ int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
   m->n_env += n_env;
   m->n_added++;
   return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Aerosol phases, the modal/binned mass representation (restating           */
+/* src/aero_phase_solver.c and src/aero_reps/aero_rep_modal_binned_mass.c)   */
+/* ------------------------------------------------------------------------ */
+
+#define AREP_MODAL_BINNED 2
+#define SEC_BINNED 1
+#define SEC_MODAL 2
+/* src/aero_phase_solver.c:14-19 */
+#define PH_MIN_MASS 1.0e-25L
+#define PH_MIN_MW 0.1L
+#define PH_MIN_DENSITY 1800.0L
+#define R_GAS 8.314472 /* src/util.h:15 */
+
+static void grow_i(int **p, int need, int *cap) {
+  if (need <= *cap) return;
+  *cap = 2 * need + 64;
+  *p = (int *)realloc(*p, sizeof(int) * (size_t)*cap);
+}
+static void grow_d(double **p, int need, int *cap) {
+  if (need <= *cap) return;
+  *cap = 2 * need + 64;
+  *p = (double *)realloc(*p, sizeof(double) * (size_t)*cap);
+}
+
+/* aero_phase_add_condensed_data (src/aero_phase_solver.c:162-189) */
+int om_add_aero_phase(OracleMech *m, int n_int, int n_float, const int *ints,
+                      const double *floats) {
+  int ic = m->aph_ilen, fc = m->aph_flen;
+  int icap = ic, fcap = fc;
+  grow_i(&m->aph_int, ic + n_int, &icap);
+  grow_d(&m->aph_flt, fc + n_float, &fcap);
+  m->aph_ioff = (int *)realloc(m->aph_ioff, sizeof(int) * (m->n_aphase + 1));
+  m->aph_foff = (int *)realloc(m->aph_foff, sizeof(int) * (m->n_aphase + 1));
+  memcpy(m->aph_int + ic, ints, sizeof(int) * n_int);
+  memcpy(m->aph_flt + fc, floats, sizeof(double) * n_float);
+  m->aph_ioff[m->n_aphase] = ic;
+  m->aph_foff[m->n_aphase] = fc;
+  m->aph_ilen += n_int;
+  m->aph_flen += n_float;
+  m->n_aphase++;
+  return 0;
+}
+
+/* aero_rep_add_condensed_data (src/aero_rep_solver.c:443-490); only the
+ * modal/binned mass representation is restated */
+int om_add_aero_rep(OracleMech *m, int type, int n_int, int n_float, int n_env,
+                    const int *ints, const double *floats) {
+  if (type != AREP_MODAL_BINNED) return 2;
+  int ic = m->arep_ilen, fc = m->arep_flen;
+  int icap = ic, fcap = fc;
+  grow_i(&m->arep_int, ic + n_int, &icap);
+  grow_d(&m->arep_flt, fc + n_float, &fcap);
+  const int k = m->n_arep;
+  m->arep_ioff = (int *)realloc(m->arep_ioff, sizeof(int) * (k + 1));
+  m->arep_foff = (int *)realloc(m->arep_foff, sizeof(int) * (k + 1));
+  m->arep_eoff = (int *)realloc(m->arep_eoff, sizeof(int) * (k + 1));
+  m->arep_type = (int *)realloc(m->arep_type, sizeof(int) * (k + 1));
+  memcpy(m->arep_int + ic, ints, sizeof(int) * n_int);
+  memcpy(m->arep_flt + fc, floats, sizeof(double) * n_float);
+  m->arep_ioff[k] = ic;
+  m->arep_foff[k] = fc;
+  m->arep_eoff[k] = m->n_aero_env;
+  m->arep_type[k] = type;
+  m->arep_ilen += n_int;
+  m->arep_flen += n_float;
+  m->n_aero_env += n_env;
+  m->n_arep++;
+  return 0;
+}
+
+/* one aerosol phase: species count, types, MW and density */
+typedef struct {
+  int n;
+  const int *type;
+  const double *mw, *dens;
+} APh;
+
+static APh aphase(const OracleMech *m, int p) {
+  const int *I = m->aph_int + m->aph_ioff[p];
+  const double *F = m->aph_flt + m->aph_foff[p];
+  APh a = {I[0], I + 1, F, F + I[0]};
+  return a;
+}
+
+static int counts_in_mass(int t) { return t == 1 || t == 2 || t == 3; }
+
+/* aero_phase_get_mass__kg_m3 (src/aero_phase_solver.c:88-117) */
+static void aph_mass(APh a, const double *y, double *mass, double *mw, double *dmass,
+                     double *dmw) {
+  long double lm = PH_MIN_MASS, mol = PH_MIN_MASS / PH_MIN_MW;
+  int k = 0;
+  for (int i = 0; i < a.n; ++i) {
+    if (!counts_in_mass(a.type[i])) continue;
+    lm += y[i];
+    mol += y[i] / (long double)a.mw[i];
+    if (dmass) dmass[k] = 1.0L;
+    if (dmw) dmw[k] = 1.0L / a.mw[i];
+    ++k;
+  }
+  *mw = (double)lm / mol;
+  if (dmw)
+    for (int j = 0; j < k; ++j) dmw[j] = (mol - dmw[j] * lm) / (mol * mol);
+  *mass = (double)lm;
+}
+
+/* aero_phase_get_volume__m3_m3 (src/aero_phase_solver.c:130-147) */
+static void aph_volume(APh a, const double *y, double *vol, double *dvol) {
+  *vol = PH_MIN_MASS / PH_MIN_DENSITY;
+  int k = 0;
+  for (int i = 0; i < a.n; ++i) {
+    if (!counts_in_mass(a.type[i])) continue;
+    *vol += y[i] / a.dens[i];
+    if (dvol) dvol[k++] = 1.0 / a.dens[i];
+  }
+}
+
+/* one modal/binned representation and a cell's env parameters */
+typedef struct {
+  int ns;
+  int *I; /* mutable: the element counts are written at registration */
+  const double *F;
+  const double *env; /* GMD[ns], GSD[ns] */
+} ARep;
+
+static ARep arep(const OracleMech *m, int r, const double *rxn_env) {
+  ARep a;
+  a.I = m->arep_int + m->arep_ioff[r];
+  a.F = m->arep_flt + m->arep_foff[r];
+  a.ns = a.I[0];
+  a.env = rxn_env ? rxn_env + m->n_env + m->arep_eoff[r] : NULL;
+  return a;
+}
+/* layout of src/aero_reps/aero_rep_modal_binned_mass.c:29-84 */
+static int sec_i(ARep a, int x) { return a.I[4 + x] - 1; }
+static int sec_f(ARep a, int x) { return a.I[4 + a.ns + x] - 1; }
+static int sec_type(ARep a, int x) { return a.I[sec_i(a, x)]; }
+static int sec_nb(ARep a, int x) { return a.I[sec_i(a, x) + 1]; }
+static int sec_np(ARep a, int x) { return a.I[sec_i(a, x) + 2]; }
+static int ph_state(ARep a, int x, int y, int b) {
+  return a.I[sec_i(a, x) + 3 + b * sec_np(a, x) + y] - 1;
+}
+static int ph_model(ARep a, int x, int y, int b) {
+  return a.I[sec_i(a, x) + 3 + sec_nb(a, x) * sec_np(a, x) + b * sec_np(a, x) + y] - 1;
+}
+static int *ph_njac(ARep a, int x, int y, int b) {
+  return &a.I[sec_i(a, x) + 3 + 2 * sec_nb(a, x) * sec_np(a, x) + b * sec_np(a, x) + y];
+}
+
+/* The C functions find a phase instance by walking sections, then bins,
+ * then the phases of a bin (src/aero_reps/aero_rep_modal_binned_mass.c:
+ * 300-330, 462-505): instance idx -> (section, bin, phase). */
+static int arep_locate(ARep a, int idx, int *x, int *b, int *y) {
+  for (int s = 0; s < a.ns; ++s)
+    for (int k = 0; k < sec_nb(a, s); ++k) {
+      if (idx < sec_np(a, s)) {
+        *x = s;
+        *b = k;
+        *y = idx;
+        return 1;
+      }
+      idx -= sec_np(a, s);
+    }
+  return 0;
+}
+
+/* effective radius [m]: modes from GMD/GSD (the update-data formula,
+ * :640-645), bins the bin radius; no state dependence */
+static double arep_radius(ARep a, int x, int b) {
+  if (sec_type(a, x) == SEC_MODAL) {
+    double ln_gsd = log(a.env[a.ns + x]);
+    return a.env[x] / 2.0 * exp(5.0 * ln_gsd * ln_gsd / 2.0);
+  }
+  return a.F[sec_f(a, x) + 3 * b + 2];
+}
+
+/* number concentration [# m-3] of a mode / bin and, if nconc_d, its partial
+ * derivatives over the mass species of all phases of the mode / bin
+ * (:176-236, :340-380) */
+static double arep_number(const OracleMech *m, ARep a, int x, int b, const double *state,
+                          double *nconc_d) {
+  double volume = 0.0;
+  double *d = nconc_d;
+  for (int y = 0; y < sec_np(a, x); ++y) {
+    APh ph = aphase(m, ph_model(a, x, y, b));
+    double pv = 0.0;
+    aph_volume(ph, state + ph_state(a, x, y, b), &pv, d);
+    volume += pv;
+    if (d) {
+      int k = 0;
+      for (int i = 0; i < ph.n; ++i) k += counts_in_mass(ph.type[i]);
+      d += k;
+    }
+  }
+  double n;
+  if (sec_type(a, x) == SEC_MODAL) {
+    const double gmd = a.env[x], gsd = a.env[a.ns + x];
+    n = volume * 6.0 / (M_PI * pow(gmd, 3) * exp(9.0 / 2.0 * pow(log(gsd), 2)));
+    if (nconc_d) {
+      const double f = 6.0 / (M_PI * pow(gmd, 3) * exp(9.0 / 2.0 * pow(log(gsd), 2)));
+      for (double *q = nconc_d; q < d; ++q) *q *= f;
+    }
+  } else {
+    const double dp = a.F[sec_f(a, x) + 3 * b];
+    n = volume * 3.0 / (4.0 * M_PI) / pow(dp / 2.0, 3);
+    if (nconc_d) {
+      const double f = 3.0 / (4.0 * M_PI) / pow(dp / 2.0, 3);
+      for (double *q = nconc_d; q < d; ++q) *q *= f;
+    }
+  }
+  return n;
+}
+
+/* mass [kg m-3] and average MW [kg mol-1] of phase y of a mode / bin, with
+ * their partials over all the mode's / bin's mass species (zero for the
+ * other phases, :462-560) */
+static void arep_phase_mass(const OracleMech *m, ARep a, int x, int b, int y0,
+                            const double *state, double *mass, double *mw, double *dmass,
+                            double *dmw) {
+  int off = 0;
+  for (int y = 0; y < sec_np(a, x); ++y) {
+    APh ph = aphase(m, ph_model(a, x, y, b));
+    int k = 0;
+    for (int i = 0; i < ph.n; ++i) k += counts_in_mass(ph.type[i]);
+    if (y == y0) {
+      aph_mass(ph, state + ph_state(a, x, y, b), mass, mw, dmass ? dmass + off : NULL,
+               dmw ? dmw + off : NULL);
+    } else {
+      for (int j = 0; j < k; ++j) {
+        if (dmass) dmass[off + j] = 0.0;
+        if (dmw) dmw[off + j] = 0.0;
+      }
+    }
+    off += k;
+  }
+}
+
+/* GMD (what 0) or GSD (what 1) of section x of representation r in one
+ * cell's env buffer, as the GMD/GSD update data set them
+ * (src/aero_reps/aero_rep_modal_binned_mass.c:602-650) */
+int om_set_aero_env(const OracleMech *m, double *rxn_env, int rep, int section, int what,
+                    double value) {
+  if (rep < 0 || rep >= m->n_arep) return 0;
+  ARep a = arep(m, rep, rxn_env);
+  if (section < 0 || section >= a.ns || sec_type(a, section) != SEC_MODAL) return 0;
+  rxn_env[m->n_env + m->arep_eoff[rep] + what * a.ns + section] = value;
+  return 1;
+}
+
+/* --- SIMPOL phase transfer (src/rxns/rxn_SIMPOL_phase_transfer.c) -------- */
+/* packed layout of :37-78 */
+typedef struct {
+  int n;
+  int *I;
+  const double *F;
+} SIM;
+static SIM simpol(const ORxn *r) {
+  SIM s = {r->ints[0], r->ints, r->fl};
+  return s;
+}
+static int sim_gas(SIM s) { return s.I[1] - 1; }
+static int sim_aero(SIM s, int x) { return s.I[2 + x] - 1; }
+static int sim_act(SIM s, int x) { return s.I[2 + s.n + x] - 1; }
+static int sim_phase(SIM s, int x) { return s.I[2 + 2 * s.n + x] - 1; }
+static int sim_rep(SIM s, int x) { return s.I[2 + 3 * s.n + x] - 1; }
+static int *sim_deriv(SIM s, int x) { return &s.I[2 + 4 * s.n + x]; }
+static int *sim_gas_act_jac(SIM s, int x) { return &s.I[3 + 5 * s.n + x]; }
+static int *sim_aero_act_jac(SIM s, int x) { return &s.I[3 + 6 * s.n + x]; }
+static int *sim_jac(SIM s, int x) { return &s.I[3 + 7 * s.n + x]; }
+static int sim_iloc(SIM s, int x) { return s.I[4 + 10 * s.n + x] - 1; }
+static int sim_nelem(SIM s, int x) { return s.I[sim_iloc(s, x)]; }
+static int *sim_phase_jac(SIM s, int x, int set, int e) {
+  return &s.I[sim_iloc(s, x) + 1 + set * sim_nelem(s, x) + e];
+}
+
+/* transition-regime condensation rate constant and its radius derivative
+ * (src/util.h:69-161, Fuchs-Sutugin) */
+static double fs_factor(double mfp, double r, double alpha) {
+  double kn = mfp / r;
+  return (0.75 * alpha * (1.0 + kn)) / (kn * kn + (1.0 + 0.283 * alpha) * kn + 0.75 * alpha);
+}
+static double fs_factor_dr(double mfp, double r, double alpha) {
+  double kn = mfp / r;
+  return (0.75 * alpha * mfp * (kn * kn + 2.0 * kn + 1.0 + (0.283 - 0.75) * alpha)) /
+         pow(r * (kn * kn + (1.0 + 0.283 * alpha) * kn + 0.75 * alpha), 2);
+}
+static double cond_k(double D, double mfp, double r, double alpha) {
+  return 4.0 * M_PI * r * D * fs_factor(mfp, r, alpha);
+}
+static double cond_k_dr(double D, double mfp, double r, double alpha) {
+  return 4.0 * M_PI * D * (fs_factor(mfp, r, alpha) + r * fs_factor_dr(mfp, r, alpha));
+}
+
+/* rate constants of one SIMPOL reaction (:220-262): MFP, alpha, K_eq and
+ * the kg m-3 -> ppm factor */
+static void simpol_env(const ORxn *r, double T, double P, double *k) {
+  const double *f = r->fl;
+  k[1] = 0.1;
+  if (f[0] != 0.0 || f[1] != 0.0) {
+    double del_g = f[0] - T * f[1];
+    k[1] = exp(-del_g / (R_GAS * T));
+    k[1] = k[1] / (1.0 + k[1]);
+  }
+  k[0] = 3.0 * f[2] / sqrt(8.0 * R_GAS * T / (M_PI * f[9]));
+  double vp = f[4] / T + f[5] + f[6] * T + f[7] * log(T);
+  vp = 101325.0 * pow(10, vp);
+  k[3] = f[8] * T / P;
+  k[2] = vp / P / f[9] * 1.0e6;
 }
 
 /* --- Jacobian element registry (restates src/Jacobian.c:105-214) -------- */
@@ -284,7 +605,7 @@ int om_build(OracleMech *m) {
     ORxn *r = &m->rx[i];
     r->ints = m->int_data + (size_t)r->ints;
     r->fl = m->float_data + (size_t)r->fl;
-    if (species_rate_type(r->type)) {
+    if (species_rate_type(r->type) || r->type == T_SIMPOL) {
       /* RXN_ID_ first; the reactant / product fields stay unused */
       r->nr = r->np = 0;
       r->n_int_prop = 0;
@@ -318,6 +639,52 @@ int om_build(OracleMech *m) {
       case T_WET_DEPOSITION: /* src/rxns/rxn_wet_deposition.c:38-49 */
         for (int s = 0; s < I[1]; ++s) jr_register(&rj, I[2 + s] - 1, I[2 + s] - 1);
         continue;
+      case T_SIMPOL: { /* src/rxns/rxn_SIMPOL_phase_transfer.c:86-151 */
+        SIM sm = simpol(r);
+        const int g = sim_gas(sm);
+        jr_register(&rj, g, g);
+        char *flag = (char *)zalloc((size_t)n);
+        for (int x = 0; x < sm.n; ++x) {
+          const int a = sim_aero(sm, x);
+          jr_register(&rj, a, g);
+          jr_register(&rj, g, a);
+          jr_register(&rj, a, a);
+          if (sim_act(sm, x) > 0) {
+            jr_register(&rj, g, sim_act(sm, x));
+            jr_register(&rj, a, sim_act(sm, x));
+          }
+          /* the representation's elements: the mass species of every phase
+           * of the instance's mode / bin (aero_rep_modal_binned_mass.c:
+           * 86-125), registered in state order */
+          memset(flag, 0, (size_t)n);
+          ARep ar = arep(m, sim_rep(sm, x), NULL);
+          int sx, sb, sy;
+          if (arep_locate(ar, sim_phase(sm, x), &sx, &sb, &sy))
+            for (int y = 0; y < sec_np(ar, sx); ++y) {
+              APh ph = aphase(m, ph_model(ar, sx, y, sb));
+              int k = 0;
+              for (int i = 0; i < ph.n; ++i)
+                if (counts_in_mass(ph.type[i])) {
+                  flag[ph_state(ar, sx, y, sb) + i] = 1;
+                  ++k;
+                }
+              *ph_njac(ar, sx, y, sb) = k;
+            }
+          int used = 0;
+          for (int e = 0; e < n; ++e) {
+            if (!flag[e]) continue;
+            jr_register(&rj, g, e);
+            jr_register(&rj, a, e);
+            *sim_phase_jac(sm, x, 0, used) = e;
+            *sim_phase_jac(sm, x, 1, used) = e;
+            ++used;
+          }
+          for (; used < sim_nelem(sm, x); ++used)
+            *sim_phase_jac(sm, x, 0, used) = *sim_phase_jac(sm, x, 1, used) = -1;
+        }
+        free(flag);
+        continue;
+      }
     }
     for (int ind = 0; ind < r->nr; ++ind) {
       for (int d = 0; d < r->nr; ++d) jr_register(&rj, R_REACT(r, d), R_REACT(r, ind));
@@ -349,6 +716,34 @@ int om_build(OracleMech *m) {
           I[2 + ns + s] = m->deriv_ids[I[2 + s] - 1];
           I[2 + 2 * ns + s] =
               jr_elem_id(m->rj_colptr, m->rj_rowid, I[2 + s] - 1, I[2 + s] - 1);
+        }
+        continue;
+      }
+      case T_SIMPOL: { /* src/rxns/rxn_SIMPOL_phase_transfer.c:160-205 */
+        SIM sm = simpol(r);
+        const int *cp = m->rj_colptr, *ri = m->rj_rowid;
+        const int g = sim_gas(sm);
+        *sim_deriv(sm, 0) = m->deriv_ids[g];
+        for (int x = 0; x < sm.n; ++x) *sim_deriv(sm, x + 1) = m->deriv_ids[sim_aero(sm, x)];
+        int ij = 0;
+        *sim_jac(sm, ij++) = jr_elem_id(cp, ri, g, g);
+        for (int x = 0; x < sm.n; ++x) {
+          const int a = sim_aero(sm, x);
+          *sim_jac(sm, ij++) = jr_elem_id(cp, ri, a, g);
+          *sim_jac(sm, ij++) = jr_elem_id(cp, ri, g, a);
+          *sim_jac(sm, ij++) = jr_elem_id(cp, ri, a, a);
+          if (sim_act(sm, x) > 0) {
+            *sim_gas_act_jac(sm, x) = jr_elem_id(cp, ri, g, sim_act(sm, x));
+            *sim_aero_act_jac(sm, x) = jr_elem_id(cp, ri, a, sim_act(sm, x));
+          } else {
+            *sim_gas_act_jac(sm, x) = -1;
+            *sim_aero_act_jac(sm, x) = -1;
+          }
+          for (int e = 0; e < sim_nelem(sm, x); ++e) {
+            int *pg = sim_phase_jac(sm, x, 0, e), *pa = sim_phase_jac(sm, x, 1, e);
+            if (*pg > 0) *pg = jr_elem_id(cp, ri, g, *pg);
+            if (*pa > 0) *pa = jr_elem_id(cp, ri, a, *pa);
+          }
         }
         continue;
       }
@@ -413,12 +808,22 @@ void om_free(OracleMech *m) {
   free(m->sj_colptr);
   free(m->sj_rowid);
   free(m->rxn_to_solver);
+  free(m->aph_int);
+  free(m->aph_ioff);
+  free(m->aph_foff);
+  free(m->aph_flt);
+  free(m->arep_int);
+  free(m->arep_ioff);
+  free(m->arep_foff);
+  free(m->arep_eoff);
+  free(m->arep_type);
+  free(m->arep_flt);
   if (m->built) lu_free(&m->lu);
   free(m);
 }
 
 int om_n_dep_var(const OracleMech *m) { return m->n_dep; }
-int om_n_rxn_env_data(const OracleMech *m) { return m->n_env; }
+int om_n_rxn_env_data(const OracleMech *m) { return m->n_env + m->n_aero_env; }
 int om_n_rxn_jac_elem(const OracleMech *m) { return m->n_rxn_jac; }
 int om_n_solver_jac_elem(const OracleMech *m) { return m->n_solver_jac; }
 int om_n_lu_elem(const OracleMech *m) { return m->lu.nnz; }
@@ -522,6 +927,9 @@ void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
       case T_WET_DEPOSITION:     /* src/rxns/rxn_wet_deposition.c:124-136 */
         k[0] = f[0] * k[1];
         break;
+      case T_SIMPOL:
+        simpol_env(r, T, P, k);
+        break;
     }
   }
 }
@@ -563,6 +971,38 @@ void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
         for (int s = 0; s < ns; ++s)
           if (I[2 + ns + s] >= 0)
             add_value(P, L, I[2 + ns + s], -(k * (long double)state[I[2 + s] - 1]));
+        continue;
+      }
+      case T_SIMPOL: { /* src/rxns/rxn_SIMPOL_phase_transfer.c:337-450 */
+        SIM sm = simpol(r);
+        const double *kk = rxn_env + r->env_off;
+        for (int x = 0; x < sm.n; ++x) {
+          ARep ar = arep(m, sim_rep(sm, x), rxn_env);
+          int sx, sb, sy;
+          if (!arep_locate(ar, sim_phase(sm, x), &sx, &sb, &sy)) continue;
+          const double radius = arep_radius(ar, sx, sb);
+          const double nconc = arep_number(m, ar, sx, sb, state, NULL);
+          double mass, mw;
+          arep_phase_mass(m, ar, sx, sb, sy, state, &mass, &mw, NULL, NULL);
+          long double cond = cond_k(sm.F[2], kk[0], radius, kk[1]);
+          long double evap = cond * (kk[2] * mw / mass);
+          long double act = 1.0;
+          if (sim_act(sm, x) > -1) act = state[sim_act(sm, x)];
+          evap *= act;
+          cond *= state[sim_gas(sm)];
+          evap *= state[sim_aero(sm, x)];
+          /* total-particle mass concentrations (this representation's
+           * aero_conc_type) */
+          const int dg = *sim_deriv(sm, 0), da = *sim_deriv(sm, 1 + x);
+          if (dg >= 0) {
+            add_value(P, L, dg, nconc * evap);
+            add_value(P, L, dg, -nconc * cond);
+          }
+          if (da >= 0) {
+            add_value(P, L, da, -nconc * evap / kk[3]);
+            add_value(P, L, da, nconc * cond / kk[3]);
+          }
+        }
         continue;
       }
     }
@@ -614,6 +1054,67 @@ void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
         const int ns = I[1];
         for (int s = 0; s < ns; ++s)
           if (I[2 + 2 * ns + s] >= 0) L[I[2 + 2 * ns + s]] += rxn_env[r->env_off];
+        continue;
+      }
+      case T_SIMPOL: { /* src/rxns/rxn_SIMPOL_phase_transfer.c:463-744 */
+        SIM sm = simpol(r);
+        const double *kk = rxn_env + r->env_off;
+        const double Kp = kk[3];
+        for (int x = 0; x < sm.n; ++x) {
+          ARep ar = arep(m, sim_rep(sm, x), rxn_env);
+          int sx, sb, sy;
+          if (!arep_locate(ar, sim_phase(sm, x), &sx, &sb, &sy)) continue;
+          const int ne = sim_nelem(sm, x);
+          double *nd = (double *)zalloc(sizeof(double) * (3 * (size_t)ne + 1));
+          const double radius = arep_radius(ar, sx, sb);
+          const double nconc = arep_number(m, ar, sx, sb, state, nd);
+          double mass, mw;
+          arep_phase_mass(m, ar, sx, sb, sy, state, &mass, &mw, nd + ne, nd + 2 * ne);
+          long double cond = cond_k(sm.F[2], kk[0], radius, kk[1]);
+          long double evap = cond * (kk[2] * mw / mass);
+          long double act = 1.0;
+          if (sim_act(sm, x) > -1) act = state[sim_act(sm, x)];
+          const double yg = state[sim_gas(sm)], ya = state[sim_aero(sm, x)];
+          const int jgg = *sim_jac(sm, 0), jag = *sim_jac(sm, 1 + 3 * x);
+          const int jga = *sim_jac(sm, 2 + 3 * x), jaa = *sim_jac(sm, 3 + 3 * x);
+          if (jga >= 0) P[jga] += nconc * evap * act;
+          if (jgg >= 0) L[jgg] += nconc * cond;
+          if (jag >= 0) P[jag] += nconc * cond / Kp;
+          if (jaa >= 0) L[jaa] += nconc * evap * act / Kp;
+          if (*sim_gas_act_jac(sm, x) > 0) P[*sim_gas_act_jac(sm, x)] += nconc * evap * ya;
+          if (*sim_aero_act_jac(sm, x) > 0)
+            L[*sim_aero_act_jac(sm, x)] += nconc * evap / Kp * ya;
+          evap *= act;
+          cond *= yg;
+          evap *= ya;
+          /* radius partials are zero for this representation (its radii do
+           * not depend on the state), added as the reference adds them */
+          const double dcdr = cond_k_dr(sm.F[2], kk[0], radius, kk[1]) * yg;
+          const double dedr = dcdr / yg * kk[2] * mw / mass * ya;
+          const double dedm = -evap / mass;
+          const double dedw = evap / mw;
+          for (int e = 0; e < ne; ++e) {
+            const double eff = 0.0, num = nd[e], ms = nd[ne + e], mwj = nd[2 * ne + e];
+            const int jg = *sim_phase_jac(sm, x, 0, e), ja = *sim_phase_jac(sm, x, 1, e);
+            if (jg > 0) {
+              P[jg] += nconc * dedr * eff;
+              L[jg] += nconc * dcdr * eff;
+              P[jg] += evap * num;
+              L[jg] += cond * num;
+              P[jg] += nconc * dedm * ms;
+              P[jg] += nconc * dedw * mwj;
+            }
+            if (ja > 0) {
+              L[ja] += nconc * dedr / Kp * eff;
+              P[ja] += nconc * dcdr / Kp * eff;
+              L[ja] += evap / Kp * num;
+              P[ja] += cond / Kp * num;
+              L[ja] += nconc * dedm / Kp * ms;
+              L[ja] += nconc * dedw / Kp * mwj;
+            }
+          }
+          free(nd);
+        }
         continue;
       }
     }
@@ -1435,7 +1936,7 @@ static void *solve_job(void *arg) {
   b.ctx = &ctx;
   for (int c = jb->c0; c < jb->c1; ++c) {
     double *st = jb->state + (size_t)c * ns;
-    double *re = jb->rxn_env + (size_t)c * m->n_env;
+    double *re = jb->rxn_env + (size_t)c * (m->n_env + m->n_aero_env);
     /* solver_run: dependent values clamped to >= TINY, constants too
      * (src/camp_solver.c:554-567); rate constants from env (:587-603) */
     for (int i = 0, d = 0; i < ns; ++i) {

@@ -58,6 +58,16 @@ typedef int (*or_jac_fn)(void *ctx, double t, const double *y, double h,
 OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn);
 int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
                const int *ints, const double *floats);
+/* aero_phase_add_condensed_data / aero_rep_add_condensed_data (the
+ * modal/binned mass representation, type 2, only) */
+int om_add_aero_phase(OracleMech *m, int n_int, int n_float, const int *ints,
+                      const double *floats);
+int om_add_aero_rep(OracleMech *m, int type, int n_int, int n_float, int n_env,
+                    const int *ints, const double *floats);
+/* GMD (what 0) or GSD (what 1) of a mode in one cell's rxn_env buffer, whose
+ * representation part follows the reaction env parameters */
+int om_set_aero_env(const OracleMech *m, double *rxn_env_cell, int rep, int section,
+                    int what, double value);
 int om_build(OracleMech *m);
 void om_free(OracleMech *m);
 

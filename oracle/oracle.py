@@ -89,6 +89,12 @@ def oracle_lib():
         lib.om_set_photo_rate.argtypes = [vp, _f64p, C.c_int, C.c_double]
         lib.om_set_rate.restype = C.c_int
         lib.om_set_rate.argtypes = [vp, _f64p, C.c_int, C.c_int, C.c_double]
+        lib.om_add_aero_phase.restype = C.c_int
+        lib.om_add_aero_phase.argtypes = [vp, C.c_int, C.c_int, _i32p, _f64p]
+        lib.om_add_aero_rep.restype = C.c_int
+        lib.om_add_aero_rep.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p]
+        lib.om_set_aero_env.restype = C.c_int
+        lib.om_set_aero_env.argtypes = [vp, _f64p, C.c_int, C.c_int, C.c_int, C.c_double]
         lib.om_update_env.argtypes = [vp, _f64p, _f64p]
         lib.om_deriv.argtypes = [vp, _f64p, _f64p, C.c_double, _f64p, _f64p, _f64p]
         lib.om_jac.argtypes = [vp, _f64p, _f64p, C.c_double, _f64p]
@@ -150,6 +156,14 @@ def ref_lib():
         for kind in ("photolysis", "emission", "first_order_loss", "wet_deposition"):
             getattr(lib, f"rxn_{kind}_create_rate_update_data").restype = vp
             getattr(lib, f"rxn_{kind}_set_rate_update_data").argtypes = [vp, C.c_int, C.c_double]
+        lib.aero_phase_add_condensed_data.argtypes = [C.c_int, C.c_int, _i32p, _f64p, vp]
+        lib.aero_rep_add_condensed_data.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p,
+                                                    _f64p, vp]
+        lib.aero_rep_update_data.argtypes = [C.c_int, C.POINTER(C.c_int), C.c_int, vp, vp]
+        for what in ("gmd", "gsd"):
+            getattr(lib, f"aero_rep_modal_binned_mass_create_{what}_update_data").restype = vp
+            getattr(lib, f"aero_rep_modal_binned_mass_set_{what}_update_data").argtypes = [
+                vp, C.c_int, C.c_int, C.c_double]
         _ref_lib = lib
     return _ref_lib
 
@@ -168,6 +182,15 @@ class OracleModel:
             )
             if rc != 0:
                 raise ValueError(f"oracle rejected reaction type {r.rxn_type} (code {rc})")
+        for p in mech.aero_phases:
+            self.lib.om_add_aero_phase(self.h, p.ints.size, p.floats.size,
+                                       np.ascontiguousarray(p.ints, np.int32),
+                                       np.ascontiguousarray(p.floats, np.float64))
+        for a in mech.aero_reps:
+            if self.lib.om_add_aero_rep(self.h, a.rep_type, a.ints.size, a.floats.size, a.n_env,
+                                        np.ascontiguousarray(a.ints, np.int32),
+                                        np.ascontiguousarray(a.floats, np.float64)) != 0:
+                raise ValueError(f"oracle rejected aerosol representation type {a.rep_type}")
         if self.lib.om_build(self.h) != 0:
             raise RuntimeError("oracle sparsity build failed")
         self.n_dep = self.lib.om_n_dep_var(self.h)
@@ -219,6 +242,24 @@ class OracleModel:
         self.lib.om_update_env(self.h, np.asarray(env, np.float64), re)
         return re
 
+    def _set_row(self, re, row) -> None:
+        """One cell's host-set columns (``Mechanism.rate_columns`` order)."""
+        for j, col in enumerate(self.mech.rate_columns()):
+            v = float(row[j])
+            if col[0] == "rxn":
+                i = col[1]
+                self.lib.om_set_rate(self.h, re, self.mech.rxns[i].rxn_type,
+                                     self.mech.rate_id(i), v)
+            else:
+                self.lib.om_set_aero_env(self.h, re, col[1], col[2], 0 if col[0] == "gmd" else 1, v)
+
+    def rxn_env_row(self, env, row):
+        """rxn_env from a full row of host-set columns (rates, GMD, GSD)."""
+        re = np.zeros(max(self.n_env, 1), np.float64)
+        self._set_row(re, row)
+        self.lib.om_update_env(self.h, np.asarray(env, np.float64), re)
+        return re
+
     def deriv(self, state, rxn_env, time_step):
         f = np.zeros(self.n_dep)
         rp = np.zeros(self.n_dep)
@@ -243,12 +284,10 @@ class OracleModel:
         env = np.ascontiguousarray(env, np.float64).reshape(n_cells, 2)
         re = np.zeros((n_cells, max(self.n_env, 1)), np.float64)
         photo_rates = np.asarray(photo_rates, np.float64).reshape(n_cells, -1)
-        cols = [(self.mech.rxns[i].rxn_type, self.mech.rate_id(i)) for i in self.mech.rate_rxns()]
-        if photo_rates.shape[1] != len(cols):
-            raise ValueError("photo_rates must have one column per host-rate reaction")
+        if photo_rates.shape[1] != len(self.mech.rate_columns()):
+            raise ValueError("photo_rates must have one column per host-set value")
         for c in range(n_cells):
-            for j, (rtype, rid) in enumerate(cols):
-                self.lib.om_set_rate(self.h, re[c], rtype, rid, float(photo_rates[c, j]))
+            self._set_row(re[c], photo_rates[c])
         status = np.zeros(n_cells, np.int32)
         stats = (OracleStats * n_cells)()
         nf = self.lib.om_solve(
@@ -269,13 +308,23 @@ class RefModel:
         self.h = self.lib.ref_new(
             mech.n_state_var, n_cells, np.ascontiguousarray(mech.var_type, np.int32),
             mech.n_rxn, mech.n_rxn_int_param, mech.n_rxn_float_param, mech.n_rxn_env_param,
-            0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+            *mech.aero_sizes(), 0, 0, 0, 0,
         )
         for r in mech.rxns:
             self.lib.rxn_add_condensed_data(
                 r.rxn_type, r.ints.size, r.floats.size, r.n_env,
                 np.ascontiguousarray(r.ints, np.int32), np.ascontiguousarray(r.floats, np.float64), self.h,
             )
+        for p in mech.aero_phases:
+            self.lib.aero_phase_add_condensed_data(p.ints.size, p.floats.size,
+                                                   np.ascontiguousarray(p.ints, np.int32),
+                                                   np.ascontiguousarray(p.floats, np.float64),
+                                                   self.h)
+        for a in mech.aero_reps:
+            self.lib.aero_rep_add_condensed_data(a.rep_type, a.ints.size, a.floats.size, a.n_env,
+                                                 np.ascontiguousarray(a.ints, np.int32),
+                                                 np.ascontiguousarray(a.floats, np.float64),
+                                                 self.h)
         rc = self.lib.ref_build(self.h)
         if rc != 0:
             raise RuntimeError(f"reference sparsity build failed ({rc})")
@@ -325,10 +374,26 @@ class RefModel:
         cursor = C.c_int(0)
         self.lib.rxn_update_data(int(cell), C.byref(cursor), int(rxn_type), ud, self.h)
 
+    def set_aero(self, cell: int, rep: int, section: int, what: str, value: float) -> None:
+        """GMD or GSD of a mode through the reference's update data and
+        aero_rep_update_data (which also sets the mode's effective radius)."""
+        lib = self.lib
+        ud = getattr(lib, f"aero_rep_modal_binned_mass_create_{what}_update_data")()
+        rep_id = int(self.mech.aero_reps[rep].ints[3])
+        getattr(lib, f"aero_rep_modal_binned_mass_set_{what}_update_data")(ud, rep_id, section,
+                                                                            float(value))
+        cursor = C.c_int(0)
+        lib.aero_rep_update_data(int(cell), C.byref(cursor), 2, ud, self.h)
+
     def set_rates(self, cell: int, row) -> None:
-        """One cell's host-rate columns (``Mechanism.rate_rxns`` order)."""
-        for j, i in enumerate(self.mech.rate_rxns()):
-            self.set_rate(cell, self.mech.rxns[i].rxn_type, self.mech.rate_id(i), float(row[j]))
+        """One cell's host-set columns (``Mechanism.rate_columns`` order)."""
+        for j, col in enumerate(self.mech.rate_columns()):
+            if col[0] == "rxn":
+                i = col[1]
+                self.set_rate(cell, self.mech.rxns[i].rxn_type, self.mech.rate_id(i),
+                              float(row[j]))
+            else:
+                self.set_aero(cell, col[1], col[2], col[0], float(row[j]))
 
     def set_cell(self, cell, state, env):
         self.state[cell, :] = state

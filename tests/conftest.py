@@ -37,9 +37,11 @@ def cb05_ref():
 
 
 # golden fixtures made by tests/golden/make_golden.py from the reference's C
-# code: cb05cl_ae5, and the gas phase of MONARCH mod37 (cb05 with dry
-# deposition, emissions and the wet deposition of one aqueous phase)
-GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas")
+# code: cb05cl_ae5, the gas phase of MONARCH mod37 (cb05 with dry
+# deposition, emissions and the wet deposition of one aqueous phase), and
+# mod37 with its SOA scheme (SIMPOL partitioning into the modal/binned
+# aerosol representation)
+GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas", "monarch_mod37_soa")
 
 
 @pytest.fixture(scope="session")
@@ -47,6 +49,13 @@ def mod37():
     from camp_b200.mechanism import Mechanism
 
     return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_gas.mech.json"))
+
+
+@pytest.fixture(scope="session")
+def mod37_soa():
+    from camp_b200.mechanism import Mechanism
+
+    return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_soa.mech.json"))
 
 
 @pytest.fixture(scope="session", params=GOLDEN_MECHS)

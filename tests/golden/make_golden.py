@@ -16,7 +16,17 @@ Outputs (all small):
                          state variables (no aerosol representation is read;
                          the packed wet-deposition data lists their indices as
                          the Fortran packer would)
-  cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz
+  monarch_mod37_soa.mech.json
+                         the same gas phase with the shipped 2-product SOA
+                         scheme (4 Arrhenius + 4 SIMPOL_PHASE_TRANSFER into
+                         the "organic matter" mode) and the shipped aerosol
+                         phases and MONARCH modal/binned mass representation
+                         (7 modes and bin sets, 99 aerosol state variables);
+                         its wet deposition acts on the cloud-and-rain phase
+                         instance.  The aerosol reactions of mod37 that are
+                         not restated (HL, aqueous equilibrium, ZSR, PDFiTE)
+                         are left out
+  cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz, monarch_mod37_soa_ref.npz
                          outputs of the reference's own C code
                          (oracle/_ref/libcamp_ref.so, compiled from the
                          reference sources) on seeded cell states:
@@ -84,6 +94,21 @@ def mod37_gas(ref_root: str):
     return mech
 
 
+MOD37_SOA_FILES = MOD37_GAS_FILES + ("inorganic_species.json", "cloud_and_rain_species.json",
+                                     "tsigaridis_2_product_SOA_scheme/species.json",
+                                     "tsigaridis_2_product_SOA_scheme/mechanism.json",
+                                     "aerosol_phases.json", "aerosol_representation.json",
+                                     "wet_deposition.json")
+
+
+def mod37_soa(ref_root: str):
+    from camp_b200.aerosol import load_aerosol_mechanism
+
+    base = os.path.join(ref_root, "mechanisms/monarch_mod37")
+    return load_aerosol_mechanism([os.path.join(base, f) for f in MOD37_SOA_FILES],
+                                  name="monarch_mod37_soa")
+
+
 def edge_cells(mech, cells):
     """Appends edge-case cells to a seeded batch."""
     st, env, ph = cells.state.copy(), cells.env.copy(), cells.photo_rates.copy()
@@ -93,8 +118,10 @@ def edge_cells(mech, cells):
     s = st[0].copy()
     s[var] = 1.0e-60
     extra_s.append(s); extra_e.append([298.0, 101325.0]); extra_p.append(ph[0])
-    # dark cell
-    extra_s.append(st[1].copy()); extra_e.append(env[1]); extra_p.append(np.zeros_like(ph[1]))
+    # dark cell (every host-set reaction rate 0; GMD / GSD kept)
+    dark = ph[1].copy()
+    dark[[j for j, c in enumerate(mech.rate_columns()) if c[0] == "rxn"]] = 0.0
+    extra_s.append(st[1].copy()); extra_e.append(env[1]); extra_p.append(dark)
     # PAR nearly exhausted while its negative-yield producers are abundant
     s = st[2].copy()
     s[mech.index("PAR")] = 1.0e-12
@@ -113,6 +140,7 @@ def main(ref_root: str) -> None:
     build(with_ref=True)
     write_fixture(load_mechanism(cb05_files(ref_root), name="cb05cl_ae5"), "cb05cl_ae5")
     write_fixture(mod37_gas(ref_root), "monarch_mod37_gas")
+    write_fixture(mod37_soa(ref_root), "monarch_mod37_soa")
 
 
 def write_fixture(mech, tag: str) -> None:
@@ -144,6 +172,9 @@ def write_fixture(mech, tag: str) -> None:
     for h in H_VALUES:
         fs, rps, rls, js = [], [], [], []
         for c in range(nc):
+            # the reference keeps a mode's effective radius per solver, not
+            # per cell: apply this cell's GMD / GSD again before its f and J
+            ref.set_rates(c, photo[c])
             f, rp, rl = ref.deriv(c, h)
             j, _ = ref.jac(c, h)
             fs.append(f); rps.append(rp); rls.append(rl); js.append(j)

@@ -124,6 +124,47 @@ def test_mod37_gas_solve_matches_oracle(mod37, precision):
                  bulk_rel=1e-7 if precision == 0 else 1e-4)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mod37_soa_solve_matches_oracle(mod37_soa, precision):
+    """mod37 with SIMPOL partitioning into the modal/binned aerosol
+    representation (cells carry per-mode GMD / GSD columns)."""
+    _check_solve(mod37_soa, precision=precision, seed=17 + precision,
+                 bulk_rel=1e-7 if precision == 0 else 1e-4)
+
+
+def test_aerosol_update_data_sets_columns(mod37_soa):
+    """GMD / GSD through the reference's update-data path land in the
+    cell's mode columns, the same values set_photo_rates takes."""
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import Solver
+
+    m = mod37_soa
+    cells = make_cells(m, 3, 23)
+    cols = m.rate_columns()
+    a = Solver(m, 3)
+    a.initialize(abs_tol=np.full(m.n_state_var, 1e-8), rel_tol=1e-4, max_steps=2000)
+    a.set_photo_rates(cells.photo_rates)
+    b = Solver(m, 3)
+    b.initialize(abs_tol=np.full(m.n_state_var, 1e-8), rel_tol=1e-4, max_steps=2000)
+    rates = cells.photo_rates.copy()
+    aero = [j for j, c in enumerate(cols) if c[0] != "rxn"]
+    rates[:, aero] = 0.0
+    b.set_photo_rates(rates)
+    rep_id = int(m.aero_reps[0].ints[3])
+    for c in range(3):
+        for j in aero:
+            kind, _, sec = cols[j]
+            b.set_aero(c, rep_id, sec, kind, cells.photo_rates[c, j])
+    for j in aero:
+        idx, typ, sec = b.rate_column(j)
+        assert idx == -1 and typ in (-1, -2) and sec == cols[j][2]
+    xa, xb = cells.state.copy(), cells.state.copy()
+    a.solve(xa, cells.env, 0.0, 60.0)
+    b.solve(xb, cells.env, 0.0, 60.0)
+    np.testing.assert_array_equal(a.cell_stats()["status"], b.cell_stats()["status"])
+    np.testing.assert_array_equal(xa, xb)
+
+
 def test_failed_cells_keep_input_state(cb05):
     """A cell that cannot finish (max_steps 5) leaves its input state and
     reports TOO_MUCH_WORK, and solver_run returns 1."""

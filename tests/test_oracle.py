@@ -49,15 +49,17 @@ def _photo_dict(row):
 def test_rate_constants(gom):
     om, ref = gom
     for c in range(ref["state"].shape[0]):
-        re = om.rxn_env(ref["env"][c], _photo_dict(ref["photo"][c]))
-        np.testing.assert_allclose(re, ref["rxn_env"][c], rtol=1e-15, atol=0)
+        re = om.rxn_env_row(ref["env"][c], ref["photo"][c])
+        n = ref["rxn_env"].shape[1]  # the aerosol GMD/GSD follow in the oracle's buffer
+        np.testing.assert_allclose(re[:n], ref["rxn_env"][c], rtol=1e-15, atol=0)
 
 
 def test_deriv_and_jacobian(gom):
     om, ref = gom
     for ih, h in enumerate(ref["h"]):
         for c in range(ref["state"].shape[0]):
-            re = ref["rxn_env"][c]
+            re = om.rxn_env_row(ref["env"][c], ref["photo"][c])
+            re[:ref["rxn_env"].shape[1]] = ref["rxn_env"][c]
             st = ref["state"][c]
             f, rp, rl = om.deriv(st, re, h)
             np.testing.assert_allclose(rp, ref["r_p"][ih][c], rtol=1e-12, atol=0)
@@ -67,6 +69,21 @@ def test_deriv_and_jacobian(gom):
             j = om.jac(st, re, h)
             jr = ref["jac"][ih][c]
             assert np.all(np.abs(j - jr) <= 1e-12 * np.abs(jr) + 1e-300)
+
+
+def test_mod37_soa_composition(mod37_soa):
+    """The SOA fixture: 4 SIMPOL reactions into one mode, the modal/binned
+    representation's 99 aerosol state variables after the 86 gas species,
+    and the GMD/GSD columns of its five modes after the reaction rates."""
+    from camp_b200.mechanism import reaction_summary
+
+    m = mod37_soa
+    assert reaction_summary(m)["by_type"][10] == 4
+    rep = m.aero_reps[0]
+    assert rep.first_state == 86 and len(rep.unique_names) == 99 == m.n_state_var - 86
+    cols = m.rate_columns()
+    assert [c[0] for c in cols[-10:]] == ["gmd", "gsd"] * 5
+    assert all(c[0] == "rxn" for c in cols[:-10])
 
 
 def test_mod37_gas_composition(mod37):
@@ -83,7 +100,7 @@ def test_mod37_gas_composition(mod37):
 
 
 @pytest.mark.skipif(not ref_available(), reason="reference build absent")
-@pytest.mark.parametrize("which", ["cb05", "mod37"])
+@pytest.mark.parametrize("which", ["cb05", "mod37", "mod37_soa"])
 def test_live_against_reference_build(request, which):
     """Fresh random states through the reference build and the oracle."""
     from camp_b200.cells import make_cells
@@ -97,9 +114,10 @@ def test_live_against_reference_build(request, which):
         ref.set_cell(c, cells.state[c], cells.env[c])
         ref.set_rates(c, cells.photo_rates[c])
         ref.update_env(c)
-        re = om.rxn_env(cells.env[c], _photo_dict(cells.photo_rates[c]))
-        assert np.array_equal(re, ref.rxn_env(c))
+        re = om.rxn_env_row(cells.env[c], cells.photo_rates[c])
+        assert np.array_equal(re[:ref.n_env], ref.rxn_env(c)[:ref.n_env])
         for h in (1e-3, 30.0):
+            ref.set_rates(c, cells.photo_rates[c])  # this cell's mode radii
             f1, p1, l1 = ref.deriv(c, h)
             f2, p2, l2 = om.deriv(cells.state[c], re, h)
             np.testing.assert_allclose(p2, p1, rtol=1e-12, atol=0)
