@@ -63,7 +63,8 @@ def _tight(mech, cells, t1):
 def _same_accuracy(mech, a, b, tight, rows):
     """Two BDF runs at rtol 1e-4 differ by their global errors, so each is
     measured against the tight solution and their per-cell errors are
-    compared as distributions (median and 90th percentile)."""
+    compared as distributions (median and 90th percentile): a's within 2x
+    (plus slack) of b's."""
     ea = _tol_units(mech, a, tight, rows)
     eb = _tol_units(mech, b, tight, rows)
     assert np.median(ea) <= 2.0 * np.median(eb) + 1.0, (np.median(ea), np.median(eb))
@@ -74,17 +75,25 @@ def _same_accuracy(mech, a, b, tight, rows):
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("which", ["cb05", "mod37"])
 def test_lane_kernel_matches_warp_kernel(request, which, precision):
+    """Same outcomes as the warp kernel, and the reference algorithm's
+    accuracy (the oracle at equal tolerances), both against the tight
+    solution.  The error distributions need a few dozen finishing cells: on
+    ~20 cells the median of either kernel moves by 2x with the sample."""
     from camp_b200.cells import make_cells
+    from oracle.oracle import OracleModel
 
     mech = request.getfixturevalue(which)
-    cells = make_cells(mech, 40, 23)
+    cells = make_cells(mech, 64, 23)
     _, xw, sw = _solve(mech, cells, precision, 0, 60.0, 1500)
     _, xl, sl = _solve(mech, cells, precision, 1, 60.0, 1500)
     assert np.mean(sw == sl) >= 0.9
+    _, ost, _, yo = OracleModel(mech).solve(cells.state.copy(), cells.env, cells.photo_rates,
+                                            0.0, 60.0, 1e-4, np.full(mech.n_state_var, 1e-8),
+                                            max_steps=1500, n_threads=os.cpu_count() or 1)
     tight, tst = _tight(mech, cells, 60.0)
-    ok = (sw == 0) & (sl == 0) & (tst == 0)
-    assert ok.sum() >= 16
-    _same_accuracy(mech, xl, xw, tight, ok)
+    ok = (sw == 0) & (sl == 0) & (ost == 0) & (tst == 0)
+    assert ok.sum() >= 32
+    _same_accuracy(mech, xl, yo, tight, ok)
 
 
 @pytest.fixture(scope="module")
