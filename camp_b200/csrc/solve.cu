@@ -364,14 +364,13 @@ __device__ __noinline__ void simpol_partials(const char* tb, const double* y, co
 __device__ __noinline__ int dev_f(const char* tb, const double* y, double h,
                                   const double* keff, double* rates, double* fscr,
                                   double* out, int lane, double* rp = nullptr,
-                                  double* rl = nullptr) {
+                                  double* rl = nullptr, bool neg_extra = false) {
   const Tab t = make_tab(tb);
   bool bad = false;
   #pragma unroll 1
   for (int i = lane; i < t.n; i += 32) bad |= y[i] < -kSmall;
   if (warp_any(bad)) return 1;
-  bool negrate = rates_of(t, y, keff, rates, lane);
-  if (t.n_simpol) negrate |= simpol_rates(tb, y, keff, rates, lane);
+  const bool negrate = rates_of(t, y, keff, rates, lane) || neg_extra;
   __syncwarp();
   const uint4* fg_unit = (const uint4*)t.fg_unit;
   const int u1 = t.fg_lane[lane + 1];
@@ -508,7 +507,6 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
       part[base + 2] = k * y0 * y1;
     }
   }
-  if (t.n_simpol) simpol_partials(tb, y, keff, part, lane);
   __syncwarp();
   const int s1 = t.jg_lane[lane + 1];
   #pragma unroll 1
@@ -545,6 +543,29 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
   }
   __syncwarp();
   return 0;
+}
+
+// f and J of a mechanism with SIMPOL instances: their pseudo-rates or
+// partials first (slots after the terms', which the mass-action passes do
+// not write, made visible to the gathers by their warp barrier), then the
+// usual evaluation.  Separate functions, so that the plain f and J keep
+// their register use.
+__device__ __noinline__ int dev_f_aero(const char* tb, const double* y, double h,
+                                       const double* keff, double* rates, double* fscr,
+                                       double* out, int lane, double* rp = nullptr,
+                                       double* rl = nullptr) {
+  const bool neg = simpol_rates(tb, y, keff, rates, lane);
+  return dev_f(tb, y, h, keff, rates, fscr, out, lane, rp, rl, neg);
+}
+template <typename JT>
+__device__ __noinline__ int dev_jac_aero(const char* tb, const double* y, double h,
+                                         const double* keff, double* part, JT* Jout, int lane,
+                                         double* jp = nullptr, double* jl = nullptr) {
+  simpol_partials(tb, y, keff, part, lane);
+  return dev_jac<JT>(tb, y, h, keff, part, Jout, lane, jp, jl);
+}
+__device__ __forceinline__ bool has_simpol(const char* tb) {
+  return reinterpret_cast<const BlobOff*>(tb)->n_simpol > 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -758,6 +779,7 @@ struct Cell {
   const char* tb;     // shared-memory tables
   const double* atol;
   int lu_mode;        // 0 = level schedule over the lanes, 1 = one lane
+  bool aero;          // the mechanism has SIMPOL instances
   int lane, n;
   double* zb;  // Nordsieck history: column j at zb + j*n
   double *ewt, *acor, *y, *ftemp, *tempv, *rates, *keff, *fscr;
@@ -783,7 +805,8 @@ struct Cell {
     return dsqrt(ddiv(warp_sum(s), (double)n));
   }
   __device__ int f(const double* yy, double* out) {
-    return dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
+    return aero ? dev_f_aero(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane)
+                : dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
   }
   __device__ bool set_ewt(const double* yy) {
     bool bad = false;
@@ -962,7 +985,9 @@ struct Cell {
       nje++;
       nstlj = nst;
       jcur = 1;
-      if (dev_jac<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane)) return 1;
+      if (aero ? dev_jac_aero<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane)
+               : dev_jac<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane))
+        return 1;
     }
     const bool ok = lu_mode ? dev_form_factor_seq<LT>(tb, J, gamma, LU, dinv, lane)
                             : dev_form_factor<LT>(tb, J, gamma, LU, dinv, lane);
@@ -1321,6 +1346,7 @@ template <typename LT>
 __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char* base,
                           int gwarp, int lane) {
   c.tb = tab;
+  c.aero = has_simpol(tab);
   c.atol = make_tab(tab).atol;
   c.lane = lane;
   c.n = a.off.n;
@@ -1454,13 +1480,21 @@ __global__ void eval_kernel(EvalArgs a) {
                a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, keff, lane);
   if (!a.do_jac) {
     double* out = (double*)(base + a.lay.ftemp);
-    dev_f(smem, y, a.h, keff, rates, fscr, out, lane, a.rp + (size_t)cell * t.n,
-          a.rl + (size_t)cell * t.n);
+    if (has_simpol(smem))
+      dev_f_aero(smem, y, a.h, keff, rates, fscr, out, lane, a.rp + (size_t)cell * t.n,
+                 a.rl + (size_t)cell * t.n);
+    else
+      dev_f(smem, y, a.h, keff, rates, fscr, out, lane, a.rp + (size_t)cell * t.n,
+            a.rl + (size_t)cell * t.n);
     #pragma unroll 1
     for (int i = lane; i < t.n; i += 32) a.f[(size_t)cell * t.n + i] = out[i];
   } else {
-    dev_jac<double>(smem, y, a.h, keff, rates, a.jv + (size_t)cell * t.n_jac, lane,
-                    a.jp + (size_t)cell * t.n_jac, a.jl + (size_t)cell * t.n_jac);
+    if (has_simpol(smem))
+      dev_jac_aero<double>(smem, y, a.h, keff, rates, a.jv + (size_t)cell * t.n_jac, lane,
+                           a.jp + (size_t)cell * t.n_jac, a.jl + (size_t)cell * t.n_jac);
+    else
+      dev_jac<double>(smem, y, a.h, keff, rates, a.jv + (size_t)cell * t.n_jac, lane,
+                      a.jp + (size_t)cell * t.n_jac, a.jl + (size_t)cell * t.n_jac);
   }
 }
 
@@ -1515,8 +1549,10 @@ __global__ void jac_check_kernel(CheckArgs c) {
   __syncwarp();
   compute_keff(m, st, a.env[2 * cell], a.env[2 * cell + 1],
                a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, keff, lane);
-  if (dev_f(smem, y, a.h, keff, rates, fscr, f0, lane, rp0, rl0) ||
-      dev_jac<double>(smem, y, a.h, keff, rates, J, lane)) {
+  const bool aero = has_simpol(smem);
+  if (dev_f_aero(smem, y, a.h, keff, rates, fscr, f0, lane, rp0, rl0) ||
+      (aero ? dev_jac_aero<double>(smem, y, a.h, keff, rates, J, lane)
+            : dev_jac<double>(smem, y, a.h, keff, rates, J, lane))) {
     if (lane == 0) {
       c.nfail[cell] = -1;
       c.worst[cell] = -1.0;
@@ -1539,10 +1575,10 @@ __global__ void jac_check_kernel(CheckArgs c) {
       const double dx = x * scale;
       if (lane == 0) y[j] = x + dx;
       __syncwarp();
-      int r = dev_f(smem, y, a.h, keff, rates, fscr, f1, lane);
+      int r = dev_f_aero(smem, y, a.h, keff, rates, fscr, f1, lane);
       if (lane == 0) y[j] = x + 0.5 * dx;
       __syncwarp();
-      r |= dev_f(smem, y, a.h, keff, rates, fscr, f2, lane);
+      r |= dev_f_aero(smem, y, a.h, keff, rates, fscr, f2, lane);
       if (lane == 0) y[j] = x;
       __syncwarp();
       if (r) continue;
