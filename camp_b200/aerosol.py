@@ -16,14 +16,16 @@ What is restated, from the reference's Fortran:
   ``phase_ids`` (``src/aero_rep_data.F90``) and ``num_jac_elem`` (``:964-996``)
   the instance ids and element counts;
 * ``rxn_SIMPOL_phase_transfer_t%initialize``
-  (``src/rxns/rxn_SIMPOL_phase_transfer.F90:220-470``) and the WET_DEPOSITION
+  (``src/rxns/rxn_SIMPOL_phase_transfer.F90:220-470``),
+  ``rxn_HL_phase_transfer_t%initialize``
+  (``src/rxns/rxn_HL_phase_transfer.F90:170-398``) and the WET_DEPOSITION
   packer over every instance of a phase
   (``src/rxns/rxn_wet_deposition.F90:172-254``).
 
 Aerosol-representation ids (``AERO_REP_ID_``) are given 1, 2, ... as a host
 does through ``set_id`` before it creates GMD/GSD update data.  Other aerosol
-types (single particle, HL and SIMPOL's aqueous relatives, sub-models) are
-not packed here.
+types (single particle, aqueous equilibrium, condensed-phase reactions,
+sub-models) are not packed here.
 """
 from __future__ import annotations
 
@@ -39,6 +41,7 @@ from .mechanism import (CHEM_SPEC_ACTIVITY_COEFF, CHEM_SPEC_CONSTANT, CHEM_SPEC_
                         _SpeciesDB, assign_rate_ids, pack_reaction)
 
 AERO_REP_MODAL_BINNED_MASS = 2  # src/aero_rep_solver.c:20
+RXN_HL_PHASE_TRANSFER = 6       # src/rxn_solver.c:24
 RXN_SIMPOL_PHASE_TRANSFER = 10  # src/rxn_solver.c:26
 BINNED, MODAL = 1, 2            # src/aero_reps/aero_rep_modal_binned_mass.c:25-26
 UNIV_GAS_CONST = 8.314472       # src/constants.F90
@@ -304,6 +307,82 @@ def pack_simpol(rxn: dict, db: _SpeciesDB, gas_index: dict[str, int], reps: list
     return PackedRxn(RXN_SIMPOL_PHASE_TRANSFER, ints, floats, 4, str(rxn.get("rxn id", "")))
 
 
+def pack_hl(rxn: dict, db: _SpeciesDB, gas_index: dict[str, int], reps: list[AeroRep],
+            phases: list[AeroPhase]) -> PackedRxn:
+    """HL_PHASE_TRANSFER (src/rxns/rxn_HL_phase_transfer.F90:170-398).
+
+    ints: ``[NUM_AERO_PHASE_, GAS_SPEC_, DERIV_ID_(0..n), JAC_ID_(0..5n),
+    PHASE_INT_LOC_(n), PHASE_REAL_LOC_(n)]`` then per instance ``[AERO_SPEC_,
+    AERO_WATER_, AERO_PHASE_ID_, AERO_REP_ID_, NUM_AERO_PHASE_JAC_ELEM_,
+    PHASE_JAC_ID_(2 x elements)]``; floats: ``[DELTA_H_, DELTA_S_,
+    DIFF_COEFF_, PRE_C_AVG_, A_, C_, CONV_, MW_]`` then per instance
+    ``[SMALL_WATER_CONC_, EFF_RAD_JAC_ELEM_(e), NUM_CONC_JAC_ELEM_(e)]``."""
+    gas = rxn["gas-phase species"]
+    phase = rxn["aerosol phase"]
+    aero = rxn["aerosol-phase species"]
+    water = rxn.get("aerosol-phase water")
+    if water is None:
+        raise ValueError(f"Missing aerosol-phase water for HL partitioning of {gas} to {aero}")
+    inst = []   # (rep index, species unique name, water unique name, phase id)
+    for ri, rep in enumerate(reps):
+        names = rep.names(phases, phase, aero)
+        if not names:
+            continue
+        wnames = rep.names(phases, phase, water)
+        if len(wnames) != len(names):
+            raise ValueError(f"Missing species {aero} or {water} in phase {phase}")
+        pids = rep.phase_ids(phases, phase)
+        for k, nm in enumerate(names):
+            inst.append((ri, nm, wnames[k], pids[k]))
+    if not inst:
+        raise ValueError(f"No aerosol phase instances for HL partitioning of {aero}")
+    n = len(inst)
+    n_elem = [reps[ri].num_jac_elem(phases, pid) for ri, _, _, pid in inst]
+    E = sum(n_elem)
+    ints = np.zeros(4 + 13 * n + 2 * E, np.int32)
+    floats = np.zeros(8 + n + 2 * E, np.float64)
+    ints[0] = n
+    if gas not in gas_index:
+        raise KeyError(f"Missing gas-phase species {gas}")
+    ints[1] = gas_index[gas]
+    loc_i, loc_f = 8 * n + 5, 9  # PHASE_INT_LOC_(1), PHASE_REAL_LOC_(1), 1-based
+    for x, (ri, nm, wn, pid) in enumerate(inst):
+        rep = reps[ri]
+        ints[4 + 6 * n + x] = loc_i
+        ints[4 + 7 * n + x] = loc_f
+        li = loc_i - 1
+        ints[li] = rep.state_id(nm)        # AERO_SPEC_
+        ints[li + 1] = rep.state_id(wn)    # AERO_WATER_
+        ints[li + 2] = pid                 # AERO_PHASE_ID_
+        ints[li + 3] = ri + 1              # AERO_REP_ID_
+        ints[li + 4] = n_elem[x]           # NUM_AERO_PHASE_JAC_ELEM_
+        loc_i += 5 + 2 * n_elem[x]
+        loc_f += 1 + 2 * n_elem[x]
+    assert loc_i - 1 == ints.size and loc_f - 1 == floats.size
+    gp = db.props[gas]
+    ap = db.props[aero]
+    mw = float(ap["molecular weight [kg mol-1]"])
+    for key in ("HLC(298K) [M Pa-1]", "HLC exp factor [K]", "diffusion coeff [m2 s-1]",
+                "molecular weight [kg mol-1]"):
+        if key not in gp:
+            raise KeyError(f"Missing '{key}' for gas-phase species {gas} of HL partitioning")
+    if "N star" in gp:
+        ns = float(gp["N star"])
+        dh = (-10.0 * (ns - 1.0) + 7.53 * (ns ** (2.0 / 3.0) - 1.0) - 1.0) * 4184.0
+        ds = (-32.0 * (ns - 1.0) + 9.21 * (ns ** (2.0 / 3.0) - 1.0) - 1.3) * 4.184
+    else:
+        dh = ds = 0.0
+    floats[0], floats[1] = dh, ds
+    floats[2] = float(gp["diffusion coeff [m2 s-1]"])
+    # sqrt(8.0*R/(pi*MW)): the Fortran 8.0 is default-kind, R and pi are dp
+    floats[3] = math.sqrt(8.0 * UNIV_GAS_CONST / (PI * float(gp["molecular weight [kg mol-1]"])))
+    floats[4] = float(gp["HLC(298K) [M Pa-1]"])
+    floats[5] = float(gp["HLC exp factor [K]"])
+    floats[6] = UNIV_GAS_CONST / mw * 1.0e6
+    floats[7] = mw
+    return PackedRxn(RXN_HL_PHASE_TRANSFER, ints, floats, 4, str(rxn.get("rxn id", "")))
+
+
 def pack_wet_deposition_phase(rxn: dict, reps: list[AeroRep],
                               phases: list[AeroPhase]) -> PackedRxn:
     from .mechanism import pack_wet_deposition
@@ -375,6 +454,8 @@ def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mec
         for r in rx:
             if r["type"] == "SIMPOL_PHASE_TRANSFER":
                 rxns.append(pack_simpol(r, db, gas_index, reps, phases))
+            elif r["type"] == "HL_PHASE_TRANSFER":
+                rxns.append(pack_hl(r, db, gas_index, reps, phases))
             elif r["type"] == "WET_DEPOSITION":
                 rxns.append(pack_wet_deposition_phase(r, reps, phases))
             else:

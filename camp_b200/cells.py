@@ -80,6 +80,23 @@ def photolysis_columns(mech: Mechanism) -> np.ndarray:
                        for c in mech.rate_columns()], dtype=bool)
 
 
+def hl_water_indices(mech: Mechanism) -> set[int]:
+    """State indices of the aerosol-phase water that HL partitioning divides
+    by (AERO_WATER_ of every instance,
+    src/rxns/rxn_HL_phase_transfer.c:49-57)."""
+    from .aerosol import RXN_HL_PHASE_TRANSFER
+
+    out = set()
+    for r in mech.rxns:
+        if r.rxn_type != RXN_HL_PHASE_TRANSFER:
+            continue
+        n = int(r.ints[0])
+        for x in range(n):
+            iloc = int(r.ints[4 + 6 * n + x]) - 1
+            out.add(int(r.ints[iloc + 1]) - 1)
+    return out
+
+
 def _aerosol_cells(mech: Mechanism, rng, state: np.ndarray, photo: np.ndarray) -> None:
     """Per-cell aerosol state and mode GMD/GSD columns (module docstring)."""
     from .aerosol import MODAL
@@ -87,10 +104,44 @@ def _aerosol_cells(mech: Mechanism, rng, state: np.ndarray, photo: np.ndarray) -
     n_cells = state.shape[0]
     cols = mech.rate_columns()
     col_of = {c: j for j, c in enumerate(cols)}
+    water = hl_water_indices(mech)
     for ri, rep in enumerate(mech.aero_reps):
         inst = 0
         for si, sec in enumerate(rep.sections):
             nb = sec.n_bins
+
+            def first_of(j: int) -> int:  # first state index of instance j
+                return rep.first_state + sum(len(mech.aero_phases[q].species)
+                                             for q in rep.instances[:j])
+
+            cloud = any(first_of(j) + k in water
+                        for j in range(inst, inst + len(sec.phases) * nb)
+                        for k in range(len(mech.aero_phases[rep.instances[j]].species)))
+            if cloud:
+                # liquid water around the representation's own mode size
+                if sec.kind == MODAL:
+                    gmd = sec.gmd * np.exp(rng.uniform(np.log(0.5), np.log(2.0), n_cells))
+                    photo[:, col_of[("gmd", ri, si)]] = gmd
+                    photo[:, col_of[("gsd", ri, si)]] = np.full(n_cells, sec.gsd)
+                lwc = np.exp(rng.uniform(np.log(1e-5), np.log(1e-3), (n_cells, nb)))
+                for pi in sec.phases:
+                    ph = mech.aero_phases[pi]
+                    w = rng.uniform(0.0, 1.0, (n_cells, nb, len(ph.species)))
+                    for b in range(nb):
+                        first = first_of(inst)
+                        dis = [k for k, t in enumerate(ph.types)
+                               if t in (1, 2, 3) and first + k not in water]
+                        wsum = w[:, b, dis].sum(axis=1) if dis else np.ones(n_cells)
+                        share = lwc[:, b] / len(sec.phases)
+                        for k, t in enumerate(ph.types):
+                            if first + k in water:
+                                state[:, first + k] = share
+                            elif t in (1, 2, 3):
+                                state[:, first + k] = share * 1.0e-3 * w[:, b, k] / wsum
+                            else:
+                                state[:, first + k] = 1.0
+                        inst += 1
+                continue
             if sec.kind == MODAL:
                 gmd = np.exp(rng.uniform(np.log(20e-9), np.log(500e-9), n_cells))
                 gsd = np.full(n_cells, sec.gsd)

@@ -191,7 +191,9 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     const SimpolInst& si = t.simpol[k];
     const int first = (int)si_elem.size();
     int nd = 0;
-    for (size_t j = 0; j < si.elem.size(); ++j) {
+    // HL instances have no element partials (see SimpolInst)
+    const size_t ne = si.type == RXN_SIMPOL_PHASE_TRANSFER ? si.elem.size() : 0;
+    for (size_t j = 0; j < ne; ++j) {
       const int d = std::lower_bound(t.dep_state.begin(), t.dep_state.end(), si.elem[j]) -
                     t.dep_state.begin();
       if (d >= n || t.dep_state[d] != si.elem[j]) continue;  // not a dependent variable
@@ -375,7 +377,7 @@ namespace campb {
 bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
                      std::vector<uint8_t>* blob, LaneOff* off, std::string* err) {
   if (t.n_simpol > 0) {
-    *err = "the lane-per-cell kernel does not evaluate SIMPOL phase transfer";
+    *err = "the lane-per-cell kernel does not evaluate SIMPOL or HL phase transfer";
     return false;
   }
   const int n = t.n;

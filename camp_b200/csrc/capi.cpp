@@ -855,10 +855,30 @@ int camp_b200_eval_jac(void* solver_data, const double* state, const double* env
   Solver* s = S(solver_data);
   if (!s->ready || n_cells <= 0 || n_cells > s->n_cells) return -1;
   std::string err;
+  // the device evaluates the live entries; the output has every solver
+  // Jacobian entry, the others (HL's element partials) being zero
+  const campb::Model& m = *s->model;
+  const std::vector<int>& map = m.device_to_solver();
+  const size_t nd = map.size(), ns = m.solver_rowid().size();
+  const bool same = nd == ns;
+  std::vector<double> dp, dl;
+  if (!same) {
+    dp.resize((size_t)n_cells * nd);
+    dl.resize((size_t)n_cells * nd);
+  }
   if (!s->engine->eval_jac(state, env, s->n_photo ? s->photo.data() : nullptr, n_cells, h,
-                           j_prod, j_loss, &err)) {
+                           same ? j_prod : dp.data(), same ? j_loss : dl.data(), &err)) {
     set_error(err);
     return -1;
+  }
+  if (!same) {
+    std::fill(j_prod, j_prod + (size_t)n_cells * ns, 0.0);
+    std::fill(j_loss, j_loss + (size_t)n_cells * ns, 0.0);
+    for (int c = 0; c < n_cells; ++c)
+      for (size_t e = 0; e < nd; ++e) {
+        j_prod[(size_t)c * ns + map[e]] = dp[(size_t)c * nd + e];
+        j_loss[(size_t)c * ns + map[e]] = dl[(size_t)c * nd + e];
+      }
   }
   return 0;
 }

@@ -21,6 +21,7 @@ bool type_layout(int type, int* n_int_prop, int* n_float_prop) {
     case RXN_EMISSION: *n_int_prop = 3; *n_float_prop = 1; return true;
     case RXN_WET_DEPOSITION: *n_int_prop = 2; *n_float_prop = 1; return true;
     case RXN_SIMPOL_PHASE_TRANSFER: *n_int_prop = 2; *n_float_prop = 10; return true;
+    case RXN_HL_PHASE_TRANSFER: *n_int_prop = 2; *n_float_prop = 8; return true;
     default: return false;
   }
 }
@@ -86,7 +87,8 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
   if (!type_layout(type, &r.n_int_prop, &r.n_float_prop))
     return fail("reaction type " + std::to_string(type) +
                 " is not supported (ARRHENIUS, TROE, CMAQ_H2O2, CMAQ_OH_HNO3, PHOTOLYSIS, "
-                "FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION and SIMPOL_PHASE_TRANSFER only)");
+                "FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION, SIMPOL_PHASE_TRANSFER and "
+                "HL_PHASE_TRANSFER only)");
   const std::string malformed = "malformed packed data for reaction " + std::to_string(idx);
   if (n_int < r.n_int_prop || n_float < r.n_float_prop) return fail(malformed);
   const int o = r.int_off;  // rxn_int_ position of ints[0]
@@ -123,9 +125,11 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
       r.rid_at = o;
       break;
     }
-    case RXN_SIMPOL_PHASE_TRANSFER: {  // src/rxns/rxn_SIMPOL_phase_transfer.c:37-78
-      // no mass-action terms: its instances are resolved against the
-      // aerosol representation at solver_initialize
+    case RXN_SIMPOL_PHASE_TRANSFER:  // src/rxns/rxn_SIMPOL_phase_transfer.c:37-78
+    case RXN_HL_PHASE_TRANSFER: {    // src/rxns/rxn_HL_phase_transfer.c:37-63
+      // no mass-action terms: the instances are resolved against the
+      // aerosol representation at solver_initialize (both layouts hold
+      // 4 + 13 n ints before the element lists)
       const int na = ints[0];
       if (na < 1 || n_int < 4 + 13 * na) return fail(malformed);
       if (ints[1] < 1 || ints[1] > n_state_)
@@ -242,109 +246,169 @@ struct SimpolView {
   int nelem(int x) const { return I[iloc(x)]; }
   int& phase_jac(int x, int set, int e) const { return I[iloc(x) + 1 + set * nelem(x) + e]; }
 };
+// views of the packed HL data, 0-based within the reaction's ints
+// (src/rxns/rxn_HL_phase_transfer.c:37-63)
+struct HlView {
+  int* I;
+  int n;
+  int gas() const { return I[1] - 1; }
+  int& deriv(int x) const { return I[2 + x]; }
+  int& jac(int x) const { return I[3 + n + x]; }
+  int iloc(int x) const { return I[4 + 6 * n + x] - 1; }
+  int aero(int x) const { return I[iloc(x)] - 1; }
+  int water(int x) const { return I[iloc(x) + 1] - 1; }
+  int phase(int x) const { return I[iloc(x) + 2] - 1; }
+  int rep(int x) const { return I[iloc(x) + 3] - 1; }
+  int nelem(int x) const { return I[iloc(x) + 4]; }
+  int& phase_jac(int x, int set, int e) const { return I[iloc(x) + 5 + set * nelem(x) + e]; }
+};
 }  // namespace
 
-// The instances of every SIMPOL reaction against its representation: the
-// mode or bin of the instance found the way the representation's C
-// functions walk it (sections, then bins, then the phases of a bin,
-// src/aero_reps/aero_rep_modal_binned_mass.c:300-330), the element list,
-// the element counts written into the representation and the state indices
-// written into PHASE_JAC_ID_ as get_used_jac_elem does
-// (src/rxns/rxn_SIMPOL_phase_transfer.c:86-151).
+// Locates phase instance `phase` of representation si->rep the way the
+// representation's C functions walk it (sections, then bins, then the phases
+// of a bin, src/aero_reps/aero_rep_modal_binned_mass.c:300-330) and fills
+// the section, bin, mode columns and element list of si; the element counts
+// are written into the representation as its get_used_jac_elem does
+// (:86-125).
+bool Model::resolve_instance(SimpolInst* si, int phase, int ri, std::string* err) {
+  const std::string what = (si->type == RXN_HL_PHASE_TRANSFER ? "HL reaction " : "SIMPOL reaction ") +
+                           std::to_string(ri);
+  if (si->rep < 0 || si->rep >= (int)arep_int_.size()) {
+    *err = what + " names a missing aerosol representation";
+    return false;
+  }
+  std::vector<int>& R = arep_int_[si->rep];
+  const std::vector<double>& RF = arep_flt_[si->rep];
+  const int ns = R[0];
+  int idx = phase, found = 0;
+  for (int s = 0; s < ns && !found; ++s) {
+    const int li = R[4 + s] - 1;
+    for (int b = 0; b < R[li + 1] && !found; ++b) {
+      if (idx < R[li + 2]) {
+        si->section = s;
+        si->bin = b;
+        si->phase = idx;
+        found = 1;
+      } else {
+        idx -= R[li + 2];
+      }
+    }
+  }
+  if (!found) {
+    *err = what + " names a missing phase instance";
+    return false;
+  }
+  const int li = R[4 + si->section] - 1, lf = R[4 + ns + si->section] - 1;
+  const int nb = R[li + 1], np = R[li + 2];
+  si->kind = R[li];
+  si->n_phases = np;
+  si->bin_dp = RF[lf + 3 * si->bin];
+  if (si->kind == SECTION_MODAL) {
+    int k = 0;
+    for (; k < (int)modes_.size(); ++k)
+      if (modes_[k].first == si->rep && modes_[k].second == si->section) break;
+    si->gmd_col = n_host_rate_ + 2 * k;
+    si->gsd_col = si->gmd_col + 1;
+  }
+  for (int y = 0; y < np; ++y) {
+    const int st0 = R[li + 3 + si->bin * np + y] - 1;
+    const int ph = R[li + 3 + nb * np + si->bin * np + y] - 1;
+    if (ph < 0 || ph >= (int)aph_int_.size()) {
+      *err = "aerosol representation names a missing phase";
+      return false;
+    }
+    const std::vector<int>& P = aph_int_[ph];
+    const std::vector<double>& PF = aph_flt_[ph];
+    int cnt = 0;
+    for (int i = 0; i < P[0]; ++i) {
+      const int t = P[1 + i];
+      if (t != VAR_VARIABLE && t != VAR_CONSTANT && t != 3) continue;
+      si->elem.push_back(st0 + i);
+      si->inv_rho.push_back(1.0 / PF[P[0] + i]);
+      si->inv_mw.push_back(y == si->phase ? 1.0 / PF[i] : 0.0);
+      si->in_phase.push_back(y == si->phase ? 1 : 0);
+      ++cnt;
+    }
+    R[li + 3 + 2 * nb * np + si->bin * np + y] = cnt;  // PHASE_NUM_JAC_ELEM_
+  }
+  for (int sp : {si->gas, si->aero})
+    if (sp < 0 || sp >= n_state_ || var_type_[sp] != VAR_VARIABLE) {
+      *err = what + ": the gas and aerosol species must be variable state variables";
+      return false;
+    }
+  return true;
+}
+
+// The instances of every SIMPOL and HL reaction against their
+// representation, in mechanism order, with the state indices of their
+// elements written into PHASE_JAC_ID_ as get_used_jac_elem does
+// (src/rxns/rxn_SIMPOL_phase_transfer.c:86-151,
+// src/rxns/rxn_HL_phase_transfer.c:72-138).
 bool Model::resolve_simpol(std::string* err) {
   simpol_.clear();
   for (size_t ri = 0; ri < rxns_.size(); ++ri) {
     const Rxn& r = rxns_[ri];
-    if (r.type != RXN_SIMPOL_PHASE_TRANSFER) continue;
-    SimpolView v{&rxn_int_[r.int_off], rxn_int_[r.int_off]};
-    for (int x = 0; x < v.n; ++x) {
-      SimpolInst si;
-      si.rxn = (int)ri;
-      si.x = x;
-      for (int q = 0; q < 10; ++q) si.prm[q] = rxn_float_[r.float_off + q];
-      si.gas = v.gas();
-      si.aero = v.aero(x);
-      si.act = v.act(x);
-      si.rep = v.rep(x);
-      if (si.rep < 0 || si.rep >= (int)arep_int_.size()) {
-        *err = "SIMPOL reaction " + std::to_string(ri) + " names a missing aerosol representation";
-        return false;
-      }
-      std::vector<int>& R = arep_int_[si.rep];
-      const std::vector<double>& RF = arep_flt_[si.rep];
-      const int ns = R[0];
-      int idx = v.phase(x), found = 0;
-      for (int s = 0; s < ns && !found; ++s) {
-        const int li = R[4 + s] - 1;
-        for (int b = 0; b < R[li + 1] && !found; ++b) {
-          if (idx < R[li + 2]) {
-            si.section = s;
-            si.bin = b;
-            si.phase = idx;
-            found = 1;
-          } else {
-            idx -= R[li + 2];
-          }
-        }
-      }
-      if (!found) {
-        *err = "SIMPOL reaction " + std::to_string(ri) + " names a missing phase instance";
-        return false;
-      }
-      const int li = R[4 + si.section] - 1, lf = R[4 + ns + si.section] - 1;
-      const int nb = R[li + 1], np = R[li + 2];
-      si.kind = R[li];
-      si.n_phases = np;
-      si.bin_dp = RF[lf + 3 * si.bin];
-      if (si.kind == SECTION_MODAL) {
-        int k = 0;
-        for (; k < (int)modes_.size(); ++k)
-          if (modes_[k].first == si.rep && modes_[k].second == si.section) break;
-        si.gmd_col = n_host_rate_ + 2 * k;
-        si.gsd_col = si.gmd_col + 1;
-      }
-      for (int y = 0; y < np; ++y) {
-        const int st0 = R[li + 3 + si.bin * np + y] - 1;
-        const int ph = R[li + 3 + nb * np + si.bin * np + y] - 1;
-        if (ph < 0 || ph >= (int)aph_int_.size()) {
-          *err = "aerosol representation names a missing phase";
+    if (r.type == RXN_SIMPOL_PHASE_TRANSFER) {
+      SimpolView v{&rxn_int_[r.int_off], rxn_int_[r.int_off]};
+      for (int x = 0; x < v.n; ++x) {
+        SimpolInst si;
+        si.type = RXN_SIMPOL_PHASE_TRANSFER;
+        si.rxn = (int)ri;
+        si.x = x;
+        for (int q = 0; q < 10; ++q) si.prm[q] = rxn_float_[r.float_off + q];
+        si.gas = v.gas();
+        si.aero = v.aero(x);
+        si.act = v.act(x);
+        si.rep = v.rep(x);
+        if (!resolve_instance(&si, v.phase(x), (int)ri, err)) return false;
+        if ((int)si.elem.size() > v.nelem(x)) {
+          *err = "SIMPOL reaction " + std::to_string(ri) + ": more Jacobian elements than packed";
           return false;
         }
-        const std::vector<int>& P = aph_int_[ph];
-        const std::vector<double>& PF = aph_flt_[ph];
-        int cnt = 0;
-        for (int i = 0; i < P[0]; ++i) {
-          const int t = P[1 + i];
-          if (t != VAR_VARIABLE && t != VAR_CONSTANT && t != 3) continue;
-          si.elem.push_back(st0 + i);
-          si.inv_rho.push_back(1.0 / PF[P[0] + i]);
-          si.inv_mw.push_back(y == si.phase ? 1.0 / PF[i] : 0.0);
-          si.in_phase.push_back(y == si.phase ? 1 : 0);
-          ++cnt;
+        for (int e = 0; e < v.nelem(x); ++e) {
+          const int val = e < (int)si.elem.size() ? si.elem[e] : -1;
+          v.phase_jac(x, 0, e) = val;
+          v.phase_jac(x, 1, e) = val;
         }
-        R[li + 3 + 2 * nb * np + si.bin * np + y] = cnt;  // PHASE_NUM_JAC_ELEM_
-      }
-      if ((int)si.elem.size() > v.nelem(x)) {
-        *err = "SIMPOL reaction " + std::to_string(ri) + ": more Jacobian elements than packed";
-        return false;
-      }
-      for (int e = 0; e < v.nelem(x); ++e) {
-        const int val = e < (int)si.elem.size() ? si.elem[e] : -1;
-        v.phase_jac(x, 0, e) = val;
-        v.phase_jac(x, 1, e) = val;
-      }
-      for (int sp : {si.gas, si.aero})
-        if (sp < 0 || sp >= n_state_ || var_type_[sp] != VAR_VARIABLE) {
+        if (si.act >= 0 && (si.act >= n_state_ || var_type_[si.act] == VAR_VARIABLE)) {
           *err = "SIMPOL reaction " + std::to_string(ri) +
-                 ": the gas and aerosol species must be variable state variables";
+                 ": a variable activity coefficient is not supported";
           return false;
         }
-      if (si.act >= 0 && (si.act >= n_state_ || var_type_[si.act] == VAR_VARIABLE)) {
-        *err = "SIMPOL reaction " + std::to_string(ri) +
-               ": a variable activity coefficient is not supported";
-        return false;
+        simpol_.push_back(si);
       }
-      simpol_.push_back(si);
+    } else if (r.type == RXN_HL_PHASE_TRANSFER) {
+      HlView v{&rxn_int_[r.int_off], rxn_int_[r.int_off]};
+      for (int x = 0; x < v.n; ++x) {
+        SimpolInst si;
+        si.type = RXN_HL_PHASE_TRANSFER;
+        si.rxn = (int)ri;
+        si.x = x;
+        for (int q = 0; q < 8; ++q) si.prm[q] = rxn_float_[r.float_off + q];
+        si.gas = v.gas();
+        si.aero = v.aero(x);
+        si.water = v.water(x);
+        si.rep = v.rep(x);
+        if (!resolve_instance(&si, v.phase(x), (int)ri, err)) return false;
+        if ((int)si.elem.size() > v.nelem(x)) {
+          *err = "HL reaction " + std::to_string(ri) + ": more Jacobian elements than packed";
+          return false;
+        }
+        for (int e = 0; e < v.nelem(x); ++e) {
+          const int val = e < (int)si.elem.size() ? si.elem[e] : -1;
+          v.phase_jac(x, 0, e) = val;
+          v.phase_jac(x, 1, e) = val;
+        }
+        // the water divides the evaporation rate; a water that the solver
+        // integrates would need its own partials (:365-373), which this
+        // build does not evaluate
+        if (si.water < 0 || si.water >= n_state_ || var_type_[si.water] == VAR_VARIABLE) {
+          *err = "HL reaction " + std::to_string(ri) +
+                 ": the aerosol-phase water must be a constant (not variable) state variable";
+          return false;
+        }
+        simpol_.push_back(si);
+      }
     }
   }
   return true;
@@ -361,32 +425,48 @@ int Model::rxn_elem_id(int dep, int ind) const {
 // 1445-1460 and the get_used_jac_elem functions, e.g.
 // src/rxns/rxn_arrhenius.c:44-60, rxn_first_order_loss.c:37-46,
 // rxn_wet_deposition.c:38-49; EMISSION registers none).
+//
+// A second registry keeps the live elements only: all of the above except
+// HL's elements, whose partials are zero for the modal/binned
+// representation.  The reference's solver Jacobian keeps them as stored
+// zeros; the LU built here leaves them out.
 void Model::build_rxn_jacobian() {
-  Registry reg(n_state_);
-  for (int i = 0; i < n_state_; ++i) reg.add(i, i);
+  Registry reg(n_state_), live(n_state_);
+  auto add = [&](int dep, int ind, bool is_live) {
+    reg.add(dep, ind);
+    if (is_live) live.add(dep, ind);
+  };
+  for (int i = 0; i < n_state_; ++i) add(i, i, true);
   for (const Rxn& r : rxns_)
     for (const Term& t : r.terms)
       for (int ind : t.react) {
-        for (int d : t.react) reg.add(d, ind);
-        for (int d : t.prod) reg.add(d, ind);
+        for (int d : t.react) add(d, ind, true);
+        for (int d : t.prod) add(d, ind, true);
       }
   // SIMPOL (src/rxns/rxn_SIMPOL_phase_transfer.c:86-151): gas and aerosol
-  // species against each other, the activity coefficient and the elements
+  // species against each other, the activity coefficient and the elements;
+  // HL (src/rxns/rxn_HL_phase_transfer.c:72-138): the same with the
+  // aerosol-phase water in place of the activity coefficient
   for (const SimpolInst& si : simpol_) {
-    reg.add(si.gas, si.gas);
-    reg.add(si.aero, si.gas);
-    reg.add(si.gas, si.aero);
-    reg.add(si.aero, si.aero);
-    if (si.act > 0) {
-      reg.add(si.gas, si.act);
-      reg.add(si.aero, si.act);
+    const bool hl = si.type == RXN_HL_PHASE_TRANSFER;
+    add(si.gas, si.gas, true);
+    add(si.aero, si.gas, true);
+    add(si.gas, si.aero, true);
+    add(si.aero, si.aero, true);
+    if (hl) {
+      add(si.gas, si.water, true);
+      add(si.aero, si.water, true);
+    } else if (si.act > 0) {
+      add(si.gas, si.act, true);
+      add(si.aero, si.act, true);
     }
     for (int e : si.elem) {
-      reg.add(si.gas, e);
-      reg.add(si.aero, e);
+      add(si.gas, e, !hl);
+      add(si.aero, e, !hl);
     }
   }
   reg.to_csc(&rj_colptr_, &rj_rowid_);
+  live.to_csc(&rl_colptr_, &rl_rowid_);
 }
 
 // DERIV_ID and JAC_ID written back into the packed ints, as rxn_update_ids
@@ -434,27 +514,65 @@ void Model::update_ids() {
       }
     }
   }
+  // HL (src/rxns/rxn_HL_phase_transfer.c:149-186; the small water
+  // concentration it also sets, :188-193, is never read)
+  for (const Rxn& r : rxns_) {
+    if (r.type != RXN_HL_PHASE_TRANSFER) continue;
+    HlView v{&rxn_int_[r.int_off], rxn_int_[r.int_off]};
+    const int g = v.gas();
+    v.deriv(0) = deriv_ids_[g];
+    for (int x = 0; x < v.n; ++x) v.deriv(x + 1) = deriv_ids_[v.aero(x)];
+    int ij = 0;
+    v.jac(ij++) = rxn_elem_id(g, g);
+    for (int x = 0; x < v.n; ++x) {
+      const int a = v.aero(x), w = v.water(x);
+      v.jac(ij++) = rxn_elem_id(a, g);
+      v.jac(ij++) = rxn_elem_id(g, a);
+      v.jac(ij++) = rxn_elem_id(a, a);
+      v.jac(ij++) = rxn_elem_id(g, w);
+      v.jac(ij++) = rxn_elem_id(a, w);
+      for (int e = 0; e < v.nelem(x); ++e) {
+        if (v.phase_jac(x, 0, e) > 0) v.phase_jac(x, 0, e) = rxn_elem_id(g, v.phase_jac(x, 0, e));
+        if (v.phase_jac(x, 1, e) > 0) v.phase_jac(x, 1, e) = rxn_elem_id(a, v.phase_jac(x, 1, e));
+      }
+    }
+  }
 }
 
 // Solver Jacobian: the variable x variable entries of the reaction Jacobian
 // (src/camp_solver.c:1559-1633; a gas-phase model has no sub-model
 // parameters, so every map entry has param_id 0).
+//
+// The same over the live reaction elements gives the device's Jacobian, with
+// the solver entry of each of its entries.
 void Model::build_solver_jacobian() {
-  Registry reg(n_state_);
-  for (int ind = 0; ind < n_state_; ++ind)
-    for (int dep = 0; dep < n_state_; ++dep) {
-      if (var_type_[dep] != VAR_VARIABLE || var_type_[ind] != VAR_VARIABLE) continue;
-      if (rxn_elem_id(dep, ind) == -1) continue;
-      reg.add(dep, ind);
+  auto build = [&](const std::vector<int>& rcp, const std::vector<int>& rri,
+                   std::vector<int>* colptr, std::vector<int>* rowid) {
+    Registry reg(n_state_);
+    for (int ind = 0; ind < n_state_; ++ind) {
+      if (var_type_[ind] != VAR_VARIABLE) continue;
+      for (int e = rcp[ind]; e < rcp[ind + 1]; ++e)
+        if (var_type_[rri[e]] == VAR_VARIABLE) reg.add(rri[e], ind);
     }
-  std::vector<int> cp, ri;
-  reg.to_csc(&cp, &ri);
-  sj_colptr_.assign(n_dep_ + 1, 0);
-  for (int c = 0; c < n_state_; ++c)
-    if (deriv_ids_[c] >= 0) sj_colptr_[deriv_ids_[c]] = cp[c];
-  sj_colptr_[n_dep_] = (int)ri.size();
-  sj_rowid_.resize(ri.size());
-  for (size_t e = 0; e < ri.size(); ++e) sj_rowid_[e] = deriv_ids_[ri[e]];
+    std::vector<int> cp, ri;
+    reg.to_csc(&cp, &ri);
+    colptr->assign(n_dep_ + 1, 0);
+    for (int c = 0; c < n_state_; ++c)
+      if (deriv_ids_[c] >= 0) (*colptr)[deriv_ids_[c]] = cp[c];
+    (*colptr)[n_dep_] = (int)ri.size();
+    rowid->resize(ri.size());
+    for (size_t e = 0; e < ri.size(); ++e) (*rowid)[e] = deriv_ids_[ri[e]];
+  };
+  build(rj_colptr_, rj_rowid_, &sj_colptr_, &sj_rowid_);
+  build(rl_colptr_, rl_rowid_, &dj_colptr_, &dj_rowid_);
+  dj_to_sj_.assign(dj_rowid_.size(), -1);
+  for (int c = 0; c < n_dep_; ++c) {
+    int q = sj_colptr_[c];
+    for (int e = dj_colptr_[c]; e < dj_colptr_[c + 1]; ++e) {
+      while (sj_rowid_[q] != dj_rowid_[e]) ++q;  // both columns sorted, live a subset
+      dj_to_sj_[e] = q;
+    }
+  }
 }
 
 // Fixed elimination order for the per-cell LU of I - gamma*J: diagonal
@@ -470,7 +588,7 @@ void Model::build_lu() {
   Tables& t = tab_;
   std::vector<std::vector<char>> P(n, std::vector<char>(n, 0));
   for (int c = 0; c < n; ++c)
-    for (int e = sj_colptr_[c]; e < sj_colptr_[c + 1]; ++e) P[sj_rowid_[e]][c] = 1;
+    for (int e = dj_colptr_[c]; e < dj_colptr_[c + 1]; ++e) P[dj_rowid_[e]][c] = 1;
   for (int i = 0; i < n; ++i) P[i][i] = 1;
   std::vector<char> done(n, 0);
   std::vector<int> rc(n), cc(n);
@@ -772,7 +890,7 @@ void Model::build_tables() {
   t.n = n_dep_;
   t.n_state = n_state_;
   t.n_rxn = n_terms_;
-  t.n_jac = (int)sj_rowid_.size();
+  t.n_jac = (int)dj_rowid_.size();
   t.dep_state.clear();
   for (int i = 0; i < n_state_; ++i)
     if (var_type_[i] == VAR_VARIABLE) t.dep_state.push_back(i);
@@ -803,9 +921,10 @@ void Model::build_tables() {
   }
   t.n_photo = n_host_rate();
   t.n_part = (int)t.rx_vdep.size();
-  // SIMPOL instances: 4 pseudo-rates each after the terms' rates, 8 per-cell
-  // constants after the terms' rate constants, and their Jacobian partials
-  // (4 + 4 per dependent element) after the terms' partials
+  // SIMPOL and HL instances: 4 pseudo-rates each after the terms' rates, 8
+  // per-cell constants after the terms' rate constants, and their Jacobian
+  // partials (4, plus 4 per dependent element for SIMPOL) after the terms'
+  // partials
   t.simpol = simpol_;
   t.n_simpol = (int)simpol_.size();
   t.n_rates = t.n_rxn + 4 * t.n_simpol;
@@ -815,7 +934,8 @@ void Model::build_tables() {
   for (const SimpolInst& si : simpol_) {
     t.si_part0.push_back(n_part_all);
     int nd = 0;
-    for (int e : si.elem) nd += var_type_[e] == VAR_VARIABLE;
+    if (si.type == RXN_SIMPOL_PHASE_TRANSFER)
+      for (int e : si.elem) nd += var_type_[e] == VAR_VARIABLE;
     n_part_all += 4 + 4 * nd;
   }
   t.n_part_all = n_part_all;
@@ -842,9 +962,10 @@ void Model::build_tables() {
         }
         ++ti;
       }
-      // SIMPOL at its place in the mechanism: the gas gains evaporation and
-      // loses condensation, the aerosol species the reverse
-      // (src/rxns/rxn_SIMPOL_phase_transfer.c:414-446)
+      // SIMPOL and HL at their place in the mechanism: the gas gains
+      // evaporation and loses condensation, the aerosol species the reverse
+      // (src/rxns/rxn_SIMPOL_phase_transfer.c:414-446,
+      // src/rxns/rxn_HL_phase_transfer.c:313-328)
       for (; ks < t.n_simpol && simpol_[ks].rxn == (int)ri; ++ks) {
         const int base = t.n_rxn + 4 * ks;
         const int dg = deriv_ids_[simpol_[ks].gas], da = deriv_ids_[simpol_[ks].aero];
@@ -872,8 +993,8 @@ void Model::build_tables() {
   std::vector<std::vector<int>> jpart(t.n_jac), jind(t.n_jac);
   std::vector<std::vector<double>> jco(t.n_jac);
   auto slot_of = [&](int row, int col) {
-    for (int e = sj_colptr_[col]; e < sj_colptr_[col + 1]; ++e)
-      if (sj_rowid_[e] == row) return e;
+    for (int e = dj_colptr_[col]; e < dj_colptr_[col + 1]; ++e)
+      if (dj_rowid_[e] == row) return e;
     return -1;
   };
   {
@@ -900,9 +1021,10 @@ void Model::build_tables() {
         ++ti;
       }
   }
-  // SIMPOL partials: losses (jg_ind -1) and unguarded productions (-2) of
-  // the gas and aerosol rows against each other and every dependent element
-  // (src/rxns/rxn_SIMPOL_phase_transfer.c:615-744, total-mass branch)
+  // SIMPOL and HL partials: losses (jg_ind -1) and unguarded productions
+  // (-2) of the gas and aerosol rows against each other and, for SIMPOL,
+  // every dependent element (src/rxns/rxn_SIMPOL_phase_transfer.c:615-744,
+  // total-mass branch; src/rxns/rxn_HL_phase_transfer.c:400-439)
   for (int k = 0; k < t.n_simpol; ++k) {
     const SimpolInst& si = simpol_[k];
     const int p0 = t.si_part0[k];
@@ -917,6 +1039,7 @@ void Model::build_tables() {
     add(da, dg, p0 + 1, false);
     add(dg, da, p0 + 2, false);
     add(da, da, p0 + 3, true);
+    if (si.type != RXN_SIMPOL_PHASE_TRANSFER) continue;
     int j = 0;
     for (int es : si.elem) {
       if (var_type_[es] != VAR_VARIABLE) continue;
@@ -933,11 +1056,11 @@ void Model::build_tables() {
   t.jg_lupos.assign(t.n_jac, 0);
   t.jg_row.assign(t.n_jac, 0);
   for (int c = 0; c < n_dep_; ++c)
-    for (int e = sj_colptr_[c]; e < sj_colptr_[c + 1]; ++e) {
-      int pr = t.lu_iperm[sj_rowid_[e]], pc = t.lu_iperm[c];
+    for (int e = dj_colptr_[c]; e < dj_colptr_[c + 1]; ++e) {
+      int pr = t.lu_iperm[dj_rowid_[e]], pc = t.lu_iperm[c];
       for (int q = t.lu_rowptr[pr]; q < t.lu_rowptr[pr + 1]; ++q)
         if (t.lu_col[q] == pc) t.jg_lupos[e] = q;
-      t.jg_row[e] = sj_rowid_[e];
+      t.jg_row[e] = dj_rowid_[e];
     }
   for (int e = 0; e < t.n_jac; ++e) {
     t.jg_ptr[e] = (int)t.jg_part.size();

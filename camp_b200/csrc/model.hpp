@@ -17,6 +17,7 @@ enum : int {
   RXN_CMAQ_H2O2 = 3,
   RXN_CMAQ_OH_HNO3 = 4,
   RXN_PHOTOLYSIS = 5,
+  RXN_HL_PHASE_TRANSFER = 6,
   RXN_FIRST_ORDER_LOSS = 12,
   RXN_EMISSION = 13,
   RXN_WET_DEPOSITION = 14,
@@ -35,22 +36,30 @@ inline bool host_rate_type(int type) {
          type == RXN_WET_DEPOSITION;
 }
 
-// One SIMPOL phase instance (a reaction's partitioning into one phase of
-// one mode or bin).  Elements are the mass species (variable, constant,
-// PSSA) of every phase of the mode or bin in state order: the number
-// concentration depends on all of them, the phase mass and mean molecular
-// weight on those of the instance's phase
-// (src/aero_reps/aero_rep_modal_binned_mass.c:86-125).
+// One phase instance of a SIMPOL or HL phase-transfer reaction (its
+// partitioning into one phase of one mode or bin).  Elements are the mass
+// species (variable, constant, PSSA) of every phase of the mode or bin in
+// state order: the number concentration depends on all of them, the phase
+// mass and mean molecular weight on those of the instance's phase
+// (src/aero_reps/aero_rep_modal_binned_mass.c:86-125).  HL registers the
+// same elements, but its partials over them are zero for this
+// representation (radii do not depend on the state and its number
+// concentration is 1, src/rxns/rxn_HL_phase_transfer.c:386-399): they
+// take no part in the device tables.
 struct SimpolInst {
+  int type = RXN_SIMPOL_PHASE_TRANSFER;  // or RXN_HL_PHASE_TRANSFER
   int rxn = 0, x = 0;              // reaction, instance within it
   int gas = 0, aero = 0, act = -1;  // state indices (act: -1 when none)
+  int water = -1;                   // HL: aerosol-phase water (state index)
   int rep = 0, section = 0, bin = 0, phase = 0;
   int kind = SECTION_MODAL;
   int gmd_col = -1, gsd_col = -1;   // host-set columns of a mode's GMD / GSD
   double bin_dp = 0.0;              // bin diameter [m] (bins)
   int n_phases = 0;                 // phases of the mode or bin (volume floors)
   // the reaction's float parameters: DELTA_H DELTA_S DIFF_COEFF PRE_C_AVG
-  // B1..B4 CONV MW (src/rxns/rxn_SIMPOL_phase_transfer.c:31-40)
+  // B1..B4 CONV MW (SIMPOL, src/rxns/rxn_SIMPOL_phase_transfer.c:31-40) or
+  // DELTA_H DELTA_S DIFF_COEFF PRE_C_AVG A C CONV MW (HL,
+  // src/rxns/rxn_HL_phase_transfer.c:29-36)
   double prm[10] = {0.0};
   std::vector<int> elem;            // state indices
   std::vector<double> inv_rho, inv_mw;  // 1/density; 1/MW in the phase, else 0
@@ -96,7 +105,7 @@ struct Tables {
   int n_state = 0;  // state variables per cell
   int n_rxn = 0;     // mass-action terms (Rxn::terms of every reaction)
   int n_part = 0;   // variable-reactant occurrences (rate partials)
-  int n_jac = 0;    // solver Jacobian entries
+  int n_jac = 0;    // live solver Jacobian entries (Model::device_colptr)
   int n_lu = 0;     // L+U entries
   int n_photo = 0;  // host-rate columns (reactions of a host_rate_type)
   int n_flev = 0, n_blev = 0;
@@ -122,8 +131,9 @@ struct Tables {
   int n_keff = 0;      // n_rxn + 8 n_simpol
   int n_rates = 0;     // n_rxn + 4 n_simpol
   std::vector<double> fg_coef;
-  // J gather by solver Jacobian entry (CSC order); jg_ind: -1 loss, -2
-  // unguarded product (SIMPOL), else the guard's independent species
+  // J gather by live solver Jacobian entry (CSC order); jg_ind: -1 loss,
+  // -2 unguarded product (phase transfer), else the guard's independent
+  // species
   std::vector<int> jg_ptr, jg_part, jg_ind, jg_lupos, jg_row;
   std::vector<double> jg_coef;
   // LU structure in pivot order
@@ -189,8 +199,16 @@ class Model {
   const std::vector<int>& rxn_int() const { return rxn_int_; }
   const std::vector<double>& rxn_float() const { return rxn_float_; }
   const std::vector<Rxn>& rxns() const { return rxns_; }
+  // the solver Jacobian as the reference builds it (every registered
+  // variable x variable element, src/camp_solver.c:1559-1633)
   const std::vector<int>& solver_colptr() const { return sj_colptr_; }
   const std::vector<int>& solver_rowid() const { return sj_rowid_; }
+  // its live entries, the ones some reaction can make non-zero, which the
+  // LU and the device tables use (every entry for mechanisms without HL
+  // phase transfer), and the solver entry of each
+  const std::vector<int>& device_colptr() const { return dj_colptr_; }
+  const std::vector<int>& device_rowid() const { return dj_rowid_; }
+  const std::vector<int>& device_to_solver() const { return dj_to_sj_; }
   const Tables& tables() const { return tab_; }
   bool built() const { return built_; }
 
@@ -212,6 +230,7 @@ class Model {
                              const std::vector<int>& blev, int nbl);
   void build_tables();
   bool resolve_simpol(std::string* err);
+  bool resolve_instance(SimpolInst* si, int phase, int ri, std::string* err);
   int rxn_elem_id(int dep, int ind) const;
 
   int n_state_, n_cells_, n_dep_, n_rxn_;
@@ -228,7 +247,9 @@ class Model {
   std::vector<SimpolInst> simpol_;
   std::vector<int> deriv_ids_;
   std::vector<int> rj_colptr_, rj_rowid_;
+  std::vector<int> rl_colptr_, rl_rowid_;  // live subset of the reaction Jacobian
   std::vector<int> sj_colptr_, sj_rowid_;
+  std::vector<int> dj_colptr_, dj_rowid_, dj_to_sj_;
   Tables tab_;
   bool built_ = false;
 };

@@ -26,13 +26,15 @@ struct DevMech {
   const int *fl_ptr, *fl_rows, *bl_ptr, *bl_rows;
   const int *dep_state, *const_state;
   const double* atol;  // per dependent variable
-  // SIMPOL instances: the reaction's 10 float parameters, section kind,
-  // GMD / GSD columns (modes) or bin diameter, activity coefficient state
-  // index (-1: none), phases of the mode or bin, and its constant (not
+  // SIMPOL and HL instances: reaction type, the reaction's float
+  // parameters (10 slots), section kind, GMD / GSD columns (modes) or bin
+  // diameter, activity coefficient state index (-1: none), HL water state
+  // index, phases of the mode or bin, and (SIMPOL) its constant (not
   // dependent) mass species: state index, 1/density, 1/MW and in-phase flag
   int n_simpol;
   const double* si_prm;
-  const int *si_kind, *si_gmd_col, *si_gsd_col, *si_act, *si_nph, *si_cptr, *si_cidx;
+  const int *si_type, *si_kind, *si_gmd_col, *si_gsd_col, *si_act, *si_water, *si_nph,
+      *si_cptr, *si_cidx;
   const double *si_dp, *si_cinv_rho, *si_cinv_mw, *si_cin;
 };
 
@@ -100,21 +102,27 @@ static __device__ double rate_constant(const DevMech& m, int r, double T, double
 // src/aero_reps/aero_rep_modal_binned_mass.c:176-236,
 // src/aero_phase_solver.c:14-19,88-147).  A mode's radius and number factor
 // follow from the cell's GMD / GSD columns.
+//
+// An HL instance (src/rxns/rxn_HL_phase_transfer.c:209-247, 262-330) fills
+// the same slots so that the SIMPOL rate formulas give its rates: number
+// factor, activity, volume and mass 1, and "moles" K_H * water, so that the
+// evaporation rate constant k_c K_eq / moles is k_c / (K_H water), K_H being
+// the Henry's law constant in kg_x / kg_H2O / ppm and the water the cell's
+// (constant) aerosol-phase water.
 static __device__ void simpol_constants(const DevMech& m, int k,
                                                      const double* cell_state, double T,
                                                      double P, const double* photo_cell,
                                                      double* c) {
   constexpr double R = 8.314472, PI = 3.14159265358979323846;
   const double* f = m.si_prm + 10 * k;
+  const bool hl = ldg(m.si_type + k) == RXN_HL_PHASE_TRANSFER;
   double alpha = 0.1;
   if (f[0] != 0.0 || f[1] != 0.0) {
     const double del_g = f[0] - T * f[1];
     alpha = exp(-del_g / (R * T));
     alpha = alpha / (1.0 + alpha);
   }
-  const double mfp = 3.0 * f[2] / sqrt(8.0 * R * T / (PI * f[9]));
-  double vp = f[4] / T + f[5] + f[6] * T + f[7] * log(T);
-  vp = 101325.0 * pow(10.0, vp);
+  const double mfp = 3.0 * f[2] / sqrt(8.0 * R * T / (PI * (hl ? f[7] : f[9])));
   double radius, nfac;
   if (ldg(m.si_kind + k) == SECTION_MODAL) {
     const double gmd = photo_cell ? photo_cell[ldg(m.si_gmd_col + k)] : 0.0;
@@ -131,6 +139,19 @@ static __device__ void simpol_constants(const DevMech& m, int k,
   const double fs = (0.75 * alpha * (1.0 + kn)) /
                     (kn * kn + (1.0 + 0.283 * alpha) * kn + 0.75 * alpha);
   c[0] = 4.0 * PI * radius * f[2] * fs;
+  if (hl) {
+    double kh = f[4] * P * 1.0e-6;
+    if (f[5] != 0.0) kh *= exp(f[5] * (1.0 / T - 1.0 / 298.0));
+    kh *= f[7];
+    const double w = cell_state[ldg(m.si_water + k)];
+    c[1] = 1.0;
+    c[2] = 1.0 / (f[6] * T / P);
+    c[3] = c[4] = c[5] = c[6] = 1.0;
+    c[7] = kh * (w > bdf::kTiny ? w : bdf::kTiny);
+    return;
+  }
+  double vp = f[4] / T + f[5] + f[6] * T + f[7] * log(T);
+  vp = 101325.0 * pow(10.0, vp);
   c[1] = vp / P / f[9] * 1.0e6;
   c[2] = 1.0 / (f[8] * T / P);
   c[3] = nfac;

@@ -1745,16 +1745,20 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   m.n_const = (int)cst.size();
   // SIMPOL instances (device-side constants; see rates.cuh)
   std::vector<double> si_prm, si_dp, si_cinv_rho, si_cinv_mw, si_cin;
-  std::vector<int> si_kind, si_gmd, si_gsd, si_act, si_nph, si_cptr(1, 0), si_cidx;
+  std::vector<int> si_type, si_kind, si_gmd, si_gsd, si_act, si_water, si_nph, si_cptr(1, 0),
+      si_cidx;
   for (const SimpolInst& si : t.simpol) {
     si_prm.insert(si_prm.end(), si.prm, si.prm + 10);
+    si_type.push_back(si.type);
     si_kind.push_back(si.kind);
     si_gmd.push_back(si.gmd_col);
     si_gsd.push_back(si.gsd_col);
     si_dp.push_back(si.bin_dp);
     si_act.push_back(si.act);
+    si_water.push_back(si.water);
     si_nph.push_back(si.n_phases);
-    for (size_t j = 0; j < si.elem.size(); ++j) {
+    const size_t ne = si.type == RXN_SIMPOL_PHASE_TRANSFER ? si.elem.size() : 0;
+    for (size_t j = 0; j < ne; ++j) {
       if (model.var_type()[si.elem[j]] == VAR_VARIABLE) continue;
       si_cidx.push_back(si.elem[j]);
       si_cinv_rho.push_back(si.inv_rho[j]);
@@ -1766,10 +1770,12 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   m.n_simpol = t.n_simpol;
   Packer pk;
   pk.add(si_prm, &m.si_prm);
+  pk.add(si_type, &m.si_type);
   pk.add(si_kind, &m.si_kind);
   pk.add(si_gmd, &m.si_gmd_col);
   pk.add(si_gsd, &m.si_gsd_col);
   pk.add(si_act, &m.si_act);
+  pk.add(si_water, &m.si_water);
   pk.add(si_nph, &m.si_nph);
   pk.add(si_cptr, &m.si_cptr);
   pk.add(si_cidx, &m.si_cidx);
@@ -1795,7 +1801,7 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   pk.add(t.jg_ind, &m.jg_ind);
   pk.add(t.jg_lupos, &m.jg_lupos);
   pk.add(t.jg_row, &m.jg_row);
-  pk.add(model.solver_colptr(), &m.jac_colptr);
+  pk.add(model.device_colptr(), &m.jac_colptr);
   pk.add(t.jg_coef, &m.jg_coef);
   pk.add(t.lu_perm, &m.lu_perm);
   pk.add(t.lu_rowptr, &m.lu_rowptr);

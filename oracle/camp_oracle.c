@@ -25,6 +25,7 @@
 #define T_EMISSION 13
 #define T_WET_DEPOSITION 14
 #define T_SIMPOL 10
+#define T_HL 6
 
 /* types whose packed data is not the NUM_REACT_/NUM_PROD_ layout */
 static int species_rate_type(int t) {
@@ -118,7 +119,7 @@ int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
                const int *ints, const double *floats) {
   if (m->n_added >= m->n_rxn) return 1;
   if ((type < T_ARRHENIUS || type > T_PHOTOLYSIS) && !species_rate_type(type) &&
-      type != T_SIMPOL)
+      type != T_SIMPOL && type != T_HL)
     return 2;
   if (m->int_size + n_int + 1 > m->int_cap) {
     m->int_cap = 2 * (m->int_size + n_int + 1) + 64;
@@ -455,6 +456,48 @@ static void simpol_env(const ORxn *r, double T, double P, double *k) {
   k[2] = vp / P / f[9] * 1.0e6;
 }
 
+/* --- HL phase transfer (src/rxns/rxn_HL_phase_transfer.c) --------------- */
+/* packed layout of :29-63 */
+typedef struct {
+  int n;
+  int *I;
+  const double *F;
+} HLV;
+static HLV hlv(const ORxn *r) {
+  HLV s = {r->ints[0], r->ints, r->fl};
+  return s;
+}
+static int hl_gas(HLV s) { return s.I[1] - 1; }
+static int *hl_deriv(HLV s, int x) { return &s.I[2 + x]; }
+static int *hl_jac(HLV s, int x) { return &s.I[3 + s.n + x]; }
+static int hl_iloc(HLV s, int x) { return s.I[4 + 6 * s.n + x] - 1; }
+static int hl_aero(HLV s, int x) { return s.I[hl_iloc(s, x)] - 1; }
+static int hl_water(HLV s, int x) { return s.I[hl_iloc(s, x) + 1] - 1; }
+static int hl_phase(HLV s, int x) { return s.I[hl_iloc(s, x) + 2] - 1; }
+static int hl_rep(HLV s, int x) { return s.I[hl_iloc(s, x) + 3] - 1; }
+static int hl_nelem(HLV s, int x) { return s.I[hl_iloc(s, x) + 4]; }
+static int *hl_phase_jac(HLV s, int x, int set, int e) {
+  return &s.I[hl_iloc(s, x) + 5 + set * hl_nelem(s, x) + e];
+}
+
+/* rate constants of one HL reaction (:209-247): MFP, alpha, the Henry's law
+ * equilibrium constant in kg_x / kg_H2O / ppm and the kg m-3 -> ppm factor */
+static void hl_env(const ORxn *r, double T, double P, double *k) {
+  const double *f = r->fl;
+  k[1] = 0.1;
+  if (f[0] != 0.0 || f[1] != 0.0) {
+    double del_g = f[0] - T * f[1];
+    k[1] = exp(-del_g / (R_GAS * T));
+    k[1] = k[1] / (1.0 + k[1]);
+  }
+  k[0] = 3.0 * f[2] / sqrt(8.0 * R_GAS * T / (M_PI * f[7]));
+  if (f[5] == 0.0)
+    k[2] = f[4] * P * 1.0e-6 * f[7];
+  else
+    k[2] = f[4] * P * 1.0e-6 * exp(f[5] * (1.0 / T - 1.0 / 298.0)) * f[7];
+  k[3] = f[6] * T / P;
+}
+
 /* --- Jacobian element registry (restates src/Jacobian.c:105-214) -------- */
 typedef struct {
   int n;
@@ -594,6 +637,27 @@ static void lu_free(LUSym *lu) {
   free(lu->a_to_lu);
 }
 
+/* The representation's elements for a phase instance: the mass species of
+ * every phase of the instance's mode / bin (aero_rep_modal_binned_mass.c:
+ * 86-125), flagged in state order; the representation's PHASE_NUM_JAC_ELEM_
+ * is written as its get_used_jac_elem writes it. */
+static void instance_elements(const OracleMech *m, int rep, int phase, char *flag) {
+  memset(flag, 0, (size_t)m->n_state);
+  ARep ar = arep(m, rep, NULL);
+  int sx, sb, sy;
+  if (!arep_locate(ar, phase, &sx, &sb, &sy)) return;
+  for (int y = 0; y < sec_np(ar, sx); ++y) {
+    APh ph = aphase(m, ph_model(ar, sx, y, sb));
+    int k = 0;
+    for (int i = 0; i < ph.n; ++i)
+      if (counts_in_mass(ph.type[i])) {
+        flag[ph_state(ar, sx, y, sb) + i] = 1;
+        ++k;
+      }
+    *ph_njac(ar, sx, y, sb) = k;
+  }
+}
+
 /* Builds the sparsity as get_jac_init does for a gas-only model
  * (src/camp_solver.c:1440-1683): diagonal plus the reaction elements of
  * every reaction (src/rxns/rxn_arrhenius.c:44-60 and the same loop in the
@@ -605,8 +669,9 @@ int om_build(OracleMech *m) {
     ORxn *r = &m->rx[i];
     r->ints = m->int_data + (size_t)r->ints;
     r->fl = m->float_data + (size_t)r->fl;
-    if (species_rate_type(r->type) || r->type == T_SIMPOL) {
-      /* RXN_ID_ first; the reactant / product fields stay unused */
+    if (species_rate_type(r->type) || r->type == T_SIMPOL || r->type == T_HL) {
+      /* RXN_ID_ first (host-rate types); the reactant / product fields stay
+       * unused */
       r->nr = r->np = 0;
       r->n_int_prop = 0;
       r->n_float_prop = 1;
@@ -653,23 +718,7 @@ int om_build(OracleMech *m) {
             jr_register(&rj, g, sim_act(sm, x));
             jr_register(&rj, a, sim_act(sm, x));
           }
-          /* the representation's elements: the mass species of every phase
-           * of the instance's mode / bin (aero_rep_modal_binned_mass.c:
-           * 86-125), registered in state order */
-          memset(flag, 0, (size_t)n);
-          ARep ar = arep(m, sim_rep(sm, x), NULL);
-          int sx, sb, sy;
-          if (arep_locate(ar, sim_phase(sm, x), &sx, &sb, &sy))
-            for (int y = 0; y < sec_np(ar, sx); ++y) {
-              APh ph = aphase(m, ph_model(ar, sx, y, sb));
-              int k = 0;
-              for (int i = 0; i < ph.n; ++i)
-                if (counts_in_mass(ph.type[i])) {
-                  flag[ph_state(ar, sx, y, sb) + i] = 1;
-                  ++k;
-                }
-              *ph_njac(ar, sx, y, sb) = k;
-            }
+          instance_elements(m, sim_rep(sm, x), sim_phase(sm, x), flag);
           int used = 0;
           for (int e = 0; e < n; ++e) {
             if (!flag[e]) continue;
@@ -681,6 +730,34 @@ int om_build(OracleMech *m) {
           }
           for (; used < sim_nelem(sm, x); ++used)
             *sim_phase_jac(sm, x, 0, used) = *sim_phase_jac(sm, x, 1, used) = -1;
+        }
+        free(flag);
+        continue;
+      }
+      case T_HL: { /* src/rxns/rxn_HL_phase_transfer.c:72-138 */
+        HLV hl = hlv(r);
+        const int g = hl_gas(hl);
+        jr_register(&rj, g, g);
+        char *flag = (char *)zalloc((size_t)n);
+        for (int x = 0; x < hl.n; ++x) {
+          const int a = hl_aero(hl, x), w = hl_water(hl, x);
+          jr_register(&rj, a, g);
+          jr_register(&rj, g, a);
+          jr_register(&rj, a, a);
+          jr_register(&rj, g, w);
+          jr_register(&rj, a, w);
+          instance_elements(m, hl_rep(hl, x), hl_phase(hl, x), flag);
+          int used = 0;
+          for (int e = 0; e < n; ++e) {
+            if (!flag[e]) continue;
+            jr_register(&rj, g, e);
+            jr_register(&rj, a, e);
+            *hl_phase_jac(hl, x, 0, used) = e;
+            *hl_phase_jac(hl, x, 1, used) = e;
+            ++used;
+          }
+          for (; used < hl_nelem(hl, x); ++used)
+            *hl_phase_jac(hl, x, 0, used) = *hl_phase_jac(hl, x, 1, used) = -1;
         }
         free(flag);
         continue;
@@ -741,6 +818,30 @@ int om_build(OracleMech *m) {
           }
           for (int e = 0; e < sim_nelem(sm, x); ++e) {
             int *pg = sim_phase_jac(sm, x, 0, e), *pa = sim_phase_jac(sm, x, 1, e);
+            if (*pg > 0) *pg = jr_elem_id(cp, ri, g, *pg);
+            if (*pa > 0) *pa = jr_elem_id(cp, ri, a, *pa);
+          }
+        }
+        continue;
+      }
+      case T_HL: { /* src/rxns/rxn_HL_phase_transfer.c:149-186; the small
+                    * water concentration it also sets (:188-193) is unused */
+        HLV hl = hlv(r);
+        const int *cp = m->rj_colptr, *ri = m->rj_rowid;
+        const int g = hl_gas(hl);
+        *hl_deriv(hl, 0) = m->deriv_ids[g];
+        for (int x = 0; x < hl.n; ++x) *hl_deriv(hl, x + 1) = m->deriv_ids[hl_aero(hl, x)];
+        int ij = 0;
+        *hl_jac(hl, ij++) = jr_elem_id(cp, ri, g, g);
+        for (int x = 0; x < hl.n; ++x) {
+          const int a = hl_aero(hl, x), w = hl_water(hl, x);
+          *hl_jac(hl, ij++) = jr_elem_id(cp, ri, a, g);
+          *hl_jac(hl, ij++) = jr_elem_id(cp, ri, g, a);
+          *hl_jac(hl, ij++) = jr_elem_id(cp, ri, a, a);
+          *hl_jac(hl, ij++) = jr_elem_id(cp, ri, g, w);
+          *hl_jac(hl, ij++) = jr_elem_id(cp, ri, a, w);
+          for (int e = 0; e < hl_nelem(hl, x); ++e) {
+            int *pg = hl_phase_jac(hl, x, 0, e), *pa = hl_phase_jac(hl, x, 1, e);
             if (*pg > 0) *pg = jr_elem_id(cp, ri, g, *pg);
             if (*pa > 0) *pa = jr_elem_id(cp, ri, a, *pa);
           }
@@ -930,6 +1031,9 @@ void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
       case T_SIMPOL:
         simpol_env(r, T, P, k);
         break;
+      case T_HL:
+        hl_env(r, T, P, k);
+        break;
     }
   }
 }
@@ -1001,6 +1105,32 @@ void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
           if (da >= 0) {
             add_value(P, L, da, -nconc * evap / kk[3]);
             add_value(P, L, da, nconc * cond / kk[3]);
+          }
+        }
+        continue;
+      }
+      case T_HL: { /* src/rxns/rxn_HL_phase_transfer.c:262-330 */
+        HLV hl = hlv(r);
+        const double *kk = rxn_env + r->env_off;
+        for (int x = 0; x < hl.n; ++x) {
+          ARep ar = arep(m, hl_rep(hl, x), rxn_env);
+          int sx, sb, sy;
+          if (!arep_locate(ar, hl_phase(hl, x), &sx, &sb, &sy)) continue;
+          const double radius = arep_radius(ar, sx, sb);
+          /* total-particle mass concentrations: number_conc stays 1 */
+          const double nconc = 1.0;
+          long double cond = cond_k(hl.F[2], kk[0], radius, kk[1]);
+          long double evap = cond / kk[2];
+          cond *= state[hl_gas(hl)];
+          evap *= state[hl_aero(hl, x)] / state[hl_water(hl, x)];
+          const int dg = *hl_deriv(hl, 0), da = *hl_deriv(hl, 1 + x);
+          if (dg >= 0) {
+            add_value(P, L, dg, nconc * evap);
+            add_value(P, L, dg, -nconc * cond);
+          }
+          if (da >= 0) {
+            add_value(P, L, da, -evap / kk[3]);
+            add_value(P, L, da, cond / kk[3]);
           }
         }
         continue;
@@ -1114,6 +1244,51 @@ void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
             }
           }
           free(nd);
+        }
+        continue;
+      }
+      case T_HL: { /* src/rxns/rxn_HL_phase_transfer.c:343-494 */
+        HLV hl = hlv(r);
+        const double *kk = rxn_env + r->env_off;
+        const double Kp = kk[3];
+        for (int x = 0; x < hl.n; ++x) {
+          ARep ar = arep(m, hl_rep(hl, x), rxn_env);
+          int sx, sb, sy;
+          if (!arep_locate(ar, hl_phase(hl, x), &sx, &sb, &sy)) continue;
+          const double radius = arep_radius(ar, sx, sb);
+          /* total-particle mass concentrations: number 1, its partials 0;
+           * the radius partials of modes and bins are 0 as well */
+          const double nconc = 1.0, eff = 0.0, num = 0.0;
+          long double cond = cond_k(hl.F[2], kk[0], radius, kk[1]);
+          long double evap = cond / kk[2];
+          const double yg = state[hl_gas(hl)], ya = state[hl_aero(hl, x)];
+          const double yw = state[hl_water(hl, x)];
+          const int j0 = *hl_jac(hl, 0), jag = *hl_jac(hl, 1 + 5 * x);
+          const int jga = *hl_jac(hl, 2 + 5 * x), jaa = *hl_jac(hl, 3 + 5 * x);
+          const int jgw = *hl_jac(hl, 4 + 5 * x), jaw = *hl_jac(hl, 5 + 5 * x);
+          if (j0 >= 0) L[j0] += nconc * cond;
+          if (jga >= 0) P[jga] += nconc * evap / yw;
+          if (jgw >= 0) P[jgw] += -nconc * evap * ya / yw / yw;
+          if (jag >= 0) P[jag] += cond / Kp;
+          if (jaa >= 0) L[jaa] += evap / yw / Kp;
+          if (jaw >= 0) L[jaw] += -evap * ya / Kp / yw / yw;
+          cond *= yg;
+          evap *= ya / yw;
+          const long double dcdr = cond_k_dr(hl.F[2], kk[0], radius, kk[1]) * yg;
+          const long double dedr = dcdr / yg / kk[2] * ya / yw;
+          for (int e = 0; e < hl_nelem(hl, x); ++e) {
+            const int jg = *hl_phase_jac(hl, x, 0, e), ja = *hl_phase_jac(hl, x, 1, e);
+            if (jg > 0) {
+              P[jg] += nconc * dedr * eff;
+              L[jg] += nconc * dcdr * eff;
+              P[jg] += evap * num;
+              L[jg] += cond * num;
+            }
+            if (ja > 0) {
+              L[ja] += dedr / Kp * eff;
+              P[ja] += dcdr / Kp * eff;
+            }
+          }
         }
         continue;
       }

@@ -131,6 +131,7 @@ def ref_lib():
         lib.rxn_add_condensed_data.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p, vp]
         lib.ref_build.restype = C.c_int
         lib.ref_build.argtypes = [vp]
+        lib.ref_set_abs_tol.argtypes = [vp, _f64p]
         for name in (
             "ref_n_dep_var",
             "ref_n_rxn_jac_elem",
@@ -325,6 +326,7 @@ class RefModel:
                                                  np.ascontiguousarray(a.ints, np.int32),
                                                  np.ascontiguousarray(a.floats, np.float64),
                                                  self.h)
+        self.lib.ref_set_abs_tol(self.h, np.ascontiguousarray(mech.abs_tol, np.float64))
         rc = self.lib.ref_build(self.h)
         if rc != 0:
             raise RuntimeError(f"reference sparsity build failed ({rc})")

@@ -76,6 +76,11 @@ void *ref_new(int n_state_var, int n_cells, const int *var_type, int n_rxn,
     if (var_type[i] == CHEM_SPEC_VARIABLE) ++n_dep;
   }
   md->n_per_cell_dep_var = n_dep;
+  /* solver_initialize points the model at the caller's absolute tolerances
+   * before the sparsity build (src/camp_solver.c:431); HL phase transfer
+   * reads them in its update_ids (src/rxns/rxn_HL_phase_transfer.c:188-193).
+   * Zero until ref_set_abs_tol. */
+  md->abs_tol = (double *)xmalloc(sizeof(double) * n_state_var);
   if (time_derivative_initialize(&rs->sd.time_deriv, (unsigned)n_dep) != 1) {
     fprintf(stderr, "ref_glue: time derivative init failed\n");
     exit(EXIT_FAILURE);
@@ -122,6 +127,12 @@ void *ref_new(int n_state_var, int n_cells, const int *var_type, int n_rxn,
   md->n_sub_model = n_sub_model;
   rs->sd.no_solve = (n_rxn == 0);
   return rs;
+}
+
+/* Per-state absolute tolerances (the array solver_initialize receives). */
+void ref_set_abs_tol(void *h, const double *abs_tol) {
+  ModelData *md = &((RefSolver *)h)->sd.model_data;
+  memcpy(md->abs_tol, abs_tol, sizeof(double) * md->n_per_cell_state_var);
 }
 
 /* Sparsity, id update and Jacobian map: restates get_jac_init
@@ -374,6 +385,7 @@ void ref_free(void *h) {
   free(rs->J_rxn);
   free(rs->solver_col_ptrs);
   free(rs->solver_row_ids);
+  free(rs->sd.model_data.abs_tol);
   free(rs);
 }
 

@@ -41,7 +41,7 @@ def cb05_ref():
 # deposition, emissions and the wet deposition of one aqueous phase), and
 # mod37 with its SOA scheme (SIMPOL partitioning into the modal/binned
 # aerosol representation)
-GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas", "monarch_mod37_soa")
+GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas", "monarch_mod37_soa", "monarch_mod37_aero")
 
 
 @pytest.fixture(scope="session")
@@ -56,6 +56,13 @@ def mod37_soa():
     from camp_b200.mechanism import Mechanism
 
     return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_soa.mech.json"))
+
+
+@pytest.fixture(scope="session")
+def mod37_aero():
+    from camp_b200.mechanism import Mechanism
+
+    return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_aero.mech.json"))
 
 
 @pytest.fixture(scope="session", params=GOLDEN_MECHS)
@@ -176,3 +183,81 @@ def species_rate_case(kind):
     mech = Mechanism(kind.lower(), names, np.ones(n, np.int32), np.full(n, 1.0e-12), 1.0e-10,
                      rxns, ids)
     return mech, y0, first, rates, truth
+
+
+# One HL_PHASE_TRANSFER reaction of gas G into "G_aq" of a single aqueous
+# mode whose water is a constant species: with the modal/binned
+# representation's number concentration of 1 the system is linear,
+#   dG/dt = k_c G_aq / (K_H W) - k_c G,   dG_aq/dt = -(dG/dt) / K,
+# G + K G_aq is conserved and both relax at lambda = k_c (1 + 1 / (K_H W K)).
+HL_ENV = (272.5, 101253.3)              # T (K), P (Pa)
+HL_MODE = (2.0e-5, 1.5)                 # GMD (m), GSD
+HL_WATER = 1.0e-6                       # kg m-3
+HL_LAMBDA = 0.1                         # s-1, sets the Henry's law constant
+HL_Y0 = (0.5, 1.0e-6)                   # G (ppm), G_aq (kg m-3)
+HL_D, HL_MW, HL_C = 1.5e-5, 0.048, 2300.0
+
+
+def hl_rates(T, P, gmd, gsd, hlc):
+    """k_c, K_H and the kg m-3 -> ppm factor K of the reference's HL
+    (src/rxns/rxn_HL_phase_transfer.c:209-247, src/util.h:50-135): mass
+    accommodation 0.1 (no N*), the mode's effective radius."""
+    R, PI = 8.314472, np.pi
+    alpha = 0.1
+    mfp = 3.0 * HL_D / np.sqrt(8.0 * R * T / (PI * HL_MW))
+    r = gmd / 2.0 * np.exp(5.0 * np.log(gsd) ** 2 / 2.0)
+    kn = mfp / r
+    fs = 0.75 * alpha * (1.0 + kn) / (kn * kn + (1.0 + 0.283 * alpha) * kn + 0.75 * alpha)
+    kc = 4.0 * PI * r * HL_D * fs
+    kh = hlc * P * 1.0e-6 * np.exp(HL_C * (1.0 / T - 1.0 / 298.0)) * HL_MW
+    K = R / HL_MW * 1.0e6 * T / P
+    return kc, kh, K
+
+
+def hl_case(tmp_dir):
+    """(mechanism, y0, host columns (GMD, GSD), closed form G, G_aq at t)."""
+    import json
+
+    from camp_b200.aerosol import load_aerosol_mechanism
+
+    T, P = HL_ENV
+    kc, kh1, K = hl_rates(T, P, *HL_MODE, 1.0)
+    # the Henry's law constant that gives the chosen relaxation rate
+    hlc = kc / ((HL_LAMBDA - kc) * HL_WATER * K) / kh1
+    doc = {"camp-data": [
+        {"name": "G", "type": "CHEM_SPEC", "molecular weight [kg mol-1]": HL_MW,
+         "diffusion coeff [m2 s-1]": HL_D, "HLC(298K) [M Pa-1]": hlc,
+         "HLC exp factor [K]": HL_C, "absolute integration tolerance": 1e-14},
+        {"name": "G_aq", "type": "CHEM_SPEC", "phase": "AEROSOL",
+         "molecular weight [kg mol-1]": HL_MW, "density [kg m-3]": 1000.0,
+         "absolute integration tolerance": 1e-20},
+        {"name": "H2O_aq", "type": "CHEM_SPEC", "phase": "AEROSOL", "tracer type": "CONSTANT",
+         "molecular weight [kg mol-1]": 0.01801528, "density [kg m-3]": 1000.0},
+        {"name": "aqueous", "type": "AERO_PHASE", "species": ["G_aq", "H2O_aq"]},
+        {"name": "rep", "type": "AERO_REP_MODAL_BINNED_MASS", "modes/bins": {
+            "the mode": {"type": "MODAL", "phases": ["aqueous"], "shape": "LOG_NORMAL",
+                         "geometric mean diameter [m]": HL_MODE[0],
+                         "geometric standard deviation": HL_MODE[1]}}},
+        {"name": "hl", "type": "MECHANISM", "reactions": [
+            {"type": "HL_PHASE_TRANSFER", "gas-phase species": "G",
+             "aerosol phase": "aqueous", "aerosol-phase species": "G_aq",
+             "aerosol-phase water": "H2O_aq"}]},
+    ]}
+    path = os.path.join(str(tmp_dir), "hl.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    mech = load_aerosol_mechanism([path], name="hl")
+    assert mech.species == ["G", "the mode.aqueous.G_aq", "the mode.aqueous.H2O_aq"]
+    y0 = np.array([HL_Y0[0], HL_Y0[1], HL_WATER])
+    cols = np.array(HL_MODE)
+    kc, kh, K = hl_rates(T, P, *HL_MODE, hlc)
+    lam = kc * (1.0 + 1.0 / (kh * HL_WATER * K))
+    assert abs(lam - HL_LAMBDA) < 1e-12 * HL_LAMBDA
+    total = HL_Y0[0] + K * HL_Y0[1]
+    g_eq = total / (1.0 + K * kh * HL_WATER)
+
+    def truth(times):
+        g = g_eq + (HL_Y0[0] - g_eq) * np.exp(-lam * np.asarray(times, np.float64))
+        return np.stack([g, (total - g) / K], axis=-1)
+
+    return mech, y0, cols, truth

@@ -1,6 +1,6 @@
 """Generates the committed golden fixtures from the reference (run here only).
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py [REFERENCE_ROOT [TAG ...]]
 
 Outputs (all small):
   cb05cl_ae5.mech.json   packed cb05cl_ae5 mechanism as the Fortran caller
@@ -24,9 +24,16 @@ Outputs (all small):
                          (7 modes and bin sets, 99 aerosol state variables);
                          its wet deposition acts on the cloud-and-rain phase
                          instance.  The aerosol reactions of mod37 that are
-                         not restated (HL, aqueous equilibrium, ZSR, PDFiTE)
-                         are left out
-  cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz, monarch_mod37_soa_ref.npz
+                         not restated (aqueous equilibrium, ZSR, PDFiTE) are
+                         left out
+  monarch_mod37_aero.mech.json
+                         the SOA fixture plus the shipped partitioning of 35
+                         gas-phase species into cloud and rain water
+                         (cloud_and_rain_partitioning.json: HL_PHASE_TRANSFER
+                         into the "clouds and rain" mode, aerosol-phase water
+                         H2O_aq a constant species)
+  cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz, monarch_mod37_soa_ref.npz,
+  monarch_mod37_aero_ref.npz
                          outputs of the reference's own C code
                          (oracle/_ref/libcamp_ref.so, compiled from the
                          reference sources) on seeded cell states:
@@ -109,6 +116,17 @@ def mod37_soa(ref_root: str):
                                   name="monarch_mod37_soa")
 
 
+MOD37_AERO_FILES = MOD37_SOA_FILES + ("cloud_and_rain_partitioning.json",)
+
+
+def mod37_aero(ref_root: str):
+    from camp_b200.aerosol import load_aerosol_mechanism
+
+    base = os.path.join(ref_root, "mechanisms/monarch_mod37")
+    return load_aerosol_mechanism([os.path.join(base, f) for f in MOD37_AERO_FILES],
+                                  name="monarch_mod37_aero")
+
+
 def edge_cells(mech, cells):
     """Appends edge-case cells to a seeded batch."""
     st, env, ph = cells.state.copy(), cells.env.copy(), cells.photo_rates.copy()
@@ -133,14 +151,20 @@ def edge_cells(mech, cells):
             np.vstack([ph, np.asarray(extra_p)]))
 
 
-def main(ref_root: str) -> None:
+def main(ref_root: str, only: list[str] | None = None) -> None:
     sys.path.insert(0, ROOT)
     from oracle.oracle import build  # noqa: E402
 
     build(with_ref=True)
-    write_fixture(load_mechanism(cb05_files(ref_root), name="cb05cl_ae5"), "cb05cl_ae5")
-    write_fixture(mod37_gas(ref_root), "monarch_mod37_gas")
-    write_fixture(mod37_soa(ref_root), "monarch_mod37_soa")
+    makers = {
+        "cb05cl_ae5": lambda: load_mechanism(cb05_files(ref_root), name="cb05cl_ae5"),
+        "monarch_mod37_gas": lambda: mod37_gas(ref_root),
+        "monarch_mod37_soa": lambda: mod37_soa(ref_root),
+        "monarch_mod37_aero": lambda: mod37_aero(ref_root),
+    }
+    for tag, make in makers.items():
+        if not only or tag in only:
+            write_fixture(make(), tag)
 
 
 def write_fixture(mech, tag: str) -> None:
@@ -186,4 +210,5 @@ def write_fixture(mech, tag: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # make_golden.py [REFERENCE_ROOT [TAG ...]]: all fixtures, or the named ones
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)

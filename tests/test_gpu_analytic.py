@@ -106,3 +106,27 @@ def test_host_rate_types_known_answer(kind, precision):
     expect = truth(np.arange(1, 11))
     for c in range(n):
         np.testing.assert_allclose(out[:, c], expect, rtol=1e-7, atol=1e-14)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_hl_closed_form(tmp_path, precision):
+    """HL partitioning into one aqueous mode with constant water: the
+    relaxation to the Henry's law equilibrium (conftest.hl_case) through
+    the C ABI, the mode's GMD / GSD set per cell."""
+    from conftest import HL_ENV, hl_case
+
+    from camp_b200.solver import Solver
+
+    mech, y0, cols, truth = hl_case(tmp_path)
+    n = len(TIMES)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.array([1e-14, 1e-20, 1e-14]), rel_tol=1e-10, max_steps=100000)
+    s.set_precision(precision)
+    s.set_photo_rates(np.tile(cols, (n, 1)))
+    env = np.tile(np.array(HL_ENV), (n, 1))
+    out = np.zeros((n, 2))
+    for c, t in enumerate(TIMES):
+        x = np.tile(y0, (n, 1))
+        assert s.solve(x, env, 0.0, t) == 0, s.cell_stats()["status"]
+        out[c] = x[c, :2]
+    np.testing.assert_allclose(out, truth(TIMES), rtol=1e-6, atol=1e-18)

@@ -1,7 +1,8 @@
 """GPU parity: the CUDA path through the C ABI against the reference's C
-derivative/Jacobian (golden fixtures: cb05cl_ae5 and the gas phase of MONARCH
-mod37 with its deposition and emission reactions) and against the CPU
-oracle's solve."""
+derivative/Jacobian (golden fixtures: cb05cl_ae5, the gas phase of MONARCH
+mod37 with its deposition and emission reactions, mod37 with SIMPOL SOA
+partitioning, and with HL partitioning into cloud and rain water as well)
+and against the CPU oracle's solve."""
 import numpy as np
 import pytest
 
@@ -129,6 +130,15 @@ def test_mod37_soa_solve_matches_oracle(mod37_soa, precision):
     """mod37 with SIMPOL partitioning into the modal/binned aerosol
     representation (cells carry per-mode GMD / GSD columns)."""
     _check_solve(mod37_soa, precision=precision, seed=17 + precision,
+                 bulk_rel=1e-7 if precision == 0 else 1e-4)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mod37_aero_solve_matches_oracle(mod37_aero, precision):
+    """mod37 with SIMPOL and the 35 HL reactions into cloud and rain water
+    (the LU without HL's zero element partials; the oracle factors the
+    reference's full pattern)."""
+    _check_solve(mod37_aero, precision=precision, seed=19 + precision,
                  bulk_rel=1e-7 if precision == 0 else 1e-4)
 
 

@@ -86,6 +86,27 @@ def test_mod37_soa_composition(mod37_soa):
     assert all(c[0] == "rxn" for c in cols[:-10])
 
 
+def test_mod37_aero_composition(mod37_soa, mod37_aero):
+    """The aerosol fixture: the SOA fixture's state plus 35 HL reactions into
+    the "clouds and rain" mode, whose water (H2O_aq) is a constant species;
+    the reference registers the mode's elements against the gas and aerosol
+    species (3803 solver Jacobian entries)."""
+    from camp_b200.aerosol import RXN_HL_PHASE_TRANSFER
+    from camp_b200.cells import hl_water_indices
+    from camp_b200.mechanism import reaction_summary
+
+    m = mod37_aero
+    assert reaction_summary(m)["by_type"][RXN_HL_PHASE_TRANSFER] == 35
+    assert m.species == mod37_soa.species
+    water = hl_water_indices(m)
+    assert [m.species[i] for i in water] == ["clouds and rain.cloud and rain water.H2O_aq"]
+    assert all(m.var_type[i] == 2 for i in water)
+    for r in m.rxns:
+        if r.rxn_type == RXN_HL_PHASE_TRANSFER:
+            iloc = r.ints[4 + 6] - 1  # PHASE_INT_LOC_(1) of a single instance
+            assert r.ints[0] == 1 and r.ints.size == 4 + 13 + 2 * r.ints[iloc + 4]
+
+
 def test_mod37_gas_composition(mod37):
     """The mod37 gas-phase fixture holds every host-rate type: its rate
     columns are photolysis, dry deposition, emissions and the wet
@@ -100,7 +121,7 @@ def test_mod37_gas_composition(mod37):
 
 
 @pytest.mark.skipif(not ref_available(), reason="reference build absent")
-@pytest.mark.parametrize("which", ["cb05", "mod37", "mod37_soa"])
+@pytest.mark.parametrize("which", ["cb05", "mod37", "mod37_soa", "mod37_aero"])
 def test_live_against_reference_build(request, which):
     """Fresh random states through the reference build and the oracle."""
     from camp_b200.cells import make_cells
@@ -239,3 +260,21 @@ def test_host_rate_updates_match_reference(kind):
     np.testing.assert_allclose(l2, l1, rtol=1e-15, atol=0)
     j1, _ = ref.jac(0, 1.0)
     np.testing.assert_allclose(om.jac(y0, re, 1.0), j1, rtol=1e-15, atol=0)
+
+
+def test_hl_closed_form(tmp_path):
+    """HL partitioning into one aqueous mode (constant water) relaxes to the
+    Henry's law equilibrium at the rate the reference's rate constants give,
+    G + K G_aq conserved."""
+    from conftest import HL_ENV, hl_case
+
+    mech, y0, cols, truth = hl_case(tmp_path)
+    om = OracleModel(mech)
+    abs_tol = np.array([1e-14, 1e-20, 1e-14])
+    out = []
+    for t in (5.0, 20.0, 60.0):
+        nf, status, _, y = om.solve(y0[None, :].copy(), np.array([HL_ENV]), cols[None, :], 0.0,
+                                    t, 1e-10, abs_tol, max_steps=100000)
+        assert nf == 0, status
+        out.append(y[0, :2])
+    np.testing.assert_allclose(out, truth([5.0, 20.0, 60.0]), rtol=1e-7, atol=1e-18)
