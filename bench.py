@@ -41,6 +41,11 @@ MECH_FILE = os.path.join(ROOT, "tests", "golden", "cb05cl_ae5.mech.json")
 # gas phase of MONARCH mod37 (cb05 + dry deposition + emissions + the wet
 # deposition of its cloud-and-rain phase), packed from the shipped files
 MOD37_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_gas.mech.json")
+# the same with the shipped 2-product SOA scheme (SIMPOL partitioning into the
+# modal/binned aerosol representation), and with the partitioning of 35 gas
+# species into cloud and rain water (HL) as well
+MOD37_SOA_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_soa.mech.json")
+MOD37_AERO_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_aero.mech.json")
 # compulsory HBM bytes per cell-step of cb05cl_ae5: state read (80 x 8),
 # env (16), photolysis base rates (25 x 8), dependent state write (74 x 8)
 METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
@@ -68,7 +73,7 @@ def parse():
     ap.add_argument("--no-1e5", action="store_true",
                     help="skip the 1e5-cell single-host-step measurement")
     ap.add_argument("--no-mod37", action="store_true",
-                    help="skip the mod37 gas-phase (deposition + emission) block")
+                    help="skip the mod37 blocks (gas phase; SOA; SOA + cloud partitioning)")
     ap.add_argument("--no-cost-order", action="store_true",
                     help="fetch cells in index order instead of longest-first")
     ap.add_argument("--no-graph", action="store_true",
@@ -235,17 +240,18 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 def serving_run(args, precision):
     """Open-loop Poisson arrivals of column requests at each rate: 10-200
-    cells per column, 70 % cb05cl_ae5 and 30 % the gas phase of MONARCH mod37
-    (its SIMPOL / aerosol-phase reactions are outside this solver; its dry
-    deposition, emissions and wet deposition are in), host steps of 60, 300
-    or 900 s.  Latency is submit-to-completion inside the library."""
+    cells per column, 70 % cb05cl_ae5 and 30 % MONARCH mod37 with its SOA
+    scheme (dry deposition, emissions, wet deposition and SIMPOL partitioning
+    into the modal/binned representation, per-cell mode GMD / GSD), host
+    steps of 60, 300 or 900 s.  Latency is submit-to-completion inside the
+    library."""
     from camp_b200.cells import make_cells, photo_base_rates
     from camp_b200.mechanism import Mechanism
     from camp_b200.serve import Server
     from camp_b200.solver import Solver
 
     cb05 = Mechanism.load(MECH_FILE)
-    mod37 = Mechanism.load(MOD37_FILE)
+    mod37 = Mechanism.load(MOD37_SOA_FILE)
     mechs = [(cb05, photo_base_rates(cb05)), (mod37, photo_base_rates(mod37))]
     solvers = []
     for m, _ in mechs:
@@ -305,9 +311,9 @@ def serving_run(args, precision):
     server.close()
     for s in solvers:
         s.free()
-    return {"mix": "70% cb05cl_ae5 / 30% monarch_mod37 gas phase (cb05 + dry deposition, "
-                   "emissions, wet deposition; no aerosol partitioning); 10-200 cells; "
-                   "host steps 60/300/900 s; Poisson arrivals",
+    return {"mix": "70% cb05cl_ae5 / 30% monarch_mod37 with SOA (cb05 + dry deposition, "
+                   "emissions, wet deposition, SIMPOL partitioning into the modal/binned "
+                   "representation); 10-200 cells; host steps 60/300/900 s; Poisson arrivals",
             "precision": "mixed" if precision == 1 else "fp64", "slots": 8,
             "seconds_per_rate": args.serve_seconds, "rates": out}
 
@@ -320,7 +326,7 @@ def run_1e5(mech, args, dev, stream, n=100000):
     the sequence (the most expensive one: every cell starts from its seeded
     state), mixed and FP64, device-resident, longest-first order from a
     previous identical run; device time of the second run.  Also used with
-    another mechanism and cell count for the mod37 gas-phase block."""
+    another mechanism and cell count for the mod37 blocks."""
     import torch
 
     from camp_b200.cells import make_cells
@@ -480,9 +486,11 @@ def run_gpu_arm(args):
     at_1e5 = None
     if world == 1 and not args.no_1e5:
         at_1e5 = run_1e5(mech, args, dev, stream)
-    mod37 = None
+    mod37 = mod37_soa = mod37_aero = None
     if world == 1 and not args.no_mod37:
         mod37 = run_1e5(Mechanism.load(MOD37_FILE), args, dev, stream, n=10000)
+        mod37_soa = run_1e5(Mechanism.load(MOD37_SOA_FILE), args, dev, stream, n=10000)
+        mod37_aero = run_1e5(Mechanism.load(MOD37_AERO_FILE), args, dev, stream, n=10000)
     if rank != 0:
         solver.free()
         replicas.finalize(world)
@@ -547,6 +555,8 @@ def run_gpu_arm(args):
         "serving": serving,
         "cells_1e5": at_1e5,
         "mod37_gas": mod37,
+        "mod37_soa": mod37_soa,
+        "mod37_aero": mod37_aero,
     }
     print(json.dumps(line), flush=True)
     solver.free()

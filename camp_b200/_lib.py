@@ -59,6 +59,7 @@ EXPORTED = [
     "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_solver_from_json",
     "camp_b200_n_state_var", "camp_b200_state_name", "camp_b200_json_tolerances",
     "camp_b200_get_var_type", "camp_b200_rxn_float_data_size", "camp_b200_get_rxn_float_data",
+    "camp_b200_get_aero_data",
     "camp_b200_server_new", "camp_b200_server_add_solver",
     "camp_b200_server_submit", "camp_b200_server_wait", "camp_b200_server_pending",
     "camp_b200_server_free",
@@ -163,6 +164,9 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_get_var_type.argtypes = [vp, _i32p]
     lib.camp_b200_get_rxn_float_data.restype = ip
     lib.camp_b200_get_rxn_float_data.argtypes = [vp, _f64p]
+    lib.camp_b200_get_aero_data.restype = ip
+    lib.camp_b200_get_aero_data.argtypes = [vp, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                            vp, vp]
     lib.camp_b200_check_jac.restype = ip
     lib.camp_b200_check_jac.argtypes = [vp, _f64p, _f64p, ip, dp, dp, dp, _f64p, _i32p]
     lib.camp_b200_server_new.restype = vp

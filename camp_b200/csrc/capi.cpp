@@ -986,12 +986,31 @@ void* camp_b200_solver_from_json(const char* const* files, int n_files, int n_ce
     set_error("camp_b200_solver_from_json: " + err);
     return nullptr;
   }
+  int ph_i = 0, ph_f = 0, rp_i = 0, rp_f = 0, rp_e = 0;
+  for (const auto& p : lm.phases) {
+    ph_i += (int)p.ints.size();
+    ph_f += (int)p.floats.size();
+  }
+  for (const auto& r : lm.reps) {
+    rp_i += (int)r.ints.size();
+    rp_f += (int)r.floats.size();
+    rp_e += r.n_env;
+  }
   void* sd = solver_new((int)lm.species.size(), n_cells, lm.var_type.data(), (int)lm.rxns.size(),
-                        lm.n_int(), lm.n_float(), lm.n_env(), 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+                        lm.n_int(), lm.n_float(), lm.n_env(), (int)lm.phases.size(), ph_i, ph_f,
+                        (int)lm.reps.size(), rp_i, rp_f, rp_e, 0, 0, 0, 0);
   if (!sd) return nullptr;
+  // reactions, then phases and representations, the order of
+  // camp_solver_data%initialize (src/camp_solver_data.F90:635-700)
   for (auto& r : lm.rxns)
     rxn_add_condensed_data(r.type, (int)r.ints.size(), (int)r.floats.size(), r.n_env,
                            r.ints.data(), r.floats.data(), sd);
+  for (auto& p : lm.phases)
+    aero_phase_add_condensed_data((int)p.ints.size(), (int)p.floats.size(), p.ints.data(),
+                                  p.floats.data(), sd);
+  for (auto& r : lm.reps)
+    aero_rep_add_condensed_data(r.type, (int)r.ints.size(), (int)r.floats.size(), r.n_env,
+                                r.ints.data(), r.floats.data(), sd);
   Solver* s = S(sd);
   if (s->add_error) {
     set_error("camp_b200_solver_from_json: " + s->add_error_msg);
@@ -1029,6 +1048,20 @@ int camp_b200_json_tolerances(void* solver_data, double* abs_tol, double* rel_to
 int camp_b200_get_var_type(void* solver_data, int* out) {
   Solver* s = S(solver_data);
   std::copy(s->var_type.begin(), s->var_type.end(), out);
+  return 0;
+}
+
+int camp_b200_get_aero_data(void* solver_data, int which, int index, int* n_int, int* n_float,
+                            int* ints, double* floats) {
+  const Model& m = *S(solver_data)->model;
+  const int count = which == 0 ? m.n_aero_phase() : which == 1 ? m.n_aero_rep() : -1;
+  if (index < 0 || index >= count) return -1;
+  const std::vector<int>& I = which == 0 ? m.aero_phase_int(index) : m.aero_rep_int(index);
+  const std::vector<double>& F = which == 0 ? m.aero_phase_float(index) : m.aero_rep_float(index);
+  if (n_int) *n_int = (int)I.size();
+  if (n_float) *n_float = (int)F.size();
+  if (ints) std::copy(I.begin(), I.end(), ints);
+  if (floats) std::copy(F.begin(), F.end(), floats);
   return 0;
 }
 

@@ -16,6 +16,13 @@ constexpr int kUnknown = 0, kVariable = 1, kConstant = 2, kPssa = 3, kActivity =
 // reaction type ids, src/rxn_solver.c:19-35
 constexpr int kArrhenius = 1, kTroe = 2, kCmaqH2O2 = 3, kCmaqOHHNO3 = 4, kPhotolysis = 5;
 constexpr int kFirstOrderLoss = 12, kEmission = 13, kWetDeposition = 14;
+constexpr int kHl = 6, kSimpol = 10;
+// aerosol representation and section types,
+// src/aero_rep_solver.c:20, src/aero_reps/aero_rep_modal_binned_mass.c:25-26
+constexpr int kModalBinned = 2, kBinned = 1, kModal = 2;
+constexpr double kPi = 3.14159265358979323846;
+// the Fortran packer's -9999.9 is a default-kind (single precision) literal
+constexpr double kUnset = (double)-9999.9f;
 // physical constants, src/constants.F90:37-41
 constexpr double kBoltzmann = 1.3806505e-23;
 constexpr double kAvogadro = 6.02214179e23;
@@ -87,6 +94,19 @@ struct SpeciesDb {
   bool is_gas(const std::string& n) const {
     const Spec& s = spec.at(n);
     return s.phase.empty() || s.phase == "GAS";
+  }
+  const Json* prop(const std::string& n, const std::string& key) const {
+    for (const auto& p : spec.at(n).props)
+      if (p.first == key) return p.second;
+    return nullptr;
+  }
+  // a numeric property that must be present
+  bool number(const std::string& n, const std::string& key, double* v, std::string* err) const {
+    const Json* j = prop(n, key);
+    bool ok = j != nullptr;
+    if (ok) *v = as_number(*j, &ok);
+    if (!ok) *err = "Missing or non-numeric '" + key + "' for species " + n;
+    return ok;
   }
   int var_type(const std::string& n) const {
     int t = spec.at(n).type;
@@ -236,8 +256,8 @@ bool pack_reaction(const Json& r, const std::map<std::string, int>& gas_index, L
     out->ints = loss ? std::vector<int>{-1, id, 0, 0} : std::vector<int>{-1, id, 0};
     out->n_env = 2;
   } else if (type == "WET_DEPOSITION") {
-    *err = "WET_DEPOSITION removes the species of an aerosol phase, and aerosol phases are "
-           "not read from JSON here; add it as packed data (rxn_add_condensed_data)";
+    *err = "WET_DEPOSITION removes the species of an aerosol phase, and the input defines no "
+           "aerosol representation";
     return false;
   } else {
     *err = "reaction type " + type + " is not supported";
@@ -249,6 +269,448 @@ bool pack_reaction(const Json& r, const std::map<std::string, int>& gas_index, L
   }
   f.insert(f.end(), ylds.begin(), ylds.end());
   out->floats = std::move(f);
+  return true;
+}
+
+// --- aerosol phases and the modal/binned mass representation -----------
+
+bool mass_species(int t) { return t == kVariable || t == kConstant || t == kPssa; }
+
+// aero_phase_data_t%initialize (src/aero_phase_data.F90:306-385):
+// [NUM_STATE_VAR, SPEC_TYPE(x)], floats [MW(x), DENSITY(x)]
+bool pack_phase(const std::string& name, const std::vector<std::string>& species,
+                const SpeciesDb& db, LoadedPhase* out, std::string* err) {
+  out->name = name;
+  out->species = species;
+  const int n = (int)species.size();
+  out->ints.assign(1 + n, 0);
+  out->floats.assign(2 * n, 0.0);
+  out->ints[0] = n;
+  for (int i = 0; i < n; ++i) {
+    const std::string& sp = species[i];
+    if (!db.spec.count(sp)) {
+      *err = "Missing property set for species '" + sp + "' in aerosol phase '" + name + "'";
+      return false;
+    }
+    if (db.spec.at(sp).phase != "AEROSOL") {
+      *err = "Trying to add non-aerosol phase species to aerosol phase " + name +
+             "; species: " + sp;
+      return false;
+    }
+    const int t = db.var_type(sp);
+    out->ints[1 + i] = t;
+    if (mass_species(t) && (!db.number(sp, "molecular weight [kg mol-1]", &out->floats[i], err) ||
+                            !db.number(sp, "density [kg m-3]", &out->floats[n + i], err)))
+      return false;
+  }
+  return true;
+}
+
+struct Section {
+  std::string name;
+  int kind = kModal, n_bins = 1;
+  std::vector<int> phases;  // indices into the phase list
+};
+
+// A representation as the reaction packers query it (src/aero_rep_data.F90
+// unique_names / spec_state_id / phase_ids / num_jac_elem).
+struct Rep {
+  LoadedRep data;
+  int first_state = 0;  // 0-based state index of its first species
+  std::vector<Section> sections;
+  std::vector<std::string> unique;
+  std::vector<int> instances;  // phase index of each instance, Fortran order
+
+  // "section.[bin.]phase.species", optionally filtered by phase and species
+  std::vector<std::string> names(const std::vector<LoadedPhase>& ph, const std::string* phase,
+                                 const std::string* spec) const {
+    std::vector<std::string> out;
+    for (const Section& sec : sections)
+      for (int pi : sec.phases) {
+        if (phase && ph[pi].name != *phase) continue;
+        for (int b = 0; b < sec.n_bins; ++b) {
+          const std::string bin = sec.n_bins > 1 ? std::to_string(b + 1) + "." : "";
+          for (const std::string& sp : ph[pi].species)
+            if (!spec || sp == *spec) out.push_back(sec.name + "." + bin + ph[pi].name + "." + sp);
+        }
+      }
+    return out;
+  }
+  int state_id(const std::string& un) const {  // 1-based
+    for (size_t k = 0; k < unique.size(); ++k)
+      if (unique[k] == un) return first_state + 1 + (int)k;
+    return -1;
+  }
+  std::vector<int> phase_ids(const std::vector<LoadedPhase>& ph, const std::string& name) const {
+    std::vector<int> out;
+    for (size_t i = 0; i < instances.size(); ++i)
+      if (ph[instances[i]].name == name) out.push_back((int)i + 1);
+    return out;
+  }
+  // mass species of every phase of the instance's mode or bin
+  // (src/aero_reps/aero_rep_modal_binned_mass.F90:964-996)
+  int num_jac_elem(const std::vector<LoadedPhase>& ph, int phase_id) const {
+    int start = 0, left = phase_id;
+    for (const Section& sec : sections) {
+      const int size = (int)sec.phases.size() * sec.n_bins;
+      if (left <= size) {
+        const int b = (left - 1) % sec.n_bins;
+        int n = 0;
+        for (size_t k = 0; k < sec.phases.size(); ++k) {
+          const LoadedPhase& p = ph[instances[start + b + k * sec.n_bins]];
+          for (int i = 0; i < p.ints[0]; ++i) n += mass_species(p.ints[1 + i]);
+        }
+        return n;
+      }
+      left -= size;
+      start += size;
+    }
+    return 0;
+  }
+};
+
+// aero_rep_modal_binned_mass_t%initialize
+// (src/aero_reps/aero_rep_modal_binned_mass.F90:334-661) for a
+// representation whose species start at 1-based state id first_state_1
+bool pack_modal_binned(const Json& o, const std::vector<LoadedPhase>& phases, int first_state_1,
+                       Rep* rep, std::string* err) {
+  const std::string name = o.get("name") ? o.get("name")->str : "";
+  const Json* secs = o.get("modes/bins");
+  if (!secs || secs->kind != Json::Object || secs->obj.empty()) {
+    *err = "No sections or bins specified for modal/binned mass aerosol representation '" + name +
+           "'";
+    return false;
+  }
+  bool ok = true;
+  std::vector<const Json*> sj;
+  for (const auto& kv : secs->obj) {
+    Section sec;
+    sec.name = kv.first;
+    const Json* t = kv.second.get("type");
+    const std::string type = t ? t->str : "";
+    if (type == "MODAL") {
+      sec.kind = kModal;
+    } else if (type == "BINNED") {
+      sec.kind = kBinned;
+      const Json* nb = kv.second.get("bins");
+      sec.n_bins = nb ? (int)SpeciesDb::as_number(*nb, &ok) : 0;
+      if (!ok || sec.n_bins < 2) {
+        *err = "Invalid number of bins for section '" + sec.name + "'";
+        return false;
+      }
+    } else {
+      *err = "Invalid type for section '" + sec.name + "'";
+      return false;
+    }
+    const Json* pl = kv.second.get("phases");
+    if (pl)
+      for (const Json& pn : pl->arr) {
+        int idx = -1;
+        for (size_t k = 0; k < phases.size(); ++k)
+          if (phases[k].name == pn.str) idx = (int)k;
+        if (idx < 0) {
+          *err = "Non-existant aerosol phase '" + pn.str + "' specified for mode '" + sec.name + "'";
+          return false;
+        }
+        sec.phases.push_back(idx);
+      }
+    rep->sections.push_back(sec);
+    sj.push_back(&kv.second);
+  }
+  const int ns = (int)rep->sections.size();
+  int n_int = 4 + 2 * ns, n_float = 0;
+  for (const Section& sec : rep->sections) {
+    const int np = (int)sec.phases.size();
+    n_int += 3 + 3 * sec.n_bins * np;
+    n_float += 3 * sec.n_bins + 2 * sec.n_bins * np;
+  }
+  std::vector<int>& I = rep->data.ints;
+  std::vector<double>& F = rep->data.floats;
+  I.assign(n_int, 0);
+  F.assign(n_float, 0.0);
+  I[0] = ns;
+  I[1] = n_int;
+  I[2] = n_float;
+  I[3] = -1;
+  int loc_i = 4 + 2 * ns + 1, loc_f = 1, state = first_state_1;  // 1-based locations
+  for (int x = 0; x < ns; ++x) {
+    const Section& sec = rep->sections[x];
+    I[4 + x] = loc_i;
+    I[4 + ns + x] = loc_f;
+    const int li = loc_i - 1, lf = loc_f - 1, nb = sec.n_bins, np = (int)sec.phases.size();
+    I[li] = sec.kind;
+    I[li + 1] = nb;
+    I[li + 2] = np;
+    if (sec.kind == kModal) {
+      F[lf + 2] = kUnset;  // effective radius
+      F[lf + 1] = kUnset;  // number concentration
+    } else {
+      const Json* jlo = sj[x]->get("minimum diameter [m]");
+      const Json* jhi = sj[x]->get("maximum diameter [m]");
+      const Json* jsc = sj[x]->get("scale");
+      if (!jlo || !jhi || !jsc) {
+        *err = "Missing diameter range or scale for bin '" + sec.name + "'";
+        return false;
+      }
+      const double lo = SpeciesDb::as_number(*jlo, &ok), hi = SpeciesDb::as_number(*jhi, &ok);
+      for (int b = 0; b < nb; ++b) {
+        double dp;
+        if (jsc->str == "LINEAR") {
+          dp = lo + b * (hi - lo) / (nb - 1);
+        } else if (jsc->str == "LOG") {
+          const double d_log = (std::log10(hi) - std::log10(lo)) / (nb - 1);
+          dp = std::pow(10.0, std::log10(lo) + b * d_log);
+        } else {
+          *err = "Invalid scale specified for bin '" + sec.name + "'";
+          return false;
+        }
+        F[lf + 3 * b] = dp;
+        F[lf + 3 * b + 2] = dp / 2.0;
+        F[lf + 3 * b + 1] = kUnset;
+      }
+    }
+    for (int y = 0; y < np; ++y)
+      for (int b = 0; b < nb; ++b) {
+        I[li + 3 + b * np + y] = state;                           // PHASE_STATE_ID_
+        I[li + 3 + nb * np + b * np + y] = sec.phases[y] + 1;     // PHASE_MODEL_DATA_ID_
+        state += (int)phases[sec.phases[y]].species.size();
+        rep->instances.push_back(sec.phases[y]);
+      }
+    loc_i += 3 + 3 * nb * np;
+    loc_f += 3 * nb + 2 * nb * np;
+  }
+  if (!ok) {
+    *err = "non-numeric parameter in aerosol representation '" + name + "'";
+    return false;
+  }
+  rep->data.type = kModalBinned;
+  rep->data.name = name;
+  rep->data.n_env = 2 * ns;
+  rep->first_state = first_state_1 - 1;
+  rep->unique = rep->names(phases, nullptr, nullptr);
+  return true;
+}
+
+// N* -> enthalpy and entropy of the mass accommodation coefficient
+// (src/rxns/rxn_SIMPOL_phase_transfer.F90, rxn_HL_phase_transfer.F90)
+void n_star_terms(const SpeciesDb& db, const std::string& gas, double* dh, double* ds,
+                  bool* ok) {
+  *dh = *ds = 0.0;
+  if (const Json* j = db.prop(gas, "N star")) {
+    const double ns = SpeciesDb::as_number(*j, ok);
+    *dh = (-10.0 * (ns - 1.0) + 7.53 * (std::pow(ns, 2.0 / 3.0) - 1.0) - 1.0) * 4184.0;
+    *ds = (-32.0 * (ns - 1.0) + 9.21 * (std::pow(ns, 2.0 / 3.0) - 1.0) - 1.3) * 4.184;
+  }
+}
+
+const std::string* json_str(const Json& r, const char* key) {
+  const Json* j = r.get(key);
+  return j && j->kind == Json::String ? &j->str : nullptr;
+}
+
+// One phase instance of a partitioning reaction: representation, species
+// and second species (activity coefficient or water) unique names, phase id
+struct Inst {
+  int rep;
+  std::string name, second;
+  int phase_id;
+};
+
+// the instances of (phase, species) over every representation, with the
+// second species' names beside them (an empty list when absent)
+bool instances_of(const std::vector<Rep>& reps, const std::vector<LoadedPhase>& phases,
+                  const std::string& phase, const std::string& spec, const std::string* second,
+                  std::vector<Inst>* out, std::string* err) {
+  for (size_t ri = 0; ri < reps.size(); ++ri) {
+    const std::vector<std::string> names = reps[ri].names(phases, &phase, &spec);
+    if (names.empty()) continue;
+    std::vector<std::string> sec;
+    if (second) {
+      sec = reps[ri].names(phases, &phase, second);
+      if (sec.size() != names.size()) {
+        *err = "Missing species " + spec + " or " + *second + " in phase " + phase;
+        return false;
+      }
+    }
+    const std::vector<int> pids = reps[ri].phase_ids(phases, phase);
+    for (size_t k = 0; k < names.size(); ++k)
+      out->push_back({(int)ri, names[k], second ? sec[k] : "", pids[k]});
+  }
+  if (out->empty()) {
+    *err = "No aerosol phase instances for partitioning of " + spec + " into " + phase;
+    return false;
+  }
+  return true;
+}
+
+// rxn_SIMPOL_phase_transfer_t%initialize
+// (src/rxns/rxn_SIMPOL_phase_transfer.F90:220-470)
+bool pack_simpol(const Json& r, const SpeciesDb& db, const std::map<std::string, int>& gas_index,
+                 const std::vector<Rep>& reps, const std::vector<LoadedPhase>& phases,
+                 LoadedRxn* out, std::string* err) {
+  const std::string* gas = json_str(r, "gas-phase species");
+  const std::string* phase = json_str(r, "aerosol phase");
+  const std::string* aero = json_str(r, "aerosol-phase species");
+  const std::string* act = json_str(r, "aerosol-phase activity coefficient");
+  if (!gas || !phase || !aero) {
+    *err = "SIMPOL phase transfer reaction is missing a species or phase name";
+    return false;
+  }
+  std::vector<Inst> inst;
+  if (!instances_of(reps, phases, *phase, *aero, act, &inst, err)) return false;
+  const int n = (int)inst.size();
+  std::vector<int> ne(n);
+  int E = 0;
+  for (int x = 0; x < n; ++x) E += ne[x] = reps[inst[x].rep].num_jac_elem(phases, inst[x].phase_id);
+  std::vector<int>& I = out->ints;
+  std::vector<double>& F = out->floats;
+  I.assign(4 + 13 * n + 2 * E, 0);
+  F.assign(10 + 4 * E, 0.0);
+  I[0] = n;
+  auto g = gas_index.find(*gas);
+  if (g == gas_index.end()) {
+    *err = "Missing gas-phase species " + *gas;
+    return false;
+  }
+  I[1] = g->second;
+  int loc_i = 12 * n + 5, loc_f = 11;  // PHASE_INT_LOC_(1), PHASE_REAL_LOC_(1), 1-based
+  for (int x = 0; x < n; ++x) {
+    const Rep& rp = reps[inst[x].rep];
+    I[4 + 10 * n + x] = loc_i;
+    I[4 + 11 * n + x] = loc_f;
+    I[loc_i - 1] = ne[x];                                            // NUM_AERO_PHASE_JAC_ELEM_
+    I[2 + x] = rp.state_id(inst[x].name);                            // AERO_SPEC_
+    I[2 + n + x] = act ? rp.state_id(inst[x].second) : -1;           // AERO_ACT_ID_
+    I[2 + 2 * n + x] = inst[x].phase_id;                             // AERO_PHASE_ID_
+    I[2 + 3 * n + x] = inst[x].rep + 1;                              // AERO_REP_ID_
+    loc_i += 1 + 2 * ne[x];
+    loc_f += 4 * ne[x];
+  }
+  bool ok = true;
+  double mw, gas_mw, dh, ds;
+  if (!db.spec.count(*aero) || !db.number(*aero, "molecular weight [kg mol-1]", &mw, err) ||
+      !db.number(*gas, "diffusion coeff [m2 s-1]", &F[2], err) ||
+      !db.number(*gas, "molecular weight [kg mol-1]", &gas_mw, err))
+    return false;
+  n_star_terms(db, *gas, &dh, &ds, &ok);
+  const Json* b = r.get("B");
+  if (!b || b->kind != Json::Array || b->arr.size() != 4) {
+    *err = "Incorrect number of 'B' parameters";
+    return false;
+  }
+  F[0] = dh;
+  F[1] = ds;
+  F[3] = std::sqrt(8.0 * kGasConst / (kPi * gas_mw));
+  for (int k = 0; k < 4; ++k) F[4 + k] = SpeciesDb::as_number(b->arr[k], &ok);
+  F[8] = kGasConst / mw * 1.0e6;
+  F[9] = mw;
+  if (!ok) {
+    *err = "non-numeric SIMPOL parameter";
+    return false;
+  }
+  out->type = kSimpol;
+  out->n_env = 4;
+  return true;
+}
+
+// rxn_HL_phase_transfer_t%initialize (src/rxns/rxn_HL_phase_transfer.F90:170-398)
+bool pack_hl(const Json& r, const SpeciesDb& db, const std::map<std::string, int>& gas_index,
+             const std::vector<Rep>& reps, const std::vector<LoadedPhase>& phases,
+             LoadedRxn* out, std::string* err) {
+  const std::string* gas = json_str(r, "gas-phase species");
+  const std::string* phase = json_str(r, "aerosol phase");
+  const std::string* aero = json_str(r, "aerosol-phase species");
+  const std::string* water = json_str(r, "aerosol-phase water");
+  if (!gas || !phase || !aero || !water) {
+    *err = "HL phase transfer reaction is missing a species, phase or water name";
+    return false;
+  }
+  std::vector<Inst> inst;
+  if (!instances_of(reps, phases, *phase, *aero, water, &inst, err)) return false;
+  const int n = (int)inst.size();
+  std::vector<int> ne(n);
+  int E = 0;
+  for (int x = 0; x < n; ++x) E += ne[x] = reps[inst[x].rep].num_jac_elem(phases, inst[x].phase_id);
+  std::vector<int>& I = out->ints;
+  std::vector<double>& F = out->floats;
+  I.assign(4 + 13 * n + 2 * E, 0);
+  F.assign(8 + n + 2 * E, 0.0);
+  I[0] = n;
+  auto g = gas_index.find(*gas);
+  if (g == gas_index.end()) {
+    *err = "Missing gas-phase species " + *gas;
+    return false;
+  }
+  I[1] = g->second;
+  int loc_i = 8 * n + 5, loc_f = 9;  // PHASE_INT_LOC_(1), PHASE_REAL_LOC_(1), 1-based
+  for (int x = 0; x < n; ++x) {
+    const Rep& rp = reps[inst[x].rep];
+    I[4 + 6 * n + x] = loc_i;
+    I[4 + 7 * n + x] = loc_f;
+    const int li = loc_i - 1;
+    I[li] = rp.state_id(inst[x].name);       // AERO_SPEC_
+    I[li + 1] = rp.state_id(inst[x].second);  // AERO_WATER_
+    I[li + 2] = inst[x].phase_id;             // AERO_PHASE_ID_
+    I[li + 3] = inst[x].rep + 1;              // AERO_REP_ID_
+    I[li + 4] = ne[x];                        // NUM_AERO_PHASE_JAC_ELEM_
+    loc_i += 5 + 2 * ne[x];
+    loc_f += 1 + 2 * ne[x];
+  }
+  bool ok = true;
+  double mw, gas_mw, dh, ds;
+  if (!db.spec.count(*aero) || !db.number(*aero, "molecular weight [kg mol-1]", &mw, err) ||
+      !db.number(*gas, "HLC(298K) [M Pa-1]", &F[4], err) ||
+      !db.number(*gas, "HLC exp factor [K]", &F[5], err) ||
+      !db.number(*gas, "diffusion coeff [m2 s-1]", &F[2], err) ||
+      !db.number(*gas, "molecular weight [kg mol-1]", &gas_mw, err))
+    return false;
+  n_star_terms(db, *gas, &dh, &ds, &ok);
+  if (!ok) {
+    *err = "non-numeric N star for species " + *gas;
+    return false;
+  }
+  F[0] = dh;
+  F[1] = ds;
+  F[3] = std::sqrt(8.0 * kGasConst / (kPi * gas_mw));
+  F[6] = kGasConst / mw * 1.0e6;
+  F[7] = mw;
+  out->type = kHl;
+  out->n_env = 4;
+  return true;
+}
+
+// WET_DEPOSITION over every instance of a phase
+// (src/rxns/rxn_wet_deposition.F90:172-254): RXN_ID_ NUM_SPEC_ REACT_(s)
+// DERIV_ID_(s) JAC_ID_(s); SCALING_
+bool pack_wet_deposition(const Json& r, const std::vector<Rep>& reps,
+                         const std::vector<LoadedPhase>& phases, LoadedRxn* out,
+                         std::string* err) {
+  const std::string* phase = json_str(r, "aerosol phase");
+  if (!phase) {
+    *err = "Wet deposition reaction is missing an aerosol phase";
+    return false;
+  }
+  std::vector<int> ids;
+  for (const Rep& rp : reps)
+    for (const std::string& un : rp.names(phases, phase, nullptr)) ids.push_back(rp.state_id(un));
+  if (ids.empty()) {
+    *err = "No aerosol phase instances for wet deposition of " + *phase;
+    return false;
+  }
+  const int ns = (int)ids.size();
+  out->ints.assign(2 + 3 * ns, 0);
+  out->ints[0] = -1;
+  out->ints[1] = ns;
+  for (int k = 0; k < ns; ++k) out->ints[2 + k] = ids[k];
+  bool ok = true;
+  const Json* sc = r.get("scaling factor");
+  out->floats = {sc ? SpeciesDb::as_number(*sc, &ok) : 1.0};
+  if (!ok) {
+    *err = "non-numeric wet deposition scaling factor";
+    return false;
+  }
+  out->type = kWetDeposition;
+  out->n_env = 2;
   return true;
 }
 
@@ -275,6 +737,8 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
   std::vector<Json> docs(files.size());
   SpeciesDb db;
   std::vector<std::pair<std::string, std::vector<const Json*>>> mechs;
+  std::vector<std::pair<std::string, std::vector<std::string>>> phase_json;
+  std::vector<const Json*> rep_json;
   bool have_rel = false;
   for (size_t f = 0; f < files.size(); ++f) {
     if (!read_json_file(files[f], &docs[f], err)) return false;
@@ -296,6 +760,27 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
         }
         if (const Json* rx = o.get("reactions"))
           for (const Json& r : rx->arr) list->push_back(&r);
+      } else if (type == "AERO_PHASE") {
+        // phases of the same name merge their species lists
+        const std::string name = o.get("name") ? o.get("name")->str : "";
+        std::vector<std::string>* list = nullptr;
+        for (auto& ph : phase_json)
+          if (ph.first == name) list = &ph.second;
+        if (!list) {
+          phase_json.push_back({name, {}});
+          list = &phase_json.back().second;
+        }
+        if (const Json* sp = o.get("species"))
+          for (const Json& j : sp->arr) list->push_back(j.str);
+      } else if (type.rfind("AERO_REP_", 0) == 0) {
+        if (type != "AERO_REP_MODAL_BINNED_MASS") {
+          *err = "aerosol representation " + type + " is not supported";
+          return false;
+        }
+        rep_json.push_back(&o);
+      } else if (type.rfind("SUB_MODEL_", 0) == 0) {
+        *err = "sub-model " + type + " is not supported";
+        return false;
       } else if (type == "RELATIVE_TOLERANCE") {
         bool ok = true;
         const double v = o.get("value") ? SpeciesDb::as_number(*o.get("value"), &ok) : 0.0;
@@ -325,11 +810,55 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
       return false;
     }
   }
+  // aerosol phases, then the representations' species after the gas phase
+  // (src/camp_core.F90:660-760), each representation's id its position
+  out->phases.clear();
+  for (const auto& ph : phase_json) {
+    LoadedPhase lp;
+    if (!pack_phase(ph.first, ph.second, db, &lp, err)) return false;
+    out->phases.push_back(std::move(lp));
+  }
+  std::vector<Rep> reps;
+  int next_state = (int)out->species.size() + 1;
+  for (const Json* o : rep_json) {
+    Rep rp;
+    if (!pack_modal_binned(*o, out->phases, next_state, &rp, err)) return false;
+    next_state += (int)rp.unique.size();
+    reps.push_back(std::move(rp));
+  }
+  out->reps.clear();
+  for (size_t i = 0; i < reps.size(); ++i) {
+    reps[i].data.ints[3] = (int)i + 1;  // AERO_REP_ID_ as set_id gives it
+    out->reps.push_back(reps[i].data);
+    for (const std::string& un : reps[i].unique) {
+      const std::string sp = un.substr(un.rfind('.') + 1);
+      bool ok = true;
+      out->species.push_back(un);
+      out->var_type.push_back(db.var_type(sp));
+      out->abs_tol.push_back(db.abs_tol(sp, &ok));
+      if (!ok) {
+        *err = "non-numeric absolute tolerance for species " + sp;
+        return false;
+      }
+    }
+  }
   out->rxns.clear();
   for (const auto& m : mechs)
     for (const Json* r : m.second) {
       LoadedRxn lr;
-      if (!pack_reaction(*r, gas_index, &lr, err)) return false;
+      const Json* jt = r->get("type");
+      const std::string type = jt ? jt->str : "";
+      bool done;
+      if (type == "SIMPOL_PHASE_TRANSFER")
+        done = pack_simpol(*r, db, gas_index, reps, out->phases, &lr, err);
+      else if (type == "HL_PHASE_TRANSFER")
+        done = pack_hl(*r, db, gas_index, reps, out->phases, &lr, err);
+      else if (type == "WET_DEPOSITION" && !reps.empty())
+        done = pack_wet_deposition(*r, reps, out->phases, &lr, err);
+      else
+        done = pack_reaction(*r, gas_index, &lr, err);
+      if (!done) return false;
+      if (const Json* jl = r->get("rxn id")) lr.label = jl->kind == Json::String ? jl->str : "";
       out->rxns.push_back(std::move(lr));
     }
   // reaction ids of the host-rate types: one sequence in mechanism order, as

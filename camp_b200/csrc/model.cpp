@@ -965,7 +965,7 @@ void Model::build_tables() {
       // SIMPOL and HL at their place in the mechanism: the gas gains
       // evaporation and loses condensation, the aerosol species the reverse
       // (src/rxns/rxn_SIMPOL_phase_transfer.c:414-446,
-      // src/rxns/rxn_HL_phase_transfer.c:313-328)
+      // src/rxns/rxn_HL_phase_transfer.c:323-339)
       for (; ks < t.n_simpol && simpol_[ks].rxn == (int)ri; ++ks) {
         const int base = t.n_rxn + 4 * ks;
         const int dg = deriv_ids_[simpol_[ks].gas], da = deriv_ids_[simpol_[ks].aero];
@@ -1024,7 +1024,7 @@ void Model::build_tables() {
   // SIMPOL and HL partials: losses (jg_ind -1) and unguarded productions
   // (-2) of the gas and aerosol rows against each other and, for SIMPOL,
   // every dependent element (src/rxns/rxn_SIMPOL_phase_transfer.c:615-744,
-  // total-mass branch; src/rxns/rxn_HL_phase_transfer.c:400-439)
+  // total-mass branch; src/rxns/rxn_HL_phase_transfer.c:412-439)
   for (int k = 0; k < t.n_simpol; ++k) {
     const SimpolInst& si = simpol_[k];
     const int p0 = t.si_part0[k];

@@ -177,6 +177,12 @@ class Model {
                     const double* floats, std::string* err);
   int n_aero_phase() const { return (int)aph_int_.size(); }
   int n_aero_rep() const { return (int)arep_int_.size(); }
+  // condensed data of phase / representation k (representations: the
+  // element counts are written at solver_initialize)
+  const std::vector<int>& aero_phase_int(int k) const { return aph_int_[k]; }
+  const std::vector<double>& aero_phase_float(int k) const { return aph_flt_[k]; }
+  const std::vector<int>& aero_rep_int(int k) const { return arep_int_[k]; }
+  const std::vector<double>& aero_rep_float(int k) const { return arep_flt_[k]; }
   // modes of every representation, (representation, section) in order: the
   // GMD / GSD host-set columns after the reaction columns
   const std::vector<std::pair<int, int>>& modes() const { return modes_; }

@@ -115,8 +115,9 @@ void rxn_wet_deposition_set_rate_update_data(void *update_data, int rxn_id,
 /* replace src/aero_phase_solver.c:175,210, src/aero_rep_solver.c:443,492,546
  * and src/sub_model_solver.c:413,468,509.  Aerosol phases and the
  * modal/binned mass representation (type 2) are solved with SIMPOL
- * partitioning (reaction type 10); other representation types and any
- * sub-model are rejected at solver_initialize. */
+ * (reaction type 10) and HL (type 6, constant aerosol-phase water)
+ * partitioning; other representation types and any sub-model are rejected
+ * at solver_initialize. */
 void aero_phase_add_condensed_data(int n_int_param, int n_float_param,
                                    int *int_param, double *float_param,
                                    void *solver_data);
@@ -288,7 +289,9 @@ int camp_b200_get_lu_order(void *solver_data, int *perm);
  * buffers), through the same device code the solver uses: rate constants
  * from env and the photolysis rates set for those cells, then f (production,
  * loss, net) and the solver Jacobian (CSC order of camp_b200_get_solver_jac,
- * production and loss parts) at time step h. */
+ * production and loss parts) at time step h.  Entries that no reaction can
+ * make non-zero (HL's partials over the mode's mass species, zero for the
+ * modal/binned representation) are output as zero; the LU leaves them out. */
 int camp_b200_eval_deriv(void *solver_data, const double *state, const double *env,
                          int n_cells, double h, double *r_p, double *r_l,
                          double *deriv);
@@ -331,15 +334,21 @@ void camp_b200_server_free(void *server);
 /* CAMP JSON input without the Fortran camp_core                            */
 /* ---------------------------------------------------------------------- */
 
-/* replaces the Fortran camp_core's input reading and reaction packing
+/* replaces the Fortran camp_core's input reading and packing
  * (src/camp_core.F90:303-798, src/chem_spec_data.F90, src/rxns/rxn_*.F90
- * initialize) for gas-phase mechanisms: reads CAMP JSON files (CHEM_SPEC,
- * MECHANISM and RELATIVE_TOLERANCE objects), orders the state (gas species
- * in order of first appearance), packs every reaction and calls solver_new
- * and rxn_add_condensed_data.  Reactions whose rate the host sets
- * (PHOTOLYSIS, FIRST_ORDER_LOSS, EMISSION) get the ids 1, 2, ... in
- * mechanism order.  WET_DEPOSITION needs aerosol phases and is rejected.  Then call solver_initialize (tolerances
- * from camp_b200_json_tolerances) and solver_run.  NULL on error. */
+ * initialize, src/aero_phase_data.F90:306-385,
+ * src/aero_reps/aero_rep_modal_binned_mass.F90:334-661): reads CAMP JSON
+ * files (CHEM_SPEC, MECHANISM, RELATIVE_TOLERANCE, AERO_PHASE and
+ * AERO_REP_MODAL_BINNED_MASS objects), orders the state (gas species in order
+ * of first appearance, then each representation's species), packs every
+ * reaction, phase and representation and calls solver_new,
+ * rxn_add_condensed_data, aero_phase_add_condensed_data and
+ * aero_rep_add_condensed_data.  Reactions whose rate the host sets
+ * (PHOTOLYSIS, FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION) get the ids
+ * 1, 2, ... in mechanism order, representations the ids 1, 2, ... in order.
+ * Other representation types and sub-models are rejected.  Then call
+ * solver_initialize (tolerances from camp_b200_json_tolerances) and
+ * solver_run.  NULL on error. */
 void *camp_b200_solver_from_json(const char *const *files, int n_files, int n_cells);
 int camp_b200_n_state_var(void *solver_data);
 /* name of state variable i into buf (NUL-terminated, truncated to buf_len);
@@ -351,6 +360,13 @@ int camp_b200_json_tolerances(void *solver_data, double *abs_tol, double *rel_to
 int camp_b200_get_var_type(void *solver_data, int *out);
 int camp_b200_rxn_float_data_size(void *solver_data);
 int camp_b200_get_rxn_float_data(void *solver_data, double *out);
+/* condensed data of aerosol phase (which 0) or representation (which 1)
+ * `index` as added (aero_phase_add_condensed_data /
+ * aero_rep_add_condensed_data; a representation's element counts are
+ * written at solver_initialize): sizes into n_int / n_float and, where
+ * non-NULL, the arrays; -1 for a bad index */
+int camp_b200_get_aero_data(void *solver_data, int which, int index, int *n_int,
+                            int *n_float, int *ints, double *floats);
 
 /* ---------------------------------------------------------------------- */
 /* Debug: finite-difference audit of the analytic Jacobian                  */

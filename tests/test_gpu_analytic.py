@@ -11,6 +11,8 @@ golden fixture, so the comparison checks the device integrator:
 
     A = exp(-k1 t),  B = k1 / (k2 - k1) (exp(-k1 t) - exp(-k2 t)),  C = 1 - A - B.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -130,3 +132,38 @@ def test_hl_closed_form(tmp_path, precision):
         assert s.solve(x, env, 0.0, t) == 0, s.cell_stats()["status"]
         out[c] = x[c, :2]
     np.testing.assert_allclose(out, truth(TIMES), rtol=1e-6, atol=1e-18)
+
+
+def test_hl_through_json_entry_point(tmp_path):
+    """The HL case read by the C++ JSON reader (camp_b200_solver_from_json:
+    phases, the modal representation and the HL reaction packed in C++),
+    its mode columns set through the representation's update data."""
+    import ctypes as C
+
+    from conftest import HL_ENV, HL_MODE, hl_case
+
+    from camp_b200 import _lib
+
+    _, y0, _, truth = hl_case(tmp_path)
+    lib = _lib.load()
+    paths = (C.c_char_p * 1)(os.path.join(str(tmp_path), "hl.json").encode())
+    n = 2
+    h = lib.camp_b200_solver_from_json(paths, 1, n)
+    assert h, _lib.last_error()
+    try:
+        lib.solver_initialize(h, np.array([1e-14, 1e-20, 1e-14]), 1e-10, 100000, 1000)
+        assert lib.camp_b200_is_ready(h), _lib.last_error()
+        for what, val in (("gmd", HL_MODE[0]), ("gsd", HL_MODE[1])):
+            ud = getattr(lib, f"aero_rep_modal_binned_mass_create_{what}_update_data")()
+            getattr(lib, f"aero_rep_modal_binned_mass_set_{what}_update_data")(ud, 1, 0, val)
+            for c in range(n):
+                rep_id = C.c_int(0)
+                lib.aero_rep_update_data(c, C.byref(rep_id), 2, ud, h)
+            lib.solver_free_update_data(ud)
+        state = np.ascontiguousarray(np.tile(y0, (n, 1)))
+        env = np.ascontiguousarray(np.tile(np.array(HL_ENV), (n, 1)))
+        assert lib.solver_run(h, state.reshape(-1), env.reshape(-1), 0.0, 30.0) == 0
+    finally:
+        lib.solver_free(h)
+    np.testing.assert_allclose(state[:, :2], np.tile(truth([30.0])[0], (n, 1)), rtol=1e-6,
+                               atol=1e-18)

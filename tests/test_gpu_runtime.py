@@ -42,15 +42,15 @@ def test_autotune_keeps_results(cb05):
     np.testing.assert_allclose(out, ref, rtol=RTOL, atol=0)
 
 
-def test_serving_mix_equals_alone(cb05, mod37):
-    """Columns of cb05cl_ae5 and of the mod37 gas phase (with deposition and
-    emissions), 10-200 cells and host steps of 60/300/900 s submitted back to
-    back; each result equals the same column solved alone through
-    solver_run."""
+def test_serving_mix_equals_alone(cb05, mod37_aero):
+    """Columns of cb05cl_ae5 and of mod37 with its aerosol chemistry
+    (deposition, emissions, SIMPOL and HL partitioning, per-cell mode GMD /
+    GSD), 10-200 cells and host steps of 60/300/900 s submitted back to back;
+    each result equals the same column solved alone through solver_run."""
     from camp_b200.cells import make_cells, photo_base_rates
     from camp_b200.serve import Server
 
-    mechs = [(cb05, photo_base_rates(cb05)), (mod37, photo_base_rates(mod37))]
+    mechs = [(cb05, photo_base_rates(cb05)), (mod37_aero, photo_base_rates(mod37_aero))]
     solvers = [_solver(m, 200) for m, _ in mechs]
     server = Server(n_slots=6, device_mb=512, host_mb=128)
     ids = [server.add_solver(s) for s in solvers]

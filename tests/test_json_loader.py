@@ -21,11 +21,12 @@ def _cpp_solver(files, n_cells=2):
     return lib, h
 
 
-def _compare(files):
+def _compare(files, aerosol=False):
+    from camp_b200.aerosol import load_aerosol_mechanism
     from camp_b200.mechanism import load_mechanism
     from camp_b200.solver import Solver
 
-    mech = load_mechanism(files)
+    mech = load_aerosol_mechanism(files) if aerosol else load_mechanism(files)
     lib, h = _cpp_solver(files)
     try:
         ns = lib.camp_b200_n_state_var(h)
@@ -57,6 +58,19 @@ def _compare(files):
         lib.camp_b200_get_rxn_float_data(h, fa)
         py.lib.camp_b200_get_rxn_float_data(py._h, fb)
         np.testing.assert_array_equal(fa, fb)
+        # aerosol phases and representations as added
+        for which, objs in ((0, mech.aero_phases), (1, mech.aero_reps)):
+            for k, o in enumerate(objs):
+                ni_, nf_ = C.c_int(), C.c_int()
+                assert lib.camp_b200_get_aero_data(h, which, k, C.byref(ni_), C.byref(nf_),
+                                                   None, None) == 0
+                ia, fa_ = np.zeros(ni_.value, np.int32), np.zeros(nf_.value)
+                lib.camp_b200_get_aero_data(h, which, k, None, None, ia.ctypes.data,
+                                            fa_.ctypes.data)
+                np.testing.assert_array_equal(ia, o.ints)
+                np.testing.assert_array_equal(fa_, o.floats)
+            assert lib.camp_b200_get_aero_data(h, which, len(objs), None, None, None,
+                                               None) == -1
         py.free()
     finally:
         lib.solver_free(h)
@@ -163,3 +177,77 @@ def test_errors_are_reported(tmp_path):
     arr = (C.c_char_p * 1)(p.encode())
     assert not lib.camp_b200_solver_from_json(arr, 1, 1)
     assert "Missing species: X" in _lib.last_error()
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_MOD37), reason="reference tree not present")
+def test_mod37_aerosol_from_reference_files():
+    """The shipped mod37 files with the SOA scheme, aerosol phases, the
+    MONARCH modal/binned representation (7 modes and bin sets), the wet
+    deposition of cloud and rain water and its 35 HL partitioning
+    reactions."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import MOD37_AERO_FILES
+
+    _compare([os.path.join(REF_MOD37, f) for f in MOD37_AERO_FILES], aerosol=True)
+
+
+def test_aerosol_options(tmp_path):
+    """A mode and LINEAR / LOG bin sets over two phases, a phase split over
+    two objects, SIMPOL with an activity coefficient and with N*, HL and
+    WET_DEPOSITION over every instance of a phase, species merged across
+    files."""
+    doc = {"camp-data": [
+        {"name": "G1", "type": "CHEM_SPEC", "molecular weight [kg mol-1]": 0.1,
+         "diffusion coeff [m2 s-1]": 1.0e-5, "N star": 2.5},
+        {"name": "G2", "type": "CHEM_SPEC", "molecular weight [kg mol-1]": 0.05,
+         "diffusion coeff [m2 s-1]": 1.2e-5, "HLC(298K) [M Pa-1]": 3.0e-4,
+         "HLC exp factor [K]": 0.0},
+        {"name": "O1", "type": "CHEM_SPEC", "phase": "AEROSOL",
+         "molecular weight [kg mol-1]": 0.15, "density [kg m-3]": 1400.0},
+        {"name": "W", "type": "CHEM_SPEC", "phase": "AEROSOL", "tracer type": "CONSTANT",
+         "molecular weight [kg mol-1]": 0.018, "density [kg m-3]": 1000.0,
+         "absolute integration tolerance": 1e-5},
+        {"name": "X", "type": "CHEM_SPEC", "phase": "AEROSOL",
+         "molecular weight [kg mol-1]": 0.05, "density [kg m-3]": 1000.0},
+        {"name": "GAM", "type": "CHEM_SPEC", "tracer type": "ACTIVITY_COEFF", "phase": "AEROSOL"},
+        {"name": "org", "type": "AERO_PHASE", "species": ["O1"]},
+        {"name": "aq", "type": "AERO_PHASE", "species": ["W", "X"]},
+        {"name": "org", "type": "AERO_PHASE", "species": ["GAM"]},
+        {"name": "rep", "type": "AERO_REP_MODAL_BINNED_MASS", "modes/bins": {
+            "fine": {"type": "MODAL", "phases": ["org", "aq"], "shape": "LOG_NORMAL",
+                     "geometric mean diameter [m]": 1.0e-7, "geometric standard deviation": 1.8},
+            "lin": {"type": "BINNED", "phases": ["aq"], "bins": 3, "scale": "LINEAR",
+                    "minimum diameter [m]": 1.0e-6, "maximum diameter [m]": 5.0e-6},
+            "log": {"type": "BINNED", "phases": ["org", "aq"], "bins": 4, "scale": "LOG",
+                    "minimum diameter [m]": 1.0e-8, "maximum diameter [m]": 1.0e-5}}},
+        {"name": "m", "type": "MECHANISM", "reactions": [
+            {"type": "ARRHENIUS", "reactants": {"G1": {}}, "products": {"G2": {}}, "A": 1e-3},
+            {"type": "SIMPOL_PHASE_TRANSFER", "gas-phase species": "G1", "aerosol phase": "org",
+             "aerosol-phase species": "O1", "aerosol-phase activity coefficient": "GAM",
+             "B": [-1.97e3, 2.91, 1.96e-3, -0.496]},
+            {"type": "HL_PHASE_TRANSFER", "gas-phase species": "G2", "aerosol phase": "aq",
+             "aerosol-phase species": "X", "aerosol-phase water": "W", "rxn id": "hl"},
+            {"type": "WET_DEPOSITION", "aerosol phase": "aq", "scaling factor": 0.5},
+            {"type": "PHOTOLYSIS", "reactants": {"G2": {}}, "products": {"G1": {}}},
+        ]},
+    ]}
+    p = os.path.join(tmp_path, "aero.json")
+    with open(p, "w") as fh:
+        json.dump(doc, fh)
+    _compare([p], aerosol=True)
+
+
+@pytest.mark.parametrize("obj", [
+    {"name": "sp", "type": "AERO_REP_SINGLE_PARTICLE"},
+    {"name": "zsr", "type": "SUB_MODEL_ZSR_AEROSOL_WATER"},
+])
+def test_unsupported_aerosol_objects(tmp_path, obj):
+    p = os.path.join(tmp_path, "x.json")
+    with open(p, "w") as fh:
+        json.dump({"camp-data": [{"name": "A", "type": "CHEM_SPEC"}, obj]}, fh)
+    lib = _lib.load()
+    arr = (C.c_char_p * 1)(p.encode())
+    assert not lib.camp_b200_solver_from_json(arr, 1, 1)
+    assert obj["type"] in _lib.last_error()
