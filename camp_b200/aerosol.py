@@ -18,14 +18,16 @@ What is restated, from the reference's Fortran:
 * ``rxn_SIMPOL_phase_transfer_t%initialize``
   (``src/rxns/rxn_SIMPOL_phase_transfer.F90:220-470``),
   ``rxn_HL_phase_transfer_t%initialize``
-  (``src/rxns/rxn_HL_phase_transfer.F90:170-398``) and the WET_DEPOSITION
+  (``src/rxns/rxn_HL_phase_transfer.F90:170-398``),
+  ``rxn_aqueous_equilibrium_t%initialize``
+  (``src/rxns/rxn_aqueous_equilibrium.F90:170-493``) and the WET_DEPOSITION
   packer over every instance of a phase
   (``src/rxns/rxn_wet_deposition.F90:172-254``).
 
 Aerosol-representation ids (``AERO_REP_ID_``) are given 1, 2, ... as a host
 does through ``set_id`` before it creates GMD/GSD update data.  Other aerosol
-types (single particle, aqueous equilibrium, condensed-phase reactions,
-sub-models) are not packed here.
+types (single particle, condensed-phase reactions, sub-models) are not
+packed here.
 """
 from __future__ import annotations
 
@@ -42,6 +44,7 @@ from .mechanism import (CHEM_SPEC_ACTIVITY_COEFF, CHEM_SPEC_CONSTANT, CHEM_SPEC_
 
 AERO_REP_MODAL_BINNED_MASS = 2  # src/aero_rep_solver.c:20
 RXN_HL_PHASE_TRANSFER = 6       # src/rxn_solver.c:24
+RXN_AQUEOUS_EQUILIBRIUM = 7     # src/rxn_solver.c:25
 RXN_SIMPOL_PHASE_TRANSFER = 10  # src/rxn_solver.c:26
 BINNED, MODAL = 1, 2            # src/aero_reps/aero_rep_modal_binned_mass.c:25-26
 UNIV_GAS_CONST = 8.314472       # src/constants.F90
@@ -383,6 +386,89 @@ def pack_hl(rxn: dict, db: _SpeciesDB, gas_index: dict[str, int], reps: list[Aer
     return PackedRxn(RXN_HL_PHASE_TRANSFER, ints, floats, 4, str(rxn.get("rxn id", "")))
 
 
+def pack_aqueous_equilibrium(rxn: dict, db: _SpeciesDB, reps: list[AeroRep],
+                             phases: list[AeroPhase]) -> PackedRxn:
+    """AQUEOUS_EQUILIBRIUM (src/rxns/rxn_aqueous_equilibrium.F90:170-493).
+
+    ints: ``[NUM_REACT_, NUM_PROD_, NUM_AERO_PHASE_, REACT_(phase, r),
+    PROD_(phase, p), WATER_(phase), ACTIVITY_COEFF_(phase), DERIV_ID_ ...,
+    JAC_ID_ ...]``; floats: ``[A_, C_, RATE_CONST_REVERSE_, WATER_CONC_,
+    ACTIVITY_COEFF_VALUE_, MASS_FRAC_TO_M_(r, p), REACT_CONC_(r),
+    PROD_CONC_(p), SMALL_WATER_CONC_(phase), SMALL_CONC_(phase)]``; one env
+    parameter (the forward rate constant)."""
+    phase = rxn["aerosol phase"]
+    water = rxn.get("aerosol-phase water")
+    if water is None:
+        raise ValueError("Missing aerosol-phase water for aqueous equilibrium reaction")
+
+    def expand(block: dict) -> list[str]:
+        out = []
+        for name, props in (block or {}).items():
+            out.extend([name] * int((props or {}).get("qty", 1)))
+        return out
+
+    react, prod = expand(rxn.get("reactants")), expand(rxn.get("products"))
+    nr, np_ = len(react), len(prod)
+    ns = nr + np_
+    present = [ri for ri, rep in enumerate(reps) if rep.phase_ids(phases, phase)]
+    n_phase = sum(len(reps[ri].names(phases, phase, water)) for ri in present)
+    if n_phase == 0:
+        raise ValueError(f"No aerosol phase '{phase}' present.")
+    ints = np.zeros(3 + n_phase * (ns * (ns + 4) + 2), np.int32)
+    floats = np.zeros(5 + 2 * ns + 2 * n_phase, np.float64)
+    ints[0], ints[1], ints[2] = nr, np_, n_phase
+    floats[0] = float(rxn.get("A", 1.0))
+    floats[1] = float(rxn.get("C", 0.0))
+    if "k_reverse" not in rxn:
+        raise ValueError("Missing 'k_reverse' for aqueous equilibrium reaction")
+    kr = float(rxn["k_reverse"])
+    if str(rxn.get("time_unit", "")).strip() == "MIN":
+        kr = kr / 60.0
+    floats[2] = kr
+    for k, name in enumerate(react + prod):
+        if name not in db.props or "molecular weight [kg mol-1]" not in db.props[name]:
+            raise KeyError(f"Missing 'molecular weight' for species '{name}' in aqueous "
+                           f"equilibrium reaction.")
+        floats[5 + k] = 1.0e3 / float(db.props[name]["molecular weight [kg mol-1]"])
+    ion_pair = rxn.get("ion pair", "")
+    o_prod = 3 + nr * n_phase
+    o_water = 3 + ns * n_phase
+    o_act = o_water + n_phase
+    base = 0
+    for ri in present:
+        rep = reps[ri]
+        wn = rep.names(phases, phase, water)
+        k = len(wn)
+        for j in range(k):
+            ints[o_water + base + j] = rep.state_id(wn[j])
+        if ion_pair:
+            an = rep.names(phases, phase, ion_pair)
+            if len(an) != k:
+                raise ValueError(f"Incorrect instances of ion pair '{ion_pair}' in phase "
+                                 f"'{phase}' in an aqueous equilibrium reaction")
+            if db.var_type_of(ion_pair) != CHEM_SPEC_ACTIVITY_COEFF:
+                raise ValueError(f"Ion pair '{ion_pair}' must have type 'ION_PAIR' to be used "
+                                 f"as an ion pair in an aqueous equilibrium reaction.")
+            for j in range(k):
+                ints[o_act + base + j] = rep.state_id(an[j])
+        for i, name in enumerate(react):
+            un = rep.names(phases, phase, name)
+            if len(un) != k:
+                raise ValueError(f"Incorrect instances of reactant '{name}' in phase '{phase}' "
+                                 f"in an aqueous equilibrium reaction")
+            for j in range(k):
+                ints[3 + (base + j) * nr + i] = rep.state_id(un[j])
+        for i, name in enumerate(prod):
+            un = rep.names(phases, phase, name)
+            if len(un) != k:
+                raise ValueError(f"Incorrect instances of product '{name}' in phase '{phase}' "
+                                 f"in an aqueous equilibrium reaction")
+            for j in range(k):
+                ints[o_prod + (base + j) * np_ + i] = rep.state_id(un[j])
+        base += k
+    return PackedRxn(RXN_AQUEOUS_EQUILIBRIUM, ints, floats, 1, str(rxn.get("rxn id", "")))
+
+
 def pack_wet_deposition_phase(rxn: dict, reps: list[AeroRep],
                               phases: list[AeroPhase]) -> PackedRxn:
     from .mechanism import pack_wet_deposition
@@ -456,6 +542,8 @@ def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mec
                 rxns.append(pack_simpol(r, db, gas_index, reps, phases))
             elif r["type"] == "HL_PHASE_TRANSFER":
                 rxns.append(pack_hl(r, db, gas_index, reps, phases))
+            elif r["type"] == "AQUEOUS_EQUILIBRIUM":
+                rxns.append(pack_aqueous_equilibrium(r, db, reps, phases))
             elif r["type"] == "WET_DEPOSITION":
                 rxns.append(pack_wet_deposition_phase(r, reps, phases))
             else:

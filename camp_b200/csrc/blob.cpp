@@ -52,7 +52,8 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     *err = "more than 1023 dependent variables";
     return false;
   }
-  if (t.n_rates > 65535 || t.n_part_all > 65535 || t.n_lu > 65535 || t.n_jac > 65535 ||
+  if (t.n_rates > 65535 || t.n_keff > 65535 || t.n_part_all > 65535 || t.n_lu > 65535 ||
+      t.n_jac > 65535 ||
       (int)t.fg_rxn.size() > 65535 || (int)t.jg_part.size() > 65535 ||
       (int)t.fa_pos.size() > 65535) {
     *err = "mechanism exceeds the 16-bit table encodings";
@@ -331,6 +332,38 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.si_rec = w.put(si_rec);
   o.si_elem = w.put(si_elem);
   o.si_ef = w.put(si_ef);
+  // aqueous equilibrium instance records
+  std::vector<uint16_t> aq_rec, aq_sp;
+  std::vector<double> aq_sm;
+  for (int k = 0; k < t.n_aq; ++k) {
+    const AqInst& q = t.aq[k];
+    const int first = (int)aq_sp.size();
+    int S = 0, R = 0;
+    const auto dep_of = [&](int st) {
+      const int d = (int)(std::lower_bound(t.dep_state.begin(), t.dep_state.end(), st) -
+                          t.dep_state.begin());
+      return d < n && t.dep_state[d] == st ? d : -1;
+    };
+    for (int pass = 0; pass < 2; ++pass) {
+      const std::vector<int>& list = pass == 0 ? q.react : q.prod;
+      for (size_t i = 0; i < list.size(); ++i) {
+        const int d = dep_of(list[i]);
+        if (d < 0) continue;
+        aq_sp.push_back((uint16_t)d);
+        aq_sm.push_back(q.m2m[(pass == 0 ? 0 : q.react.size()) + i]);
+        ++S;
+        R += pass == 0;
+      }
+    }
+    const uint16_t rec[8] = {(uint16_t)S, (uint16_t)R, (uint16_t)first,
+                             (uint16_t)t.aq_rate0[k], (uint16_t)t.aq_part0[k],
+                             (uint16_t)t.aq_keff0[k], 0, 0};
+    aq_rec.insert(aq_rec.end(), rec, rec + 8);
+  }
+  o.n_aq = t.n_aq;
+  o.aq_rec = w.put(aq_rec);
+  o.aq_sp = w.put(aq_sp);
+  o.aq_sm = w.put(aq_sm);
   o.n_plev = t.n_plev;
   o.lu_perm = w.put(u16(t.lu_perm));
   o.lu_src = w.put(lu_src);
@@ -376,8 +409,9 @@ namespace campb {
 
 bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
                      std::vector<uint8_t>* blob, LaneOff* off, std::string* err) {
-  if (t.n_simpol > 0) {
-    *err = "the lane-per-cell kernel does not evaluate SIMPOL or HL phase transfer";
+  if (t.n_simpol > 0 || t.n_aq > 0) {
+    *err = "the lane-per-cell kernel does not evaluate SIMPOL, HL or aqueous equilibrium "
+           "reactions";
     return false;
   }
   const int n = t.n;

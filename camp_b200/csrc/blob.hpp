@@ -55,6 +55,10 @@ struct BlobOff {
   // its 8 per-cell constants the terms' rate constants.
   int n_simpol, n_keff, n_rates, n_part_all;
   int si_rec, si_elem, si_ef;
+  // aqueous equilibrium instances: record (uint16 x 8: dependent slots,
+  // dependent reactant slots, first slot, first pseudo-rate, first partial,
+  // keff slot), per slot its dependent index (uint16) and 1e3 / MW (double)
+  int n_aq, aq_rec, aq_sp, aq_sm;
   // J gather with unguarded products (SIMPOL): they lead each slot, and
   // jg_umid (uint16 per slot) is the slot's first loss entry
   int has_ug, jg_umid;

@@ -295,6 +295,7 @@ void solver_initialize(void* solver_data, double* abs_tol, double rel_tol, int m
     return;
   }
   std::string err;
+  s->model->set_abs_tol(abs_tol);
   if (!s->model->build(&err)) {
     set_error("solver_initialize: " + err);
     return;

@@ -16,7 +16,7 @@ constexpr int kUnknown = 0, kVariable = 1, kConstant = 2, kPssa = 3, kActivity =
 // reaction type ids, src/rxn_solver.c:19-35
 constexpr int kArrhenius = 1, kTroe = 2, kCmaqH2O2 = 3, kCmaqOHHNO3 = 4, kPhotolysis = 5;
 constexpr int kFirstOrderLoss = 12, kEmission = 13, kWetDeposition = 14;
-constexpr int kHl = 6, kSimpol = 10;
+constexpr int kHl = 6, kAqueous = 7, kSimpol = 10;
 // aerosol representation and section types,
 // src/aero_rep_solver.c:20, src/aero_reps/aero_rep_modal_binned_mass.c:25-26
 constexpr int kModalBinned = 2, kBinned = 1, kModal = 2;
@@ -679,6 +679,112 @@ bool pack_hl(const Json& r, const SpeciesDb& db, const std::map<std::string, int
   return true;
 }
 
+// rxn_aqueous_equilibrium_t%initialize
+// (src/rxns/rxn_aqueous_equilibrium.F90:170-493): reactant and product
+// names (qty expanded), 1e3 / MW of each, and per phase instance the state
+// ids of reactants, products, water and ion pair
+bool pack_aqueous(const Json& r, const SpeciesDb& db, const std::vector<Rep>& reps,
+                  const std::vector<LoadedPhase>& phases, LoadedRxn* out, std::string* err) {
+  const std::string* phase = json_str(r, "aerosol phase");
+  const std::string* water = json_str(r, "aerosol-phase water");
+  if (!phase || !water) {
+    *err = "Missing aerosol phase or aerosol-phase water for aqueous equilibrium reaction";
+    return false;
+  }
+  bool ok = true;
+  auto expand = [&](const char* key) {
+    std::vector<std::string> names;
+    if (const Json* b = r.get(key))
+      for (const auto& kv : b->obj) {
+        int qty = 1;
+        if (const Json* q = kv.second.get("qty")) qty = (int)SpeciesDb::as_number(*q, &ok);
+        for (int k = 0; k < qty; ++k) names.push_back(kv.first);
+      }
+    return names;
+  };
+  const std::vector<std::string> react = expand("reactants"), prod = expand("products");
+  const int nr = (int)react.size(), np = (int)prod.size(), ns = nr + np;
+  std::vector<int> present;
+  int P = 0;
+  for (size_t ri = 0; ri < reps.size(); ++ri)
+    if (!reps[ri].phase_ids(phases, *phase).empty()) {
+      present.push_back((int)ri);
+      P += (int)reps[ri].names(phases, phase, water).size();
+    }
+  if (P == 0) {
+    *err = "No aerosol phase '" + *phase + "' present.";
+    return false;
+  }
+  std::vector<int>& I = out->ints;
+  std::vector<double>& F = out->floats;
+  I.assign(3 + P * (ns * (ns + 4) + 2), 0);
+  F.assign(5 + 2 * ns + 2 * P, 0.0);
+  I[0] = nr;
+  I[1] = np;
+  I[2] = P;
+  const Json* ja = r.get("A");
+  const Json* jc = r.get("C");
+  const Json* jk = r.get("k_reverse");
+  if (!jk) {
+    *err = "Missing 'k_reverse' for aqueous equilibrium reaction";
+    return false;
+  }
+  F[0] = ja ? SpeciesDb::as_number(*ja, &ok) : 1.0;
+  F[1] = jc ? SpeciesDb::as_number(*jc, &ok) : 0.0;
+  F[2] = SpeciesDb::as_number(*jk, &ok);
+  const std::string* tu = json_str(r, "time_unit");
+  if (tu && *tu == "MIN") F[2] = F[2] / 60.0;
+  for (int k = 0; k < ns; ++k) {
+    const std::string& name = k < nr ? react[k] : prod[k - nr];
+    double mw;
+    if (!db.spec.count(name) || !db.number(name, "molecular weight [kg mol-1]", &mw, err)) {
+      *err = "Missing 'molecular weight' for species '" + name +
+             "' in aqueous equilibrium reaction.";
+      return false;
+    }
+    F[5 + k] = 1.0e3 / mw;
+  }
+  const std::string* ion = json_str(r, "ion pair");
+  const int o_prod = 3 + nr * P, o_water = 3 + ns * P, o_act = o_water + P;
+  int base = 0;
+  for (int ri : present) {
+    const Rep& rp = reps[ri];
+    const std::vector<std::string> wn = rp.names(phases, phase, water);
+    const int k = (int)wn.size();
+    for (int j = 0; j < k; ++j) I[o_water + base + j] = rp.state_id(wn[j]);
+    if (ion && !ion->empty()) {
+      const std::vector<std::string> an = rp.names(phases, phase, ion);
+      if ((int)an.size() != k || !db.spec.count(*ion) || db.var_type(*ion) != kActivity) {
+        *err = "Ion pair '" + *ion + "' must have type 'ION_PAIR' and one instance per phase "
+               "instance in an aqueous equilibrium reaction";
+        return false;
+      }
+      for (int j = 0; j < k; ++j) I[o_act + base + j] = rp.state_id(an[j]);
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      const std::vector<std::string>& names = pass == 0 ? react : prod;
+      const int n = pass == 0 ? nr : np, o = pass == 0 ? 3 : o_prod;
+      for (int i = 0; i < n; ++i) {
+        const std::vector<std::string> un = rp.names(phases, phase, &names[i]);
+        if ((int)un.size() != k) {
+          *err = "Incorrect instances of '" + names[i] + "' in phase '" + *phase +
+                 "' in an aqueous equilibrium reaction";
+          return false;
+        }
+        for (int j = 0; j < k; ++j) I[o + (base + j) * n + i] = rp.state_id(un[j]);
+      }
+    }
+    base += k;
+  }
+  if (!ok) {
+    *err = "non-numeric aqueous equilibrium parameter";
+    return false;
+  }
+  out->type = kAqueous;
+  out->n_env = 1;
+  return true;
+}
+
 // WET_DEPOSITION over every instance of a phase
 // (src/rxns/rxn_wet_deposition.F90:172-254): RXN_ID_ NUM_SPEC_ REACT_(s)
 // DERIV_ID_(s) JAC_ID_(s); SCALING_
@@ -853,6 +959,8 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
         done = pack_simpol(*r, db, gas_index, reps, out->phases, &lr, err);
       else if (type == "HL_PHASE_TRANSFER")
         done = pack_hl(*r, db, gas_index, reps, out->phases, &lr, err);
+      else if (type == "AQUEOUS_EQUILIBRIUM")
+        done = pack_aqueous(*r, db, reps, out->phases, &lr, err);
       else if (type == "WET_DEPOSITION" && !reps.empty())
         done = pack_wet_deposition(*r, reps, out->phases, &lr, err);
       else

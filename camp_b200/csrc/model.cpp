@@ -22,6 +22,7 @@ bool type_layout(int type, int* n_int_prop, int* n_float_prop) {
     case RXN_WET_DEPOSITION: *n_int_prop = 2; *n_float_prop = 1; return true;
     case RXN_SIMPOL_PHASE_TRANSFER: *n_int_prop = 2; *n_float_prop = 10; return true;
     case RXN_HL_PHASE_TRANSFER: *n_int_prop = 2; *n_float_prop = 8; return true;
+    case RXN_AQUEOUS_EQUILIBRIUM: *n_int_prop = 3; *n_float_prop = 5; return true;
     default: return false;
   }
 }
@@ -87,8 +88,8 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
   if (!type_layout(type, &r.n_int_prop, &r.n_float_prop))
     return fail("reaction type " + std::to_string(type) +
                 " is not supported (ARRHENIUS, TROE, CMAQ_H2O2, CMAQ_OH_HNO3, PHOTOLYSIS, "
-                "FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION, SIMPOL_PHASE_TRANSFER and "
-                "HL_PHASE_TRANSFER only)");
+                "FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION, SIMPOL_PHASE_TRANSFER, "
+                "HL_PHASE_TRANSFER and AQUEOUS_EQUILIBRIUM only)");
   const std::string malformed = "malformed packed data for reaction " + std::to_string(idx);
   if (n_int < r.n_int_prop || n_float < r.n_float_prop) return fail(malformed);
   const int o = r.int_off;  // rxn_int_ position of ints[0]
@@ -134,6 +135,21 @@ bool Model::add_rxn(int type, int n_int, int n_float, int n_env,
       if (na < 1 || n_int < 4 + 13 * na) return fail(malformed);
       if (ints[1] < 1 || ints[1] > n_state_)
         return fail("species index out of range in reaction " + std::to_string(idx));
+      break;
+    }
+    case RXN_AQUEOUS_EQUILIBRIUM: {  // src/rxns/rxn_aqueous_equilibrium.c:27-56
+      // resolved into instances at solver_initialize
+      const int nr = ints[0], np = ints[1], P = ints[2], ns = nr + np;
+      if (nr < 1 || np < 1 || P < 1 || n_int < 3 + P * (ns * (ns + 4) + 2) ||
+          n_float < 5 + 2 * ns + 2 * P)
+        return fail(malformed);
+      for (int x = 0; x < P * (ns + 2); ++x) {  // reactants, products, water, activity
+        const int sp = ints[3 + x];
+        const bool act = x >= P * (ns + 1);
+        if (act && sp == 0) continue;  // no ion pair
+        if (sp < 1 || sp > n_state_)
+          return fail("species index out of range in reaction " + std::to_string(idx));
+      }
       break;
     }
     default: {  // NUM_REACT_ NUM_PROD_ [RXN_ID_] REACT_ PROD_ DERIV_ID_ JAC_ID_, yields
@@ -262,7 +278,59 @@ struct HlView {
   int nelem(int x) const { return I[iloc(x) + 4]; }
   int& phase_jac(int x, int set, int e) const { return I[iloc(x) + 5 + set * nelem(x) + e]; }
 };
+// views of the packed aqueous equilibrium data, 0-based within the
+// reaction's ints and floats (src/rxns/rxn_aqueous_equilibrium.c:27-56)
+struct AqView {
+  int* I;
+  const double* F;
+  int nr() const { return I[0]; }
+  int np() const { return I[1]; }
+  int P() const { return I[2]; }
+  int react(int x) const { return I[3 + x] - 1; }
+  int prod(int x) const { return I[3 + nr() * P() + x] - 1; }
+  int water(int x) const { return I[3 + (nr() + np()) * P() + x] - 1; }
+  int act(int x) const { return I[3 + (nr() + np() + 1) * P() + x] - 1; }
+  int& deriv(int x) const { return I[3 + (nr() + np() + 2) * P() + x]; }
+  int& jac(int x) const { return I[3 + (2 * (nr() + np()) + 2) * P() + x]; }
+  double m2m(int x) const { return F[5 + x]; }
+};
 }  // namespace
+
+// Aqueous equilibrium instances (one per phase instance of a reaction).
+// The water and the ion pair's activity coefficient must be constant
+// species: the reference's partials over them
+// (src/rxns/rxn_aqueous_equilibrium.c:497-540) then fall outside the solver
+// Jacobian, and per cell they are constants.
+bool Model::resolve_aq(std::string* err) {
+  aq_.clear();
+  for (size_t ri = 0; ri < rxns_.size(); ++ri) {
+    const Rxn& r = rxns_[ri];
+    if (r.type != RXN_AQUEOUS_EQUILIBRIUM) continue;
+    AqView v{&rxn_int_[r.int_off], &rxn_float_[r.float_off]};
+    for (int p = 0; p < v.P(); ++p) {
+      AqInst q;
+      q.rxn = (int)ri;
+      q.p = p;
+      for (int i = 0; i < v.nr(); ++i) q.react.push_back(v.react(p * v.nr() + i));
+      for (int i = 0; i < v.np(); ++i) q.prod.push_back(v.prod(p * v.np() + i));
+      for (int i = 0; i < v.nr() + v.np(); ++i) q.m2m.push_back(v.m2m(i));
+      q.water = v.water(p);
+      q.act = v.act(p);
+      q.A = v.F[0];
+      q.C = v.F[1];
+      q.kr = v.F[2];
+      if (var_type_[q.water] == VAR_VARIABLE || (q.act >= 0 && var_type_[q.act] == VAR_VARIABLE)) {
+        *err = "aqueous equilibrium reaction " + std::to_string(ri) +
+               ": the aerosol-phase water and the ion pair must be constant (not variable) "
+               "state variables";
+        return false;
+      }
+      q.thr = abs_tol_.empty() ? 0.0 : 1.0e-4 * (abs_tol_[q.water] / 10.0);
+      aq_.push_back(q);
+    }
+  }
+  return true;
+}
 
 // Locates phase instance `phase` of representation si->rep the way the
 // representation's C functions walk it (sections, then bins, then the phases
@@ -465,6 +533,20 @@ void Model::build_rxn_jacobian() {
       add(si.aero, e, !hl);
     }
   }
+  // aqueous equilibrium (src/rxns/rxn_aqueous_equilibrium.c:70-127): the
+  // forward and reverse mass-action pairs, water and activity coefficient
+  for (const AqInst& q : aq_) {
+    for (const std::vector<int>* ind : {&q.react, &q.prod})
+      for (int i : *ind) {
+        for (int d : q.react) add(d, i, true);
+        for (int d : q.prod) add(d, i, true);
+      }
+    for (int d : q.react) add(d, q.water, true);
+    for (int d : q.prod) add(d, q.water, true);
+    if (q.act < 0) continue;
+    for (int d : q.react) add(d, q.act, true);
+    for (int d : q.prod) add(d, q.act, true);
+  }
   reg.to_csc(&rj_colptr_, &rj_rowid_);
   live.to_csc(&rl_colptr_, &rl_rowid_);
 }
@@ -512,6 +594,27 @@ void Model::update_ids() {
         if (v.phase_jac(x, 0, e) > 0) v.phase_jac(x, 0, e) = rxn_elem_id(g, v.phase_jac(x, 0, e));
         if (v.phase_jac(x, 1, e) > 0) v.phase_jac(x, 1, e) = rxn_elem_id(a, v.phase_jac(x, 1, e));
       }
+    }
+  }
+  // aqueous equilibrium (src/rxns/rxn_aqueous_equilibrium.c:132-209; the
+  // small concentrations it also sets are kept per instance, AqInst::thr)
+  for (const Rxn& r : rxns_) {
+    if (r.type != RXN_AQUEOUS_EQUILIBRIUM) continue;
+    AqView v{&rxn_int_[r.int_off], &rxn_float_[r.float_off]};
+    const int nr = v.nr(), np = v.np();
+    int id = 0, ij = 0;
+    for (int p = 0; p < v.P(); ++p) {
+      for (int i = 0; i < nr; ++i) v.deriv(id++) = deriv_ids_[v.react(p * nr + i)];
+      for (int i = 0; i < np; ++i) v.deriv(id++) = deriv_ids_[v.prod(p * np + i)];
+    }
+    for (int p = 0; p < v.P(); ++p) {
+      std::vector<int> dep;
+      for (int i = 0; i < nr; ++i) dep.push_back(v.react(p * nr + i));
+      for (int i = 0; i < np; ++i) dep.push_back(v.prod(p * np + i));
+      for (int ind : dep)
+        for (int d : dep) v.jac(ij++) = rxn_elem_id(d, ind);
+      for (int d : dep) v.jac(ij++) = rxn_elem_id(d, v.water(p));
+      for (int d : dep) v.jac(ij++) = v.act(p) < 0 ? -1 : rxn_elem_id(d, v.act(p));
     }
   }
   // HL (src/rxns/rxn_HL_phase_transfer.c:149-186; the small water
@@ -938,13 +1041,33 @@ void Model::build_tables() {
       for (int e : si.elem) nd += var_type_[e] == VAR_VARIABLE;
     n_part_all += 4 + 4 * nd;
   }
+  // aqueous equilibrium instances: 2 per-cell constants (forward, reverse)
+  // after the SIMPOL constants, a loss and a gain pseudo-rate per dependent
+  // species slot after the SIMPOL pseudo-rates, and per dependent
+  // independent slot a partial for every dependent row slot
+  t.aq = aq_;
+  t.n_aq = (int)aq_.size();
+  t.aq_keff0.clear();
+  t.aq_rate0.clear();
+  t.aq_part0.clear();
+  for (const AqInst& q : aq_) {
+    int S = 0;
+    for (int sp : q.react) S += var_type_[sp] == VAR_VARIABLE;
+    for (int sp : q.prod) S += var_type_[sp] == VAR_VARIABLE;
+    t.aq_keff0.push_back(t.n_keff);
+    t.n_keff += 2;
+    t.aq_rate0.push_back(t.n_rates);
+    t.n_rates += 2 * S;
+    t.aq_part0.push_back(n_part_all);
+    n_part_all += S * S;
+  }
   t.n_part_all = n_part_all;
   // f gather: per dependent species, in term order, reactant occurrences
   // (loss, coefficient -1) before products (coefficient yield)
   std::vector<std::vector<int>> frx(n_dep_), fpr(n_dep_);
   std::vector<std::vector<double>> fco(n_dep_);
   {
-    int ti = 0, ks = 0;
+    int ti = 0, ks = 0, ka = 0;
     for (size_t ri = 0; ri < rxns_.size(); ++ri) {
       const Rxn& r = rxns_[ri];
       for (const Term& tm : r.terms) {
@@ -973,6 +1096,18 @@ void Model::build_tables() {
         frx[dg].push_back(base + 1); fco[dg].push_back(-1.0); fpr[dg].push_back(FG_LOSS);
         frx[da].push_back(base + 2); fco[da].push_back(-1.0); fpr[da].push_back(FG_LOSS);
         frx[da].push_back(base + 3); fco[da].push_back(1.0); fpr[da].push_back(FG_SOURCE);
+      }
+      // aqueous equilibrium: per dependent species slot its loss and gain
+      // pseudo-rates (src/rxns/rxn_aqueous_equilibrium.c:361-390)
+      for (; ka < t.n_aq && aq_[ka].rxn == (int)ri; ++ka) {
+        int k = 0;
+        for (const std::vector<int>* list : {&aq_[ka].react, &aq_[ka].prod})
+          for (int sp : *list) {
+            if (var_type_[sp] != VAR_VARIABLE) continue;
+            const int d = deriv_ids_[sp], base = t.aq_rate0[ka] + 2 * k++;
+            frx[d].push_back(base); fco[d].push_back(-1.0); fpr[d].push_back(FG_LOSS);
+            frx[d].push_back(base + 1); fco[d].push_back(1.0); fpr[d].push_back(FG_SOURCE);
+          }
       }
     }
   }
@@ -1051,6 +1186,27 @@ void Model::build_tables() {
       ++j;
     }
   }
+  // aqueous equilibrium partials: row slot b against independent slot a,
+  // a loss where both are reactants or both products, else an unguarded
+  // production (src/rxns/rxn_aqueous_equilibrium.c:436-479)
+  for (int k = 0; k < t.n_aq; ++k) {
+    const AqInst& q = aq_[k];
+    std::vector<int> sd;
+    std::vector<char> isr;
+    for (int sp : q.react)
+      if (var_type_[sp] == VAR_VARIABLE) sd.push_back(deriv_ids_[sp]), isr.push_back(1);
+    for (int sp : q.prod)
+      if (var_type_[sp] == VAR_VARIABLE) sd.push_back(deriv_ids_[sp]), isr.push_back(0);
+    const int S = (int)sd.size(), p0 = t.aq_part0[k];
+    for (int a = 0; a < S; ++a)
+      for (int b = 0; b < S; ++b) {
+        const bool loss = isr[a] == isr[b];
+        const int e = slot_of(sd[b], sd[a]);
+        jpart[e].push_back(p0 + a * S + b);
+        jco[e].push_back(loss ? -1.0 : 1.0);
+        jind[e].push_back(loss ? -1 : -2);
+      }
+  }
   t.jg_ptr.assign(t.n_jac + 1, 0);
   t.jg_part.clear(); t.jg_coef.clear(); t.jg_ind.clear();
   t.jg_lupos.assign(t.n_jac, 0);
@@ -1082,6 +1238,7 @@ bool Model::build(std::string* err) {
     return false;
   }
   if (!resolve_simpol(err)) return false;
+  if (!resolve_aq(err)) return false;
   build_rxn_jacobian();
   update_ids();
   build_solver_jacobian();

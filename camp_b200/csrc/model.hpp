@@ -18,6 +18,7 @@ enum : int {
   RXN_CMAQ_OH_HNO3 = 4,
   RXN_PHOTOLYSIS = 5,
   RXN_HL_PHASE_TRANSFER = 6,
+  RXN_AQUEOUS_EQUILIBRIUM = 7,
   RXN_FIRST_ORDER_LOSS = 12,
   RXN_EMISSION = 13,
   RXN_WET_DEPOSITION = 14,
@@ -64,6 +65,24 @@ struct SimpolInst {
   std::vector<int> elem;            // state indices
   std::vector<double> inv_rho, inv_mw;  // 1/density; 1/MW in the phase, else 0
   std::vector<char> in_phase;
+};
+
+// One phase instance of an aqueous equilibrium reaction
+// (src/rxns/rxn_aqueous_equilibrium.c:27-56): forward rate
+// k_f prod(c_i m_i) / W^(n_r - 1), reverse rate k_r gamma prod(c_j m_j) /
+// W^(n_p - 1), with m = 1e3 / MW (mass fraction -> M), W the aerosol-phase
+// water and gamma the ion pair's activity coefficient; each reactant loses
+// the forward rate / m_i and gains the reverse rate / m_i, each product the
+// reverse.  W and gamma are constant species, so per cell the constant
+// factors fold into two rate constants and the dependent species keep
+// mass-action form.
+struct AqInst {
+  int rxn = 0, p = 0;                 // reaction, phase instance within it
+  std::vector<int> react, prod;       // state indices
+  std::vector<double> m2m;            // MASS_FRAC_TO_M_: reactants, then products
+  int water = -1, act = -1;           // state indices (act: -1 when none)
+  double A = 1.0, C = 0.0, kr = 0.0;  // equilibrium constant parameters, k_reverse
+  double thr = 0.0;                   // water below which the reaction is off
 };
 
 // kinds of f gather entries (Tables::fg_prod)
@@ -127,9 +146,16 @@ struct Tables {
   int n_simpol = 0;
   std::vector<SimpolInst> simpol;
   std::vector<int> si_part0;
-  int n_part_all = 0;  // n_part + SIMPOL partials
-  int n_keff = 0;      // n_rxn + 8 n_simpol
-  int n_rates = 0;     // n_rxn + 4 n_simpol
+  // aqueous equilibrium instances: per-cell constants at keff slots
+  // aq_keff0 (forward, reverse), pseudo-rates from aq_rate0 (a loss and a
+  // gain per dependent species slot), partials from aq_part0 (per dependent
+  // independent slot, every dependent row slot)
+  int n_aq = 0;
+  std::vector<AqInst> aq;
+  std::vector<int> aq_keff0, aq_rate0, aq_part0;
+  int n_part_all = 0;  // n_part + SIMPOL and aqueous partials
+  int n_keff = 0;      // n_rxn + 8 n_simpol + 2 n_aq
+  int n_rates = 0;     // n_rxn + 4 n_simpol + aqueous pseudo-rates
   std::vector<double> fg_coef;
   // J gather by live solver Jacobian entry (CSC order); jg_ind: -1 loss,
   // -2 unguarded product (phase transfer), else the guard's independent
@@ -194,6 +220,10 @@ class Model {
   // reaction Jacobian, DERIV_ID/JAC_ID, solver Jacobian; then the LU
   // elimination order and the device tables.  Returns false on error.
   bool build(std::string* err);
+  // the absolute tolerances solver_initialize receives (per state
+  // variable): they set the aqueous equilibrium's minimum water
+  // (src/rxns/rxn_aqueous_equilibrium.c:222-227)
+  void set_abs_tol(const double* abs_tol) { abs_tol_.assign(abs_tol, abs_tol + n_state_); }
 
   int n_state() const { return n_state_; }
   int n_cells() const { return n_cells_; }
@@ -237,6 +267,7 @@ class Model {
   void build_tables();
   bool resolve_simpol(std::string* err);
   bool resolve_instance(SimpolInst* si, int phase, int ri, std::string* err);
+  bool resolve_aq(std::string* err);
   int rxn_elem_id(int dep, int ind) const;
 
   int n_state_, n_cells_, n_dep_, n_rxn_;
@@ -251,6 +282,8 @@ class Model {
   std::vector<int> arep_type_;
   std::vector<std::pair<int, int>> modes_;
   std::vector<SimpolInst> simpol_;
+  std::vector<AqInst> aq_;
+  std::vector<double> abs_tol_;
   std::vector<int> deriv_ids_;
   std::vector<int> rj_colptr_, rj_rowid_;
   std::vector<int> rl_colptr_, rl_rowid_;  // live subset of the reaction Jacobian

@@ -36,6 +36,13 @@ struct DevMech {
   const int *si_type, *si_kind, *si_gmd_col, *si_gsd_col, *si_act, *si_water, *si_nph,
       *si_cptr, *si_cidx;
   const double *si_dp, *si_cinv_rho, *si_cinv_mw, *si_cin;
+  // aqueous equilibrium instances: A, C, k_reverse and the minimum water;
+  // water and activity coefficient state indices (-1: none) and reactant /
+  // product counts; the constant (not dependent) reactants and products:
+  // state index, 1e3 / MW, reactant flag
+  int n_aq;
+  const double *aq_prm, *aq_cm;
+  const int *aq_int, *aq_cptr, *aq_cidx, *aq_cr;
 };
 
 template <typename T>
@@ -170,9 +177,44 @@ static __device__ void simpol_constants(const DevMech& m, int k,
   c[7] = mol;
 }
 
+// Forward and reverse rate constants of aqueous equilibrium instance q
+// (src/rxns/rxn_aqueous_equilibrium.c:244-262, 278-305) with the constant
+// factors folded in: k_f = K_eq k_r times (c m) of each constant reactant
+// and 1 / W per reactant after the first; k_r times the activity
+// coefficient, (c m) of each constant product and 1 / W per product after
+// the first.  Both are zero when the water is below its minimum (:331-336).
+static __device__ void aq_constants(const DevMech& m, int q, const double* cell_state, double T,
+                                    double* c) {
+  const double* f = m.aq_prm + 4 * q;
+  const int* ii = m.aq_int + 4 * q;
+  double w = cell_state[ldg(ii)];
+  w = w > bdf::kTiny ? w : bdf::kTiny;
+  if (w < ldg(f + 3)) {
+    c[0] = c[1] = 0.0;
+    return;
+  }
+  const double eq = f[1] == 0.0 ? f[0] : f[0] * exp(f[1] * (1.0 / T - 1.0 / 298.0));
+  double kf = eq * f[2], kr = f[2];
+  const int act = ldg(ii + 1);
+  if (act >= 0) kr *= cell_state[act];
+  for (int j = ldg(m.aq_cptr + q); j < ldg(m.aq_cptr + q + 1); ++j) {
+    double v = cell_state[ldg(m.aq_cidx + j)];
+    v = (v > bdf::kTiny ? v : bdf::kTiny) * ldg(m.aq_cm + j);
+    if (ldg(m.aq_cr + j))
+      kf *= v;
+    else
+      kr *= v;
+  }
+  for (int i = 1; i < ldg(ii + 2); ++i) kf /= w;
+  for (int i = 1; i < ldg(ii + 3); ++i) kr /= w;
+  c[0] = kf;
+  c[1] = kr;
+}
+
 // k of every reaction times the (clamped) constant-species concentrations it
 // multiplies; constant species are clamped to TINY as solver_run does.  The
-// SIMPOL constants follow the terms' (keff[n_rxn + 8 k ..]).
+// SIMPOL constants follow the terms' (keff[n_rxn + 8 k ..]), then the
+// aqueous equilibrium ones (keff[n_rxn + 8 n_simpol + 2 q ..]).
 static __device__ void compute_keff(const DevMech& m, const double* cell_state,
                              double T, double P, const double* photo_cell,
                              double* keff, int lane) {
@@ -186,6 +228,8 @@ static __device__ void compute_keff(const DevMech& m, const double* cell_state,
   }
   for (int k = lane; k < m.n_simpol; k += 32)
     simpol_constants(m, k, cell_state, T, P, photo_cell, keff + m.n_rxn + 8 * k);
+  for (int q = lane; q < m.n_aq; q += 32)
+    aq_constants(m, q, cell_state, T, keff + m.n_rxn + 8 * m.n_simpol + 2 * q);
   __syncwarp();
 }
 

@@ -141,9 +141,9 @@ struct Tab {
   const double* atol;
   const uint16_t *lu_rowptr, *lu_col;
   const uint32_t *upd_ptr, *upd;
-  const uint16_t *si_rec, *si_elem, *jg_umid;
-  const double* si_ef;
-  int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev, n_simpol, has_ug;
+  const uint16_t *si_rec, *si_elem, *jg_umid, *aq_rec, *aq_sp;
+  const double *si_ef, *aq_sm;
+  int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev, n_simpol, has_ug, n_aq;
 };
 
 __device__ __forceinline__ Tab make_tab(const char* b) {
@@ -175,6 +175,10 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.jg_umid = (const uint16_t*)(b + o.jg_umid);
   t.n_simpol = o.n_simpol;
   t.has_ug = o.has_ug;
+  t.aq_rec = (const uint16_t*)(b + o.aq_rec);
+  t.aq_sp = (const uint16_t*)(b + o.aq_sp);
+  t.aq_sm = (const double*)(b + o.aq_sm);
+  t.n_aq = o.n_aq;
   t.fb_lane = (const uint16_t*)(b + o.fb_lane);
   t.fb_unit = (const uint32_t*)(b + o.fb_unit);
   t.fb_pair = (const uint32_t*)(b + o.fb_pair);
@@ -353,6 +357,76 @@ __device__ __noinline__ void simpol_partials(const char* tb, const double* y, co
       p[5 + 4 * j] = gl;
       p[6 + 4 * j] = s.evap * s.inv_k * num + (s.N * dedm * dm + s.N * dedw * dw) * s.inv_k;
       p[7 + 4 * j] = gl * s.inv_k;
+    }
+  }
+}
+
+// Aqueous equilibrium, one lane per instance
+// (src/rxns/rxn_aqueous_equilibrium.c:266-393, 403-540): the forward and
+// reverse rates from the per-cell constants (keff slots: forward, reverse,
+// with the constant species, water powers and activity coefficient folded
+// in) times (c m) of each dependent reactant or product slot.
+__device__ __forceinline__ void aq_fr(const Tab& t, const uint16_t* rec, const double* y,
+                                      const double* keff, double* rf, double* rr) {
+  const int S = rec[0], R = rec[1], s0 = rec[2];
+  double f = keff[rec[5]], r = keff[rec[5] + 1];
+  #pragma unroll 1
+  for (int k = 0; k < S; ++k) {
+    const double v = state_of(y[t.aq_sp[s0 + k]]) * t.aq_sm[s0 + k];
+    if (k < R)
+      f *= v;
+    else
+      r *= v;
+  }
+  *rf = f;
+  *rr = r;
+}
+
+// per dependent slot a loss and a gain pseudo-rate: a reactant loses
+// rf / m and gains rr / m, a product the reverse; returns (warp-uniform)
+// whether any is negative
+__device__ __noinline__ bool aq_rates(const char* tb, const double* y, const double* keff,
+                                      double* rates, int lane) {
+  const Tab t = make_tab(tb);
+  bool neg = false;
+  #pragma unroll 1
+  for (int q = lane; q < t.n_aq; q += 32) {
+    const uint16_t* rec = t.aq_rec + 8 * q;
+    double rf, rr;
+    aq_fr(t, rec, y, keff, &rf, &rr);
+    const int S = rec[0], R = rec[1], s0 = rec[2];
+    double* r = rates + rec[3];
+    #pragma unroll 1
+    for (int k = 0; k < S; ++k) {
+      const double m = t.aq_sm[s0 + k];
+      r[2 * k] = ddiv(k < R ? rf : rr, m);
+      r[2 * k + 1] = ddiv(k < R ? rr : rf, m);
+      neg |= r[2 * k] < 0.0 || r[2 * k + 1] < 0.0;
+    }
+  }
+  return warp_any(neg);
+}
+
+// partials: independent slot a (rate rf for a reactant, rr for a product,
+// divided by its concentration), row slot k (divided by its m); zero when
+// the rate is zero, as the reference skips those
+__device__ __noinline__ void aq_partials(const char* tb, const double* y, const double* keff,
+                                         double* part, int lane) {
+  const Tab t = make_tab(tb);
+  #pragma unroll 1
+  for (int q = lane; q < t.n_aq; q += 32) {
+    const uint16_t* rec = t.aq_rec + 8 * q;
+    double rf, rr;
+    aq_fr(t, rec, y, keff, &rf, &rr);
+    const int S = rec[0], R = rec[1], s0 = rec[2];
+    double* p = part + rec[4];
+    #pragma unroll 1
+    for (int a = 0; a < S; ++a) {
+      const double rate = a < R ? rf : rr;
+      const double ca = state_of(y[t.aq_sp[s0 + a]]);
+      #pragma unroll 1
+      for (int k = 0; k < S; ++k)
+        p[a * S + k] = rate != 0.0 ? ddiv(ddiv(rate, ca), t.aq_sm[s0 + k]) : 0.0;
     }
   }
 }
@@ -554,7 +628,8 @@ __device__ __noinline__ int dev_f_aero(const char* tb, const double* y, double h
                                        const double* keff, double* rates, double* fscr,
                                        double* out, int lane, double* rp = nullptr,
                                        double* rl = nullptr) {
-  const bool neg = simpol_rates(tb, y, keff, rates, lane);
+  bool neg = simpol_rates(tb, y, keff, rates, lane);
+  neg |= aq_rates(tb, y, keff, rates, lane);
   return dev_f(tb, y, h, keff, rates, fscr, out, lane, rp, rl, neg);
 }
 template <typename JT>
@@ -562,10 +637,12 @@ __device__ __noinline__ int dev_jac_aero(const char* tb, const double* y, double
                                          const double* keff, double* part, JT* Jout, int lane,
                                          double* jp = nullptr, double* jl = nullptr) {
   simpol_partials(tb, y, keff, part, lane);
+  aq_partials(tb, y, keff, part, lane);
   return dev_jac<JT>(tb, y, h, keff, part, Jout, lane, jp, jl);
 }
 __device__ __forceinline__ bool has_simpol(const char* tb) {
-  return reinterpret_cast<const BlobOff*>(tb)->n_simpol > 0;
+  const BlobOff* o = reinterpret_cast<const BlobOff*>(tb);
+  return o->n_simpol > 0 || o->n_aq > 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1768,7 +1845,31 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
     si_cptr.push_back((int)si_cidx.size());
   }
   m.n_simpol = t.n_simpol;
+  // aqueous equilibrium instances (device-side constants; see rates.cuh)
+  std::vector<double> aq_prm, aq_cm;
+  std::vector<int> aq_int, aq_cptr(1, 0), aq_cidx, aq_cr;
+  for (const AqInst& q : t.aq) {
+    aq_prm.insert(aq_prm.end(), {q.A, q.C, q.kr, q.thr});
+    aq_int.insert(aq_int.end(), {q.water, q.act, (int)q.react.size(), (int)q.prod.size()});
+    for (int pass = 0; pass < 2; ++pass) {
+      const std::vector<int>& list = pass == 0 ? q.react : q.prod;
+      for (size_t i = 0; i < list.size(); ++i) {
+        if (model.var_type()[list[i]] == VAR_VARIABLE) continue;
+        aq_cidx.push_back(list[i]);
+        aq_cm.push_back(q.m2m[(pass == 0 ? 0 : q.react.size()) + i]);
+        aq_cr.push_back(pass == 0 ? 1 : 0);
+      }
+    }
+    aq_cptr.push_back((int)aq_cidx.size());
+  }
+  m.n_aq = t.n_aq;
   Packer pk;
+  pk.add(aq_prm, &m.aq_prm);
+  pk.add(aq_cm, &m.aq_cm);
+  pk.add(aq_int, &m.aq_int);
+  pk.add(aq_cptr, &m.aq_cptr);
+  pk.add(aq_cidx, &m.aq_cidx);
+  pk.add(aq_cr, &m.aq_cr);
   pk.add(si_prm, &m.si_prm);
   pk.add(si_type, &m.si_type);
   pk.add(si_kind, &m.si_kind);

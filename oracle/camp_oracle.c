@@ -26,6 +26,7 @@
 #define T_WET_DEPOSITION 14
 #define T_SIMPOL 10
 #define T_HL 6
+#define T_AQ 7
 
 /* types whose packed data is not the NUM_REACT_/NUM_PROD_ layout */
 static int species_rate_type(int t) {
@@ -53,6 +54,10 @@ typedef struct {
   const double *fl;    /* packed float data of this reaction */
   int n_float_prop;
   int env_off;
+  /* aqueous equilibrium: per phase instance, the water below which the
+   * reaction is off (MIN_WATER_ x SMALL_WATER_CONC_, set from the absolute
+   * tolerances as update_ids does) */
+  double *aq_thr;
 } ORxn;
 
 #define R_REACT(r, x) ((r)->ints[(r)->n_int_prop + (x)] - 1)
@@ -119,7 +124,7 @@ int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
                const int *ints, const double *floats) {
   if (m->n_added >= m->n_rxn) return 1;
   if ((type < T_ARRHENIUS || type > T_PHOTOLYSIS) && !species_rate_type(type) &&
-      type != T_SIMPOL && type != T_HL)
+      type != T_SIMPOL && type != T_HL && type != T_AQ)
     return 2;
   if (m->int_size + n_int + 1 > m->int_cap) {
     m->int_cap = 2 * (m->int_size + n_int + 1) + 64;
@@ -498,6 +503,37 @@ static void hl_env(const ORxn *r, double T, double P, double *k) {
   k[3] = f[6] * T / P;
 }
 
+/* --- aqueous equilibrium (src/rxns/rxn_aqueous_equilibrium.c) ---------- */
+/* packed layout of :27-56 */
+#define AQ_MIN_WATER 1.0e-4 /* :24 */
+typedef struct {
+  int nr, np, P;
+  int *I;
+  const double *F;
+} AQV;
+static AQV aqv(const ORxn *r) {
+  AQV q = {r->ints[0], r->ints[1], r->ints[2], r->ints, r->fl};
+  return q;
+}
+static int aq_react(AQV q, int x) { return q.I[3 + x] - 1; }
+static int aq_prod(AQV q, int x) { return q.I[3 + q.nr * q.P + x] - 1; }
+static int aq_water(AQV q, int x) { return q.I[3 + (q.nr + q.np) * q.P + x] - 1; }
+static int aq_act(AQV q, int x) { return q.I[3 + (q.nr + q.np + 1) * q.P + x] - 1; }
+static int *aq_deriv(AQV q, int x) { return &q.I[3 + (q.nr + q.np + 2) * q.P + x]; }
+static int *aq_jac(AQV q, int x) { return &q.I[3 + (2 * (q.nr + q.np) + 2) * q.P + x]; }
+static double aq_m2m(AQV q, int x) { return q.F[5 + x]; }
+
+/* SMALL_WATER_CONC_ = abs_tol[water] / 10 (:222-227), times MIN_WATER_ */
+static void aq_thresholds(const OracleMech *m, const double *abs_tol) {
+  for (int i = 0; i < m->n_rxn; ++i) {
+    const ORxn *r = &m->rx[i];
+    if (r->type != T_AQ) continue;
+    AQV q = aqv(r);
+    for (int p = 0; p < q.P; ++p)
+      r->aq_thr[p] = AQ_MIN_WATER * (abs_tol ? abs_tol[aq_water(q, p)] / 10.0 : 0.0);
+  }
+}
+
 /* --- Jacobian element registry (restates src/Jacobian.c:105-214) -------- */
 typedef struct {
   int n;
@@ -669,6 +705,14 @@ int om_build(OracleMech *m) {
     ORxn *r = &m->rx[i];
     r->ints = m->int_data + (size_t)r->ints;
     r->fl = m->float_data + (size_t)r->fl;
+    if (r->type == T_AQ) {
+      AQV q = aqv(r);
+      r->aq_thr = (double *)zalloc(sizeof(double) * (size_t)(q.P + 1));
+      r->nr = r->np = 0;
+      r->n_int_prop = 3;
+      r->n_float_prop = 5;
+      continue;
+    }
     if (species_rate_type(r->type) || r->type == T_SIMPOL || r->type == T_HL) {
       /* RXN_ID_ first (host-rate types); the reactant / product fields stay
        * unused */
@@ -732,6 +776,27 @@ int om_build(OracleMech *m) {
             *sim_phase_jac(sm, x, 0, used) = *sim_phase_jac(sm, x, 1, used) = -1;
         }
         free(flag);
+        continue;
+      }
+      case T_AQ: { /* src/rxns/rxn_aqueous_equilibrium.c:70-127 */
+        AQV q = aqv(r);
+        for (int p = 0; p < q.P; ++p) {
+          for (int i = 0; i < q.nr; ++i) {
+            const int ind = aq_react(q, p * q.nr + i);
+            for (int d = 0; d < q.nr; ++d) jr_register(&rj, aq_react(q, p * q.nr + d), ind);
+            for (int d = 0; d < q.np; ++d) jr_register(&rj, aq_prod(q, p * q.np + d), ind);
+          }
+          for (int i = 0; i < q.np; ++i) {
+            const int ind = aq_prod(q, p * q.np + i);
+            for (int d = 0; d < q.nr; ++d) jr_register(&rj, aq_react(q, p * q.nr + d), ind);
+            for (int d = 0; d < q.np; ++d) jr_register(&rj, aq_prod(q, p * q.np + d), ind);
+          }
+          for (int d = 0; d < q.nr; ++d) jr_register(&rj, aq_react(q, p * q.nr + d), aq_water(q, p));
+          for (int d = 0; d < q.np; ++d) jr_register(&rj, aq_prod(q, p * q.np + d), aq_water(q, p));
+          if (aq_act(q, p) < 0) continue;
+          for (int d = 0; d < q.nr; ++d) jr_register(&rj, aq_react(q, p * q.nr + d), aq_act(q, p));
+          for (int d = 0; d < q.np; ++d) jr_register(&rj, aq_prod(q, p * q.np + d), aq_act(q, p));
+        }
         continue;
       }
       case T_HL: { /* src/rxns/rxn_HL_phase_transfer.c:72-138 */
@@ -824,6 +889,34 @@ int om_build(OracleMech *m) {
         }
         continue;
       }
+      case T_AQ: { /* src/rxns/rxn_aqueous_equilibrium.c:132-209 */
+        AQV q = aqv(r);
+        const int *cp = m->rj_colptr, *ri = m->rj_rowid;
+        int id = 0;
+        for (int p = 0; p < q.P; ++p) {
+          for (int i = 0; i < q.nr; ++i) *aq_deriv(q, id++) = m->deriv_ids[aq_react(q, p * q.nr + i)];
+          for (int i = 0; i < q.np; ++i) *aq_deriv(q, id++) = m->deriv_ids[aq_prod(q, p * q.np + i)];
+        }
+        int ij = 0;
+        for (int p = 0; p < q.P; ++p) {
+          for (int i = 0; i < q.nr; ++i) {
+            const int ind = aq_react(q, p * q.nr + i);
+            for (int d = 0; d < q.nr; ++d) *aq_jac(q, ij++) = jr_elem_id(cp, ri, aq_react(q, p * q.nr + d), ind);
+            for (int d = 0; d < q.np; ++d) *aq_jac(q, ij++) = jr_elem_id(cp, ri, aq_prod(q, p * q.np + d), ind);
+          }
+          for (int i = 0; i < q.np; ++i) {
+            const int ind = aq_prod(q, p * q.np + i);
+            for (int d = 0; d < q.nr; ++d) *aq_jac(q, ij++) = jr_elem_id(cp, ri, aq_react(q, p * q.nr + d), ind);
+            for (int d = 0; d < q.np; ++d) *aq_jac(q, ij++) = jr_elem_id(cp, ri, aq_prod(q, p * q.np + d), ind);
+          }
+          for (int d = 0; d < q.nr; ++d) *aq_jac(q, ij++) = jr_elem_id(cp, ri, aq_react(q, p * q.nr + d), aq_water(q, p));
+          for (int d = 0; d < q.np; ++d) *aq_jac(q, ij++) = jr_elem_id(cp, ri, aq_prod(q, p * q.np + d), aq_water(q, p));
+          const int a = aq_act(q, p);
+          for (int d = 0; d < q.nr; ++d) *aq_jac(q, ij++) = a < 0 ? -1 : jr_elem_id(cp, ri, aq_react(q, p * q.nr + d), a);
+          for (int d = 0; d < q.np; ++d) *aq_jac(q, ij++) = a < 0 ? -1 : jr_elem_id(cp, ri, aq_prod(q, p * q.np + d), a);
+        }
+        continue;
+      }
       case T_HL: { /* src/rxns/rxn_HL_phase_transfer.c:149-186; the small
                     * water concentration it also sets (:188-193) is unused */
         HLV hl = hlv(r);
@@ -899,6 +992,7 @@ int om_build(OracleMech *m) {
 
 void om_free(OracleMech *m) {
   if (!m) return;
+  for (int i = 0; i < m->n_rxn; ++i) free(m->rx[i].aq_thr);
   free(m->var_type);
   free(m->int_data);
   free(m->float_data);
@@ -1034,6 +1128,9 @@ void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
       case T_HL:
         hl_env(r, T, P, k);
         break;
+      case T_AQ: /* src/rxns/rxn_aqueous_equilibrium.c:244-262 */
+        k[0] = (f[1] == 0.0 ? f[0] : f[0] * exp(f[1] * (1.0 / T - 1.0 / 298.0))) * f[2];
+        break;
     }
   }
 }
@@ -1105,6 +1202,43 @@ void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
           if (da >= 0) {
             add_value(P, L, da, -nconc * evap / kk[3]);
             add_value(P, L, da, nconc * cond / kk[3]);
+          }
+        }
+        continue;
+      }
+      case T_AQ: { /* src/rxns/rxn_aqueous_equilibrium.c:266-393 */
+        AQV q = aqv(r);
+        const double kf = rxn_env[r->env_off], kr = q.F[2];
+        for (int p = 0, id = 0; p < q.P; ++p) {
+          const long double water = state[aq_water(q, p)];
+          if (water < r->aq_thr[p]) {
+            id += q.nr + q.np;
+            continue;
+          }
+          long double rf = (long double)state[aq_react(q, p * q.nr)] * aq_m2m(q, 0);
+          for (int i = 1; i < q.nr; ++i)
+            rf *= state[aq_react(q, p * q.nr + i)] * aq_m2m(q, i) / water;
+          long double rr = (long double)state[aq_prod(q, p * q.np)] * aq_m2m(q, q.nr);
+          rr *= (long double)(aq_act(q, p) >= 0 ? state[aq_act(q, p)] : 1.0);
+          for (int i = 1; i < q.np; ++i)
+            rr *= state[aq_prod(q, p * q.np + i)] * aq_m2m(q, q.nr + i) / water;
+          rf = kf * rf;
+          rr = kr * rr;
+          if (rf - rr == 0.0) {
+            id += q.nr + q.np;
+            continue;
+          }
+          for (int i = 0; i < q.nr; ++i, ++id) {
+            const int d = *aq_deriv(q, id);
+            if (d < 0) continue;
+            add_value(P, L, d, -rf / aq_m2m(q, i));
+            add_value(P, L, d, rr / aq_m2m(q, i));
+          }
+          for (int i = 0; i < q.np; ++i, ++id) {
+            const int d = *aq_deriv(q, id);
+            if (d < 0) continue;
+            add_value(P, L, d, rf / aq_m2m(q, q.nr + i));
+            add_value(P, L, d, -rr / aq_m2m(q, q.nr + i));
           }
         }
         continue;
@@ -1244,6 +1378,60 @@ void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
             }
           }
           free(nd);
+        }
+        continue;
+      }
+      case T_AQ: { /* src/rxns/rxn_aqueous_equilibrium.c:403-540 */
+        AQV q = aqv(r);
+        const int ns = q.nr + q.np;
+        for (int p = 0, ij = 0; p < q.P; ++p) {
+          const long double water = state[aq_water(q, p)];
+          if (water < r->aq_thr[p]) {
+            ij += ns * (ns + 2);
+            continue;
+          }
+          long double fr = rxn_env[r->env_off];
+          for (int i = 0; i < q.nr; ++i) fr *= state[aq_react(q, p * q.nr + i)] * aq_m2m(q, i) / water;
+          long double rr = q.F[2];
+          for (int i = 0; i < q.np; ++i)
+            rr *= state[aq_prod(q, p * q.np + i)] * aq_m2m(q, q.nr + i) / water;
+          const int a = aq_act(q, p);
+          if (a >= 0) rr *= state[a];
+          for (int i = 0; i < q.nr; ++i) {
+            const double c = state[aq_react(q, p * q.nr + i)];
+            for (int d = 0; d < q.nr; ++d, ++ij)
+              if (*aq_jac(q, ij) >= 0 && fr != 0.0) L[*aq_jac(q, ij)] += fr / c / aq_m2m(q, d) * water;
+            for (int d = 0; d < q.np; ++d, ++ij)
+              if (*aq_jac(q, ij) >= 0 && fr != 0.0)
+                P[*aq_jac(q, ij)] += fr / c / aq_m2m(q, q.nr + d) * water;
+          }
+          for (int i = 0; i < q.np; ++i) {
+            const double c = state[aq_prod(q, p * q.np + i)];
+            for (int d = 0; d < q.nr; ++d, ++ij)
+              if (*aq_jac(q, ij) >= 0 && rr != 0.0) P[*aq_jac(q, ij)] += rr / c / aq_m2m(q, d) * water;
+            for (int d = 0; d < q.np; ++d, ++ij)
+              if (*aq_jac(q, ij) >= 0 && rr != 0.0)
+                L[*aq_jac(q, ij)] += rr / c / aq_m2m(q, q.nr + d) * water;
+          }
+          for (int d = 0; d < q.nr; ++d, ++ij) {
+            if (*aq_jac(q, ij) < 0) continue;
+            L[*aq_jac(q, ij)] += -fr / aq_m2m(q, d) * (q.nr - 1);
+            P[*aq_jac(q, ij)] += -rr / aq_m2m(q, d) * (q.np - 1);
+          }
+          for (int d = 0; d < q.np; ++d, ++ij) {
+            if (*aq_jac(q, ij) < 0) continue;
+            P[*aq_jac(q, ij)] += -fr / aq_m2m(q, q.nr + d) * (q.nr - 1);
+            L[*aq_jac(q, ij)] += -rr / aq_m2m(q, q.nr + d) * (q.np - 1);
+          }
+          if (a < 0) {
+            ij += ns;
+            continue;
+          }
+          for (int d = 0; d < q.nr; ++d, ++ij)
+            if (*aq_jac(q, ij) >= 0) P[*aq_jac(q, ij)] += rr / state[a] / aq_m2m(q, d) * water;
+          for (int d = 0; d < q.np; ++d, ++ij)
+            if (*aq_jac(q, ij) >= 0)
+              L[*aq_jac(q, ij)] += rr / state[a] / aq_m2m(q, q.nr + d) * water;
         }
         continue;
       }
@@ -2144,11 +2332,16 @@ static void *solve_job(void *arg) {
   return NULL;
 }
 
+/* The absolute tolerances solver_initialize receives (per state variable):
+ * they set the aqueous equilibrium's minimum water. */
+void om_set_abs_tol(const OracleMech *m, const double *abs_tol) { aq_thresholds(m, abs_tol); }
+
 int om_solve(const OracleMech *m, int n_cells, double *state, const double *env,
              double *rxn_env, double t0, double t1, double rtol,
              const double *abs_tol, int max_steps, int max_conv_fails,
              int n_threads, int *status, OracleStats *stats) {
   if (!m->built) return -1;
+  aq_thresholds(m, abs_tol);
   if (n_threads < 1) n_threads = 1;
   if (n_threads > n_cells) n_threads = n_cells > 0 ? n_cells : 1;
   SolveJob *jobs = (SolveJob *)zalloc(sizeof(SolveJob) * n_threads);

@@ -69,6 +69,10 @@ int om_add_aero_rep(OracleMech *m, int type, int n_int, int n_float, int n_env,
 int om_set_aero_env(const OracleMech *m, double *rxn_env_cell, int rep, int section,
                     int what, double value);
 int om_build(OracleMech *m);
+/* the absolute tolerances (per state variable) that set the aqueous
+ * equilibrium's minimum water, as solver_initialize's do; om_solve sets
+ * them from its own argument */
+void om_set_abs_tol(const OracleMech *m, const double *abs_tol);
 void om_free(OracleMech *m);
 
 int om_n_dep_var(const OracleMech *m);

@@ -70,6 +70,7 @@ def oracle_lib():
         lib.om_add_rxn.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p]
         lib.om_build.restype = C.c_int
         lib.om_build.argtypes = [vp]
+        lib.om_set_abs_tol.argtypes = [vp, _f64p]
         lib.om_free.argtypes = [vp]
         for name in (
             "om_n_dep_var",
@@ -194,6 +195,8 @@ class OracleModel:
                 raise ValueError(f"oracle rejected aerosol representation type {a.rep_type}")
         if self.lib.om_build(self.h) != 0:
             raise RuntimeError("oracle sparsity build failed")
+        # the mechanism's tolerances, as solver_initialize would pass them
+        self.lib.om_set_abs_tol(self.h, np.ascontiguousarray(mech.abs_tol, np.float64))
         self.n_dep = self.lib.om_n_dep_var(self.h)
         self.n_env = self.lib.om_n_rxn_env_data(self.h)
         self.n_rxn_jac = self.lib.om_n_rxn_jac_elem(self.h)

@@ -261,3 +261,63 @@ def hl_case(tmp_dir):
         return np.stack([g, (total - g) / K], axis=-1)
 
     return mech, y0, cols, truth
+
+
+# One AQUEOUS_EQUILIBRIUM reaction A <-> B in one aqueous mode, water and the
+# ion pair's activity coefficient constant species: in molar amounts
+# a = A m_A, b = B m_B (m = 1e3 / MW) it is linear,
+#   da/dt = -k_f a + k_r g b,  db/dt = -da/dt,
+# relaxing at k_f + k_r g to a / b = k_r g / k_f.
+AQ_ENV = (285.0, 9.5e4)
+AQ_PRM = {"A": 2.0, "C": 300.0, "k_reverse": 0.04}
+AQ_GAMMA = 1.5
+AQ_MW = (0.06, 0.09)                    # A, B (kg mol-1)
+AQ_Y0 = (2.0e-9, 5.0e-10)               # A, B (kg m-3)
+
+
+def aq_case(tmp_dir):
+    """(mechanism, y0, host columns (GMD, GSD), closed form A, B at t)."""
+    import json
+
+    from camp_b200.aerosol import load_aerosol_mechanism
+
+    doc = {"camp-data": [
+        {"name": "AQA", "type": "CHEM_SPEC", "phase": "AEROSOL",
+         "molecular weight [kg mol-1]": AQ_MW[0], "density [kg m-3]": 1000.0,
+         "absolute integration tolerance": 1e-20},
+        {"name": "AQB", "type": "CHEM_SPEC", "phase": "AEROSOL",
+         "molecular weight [kg mol-1]": AQ_MW[1], "density [kg m-3]": 1000.0,
+         "absolute integration tolerance": 1e-20},
+        {"name": "H2O_aq", "type": "CHEM_SPEC", "phase": "AEROSOL", "tracer type": "CONSTANT",
+         "molecular weight [kg mol-1]": 0.01801528, "density [kg m-3]": 1000.0},
+        {"name": "A-B", "type": "CHEM_SPEC", "tracer type": "ION_PAIR"},
+        {"name": "aqueous", "type": "AERO_PHASE", "species": ["H2O_aq", "AQA", "AQB", "A-B"]},
+        {"name": "rep", "type": "AERO_REP_MODAL_BINNED_MASS", "modes/bins": {
+            "the mode": {"type": "MODAL", "phases": ["aqueous"], "shape": "LOG_NORMAL",
+                         "geometric mean diameter [m]": 2.0e-7,
+                         "geometric standard deviation": 1.6}}},
+        {"name": "aq", "type": "MECHANISM", "reactions": [
+            dict({"type": "AQUEOUS_EQUILIBRIUM", "aerosol phase": "aqueous",
+                  "aerosol-phase water": "H2O_aq", "ion pair": "A-B",
+                  "reactants": {"AQA": {}}, "products": {"AQB": {}}}, **AQ_PRM)]},
+    ]}
+    path = os.path.join(str(tmp_dir), "aq.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    mech = load_aerosol_mechanism([path], name="aq")
+    names = ["the mode.aqueous." + n for n in ("H2O_aq", "AQA", "AQB", "A-B")]
+    assert mech.species == names
+    y0 = np.array([1.0e-6, AQ_Y0[0], AQ_Y0[1], AQ_GAMMA])
+    T = AQ_ENV[0]
+    kf = AQ_PRM["A"] * np.exp(AQ_PRM["C"] * (1.0 / T - 1.0 / 298.0)) * AQ_PRM["k_reverse"]
+    kr = AQ_PRM["k_reverse"] * AQ_GAMMA
+    ma, mb = 1.0e3 / AQ_MW[0], 1.0e3 / AQ_MW[1]
+    a0, b0 = AQ_Y0[0] * ma, AQ_Y0[1] * mb
+    lam = kf + kr
+    a_eq = (a0 + b0) * kr / lam
+
+    def truth(times):
+        a = a_eq + (a0 - a_eq) * np.exp(-lam * np.asarray(times, np.float64))
+        return np.stack([a / ma, (a0 + b0 - a) / mb], axis=-1)
+
+    return mech, y0, np.array([2.0e-7, 1.6]), truth

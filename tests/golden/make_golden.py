@@ -23,15 +23,18 @@ Outputs (all small):
                          phases and MONARCH modal/binned mass representation
                          (7 modes and bin sets, 99 aerosol state variables);
                          its wet deposition acts on the cloud-and-rain phase
-                         instance.  The aerosol reactions of mod37 that are
-                         not restated (aqueous equilibrium, ZSR, PDFiTE) are
-                         left out
+                         instance.  The sub-models of mod37 (ZSR water,
+                         PDFiTE activity) are not restated and are left out
   monarch_mod37_aero.mech.json
                          the SOA fixture plus the shipped partitioning of 35
                          gas-phase species into cloud and rain water
                          (cloud_and_rain_partitioning.json: HL_PHASE_TRANSFER
                          into the "clouds and rain" mode, aerosol-phase water
-                         H2O_aq a constant species)
+                         H2O_aq a constant species) and the 5 aqueous
+                         equilibria of the sulfate mode
+                         (inorganic_reactions.json; their ion pairs'
+                         activity coefficients are constant species here, as
+                         without the PDFiTE sub-model)
   cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz, monarch_mod37_soa_ref.npz,
   monarch_mod37_aero_ref.npz
                          outputs of the reference's own C code
@@ -116,7 +119,8 @@ def mod37_soa(ref_root: str):
                                   name="monarch_mod37_soa")
 
 
-MOD37_AERO_FILES = MOD37_SOA_FILES + ("cloud_and_rain_partitioning.json",)
+MOD37_AERO_FILES = MOD37_SOA_FILES + ("cloud_and_rain_partitioning.json",
+                                      "inorganic_reactions.json")
 
 
 def mod37_aero(ref_root: str):

@@ -139,8 +139,8 @@ def test_mod37_packer_matches_fixture(mod37):
 
 def test_hl_elements_stay_out_of_the_lu(mod37_soa, mod37_aero, lib):
     """The reference registers every mass species of the cloud-and-rain mode
-    against each HL gas and aerosol species (3803 solver Jacobian entries,
-    863 without HL).  Those partials are zero for the modal/binned
+    against each HL gas and aerosol species (3827 solver Jacobian entries
+    with mod37's aqueous equilibria, 863 without HL or those).  Those partials are zero for the modal/binned
     representation, so the exported sparsity keeps them while the LU leaves
     them out: it grows by the HL couplings only, where the full pattern
     fills to 4563 entries."""
@@ -151,5 +151,5 @@ def test_hl_elements_stay_out_of_the_lu(mod37_soa, mod37_aero, lib):
         s = Solver(m, 2)
         s.build_sparsity_only()
         sizes.append((len(s.solver_jac()[1]), s.n_lu()))
-    assert sizes[0][0] == 863 and sizes[1][0] == 3803
+    assert sizes[0][0] == 863 and sizes[1][0] == 3827
     assert sizes[1][1] <= 1.1 * sizes[0][1]

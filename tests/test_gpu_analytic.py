@@ -167,3 +167,26 @@ def test_hl_through_json_entry_point(tmp_path):
         lib.solver_free(h)
     np.testing.assert_allclose(state[:, :2], np.tile(truth([30.0])[0], (n, 1)), rtol=1e-6,
                                atol=1e-18)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_aqueous_equilibrium_closed_form(tmp_path, precision):
+    """A <-> B in one aqueous mode (conftest.aq_case) through the C ABI."""
+    from conftest import AQ_ENV, aq_case
+
+    from camp_b200.solver import Solver
+
+    mech, y0, cols, truth = aq_case(tmp_path)
+    n = len(TIMES)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.array([1e-14, 1e-20, 1e-20, 1e-14]), rel_tol=1e-10,
+                 max_steps=100000)
+    s.set_precision(precision)
+    s.set_photo_rates(np.tile(cols, (n, 1)))
+    env = np.tile(np.array(AQ_ENV), (n, 1))
+    out = np.zeros((n, 2))
+    for c, t in enumerate(TIMES):
+        x = np.tile(y0, (n, 1))
+        assert s.solve(x, env, 0.0, t) == 0, s.cell_stats()["status"]
+        out[c] = x[c, 1:3]
+    np.testing.assert_allclose(out, truth(TIMES), rtol=1e-6, atol=1e-20)

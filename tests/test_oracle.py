@@ -278,3 +278,20 @@ def test_hl_closed_form(tmp_path):
         assert nf == 0, status
         out.append(y[0, :2])
     np.testing.assert_allclose(out, truth([5.0, 20.0, 60.0]), rtol=1e-7, atol=1e-18)
+
+
+def test_aqueous_equilibrium_closed_form(tmp_path):
+    """A <-> B in one aqueous mode (constant water and ion pair) relaxes to
+    the equilibrium ratio k_r gamma / k_f at the rate k_f + k_r gamma."""
+    from conftest import AQ_ENV, aq_case
+
+    mech, y0, cols, truth = aq_case(tmp_path)
+    om = OracleModel(mech)
+    abs_tol = np.array([1e-14, 1e-20, 1e-20, 1e-14])
+    out = []
+    for t in (5.0, 20.0, 60.0):
+        nf, status, _, y = om.solve(y0[None, :].copy(), np.array([AQ_ENV]), cols[None, :], 0.0,
+                                    t, 1e-10, abs_tol, max_steps=100000)
+        assert nf == 0, status
+        out.append(y[0, 1:3])
+    np.testing.assert_allclose(out, truth([5.0, 20.0, 60.0]), rtol=1e-7, atol=1e-20)
