@@ -53,8 +53,8 @@ struct LoadedMechanism {
 // Reads CAMP JSON files ({"camp-data": [...]} with CHEM_SPEC, MECHANISM,
 // RELATIVE_TOLERANCE, AERO_PHASE and AERO_REP_MODAL_BINNED_MASS objects) and
 // packs the reactions: the gas-phase types, and SIMPOL_PHASE_TRANSFER,
-// HL_PHASE_TRANSFER and WET_DEPOSITION over the phase instances of the
-// representations.  Reactions whose rate the host sets (PHOTOLYSIS,
+// HL_PHASE_TRANSFER, AQUEOUS_EQUILIBRIUM and WET_DEPOSITION over the phase
+// instances of the representations.  Reactions whose rate the host sets (PHOTOLYSIS,
 // FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION) get ids 1, 2, ... in mechanism
 // order; representations get ids 1, 2, ... in order.  Other representation
 // types and sub-models are refused.

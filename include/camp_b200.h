@@ -115,9 +115,10 @@ void rxn_wet_deposition_set_rate_update_data(void *update_data, int rxn_id,
 /* replace src/aero_phase_solver.c:175,210, src/aero_rep_solver.c:443,492,546
  * and src/sub_model_solver.c:413,468,509.  Aerosol phases and the
  * modal/binned mass representation (type 2) are solved with SIMPOL
- * (reaction type 10) and HL (type 6, constant aerosol-phase water)
- * partitioning; other representation types and any sub-model are rejected
- * at solver_initialize. */
+ * (reaction type 10) and HL (type 6) partitioning and aqueous equilibrium
+ * (type 7), the aerosol-phase water and ion pairs being constant species;
+ * other representation types and any sub-model are rejected at
+ * solver_initialize. */
 void aero_phase_add_condensed_data(int n_int_param, int n_float_param,
                                    int *int_param, double *float_param,
                                    void *solver_data);
@@ -341,7 +342,8 @@ void camp_b200_server_free(void *server);
  * files (CHEM_SPEC, MECHANISM, RELATIVE_TOLERANCE, AERO_PHASE and
  * AERO_REP_MODAL_BINNED_MASS objects), orders the state (gas species in order
  * of first appearance, then each representation's species), packs every
- * reaction, phase and representation and calls solver_new,
+ * reaction (SIMPOL, HL, aqueous equilibrium and wet deposition over the
+ * phase instances included), phase and representation and calls solver_new,
  * rxn_add_condensed_data, aero_phase_add_condensed_data and
  * aero_rep_add_condensed_data.  Reactions whose rate the host sets
  * (PHOTOLYSIS, FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION) get the ids
