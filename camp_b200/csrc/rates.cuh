@@ -177,38 +177,47 @@ static __device__ void simpol_constants(const DevMech& m, int k,
   c[7] = mol;
 }
 
-// Forward and reverse rate constants of aqueous equilibrium instance q
-// (src/rxns/rxn_aqueous_equilibrium.c:244-262, 278-305) with the constant
-// factors folded in: k_f = K_eq k_r times (c m) of each constant reactant
-// and 1 / W per reactant after the first; k_r times the activity
-// coefficient, (c m) of each constant product and 1 / W per product after
-// the first.  Both are zero when the water is below its minimum (:331-336).
-static __device__ void aq_constants(const DevMech& m, int q, const double* cell_state, double T,
-                                    double* c) {
-  const double* f = m.aq_prm + 4 * q;
-  const int* ii = m.aq_int + 4 * q;
-  double w = cell_state[ldg(ii)];
-  w = w > bdf::kTiny ? w : bdf::kTiny;
-  if (w < ldg(f + 3)) {
-    c[0] = c[1] = 0.0;
-    return;
+// Forward and reverse rate constants of every aqueous equilibrium instance
+// (src/rxns/rxn_aqueous_equilibrium.c:244-262, 278-305), one lane per
+// instance, into keff[2 q], keff[2 q + 1], with the constant factors folded
+// in: k_f = K_eq k_r times (c m) of each constant reactant and 1 / W per
+// reactant after the first; k_r times the activity coefficient, (c m) of
+// each constant product and 1 / W per product after the first.  Both are
+// zero when the water is below its minimum (:331-336).  Out of line and
+// over plain pointers, so that mechanisms without these reactions keep the
+// solve kernel's register allocation.
+static __device__ __noinline__ void aq_constants(const double* prm, const int* ii,
+                                                 const int* cptr, const int* cidx,
+                                                 const double* cm, const int* cr, int n_aq,
+                                                 const double* cell_state, double T,
+                                                 double* keff, int lane) {
+  for (int q = lane; q < n_aq; q += 32) {
+    const double* f = prm + 4 * q;
+    const int* iq = ii + 4 * q;
+    double* c = keff + 2 * q;
+    double w = cell_state[ldg(iq)];
+    w = w > bdf::kTiny ? w : bdf::kTiny;
+    if (w < ldg(f + 3)) {
+      c[0] = c[1] = 0.0;
+      continue;
+    }
+    const double eq = f[1] == 0.0 ? f[0] : f[0] * exp(f[1] * (1.0 / T - 1.0 / 298.0));
+    double kf = eq * f[2], kr = f[2];
+    const int act = ldg(iq + 1);
+    if (act >= 0) kr *= cell_state[act];
+    for (int j = ldg(cptr + q); j < ldg(cptr + q + 1); ++j) {
+      double v = cell_state[ldg(cidx + j)];
+      v = (v > bdf::kTiny ? v : bdf::kTiny) * ldg(cm + j);
+      if (ldg(cr + j))
+        kf *= v;
+      else
+        kr *= v;
+    }
+    for (int i = 1; i < ldg(iq + 2); ++i) kf /= w;
+    for (int i = 1; i < ldg(iq + 3); ++i) kr /= w;
+    c[0] = kf;
+    c[1] = kr;
   }
-  const double eq = f[1] == 0.0 ? f[0] : f[0] * exp(f[1] * (1.0 / T - 1.0 / 298.0));
-  double kf = eq * f[2], kr = f[2];
-  const int act = ldg(ii + 1);
-  if (act >= 0) kr *= cell_state[act];
-  for (int j = ldg(m.aq_cptr + q); j < ldg(m.aq_cptr + q + 1); ++j) {
-    double v = cell_state[ldg(m.aq_cidx + j)];
-    v = (v > bdf::kTiny ? v : bdf::kTiny) * ldg(m.aq_cm + j);
-    if (ldg(m.aq_cr + j))
-      kf *= v;
-    else
-      kr *= v;
-  }
-  for (int i = 1; i < ldg(ii + 2); ++i) kf /= w;
-  for (int i = 1; i < ldg(ii + 3); ++i) kr /= w;
-  c[0] = kf;
-  c[1] = kr;
 }
 
 // k of every reaction times the (clamped) constant-species concentrations it
@@ -228,8 +237,9 @@ static __device__ void compute_keff(const DevMech& m, const double* cell_state,
   }
   for (int k = lane; k < m.n_simpol; k += 32)
     simpol_constants(m, k, cell_state, T, P, photo_cell, keff + m.n_rxn + 8 * k);
-  for (int q = lane; q < m.n_aq; q += 32)
-    aq_constants(m, q, cell_state, T, keff + m.n_rxn + 8 * m.n_simpol + 2 * q);
+  if (m.n_aq > 0)
+    aq_constants(m.aq_prm, m.aq_int, m.aq_cptr, m.aq_cidx, m.aq_cm, m.aq_cr, m.n_aq, cell_state,
+                 T, keff + m.n_rxn + 8 * m.n_simpol, lane);
   __syncwarp();
 }
 

@@ -431,6 +431,20 @@ __device__ __noinline__ void aq_partials(const char* tb, const double* y, const 
   }
 }
 
+// Both aerosol passes behind one call, so that the wrappers below keep a
+// single call site each (the solve kernel's register allocation follows
+// them).
+__device__ __noinline__ bool aero_rates(const char* tb, const double* y, const double* keff,
+                                        double* rates, int lane) {
+  const bool neg = simpol_rates(tb, y, keff, rates, lane);
+  return aq_rates(tb, y, keff, rates, lane) || neg;
+}
+__device__ __noinline__ void aero_partials(const char* tb, const double* y, const double* keff,
+                                           double* part, int lane) {
+  simpol_partials(tb, y, keff, part, lane);
+  aq_partials(tb, y, keff, part, lane);
+}
+
 // Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
 // When rp/rl are given, the production and loss sums are written too.
 // Species lists are processed in lane-balanced units; lists split over
@@ -619,7 +633,8 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
   return 0;
 }
 
-// f and J of a mechanism with SIMPOL instances: their pseudo-rates or
+// f and J of a mechanism with SIMPOL, HL or aqueous equilibrium instances:
+// their pseudo-rates or
 // partials first (slots after the terms', which the mass-action passes do
 // not write, made visible to the gathers by their warp barrier), then the
 // usual evaluation.  Separate functions, so that the plain f and J keep
@@ -628,16 +643,14 @@ __device__ __noinline__ int dev_f_aero(const char* tb, const double* y, double h
                                        const double* keff, double* rates, double* fscr,
                                        double* out, int lane, double* rp = nullptr,
                                        double* rl = nullptr) {
-  bool neg = simpol_rates(tb, y, keff, rates, lane);
-  neg |= aq_rates(tb, y, keff, rates, lane);
+  const bool neg = aero_rates(tb, y, keff, rates, lane);
   return dev_f(tb, y, h, keff, rates, fscr, out, lane, rp, rl, neg);
 }
 template <typename JT>
 __device__ __noinline__ int dev_jac_aero(const char* tb, const double* y, double h,
                                          const double* keff, double* part, JT* Jout, int lane,
                                          double* jp = nullptr, double* jl = nullptr) {
-  simpol_partials(tb, y, keff, part, lane);
-  aq_partials(tb, y, keff, part, lane);
+  aero_partials(tb, y, keff, part, lane);
   return dev_jac<JT>(tb, y, h, keff, part, Jout, lane, jp, jl);
 }
 __device__ __forceinline__ bool has_simpol(const char* tb) {
