@@ -47,8 +47,10 @@ Outputs (all small):
 
 The cell states follow the workload distribution (camp_b200/cells.py, seed
 20241203) plus a few edge-case cells: concentrations exactly at TINY, a dark
-cell (all photolysis rates zero) and a cell where PAR is nearly exhausted so
-the negative-yield guard of the reference switches contributions off.
+cell (all photolysis rates zero), a cell where PAR is nearly exhausted so
+the negative-yield guard of the reference switches contributions off, and,
+for mechanisms with aqueous equilibria, a cell whose aerosol water is below
+their minimum, which switches them off.
 """
 from __future__ import annotations
 
@@ -151,6 +153,18 @@ def edge_cells(mech, cells):
         if name in mech.species:
             s[mech.index(name)] = 50.0
     extra_s.append(s); extra_e.append([300.0, 1.0e5]); extra_p.append(ph[2])
+    # aqueous equilibria: their water below the reaction's minimum
+    # (1e-4 x absolute tolerance / 10), which switches them off
+    water = set()
+    for r in mech.rxns:
+        if r.rxn_type == 7:  # AQUEOUS_EQUILIBRIUM
+            nr, np_, nph = int(r.ints[0]), int(r.ints[1]), int(r.ints[2])
+            water.update(int(r.ints[3 + (nr + np_) * nph + k]) - 1 for k in range(nph))
+    if water:
+        s = st[3].copy()
+        for i in water:
+            s[i] = 1.0e-4 * mech.abs_tol[i] / 10.0 / 10.0
+        extra_s.append(s); extra_e.append(env[3]); extra_p.append(ph[3])
     return (np.vstack([st, np.asarray(extra_s)]), np.vstack([env, np.asarray(extra_e)]),
             np.vstack([ph, np.asarray(extra_p)]))
 
