@@ -153,3 +153,32 @@ def test_hl_elements_stay_out_of_the_lu(mod37_soa, mod37_aero, lib):
         sizes.append((len(s.solver_jac()[1]), s.n_lu()))
     assert sizes[0][0] == 863 and sizes[1][0] == 3827
     assert sizes[1][1] <= 1.1 * sizes[0][1]
+
+
+@pytest.mark.parametrize("case", ["hl", "aq"])
+def test_variable_water_is_refused(tmp_path, case, lib):
+    """HL and aqueous equilibrium divide by the aerosol-phase water; a water
+    that the solver integrates would need its partials, which this build
+    does not evaluate, so solver_initialize refuses it with a reason
+    (before any device work)."""
+    import json
+
+    from conftest import aq_case, hl_case
+
+    from camp_b200 import _lib
+    from camp_b200.aerosol import load_aerosol_mechanism
+    from camp_b200.solver import Solver
+
+    (hl_case if case == "hl" else aq_case)(tmp_path)
+    path = os.path.join(str(tmp_path), f"{case}.json")
+    doc = json.load(open(path))
+    for o in doc["camp-data"]:
+        if o.get("name") == "H2O_aq":
+            o["tracer type"] = "VARIABLE"
+    with open(path, "w") as fh:
+        json.dump(doc, fh)
+    mech = load_aerosol_mechanism([path])
+    s = Solver(mech, 2)
+    s.build_sparsity_only()
+    assert not s.ready
+    assert "constant" in _lib.last_error()
