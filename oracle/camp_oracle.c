@@ -102,6 +102,10 @@ struct OracleMech {
   double *aph_flt;
   int *arep_int, *arep_ioff, *arep_foff, *arep_eoff, *arep_type, arep_ilen, arep_flen;
   double *arep_flt;
+  /* experiment switches (om_set_experiment); zero = the reference's semantics
+   * and this oracle's positivity rule */
+  double guard_step;
+  int positivity;
 };
 
 OracleMech *om_new(int n_state_var, const int *var_type, int n_rxn) {
@@ -1622,7 +1626,16 @@ typedef struct {
   long nst, nfe, nsetups, netf, nni, ncfn, nje, nstlp, nstlj;
   int jcur;
   double etaqm1, etaq, etaqp1;
+  /* experiment switches copied from the mechanism (om_set_experiment) */
+  double guard_step;
+  int positivity;
+  double *yprev, *hfprev, *gtmp; /* guess-helper work (y_{n-1}, h f_{n-1}) */
 } Bdf;
+
+/* The step that f and J see as their time_step: the integrator's current
+ * step (CVodeGetCurrentStep, src/camp_solver.c:872-876), or a fixed step
+ * when an experiment sets one. */
+static double f_step(const Bdf *b) { return b->guard_step > 0.0 ? b->guard_step : b->h; }
 
 static double wrms(const double *v, const double *w, int n) {
   double s = 0.0;
@@ -1790,7 +1803,7 @@ static int bdf_lsetup(Bdf *b, int convfail, const double *ypred) {
     b->nje++;
     b->nstlj = b->nst;
     b->jcur = 1;
-    int r = b->jac(b->ctx, b->tn, ypred, b->h, b->savedJ);
+    int r = b->jac(b->ctx, b->tn, ypred, f_step(b), b->savedJ);
     if (r < 0) return -1;
     if (r > 0) return 1;
   }
@@ -1827,7 +1840,7 @@ static int bdf_newton_iteration(Bdf *b, int projected) {
       return NL_CONV_FAIL;
     }
     delp = del;
-    int r = b->f(b->ctx, b->tn, b->y, b->h, b->ftemp);
+    int r = b->f(b->ctx, b->tn, b->y, f_step(b), b->ftemp);
     b->nfe++;
     if (r < 0) return -1;
     if (r > 0) {
@@ -1887,6 +1900,48 @@ static int bdf_check_constraints(Bdf *b) {
   return NL_CONSTR_RECVR;
 }
 
+/* Restatement of the reference's guess_helper (src/camp_solver.c:1321-1408)
+ * in its prediction form (h_n > 0), for the positivity experiments: when the
+ * predicted state has a value below -SMALL, advance y_{n-1} over the step by
+ * at most GUESS_MAX_ITER explicit Euler sub-steps, each cut just short of the
+ * first zero crossing (x 0.95 + 0.1 iter / GUESS_MAX_ITER), re-evaluating f
+ * after each, and start Newton from 0.999 of the resulting correction.  The
+ * modified CVODE's call site is not in the reference tree; this calls it once
+ * per prediction.  Returns 1 when acor holds a correction, 0 when none was
+ * needed, -1 when f failed. */
+#define GUESS_MAX_ITER 5
+static int guess_helper(Bdf *b) {
+  int n = b->n;
+  double ymin = b->zn[0][0];
+  for (int i = 1; i < n; ++i) ymin = b->zn[0][i] < ymin ? b->zn[0][i] : ymin;
+  if (ymin > -SMALL) return 0;
+  double h_n = b->h, t_n = b->tn;
+  double *y = b->gtmp, *f = b->acor;
+  memcpy(y, b->yprev, sizeof(double) * n);
+  for (int i = 0; i < n; ++i) f[i] = b->hfprev[i] / h_n;
+  double t_0 = t_n - h_n, t_j = 0.0;
+  for (int iter = 0; iter < GUESS_MAX_ITER && t_0 + t_j < t_n; iter++) {
+    double h_j = t_n - (t_0 + t_j);
+    int i_fast = -1;
+    for (int i = 0; i < n; i++) {
+      double t_star = -y[i] / f[i];
+      if ((t_star > 0.0 || (t_star == 0.0 && f[i] < 0.0)) && t_star < h_j) {
+        h_j = t_star;
+        i_fast = i;
+      }
+    }
+    if (i_fast >= 0) h_j *= 0.95 + 0.1 * iter / (double)GUESS_MAX_ITER;
+    if (t_n < t_0 + t_j + h_j) h_j = t_n - (t_0 + t_j);
+    for (int i = 0; i < n; ++i) y[i] += h_j * f[i];
+    t_j += h_j;
+    int r = b->f(b->ctx, t_0 + t_j, y, f_step(b), f);
+    b->nfe++;
+    if (r != 0) return -1;
+  }
+  for (int i = 0; i < n; ++i) b->acor[i] = 0.999 * (y[i] - b->zn[0][i]);
+  return 1;
+}
+
 static int bdf_nls(Bdf *b, int nflag) {
   int convfail = ((nflag == FIRST_CALL) || (nflag == PREV_ERR_FAIL))
                      ? NO_FAILURES
@@ -1895,14 +1950,23 @@ static int bdf_nls(Bdf *b, int nflag) {
                    (b->nst == 0) || (b->nst >= b->nstlp + MSBP) ||
                    (fabs(b->gamrat - 1.0) > DGMAX);
   int projected = 0;
-  for (int i = 0; i < b->n; ++i) {
-    double a = b->zn[0][i] < 0.0 ? -b->zn[0][i] : 0.0;
-    if (a != 0.0) projected = 1;
-    b->acor[i] = a;
-    b->y[i] = b->zn[0][i] + a;
+  if (b->positivity == OM_POS_GUESS_HELPER || b->positivity == OM_POS_GUESS_HELPER_ONLY) {
+    projected = guess_helper(b) == 1;
+    for (int i = 0; i < b->n; ++i) {
+      if (!projected) b->acor[i] = 0.0;
+      b->y[i] = b->zn[0][i] + b->acor[i];
+    }
+  } else {
+    int project = b->positivity == OM_POS_PROJECT;
+    for (int i = 0; i < b->n; ++i) {
+      double a = (project && b->zn[0][i] < 0.0) ? -b->zn[0][i] : 0.0;
+      if (a != 0.0) projected = 1;
+      b->acor[i] = a;
+      b->y[i] = b->zn[0][i] + a;
+    }
   }
   for (;;) {
-    int r = b->f(b->ctx, b->tn, b->y, b->h, b->ftemp);
+    int r = b->f(b->ctx, b->tn, b->y, f_step(b), b->ftemp);
     b->nfe++;
     if (r < 0) return OR_RHSFUNC_FAIL;
     if (r > 0) return NL_RHS_RECVR;
@@ -1918,12 +1982,15 @@ static int bdf_nls(Bdf *b, int nflag) {
     }
     int ier = bdf_newton_iteration(b, projected);
     if (ier < 0) return OR_RHSFUNC_FAIL;
-    if (ier == NL_OK) return bdf_check_constraints(b);
+    if (ier == NL_OK)
+      return (b->positivity == OM_POS_PROJECT || b->positivity == OM_POS_GUESS_HELPER)
+                 ? bdf_check_constraints(b)
+                 : NL_OK;
     if (ier != NL_TRY_AGAIN) return ier;
     call_setup = 1;
     convfail = FAIL_BAD_J;
     for (int i = 0; i < b->n; ++i) {
-      double a = b->zn[0][i] < 0.0 ? -b->zn[0][i] : 0.0;
+      double a = (b->positivity == OM_POS_PROJECT && b->zn[0][i] < 0.0) ? -b->zn[0][i] : 0.0;
       b->acor[i] = a;
       b->y[i] = b->zn[0][i] + a;
     }
@@ -1981,7 +2048,7 @@ static int bdf_error_test(Bdf *b, int *nflag, double saved_t, int *nef,
   b->next_h = b->h;
   b->hscale = b->h;
   b->qwait = LONG_WAIT;
-  int r = b->f(b->ctx, b->tn, b->zn[0], b->h, b->tempv);
+  int r = b->f(b->ctx, b->tn, b->zn[0], f_step(b), b->tempv);
   b->nfe++;
   if (r < 0) return OR_RHSFUNC_FAIL;
   if (r > 0) return OR_UNREC_RHSFUNC_ERR;
@@ -2070,6 +2137,10 @@ static int bdf_step(Bdf *b) {
   int ncf = 0, nef = 0, nflag = FIRST_CALL;
   if ((b->nst > 0) && (b->hprime != b->h)) bdf_adjust_params(b);
   for (;;) {
+    if (b->positivity == OM_POS_GUESS_HELPER || b->positivity == OM_POS_GUESS_HELPER_ONLY) {
+      memcpy(b->yprev, b->zn[0], sizeof(double) * b->n);
+      memcpy(b->hfprev, b->zn[1], sizeof(double) * b->n);
+    }
     bdf_predict(b);
     bdf_set(b);
     nflag = bdf_nls(b, nflag);
@@ -2103,7 +2174,7 @@ typedef struct {
 } BdfWork;
 
 static void bdf_alloc(Bdf *b, BdfWork *wk, int n, int annz, int lunnz) {
-  size_t tot = (size_t)n * (LMAX + 8) + (size_t)annz + (size_t)lunnz;
+  size_t tot = (size_t)n * (LMAX + 11) + (size_t)annz + (size_t)lunnz;
   wk->mem = (double *)zalloc(sizeof(double) * (tot + 8));
   double *p = wk->mem;
   for (int j = 0; j < LMAX; ++j, p += n) b->zn[j] = p;
@@ -2115,7 +2186,10 @@ static void bdf_alloc(Bdf *b, BdfWork *wk, int n, int annz, int lunnz) {
   b->w = p; p += n;
   b->z = p; p += n;
   b->savedJ = p; p += annz;
-  b->LU = p;
+  b->LU = p; p += lunnz;
+  b->yprev = p; p += n;
+  b->hfprev = p; p += n;
+  b->gtmp = p;
 }
 
 /* One cell from t0 to tout with initial step h0 (CVodeReInit + CVode in
@@ -2148,7 +2222,7 @@ static int bdf_integrate(Bdf *b, double t0, double tout, double h0, double *y,
   }
   b->next_h = 0.0;
   {
-    int r = b->f(b->ctx, t0, b->zn[0], h0, b->zn[1]);
+    int r = b->f(b->ctx, t0, b->zn[0], b->guard_step > 0.0 ? b->guard_step : h0, b->zn[1]);
     b->nfe++;
     if (r != 0) {
       flag = r < 0 ? OR_RHSFUNC_FAIL : OR_REPTD_RHSFUNC_ERR;
@@ -2294,6 +2368,8 @@ static void *solve_job(void *arg) {
   b.max_steps = jb->max_steps;
   b.maxncf = jb->max_conv_fails;
   b.maxnef = jb->max_conv_fails;
+  b.guard_step = m->guard_step;
+  b.positivity = m->positivity;
   CellCtx ctx;
   ctx.m = m;
   b.ctx = &ctx;
@@ -2335,6 +2411,13 @@ static void *solve_job(void *arg) {
 /* The absolute tolerances solver_initialize receives (per state variable):
  * they set the aqueous equilibrium's minimum water. */
 void om_set_abs_tol(const OracleMech *m, const double *abs_tol) { aq_thresholds(m, abs_tol); }
+
+int om_set_experiment(OracleMech *m, double guard_step, int positivity) {
+  if (guard_step < 0.0 || positivity < OM_POS_PROJECT || positivity > OM_POS_NONE) return 1;
+  m->guard_step = guard_step;
+  m->positivity = positivity;
+  return 0;
+}
 
 int om_solve(const OracleMech *m, int n_cells, double *state, const double *env,
              double *rxn_env, double t0, double t1, double rtol,
@@ -2397,6 +2480,8 @@ int om_solve_cb(const OracleMech *m, int n_cells, double *y_dep, double t0,
   b.max_steps = max_steps;
   b.maxncf = max_conv_fails;
   b.maxnef = max_conv_fails;
+  b.guard_step = m->guard_step;
+  b.positivity = m->positivity;
   int nf = 0;
   for (int c = 0; c < n_cells; ++c) {
     b.ctx = ctxs[c];

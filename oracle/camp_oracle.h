@@ -75,6 +75,26 @@ int om_build(OracleMech *m);
 void om_set_abs_tol(const OracleMech *m, const double *abs_tol);
 void om_free(OracleMech *m);
 
+/* Experiment switches of the integrator (defaults 0, 0):
+ *   guard_step  0 = f and J get the integrator's current step as their
+ *               time_step, as the reference's f does through
+ *               CVodeGetCurrentStep (src/camp_solver.c:872-876), which the
+ *               negative-yield product guard multiplies
+ *               (src/rxns/rxn_arrhenius.c:153-160); > 0 = that fixed step
+ *               instead (not the reference's semantics; it shows what the
+ *               step dependence of the guard costs);
+ *   positivity  how a predicted or corrected state below zero is handled:
+ *               OM_POS_PROJECT (this oracle's rule and the device's),
+ *               OM_POS_GUESS_HELPER (the reference's guess_helper restated,
+ *               with the constraint check), OM_POS_GUESS_HELPER_ONLY, or
+ *               OM_POS_NONE (plain CVODE).
+ * Returns nonzero for an invalid setting. */
+#define OM_POS_PROJECT 0
+#define OM_POS_GUESS_HELPER 1
+#define OM_POS_GUESS_HELPER_ONLY 2
+#define OM_POS_NONE 3
+int om_set_experiment(OracleMech *m, double guard_step, int positivity);
+
 int om_n_dep_var(const OracleMech *m);
 int om_n_rxn_env_data(const OracleMech *m);
 int om_n_rxn_jac_elem(const OracleMech *m);

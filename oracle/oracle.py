@@ -71,6 +71,8 @@ def oracle_lib():
         lib.om_build.restype = C.c_int
         lib.om_build.argtypes = [vp]
         lib.om_set_abs_tol.argtypes = [vp, _f64p]
+        lib.om_set_experiment.restype = C.c_int
+        lib.om_set_experiment.argtypes = [vp, C.c_double, C.c_int]
         lib.om_free.argtypes = [vp]
         for name in (
             "om_n_dep_var",
@@ -208,6 +210,16 @@ class OracleModel:
             self.lib.om_free(self.h)
         except Exception:
             pass
+
+    # positivity rules of set_experiment (camp_oracle.h)
+    POS_PROJECT, POS_GUESS_HELPER, POS_GUESS_HELPER_ONLY, POS_NONE = 0, 1, 2, 3
+
+    def set_experiment(self, guard_step: float = 0.0, positivity: int = 0) -> None:
+        """Integrator experiment switches (camp_oracle.h om_set_experiment):
+        a fixed time_step for f and J instead of the current step (0 = the
+        reference's semantics), and the positivity rule."""
+        if self.lib.om_set_experiment(self.h, float(guard_step), int(positivity)) != 0:
+            raise ValueError("invalid experiment setting")
 
     def solver_jac(self):
         cp = np.zeros(self.n_dep + 1, np.int32)
