@@ -1,25 +1,30 @@
-"""Benchmark: cell-steps/s of the per-cell chemistry solve on B200.
+"""Benchmark: successful cell-steps/s of the per-cell chemistry solve on B200.
 
 Workload (default): the cb05cl_ae5 gas-phase mechanism (74 dependent species,
-186 reactions) on 10 000 seeded synthetic cells (--cells 100000 for the 1e5
-case; the persistent kernel keeps every SM busy from ~2 000 cells up, so the
-throughput per cell-step is the same), host steps of 60 s, rtol
-1e-4, atol 1e-8 ppm, the reference's default limits (10 000 internal steps,
-1 000 convergence / error-test failures).  Cell states: T ~ U(260, 310) K,
-P ~ U(5e4, 1.013e5) Pa, photolysis = 1e-4 s^-1 base set (jo2 = 0) x U[0,1],
-variable species log-uniform 1e-6..1e2 ppm (seed 20241203).
+186 reactions) on 100 000 seeded synthetic cells per GPU, the 10-step
+sequence of 60 s host steps, rtol 1e-4, atol 1e-8 ppm, the reference's
+default limits (10 000 internal steps, 1 000 convergence / error-test
+failures).  Cell states: T ~ U(260, 310) K, P ~ U(5e4, 1.013e5) Pa,
+photolysis = 1e-4 s^-1 base set (jo2 = 0) x U[0,1], variable species
+log-uniform 1e-6..1e2 ppm (seed 20241203).  No dataset exists for this path;
+seeded synthetic cells with the workload's distributions stand in for it.
 
 One bench "step" is one host time step: every cell advanced over 60 s by its
-own BDF integration.  The 10-step sequence of the workload restarts from the
-seeded initial state every 10 steps.  value = cells x steps / device time of
-the timed steps (CUDA events on the launch stream, L2 flushed between steps),
-max over ranks; e2e = the same through solver_run with pinned host buffers
-(host<->device copies inside the timed region, host clock).
+own BDF integration.  The sequence restarts from the seeded state every 10
+steps (warm-up steps included).  About a quarter of these cells cannot
+finish a host step under the reference's semantics (they end in
+TOO_MUCH_WORK after 10 000 internal steps; see tests/test_hard_cells.py), so
+value counts successful cell-steps only: cells that finished their host step
+x steps / device time of the timed steps (CUDA events on the launch stream,
+L2 flushed between steps), max over ranks; every cell-step, failed or not, is
+reported beside it.  e2e = the same through solver_run with pinned host
+buffers (host<->device copies inside the timed region, host clock) over the
+first --e2e-steps steps of the sequence.
 
 --impl reference times the reference's own C derivative/Jacobian code
 (compiled from the reference sources into oracle/_ref) driven by the restated
-CVODE BDF and sparse LU on all host cores, on a bounded sample of the same
-workload (the same 10-step sequence for a subset of the cells).
+CVODE BDF and sparse LU on all host cores, on a sample of 1 024 cells of the
+same workload with the GPU arm's mix of host-step positions in the sequence.
 """
 from __future__ import annotations
 
@@ -46,13 +51,13 @@ MOD37_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_gas.mech.json"
 # species into cloud and rain water (HL) as well
 MOD37_SOA_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_soa.mech.json")
 MOD37_AERO_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_aero.mech.json")
-# compulsory HBM bytes per cell-step of cb05cl_ae5: state read (80 x 8),
-# env (16), photolysis base rates (25 x 8), dependent state write (74 x 8)
 METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
-# DRAM bytes (read + write) per cell of one solve launch, from the ncu capture
-# summarised in profiles/solve_kernel_mixed_cb05_2000cells.md (3.19 MB for
-# 2 000 cells); the launch's traffic grows with the cells it processes
+# DRAM bytes (read + write) per cell of one solve launch, from an ncu capture
+# of the solve kernel on 2 000 cells (3.19 MB); the launch's traffic grows
+# with the cells it processes
 TRAFFIC_BYTES_PER_CELL = 3.187e6 / 2000
+# nominal B200 FP64 (non-tensor) peak, for the algorithmic-flop fraction
+FP64_PEAK_TFLOPS = 40.0
 
 
 def parse():
@@ -61,17 +66,24 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cells", type=int, default=10000)
+    ap.add_argument("--cells", type=int, default=100000)
     ap.add_argument("--dt", type=float, default=60.0)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=3,
+                    help="timed steps of the FP64 comparison (first steps of the sequence)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="timed steps of the end-to-end measurement (first steps of the sequence)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=128)
+    ap.add_argument("--cpu-sample", type=int, default=1024,
+                    help="cells of the reference arm's sample")
+    ap.add_argument("--cpu-baseline-sample", type=int, default=256,
+                    help="cells of the GPU arm's cpu_baseline sample")
+    ap.add_argument("--cpu-one-core", type=int, default=24,
+                    help="cells timed on one core for the single-core figure")
     ap.add_argument("--max-steps", type=int, default=10000)
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--no-1e5", action="store_true",
-                    help="skip the 1e5-cell single-host-step measurement")
     ap.add_argument("--no-mod37", action="store_true",
                     help="skip the mod37 blocks (gas phase; SOA; SOA + cloud partitioning)")
     ap.add_argument("--no-cost-order", action="store_true",
@@ -161,42 +173,79 @@ def barrier(world):
 # ---------------------------------------------------------------------------
 # CPU reference arm
 # ---------------------------------------------------------------------------
-def cpu_reference_run(mech, cells, steps, warmup, dt, sample, max_steps):
-    """Times the reference's C f/J + restated BDF on all host cores; each step
-    is the same host step of the 10-step sequence for `sample` cells."""
-    from oracle.oracle import ref_available, ref_solve, OracleModel
+def sequence_positions(steps: int, warmup: int) -> list[int]:
+    """Host-step position in the 10-step sequence of each timed step (the
+    sequence restarts from the seeded state every 10 steps, warm-up steps
+    included)."""
+    return [(warmup + k) % 10 for k in range(steps)]
+
+
+def cpu_sample_run(mech, n_sample, positions, dt, max_steps, one_core_cells):
+    """Successful cell-steps/s of the CPU path on a sample of the workload:
+    the first n_sample seeded cells of the GPU arm, cell i taken at host-step
+    position positions[i % len(positions)] of the sequence (so the sample has
+    the timed region's mix of positions and hard cells).  Each cell is first
+    advanced, untimed, to its position (a cell that fails keeps its state, as
+    solver_run leaves it, so it is not advanced again); then every cell's
+    host step is timed as one job on all host cores (cells taken in chunks of
+    8 by the threads) and, for the single-core figure, one_core_cells of
+    them spread evenly over the sample on one thread."""
+    from camp_b200.cells import make_cells
+    from oracle.oracle import OracleModel, ref_available, ref_solve
 
     n_threads = os.cpu_count() or 1
     atol = np.full(mech.n_state_var, 1e-8)
     kind = "reference" if ref_available() else "port"
-    sub = cells.slice(0, sample)
-    state = sub.state.copy()
-    times = []
     om = None if kind == "reference" else OracleModel(mech)
-    for it in range(warmup + steps):
-        if it % 10 == 0:
-            state = sub.state.copy()
-        t0 = time.perf_counter()
+
+    def solve(st, env, photo, threads):
         if kind == "reference":
-            ref_solve(mech, state, sub.env, sub.photo_rates, 0.0, dt, 1e-4, atol,
-                      max_steps=max_steps, n_threads=n_threads)
-        else:
-            om.solve(state, sub.env, sub.photo_rates, 0.0, dt, 1e-4, atol,
-                     max_steps=max_steps, n_threads=n_threads)
-        if it >= warmup:
-            times.append(time.perf_counter() - t0)
-    per_step = float(np.mean(times))
+            status, _ = ref_solve(mech, st, env, photo, 0.0, dt, 1e-4, atol, max_steps=max_steps,
+                                  n_threads=threads, chunk=8)
+            return status
+        _, status, _, _ = om.solve(st, env, photo, 0.0, dt, 1e-4, atol, max_steps=max_steps,
+                                   n_threads=threads)
+        return status
+
+    cells = make_cells(mech, n_sample, SEED)
+    pos = np.asarray([positions[i % len(positions)] for i in range(n_sample)])
+    state = cells.state.copy()
+    stuck = np.zeros(n_sample, bool)
+    for j in range(1, 10):
+        idx = np.nonzero((pos >= j) & ~stuck)[0]
+        if idx.size == 0:
+            continue
+        st = np.ascontiguousarray(state[idx])
+        status = solve(st, cells.env[idx], cells.photo_rates[idx], n_threads)
+        state[idx] = st
+        stuck[idx[status != 0]] = True
+    timed = state.copy()
+    t0 = time.perf_counter()
+    status = solve(timed, cells.env, cells.photo_rates, n_threads)
+    wall = time.perf_counter() - t0
+    ok = int(np.count_nonzero(status == 0))
+    m = min(one_core_cells, n_sample)
+    sel = np.linspace(0, n_sample - 1, m).astype(int)  # spread over the sample
+    one = state[sel].copy()
+    t0 = time.perf_counter()
+    st1 = solve(one, cells.env[sel], cells.photo_rates[sel], 1)
+    wall1 = time.perf_counter() - t0
+    how = ("reference C f/J compiled from the reference sources + restated CVODE BDF / sparse LU"
+           if kind == "reference" else
+           "oracle C restatement of the reference f/J + restated CVODE BDF / sparse LU")
     return {
-        "value": sample / per_step,
+        "value": ok / wall,
         "unit": "cell-steps/s",
         "cores": n_threads,
         "kind": kind,
-        "sample": (f"{sample} cells x {steps} host steps of {dt:g} s (the workload's 10-step "
-                   f"sequence for the first {sample} seeded cells); "
-                   + ("reference C f/J compiled from the reference sources + restated "
-                      "CVODE BDF / sparse LU" if kind == "reference" else
-                      "oracle C restatement of the reference f/J + restated CVODE BDF / sparse LU")),
-        "ms_per_step": per_step * 1e3,
+        "sample": (f"{n_sample} seeded cells of the workload, one host step of {dt:g} s each at "
+                   f"the timed region's sequence positions {sorted(set(positions))}; "
+                   f"successful cell-steps / wall time on {n_threads} threads; {how}"),
+        "all_cell_steps_per_s": n_sample / wall,
+        "ok_cell_fraction": ok / n_sample,
+        "one_core": {"value": int(np.count_nonzero(st1 == 0)) / wall1, "cells": m,
+                     "all_cell_steps_per_s": m / wall1},
+        "wall_s": wall,
     }
 
 
@@ -205,13 +254,12 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from camp_b200.cells import make_cells
     from camp_b200.mechanism import Mechanism
 
     mech = Mechanism.load(MECH_FILE)
-    cells = make_cells(mech, args.cpu_sample, SEED)
-    cb = cpu_reference_run(mech, cells, args.steps, args.warmup, args.dt, args.cpu_sample,
-                           args.max_steps)
+    positions = sequence_positions(args.steps, args.warmup)
+    cb = cpu_sample_run(mech, args.cpu_sample, positions, args.dt, args.max_steps,
+                        args.cpu_one_core)
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -220,15 +268,20 @@ def run_reference_arm(args):
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": cb["ms_per_step"],
+        "ms_per_step": 1e3 * cb["wall_s"] / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "cb05cl_ae5 cell states, host steps of 60 s, rtol 1e-4, atol 1e-8 ppm",
-                   "cells_per_step": args.cpu_sample, "dt_s": args.dt},
+        "config": {"workload": "cb05cl_ae5, the GPU arm's seeded cells, host steps of 60 s "
+                               "(10-step sequence), rtol 1e-4, atol 1e-8 ppm, max "
+                               f"{args.max_steps} internal steps",
+                   "cells_sampled": args.cpu_sample, "dt_s": args.dt, "seed": SEED},
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "all_cell_steps_per_s": cb["all_cell_steps_per_s"],
+        "ok_cell_fraction": cb["ok_cell_fraction"],
+        "one_core": cb["one_core"],
         "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -319,14 +372,62 @@ def serving_run(args, precision):
 
 
 # ---------------------------------------------------------------------------
-# 1e5 cells, one host step
+# Algorithmic flops
 # ---------------------------------------------------------------------------
-def run_1e5(mech, args, dev, stream, n=100000):
-    """The metric's cell count: 1e5 seeded cells over the first host step of
-    the sequence (the most expensive one: every cell starts from its seeded
-    state), mixed and FP64, device-resident, longest-first order from a
-    previous identical run; device time of the second run.  Also used with
-    another mechanism and cell count for the mod37 blocks."""
+def flop_model(mech, solver) -> dict:
+    """Flops of each counted operation of one cell, from the mechanism and
+    the solver's sparsity and elimination order: f (rate = k x reactants,
+    one add per loss or gain, one multiply per yield, P - L per species), J
+    (the partials and their gathers, 2 nr (nr + np) per reaction), the LU of
+    M = I - gamma J (2 per Schur update, 1 per L scaling, 1 reciprocal per
+    pivot, 2 per entry of M), one solve (2 per LU entry) and the BDF vector
+    work of one internal step (prediction, Newton updates, norms, error
+    test, history update: about 30 per dependent species)."""
+    f = j = 0
+    for r in mech.rxns:
+        nr, npd = int(r.ints[0]), int(r.ints[1])
+        f += nr + nr + 2 * npd
+        j += 2 * nr * (nr + npd)
+    n = mech.n_dep_var
+    f += n
+    cp, ri = solver.solver_jac()
+    perm = solver.lu_order()
+    pos = np.empty(n, int)
+    pos[perm] = np.arange(n)
+    rows = [set() for _ in range(n)]  # pattern in pivot order, by row
+    for c in range(n):
+        for r in ri[cp[c]:cp[c + 1]]:
+            rows[pos[r]].add(pos[c])
+    for i in range(n):
+        rows[i].add(i)
+    upd = scal = 0
+    for k in range(n):  # right-looking symbolic elimination
+        urow = [c for c in rows[k] if c > k]
+        for i in range(k + 1, n):
+            if k in rows[i]:
+                scal += 1
+                upd += len(urow)
+                rows[i].update(urow)
+    nnz = sum(len(r) for r in rows)
+    return {"f": f, "jac": j, "lu": 2 * upd + scal + n + 2 * nnz, "solve": 2 * nnz,
+            "bdf_step": 30 * n, "lu_entries": nnz, "lu_entries_solver": solver.n_lu()}
+
+
+def counted_flops(model: dict, stats) -> float:
+    """Flops of the operations the per-cell counters recorded."""
+    return float(model["f"] * stats["nfe"].sum() + model["jac"] * stats["nje"].sum()
+                 + model["lu"] * stats["nsetups"].sum() + model["solve"] * stats["nni"].sum()
+                 + model["bdf_step"] * stats["nst"].sum())
+
+
+# ---------------------------------------------------------------------------
+# First host step of other mechanisms
+# ---------------------------------------------------------------------------
+def run_first_step(mech, args, dev, stream, n):
+    """n seeded cells of another mechanism over the first host step of the
+    sequence (every cell from its seeded state), mixed and FP64,
+    device-resident, longest-first order from a previous identical run;
+    device time of the second run."""
     import torch
 
     from camp_b200.cells import make_cells
@@ -359,11 +460,14 @@ def run_1e5(mech, args, dev, stream, n=100000):
             torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         st = s.cell_stats(n)
-        nst = int(st["nst"].sum())
-        out[name] = {"cell_steps_per_s": n / (ms / 1e3), "internal_steps_per_s": nst / (ms / 1e3),
-                     "ms": ms, "ok_cell_fraction": float(np.mean(st["status"] == 0))}
+        ok = int(np.count_nonzero(st["status"] == 0))
+        out[name] = {"ok_cell_steps_per_s": ok / (ms / 1e3),
+                     "cell_steps_per_s": n / (ms / 1e3),
+                     "internal_steps_per_s": int(st["nst"].sum()) / (ms / 1e3),
+                     "ms": ms, "ok_cell_fraction": ok / n}
         s.free()
-    out["mixed_over_fp64"] = out["mixed"]["cell_steps_per_s"] / out["fp64"]["cell_steps_per_s"]
+    out["mixed_over_fp64"] = (out["mixed"]["ok_cell_steps_per_s"]
+                              / out["fp64"]["ok_cell_steps_per_s"])
     return out
 
 
@@ -407,14 +511,15 @@ def run_gpu_arm(args):
     init_state = torch.from_numpy(cells.state).to(dev)
     d_env = torch.from_numpy(cells.env).to(dev)
     d_photo = torch.from_numpy(np.ascontiguousarray(cells.photo_rates)).to(dev)
+    stat_keys = ("nst", "nfe", "nje", "nsetups", "nni")
 
     def device_run(s, steps, warmup):
         """warmup + timed host steps on device-resident inputs."""
         d_state = init_state.clone()
         # every input resident in HBM: photolysis rates from device memory too
         s.set_photo_rates_device(d_photo, n)
-        step_ms, ok_cells, launches0 = [], [], None
-        kernel_ms = []
+        step_ms, kernel_ms, ok_cells, launches0 = [], [], [], None
+        counters = {k: 0 for k in stat_keys}
         for it in range(warmup + steps):
             if it % 10 == 0:
                 d_state.copy_(init_state)
@@ -435,72 +540,95 @@ def run_gpu_arm(args):
                 kernel_ms.append(s.last_kernel_ms())
                 st = s.cell_stats(n)
                 ok_cells.append(int(np.count_nonzero(st["status"] == 0)))
+                for k in stat_keys:
+                    counters[k] += int(st[k].sum())
         torch.cuda.synchronize()
         barrier(world)
         launches = s.kernel_launches() - launches0
-        return step_ms, kernel_ms, ok_cells, launches, s.cell_stats(n)
+        return step_ms, kernel_ms, ok_cells, launches, counters
 
     prec = MIXED if args.precision == "mixed" else FP64
     solver = make_solver(prec)
     with ClockSampler(local) as clk:
-        step_ms, kernel_ms, ok_cells, launches, last_stats = device_run(solver, args.steps, args.warmup)
+        step_ms, kernel_ms, ok_cells, launches, counters = device_run(solver, args.steps,
+                                                                      args.warmup)
     total_s = max_over_ranks(sum(step_ms) / 1e3, world)
-    value = replicas.aggregate_throughput(n, args.steps, world, total_s)
+    ok_total = replicas.sum_over_ranks(sum(ok_cells), world)
+    value = ok_total / total_s
+    all_value = replicas.aggregate_throughput(n, args.steps, world, total_s)
     fp64 = None
     if not args.no_fp64_compare:
+        k64 = min(args.fp64_steps, args.steps)
         s64 = make_solver(FP64)
-        sm64, km64, ok64, _, _ = device_run(s64, args.steps, min(args.warmup, 3))
+        sm64, km64, ok64, _, c64 = device_run(s64, k64, 1)
         t64 = max_over_ranks(sum(sm64) / 1e3, world)
-        fp64 = {"value": replicas.aggregate_throughput(n, args.steps, world, t64),
+        ok64_total = replicas.sum_over_ranks(sum(ok64), world)
+        # the mixed form over the same first steps of the sequence
+        same = min(k64, args.steps)
+        fp64 = {"value": ok64_total / t64,
                 "unit": "cell-steps/s",
-                "ms_per_step": 1e3 * t64 / args.steps,
-                "ok_cell_fraction": float(np.mean(ok64)) / n}
+                "steps": k64,
+                "ms_per_step": 1e3 * t64 / k64,
+                "all_cell_steps_per_s": replicas.aggregate_throughput(n, k64, world, t64),
+                "ok_cell_fraction": float(np.mean(ok64)) / n,
+                "note": f"first {k64} timed steps of the sequence after 1 warm-up step"}
         s64.free()
+        # the mixed form over the same sequence positions, for the ratio
+        sm_m, _, ok_m, _, _ = device_run(solver, k64, 1)
+        tm = max_over_ranks(sum(sm_m) / 1e3, world)
+        okm_total = replicas.sum_over_ranks(sum(ok_m), world)
+        fp64["mixed_same_steps"] = okm_total / tm
+        fp64["mixed_over_fp64"] = fp64["mixed_same_steps"] / fp64["value"]
     e2e = None
     if not args.no_e2e:
+        ke = min(args.e2e_steps, args.steps)
         # pinned host buffers; copies inside the timed region
         h_state = torch.empty((n, mech.n_state_var), dtype=torch.float64, pin_memory=True)
         h_env = torch.from_numpy(cells.env).pin_memory()
         hs, he = h_state.numpy(), h_env.numpy()
         # end to end: photolysis rates travel from the host with each run
         solver.set_photo_rates_device(None)
-        times = []
-        for it in range(args.warmup + args.steps):
-            if it % 10 == 0:
-                hs[:] = cells.state
+        times, oks = [], []
+        for it in range(1 + ke):
+            if it % 10 == 0 or it == 1:
+                hs[:] = cells.state  # warm-up, then the sequence from its start
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             solver.solve(hs, he, 0.0, args.dt)
-            if it >= args.warmup:
+            if it >= 1:
                 times.append(time.perf_counter() - t0)
+                oks.append(int(np.count_nonzero(solver.cell_stats(n)["status"] == 0)))
         te = max_over_ranks(sum(times), world)
         n_photo = solver.n_photo
-        e2e = {"value": replicas.aggregate_throughput(n, args.steps, world, te),
+        e2e = {"value": replicas.sum_over_ranks(sum(oks), world) / te,
                "unit": "cell-steps/s",
                "h2d_bytes_per_step": int(8 * n * (mech.n_state_var + 2 + n_photo)),
-               "d2h_bytes_per_step": int(8 * n * mech.n_state_var + 56 * n)}
+               "d2h_bytes_per_step": int(8 * n * mech.n_state_var + 56 * n),
+               "steps": ke,
+               "all_cell_steps_per_s": replicas.aggregate_throughput(n, ke, world, te),
+               "note": f"solver_run on pinned host buffers, first {ke} steps of the sequence "
+                       "after 1 warm-up step, host clock"}
     serving = None
     if world == 1 and not args.no_serving:
         serving = serving_run(args, prec)
-    at_1e5 = None
-    if world == 1 and not args.no_1e5:
-        at_1e5 = run_1e5(mech, args, dev, stream)
     mod37 = mod37_soa = mod37_aero = None
     if world == 1 and not args.no_mod37:
-        mod37 = run_1e5(Mechanism.load(MOD37_FILE), args, dev, stream, n=10000)
-        mod37_soa = run_1e5(Mechanism.load(MOD37_SOA_FILE), args, dev, stream, n=10000)
-        mod37_aero = run_1e5(Mechanism.load(MOD37_AERO_FILE), args, dev, stream, n=10000)
+        mod37 = run_first_step(Mechanism.load(MOD37_FILE), args, dev, stream, 10000)
+        mod37_soa = run_first_step(Mechanism.load(MOD37_SOA_FILE), args, dev, stream, 10000)
+        mod37_aero = run_first_step(Mechanism.load(MOD37_AERO_FILE), args, dev, stream, 10000)
+    fm = flop_model(mech, solver)
     if rank != 0:
         solver.free()
         replicas.finalize(world)
         return
     cb = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu_cells = make_cells(mech, args.cpu_sample, SEED)
-        cb = cpu_reference_run(mech, cpu_cells, min(args.steps, 10), 1, args.dt, args.cpu_sample,
-                               args.max_steps)
-        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = cpu_sample_run(mech, args.cpu_baseline_sample,
+                            sequence_positions(args.steps, args.warmup), args.dt,
+                            args.max_steps, args.cpu_one_core)
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "one_core",
+                                 "ok_cell_fraction")}
     bpcs = bytes_per_cell_step(mech)
     mean_kernel_s = float(np.mean(kernel_ms)) / 1e3
     achieved = bpcs * n / mean_kernel_s / 1e9
@@ -510,6 +638,9 @@ def run_gpu_arm(args):
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
+    flops = counted_flops(fm, {k: np.asarray([counters[k]]) for k in stat_keys})
+    tflops = flops / (sum(kernel_ms) / 1e3) / 1e12
+    internal = counters["nst"]
     line = {
         "metric": METRIC,
         "value": value,
@@ -527,13 +658,15 @@ def run_gpu_arm(args):
         "config": {
             "workload": f"cb05cl_ae5, {n} cells per GPU, host steps of {args.dt:g} s "
                         "(10-step sequence), rtol 1e-4, atol 1e-8 ppm, max "
-                        f"{args.max_steps} internal steps",
+                        f"{args.max_steps} internal steps; value counts cells that finish "
+                        "their host step",
             "cells_per_gpu": n, "dt_s": args.dt, "precision": args.precision,
             "l2": "flushed (256 MB write) before every timed step",
             "seed": SEED,
         },
+        "all_cell_steps_per_s": all_value,
         "ok_cell_fraction": float(np.mean(ok_cells)) / n,
-        "internal_steps_per_cell_step": float(np.mean(last_stats["nst"])),
+        "internal_steps_per_cell_step": internal / (n * args.steps),
         "fp64": fp64,
         "e2e": e2e,
         "gpu_launches": launches,
@@ -547,13 +680,23 @@ def run_gpu_arm(args):
             "traffic": TRAFFIC_BYTES_PER_CELL * n,
             "note": f"{bpcs} compulsory bytes per cell-step x cells / mean solve-kernel time "
                     "(of measured peak); traffic = ncu DRAM bytes per launch scaled from a "
-                    "2000-cell capture; the kernel is bound by dependent-issue latency (IPC "
-                    "1.0, FP64 pipe 4.4 %, profiles/solve_kernel_mixed_cb05_2000cells.md), "
-                    "not by HBM",
+                    "2000-cell capture.  HBM is not what bounds this kernel: see issue_bound",
+        },
+        "issue_bound": {
+            "bound": "dependent-issue latency (warp per cell, cells resident in shared memory)",
+            "achieved_fp64_tflops": tflops,
+            "peak_fp64_tflops_nominal": FP64_PEAK_TFLOPS,
+            "flop_frac": tflops / FP64_PEAK_TFLOPS,
+            "flops_per_internal_step": flops / max(internal, 1),
+            "internal_steps_per_s": internal / (sum(kernel_ms) / 1e3),
+            "flop_model": fm,
+            "note": "algorithmic flops of the counted f / J / LU / solve / BDF-step operations "
+                    "(per-cell device counters) / kernel time, against the nominal FP64 peak; "
+                    "ncu: IPC ~1.0 of 4, FP64 pipe ~4 %, warp stalls on fixed-latency "
+                    "dependencies and shared-memory loads",
         },
         "cpu_baseline": cb,
         "serving": serving,
-        "cells_1e5": at_1e5,
         "mod37_gas": mod37,
         "mod37_soa": mod37_soa,
         "mod37_aero": mod37_aero,

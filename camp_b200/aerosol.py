@@ -24,10 +24,15 @@ What is restated, from the reference's Fortran:
   packer over every instance of a phase
   (``src/rxns/rxn_wet_deposition.F90:172-254``).
 
+* the ZSR aerosol-water and PD-FiTE activity sub-models
+  (``src/sub_models/sub_model_ZSR_aerosol_water.F90:215-500``,
+  ``src/sub_models/sub_model_PDFiTE.F90:250-700``), in camp_core's priority
+  order.
+
 Aerosol-representation ids (``AERO_REP_ID_``) are given 1, 2, ... as a host
 does through ``set_id`` before it creates GMD/GSD update data.  Other aerosol
-types (single particle, condensed-phase reactions, sub-models) are not
-packed here.
+types (single particle, condensed-phase reactions, UNIFAC) are not packed
+here.
 """
 from __future__ import annotations
 
@@ -39,7 +44,8 @@ from typing import Iterable
 import numpy as np
 
 from .mechanism import (CHEM_SPEC_ACTIVITY_COEFF, CHEM_SPEC_CONSTANT, CHEM_SPEC_PSSA,
-                        CHEM_SPEC_VARIABLE, RXN_WET_DEPOSITION, Mechanism, PackedRxn, _read_json,
+                        CHEM_SPEC_VARIABLE, RXN_WET_DEPOSITION, SUB_MODEL_PDFITE,
+                        SUB_MODEL_ZSR_AEROSOL_WATER, Mechanism, PackedRxn, SubModel, _read_json,
                         _SpeciesDB, assign_rate_ids, pack_reaction)
 
 AERO_REP_MODAL_BINNED_MASS = 2  # src/aero_rep_solver.c:20
@@ -48,6 +54,10 @@ RXN_AQUEOUS_EQUILIBRIUM = 7     # src/rxn_solver.c:25
 RXN_SIMPOL_PHASE_TRANSFER = 10  # src/rxn_solver.c:26
 BINNED, MODAL = 1, 2            # src/aero_reps/aero_rep_modal_binned_mass.c:25-26
 UNIV_GAS_CONST = 8.314472       # src/constants.F90
+# sub-model calculation priorities (lower first):
+# src/sub_models/sub_model_ZSR_aerosol_water.F90:705-714,
+# src/sub_models/sub_model_PDFiTE.F90:865-874
+SUB_MODEL_PRIORITY = {"SUB_MODEL_ZSR_AEROSOL_WATER": 1.0, "SUB_MODEL_PDFITE": 2.0}
 PI = 3.14159265358979323846
 # the Fortran packer's -9999.9 is a default-kind (single precision) literal
 UNSET = float(np.float32(-9999.9))
@@ -481,6 +491,219 @@ def pack_wet_deposition_phase(rxn: dict, reps: list[AeroRep],
     return pack_wet_deposition(ids, float(rxn.get("scaling factor", 1.0)), str(rxn.get("rxn id", "")))
 
 
+def _instances(reps: list[AeroRep], phases: list[AeroPhase], phase: str,
+               spec: str) -> list[int]:
+    """1-based state ids of a species in every instance of a phase, over the
+    representations in order (unique_names + spec_state_id)."""
+    out = []
+    for rep in reps:
+        out += [rep.state_id(nm) for nm in rep.names(phases, phase, spec)]
+    return out
+
+
+def _relative_id(reps, phases, phase, spec, water_ids, what) -> int:
+    """State id of spec relative to the aerosol water of the same instance,
+    the same for every instance (the Fortran packers' relative ids)."""
+    ids = _instances(reps, phases, phase, spec)
+    if len(ids) != len(water_ids):
+        raise ValueError(f"Incorrect number of instances of {what} '{spec}' in phase '{phase}'")
+    rel = {i - w for i, w in zip(ids, water_ids)}
+    if len(rel) != 1:
+        raise ValueError(f"{what} '{spec}' is not at the same place in every instance")
+    return rel.pop()
+
+
+def _ion_pair_ions(ions: dict, db: _SpeciesDB, what: str) -> list[tuple[str, int, float, int]]:
+    """(name, qty, molecular weight, charge) of the two ions of a pair, in
+    their JSON order; the pair must be neutral."""
+    if len(ions) != 2:
+        raise ValueError(f"Invalid number of unique ions for ion pair in {what}: "
+                         f"expected 2, got {len(ions)}")
+    out = []
+    total = 0
+    for ion, props in ions.items():
+        qty = int((props or {}).get("qty", 1))
+        if ion not in db.props:
+            raise KeyError(f"Missing species properties for ion '{ion}' in {what}")
+        sp = db.props[ion]
+        if "molecular weight [kg mol-1]" not in sp or "charge" not in sp:
+            raise KeyError(f"Missing molecular weight or charge for ion '{ion}' in {what}")
+        charge = int(sp["charge"])
+        if charge == 0:
+            raise ValueError(f"Neutral species '{ion}' not allowed in an ion pair in {what}")
+        total += qty * charge
+        out.append((ion, qty, float(sp["molecular weight [kg mol-1]"]), charge))
+    if total != 0:
+        raise ValueError(f"Charge imbalance for an ion pair in {what}: total charge {total}")
+    return out
+
+
+def pack_zsr_aerosol_water(obj: dict, db: _SpeciesDB, gas_index: dict[str, int],
+                           reps: list[AeroRep], phases: list[AeroPhase]) -> SubModel:
+    """SUB_MODEL_ZSR_AEROSOL_WATER
+    (src/sub_models/sub_model_ZSR_aerosol_water.F90:215-500).
+
+    ints: ``[NUM_PHASE_, GAS_WATER_ID_, NUM_ION_PAIR_, TOTAL_INT_PARAM_,
+    TOTAL_FLOAT_PARAM_, PHASE_ID_(p), PAIR_INT_PARAM_LOC_(x),
+    PAIR_FLOAT_PARAM_LOC_(x)]`` and per ion pair, JACOBSON: ``[TYPE_ 1,
+    NUM_CATION_, NUM_ANION_, CATION_ID_, ANION_ID_, NUM_Y_, GAS_WATER_JAC_ID_
+    (p), CATION_JAC_ID_(p), ANION_JAC_ID_(p)]``, floats ``[low_RH_,
+    CATION_MW_, ANION_MW_, Y_(j)]``; EQSAM: ints ``[TYPE_ 2, NUM_ION_,
+    GAS_WATER_JAC_ID_(p), ION_ID_(y), ION_JAC_ID_(p, y)]``, floats ``[NW_,
+    ZW_, ION_PAIR_MW_, ION_MW_(y)]``.  Ion and water ids are relative to the
+    phase instance's aerosol water; Jacobian ids are written by the solver.
+    One env parameter (ppm of gas water -> relative humidity)."""
+    what = "ZSR aerosol water"
+    phase = obj["aerosol phase"]
+    water = obj["aerosol-phase water"]
+    if db.var_type_of(water) != CHEM_SPEC_CONSTANT:
+        raise ValueError(f"ZSR calculated species {water} must be of tracer type CONSTANT")
+    water_ids = _instances(reps, phases, phase, water)
+    n_phase = len(water_ids)
+    if n_phase == 0:
+        raise ValueError(f"Aerosol phase '{phase}' not present in any aerosol representation "
+                         f"for {what}")
+    pairs = list((obj.get("ion pairs") or {}).items())
+    if not pairs:
+        raise ValueError(f"Empty ion pair set in {what}")
+    n_int = 5 + n_phase + 2 * len(pairs)
+    n_flt = 0
+    for _, pr in pairs:
+        if pr["type"] == "JACOBSON":
+            n_int += 6 + 3 * n_phase
+            n_flt += 3 + len(pr["Y_j"])
+        elif pr["type"] == "EQSAM":
+            n_ion = len(pr["ions"])
+            n_int += 2 + n_phase + (1 + n_phase) * n_ion
+            n_flt += 3 + n_ion
+        else:
+            raise ValueError(f"Invalid activity type specified for {what}: '{pr['type']}'")
+    ints = np.zeros(n_int, np.int32)
+    flts = np.zeros(n_flt, np.float64)
+    gw = obj["gas-phase water"]
+    if gw not in gas_index:
+        raise KeyError(f"Cannot find gas-phase water species '{gw}' for {what}")
+    ints[0:5] = (n_phase, gas_index[gw], len(pairs), n_int, n_flt)
+    ints[5:5 + n_phase] = water_ids
+    ii, ff = 5 + n_phase + 2 * len(pairs), 0
+    for x, (pname, pr) in enumerate(pairs):
+        ints[5 + n_phase + x] = ii + 1
+        ints[5 + n_phase + len(pairs) + x] = ff + 1
+        if pr["type"] == "JACOBSON":
+            ints[ii] = 1
+            ys = [float(v) for v in pr["Y_j"]]
+            ints[ii + 5] = len(ys)
+            flts[ff + 3:ff + 3 + len(ys)] = ys
+            if "low RH" not in pr:
+                raise KeyError(f"Missing 'low RH' value for ion pair '{pname}' in {what}")
+            flts[ff] = float(pr["low RH"])
+            for ion, qty, mw, charge in _ion_pair_ions(pr["ions"], db, what):
+                rel = _relative_id(reps, phases, phase, ion, water_ids, "ion")
+                if charge > 0:
+                    ints[ii + 1], flts[ff + 1], ints[ii + 3] = qty, mw, rel
+                else:
+                    ints[ii + 2], flts[ff + 2], ints[ii + 4] = qty, mw, rel
+            ii += 6 + 3 * n_phase
+            ff += 3 + len(ys)
+        else:
+            ions = list(pr["ions"].keys())
+            flts[ff], flts[ff + 1], flts[ff + 2] = float(pr["NW"]), float(pr["ZW"]), float(pr["MW"])
+            ints[ii] = 2
+            ints[ii + 1] = len(ions)
+            for y, ion in enumerate(ions):
+                if ion not in db.props or "molecular weight [kg mol-1]" not in db.props[ion]:
+                    raise KeyError(f"Missing molecular weight for ion '{ion}' in {what}")
+                flts[ff + 3 + y] = float(db.props[ion]["molecular weight [kg mol-1]"])
+                ints[ii + 2 + n_phase + y] = _relative_id(reps, phases, phase, ion, water_ids,
+                                                          "ion")
+            ii += 2 + n_phase + (1 + n_phase) * len(ions)
+            ff += 3 + len(ions)
+    return SubModel(SUB_MODEL_ZSR_AEROSOL_WATER, ints, flts, 1, str(obj.get("name", "")))
+
+
+def pack_pdfite(obj: dict, db: _SpeciesDB, gas_index: dict[str, int], reps: list[AeroRep],
+                phases: list[AeroPhase]) -> SubModel:
+    """SUB_MODEL_PDFITE (src/sub_models/sub_model_PDFiTE.F90:250-700).
+
+    The ion pairs are those of "calculate for" in their order, then every
+    further ion pair that only appears as an interaction partner, in order
+    of first appearance (these get no interactions).  ints (initialised to
+    9999): ``[NUM_PHASE_, GAS_WATER_ID_, NUM_ION_PAIRS_, TOTAL_INT_PARAM_,
+    TOTAL_FLOAT_PARAM_, PHASE_ID_(p), PAIR_INT_PARAM_LOC_(x),
+    PAIR_FLOAT_PARAM_LOC_(x)]``, per ion pair ``[ION_PAIR_ACT_ID_,
+    NUM_CATION_, NUM_ANION_, CATION_ID_, ANION_ID_, NUM_INTER_,
+    JAC_WATER_ID_(p), JAC_CATION_ID_(p, y), JAC_ANION_ID_(p, y), NUM_B_(i),
+    INTER_SPEC_ID_(i), INTER_SPEC_LOC_(i)]``; floats (initialised to 9999)
+    per ion pair ``[CATION_MW_, ANION_MW_, CATION_N_, ANION_N_]`` then per
+    interaction ``[MIN_RH_, MAX_RH_, B_(z)]``.  One env parameter."""
+    what = "PD-FiTE activity sub-model"
+    phase = obj["aerosol phase"]
+    water = obj["aerosol-phase water"]
+    water_ids = _instances(reps, phases, phase, water)
+    n_phase = len(water_ids)
+    if n_phase == 0:
+        raise ValueError(f"Aerosol phase '{phase}' not present in any aerosol representation "
+                         f"for {what}")
+    calc = list((obj.get("calculate for") or {}).items())
+    names = [nm for nm, _ in calc]
+    n_inter_total = 0
+    for _, pr in calc:
+        for it in pr["interactions"]:
+            n_inter_total += 1
+            if it["ion pair"] not in names:
+                names.append(it["ion pair"])
+    n = len(names)
+    n_int = 5 + n_phase + 3 * n_inter_total + (8 + (1 + 2 * n) * n_phase) * n
+    n_flt = sum(2 + len(it["B"]) for _, pr in calc for it in pr["interactions"]) + 4 * n
+    ints = np.full(n_int, 9999, np.int32)
+    flts = np.full(n_flt, 9999.0, np.float64)
+    gw = obj["gas-phase water"]
+    if gw not in gas_index:
+        raise KeyError(f"Cannot find gas-phase water species '{gw}' for {what}")
+    ints[0:5] = (n_phase, gas_index[gw], n, n_int, n_flt)
+    ints[5:5 + n_phase] = water_ids
+    ii, ff = 5 + n_phase + 2 * n, 0
+    P = n_phase
+    for x, pname in enumerate(names):
+        ints[5 + P + x] = ii + 1
+        ints[5 + P + n + x] = ff + 1
+        if db.var_type_of(pname) != CHEM_SPEC_ACTIVITY_COEFF:
+            raise ValueError(f"Ion pair '{pname}' must have type ION_PAIR in {what}")
+        ints[ii] = _relative_id(reps, phases, phase, pname, water_ids, "ion pair")
+        ions = db.props[pname].get("ions")
+        if not ions:
+            raise KeyError(f"Missing ions for ion pair '{pname}' in {what}")
+        for ion, qty, mw, charge in _ion_pair_ions(ions, db, what):
+            rel = _relative_id(reps, phases, phase, ion, water_ids, "ion")
+            if charge > 0:
+                ints[ii + 1], flts[ff], ints[ii + 3] = qty, mw, rel
+            else:
+                ints[ii + 2], flts[ff + 1], ints[ii + 4] = qty, mw, rel
+        ff += 4
+        base = ii
+        ii += 6 + (1 + 2 * n) * P
+        if x < len(calc):
+            inters = calc[x][1]["interactions"]
+            ni = len(inters)
+            ints[base + 5] = ni
+            o_b = base + 6 + (1 + 2 * n) * P
+            for y, it in enumerate(inters):
+                ints[o_b + 2 * ni + y] = ff + 1          # INTER_SPEC_LOC_
+                ints[o_b + ni + y] = names.index(it["ion pair"]) + 1  # INTER_SPEC_ID_
+                lo, hi = float(it["min RH"]), float(it["max RH"])
+                if not (0.0 <= lo < 1.0) or not (0.0 < hi <= 1.0):
+                    raise ValueError(f"Invalid RH range for ion pair '{pname}' in {what}")
+                bs = [float(v) for v in it["B"]]
+                ints[o_b + y] = len(bs)                    # NUM_B_
+                flts[ff], flts[ff + 1] = lo, hi
+                flts[ff + 2:ff + 2 + len(bs)] = bs
+                ff += 2 + len(bs)
+                ii += 3
+        else:
+            ints[base + 5] = 0
+    return SubModel(SUB_MODEL_PDFITE, ints, flts, 1, str(obj.get("name", "")))
+
+
 def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mechanism:
     """Loads CAMP JSON input with aerosol phases and modal/binned mass
     representations (plus any gas-phase content), packed for the C solver.
@@ -490,6 +713,7 @@ def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mec
     mechs: list[tuple[str, list[dict]]] = []
     phase_json: list[dict] = []
     rep_json: list[dict] = []
+    sub_json: list[dict] = []
     rel_tol = None
     for path in files:
         for obj in _read_json(path).get("camp-data", []):
@@ -515,7 +739,15 @@ def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mec
                     raise NotImplementedError(f"aerosol representation {t} is not supported")
                 rep_json.append(obj)
             elif t is not None and t.startswith("SUB_MODEL_"):
-                raise NotImplementedError(f"sub-model {t} is not supported")
+                if t not in SUB_MODEL_PRIORITY:
+                    raise NotImplementedError(f"sub-model {t} is not supported")
+                if any(o.get("name") == obj.get("name") for o in sub_json):
+                    raise NotImplementedError(f"sub-model '{obj.get('name')}' is defined twice")
+                # camp_core places a new sub-model before the first one of
+                # larger priority value (src/camp_core.F90:575-605)
+                at = next((i for i, o in enumerate(sub_json)
+                           if SUB_MODEL_PRIORITY[t] < SUB_MODEL_PRIORITY[o["type"]]), len(sub_json))
+                sub_json.insert(at, obj)
             elif t == "RELATIVE_TOLERANCE":
                 rel_tol = float(obj["value"])
     gas = db.gas_species()
@@ -549,6 +781,10 @@ def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mec
             else:
                 rxns.append(pack_reaction(r, gas_id))
     rate_ids = assign_rate_ids(rxns)
+    subs = []
+    for obj in sub_json:
+        pack = pack_zsr_aerosol_water if obj["type"] == "SUB_MODEL_ZSR_AEROSOL_WATER" else pack_pdfite
+        subs.append(pack(obj, db, gas_index, reps, phases))
     species = list(gas)
     var_type = [db.var_type_of(n) for n in gas]
     abs_tol = [db.abs_tol_of(n) for n in gas]
@@ -563,7 +799,7 @@ def load_aerosol_mechanism(files: Iterable[str], name: str | None = None) -> Mec
         name=name or (mechs[0][0] if mechs else "mechanism"), species=species,
         var_type=np.asarray(var_type, np.int32), abs_tol=np.asarray(abs_tol, np.float64),
         rel_tol=rel_tol if rel_tol is not None else 1.0e-8, rxns=rxns, rate_ids=rate_ids,
-        species_props=props, aero_phases=phases, aero_reps=reps)
+        species_props=props, aero_phases=phases, aero_reps=reps, sub_models=subs)
 
 
 def modal_sections(mech: Mechanism) -> list[tuple[int, int]]:

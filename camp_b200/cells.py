@@ -214,6 +214,26 @@ def make_cells(
     return CellBatch(state=state, env=env, photo_rates=photo, seed=seed)
 
 
+def make_cells_near_init(mech: Mechanism, n_cells: int, seed: int,
+                         spread: float = 3.0) -> CellBatch:
+    """Cells around the mechanism's own initial state: every variable
+    species at its "init conc" (the cb05cl_ae5 test's initial state,
+    ``test/chemistry/cb05cl_ae5/cb05cl_ae5_init.json``; 0 where none is
+    given) times a per-cell, per-species factor log-uniform in
+    [1/spread, spread]; T, P and the host-set rates as in ``make_cells``.
+    Unlike the log-uniform workload, whose radicals start up to 1e2 ppm, such
+    cells have a solution that the tolerances determine: two runs that
+    differ by roundoff agree to far inside 1e-3 on every species."""
+    cells = make_cells(mech, n_cells, seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 0x5EED))
+    var = mech.var_type == CHEM_SPEC_VARIABLE
+    init = np.asarray([float(mech.species_props.get(s, {}).get("init conc", 0.0))
+                       for s in mech.species])
+    fac = np.exp(rng.uniform(-np.log(spread), np.log(spread), (n_cells, mech.n_state_var)))
+    cells.state[:, var] = (init[None, :] * fac)[:, var]
+    return cells
+
+
 def constant_values(mech: Mechanism) -> dict[str, float]:
     """'init conc' of each non-variable species (packed fixtures keep these)."""
     out = {}

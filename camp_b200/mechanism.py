@@ -89,6 +89,32 @@ class PackedRxn:
     label: str = ""
 
 
+SUB_MODEL_UNIFAC = 1             # src/sub_model_solver.c:16-18
+SUB_MODEL_ZSR_AEROSOL_WATER = 2
+SUB_MODEL_PDFITE = 3
+
+
+@dataclass
+class SubModel:
+    """One sub-model as sub_model_add_condensed_data receives it."""
+
+    sub_type: int
+    ints: np.ndarray
+    floats: np.ndarray
+    n_env: int
+    name: str = ""
+
+    def to_dict(self) -> dict:
+        return {"type": int(self.sub_type), "ints": [int(v) for v in self.ints],
+                "floats": [float(v) for v in self.floats], "n_env": int(self.n_env),
+                "name": self.name}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "SubModel":
+        return cls(int(d["type"]), np.asarray(d["ints"], np.int32),
+                   np.asarray(d["floats"], np.float64), int(d["n_env"]), d.get("name", ""))
+
+
 @dataclass
 class Mechanism:
     """State layout plus packed reactions for one solver instance."""
@@ -106,6 +132,9 @@ class Mechanism:
     # aero_rep_add_condensed_data receive them (camp_b200.aerosol)
     aero_phases: list = field(default_factory=list)
     aero_reps: list = field(default_factory=list)
+    # sub-models in the order sub_model_add_condensed_data receives them
+    # (camp_core sorts them by priority: ZSR water before PD-FiTE activity)
+    sub_models: list = field(default_factory=list)
 
     @property
     def n_state_var(self) -> int:
@@ -139,6 +168,12 @@ class Mechanism:
                 len(rp), int(sum(r.ints.size for r in rp)), int(sum(r.floats.size for r in rp)),
                 int(sum(r.n_env for r in rp))]
 
+    def sub_sizes(self) -> list[int]:
+        """solver_new's sub-model counts: number, ints, floats, env parameters."""
+        sm = self.sub_models
+        return [len(sm), int(sum(m.ints.size for m in sm)), int(sum(m.floats.size for m in sm)),
+                int(sum(m.n_env for m in sm))]
+
     def index(self, name: str) -> int:
         return self.species.index(name)
 
@@ -170,6 +205,7 @@ class Mechanism:
             },
             "aero_phases": [p.to_dict() for p in self.aero_phases],
             "aero_reps": [r.to_dict() for r in self.aero_reps],
+            "sub_models": [m.to_dict() for m in self.sub_models],
         }
 
     @classmethod
@@ -198,6 +234,7 @@ class Mechanism:
             species_props={n: {"init conc": v} for n, v in d.get("init_conc", {}).items()},
             aero_phases=[AeroPhase.from_dict(p) for p in d.get("aero_phases", [])],
             aero_reps=[AeroRep.from_dict(r) for r in d.get("aero_reps", [])],
+            sub_models=[SubModel.from_dict(m) for m in d.get("sub_models", [])],
         )
 
     def save(self, path: str) -> None:

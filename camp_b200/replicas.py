@@ -2,8 +2,9 @@
 
 Cells are independent, so N GPUs run N replicas of the solve on disjoint
 seeded cell sets with no collective on the data path (weak scaling).  The
-only cross-rank steps are the barrier around the timed region and the
-max-over-ranks of its device time.  One process per GPU; NCCL on GPUs, gloo
+only cross-rank steps are the barrier around the timed region, the
+max-over-ranks of its device time and the sum over ranks of the cells that
+finished.  One process per GPU; NCCL on GPUs, gloo
 for the CPU tests of this logic.
 """
 from __future__ import annotations
@@ -46,6 +47,19 @@ def max_over_ranks(x: float, world: int) -> float:
     dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
     t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    """Sum of a per-rank count (successful cell-steps) over the job."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 

@@ -160,6 +160,8 @@ def ref_lib():
         for kind in ("photolysis", "emission", "first_order_loss", "wet_deposition"):
             getattr(lib, f"rxn_{kind}_create_rate_update_data").restype = vp
             getattr(lib, f"rxn_{kind}_set_rate_update_data").argtypes = [vp, C.c_int, C.c_double]
+        lib.sub_model_add_condensed_data.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p,
+                                                     _f64p, vp]
         lib.aero_phase_add_condensed_data.argtypes = [C.c_int, C.c_int, _i32p, _f64p, vp]
         lib.aero_rep_add_condensed_data.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p,
                                                     _f64p, vp]
@@ -324,7 +326,7 @@ class RefModel:
         self.h = self.lib.ref_new(
             mech.n_state_var, n_cells, np.ascontiguousarray(mech.var_type, np.int32),
             mech.n_rxn, mech.n_rxn_int_param, mech.n_rxn_float_param, mech.n_rxn_env_param,
-            *mech.aero_sizes(), 0, 0, 0, 0,
+            *mech.aero_sizes(), *mech.sub_sizes(),
         )
         for r in mech.rxns:
             self.lib.rxn_add_condensed_data(
@@ -341,6 +343,12 @@ class RefModel:
                                                  np.ascontiguousarray(a.ints, np.int32),
                                                  np.ascontiguousarray(a.floats, np.float64),
                                                  self.h)
+        for sm in mech.sub_models:
+            self.lib.sub_model_add_condensed_data(sm.sub_type, sm.ints.size, sm.floats.size,
+                                                  sm.n_env,
+                                                  np.ascontiguousarray(sm.ints, np.int32),
+                                                  np.ascontiguousarray(sm.floats, np.float64),
+                                                  self.h)
         self.lib.ref_set_abs_tol(self.h, np.ascontiguousarray(mech.abs_tol, np.float64))
         rc = self.lib.ref_build(self.h)
         if rc != 0:
@@ -446,11 +454,14 @@ def _ref_cb_setup(lib):
 
 
 def ref_solve(mech, state, env, photo_rates, t0, t1, rtol, abs_tol, max_steps=10000,
-              max_conv_fails=1000, n_threads=None):
+              max_conv_fails=1000, n_threads=None, chunk=None):
     """Per-cell solve with the reference's own f/J (compiled reference C code)
     driven by the restated BDF and sparse LU.  Cells are split over threads,
-    each with its own reference model object.  state is updated in place
-    (dependent variables of successful cells, as solver_run does).
+    each with its own reference model object: contiguous ranges, or, with
+    ``chunk``, chunks of that many cells that the threads take in turn (so
+    that a few slow cells do not leave the other threads idle).  state is
+    updated in place (dependent variables of successful cells, as
+    solver_run does).
 
     Returns (status, stats) arrays."""
     import os
@@ -495,8 +506,24 @@ def ref_solve(mech, state, env, photo_rates, t0, t1, rtol, abs_tol, max_steps=10
             if st_out[c] == 0:
                 state[c0 + c, dep] = np.maximum(y[c], 0.0)
 
-    bounds = [int(n_cells * t / n_threads) for t in range(n_threads + 1)]
-    th = [threading.Thread(target=work, args=(bounds[t], bounds[t + 1])) for t in range(n_threads)]
+    if chunk:
+        lock = threading.Lock()
+        nxt = [0]
+
+        def pull():
+            while True:
+                with lock:
+                    a = nxt[0]
+                    nxt[0] = min(n_cells, a + chunk)
+                if a >= n_cells:
+                    return
+                work(a, min(n_cells, a + chunk))
+
+        th = [threading.Thread(target=pull) for _ in range(n_threads)]
+    else:
+        bounds = [int(n_cells * t / n_threads) for t in range(n_threads + 1)]
+        th = [threading.Thread(target=work, args=(bounds[t], bounds[t + 1]))
+              for t in range(n_threads)]
     for t in th:
         t.start()
     for t in th:

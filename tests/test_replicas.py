@@ -26,7 +26,8 @@ def _worker(rank, world, port, out):
     replicas.barrier(w)
     local_seconds = 1.0 + r  # rank 1 is the slow one
     t = replicas.max_over_ranks(local_seconds, w)
-    out.put((r, w, t, replicas.aggregate_throughput(8, 10, w, t), float(cells.state.sum())))
+    ok = replicas.sum_over_ranks(5 + r, w)  # cells that finished on each rank
+    out.put((r, w, t, replicas.aggregate_throughput(8, 10, w, t), float(cells.state.sum()), ok))
     replicas.finalize(w)
 
 
@@ -44,11 +45,12 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=30)
         assert p.exitcode == 0
-    (r0, w0, t0, v0, s0), (r1, w1, t1, v1, s1) = res
+    (r0, w0, t0, v0, s0, k0), (r1, w1, t1, v1, s1, k1) = res
     assert (r0, r1) == (0, 1) and w0 == w1 == 2
     assert t0 == t1 == 2.0  # max over ranks
     assert v0 == v1 == 2 * 8 * 10 / 2.0
     assert s0 != s1  # disjoint seeded cells per rank
+    assert k0 == k1 == 11.0  # sum over ranks
 
 
 def test_single_rank_needs_no_group(monkeypatch):
@@ -59,3 +61,4 @@ def test_single_rank_needs_no_group(monkeypatch):
     assert replicas.init("gloo") == (1, 0, 0)
     assert replicas.max_over_ranks(3.5, 1) == 3.5
     assert replicas.aggregate_throughput(100, 10, 1, 2.0) == 500.0
+    assert replicas.sum_over_ranks(7, 1) == 7.0
