@@ -206,9 +206,15 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
 }
 
 // Copies the table blob into the front of the block's shared memory with one
-// bulk (TMA) copy completed on an mbarrier.  The wait is bounded; on timeout
-// the block records an error, waits once more (bounded) for its copy and
-// returns false.
+// bulk (TMA) copy completed on an mbarrier.  The wait is bounded: a copy of
+// at most 64 KB from this GPU's memory completes in microseconds, and the
+// first limit (2^24 polls, each suspending in try_wait) is seconds.  On
+// timeout the block records the error flag that the host reads after the
+// launch, then waits again for its own copy, with a four times longer limit,
+// so that the block does not leave while the copy may still write its shared
+// memory; only if that wait also runs out (the memory system no longer
+// answers, and the host already sees the error) does it return false with
+// the copy outstanding.
 __device__ bool stage_tables(char* dst, const void* src, int bytes, unsigned long long* bar,
                              int* err_flag) {
   const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
@@ -240,7 +246,7 @@ __device__ bool stage_tables(char* dst, const void* src, int bytes, unsigned lon
   bool ok = wait(1L << 24);
   if (!ok) {
     atomicExch(err_flag, 1);
-    wait(1L << 24);
+    wait(1L << 26);
   }
   return __syncthreads_and(ok ? 1 : 0) != 0;
 }
@@ -2512,7 +2518,11 @@ bool Engine::check_jac(const double* h_state, const double* h_env, const double*
 // contents; the counter and flag are cleared by every call, the Jacobian
 // slots are always written before they are read.  Two such calls that
 // overlap on the GPU (different streams, or different solvers on one device)
-// race on the array.
+// race on the array.  This path records no timing events and no per-cell
+// statistics in the solver (the caller's d_stats receives them), so
+// last_kernel_ms and get_cell_stats keep describing the solver's last
+// regular run.  The Nordsieck history stays in shared memory whatever the
+// solver's layout setting.
 // ---------------------------------------------------------------------------
 constexpr size_t kStaticScratchBytes = size_t(8) << 20;  // 8 MiB
 constexpr size_t kStaticHeadBytes = 256;                 // counter, error flag
@@ -2520,7 +2530,13 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 
 // Device address of the static scratch on the current device.  The host-side
 // name g_static_scratch is only a stand-in, so the address is looked up once
-// per device (with that device current) and kept.
+// per device (with that device current) and kept for the life of the
+// process; a caller that resets a device's primary context (cudaDeviceReset)
+// must not use this path on that device afterwards.  The kernels' dynamic
+// shared-memory limit is raised once per device and precision, to the most
+// any launch of this path needs (the table blob plus the largest slab set).
+static int g_static_smem_set[64][2] = {};
+
 static bool static_scratch_address(char** out, std::string* err) {
   static std::mutex mu;
   static void* addr[64] = {};
@@ -2607,24 +2623,30 @@ bool Engine::run_solve_static(double* d_state, const double* d_env, const double
   a.maxnef = s.max_conv_fails;
   a.lu_mode = s.lu_mode;
   const size_t smem = (size_t)tab + (size_t)warps * lay.bytes;
-  CK(cudaEventRecord(I->ev0, st));
-  if (s.precision == 1) {
-    CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem));
-    solve_kernel<float><<<grid, warps * 32, smem, st>>>(a);
-  } else {
-    CK(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem));
-    solve_kernel<double><<<grid, warps * 32, smem, st>>>(a);
+  {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    int& set = g_static_smem_set[dev][s.precision == 1 ? 1 : 0];
+    if ((int)smem > set) {
+      const int lim = I->max_smem;  // the device's opt-in maximum per block
+      if (s.precision == 1)
+        CK(cudaFuncSetAttribute(solve_kernel<float>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+      else
+        CK(cudaFuncSetAttribute(solve_kernel<double>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+      set = lim;
+    }
   }
+  if (s.precision == 1)
+    solve_kernel<float><<<grid, warps * 32, smem, st>>>(a);
+  else
+    solve_kernel<double><<<grid, warps * 32, smem, st>>>(a);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(I->ev1, st));
   ++launches_;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  float ms = 0.f;
-  if (cudaEventElapsedTime(&ms, I->ev0, I->ev1) == cudaSuccess) last_ms_ = ms;
   if (flag) {
     *err = "solve kernel: the table stage into shared memory did not complete";
     return false;

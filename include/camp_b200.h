@@ -230,17 +230,24 @@ int camp_b200_sync_status(void *solver_data, void *stream);
  * device memory, for callers that cannot call cudaMalloc while they run (a
  * host model whose pool allocator owns the device heap, or code running where
  * allocation is not allowed).  All buffers are the caller's: state
- * [n_cells*n_state_var] (updated in place), env [n_cells*2], host-set base
- * rates [n_cells*n_photo] (may be NULL without host-rate reactions) and the
- * per-cell results d_stats [n_cells], all in device memory.  The solve's
- * scratch lives in one static 8 MiB device array that every GPU loading this
- * library holds until exit; a mechanism needing more than that for one
- * resident cell per SM is rejected with an error, fewer resident cells are
- * used when it needs less.  The first call on a device looks up the array's
- * address; make that first call before any stream capture.  Calls share the
- * array, so two calls that overlap on the GPU race.  Waits for the stream;
- * returns 0 when the solve ran (per-cell status in d_stats) or -1 with
- * camp_b200_last_error() set. */
+ * [n_cells*n_state_var] (updated in place), env [n_cells*2], the per-cell
+ * rate matrix d_photo [n_cells*camp_b200_n_photo()] laid out as for
+ * camp_b200_set_photo_rates (host-set reaction rates, then the GMD and GSD
+ * columns of every aerosol mode, see camp_b200_rate_column; NULL only when
+ * camp_b200_n_photo() is 0) and the per-cell results d_stats [n_cells], all
+ * in device memory.  The solve's scratch lives in one static 8 MiB device
+ * array that every GPU loading this library holds until exit; a mechanism
+ * needing more than that for one resident cell per SM is rejected with an
+ * error, fewer resident cells are used when it needs less.  The first call
+ * on a device looks up the array's address and keeps it for the life of the
+ * process (do not use this call on a device after cudaDeviceReset); make
+ * that first call before any stream capture.  Calls share the array, so two
+ * calls that overlap on the GPU race.  This call records no timing and no
+ * statistics in the solver: camp_b200_last_kernel_ms and
+ * camp_b200_get_cell_stats keep describing its last regular run.  The
+ * Nordsieck history stays in shared memory whatever camp_b200_set_layout
+ * chose.  Waits for the stream; returns 0 when the solve ran (per-cell
+ * status in d_stats) or -1 with camp_b200_last_error() set. */
 int camp_b200_run_device_noalloc(void *solver_data, double *d_state,
                                  const double *d_env, const double *d_photo,
                                  camp_b200_cell_stats *d_stats, int n_cells,

@@ -50,7 +50,11 @@ class OracleStats(C.Structure):
 def build(with_ref: bool = True) -> None:
     """Builds the oracle libraries (the reference part only if its tree exists)."""
     target = "all" if with_ref else "oracle"
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    cmd = ["make", "-s", "-C", HERE, target]
+    ref = os.environ.get("CAMP_REFERENCE_ROOT")
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True)
 
 
 _oracle_lib = None

@@ -6,7 +6,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF_ROOT = "/root/reference"
+# the reference source tree (read only by the CPU tests that re-pack its
+# JSON input or compile its C sources; they skip when it is absent)
+REF_ROOT = os.environ.get("CAMP_REFERENCE_ROOT", "/root/reference")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

@@ -7,7 +7,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT, gpu_available
+from conftest import GOLDEN, REF_ROOT, ROOT, gpu_available
 
 
 def header_functions():
@@ -99,7 +99,7 @@ def test_rejects_unsupported(cb05, lib):
 
 def test_packer_matches_fixture(cb05):
     """Re-packing the reference JSON reproduces the committed packed data."""
-    ref = "/root/reference"
+    ref = REF_ROOT
     if not os.path.isdir(ref):
         pytest.skip("reference tree absent")
     import sys
@@ -120,7 +120,7 @@ def test_packer_matches_fixture(cb05):
 
 
 def test_mod37_packer_matches_fixture(mod37):
-    ref = "/root/reference"
+    ref = REF_ROOT
     if not os.path.isdir(ref):
         pytest.skip("reference tree absent")
     import sys

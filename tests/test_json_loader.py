@@ -9,8 +9,9 @@ import numpy as np
 import pytest
 
 from camp_b200 import _lib
+from conftest import REF_ROOT
 
-REF_CB05 = "/root/reference/mechanisms/cb05cl_ae5"
+REF_CB05 = os.path.join(REF_ROOT, "mechanisms", "cb05cl_ae5")
 
 
 def _cpp_solver(files, n_cells=2):
@@ -129,8 +130,8 @@ def test_every_gas_type_and_option(tmp_path):
     _compare(paths)
 
 
-REF_MOD37 = "/root/reference/mechanisms/monarch_mod37"
-REF_UNIT = "/root/reference/test/unit_rxn_data"
+REF_MOD37 = os.path.join(REF_ROOT, "mechanisms", "monarch_mod37")
+REF_UNIT = os.path.join(REF_ROOT, "test", "unit_rxn_data")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_MOD37), reason="reference tree not present")

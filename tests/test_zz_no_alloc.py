@@ -5,8 +5,10 @@ memory while they run (a host model whose pool allocator owns the device
 heap, or code running where cudaMalloc is not allowed): all buffers are the
 caller's and the solve's scratch lives in a static device array inside the
 library.  This test runs it twice in a row on the same inputs and checks each
-result against camp_b200_run_device.  The file is named so that pytest
-collects it last.
+result against camp_b200_run_device, on cb05cl_ae5 and on MONARCH mod37 with
+its SOA, cloud and aqueous aerosol chemistry (whose per-cell rate matrix
+carries every aerosol mode's GMD and GSD after the host-set reaction rates).
+The file is named so that pytest collects it last.
 """
 import ctypes as C
 
@@ -22,17 +24,24 @@ RTOL = 1e-12  # both entry points run the same kernel: results agree to round-of
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_noalloc_matches_run_device(cb05, precision):
+@pytest.mark.parametrize("which", ["cb05", "mod37_aero"])
+def test_noalloc_matches_run_device(request, which, precision):
     import torch
 
     from camp_b200 import _lib
     from camp_b200.cells import make_cells
     from camp_b200.solver import Solver
 
-    n = 300
-    cells = make_cells(cb05, n, 21)
-    s = Solver(cb05, n)
-    s.initialize(abs_tol=np.full(cb05.n_state_var, 1e-8), rel_tol=1e-4, max_steps=2000)
+    mech = request.getfixturevalue(which)
+    n = 300 if which == "cb05" else 120
+    cells = make_cells(mech, n, 21)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4, max_steps=2000)
+    # the rate matrix the caller passes: host-set reaction rates, then the
+    # GMD / GSD columns of the aerosol modes
+    assert cells.photo_rates.shape[1] == s.n_photo
+    n_mode_cols = sum(1 for c in mech.rate_columns() if c[0] != "rxn")
+    assert (n_mode_cols > 0) == (which == "mod37_aero")
     s.set_precision(precision)
     s.set_photo_rates(cells.photo_rates)
     dev = torch.device("cuda", 0)
