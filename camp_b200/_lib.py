@@ -56,6 +56,7 @@ EXPORTED = [
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
     "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
+    "camp_b200_n_mapped_values", "camp_b200_get_jac_map",
     "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_solver_from_json",
     "camp_b200_n_state_var", "camp_b200_state_name", "camp_b200_json_tolerances",
     "camp_b200_get_var_type", "camp_b200_rxn_float_data_size", "camp_b200_get_rxn_float_data",
@@ -92,6 +93,7 @@ def load(path: str = LIB_PATH):
     lib.rxn_update_data.argtypes = [ip, C.POINTER(C.c_int), ip, vp, vp]
     lib.aero_phase_add_condensed_data.argtypes = [ip, ip, _i32p, _f64p, vp]
     lib.aero_rep_add_condensed_data.argtypes = [ip, ip, ip, ip, _i32p, _f64p, vp]
+    lib.sub_model_add_condensed_data.argtypes = [ip, ip, ip, ip, _i32p, _f64p, vp]
     lib.aero_rep_update_data.argtypes = [ip, C.POINTER(C.c_int), ip, vp, vp]
     for kind in ("photolysis", "emission", "first_order_loss", "wet_deposition"):
         getattr(lib, f"rxn_{kind}_create_rate_update_data").restype = vp
@@ -141,12 +143,14 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_last_kernel_ms.restype = dp
     lib.camp_b200_last_kernel_ms.argtypes = [vp]
     for name in ("camp_b200_n_dep_var", "camp_b200_n_jac_elem", "camp_b200_n_lu_elem",
-                 "camp_b200_rxn_int_data_size"):
+                 "camp_b200_rxn_int_data_size", "camp_b200_n_mapped_values"):
         getattr(lib, name).restype = ip
         getattr(lib, name).argtypes = [vp]
     lib.camp_b200_get_solver_jac.argtypes = [vp, _i32p, _i32p]
     lib.camp_b200_get_rxn_int_data.argtypes = [vp, _i32p]
     lib.camp_b200_get_lu_order.argtypes = [vp, _i32p]
+    lib.camp_b200_get_jac_map.restype = ip
+    lib.camp_b200_get_jac_map.argtypes = [vp, _i32p]
     lib.camp_b200_eval_deriv.restype = ip
     lib.camp_b200_eval_deriv.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p, _f64p, _f64p]
     lib.camp_b200_eval_jac.restype = ip

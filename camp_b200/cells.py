@@ -13,7 +13,7 @@ Per-cell inputs follow the documented workload distributions:
   reactions keep their streams;
 * aerosol (mechanisms with a modal/binned representation, drawn last): per
   mode a geometric mean diameter log-uniform in 20-500 nm (the GSD is the
-  representation's) and a number concentration log-uniform in 1e7-1e10 m^-3,
+  representation's, 2.0 where it sets none) and a number concentration log-uniform in 1e7-1e10 m^-3,
   per bin a number concentration log-uniform in 1e3-1e6 m^-3 (bins reach
   15 um); the mode's or bin's volume is split over its mass species with
   uniform random weights into kg m^-3; activity coefficients are 1;
@@ -36,6 +36,10 @@ from .mechanism import (CHEM_SPEC_VARIABLE, RXN_EMISSION, RXN_FIRST_ORDER_LOSS, 
 EMISSION_BASE = 1.0e-8
 FIRST_ORDER_LOSS_BASE = 2.0e-5
 WET_DEPOSITION_BASE = 1.0e-4
+# GSD of a mode whose representation input sets none (the MONARCH test
+# configuration leaves GMD / GSD to the host's update data; the shipped mod37
+# modes use 2.0-2.24)
+DEFAULT_GSD = 2.0
 
 
 @dataclass
@@ -97,6 +101,20 @@ def hl_water_indices(mech: Mechanism) -> set[int]:
     return out
 
 
+def zsr_water_indices(mech: Mechanism) -> set[int]:
+    """State indices of the aerosol-phase water that a ZSR sub-model
+    computes (PHASE_ID_ of every instance,
+    src/sub_models/sub_model_ZSR_aerosol_water.c:37-40)."""
+    from .mechanism import SUB_MODEL_ZSR_AEROSOL_WATER
+
+    out = set()
+    for sm in mech.sub_models:
+        if sm.sub_type == SUB_MODEL_ZSR_AEROSOL_WATER:
+            n_phase = int(sm.ints[0])
+            out.update(int(sm.ints[5 + p]) - 1 for p in range(n_phase))
+    return out
+
+
 def _aerosol_cells(mech: Mechanism, rng, state: np.ndarray, photo: np.ndarray) -> None:
     """Per-cell aerosol state and mode GMD/GSD columns (module docstring)."""
     from .aerosol import MODAL
@@ -104,7 +122,9 @@ def _aerosol_cells(mech: Mechanism, rng, state: np.ndarray, photo: np.ndarray) -
     n_cells = state.shape[0]
     cols = mech.rate_columns()
     col_of = {c: j for j, c in enumerate(cols)}
-    water = hl_water_indices(mech)
+    # cloud-like input only where HL partitions into a water that no
+    # sub-model computes
+    water = hl_water_indices(mech) - zsr_water_indices(mech)
     for ri, rep in enumerate(mech.aero_reps):
         inst = 0
         for si, sec in enumerate(rep.sections):
@@ -144,7 +164,7 @@ def _aerosol_cells(mech: Mechanism, rng, state: np.ndarray, photo: np.ndarray) -
                 continue
             if sec.kind == MODAL:
                 gmd = np.exp(rng.uniform(np.log(20e-9), np.log(500e-9), n_cells))
-                gsd = np.full(n_cells, sec.gsd)
+                gsd = np.full(n_cells, sec.gsd if sec.gsd > 0.0 else DEFAULT_GSD)
                 photo[:, col_of[("gmd", ri, si)]] = gmd
                 photo[:, col_of[("gsd", ri, si)]] = gsd
                 number = np.exp(rng.uniform(np.log(1e7), np.log(1e10), (n_cells, 1)))

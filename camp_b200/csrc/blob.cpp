@@ -208,9 +208,10 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
       return (int)(std::lower_bound(t.dep_state.begin(), t.dep_state.end(), st) -
                    t.dep_state.begin());
     };
+    // rec[5]: HL's computed water + 1 (0: a constant water, folded per cell)
     const uint16_t rec[8] = {(uint16_t)dep_of(si.gas), (uint16_t)dep_of(si.aero),
                              (uint16_t)nd,                (uint16_t)first,
-                             (uint16_t)t.si_part0[k],     0, 0, 0};
+                             (uint16_t)t.si_part0[k],     (uint16_t)(si.water_cv + 1), 0, 0};
     si_rec.insert(si_rec.end(), rec, rec + 8);
   }
   for (int e = 0; e < t.n_jac; ++e) {
@@ -295,8 +296,8 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   Writer w;
   // the offsets themselves lead the blob, so device code can rebuild its
   // table pointers from shared memory alone
-  w.buf.resize(256, 0);
-  static_assert(sizeof(BlobOff) <= 256, "BlobOff must fit the blob header");
+  w.buf.resize(kBlobHeader, 0);
+  static_assert(sizeof(BlobOff) <= kBlobHeader, "BlobOff must fit the blob header");
   BlobOff o{};
   o.n = n;
   o.n_rxn = t.n_rxn;
@@ -333,8 +334,8 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.si_elem = w.put(si_elem);
   o.si_ef = w.put(si_ef);
   // aqueous equilibrium instance records
-  std::vector<uint16_t> aq_rec, aq_sp;
-  std::vector<double> aq_sm;
+  std::vector<uint16_t> aq_rec, aq_sp, aq_cp;
+  std::vector<double> aq_sm, aq_cpm;
   for (int k = 0; k < t.n_aq; ++k) {
     const AqInst& q = t.aq[k];
     const int first = (int)aq_sp.size();
@@ -355,15 +356,61 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
         R += pass == 0;
       }
     }
-    const uint16_t rec[8] = {(uint16_t)S, (uint16_t)R, (uint16_t)first,
-                             (uint16_t)t.aq_rate0[k], (uint16_t)t.aq_part0[k],
-                             (uint16_t)t.aq_keff0[k], 0, 0};
-    aq_rec.insert(aq_rec.end(), rec, rec + 8);
+    // rec[6]: computed water + 1 (0: constant, folded per cell) | reactant
+    // count << 8 | product count << 12 (constant species included: the
+    // powers of the water); rec[7]: computed activity coefficient + 1
+    const uint16_t wrec = (uint16_t)((q.water_cv + 1) | (q.react.size() << 8) |
+                                     (q.prod.size() << 12));
+    const int cp0 = (int)aq_cp.size();
+    for (size_t j = 0; j < q.cp_cv.size(); ++j) {
+      aq_cp.push_back((uint16_t)(q.cp_cv[j] | (q.cp_r[j] ? 0x8000 : 0)));
+      aq_cpm.push_back(q.cp_m[j]);
+    }
+    const uint16_t rec[12] = {(uint16_t)S, (uint16_t)R, (uint16_t)first,
+                              (uint16_t)t.aq_rate0[k], (uint16_t)t.aq_part0[k],
+                              (uint16_t)t.aq_keff0[k], wrec, (uint16_t)(q.act_cv + 1),
+                              (uint16_t)cp0, (uint16_t)q.cp_cv.size(), 0, 0};
+    aq_rec.insert(aq_rec.end(), rec, rec + 12);
   }
   o.n_aq = t.n_aq;
   o.aq_rec = w.put(aq_rec);
   o.aq_sp = w.put(aq_sp);
   o.aq_sm = w.put(aq_sm);
+  o.aq_cp = w.put(aq_cp);
+  o.aq_cpm = w.put(aq_cpm);
+  // sub-model programs, virtual slots and the chain
+  {
+    std::vector<uint32_t> rec;
+    std::vector<int32_t> ints;
+    std::vector<double> flts;
+    for (const SubProgram& g : t.cv) {
+      rec.push_back((uint32_t)ints.size());
+      rec.push_back((uint32_t)flts.size());
+      ints.insert(ints.end(), g.ints.begin(), g.ints.end());
+      flts.insert(flts.end(), g.flts.begin(), g.flts.end());
+    }
+    o.n_cv = t.n_cv;
+    o.n_pj = t.n_pj;
+    o.sm_keff = t.sm_keff;
+    o.sm_rec = w.put(rec);
+    o.sm_int = w.put(ints);
+    o.sm_flt = w.put(flts);
+    o.n_virt = t.n_virt;
+    o.jv_ptr = w.put(u16(t.jv_ptr));
+    o.jv_part = w.put(u16(t.jv_part));
+    o.n_chain = (int)t.ch_tgt.size();
+    o.ch_tgt = w.put(u16(t.ch_tgt));
+    o.ch_ptr = w.put(u16(t.ch_ptr));
+    std::vector<uint32_t> ent(t.ch_v.size());
+    for (size_t i = 0; i < ent.size(); ++i)
+      ent[i] = (uint32_t)t.ch_v[i] | ((uint32_t)t.ch_p[i] << 16);
+    o.ch_ent = w.put(ent);
+    if (t.n_cv > 254 || t.n_pj > 65535 || t.n_virt > 65535 || t.jv_part.size() > 65535 ||
+        t.ch_v.size() > 65535) {
+      *err = "sub-model tables exceed the 16-bit encodings";
+      return false;
+    }
+  }
   o.n_plev = t.n_plev;
   o.lu_perm = w.put(u16(t.lu_perm));
   o.lu_src = w.put(lu_src);
@@ -409,9 +456,9 @@ namespace campb {
 
 bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
                      std::vector<uint8_t>* blob, LaneOff* off, std::string* err) {
-  if (t.n_simpol > 0 || t.n_aq > 0) {
+  if (t.n_simpol > 0 || t.n_aq > 0 || t.n_cv > 0) {
     *err = "the lane-per-cell kernel does not evaluate SIMPOL, HL or aqueous equilibrium "
-           "reactions";
+           "reactions or sub-models";
     return false;
   }
   const int n = t.n;

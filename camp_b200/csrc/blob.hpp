@@ -1,7 +1,8 @@
 // Compact mechanism tables for the solve kernel.  The host packs them into one
 // 16-byte aligned blob; every block copies the blob into the front of its
 // shared memory with one bulk (TMA) copy, and all warps of the block read it
-// from there.  Offsets are in bytes from the start of the blob.
+// from there.  Offsets are in bytes from the start of the blob, whose first
+// kBlobHeader bytes hold the BlobOff itself.
 #pragma once
 
 #include <cstdint>
@@ -55,14 +56,31 @@ struct BlobOff {
   // its 8 per-cell constants the terms' rate constants.
   int n_simpol, n_keff, n_rates, n_part_all;
   int si_rec, si_elem, si_ef;
-  // aqueous equilibrium instances: record (uint16 x 8: dependent slots,
+  // aqueous equilibrium instances: record (uint16 x 12: dependent slots,
   // dependent reactant slots, first slot, first pseudo-rate, first partial,
-  // keff slot), per slot its dependent index (uint16) and 1e3 / MW (double)
-  int n_aq, aq_rec, aq_sp, aq_sm;
+  // keff slot, computed water | reactant and product counts, computed
+  // activity coefficient, first and count of the computed participants),
+  // per slot its dependent index (uint16) and 1e3 / MW (double); per
+  // computed participant its computed index | reactant << 15 (uint16) and
+  // 1e3 / MW (double)
+  int n_aq, aq_rec, aq_sp, aq_sm, aq_cp, aq_cpm;
   // J gather with unguarded products (SIMPOL): they lead each slot, and
   // jg_umid (uint16 per slot) is the slot's first loss entry
   int has_ug, jg_umid;
+  // sub-models: computed species, parameter-Jacobian elements, keff slot of
+  // PPM_TO_RH_; per computed species its program's first int and first
+  // float (2 x uint32), the program ints (int32) and floats (double).  The
+  // values sit after the pseudo-rates (f) or the partials (J), the
+  // parameter partials and the virtual slots after the values.
+  int n_cv, n_pj, sm_keff, sm_rec, sm_int, sm_flt;
+  // virtual Jacobian slots: partial lists (uint16 pointers, n_virt + 1, and
+  // uint16 partial indices); the chain by target slot: target (uint16),
+  // entry pointers (uint16, n_chain + 1), entries (uint32: virtual slot |
+  // parameter id << 16)
+  int n_virt, jv_ptr, jv_part, n_chain, ch_tgt, ch_ptr, ch_ent;
 };
+
+constexpr int kBlobHeader = 512;
 
 struct Tables;
 

@@ -40,7 +40,7 @@ struct Solver {
   int n_rxn = 0;
   std::unique_ptr<Model> model;
   std::unique_ptr<Engine> engine;
-  // aerosol phases, representations and sub-models (accepted, not solved)
+  // aerosol phases, representations and sub-models
   int n_aero_phase = 0, n_aero_rep = 0, n_sub_model = 0;
   int n_aero_phase_added = 0, n_aero_rep_added = 0, n_sub_model_added = 0;
   bool add_error = false;
@@ -214,8 +214,21 @@ void aero_rep_add_condensed_data(int aero_rep_type, int n_int_param, int n_float
     s->add_error_msg = err;
   }
 }
-void sub_model_add_condensed_data(int, int, int, int, int*, double*, void* solver_data) {
-  S(solver_data)->n_sub_model_added++;
+// sub_model_add_condensed_data (src/sub_model_solver.c:425-470): ZSR
+// aerosol water and PD-FiTE activity; other types are refused at
+// solver_initialize with the reason
+void sub_model_add_condensed_data(int sub_model_type, int n_int_param, int n_float_param,
+                                  int n_env_param, int* int_param, double* float_param,
+                                  void* solver_data) {
+  Solver* s = S(solver_data);
+  s->n_sub_model_added++;
+  std::string err;
+  if (!s->model->add_sub_model(sub_model_type, n_int_param, n_float_param, n_env_param,
+                               int_param, float_param, &err) &&
+      !s->add_error) {
+    s->add_error = true;
+    s->add_error_msg = err;
+  }
 }
 // GMD / GSD updates of the modal/binned representation
 // (src/aero_rep_solver.c:492-545,
@@ -285,13 +298,10 @@ void solver_initialize(void* solver_data, double* abs_tol, double rel_tol, int m
     set_error("solver_initialize: " + s->add_error_msg);
     return;
   }
-  if (s->n_sub_model > 0) {
-    set_error("solver_initialize: sub-models are not supported by this build");
-    return;
-  }
-  if (s->n_aero_phase_added != s->n_aero_phase || s->n_aero_rep_added != s->n_aero_rep) {
-    set_error("solver_initialize: fewer aerosol phases or representations were added than "
-              "declared in solver_new");
+  if (s->n_aero_phase_added != s->n_aero_phase || s->n_aero_rep_added != s->n_aero_rep ||
+      s->n_sub_model_added != s->n_sub_model) {
+    set_error("solver_initialize: fewer aerosol phases, representations or sub-models were "
+              "added than declared in solver_new");
     return;
   }
   std::string err;
@@ -829,6 +839,16 @@ int camp_b200_get_solver_jac(void* solver_data, int* col_ptrs, int* row_ids) {
 int camp_b200_get_rxn_int_data(void* solver_data, int* out) {
   const Model& m = *S(solver_data)->model;
   std::copy(m.rxn_int().begin(), m.rxn_int().end(), out);
+  return 0;
+}
+int camp_b200_n_mapped_values(void* solver_data) {
+  const Model& m = *S(solver_data)->model;
+  return m.built() ? (int)m.jac_map().size() / 3 : -1;
+}
+int camp_b200_get_jac_map(void* solver_data, int* triplets) {
+  const Model& m = *S(solver_data)->model;
+  if (!m.built()) return -1;
+  std::copy(m.jac_map().begin(), m.jac_map().end(), triplets);
   return 0;
 }
 int camp_b200_get_lu_order(void* solver_data, int* perm) {

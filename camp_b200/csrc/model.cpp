@@ -326,6 +326,18 @@ bool Model::resolve_aq(std::string* err) {
         return false;
       }
       q.thr = abs_tol_.empty() ? 0.0 : 1.0e-4 * (abs_tol_[q.water] / 10.0);
+      q.water_cv = cv_of_[q.water];
+      q.act_cv = q.act >= 0 ? cv_of_[q.act] : -1;
+      for (int pass = 0; pass < 2; ++pass) {
+        const std::vector<int>& list = pass == 0 ? q.react : q.prod;
+        for (size_t i = 0; i < list.size(); ++i) {
+          if (cv_of_[list[i]] < 0) continue;
+          q.cp_state.push_back(list[i]);
+          q.cp_cv.push_back(cv_of_[list[i]]);
+          q.cp_m.push_back(q.m2m[(pass == 0 ? 0 : q.react.size()) + i]);
+          q.cp_r.push_back(pass == 0 ? 1 : 0);
+        }
+      }
       aq_.push_back(q);
     }
   }
@@ -404,6 +416,19 @@ bool Model::resolve_instance(SimpolInst* si, int phase, int ri, std::string* err
       *err = what + ": the gas and aerosol species must be variable state variables";
       return false;
     }
+  if (si->type == RXN_HL_PHASE_TRANSFER) {
+    si->water_cv = si->water >= 0 && si->water < n_state_ ? cv_of_[si->water] : -1;
+  } else {
+    // a SIMPOL rate whose mode volume, phase mass or activity follows a
+    // sub-model's output would need those partials chained as well
+    bool computed = si->act >= 0 && si->act < n_state_ && cv_of_[si->act] >= 0;
+    for (int e : si->elem) computed |= cv_of_[e] >= 0;
+    if (computed) {
+      *err = what + ": partitioning into a mode or bin that holds a species computed by a "
+                    "sub-model is not supported";
+      return false;
+    }
+  }
   return true;
 }
 
@@ -480,6 +505,245 @@ bool Model::resolve_simpol(std::string* err) {
     }
   }
   return true;
+}
+
+// ---------------------------------------------------------------------------
+// Sub-models: ZSR aerosol water and PD-FiTE activity
+// ---------------------------------------------------------------------------
+namespace {
+// Packed layouts (ints after the type slot) of
+// src/sub_models/sub_model_ZSR_aerosol_water.c:27-71 and
+// src/sub_models/sub_model_PDFiTE.c:21-64: NUM_PHASE, GAS_WATER_ID
+// (1-based), NUM_ION_PAIR, the two data sizes, the phases' first state ids
+// (1-based), then per ion pair its int and float block locations (1-based).
+// Species ids of an ion pair are relative to the phase's first state id.
+struct SubView {
+  const int* I;
+  const double* F;
+  int np() const { return I[0]; }
+  int gw() const { return I[1] - 1; }
+  int npair() const { return I[2]; }
+  int phase(int p) const { return I[5 + p] - 1; }
+  int il(int x) const { return I[5 + np() + x] - 1; }
+  int fl(int x) const { return I[5 + np() + npair() + x] - 1; }
+  // ZSR: 1 = Jacobson et al. (1996), 2 = EQSAM
+  int ztype(int x) const { return I[il(x)]; }
+  int zj_ncat(int x) const { return I[il(x) + 1]; }
+  int zj_nan(int x) const { return I[il(x) + 2]; }
+  int zj_cat(int x) const { return I[il(x) + 3]; }
+  int zj_an(int x) const { return I[il(x) + 4]; }
+  int zj_ny(int x) const { return I[il(x) + 5]; }
+  int ze_nion(int x) const { return I[il(x) + 1]; }
+  int ze_ion(int x, int k) const { return I[il(x) + 2 + np() + k]; }
+  // PD-FiTE
+  int pd_act(int x) const { return I[il(x)]; }
+  int pd_ncat(int x) const { return I[il(x) + 1]; }
+  int pd_nan(int x) const { return I[il(x) + 2]; }
+  int pd_cat(int x) const { return I[il(x) + 3]; }
+  int pd_an(int x) const { return I[il(x) + 4]; }
+  int pd_ninter(int x) const { return I[il(x) + 5]; }
+  int pd_nb(int x, int y) const { return I[il(x) + 6 + (1 + 2 * npair()) * np() + y]; }
+  int pd_pair(int x, int y) const {
+    return I[il(x) + 6 + (1 + 2 * npair()) * np() + pd_ninter(x) + y] - 1;
+  }
+  int pd_loc(int x, int y) const {
+    return I[il(x) + 6 + (1 + 2 * npair()) * np() + 2 * pd_ninter(x) + y] - 1;
+  }
+};
+constexpr int kZsrJacobson = 1, kZsrEqsam = 2;
+}  // namespace
+
+bool Model::add_sub_model(int type, int n_int, int n_float, int n_env, const int* ints,
+                          const double* floats, std::string* err) {
+  if (type != SUB_MODEL_ZSR_AEROSOL_WATER && type != SUB_MODEL_PDFITE) {
+    *err = "sub-model type " + std::to_string(type) +
+           " is not supported (ZSR aerosol water and PD-FiTE activity are)";
+    return false;
+  }
+  if (n_int < 5 || n_env != 1) {
+    *err = "sub-model data does not have the ZSR / PD-FiTE layout";
+    return false;
+  }
+  sub_type_.push_back(type);
+  sub_int_.emplace_back(ints, ints + n_int);
+  sub_flt_.emplace_back(floats, floats + n_float);
+  return true;
+}
+
+// The parameter-Jacobian elements of sub-model k, (computed species, the
+// species it is computed from), in the order get_used_jac_elem registers
+// them (src/sub_models/sub_model_ZSR_aerosol_water.c:81-129,
+// src/sub_models/sub_model_PDFiTE.c:73-97).
+template <typename Fn>
+static void for_sub_elements(int type, const SubView& v, Fn fn) {
+  for (int p = 0; p < v.np(); ++p) {
+    const int w = v.phase(p);
+    if (type == SUB_MODEL_ZSR_AEROSOL_WATER) {
+      fn(w, v.gw());
+      for (int x = 0; x < v.npair(); ++x) {
+        if (v.ztype(x) == kZsrJacobson) {
+          fn(w, w + v.zj_cat(x));
+          fn(w, w + v.zj_an(x));
+        } else if (v.ztype(x) == kZsrEqsam) {
+          for (int k = 0; k < v.ze_nion(x); ++k) fn(w, w + v.ze_ion(x, k));
+        }
+      }
+    } else {
+      for (int x = 0; x < v.npair(); ++x) {
+        const int g = w + v.pd_act(x);
+        fn(g, v.gw());
+        for (int y = 0; y < v.npair(); ++y) {
+          fn(g, w + v.pd_cat(y));
+          fn(g, w + v.pd_an(y));
+        }
+      }
+    }
+  }
+}
+
+// The species the sub-models write (src/sub_models/sub_model_ZSR_aerosol_
+// water.c:228-230: every phase instance's water; src/sub_models/
+// sub_model_PDFiTE.c:196-256: each ion pair's activity coefficient up to the
+// first pair without interactions), in sub-model, phase and pair order.
+// Their inputs must be variable species and they themselves not variable; a
+// reaction may use them only where the device evaluates them per f and J:
+// as the aqueous equilibrium's water and activity coefficient and as HL's
+// aerosol-phase water.
+bool Model::resolve_sub_models(std::string* err) {
+  cv_state_.clear();
+  cv_of_.assign(n_state_, -1);
+  auto state_ok = [&](int s) { return s >= 0 && s < n_state_; };
+  for (size_t k = 0; k < sub_type_.size(); ++k) {
+    const SubView v{sub_int_[k].data(), sub_flt_[k].data()};
+    const std::string what = std::string(sub_type_[k] == SUB_MODEL_PDFITE ? "PD-FiTE" : "ZSR") +
+                             " sub-model " + std::to_string(k);
+    bool bad = false;
+    for_sub_elements(sub_type_[k], v, [&](int dep, int ind) {
+      if (!state_ok(dep) || !state_ok(ind)) {
+        bad = true;
+        return;
+      }
+      if (var_type_[ind] != VAR_VARIABLE || var_type_[dep] == VAR_VARIABLE) bad = true;
+    });
+    if (bad) {
+      *err = what + ": its inputs (gas-phase water, ions) must be variable species and the "
+                    "species it computes not variable";
+      return false;
+    }
+    for (int p = 0; p < v.np(); ++p) {
+      std::vector<int> out;
+      if (sub_type_[k] == SUB_MODEL_ZSR_AEROSOL_WATER) {
+        out.push_back(v.phase(p));
+      } else {
+        for (int x = 0; x < v.npair() && v.pd_ninter(x) > 0; ++x)
+          out.push_back(v.phase(p) + v.pd_act(x));
+      }
+      for (int s : out) {
+        if (cv_of_[s] >= 0) {
+          *err = what + ": state variable " + std::to_string(s) +
+                 " is computed by more than one sub-model";
+          return false;
+        }
+        cv_of_[s] = (int)cv_state_.size();
+        cv_state_.push_back(s);
+      }
+    }
+  }
+  // mass-action terms cannot take a computed species
+  for (const Rxn& r : rxns_)
+    for (const Term& t : r.terms)
+      for (int s : t.react)
+        if (cv_of_[s] >= 0) {
+          *err = "a gas-phase reaction uses a species that a sub-model computes";
+          return false;
+        }
+  return true;
+}
+
+int Model::param_elem_id(int dep, int ind) const {
+  for (int e = pj_colptr_[ind]; e < pj_colptr_[ind + 1]; ++e)
+    if (pj_rowid_[e] == dep) return e;
+  return -1;
+}
+
+// Parameter Jacobian (src/camp_solver.c:1520-1550, src/sub_model_solver.c:
+// 25-104): the dummy element (0, 0), which the fold uses as the unit
+// parameter, then every sub-model element.  The interdependence elements
+// (a sub-model computed from another's output) do not arise: every input is
+// a variable species (resolve_sub_models).
+void Model::build_param_jacobian() {
+  Registry reg(n_state_);
+  reg.add(0, 0);
+  Registry local(n_state_);
+  for (size_t k = 0; k < sub_type_.size(); ++k) {
+    const SubView v{sub_int_[k].data(), sub_flt_[k].data()};
+    for_sub_elements(sub_type_[k], v, [&](int dep, int ind) { local.add(dep, ind); });
+  }
+  std::vector<int> lcp, lri;
+  local.to_csc(&lcp, &lri);
+  for (int ind = 0; ind < n_state_; ++ind)
+    for (int e = lcp[ind]; e < lcp[ind + 1]; ++e) reg.add(lri[e], ind);
+  reg.to_csc(&pj_colptr_, &pj_rowid_);
+}
+
+// Per computed species its program (SubProgram) with the parameter ids of
+// its partials.
+void Model::build_sub_programs() {
+  Tables& t = tab_;
+  t.cv.assign(cv_state_.size(), SubProgram{});
+  for (size_t c = 0; c < cv_state_.size(); ++c) t.cv[c].state = cv_state_[c];
+  for (size_t k = 0; k < sub_type_.size(); ++k) {
+    const SubView v{sub_int_[k].data(), sub_flt_[k].data()};
+    const int gw = v.gw();
+    for (int p = 0; p < v.np(); ++p) {
+      const int w = v.phase(p);
+      if (sub_type_[k] == SUB_MODEL_ZSR_AEROSOL_WATER) {
+        SubProgram& g = t.cv[cv_of_[w]];
+        g.ints = {1, deriv_ids_[gw], v.npair()};
+        for (int x = 0; x < v.npair(); ++x) {
+          const double* F = v.F + v.fl(x);
+          if (v.ztype(x) == kZsrJacobson) {
+            const int c = w + v.zj_cat(x), a = w + v.zj_an(x);
+            g.ints.insert(g.ints.end(), {kZsrJacobson, deriv_ids_[c], deriv_ids_[a], v.zj_ny(x),
+                                         param_elem_id(w, gw), param_elem_id(w, c),
+                                         param_elem_id(w, a)});
+            g.flts.insert(g.flts.end(), {F[0], (double)v.zj_ncat(x), F[1], (double)v.zj_nan(x),
+                                         F[2]});
+            for (int y = 0; y < v.zj_ny(x); ++y) g.flts.push_back(F[3 + y]);
+          } else if (v.ztype(x) == kZsrEqsam) {
+            g.ints.insert(g.ints.end(), {kZsrEqsam, v.ze_nion(x), param_elem_id(w, gw)});
+            for (int i = 0; i < v.ze_nion(x); ++i) {
+              const int s = w + v.ze_ion(x, i);
+              g.ints.insert(g.ints.end(), {deriv_ids_[s], param_elem_id(w, s)});
+            }
+            g.flts.insert(g.flts.end(), {F[0] * 55.51 * 18.01 / F[2] / 1000.0, F[1]});
+            for (int i = 0; i < v.ze_nion(x); ++i) g.flts.push_back(F[3 + i]);
+          } else {
+            g.ints.push_back(0);  // unknown pair type: contributes nothing
+          }
+        }
+      } else {
+        for (int x = 0; x < v.npair() && v.pd_ninter(x) > 0; ++x) {
+          const int gs = w + v.pd_act(x);
+          SubProgram& g = t.cv[cv_of_[gs]];
+          g.ints = {2, deriv_ids_[gw], v.npair(), x, v.pd_ninter(x), param_elem_id(gs, gw)};
+          for (int j = 0; j < v.npair(); ++j) {
+            const int c = w + v.pd_cat(j), a = w + v.pd_an(j);
+            g.ints.insert(g.ints.end(), {deriv_ids_[c], deriv_ids_[a], v.pd_ncat(j) + v.pd_nan(j),
+                                         param_elem_id(gs, c), param_elem_id(gs, a)});
+            const double* F = v.F + v.fl(j);
+            g.flts.insert(g.flts.end(), {F[0], F[1]});
+          }
+          for (int y = 0; y < v.pd_ninter(x); ++y) {
+            g.ints.insert(g.ints.end(), {v.pd_pair(x, y), v.pd_nb(x, y)});
+            const double* F = v.F + v.pd_loc(x, y);
+            g.flts.insert(g.flts.end(), {F[0], F[1]});
+            for (int z = 0; z < v.pd_nb(x, y); ++z) g.flts.push_back(F[2 + z]);
+          }
+        }
+      }
+    }
+  }
 }
 
 int Model::rxn_elem_id(int dep, int ind) const {
@@ -642,21 +906,32 @@ void Model::update_ids() {
   }
 }
 
-// Solver Jacobian: the variable x variable entries of the reaction Jacobian
-// (src/camp_solver.c:1559-1633; a gas-phase model has no sub-model
-// parameters, so every map entry has param_id 0).
+// Solver Jacobian (src/camp_solver.c:1559-1633): a variable row keeps the
+// variable columns of the reaction Jacobian, and a non-variable column c
+// maps to every variable species j of a parameter element (c, j), so that
+// J[row][j] += J_rxn[row][c] * J_params[c][j].  The fold's map lists the
+// terms in reaction-Jacobian order (src/camp_solver.c:1649-1681).
 //
 // The same over the live reaction elements gives the device's Jacobian, with
-// the solver entry of each of its entries.
+// the solver entry of each of its entries; there only computed species map
+// (a constant species, or a registered activity coefficient that PD-FiTE
+// never writes, has zero parameter partials).
 void Model::build_solver_jacobian() {
-  auto build = [&](const std::vector<int>& rcp, const std::vector<int>& rri,
+  auto build = [&](const std::vector<int>& rcp, const std::vector<int>& rri, bool live,
                    std::vector<int>* colptr, std::vector<int>* rowid) {
     Registry reg(n_state_);
-    for (int ind = 0; ind < n_state_; ++ind) {
-      if (var_type_[ind] != VAR_VARIABLE) continue;
-      for (int e = rcp[ind]; e < rcp[ind + 1]; ++e)
-        if (var_type_[rri[e]] == VAR_VARIABLE) reg.add(rri[e], ind);
-    }
+    for (int ind = 0; ind < n_state_; ++ind)
+      for (int e = rcp[ind]; e < rcp[ind + 1]; ++e) {
+        const int dep = rri[e];
+        if (var_type_[dep] != VAR_VARIABLE) continue;
+        if (var_type_[ind] == VAR_VARIABLE) {
+          reg.add(dep, ind);
+          continue;
+        }
+        if (live && cv_of_[ind] < 0) continue;
+        for (int j = 0; j < n_state_; ++j)
+          if (var_type_[j] == VAR_VARIABLE && param_elem_id(ind, j) != -1) reg.add(dep, j);
+      }
     std::vector<int> cp, ri;
     reg.to_csc(&cp, &ri);
     colptr->assign(n_dep_ + 1, 0);
@@ -666,8 +941,29 @@ void Model::build_solver_jacobian() {
     rowid->resize(ri.size());
     for (size_t e = 0; e < ri.size(); ++e) (*rowid)[e] = deriv_ids_[ri[e]];
   };
-  build(rj_colptr_, rj_rowid_, &sj_colptr_, &sj_rowid_);
-  build(rl_colptr_, rl_rowid_, &dj_colptr_, &dj_rowid_);
+  build(rj_colptr_, rj_rowid_, false, &sj_colptr_, &sj_rowid_);
+  build(rl_colptr_, rl_rowid_, true, &dj_colptr_, &dj_rowid_);
+  auto sj_id = [&](int dep, int ind) {
+    const int r = deriv_ids_[dep], c = deriv_ids_[ind];
+    for (int e = sj_colptr_[c]; e < sj_colptr_[c + 1]; ++e)
+      if (sj_rowid_[e] == r) return e;
+    return -1;
+  };
+  jac_map_.clear();
+  for (int ind = 0; ind < n_state_; ++ind)
+    for (int e = rj_colptr_[ind]; e < rj_colptr_[ind + 1]; ++e) {
+      const int dep = rj_rowid_[e];
+      if (var_type_[dep] != VAR_VARIABLE) continue;
+      if (var_type_[ind] == VAR_VARIABLE) {
+        jac_map_.insert(jac_map_.end(), {sj_id(dep, ind), e, 0});
+        continue;
+      }
+      for (int j = 0; j < n_state_; ++j) {
+        const int pid = param_elem_id(ind, j);
+        if (pid != -1 && var_type_[j] == VAR_VARIABLE)
+          jac_map_.insert(jac_map_.end(), {sj_id(dep, j), e, pid});
+      }
+    }
   dj_to_sj_.assign(dj_rowid_.size(), -1);
   for (int c = 0; c < n_dep_; ++c) {
     int q = sj_colptr_[c];
@@ -1039,12 +1335,15 @@ void Model::build_tables() {
     int nd = 0;
     if (si.type == RXN_SIMPOL_PHASE_TRANSFER)
       for (int e : si.elem) nd += var_type_[e] == VAR_VARIABLE;
-    n_part_all += 4 + 4 * nd;
+    // HL with a computed water: the gas and aerosol rows against it
+    n_part_all += 4 + 4 * nd + (si.water_cv >= 0 ? 2 : 0);
   }
-  // aqueous equilibrium instances: 2 per-cell constants (forward, reverse)
-  // after the SIMPOL constants, a loss and a gain pseudo-rate per dependent
-  // species slot after the SIMPOL pseudo-rates, and per dependent
-  // independent slot a partial for every dependent row slot
+  // aqueous equilibrium instances: 3 per-cell constants (forward, reverse,
+  // minimum water) after the SIMPOL constants, a loss and a gain pseudo-rate
+  // per dependent species slot after the SIMPOL pseudo-rates, per dependent
+  // independent slot a partial for every dependent row slot, then per row
+  // slot its partial against a computed water and against a computed
+  // activity coefficient
   t.aq = aq_;
   t.n_aq = (int)aq_.size();
   t.aq_keff0.clear();
@@ -1055,13 +1354,19 @@ void Model::build_tables() {
     for (int sp : q.react) S += var_type_[sp] == VAR_VARIABLE;
     for (int sp : q.prod) S += var_type_[sp] == VAR_VARIABLE;
     t.aq_keff0.push_back(t.n_keff);
-    t.n_keff += 2;
+    t.n_keff += 3;
     t.aq_rate0.push_back(t.n_rates);
     t.n_rates += 2 * S;
     t.aq_part0.push_back(n_part_all);
-    n_part_all += S * S;
+    n_part_all += S * S + S * (q.water_cv >= 0) + S * (q.act_cv >= 0) + S * (int)q.cp_cv.size();
   }
   t.n_part_all = n_part_all;
+  // sub-models: computed species and their programs, PPM_TO_RH_ per cell
+  build_sub_programs();
+  t.n_cv = (int)cv_state_.size();
+  t.n_pj = (int)pj_rowid_.size();
+  t.sm_keff = -1;
+  if (t.n_cv > 0) t.sm_keff = t.n_keff++;
   // f gather: per dependent species, in term order, reactant occurrences
   // (loss, coefficient -1) before products (coefficient yield)
   std::vector<std::vector<int>> frx(n_dep_), fpr(n_dep_);
@@ -1207,6 +1512,88 @@ void Model::build_tables() {
         jind[e].push_back(loss ? -1 : -2);
       }
   }
+  // virtual slots: the live reaction-Jacobian elements of a variable row
+  // against a computed species, ordered by column then row
+  std::vector<int> vrow, vcol;
+  std::vector<std::vector<int>> vpart;
+  {
+    auto vslot = [&](int dep_state, int cv_state) {
+      for (size_t v = 0; v < vrow.size(); ++v)
+        if (vrow[v] == dep_state && vcol[v] == cv_state) return (int)v;
+      return -1;
+    };
+    for (int ind = 0; ind < n_state_; ++ind) {
+      if (cv_of_[ind] < 0) continue;
+      for (int e = rl_colptr_[ind]; e < rl_colptr_[ind + 1]; ++e)
+        if (var_type_[rl_rowid_[e]] == VAR_VARIABLE) {
+          vrow.push_back(rl_rowid_[e]);
+          vcol.push_back(ind);
+        }
+    }
+    vpart.assign(vrow.size(), {});
+    // HL: the gas and aerosol rows against the computed water
+    // (src/rxns/rxn_HL_phase_transfer.c:383-389, 398-404)
+    for (int k = 0; k < t.n_simpol; ++k) {
+      const SimpolInst& si = simpol_[k];
+      if (si.water_cv < 0) continue;
+      const int p0 = t.si_part0[k];
+      vpart[vslot(si.gas, si.water)].push_back(p0 + 4);
+      vpart[vslot(si.aero, si.water)].push_back(p0 + 5);
+    }
+    // aqueous equilibrium: every dependent row against the computed water
+    // and activity coefficient (src/rxns/rxn_aqueous_equilibrium.c:486-537)
+    for (int k = 0; k < t.n_aq; ++k) {
+      const AqInst& q = aq_[k];
+      std::vector<int> rows;
+      for (const std::vector<int>* list : {&q.react, &q.prod})
+        for (int sp : *list)
+          if (var_type_[sp] == VAR_VARIABLE) rows.push_back(sp);
+      const int S = (int)rows.size();
+      int p = t.aq_part0[k] + S * S;
+      if (q.water_cv >= 0)
+        for (int b = 0; b < S; ++b) vpart[vslot(rows[b], q.water)].push_back(p++);
+      if (q.act_cv >= 0)
+        for (int b = 0; b < S; ++b) vpart[vslot(rows[b], q.act)].push_back(p++);
+      // a computed reactant or product as an independent species
+      // (src/rxns/rxn_aqueous_equilibrium.c:436-479)
+      for (size_t j = 0; j < q.cp_state.size(); ++j)
+        for (int b = 0; b < S; ++b) vpart[vslot(rows[b], q.cp_state[j])].push_back(p++);
+    }
+  }
+  t.n_virt = (int)vrow.size();
+  t.jv_ptr.assign(1, 0);
+  t.jv_part.clear();
+  t.jv_row.clear();
+  for (int v = 0; v < t.n_virt; ++v) {
+    t.jv_part.insert(t.jv_part.end(), vpart[v].begin(), vpart[v].end());
+    t.jv_ptr.push_back((int)t.jv_part.size());
+    t.jv_row.push_back(deriv_ids_[vrow[v]]);
+  }
+  // the chain, grouped by target device slot: V(row, c) * P(c, j) into
+  // J(row, j) for every variable j of the computed species' parameter row
+  {
+    std::vector<std::vector<std::pair<int, int>>> by_slot(t.n_jac);
+    for (int v = 0; v < t.n_virt; ++v)
+      for (int j = 0; j < n_state_; ++j) {
+        if (var_type_[j] != VAR_VARIABLE) continue;
+        const int pid = param_elem_id(vcol[v], j);
+        if (pid < 0) continue;
+        by_slot[slot_of(deriv_ids_[vrow[v]], deriv_ids_[j])].push_back({v, pid});
+      }
+    t.ch_tgt.clear();
+    t.ch_ptr.assign(1, 0);
+    t.ch_v.clear();
+    t.ch_p.clear();
+    for (int e = 0; e < t.n_jac; ++e) {
+      if (by_slot[e].empty()) continue;
+      t.ch_tgt.push_back(e);
+      for (const auto& vp : by_slot[e]) {
+        t.ch_v.push_back(vp.first);
+        t.ch_p.push_back(vp.second);
+      }
+      t.ch_ptr.push_back((int)t.ch_v.size());
+    }
+  }
   t.jg_ptr.assign(t.n_jac + 1, 0);
   t.jg_part.clear(); t.jg_coef.clear(); t.jg_ind.clear();
   t.jg_lupos.assign(t.n_jac, 0);
@@ -1237,10 +1624,12 @@ bool Model::build(std::string* err) {
     *err = "no dependent (VARIABLE) state variables";
     return false;
   }
+  if (!resolve_sub_models(err)) return false;
   if (!resolve_simpol(err)) return false;
   if (!resolve_aq(err)) return false;
   build_rxn_jacobian();
   update_ids();
+  build_param_jacobian();
   build_solver_jacobian();
   build_lu();
   build_tables();

@@ -25,6 +25,9 @@ enum : int {
   RXN_SIMPOL_PHASE_TRANSFER = 10,
 };
 
+// sub-model type ids, src/sub_model_solver.c:16-18
+enum : int { SUB_MODEL_ZSR_AEROSOL_WATER = 2, SUB_MODEL_PDFITE = 3 };
+
 // aerosol representation types, src/aero_rep_solver.c:19-20; section types
 // of the modal/binned mass representation
 enum : int { AERO_REP_MODAL_BINNED_MASS = 2 };
@@ -65,6 +68,7 @@ struct SimpolInst {
   std::vector<int> elem;            // state indices
   std::vector<double> inv_rho, inv_mw;  // 1/density; 1/MW in the phase, else 0
   std::vector<char> in_phase;
+  int water_cv = -1;                // HL: the water's computed-species index, -1 if constant
 };
 
 // One phase instance of an aqueous equilibrium reaction
@@ -83,6 +87,40 @@ struct AqInst {
   int water = -1, act = -1;           // state indices (act: -1 when none)
   double A = 1.0, C = 0.0, kr = 0.0;  // equilibrium constant parameters, k_reverse
   double thr = 0.0;                   // water below which the reaction is off
+  // computed-species indices of the water and the activity coefficient when
+  // a sub-model computes them (-1: a constant species, folded per cell)
+  int water_cv = -1, act_cv = -1;
+  // reactants and products that a sub-model computes (the water of
+  // H2O_aq <=> H+ + OH-): state index, computed index, 1e3 / MW, reactant
+  // flag; they enter the rates per evaluation, not per cell
+  std::vector<int> cp_state, cp_cv;
+  std::vector<double> cp_m;
+  std::vector<char> cp_r;
+};
+
+// One species that a sub-model computes from the state before every f and J
+// (src/sub_model_solver.c:300-333): the aerosol-phase water of a ZSR phase
+// instance or the activity coefficient of a PD-FiTE ion pair, with a compact
+// program for its value and for its row of the parameter Jacobian.
+//   ZSR water (kind 1), ints: kind, gas-water dependent index, pair count,
+//     then per ion pair its type and
+//       Jacobson: cation, anion (dependent indices), Y count, parameter ids
+//                 of d/d(gas water), d/d(cation), d/d(anion);
+//       EQSAM: ion count, parameter id of d/d(gas water), per ion its
+//              dependent index and parameter id;
+//     floats per pair: Jacobson: low RH, cation count, cation MW, anion
+//     count, anion MW, Y...; EQSAM: NW 55.51 18.01 / MW / 1000, ZW, ion MWs.
+//   PD-FiTE activity of pair x (kind 2), ints: kind, gas-water dependent
+//     index, pair count, x, interaction count, parameter id of d/d(gas
+//     water), per pair j: cation, anion (dependent indices), cation + anion
+//     stoichiometry, parameter ids of d/d(cation j), d/d(anion j); per
+//     interaction: its pair, B count;
+//     floats: per pair cation MW, anion MW; per interaction min RH, max RH,
+//     B...
+struct SubProgram {
+  int state = -1;  // state index of the computed species
+  std::vector<int> ints;
+  std::vector<double> flts;
 };
 
 // kinds of f gather entries (Tables::fg_prod)
@@ -153,6 +191,20 @@ struct Tables {
   int n_aq = 0;
   std::vector<AqInst> aq;
   std::vector<int> aq_keff0, aq_rate0, aq_part0;
+  // sub-models: the computed species (per-cell values written before every
+  // f and J after the rates or partials), their programs, the parameter
+  // Jacobian size (its element ids index the parameter partials), and the
+  // per-cell constant PPM_TO_RH_ at keff slot sm_keff
+  int n_cv = 0, n_pj = 0, sm_keff = -1;
+  std::vector<SubProgram> cv;
+  // rate partials against computed species gather into virtual Jacobian
+  // slots (a variable row, a computed column; each partial adds with
+  // coefficient 1), which the chain then folds into the solver slots:
+  // J[ch_tgt[g]] += sum over [ch_ptr[g], ch_ptr[g+1]) of V[ch_v] * P[ch_p]
+  // (src/camp_solver.c:1096-1106 with J_params)
+  int n_virt = 0;
+  std::vector<int> jv_ptr, jv_part, jv_row;
+  std::vector<int> ch_tgt, ch_ptr, ch_v, ch_p;
   int n_part_all = 0;  // n_part + SIMPOL and aqueous partials
   int n_keff = 0;      // n_rxn + 8 n_simpol + 2 n_aq
   int n_rates = 0;     // n_rxn + 4 n_simpol + aqueous pseudo-rates
@@ -212,6 +264,17 @@ class Model {
   // modes of every representation, (representation, section) in order: the
   // GMD / GSD host-set columns after the reaction columns
   const std::vector<std::pair<int, int>>& modes() const { return modes_; }
+  // sub_model_add_condensed_data (src/sub_model_solver.c:425-470): ZSR
+  // aerosol water and PD-FiTE activity; ints without the type slot
+  bool add_sub_model(int type, int n_int, int n_float, int n_env, const int* ints,
+                     const double* floats, std::string* err);
+  int n_sub_model() const { return (int)sub_type_.size(); }
+  // the sub-model parameter Jacobian (CSC over state variables, with the
+  // dummy element (0, 0)) and the solver Jacobian fold as (solver id,
+  // reaction-Jacobian id, parameter id) triplets
+  const std::vector<int>& param_colptr() const { return pj_colptr_; }
+  const std::vector<int>& param_rowid() const { return pj_rowid_; }
+  const std::vector<int>& jac_map() const { return jac_map_; }
   // aero_rep_update_data for the modal/binned representation: the id and
   // the section of a GMD (what 0) / GSD (what 1) update -> its column, or -1
   int aero_column(int rep_id, int section, int what) const;
@@ -268,7 +331,11 @@ class Model {
   bool resolve_simpol(std::string* err);
   bool resolve_instance(SimpolInst* si, int phase, int ri, std::string* err);
   bool resolve_aq(std::string* err);
+  bool resolve_sub_models(std::string* err);
+  void build_param_jacobian();
+  void build_sub_programs();
   int rxn_elem_id(int dep, int ind) const;
+  int param_elem_id(int dep, int ind) const;
 
   int n_state_, n_cells_, n_dep_, n_rxn_;
   int n_added_ = 0, n_env_ = 0, n_terms_ = 0, n_host_rate_ = 0;
@@ -283,6 +350,12 @@ class Model {
   std::vector<std::pair<int, int>> modes_;
   std::vector<SimpolInst> simpol_;
   std::vector<AqInst> aq_;
+  // sub-models as added; computed species (state index -> computed index)
+  std::vector<int> sub_type_;
+  std::vector<std::vector<int>> sub_int_;
+  std::vector<std::vector<double>> sub_flt_;
+  std::vector<int> cv_state_, cv_of_;
+  std::vector<int> pj_colptr_, pj_rowid_, jac_map_;
   std::vector<double> abs_tol_;
   std::vector<int> deriv_ids_;
   std::vector<int> rj_colptr_, rj_rowid_;

@@ -35,14 +35,18 @@ struct DevMech {
   const double* si_prm;
   const int *si_type, *si_kind, *si_gmd_col, *si_gsd_col, *si_act, *si_water, *si_nph,
       *si_cptr, *si_cidx;
+  const int* si_wcv;  // HL: computed water index, -1 for a constant water
   const double *si_dp, *si_cinv_rho, *si_cinv_mw, *si_cin;
   // aqueous equilibrium instances: A, C, k_reverse and the minimum water;
-  // water and activity coefficient state indices (-1: none) and reactant /
-  // product counts; the constant (not dependent) reactants and products:
-  // state index, 1e3 / MW, reactant flag
+  // water and activity coefficient state indices (-1: none), reactant /
+  // product counts and the computed-species indices of the water and the
+  // activity coefficient (-1: constant); the constant (not dependent)
+  // reactants and products: state index, 1e3 / MW, reactant flag
   int n_aq;
   const double *aq_prm, *aq_cm;
   const int *aq_int, *aq_cptr, *aq_cidx, *aq_cr;
+  // keff slot of the sub-models' PPM_TO_RH_ (-1: no sub-models)
+  int sm_keff;
 };
 
 template <typename T>
@@ -154,7 +158,8 @@ static __device__ void simpol_constants(const DevMech& m, int k,
     c[1] = 1.0;
     c[2] = 1.0 / (f[6] * T / P);
     c[3] = c[4] = c[5] = c[6] = 1.0;
-    c[7] = kh * (w > bdf::kTiny ? w : bdf::kTiny);
+    // a computed water is applied per evaluation (simpol_state)
+    c[7] = ldg(m.si_wcv + k) >= 0 ? kh : kh * (w > bdf::kTiny ? w : bdf::kTiny);
     return;
   }
   double vp = f[4] / T + f[5] + f[6] * T + f[7] * log(T);
@@ -179,11 +184,13 @@ static __device__ void simpol_constants(const DevMech& m, int k,
 
 // Forward and reverse rate constants of every aqueous equilibrium instance
 // (src/rxns/rxn_aqueous_equilibrium.c:244-262, 278-305), one lane per
-// instance, into keff[2 q], keff[2 q + 1], with the constant factors folded
+// instance, into keff[3 q], keff[3 q + 1], with the constant factors folded
 // in: k_f = K_eq k_r times (c m) of each constant reactant and 1 / W per
 // reactant after the first; k_r times the activity coefficient, (c m) of
 // each constant product and 1 / W per product after the first.  Both are
-// zero when the water is below its minimum (:331-336).  Out of line and
+// zero when the water is below its minimum (:331-336).  A water or activity
+// coefficient that a sub-model computes is left out here and applied per
+// evaluation (aq_fr), with the minimum water in keff[3 q + 2].  Out of line and
 // over plain pointers, so that mechanisms without these reactions keep the
 // solve kernel's register allocation.
 static __device__ __noinline__ void aq_constants(const double* prm, const int* ii,
@@ -193,18 +200,20 @@ static __device__ __noinline__ void aq_constants(const double* prm, const int* i
                                                  double* keff, int lane) {
   for (int q = lane; q < n_aq; q += 32) {
     const double* f = prm + 4 * q;
-    const int* iq = ii + 4 * q;
-    double* c = keff + 2 * q;
+    const int* iq = ii + 6 * q;
+    double* c = keff + 3 * q;
+    const bool wdyn = ldg(iq + 4) >= 0, gdyn = ldg(iq + 5) >= 0;
     double w = cell_state[ldg(iq)];
     w = w > bdf::kTiny ? w : bdf::kTiny;
-    if (w < ldg(f + 3)) {
+    c[2] = ldg(f + 3);
+    if (!wdyn && w < ldg(f + 3)) {
       c[0] = c[1] = 0.0;
       continue;
     }
     const double eq = f[1] == 0.0 ? f[0] : f[0] * exp(f[1] * (1.0 / T - 1.0 / 298.0));
     double kf = eq * f[2], kr = f[2];
     const int act = ldg(iq + 1);
-    if (act >= 0) kr *= cell_state[act];
+    if (act >= 0 && !gdyn) kr *= cell_state[act];
     for (int j = ldg(cptr + q); j < ldg(cptr + q + 1); ++j) {
       double v = cell_state[ldg(cidx + j)];
       v = (v > bdf::kTiny ? v : bdf::kTiny) * ldg(cm + j);
@@ -213,8 +222,10 @@ static __device__ __noinline__ void aq_constants(const double* prm, const int* i
       else
         kr *= v;
     }
-    for (int i = 1; i < ldg(iq + 2); ++i) kf /= w;
-    for (int i = 1; i < ldg(iq + 3); ++i) kr /= w;
+    if (!wdyn) {
+      for (int i = 1; i < ldg(iq + 2); ++i) kf /= w;
+      for (int i = 1; i < ldg(iq + 3); ++i) kr /= w;
+    }
     c[0] = kf;
     c[1] = kr;
   }
@@ -223,7 +234,8 @@ static __device__ __noinline__ void aq_constants(const double* prm, const int* i
 // k of every reaction times the (clamped) constant-species concentrations it
 // multiplies; constant species are clamped to TINY as solver_run does.  The
 // SIMPOL constants follow the terms' (keff[n_rxn + 8 k ..]), then the
-// aqueous equilibrium ones (keff[n_rxn + 8 n_simpol + 2 q ..]).
+// aqueous equilibrium ones (keff[n_rxn + 8 n_simpol + 3 q ..]), then the
+// sub-models' PPM_TO_RH_.
 static __device__ void compute_keff(const DevMech& m, const double* cell_state,
                              double T, double P, const double* photo_cell,
                              double* keff, int lane) {
@@ -240,6 +252,13 @@ static __device__ void compute_keff(const DevMech& m, const double* cell_state,
   if (m.n_aq > 0)
     aq_constants(m.aq_prm, m.aq_int, m.aq_cptr, m.aq_cidx, m.aq_cm, m.aq_cr, m.n_aq, cell_state,
                  T, keff + m.n_rxn + 8 * m.n_simpol, lane);
+  if (m.sm_keff >= 0 && lane == 0) {
+    // PPM_TO_RH_: the MOSAIC water vapour pressure fit
+    // (src/sub_models/sub_model_ZSR_aerosol_water.c:198-214)
+    double a = 1.0 - 373.15 / T;
+    a = (((-0.1299 * a - 0.6445) * a - 1.976) * a + 13.3185) * a;
+    keff[m.sm_keff] = P / (101325.0 * exp(a)) / 1.0e6;
+  }
   __syncwarp();
 }
 

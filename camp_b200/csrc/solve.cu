@@ -47,6 +47,7 @@ constexpr int DO_ERROR_TEST = 100, PREDICT_AGAIN = 101, TRY_AGAIN = 102;
 // Cells (warps) per block of the solve kernel: its launch bound leaves 168
 // registers per thread, enough to keep the BDF state without spilling.
 constexpr int kMaxCellsPerBlock = 12;
+constexpr int kMaxCellsAero = 8;  // cells per block of the aerosol form
 
 struct Layout {  // per-warp shared-memory slice (byte offsets; -1 = not in it)
   int zn, ewt, acor, y, ftemp, tempv, rates, keff, fscr, lu, z, dinv, ctl, bytes;
@@ -141,8 +142,8 @@ struct Tab {
   const double* atol;
   const uint16_t *lu_rowptr, *lu_col;
   const uint32_t *upd_ptr, *upd;
-  const uint16_t *si_rec, *si_elem, *jg_umid, *aq_rec, *aq_sp;
-  const double *si_ef, *aq_sm;
+  const uint16_t *si_rec, *si_elem, *jg_umid, *aq_rec, *aq_sp, *aq_cp;
+  const double *si_ef, *aq_sm, *aq_cpm;
   int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev, n_simpol, has_ug, n_aq;
 };
 
@@ -178,6 +179,8 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.aq_rec = (const uint16_t*)(b + o.aq_rec);
   t.aq_sp = (const uint16_t*)(b + o.aq_sp);
   t.aq_sm = (const double*)(b + o.aq_sm);
+  t.aq_cp = (const uint16_t*)(b + o.aq_cp);
+  t.aq_cpm = (const double*)(b + o.aq_cpm);
   t.n_aq = o.n_aq;
   t.fb_lane = (const uint16_t*)(b + o.fb_lane);
   t.fb_unit = (const uint32_t*)(b + o.fb_unit);
@@ -273,6 +276,185 @@ __device__ __forceinline__ bool rates_of(const Tab& t, const double* y, const do
   return warp_any(neg);
 }
 
+// ---------------------------------------------------------------------------
+// Sub-models: the species they compute, before every f and J
+// ---------------------------------------------------------------------------
+// ZSR aerosol water of one phase instance
+// (src/sub_models/sub_model_ZSR_aerosol_water.c:225-305, Jacobian :318-437)
+// from its program (SubProgram in model.hpp); P, when given, receives the
+// partials of the water against the gas-phase water and the ions.
+__device__ double zsr_water(const int* I, const double* F, const double* y, double ppm,
+                            double* P) {
+  const double a_w = ppm * state_of(y[I[1]]);
+  const int npair = I[2];
+  double W = 1.0e-30;  // MINIMUM_WATER_MASS_
+  int ii = 3, fi = 0;
+  #pragma unroll 1
+  for (int x = 0; x < npair; ++x) {
+    const int type = I[ii++];
+    if (type == 1) {  // Jacobson et al. (1996)
+      const int ci = I[ii], ai = I[ii + 1], ny = I[ii + 2];
+      const int pg = I[ii + 3], pc = I[ii + 4], pa = I[ii + 5];
+      ii += 6;
+      const double low = F[fi], ncat = F[fi + 1], mwc = F[fi + 2], nan_ = F[fi + 3],
+                   mwa = F[fi + 4];
+      const double* Y = F + fi + 5;
+      fi += 5 + ny;
+      const double j_aw = a_w > low ? a_w : low;
+      double mol = 0.0;
+      #pragma unroll 1
+      for (int k = 0; k < ny; ++k) mol += Y[k] * dpow(j_aw, (double)k);
+      const double cat = ddiv(ddiv(ddiv(state_of(y[ci]), ncat), mwc), 1000.0);
+      const double an = ddiv(ddiv(ddiv(state_of(y[ai]), nan_), mwa), 1000.0);
+      // smooth minimum of the ion concentrations (smoothing factor -100)
+      const double ec = exp(-100.0 * cat), ea = exp(-100.0 * an);
+      const double conc = ddiv(cat * ec + an * ea, ec + ea);
+      W += ddiv(conc, mol * mol) * 1000.0;
+      if (P) {
+        double mj = Y[0], dm = 0.0;
+        #pragma unroll 1
+        for (int k = 1; k < ny; ++k) {
+          mj += Y[k] * dpow(j_aw, (double)k);
+          dm += Y[k] * k * dpow(j_aw, (double)(k - 1));
+        }
+        dm *= a_w > low ? ppm : 0.0;
+        const double den = (ec + ea) * (ec + ea);
+        const double dcc = ddiv(ec * ec + ec * ea * (1.0 + 100.0 * an - 100.0 * cat), den);
+        const double dca = ddiv(ea * ea + ec * ea * (1.0 + 100.0 * cat - 100.0 * an), den);
+        P[pg] += ddiv(-2.0 * conc, dpow(mj, 3.0)) * 1000.0 * dm;
+        P[pa] += ddiv(1.0, dpow(mj, 2.0)) * 1000.0 * dca * ddiv(1.0, nan_ * mwa * 1000.0);
+        P[pc] += ddiv(1.0, dpow(mj, 2.0)) * 1000.0 * dcc * ddiv(1.0, ncat * mwc * 1000.0);
+      }
+    } else if (type == 2) {  // EQSAM (Metzger et al., 2002)
+      const int nion = I[ii], pg = I[ii + 1];
+      ii += 2;
+      const double pre = F[fi], zw = F[fi + 1];
+      fi += 2;
+      double e_aw = a_w > 0.99 ? 0.99 : a_w;
+      e_aw = e_aw < 0.001 ? 0.001 : e_aw;
+      const double base = pre * (ddiv(1.0, e_aw) - 1.0);
+      const double mol = dpow(base, zw);
+      double dmol = 0.0;
+      if (P) {
+        const double de = (a_w > 0.99 || a_w < 0.001) ? 0.0 : ppm;
+        dmol = zw * dpow(base, zw - 1.0) * ddiv(-pre, e_aw * e_aw) * de;
+      }
+      #pragma unroll 1
+      for (int k = 0; k < nion; ++k) {
+        const int ion = I[ii], pid = I[ii + 1];
+        ii += 2;
+        const double mw = F[fi++];
+        double c = state_of(y[ion]);
+        c = c > 0.0 ? c : 0.0;
+        W += ddiv(ddiv(c, mw), mol);
+        if (P) {
+          P[pg] += ddiv(-c, mw * mol * mol) * dmol;
+          P[pid] += ddiv(c > 0.0 ? 1.0 : 0.0, mw * mol);
+        }
+      }
+    }
+  }
+  return W;
+}
+
+// PD-FiTE activity coefficient of one ion pair in one phase instance
+// (src/sub_models/sub_model_PDFiTE.c:167-259, Jacobian :273-432; Topping et
+// al. 2009, eq. 15) from its program; P, when given, receives its partials
+// against the gas-phase water and every ion.
+__device__ double pdfite_gamma(const int* I, const double* F, const double* y, double ppm,
+                               double* P) {
+  double a_w = ppm * state_of(y[I[1]]);
+  a_w = a_w < 0.0 ? 0.0 : (a_w > 1.0 ? 1.0 : a_w);
+  const int npair = I[2], x = I[3], ninter = I[4], pw = I[5];
+  const int* pr = I + 6;              // per pair: cation, anion, stoichiometry, 2 param ids
+  const int* it = pr + 5 * npair;     // per interaction: pair, B count
+  const double* fb = F + 2 * npair;   // per interaction: min RH, max RH, B...
+  auto cn = [&](int j) { return ddiv(ddiv(state_of(y[pr[5 * j]]), F[2 * j]), 1000000.0); };
+  auto an = [&](int j) { return ddiv(ddiv(state_of(y[pr[5 * j + 1]]), F[2 * j + 1]), 1000000.0); };
+  double omega = 0.0;
+  #pragma unroll 1
+  for (int j = 0; j < npair; ++j)
+    if (j != x) omega += 2.0 * pr[5 * j + 2] * cn(j) * an(j);
+  auto in_range = [&](double lo, double hi) {
+    return !((a_w <= lo || a_w > hi) && !(a_w <= 0.0 && lo <= 0.0));
+  };
+  double lng = 0.0;
+  int fi = 0;
+  #pragma unroll 1
+  for (int k = 0; k < ninter; ++k) {
+    const int j = it[2 * k], nb = it[2 * k + 1];
+    const double lo = fb[fi], hi = fb[fi + 1];
+    const double* B = fb + fi + 2;
+    fi += 2 + nb;
+    if (!in_range(lo, hi)) continue;
+    double li = 0.0;
+    #pragma unroll 1
+    for (int z = 0; z < nb; ++z) li += B[z] * dpow(a_w, (double)z);
+    if (j == x)
+      lng += li;
+    else if (omega > 0.0)
+      lng += ddiv(li * cn(j) * an(j), omega);
+  }
+  const double g = exp(lng);
+  if (P) {
+    fi = 0;
+    #pragma unroll 1
+    for (int k = 0; k < ninter; ++k) {
+      const int j = it[2 * k], nb = it[2 * k + 1];
+      const double lo = fb[fi], hi = fb[fi + 1];
+      const double* B = fb + fi + 2;
+      fi += 2 + nb;
+      if (!in_range(lo, hi)) continue;
+      double li = B[0], dli = 0.0;
+      #pragma unroll 1
+      for (int z = 1; z < nb; ++z) {
+        li += B[z] * dpow(a_w, (double)z);
+        dli += B[z] * z * dpow(a_w, (double)(z - 1));
+      }
+      dli *= ppm;
+      if (j == x) {
+        P[pw] += g * dli;
+      } else if (omega > 0.0) {
+        const double cj = cn(j), aj = an(j);
+        P[pr[5 * j + 3]] += ddiv(g * li * aj, F[2 * j] * omega) * 1.0e-6;
+        P[pr[5 * j + 4]] += ddiv(g * li * cj, F[2 * j + 1] * omega) * 1.0e-6;
+        P[pw] += ddiv(g * cj * aj, omega) * dli;
+        const double s = ddiv(-g * li * cj * aj, omega * omega) * 2.0;
+        #pragma unroll 1
+        for (int q = 0; q < npair; ++q) {
+          if (q == x) continue;
+          P[pr[5 * q + 3]] += ddiv(s * pr[5 * q + 2] * an(q), F[2 * q]) * 1.0e-6;
+          P[pr[5 * q + 4]] += ddiv(s * pr[5 * q + 2] * cn(q), F[2 * q + 1]) * 1.0e-6;
+        }
+      }
+    }
+  }
+  return g;
+}
+
+// Every computed species, one lane each, into cv; with P, also the
+// parameter Jacobian (P zeroed first; element ids index it)
+__device__ __noinline__ void sub_model_eval(const char* tb, const double* y, const double* keff,
+                                            double* cv, double* P, int lane) {
+  const BlobOff& o = *reinterpret_cast<const BlobOff*>(tb);
+  if (P) {
+    #pragma unroll 1
+    for (int i = lane; i < o.n_pj; i += 32) P[i] = 0.0;
+    __syncwarp();
+  }
+  const uint32_t* rec = (const uint32_t*)(tb + o.sm_rec);
+  const int* I0 = (const int*)(tb + o.sm_int);
+  const double* F0 = (const double*)(tb + o.sm_flt);
+  const double ppm = keff[o.sm_keff];
+  #pragma unroll 1
+  for (int c = lane; c < o.n_cv; c += 32) {
+    const int* I = I0 + rec[2 * c];
+    const double* F = F0 + rec[2 * c + 1];
+    cv[c] = I[0] == 1 ? zsr_water(I, F, y, ppm, P) : pdfite_gamma(I, F, y, ppm, P);
+  }
+  __syncwarp();
+}
+
 // SIMPOL phase transfer, one lane per instance
 // (src/rxns/rxn_SIMPOL_phase_transfer.c:337-450 and 463-744, the total-mass
 // branch of the modal/binned representation): the mode's or bin's number
@@ -286,7 +468,7 @@ struct SimpolState {
   double N, cond, evap, evap_rate, m, mol, inv_k;
 };
 __device__ __forceinline__ SimpolState simpol_state(const Tab& t, int k, const double* y,
-                                                    const double* keff) {
+                                                    const double* keff, const double* cv) {
   const uint16_t* rec = t.si_rec + 8 * k;
   const double* c = keff + t.n_rxn + 8 * k;
   double V = c[5], m = c[6], mol = c[7];
@@ -306,6 +488,8 @@ __device__ __forceinline__ SimpolState simpol_state(const Tab& t, int k, const d
   s.inv_k = c[2];
   // k_c K_eq MW / m = k_c K_eq / moles
   s.evap_rate = ddiv(c[0] * c[1], mol) * c[4];
+  // HL with a water that a sub-model computes: evaporation per water
+  if (rec[5]) s.evap_rate = ddiv(s.evap_rate, cv[rec[5] - 1]);
   s.cond = c[0] * state_of(y[rec[0]]);
   s.evap = s.evap_rate * state_of(y[rec[1]]);
   return s;
@@ -314,12 +498,12 @@ __device__ __forceinline__ SimpolState simpol_state(const Tab& t, int k, const d
 // the four pseudo-rates per instance; returns (warp-uniform) whether any is
 // negative
 __device__ __noinline__ bool simpol_rates(const char* tb, const double* y, const double* keff,
-                                          double* rates, int lane) {
+                                          const double* cv, double* rates, int lane) {
   const Tab t = make_tab(tb);
   bool neg = false;
   #pragma unroll 1
   for (int k = lane; k < t.n_simpol; k += 32) {
-    const SimpolState s = simpol_state(t, k, y, keff);
+    const SimpolState s = simpol_state(t, k, y, keff, cv);
     double* r = rates + t.n_rxn + 4 * k;
     r[0] = s.N * s.evap;            // gas gain
     r[1] = s.N * s.cond;            // gas loss
@@ -332,20 +516,28 @@ __device__ __noinline__ bool simpol_rates(const char* tb, const double* y, const
 
 // Jacobian partials per instance: gas-gas loss, aerosol-gas and gas-aerosol
 // productions, aerosol-aerosol loss, then per dependent element the gas
-// row's production and loss and the aerosol row's loss and production
+// row's production and loss and the aerosol row's loss and production; an
+// HL instance whose water a sub-model computes adds the gas and aerosol
+// rows against that water (src/rxns/rxn_HL_phase_transfer.c:383-404)
 __device__ __noinline__ void simpol_partials(const char* tb, const double* y, const double* keff,
-                                             double* part, int lane) {
+                                             const double* cv, double* part, int lane) {
   const Tab t = make_tab(tb);
   #pragma unroll 1
   for (int k = lane; k < t.n_simpol; k += 32) {
     const uint16_t* rec = t.si_rec + 8 * k;
     const double* c = keff + t.n_rxn + 8 * k;
-    const SimpolState s = simpol_state(t, k, y, keff);
+    const SimpolState s = simpol_state(t, k, y, keff, cv);
     double* p = part + rec[4];
     p[0] = s.N * c[0];
     p[1] = s.N * c[0] * s.inv_k;
     p[2] = s.N * s.evap_rate;
     p[3] = s.N * s.evap_rate * s.inv_k;
+    if (rec[5]) {
+      const double w = cv[rec[5] - 1];
+      p[4] = -ddiv(s.N * s.evap, w);
+      p[5] = ddiv(s.N * s.evap * s.inv_k, w);
+      continue;
+    }
     // d evap / d mass = -evap / m, d evap / d MW = evap / MW = evap mol / m
     const double dedm = -ddiv(s.evap, s.m);
     const double dedw = dedm * -s.mol;
@@ -372,8 +564,14 @@ __device__ __noinline__ void simpol_partials(const char* tb, const double* y, co
 // reverse rates from the per-cell constants (keff slots: forward, reverse,
 // with the constant species, water powers and activity coefficient folded
 // in) times (c m) of each dependent reactant or product slot.
+// A water or activity coefficient that a sub-model computes (rec[6], rec[7])
+// enters here: 1 / W per reactant and per product after the first, the
+// activity coefficient on the reverse rate, and no reaction below the
+// minimum water (keff slot + 2); so do computed reactants and products
+// (c m of each, rec[8], rec[9]).
 __device__ __forceinline__ void aq_fr(const Tab& t, const uint16_t* rec, const double* y,
-                                      const double* keff, double* rf, double* rr) {
+                                      const double* keff, const double* cv, double* rf,
+                                      double* rr) {
   const int S = rec[0], R = rec[1], s0 = rec[2];
   double f = keff[rec[5]], r = keff[rec[5] + 1];
   #pragma unroll 1
@@ -384,6 +582,28 @@ __device__ __forceinline__ void aq_fr(const Tab& t, const uint16_t* rec, const d
     else
       r *= v;
   }
+  #pragma unroll 1
+  for (int j = rec[8]; j < rec[8] + rec[9]; ++j) {
+    const double v = cv[t.aq_cp[j] & 0x7FFF] * t.aq_cpm[j];
+    if (t.aq_cp[j] & 0x8000)
+      f *= v;
+    else
+      r *= v;
+  }
+  const int wcv = rec[6] & 0xFF;
+  if (wcv) {
+    const double w = cv[wcv - 1];
+    if (w < keff[rec[5] + 2]) {
+      f = r = 0.0;
+    } else {
+      const int nr = (rec[6] >> 8) & 0xF, np = rec[6] >> 12;
+      #pragma unroll 1
+      for (int i = 1; i < nr; ++i) f = ddiv(f, w);
+      #pragma unroll 1
+      for (int i = 1; i < np; ++i) r = ddiv(r, w);
+    }
+  }
+  if (rec[7]) r *= cv[rec[7] - 1];
   *rf = f;
   *rr = r;
 }
@@ -392,14 +612,14 @@ __device__ __forceinline__ void aq_fr(const Tab& t, const uint16_t* rec, const d
 // rf / m and gains rr / m, a product the reverse; returns (warp-uniform)
 // whether any is negative
 __device__ __noinline__ bool aq_rates(const char* tb, const double* y, const double* keff,
-                                      double* rates, int lane) {
+                                      const double* cv, double* rates, int lane) {
   const Tab t = make_tab(tb);
   bool neg = false;
   #pragma unroll 1
   for (int q = lane; q < t.n_aq; q += 32) {
-    const uint16_t* rec = t.aq_rec + 8 * q;
+    const uint16_t* rec = t.aq_rec + 12 * q;
     double rf, rr;
-    aq_fr(t, rec, y, keff, &rf, &rr);
+    aq_fr(t, rec, y, keff, cv, &rf, &rr);
     const int S = rec[0], R = rec[1], s0 = rec[2];
     double* r = rates + rec[3];
     #pragma unroll 1
@@ -415,15 +635,18 @@ __device__ __noinline__ bool aq_rates(const char* tb, const double* y, const dou
 
 // partials: independent slot a (rate rf for a reactant, rr for a product,
 // divided by its concentration), row slot k (divided by its m); zero when
-// the rate is zero, as the reference skips those
+// the rate is zero, as the reference skips those.  Then, for a water a
+// sub-model computes, each row slot against it, and for a computed
+// activity coefficient each row slot against that
+// (src/rxns/rxn_aqueous_equilibrium.c:486-537).
 __device__ __noinline__ void aq_partials(const char* tb, const double* y, const double* keff,
-                                         double* part, int lane) {
+                                         const double* cv, double* part, int lane) {
   const Tab t = make_tab(tb);
   #pragma unroll 1
   for (int q = lane; q < t.n_aq; q += 32) {
-    const uint16_t* rec = t.aq_rec + 8 * q;
+    const uint16_t* rec = t.aq_rec + 12 * q;
     double rf, rr;
-    aq_fr(t, rec, y, keff, &rf, &rr);
+    aq_fr(t, rec, y, keff, cv, &rf, &rr);
     const int S = rec[0], R = rec[1], s0 = rec[2];
     double* p = part + rec[4];
     #pragma unroll 1
@@ -434,6 +657,42 @@ __device__ __noinline__ void aq_partials(const char* tb, const double* y, const 
       for (int k = 0; k < S; ++k)
         p[a * S + k] = rate != 0.0 ? ddiv(ddiv(rate, ca), t.aq_sm[s0 + k]) : 0.0;
     }
+    p += S * S;
+    const int wcv = rec[6] & 0xFF;
+    if (wcv) {
+      // d rate_f / d W = -(n_r - 1) rate_f / W, likewise the reverse
+      const double w = cv[wcv - 1];
+      const int nr = (rec[6] >> 8) & 0xF, np = rec[6] >> 12;
+      const double dfw = ddiv(rf * (nr - 1), w), drw = ddiv(rr * (np - 1), w);
+      #pragma unroll 1
+      for (int k = 0; k < S; ++k) {
+        const double m = t.aq_sm[s0 + k];
+        p[k] = k < R ? ddiv(dfw - drw, m) : ddiv(drw - dfw, m);
+      }
+      p += S;
+    }
+    if (rec[7]) {
+      const double dg = ddiv(rr, cv[rec[7] - 1]);
+      #pragma unroll 1
+      for (int k = 0; k < S; ++k) {
+        const double v = ddiv(dg, t.aq_sm[s0 + k]);
+        p[k] = k < R ? v : -v;
+      }
+      p += S;
+    }
+    // computed reactants / products as independent species: a loss where
+    // the participant and the row are both reactants or both products
+    #pragma unroll 1
+    for (int j = rec[8]; j < rec[8] + rec[9]; ++j, p += S) {
+      const bool jr = (t.aq_cp[j] & 0x8000) != 0;
+      const double rate = jr ? rf : rr;
+      const double ca = cv[t.aq_cp[j] & 0x7FFF];
+      #pragma unroll 1
+      for (int k = 0; k < S; ++k) {
+        const double v = rate != 0.0 ? ddiv(ddiv(rate, ca), t.aq_sm[s0 + k]) : 0.0;
+        p[k] = jr == (k < R) ? -v : v;
+      }
+    }
   }
 }
 
@@ -441,14 +700,14 @@ __device__ __noinline__ void aq_partials(const char* tb, const double* y, const 
 // single call site each (the solve kernel's register allocation follows
 // them).
 __device__ __noinline__ bool aero_rates(const char* tb, const double* y, const double* keff,
-                                        double* rates, int lane) {
-  const bool neg = simpol_rates(tb, y, keff, rates, lane);
-  return aq_rates(tb, y, keff, rates, lane) || neg;
+                                        const double* cv, double* rates, int lane) {
+  const bool neg = simpol_rates(tb, y, keff, cv, rates, lane);
+  return aq_rates(tb, y, keff, cv, rates, lane) || neg;
 }
 __device__ __noinline__ void aero_partials(const char* tb, const double* y, const double* keff,
-                                           double* part, int lane) {
-  simpol_partials(tb, y, keff, part, lane);
-  aq_partials(tb, y, keff, part, lane);
+                                           const double* cv, double* part, int lane) {
+  simpol_partials(tb, y, keff, cv, part, lane);
+  aq_partials(tb, y, keff, cv, part, lane);
 }
 
 // Returns 1 (recoverable) when some y < -SMALL, else writes f into out.
@@ -645,23 +904,62 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
 // not write, made visible to the gathers by their warp barrier), then the
 // usual evaluation.  Separate functions, so that the plain f and J keep
 // their register use.
+//
+// With sub-models, their computed species come first (after the pseudo-rates
+// in the f scratch, after the partials in the J scratch), then for J the
+// parameter Jacobian P and the virtual slots V (rate partials against the
+// computed species), which the chain folds into the solver slots:
+// J[row][j] += V[row][c] * P[c][j] (src/camp_solver.c:1063-1106).  The
+// production / loss split jp / jl, where asked for, leaves the chained terms
+// out.
 __device__ __noinline__ int dev_f_aero(const char* tb, const double* y, double h,
                                        const double* keff, double* rates, double* fscr,
                                        double* out, int lane, double* rp = nullptr,
                                        double* rl = nullptr) {
-  const bool neg = aero_rates(tb, y, keff, rates, lane);
+  const BlobOff& o = *reinterpret_cast<const BlobOff*>(tb);
+  double* cv = rates + o.n_rates;
+  if (o.n_cv > 0) sub_model_eval(tb, y, keff, cv, nullptr, lane);
+  const bool neg = aero_rates(tb, y, keff, cv, rates, lane);
   return dev_f(tb, y, h, keff, rates, fscr, out, lane, rp, rl, neg);
 }
 template <typename JT>
 __device__ __noinline__ int dev_jac_aero(const char* tb, const double* y, double h,
                                          const double* keff, double* part, JT* Jout, int lane,
                                          double* jp = nullptr, double* jl = nullptr) {
-  aero_partials(tb, y, keff, part, lane);
-  return dev_jac<JT>(tb, y, h, keff, part, Jout, lane, jp, jl);
+  const BlobOff& o = *reinterpret_cast<const BlobOff*>(tb);
+  double* cv = part + o.n_part_all;
+  double* P = cv + o.n_cv;
+  double* V = P + o.n_pj;
+  if (o.n_cv > 0) sub_model_eval(tb, y, keff, cv, P, lane);
+  aero_partials(tb, y, keff, cv, part, lane);
+  const int r = dev_jac<JT>(tb, y, h, keff, part, Jout, lane, jp, jl);
+  if (r != 0 || o.n_chain == 0) return r;
+  const uint16_t* vptr = (const uint16_t*)(tb + o.jv_ptr);
+  const uint16_t* vpart = (const uint16_t*)(tb + o.jv_part);
+  #pragma unroll 1
+  for (int v = lane; v < o.n_virt; v += 32) {
+    double s = 0.0;
+    #pragma unroll 1
+    for (int g = vptr[v]; g < vptr[v + 1]; ++g) s += part[vpart[g]];
+    V[v] = s;
+  }
+  __syncwarp();
+  const uint16_t* tgt = (const uint16_t*)(tb + o.ch_tgt);
+  const uint16_t* cptr = (const uint16_t*)(tb + o.ch_ptr);
+  const uint32_t* ent = (const uint32_t*)(tb + o.ch_ent);
+  #pragma unroll 1
+  for (int g = lane; g < o.n_chain; g += 32) {
+    double s = (double)Jout[tgt[g]];
+    #pragma unroll 1
+    for (int e = cptr[g]; e < cptr[g + 1]; ++e) s += V[ent[e] & 0xFFFFu] * P[ent[e] >> 16];
+    Jout[tgt[g]] = (JT)s;
+  }
+  __syncwarp();
+  return 0;
 }
 __device__ __forceinline__ bool has_simpol(const char* tb) {
   const BlobOff* o = reinterpret_cast<const BlobOff*>(tb);
-  return o->n_simpol > 0 || o->n_aq > 0;
+  return o->n_simpol > 0 || o->n_aq > 0 || o->n_cv > 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -870,12 +1168,11 @@ __device__ __noinline__ void dev_lsolve_seq(const char* tb, const LT* LU, const 
 // ---------------------------------------------------------------------------
 // BDF integrator state of one cell (warp-uniform scalars)
 // ---------------------------------------------------------------------------
-template <typename LT>
+template <typename LT, bool AERO>
 struct Cell {
   const char* tb;     // shared-memory tables
   const double* atol;
   int lu_mode;        // 0 = level schedule over the lanes, 1 = one lane
-  bool aero;          // the mechanism has SIMPOL instances
   int lane, n;
   double* zb;  // Nordsieck history: column j at zb + j*n
   double *ewt, *acor, *y, *ftemp, *tempv, *rates, *keff, *fscr;
@@ -901,8 +1198,10 @@ struct Cell {
     return dsqrt(ddiv(warp_sum(s), (double)n));
   }
   __device__ int f(const double* yy, double* out) {
-    return aero ? dev_f_aero(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane)
-                : dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
+    if constexpr (AERO)
+      return dev_f_aero(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
+    else
+      return dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
   }
   __device__ bool set_ewt(const double* yy) {
     bool bad = false;
@@ -1081,9 +1380,12 @@ struct Cell {
       nje++;
       nstlj = nst;
       jcur = 1;
-      if (aero ? dev_jac_aero<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane)
-               : dev_jac<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane))
-        return 1;
+      int jr;
+      if constexpr (AERO)
+        jr = dev_jac_aero<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane);
+      else
+        jr = dev_jac<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane);
+      if (jr) return 1;
     }
     const bool ok = lu_mode ? dev_form_factor_seq<LT>(tb, J, gamma, LU, dinv, lane)
                             : dev_form_factor<LT>(tb, J, gamma, LU, dinv, lane);
@@ -1438,11 +1740,10 @@ struct Cell {
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
-template <typename LT>
-__device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char* base,
+template <typename LT, bool AERO>
+__device__ void bind_cell(Cell<LT, AERO>& c, const SolveArgs& a, const char* tab, char* base,
                           int gwarp, int lane) {
   c.tb = tab;
-  c.aero = has_simpol(tab);
   c.atol = make_tab(tab).atol;
   c.lane = lane;
   c.n = a.off.n;
@@ -1474,8 +1775,12 @@ __device__ void bind_cell(Cell<LT>& c, const SolveArgs& a, const char* tab, char
   c.lu_mode = a.lu_mode;
 }
 
-template <typename LT>
-__global__ void __launch_bounds__(32 * kMaxCellsPerBlock, 1) solve_kernel(SolveArgs a) {
+// AERO: the mechanism has SIMPOL, HL, aqueous equilibrium or sub-models,
+// whose out-of-line evaluations take registers that the gas-phase form keeps
+// for itself; that form runs fewer cells per block.
+template <typename LT, bool AERO>
+__global__ void __launch_bounds__(32 * (AERO ? kMaxCellsAero : kMaxCellsPerBlock), 1)
+    solve_kernel(SolveArgs a) {
   extern __shared__ __align__(16) char smem[];
   __shared__ unsigned long long tma_bar;
   if (!stage_tables(smem, a.blob, a.stage_bytes, &tma_bar, a.err)) return;
@@ -1483,8 +1788,8 @@ __global__ void __launch_bounds__(32 * kMaxCellsPerBlock, 1) solve_kernel(SolveA
   const int wib = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * (blockDim.x >> 5) + wib;
   char* base = smem + a.tab_bytes + (size_t)wib * a.lay.bytes;
-  Cell<LT> c;
-  bind_cell<LT>(c, a, smem, base, gwarp, lane);
+  Cell<LT, AERO> c;
+  bind_cell<LT, AERO>(c, a, smem, base, gwarp, lane);
   const DevMech& m = a.m;
   const uint16_t* dep_state = make_tab(smem).dep_state;
   #pragma unroll 1
@@ -1841,8 +2146,8 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   m.n_const = (int)cst.size();
   // SIMPOL instances (device-side constants; see rates.cuh)
   std::vector<double> si_prm, si_dp, si_cinv_rho, si_cinv_mw, si_cin;
-  std::vector<int> si_type, si_kind, si_gmd, si_gsd, si_act, si_water, si_nph, si_cptr(1, 0),
-      si_cidx;
+  std::vector<int> si_type, si_kind, si_gmd, si_gsd, si_act, si_water, si_wcv, si_nph,
+      si_cptr(1, 0), si_cidx;
   for (const SimpolInst& si : t.simpol) {
     si_prm.insert(si_prm.end(), si.prm, si.prm + 10);
     si_type.push_back(si.type);
@@ -1852,6 +2157,7 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
     si_dp.push_back(si.bin_dp);
     si_act.push_back(si.act);
     si_water.push_back(si.water);
+    si_wcv.push_back(si.water_cv);
     si_nph.push_back(si.n_phases);
     const size_t ne = si.type == RXN_SIMPOL_PHASE_TRANSFER ? si.elem.size() : 0;
     for (size_t j = 0; j < ne; ++j) {
@@ -1869,11 +2175,14 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   std::vector<int> aq_int, aq_cptr(1, 0), aq_cidx, aq_cr;
   for (const AqInst& q : t.aq) {
     aq_prm.insert(aq_prm.end(), {q.A, q.C, q.kr, q.thr});
-    aq_int.insert(aq_int.end(), {q.water, q.act, (int)q.react.size(), (int)q.prod.size()});
+    aq_int.insert(aq_int.end(), {q.water, q.act, (int)q.react.size(), (int)q.prod.size(),
+                                 q.water_cv, q.act_cv});
     for (int pass = 0; pass < 2; ++pass) {
       const std::vector<int>& list = pass == 0 ? q.react : q.prod;
       for (size_t i = 0; i < list.size(); ++i) {
         if (model.var_type()[list[i]] == VAR_VARIABLE) continue;
+        if (std::find(q.cp_state.begin(), q.cp_state.end(), list[i]) != q.cp_state.end())
+          continue;  // computed by a sub-model: applied per evaluation
         aq_cidx.push_back(list[i]);
         aq_cm.push_back(q.m2m[(pass == 0 ? 0 : q.react.size()) + i]);
         aq_cr.push_back(pass == 0 ? 1 : 0);
@@ -1882,6 +2191,7 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
     aq_cptr.push_back((int)aq_cidx.size());
   }
   m.n_aq = t.n_aq;
+  m.sm_keff = t.sm_keff;
   Packer pk;
   pk.add(aq_prm, &m.aq_prm);
   pk.add(aq_cm, &m.aq_cm);
@@ -1896,6 +2206,7 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   pk.add(si_gsd, &m.si_gsd_col);
   pk.add(si_act, &m.si_act);
   pk.add(si_water, &m.si_water);
+  pk.add(si_wcv, &m.si_wcv);
   pk.add(si_nph, &m.si_nph);
   pk.add(si_cptr, &m.si_cptr);
   pk.add(si_cidx, &m.si_cidx);
@@ -1994,7 +2305,10 @@ static Layout make_layout(const BlobOff& o, int lt_size, bool with_hist,
   L.y = take(vec);
   L.ftemp = take(vec);
   L.tempv = take(vec);
-  L.rates = take(sizeof(double) * std::max(o.n_rates, o.n_part_all));
+  // the f scratch (pseudo-rates, then the computed species) and the J
+  // scratch (partials, computed species, parameter partials, virtual slots)
+  L.rates = take(sizeof(double) * std::max(o.n_rates + o.n_cv,
+                                           o.n_part_all + o.n_cv + o.n_pj + o.n_virt));
   L.keff = keff_in_smem ? take(sizeof(double) * o.n_keff) : -1;
   L.fscr = take(sizeof(double) * 2 * std::max(1, o.n_fscratch));
   // one spare slot each: the target of the grouped phases' no-op records
@@ -2018,6 +2332,18 @@ static int tab_bytes_of(const BlobOff& o, int lu_mode) {
 
 // Geometry and launch of the warp-per-cell kernel shared by the solver's own
 // launches and the serving slots.  Scratch pointers come from the caller.
+// the solve kernel's form for a mechanism: aerosol reactions or sub-models
+// take the AERO instance (fewer cells per block, see solve_kernel)
+static bool aero_form(const BlobOff& o) { return o.n_simpol > 0 || o.n_aq > 0 || o.n_cv > 0; }
+static int max_cells_of(const BlobOff& o) {
+  return aero_form(o) ? kMaxCellsAero : kMaxCellsPerBlock;
+}
+static void* solve_kernel_fn(const BlobOff& o, int precision) {
+  if (aero_form(o))
+    return precision == 1 ? (void*)solve_kernel<float, true> : (void*)solve_kernel<double, true>;
+  return precision == 1 ? (void*)solve_kernel<float, false> : (void*)solve_kernel<double, false>;
+}
+
 struct WarpLaunch {
   int grid = 0, warps = 0, tab = 0, lt = 8;
   Layout lay{};
@@ -2037,7 +2363,7 @@ static bool plan_warp_launch(const BlobOff& off, int sm_count, int max_smem,
     return false;
   }
   int warps = s.warps_per_block > 0 ? std::min(s.warps_per_block, max_warps) : max_warps;
-  warps = std::min(warps, kMaxCellsPerBlock);
+  warps = std::min(warps, max_cells_of(off));
   int bps = std::max(1, s.blocks_per_sm);
   while (bps > 1 && (size_t)bps * (w->tab + warps * w->lay.bytes) > (size_t)max_smem) --bps;
   int grid = std::min(sm_count * bps, std::max(1, max_blocks));
@@ -2058,16 +2384,10 @@ static int hist_stride_of(const BlobOff& off, const SolveSettings& s) {
 
 static bool launch_warp_kernel(SolveArgs& a, const WarpLaunch& w, int precision,
                                cudaStream_t st, std::string* err) {
-  if (precision == 1) {
-    CK(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)w.smem));
-    solve_kernel<float><<<w.grid, w.warps * 32, w.smem, st>>>(a);
-  } else {
-    CK(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)w.smem));
-    solve_kernel<double><<<w.grid, w.warps * 32, w.smem, st>>>(a);
-  }
-  CK(cudaGetLastError());
+  void* func = solve_kernel_fn(a.off, precision);
+  CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.smem));
+  void* args[] = {&a};
+  CK(cudaLaunchKernel(func, dim3(w.grid), dim3(w.warps * 32), args, w.smem, st));
   return true;
 }
 
@@ -2154,7 +2474,7 @@ bool Engine::launch_graph(SolveArgs& a, const WarpLaunch& w, int precision, void
                           std::string* err) {
   Impl* I = impl_;
   cudaStream_t st = (cudaStream_t)stream;
-  void* func = precision == 1 ? (void*)solve_kernel<float> : (void*)solve_kernel<double>;
+  void* func = solve_kernel_fn(a.off, precision);
   CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.smem));
   void* args[] = {&a};
   cudaKernelNodeParams kp{};
@@ -2267,7 +2587,7 @@ int Engine::max_cells_per_block(const SolveSettings& s) const {
   if (s.kernel != 0 || !I->warp_ok) return 0;
   const int lt = s.precision == 1 ? 4 : 8;
   const Layout lay = make_layout(I->off, lt, s.hist_global == 0, true);
-  return std::min(kMaxCellsPerBlock,
+  return std::min(max_cells_of(I->off),
                   std::max(0, (I->max_smem - tab_bytes_of(I->off, s.lu_mode)) / lay.bytes));
 }
 
@@ -2532,10 +2852,7 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 // name g_static_scratch is only a stand-in, so the address is looked up once
 // per device (with that device current) and kept for the life of the
 // process; a caller that resets a device's primary context (cudaDeviceReset)
-// must not use this path on that device afterwards.  The kernels' dynamic
-// shared-memory limit is raised once per device and precision, to the most
-// any launch of this path needs (the table blob plus the largest slab set).
-static int g_static_smem_set[64][2] = {};
+// must not use this path on that device afterwards.
 
 static bool static_scratch_address(char** out, std::string* err) {
   static std::mutex mu;
@@ -2578,7 +2895,7 @@ bool Engine::run_solve_static(double* d_state, const double* d_env, const double
     return false;
   }
   if (s.warps_per_block > 0) warps = std::min(warps, s.warps_per_block);
-  warps = std::min(warps, kMaxCellsPerBlock);
+  warps = std::min(warps, max_cells_of(I->off));
   // one resident cell keeps n_jac Jacobian values (the kernel indexes them
   // by warp); the static array bounds the number of resident cells
   const size_t per_warp = (size_t)lt * I->m.n_jac;
@@ -2623,26 +2940,13 @@ bool Engine::run_solve_static(double* d_state, const double* d_env, const double
   a.maxnef = s.max_conv_fails;
   a.lu_mode = s.lu_mode;
   const size_t smem = (size_t)tab + (size_t)warps * lay.bytes;
-  {
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    int& set = g_static_smem_set[dev][s.precision == 1 ? 1 : 0];
-    if ((int)smem > set) {
-      const int lim = I->max_smem;  // the device's opt-in maximum per block
-      if (s.precision == 1)
-        CK(cudaFuncSetAttribute(solve_kernel<float>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-      else
-        CK(cudaFuncSetAttribute(solve_kernel<double>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-      set = lim;
-    }
-  }
-  if (s.precision == 1)
-    solve_kernel<float><<<grid, warps * 32, smem, st>>>(a);
-  else
-    solve_kernel<double><<<grid, warps * 32, smem, st>>>(a);
-  CK(cudaGetLastError());
+  // set on every call: the regular entry points set the same kernel's limit
+  // to their own launch's size
+  CK(cudaFuncSetAttribute(solve_kernel_fn(I->off, s.precision),
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  void* args[] = {&a};
+  CK(cudaLaunchKernel(solve_kernel_fn(I->off, s.precision), dim3(grid), dim3(warps * 32), args,
+                      smem, st));
   ++launches_;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st));

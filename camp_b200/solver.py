@@ -43,7 +43,7 @@ class Solver:
         self._h = self.lib.solver_new(
             mech.n_state_var, self.n_cells, np.ascontiguousarray(mech.var_type, np.int32),
             mech.n_rxn, mech.n_rxn_int_param, mech.n_rxn_float_param, mech.n_rxn_env_param,
-            *mech.aero_sizes(), 0, 0, 0, 0,
+            *mech.aero_sizes(), *mech.sub_sizes(),
         )
         if not self._h:
             raise SolverError(_lib.last_error())
@@ -63,6 +63,12 @@ class Solver:
             self.lib.aero_rep_add_condensed_data(
                 a.rep_type, a.ints.size, a.floats.size, a.n_env,
                 np.ascontiguousarray(a.ints, np.int32), np.ascontiguousarray(a.floats, np.float64),
+                self._h)
+        # sub-models in priority order (src/camp_solver_data.F90:700-720)
+        for sm in mech.sub_models:
+            self.lib.sub_model_add_condensed_data(
+                sm.sub_type, sm.ints.size, sm.floats.size, sm.n_env,
+                np.ascontiguousarray(sm.ints, np.int32), np.ascontiguousarray(sm.floats, np.float64),
                 self._h)
         self.ready = False
 
@@ -298,6 +304,16 @@ class Solver:
         out = np.zeros(self.lib.camp_b200_rxn_int_data_size(self._h), np.int32)
         self.lib.camp_b200_get_rxn_int_data(self._h, out)
         return out
+
+    def jac_map(self) -> np.ndarray:
+        """The solver-Jacobian fold as (solver id, reaction-Jacobian id,
+        parameter id) rows."""
+        n = self.lib.camp_b200_n_mapped_values(self._h)
+        if n < 0:
+            raise SolverError("sparsity not built")
+        out = np.zeros(3 * max(n, 1), np.int32)
+        self.lib.camp_b200_get_jac_map(self._h, out)
+        return out[: 3 * n].reshape(n, 3)
 
     def lu_order(self) -> np.ndarray:
         out = np.zeros(self.lib.camp_b200_n_dep_var(self._h), np.int32)

@@ -292,6 +292,13 @@ int camp_b200_rxn_int_data_size(void *solver_data);
 int camp_b200_get_solver_jac(void *solver_data, int *col_ptrs, int *row_ids);
 int camp_b200_get_rxn_int_data(void *solver_data, int *out);
 int camp_b200_get_lu_order(void *solver_data, int *perm);
+/* The solver-Jacobian fold J_solver[s] += J_rxn[r] * J_params[p] as (s, r,
+ * p) triplets in the reference's order (src/camp_solver.c:1649-1681; p = 0
+ * is the unit parameter, the others the sub-model parameter Jacobian's
+ * elements): camp_b200_n_mapped_values() triplets, or -1 before
+ * solver_initialize. */
+int camp_b200_n_mapped_values(void *solver_data);
+int camp_b200_get_jac_map(void *solver_data, int *triplets);
 
 /* Device evaluation of the derivative and Jacobian for n_cells states (host
  * buffers), through the same device code the solver uses: rate constants

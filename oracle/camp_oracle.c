@@ -28,6 +28,10 @@
 #define T_HL 6
 #define T_AQ 7
 
+/* sub-model type ids, src/sub_model_solver.c:16-18 */
+#define SM_ZSR_AEROSOL_WATER 2
+#define SM_PDFITE 3
+
 /* types whose packed data is not the NUM_REACT_/NUM_PROD_ layout */
 static int species_rate_type(int t) {
   return t == T_FIRST_ORDER_LOSS || t == T_EMISSION || t == T_WET_DEPOSITION;
@@ -102,6 +106,21 @@ struct OracleMech {
   double *aph_flt;
   int *arep_int, *arep_ioff, *arep_foff, *arep_eoff, *arep_type, arep_ilen, arep_flen;
   double *arep_flt;
+  /* sub-models as sub_model_add_condensed_data receives them (ints after
+   * the type slot; the JAC ids in them are written at om_build); a cell's
+   * sub-model env parameters follow the representation's in rxn_env */
+  int n_sub, n_sub_env;
+  int *sub_type, *sub_ioff, *sub_foff, *sub_eoff, sub_ilen, sub_flen;
+  int *sub_int;
+  double *sub_flt;
+  /* sub-model parameter Jacobian (src/camp_solver.c:1520-1550): CSC over
+   * state variables with the dummy element (0, 0) first */
+  int n_param_jac;
+  int *pj_colptr, *pj_rowid;
+  /* solver Jacobian fold J_solver[s] += J_rxn[r] * J_params[p]
+   * (src/camp_solver.c:1636-1681) */
+  int n_map;
+  int *map_s, *map_r, *map_p;
   /* experiment switches (om_set_experiment); zero = the reference's semantics
    * and this oracle's positivity rule */
   double guard_step;
@@ -152,6 +171,31 @@ int om_add_rxn(OracleMech *m, int type, int n_int, int n_float, int n_env,
   m->float_size += n_float;
   m->n_env += n_env;
   m->n_added++;
+  return 0;
+}
+
+/* sub_model_add_condensed_data (src/sub_model_solver.c:425-470): the packed
+ * ints (after the type) and floats of one sub-model, in priority order */
+int om_add_sub_model(OracleMech *m, int type, int n_int, int n_float, int n_env,
+                     const int *ints, const double *floats) {
+  if (type != SM_ZSR_AEROSOL_WATER && type != SM_PDFITE) return 2;
+  const int k = m->n_sub;
+  m->sub_type = (int *)realloc(m->sub_type, sizeof(int) * (k + 1));
+  m->sub_ioff = (int *)realloc(m->sub_ioff, sizeof(int) * (k + 1));
+  m->sub_foff = (int *)realloc(m->sub_foff, sizeof(int) * (k + 1));
+  m->sub_eoff = (int *)realloc(m->sub_eoff, sizeof(int) * (k + 1));
+  m->sub_int = (int *)realloc(m->sub_int, sizeof(int) * (m->sub_ilen + n_int + 1));
+  m->sub_flt = (double *)realloc(m->sub_flt, sizeof(double) * (m->sub_flen + n_float + 1));
+  m->sub_type[k] = type;
+  m->sub_ioff[k] = m->sub_ilen;
+  m->sub_foff[k] = m->sub_flen;
+  m->sub_eoff[k] = m->n_sub_env;
+  memcpy(m->sub_int + m->sub_ilen, ints, sizeof(int) * n_int);
+  memcpy(m->sub_flt + m->sub_flen, floats, sizeof(double) * n_float);
+  m->sub_ilen += n_int;
+  m->sub_flen += n_float;
+  m->n_sub_env += n_env;
+  m->n_sub = k + 1;
   return 0;
 }
 
@@ -597,6 +641,367 @@ static int jr_elem_id(const int *colptr, const int *rowid, int dep, int ind) {
   return -1;
 }
 
+/* --- sub-models: ZSR aerosol water and PD-FiTE activity ----------------- */
+/* Packed layouts (ints after the type slot) of
+ * src/sub_models/sub_model_ZSR_aerosol_water.c:27-71 and
+ * src/sub_models/sub_model_PDFiTE.c:21-64; both start with NUM_PHASE,
+ * GAS_WATER_ID (1-based), NUM_ION_PAIR, INT_DATA_SIZE, FLOAT_DATA_SIZE, then
+ * the phase water / first-species ids (1-based) and the per-ion-pair int and
+ * float locations (1-based).  Species ids of an ion pair are relative to the
+ * phase's first state id. */
+typedef struct {
+  int *I;
+  const double *F;
+  int np, gw, npair;
+} SubV;
+
+static SubV subv(const OracleMech *m, int k) {
+  SubV s;
+  s.I = m->sub_int + m->sub_ioff[k];
+  s.F = m->sub_flt + m->sub_foff[k];
+  s.np = s.I[0];
+  s.gw = s.I[1] - 1;
+  s.npair = s.I[2];
+  return s;
+}
+static int sv_phase(SubV s, int p) { return s.I[5 + p] - 1; }
+static int sv_il(SubV s, int x) { return s.I[5 + s.np + x] - 1; }
+static int sv_fl(SubV s, int x) { return s.I[5 + s.np + s.npair + x] - 1; }
+/* ZSR, per ion pair: type 1 = Jacobson et al. (1996), 2 = EQSAM */
+#define ZSR_JACOBSON 1
+#define ZSR_EQSAM 2
+static int zsr_type(SubV s, int x) { return s.I[sv_il(s, x)]; }
+static int zj_ncat(SubV s, int x) { return s.I[sv_il(s, x) + 1]; }
+static int zj_nan(SubV s, int x) { return s.I[sv_il(s, x) + 2]; }
+static int zj_cat(SubV s, int x) { return s.I[sv_il(s, x) + 3]; }
+static int zj_an(SubV s, int x) { return s.I[sv_il(s, x) + 4]; }
+static int zj_ny(SubV s, int x) { return s.I[sv_il(s, x) + 5]; }
+static int *zj_gw_jac(SubV s, int p, int x) { return &s.I[sv_il(s, x) + 6 + p]; }
+static int *zj_cat_jac(SubV s, int p, int x) { return &s.I[sv_il(s, x) + 6 + s.np + p]; }
+static int *zj_an_jac(SubV s, int p, int x) { return &s.I[sv_il(s, x) + 6 + 2 * s.np + p]; }
+static double zj_low_rh(SubV s, int x) { return s.F[sv_fl(s, x)]; }
+static double zj_cat_mw(SubV s, int x) { return s.F[sv_fl(s, x) + 1]; }
+static double zj_an_mw(SubV s, int x) { return s.F[sv_fl(s, x) + 2]; }
+static double zj_y(SubV s, int x, int k) { return s.F[sv_fl(s, x) + 3 + k]; }
+static int ze_nion(SubV s, int x) { return s.I[sv_il(s, x) + 1]; }
+static int *ze_gw_jac(SubV s, int p, int x) { return &s.I[sv_il(s, x) + 2 + p]; }
+static int ze_ion(SubV s, int x, int k) { return s.I[sv_il(s, x) + 2 + s.np + k]; }
+static int *ze_ion_jac(SubV s, int p, int x, int k) {
+  return &s.I[sv_il(s, x) + 2 + s.np + ze_nion(s, x) + k * s.np + p];
+}
+static double ze_nw(SubV s, int x) { return s.F[sv_fl(s, x)]; }
+static double ze_zw(SubV s, int x) { return s.F[sv_fl(s, x) + 1]; }
+static double ze_pair_mw(SubV s, int x) { return s.F[sv_fl(s, x) + 2]; }
+static double ze_ion_mw(SubV s, int x, int k) { return s.F[sv_fl(s, x) + 3 + k]; }
+/* PD-FiTE, per ion pair */
+static int pd_act(SubV s, int x) { return s.I[sv_il(s, x)]; }
+static int pd_ncat(SubV s, int x) { return s.I[sv_il(s, x) + 1]; }
+static int pd_nan(SubV s, int x) { return s.I[sv_il(s, x) + 2]; }
+static int pd_cat(SubV s, int x) { return s.I[sv_il(s, x) + 3]; }
+static int pd_an(SubV s, int x) { return s.I[sv_il(s, x) + 4]; }
+static int pd_ninter(SubV s, int x) { return s.I[sv_il(s, x) + 5]; }
+static int *pd_w_jac(SubV s, int p, int x) { return &s.I[sv_il(s, x) + 6 + p]; }
+static int *pd_cat_jac(SubV s, int p, int x, int y) {
+  return &s.I[sv_il(s, x) + 6 + s.np + p * s.npair + y];
+}
+static int *pd_an_jac(SubV s, int p, int x, int y) {
+  return &s.I[sv_il(s, x) + 6 + (1 + s.npair) * s.np + p * s.npair + y];
+}
+static int pd_nb(SubV s, int x, int y) {
+  return s.I[sv_il(s, x) + 6 + (1 + 2 * s.npair) * s.np + y];
+}
+static int pd_inter_pair(SubV s, int x, int y) {
+  return s.I[sv_il(s, x) + 6 + (1 + 2 * s.npair) * s.np + pd_ninter(s, x) + y] - 1;
+}
+static int pd_inter_loc(SubV s, int x, int y) {
+  return s.I[sv_il(s, x) + 6 + (1 + 2 * s.npair) * s.np + 2 * pd_ninter(s, x) + y] - 1;
+}
+static double pd_cat_mw(SubV s, int x) { return s.F[sv_fl(s, x)]; }
+static double pd_an_mw(SubV s, int x) { return s.F[sv_fl(s, x) + 1]; }
+static double pd_min_rh(SubV s, int x, int y) { return s.F[pd_inter_loc(s, x, y)]; }
+static double pd_max_rh(SubV s, int x, int y) { return s.F[pd_inter_loc(s, x, y) + 1]; }
+static double pd_b(SubV s, int x, int y, int z) { return s.F[pd_inter_loc(s, x, y) + 2 + z]; }
+/* an interaction applies in (min RH, max RH], or [0, max RH] at a_w = 0
+ * (src/sub_models/sub_model_PDFiTE.c:218-224) */
+static int pd_in_range(SubV s, int x, int y, double a_w) {
+  const double lo = pd_min_rh(s, x, y), hi = pd_max_rh(s, x, y);
+  return !((a_w <= lo || a_w > hi) && !(a_w <= 0.0 && lo <= 0.0));
+}
+
+static const double *sub_env(const OracleMech *m, const double *rxn_env, int k) {
+  return rxn_env + m->n_env + m->n_aero_env + m->sub_eoff[k];
+}
+
+/* PPM_TO_RH_ from T and P, the MOSAIC water vapour pressure fit
+ * (src/sub_models/sub_model_ZSR_aerosol_water.c:198-214; the PD-FiTE
+ * sub-model computes the same) */
+static double ppm_to_rh(double T, double P) {
+  double a = 1.0 - 373.15 / T;
+  a = (((-0.1299 * a - 0.6445) * a - 1.976) * a + 13.3185) * a;
+  const double water_vp = 101325.0 * exp(a);
+  return P / water_vp / 1.0e6;
+}
+
+/* Jacobson molality polynomial value (squared in the water sum) and its
+ * derivative in a_w */
+static void zsr_calc(SubV s, const double *e, double *state) {
+  const long double a_w = e[0] * state[s.gw];
+  for (int p = 0; p < s.np; ++p) {
+    const int w = sv_phase(s, p);
+    long double water = 1.0e-30L; /* MINIMUM_WATER_MASS_ */
+    for (int x = 0; x < s.npair; ++x) {
+      if (zsr_type(s, x) == ZSR_JACOBSON) {
+        const long double j_aw = a_w > zj_low_rh(s, x) ? a_w : zj_low_rh(s, x);
+        long double molal = 0.0;
+        for (int k = 0; k < zj_ny(s, x); ++k) molal += zj_y(s, x, k) * pow((double)j_aw, k);
+        molal *= molal;
+        const long double cat = state[w + zj_cat(s, x)] / zj_ncat(s, x) / zj_cat_mw(s, x) / 1000.0;
+        const long double an = state[w + zj_an(s, x)] / zj_nan(s, x) / zj_an_mw(s, x) / 1000.0;
+        /* smooth minimum of the two ion concentrations, alpha = -100 */
+        const long double ec = exp((double)(-100.0 * cat)), ea = exp((double)(-100.0 * an));
+        const long double conc = (cat * ec + an * ea) / (ec + ea);
+        water += conc / molal * 1000.0;
+      } else if (zsr_type(s, x) == ZSR_EQSAM) {
+        long double e_aw = a_w > 0.99 ? 0.99 : a_w;
+        e_aw = e_aw < 0.001 ? 0.001 : e_aw;
+        long double molal =
+            ze_nw(s, x) * 55.51 * 18.01 / ze_pair_mw(s, x) / 1000.0 * (1.0 / e_aw - 1.0);
+        molal = pow((double)molal, ze_zw(s, x));
+        for (int k = 0; k < ze_nion(s, x); ++k) {
+          long double c = state[w + ze_ion(s, x, k)];
+          c = c > 0.0 ? c : 0.0;
+          water += c / ze_ion_mw(s, x, k) / molal;
+        }
+      }
+    }
+    state[w] = (double)water;
+  }
+}
+
+/* src/sub_models/sub_model_ZSR_aerosol_water.c:318-437 */
+static void zsr_jac(SubV s, const double *e, const double *state, double *JP) {
+  const long double a_w = e[0] * state[s.gw];
+  const long double daw = e[0];
+  for (int p = 0; p < s.np; ++p) {
+    const int w = sv_phase(s, p);
+    for (int x = 0; x < s.npair; ++x) {
+      if (zsr_type(s, x) == ZSR_JACOBSON) {
+        const long double j_aw = a_w > zj_low_rh(s, x) ? a_w : zj_low_rh(s, x);
+        const long double dj = a_w > zj_low_rh(s, x) ? daw : 0.0;
+        long double molal = zj_y(s, x, 0), dmolal = 0.0;
+        for (int k = 1; k < zj_ny(s, x); ++k) {
+          molal += zj_y(s, x, k) * pow((double)j_aw, k);
+          dmolal += zj_y(s, x, k) * k * pow((double)j_aw, k - 1);
+        }
+        dmolal *= dj;
+        const long double cat = state[w + zj_cat(s, x)] / zj_ncat(s, x) / zj_cat_mw(s, x) / 1000.0;
+        const long double dcat = 1.0 / zj_ncat(s, x) / zj_cat_mw(s, x) / 1000.0;
+        const long double an = state[w + zj_an(s, x)] / zj_nan(s, x) / zj_an_mw(s, x) / 1000.0;
+        const long double dan = 1.0 / zj_nan(s, x) / zj_an_mw(s, x) / 1000.0;
+        const long double ec = exp((double)(-100.0 * cat)), ea = exp((double)(-100.0 * an));
+        const long double conc = (cat * ec + an * ea) / (ec + ea);
+        const long double den = (ec + ea) * (ec + ea);
+        const long double dc_dcat = (ec * ec + ec * ea * (1.0 + 100.0 * an - 100.0 * cat)) / den;
+        const long double dc_dan = (ea * ea + ec * ea * (1.0 + 100.0 * cat - 100.0 * an)) / den;
+        JP[*zj_gw_jac(s, p, x)] += -2.0 * conc / pow((double)molal, 3) * 1000.0 * dmolal;
+        JP[*zj_an_jac(s, p, x)] += 1.0 / pow((double)molal, 2) * 1000.0 * dc_dan * dan;
+        JP[*zj_cat_jac(s, p, x)] += 1.0 / pow((double)molal, 2) * 1000.0 * dc_dcat * dcat;
+      } else if (zsr_type(s, x) == ZSR_EQSAM) {
+        long double e_aw = a_w > 0.99 ? 0.99 : a_w;
+        e_aw = e_aw < 0.001 ? 0.001 : e_aw;
+        long double de = a_w > 0.99 ? 0.0 : daw;
+        de = a_w < 0.001 ? 0.0 : de;
+        const long double pre = ze_nw(s, x) * 55.51 * 18.01 / ze_pair_mw(s, x) / 1000.0;
+        long double molal = pre * (1.0 / e_aw - 1.0);
+        long double dmolal = -pre / pow((double)e_aw, 2) * de;
+        dmolal = ze_zw(s, x) * pow((double)molal, ze_zw(s, x) - 1.0) * dmolal;
+        molal = pow((double)molal, ze_zw(s, x));
+        for (int k = 0; k < ze_nion(s, x); ++k) {
+          long double c = state[w + ze_ion(s, x, k)];
+          c = c > 0.0 ? c : 0.0;
+          const long double dc = c > 0.0 ? 1.0 : 0.0;
+          JP[*ze_gw_jac(s, p, x)] += -1.0 * c / ze_ion_mw(s, x, k) / pow((double)molal, 2) * dmolal;
+          JP[*ze_ion_jac(s, p, x, k)] += dc / ze_ion_mw(s, x, k) / molal;
+        }
+      }
+    }
+  }
+}
+
+/* moles of each ion [mol m-3] of phase instance p
+ * (src/sub_models/sub_model_PDFiTE.c:183-194) */
+static void pd_moles(SubV s, int p, const double *state, double *cn, double *an) {
+  const int base = sv_phase(s, p);
+  for (int x = 0; x < s.npair; ++x) {
+    cn[x] = state[base + pd_cat(s, x)] / pd_cat_mw(s, x) / 1000000.0;
+    an[x] = state[base + pd_an(s, x)] / pd_an_mw(s, x) / 1000000.0;
+  }
+}
+static long double pd_omega(SubV s, int x, const double *cn, const double *an) {
+  long double omega = 0.0;
+  for (int y = 0; y < s.npair; ++y) {
+    if (y == x) continue;
+    omega += (long double)2.0 * (pd_ncat(s, y) + pd_nan(s, y)) * cn[y] * an[y];
+  }
+  return omega;
+}
+
+/* src/sub_models/sub_model_PDFiTE.c:167-259 */
+static void pd_calc(SubV s, const double *e, double *state, double *cn, double *an) {
+  long double a_w = e[0] * state[s.gw];
+  if (a_w < 0.0) a_w = 0.0;
+  if (a_w > 1.0) a_w = 1.0;
+  for (int p = 0; p < s.np; ++p) {
+    pd_moles(s, p, state, cn, an);
+    for (int x = 0; x < s.npair; ++x) {
+      if (pd_ninter(s, x) == 0) break;
+      const long double omega = pd_omega(s, x, cn, an);
+      long double lng = 0.0;
+      for (int y = 0; y < pd_ninter(s, x); ++y) {
+        if (!pd_in_range(s, x, y, (double)a_w)) continue;
+        const int j = pd_inter_pair(s, x, y);
+        long double li = 0.0;
+        for (int z = 0; z < pd_nb(s, x, y); ++z) li += pd_b(s, x, y, z) * pow((double)a_w, z);
+        if (j == x)
+          lng += li;
+        else if (omega > 0.0)
+          lng += li * cn[j] * an[j] / omega;
+      }
+      state[sv_phase(s, p) + pd_act(s, x)] = exp((double)lng);
+    }
+  }
+}
+
+/* src/sub_models/sub_model_PDFiTE.c:273-432; a_w is a double here, as in
+ * the reference's Jacobian */
+static void pd_jac(SubV s, const double *e, const double *state, double *JP, double *cn,
+                   double *an) {
+  double a_w = e[0] * state[s.gw];
+  if (a_w < 0.0) a_w = 0.0;
+  if (a_w > 1.0) a_w = 1.0;
+  for (int p = 0; p < s.np; ++p) {
+    pd_moles(s, p, state, cn, an);
+    for (int x = 0; x < s.npair; ++x) {
+      if (pd_ninter(s, x) == 0) break;
+      const long double omega = pd_omega(s, x, cn, an);
+      long double lng = 0.0;
+      for (int y = 0; y < pd_ninter(s, x); ++y) {
+        if (!pd_in_range(s, x, y, a_w)) continue;
+        const int j = pd_inter_pair(s, x, y);
+        long double li = 0.0;
+        for (int z = 0; z < pd_nb(s, x, y); ++z) li += pd_b(s, x, y, z) * pow(a_w, z);
+        if (j == x)
+          lng += li;
+        else if (omega > 0.0)
+          lng += li * cn[j] * an[j] / omega;
+      }
+      const long double g = exp((double)lng);
+      for (int y = 0; y < pd_ninter(s, x); ++y) {
+        if (!pd_in_range(s, x, y, a_w)) continue;
+        const int j = pd_inter_pair(s, x, y);
+        long double li = pd_b(s, x, y, 0), dli = 0.0;
+        for (int z = 1; z < pd_nb(s, x, y); ++z) {
+          li += pd_b(s, x, y, z) * pow(a_w, z);
+          dli += pd_b(s, x, y, z) * z * pow(a_w, z - 1);
+        }
+        dli *= e[0];
+        if (j == x) {
+          JP[*pd_w_jac(s, p, x)] += g * dli;
+        } else if (omega > 0.0) {
+          JP[*pd_cat_jac(s, p, x, j)] += g * li * an[j] / pd_cat_mw(s, j) / omega * 1.0e-6;
+          JP[*pd_an_jac(s, p, x, j)] += g * li * cn[j] / pd_an_mw(s, j) / omega * 1.0e-6;
+          JP[*pd_w_jac(s, p, x)] += g * cn[j] * an[j] / omega * dli;
+          for (int k = 0; k < s.npair; ++k) {
+            if (k == x) continue;
+            JP[*pd_cat_jac(s, p, x, k)] += -g * li * cn[j] * an[j] / (omega * omega) * 2.0 *
+                                           (pd_ncat(s, k) + pd_nan(s, k)) * an[k] /
+                                           pd_cat_mw(s, k) * 1.0e-6;
+            JP[*pd_an_jac(s, p, x, k)] += -g * li * cn[j] * an[j] / (omega * omega) * 2.0 *
+                                          (pd_ncat(s, k) + pd_nan(s, k)) * cn[k] /
+                                          pd_an_mw(s, k) * 1.0e-6;
+          }
+        }
+      }
+    }
+  }
+}
+
+/* sub_model_calculate (src/sub_model_solver.c:300-333): in priority order,
+ * each writes its computed species into the state */
+static void sub_calculate(const OracleMech *m, double *state, const double *rxn_env) {
+  double cn[64], an[64];
+  for (int k = 0; k < m->n_sub; ++k) {
+    SubV s = subv(m, k);
+    if (m->sub_type[k] == SM_ZSR_AEROSOL_WATER)
+      zsr_calc(s, sub_env(m, rxn_env, k), state);
+    else
+      pd_calc(s, sub_env(m, rxn_env, k), state, cn, an);
+  }
+}
+
+/* sub_model_get_jac_contrib (src/sub_model_solver.c:341-381) into J_params
+ * (zeroed here); element 0 is the fold's unit parameter */
+static void sub_jacobian(const OracleMech *m, const double *state, const double *rxn_env,
+                         double *JP) {
+  double cn[64], an[64];
+  for (int i = 0; i < m->n_param_jac; ++i) JP[i] = 0.0;
+  for (int k = 0; k < m->n_sub; ++k) {
+    SubV s = subv(m, k);
+    if (m->sub_type[k] == SM_ZSR_AEROSOL_WATER)
+      zsr_jac(s, sub_env(m, rxn_env, k), state, JP);
+    else
+      pd_jac(s, sub_env(m, rxn_env, k), state, JP, cn, an);
+  }
+  JP[0] = 1.0;
+}
+
+/* the sub-model's parameter Jacobian elements (dep = computed species, ind =
+ * the species it is computed from) through a callback; the same walk
+ * registers them (get_used_jac_elem) and looks up their ids (update_ids) */
+typedef void (*sub_elem_fn)(void *ctx, int dep, int ind, int *id);
+static void sub_elements(const OracleMech *m, int k, sub_elem_fn fn, void *ctx) {
+  SubV s = subv(m, k);
+  for (int p = 0; p < s.np; ++p) {
+    const int w = sv_phase(s, p);
+    if (m->sub_type[k] == SM_ZSR_AEROSOL_WATER) {
+      /* src/sub_models/sub_model_ZSR_aerosol_water.c:81-129, 140-185 */
+      fn(ctx, w, s.gw, NULL);
+      for (int x = 0; x < s.npair; ++x) {
+        if (zsr_type(s, x) == ZSR_JACOBSON) {
+          fn(ctx, w, s.gw, zj_gw_jac(s, p, x));
+          fn(ctx, w, w + zj_cat(s, x), zj_cat_jac(s, p, x));
+          fn(ctx, w, w + zj_an(s, x), zj_an_jac(s, p, x));
+        } else if (zsr_type(s, x) == ZSR_EQSAM) {
+          fn(ctx, w, s.gw, ze_gw_jac(s, p, x));
+          for (int i = 0; i < ze_nion(s, x); ++i)
+            fn(ctx, w, w + ze_ion(s, x, i), ze_ion_jac(s, p, x, i));
+        }
+      }
+    } else {
+      /* src/sub_models/sub_model_PDFiTE.c:73-130 */
+      for (int x = 0; x < s.npair; ++x) {
+        const int g = w + pd_act(s, x);
+        fn(ctx, g, s.gw, pd_w_jac(s, p, x));
+        for (int y = 0; y < s.npair; ++y) {
+          fn(ctx, g, w + pd_cat(s, y), pd_cat_jac(s, p, x, y));
+          fn(ctx, g, w + pd_an(s, y), pd_an_jac(s, p, x, y));
+        }
+      }
+    }
+  }
+}
+static void sub_register_cb(void *ctx, int dep, int ind, int *id) {
+  (void)id;
+  jr_register((JacReg *)ctx, dep, ind);
+}
+typedef struct {
+  const int *colptr, *rowid;
+} PJLookup;
+static void sub_ids_cb(void *ctx, int dep, int ind, int *id) {
+  const PJLookup *l = (const PJLookup *)ctx;
+  if (id) *id = jr_elem_id(l->colptr, l->rowid, dep, ind);
+}
+
 /* --- LU symbolic: Markowitz order over diagonal pivots ------------------- */
 static void lu_symbolic(LUSym *lu, int n, const int *colptr, const int *rowid) {
   unsigned char *P = (unsigned char *)zalloc((size_t)n * n);
@@ -960,7 +1365,39 @@ int om_build(OracleMech *m) {
     }
   }
 
-  /* solver Jacobian: var x var elements of the reaction Jacobian */
+  /* sub-model parameter Jacobian (src/camp_solver.c:1520-1550): the dummy
+   * element (0, 0), then the sub-models' elements through a local Jacobian
+   * (src/sub_model_solver.c:25-104); an element whose independent species is
+   * itself computed by a sub-model would need the interdependence map, which
+   * no supported configuration has: refused */
+  JacReg pj, lj;
+  jr_init(&pj, n);
+  jr_register(&pj, 0, 0);
+  jr_init(&lj, n);
+  for (int k = 0; k < m->n_sub; ++k) sub_elements(m, k, sub_register_cb, &lj);
+  jr_build(&lj);
+  for (int ind = 0; ind < n; ++ind)
+    for (int e = lj.colptr[ind]; e < lj.colptr[ind + 1]; ++e) {
+      const int dep = lj.rowid[e];
+      jr_register(&pj, dep, ind);
+      if (dep != ind && m->var_type[ind] != VAR_VARIABLE)
+        for (int j = 0; j < n; ++j)
+          if (jr_elem_id(lj.colptr, lj.rowid, ind, j) != -1) return 3;
+    }
+  free(lj.colptr);
+  free(lj.rowid);
+  jr_build(&pj);
+  m->n_param_jac = pj.nnz;
+  m->pj_colptr = pj.colptr;
+  m->pj_rowid = pj.rowid;
+  {
+    PJLookup l = {m->pj_colptr, m->pj_rowid};
+    for (int k = 0; k < m->n_sub; ++k) sub_elements(m, k, sub_ids_cb, &l);
+  }
+
+  /* solver Jacobian (src/camp_solver.c:1559-1633): a variable row keeps its
+   * variable columns, and a non-variable column c maps to every variable
+   * species the sub-model parameter c depends on */
   JacReg sj;
   jr_init(&sj, n);
   for (int ind = 0; ind < n; ++ind)
@@ -968,7 +1405,14 @@ int om_build(OracleMech *m) {
       if (m->var_type[dep] != VAR_VARIABLE ||
           jr_elem_id(m->rj_colptr, m->rj_rowid, dep, ind) == -1)
         continue;
-      if (m->var_type[ind] == VAR_VARIABLE) jr_register(&sj, dep, ind);
+      if (m->var_type[ind] == VAR_VARIABLE) {
+        jr_register(&sj, dep, ind);
+        continue;
+      }
+      for (int j = 0; j < n; ++j)
+        if (jr_elem_id(m->pj_colptr, m->pj_rowid, ind, j) != -1 &&
+            m->var_type[j] == VAR_VARIABLE)
+          jr_register(&sj, dep, j);
     }
   jr_build(&sj);
   m->n_solver_jac = sj.nnz;
@@ -978,15 +1422,42 @@ int om_build(OracleMech *m) {
     if (m->deriv_ids[c] >= 0) m->sj_colptr[m->deriv_ids[c]] = sj.colptr[c];
   m->sj_colptr[m->n_dep] = sj.nnz;
   for (int e = 0; e < sj.nnz; ++e) m->sj_rowid[e] = m->deriv_ids[sj.rowid[e]];
+  /* the fold map (src/camp_solver.c:1649-1681), in reaction-Jacobian order;
+   * param 0 is the unit parameter */
+  int cap = m->n_rxn_jac + 16, nm = 0;
+  m->map_s = (int *)zalloc(sizeof(int) * cap);
+  m->map_r = (int *)zalloc(sizeof(int) * cap);
+  m->map_p = (int *)zalloc(sizeof(int) * cap);
   m->rxn_to_solver = (int *)zalloc(sizeof(int) * (m->n_rxn_jac + 1));
   for (int ind = 0; ind < n; ++ind)
     for (int e = m->rj_colptr[ind]; e < m->rj_colptr[ind + 1]; ++e) {
-      int dep = m->rj_rowid[e];
-      m->rxn_to_solver[e] =
-          (m->var_type[dep] == VAR_VARIABLE && m->var_type[ind] == VAR_VARIABLE)
-              ? jr_elem_id(sj.colptr, sj.rowid, dep, ind)
-              : -1;
+      const int dep = m->rj_rowid[e];
+      m->rxn_to_solver[e] = -1;
+      if (m->var_type[dep] != VAR_VARIABLE) continue;
+      for (int j = 0; j < n; ++j) {
+        int s = -1, pid = 0;
+        if (m->var_type[ind] == VAR_VARIABLE) {
+          if (j > 0) break;
+          s = jr_elem_id(sj.colptr, sj.rowid, dep, ind);
+          m->rxn_to_solver[e] = s;
+        } else {
+          pid = jr_elem_id(m->pj_colptr, m->pj_rowid, ind, j);
+          if (pid == -1 || m->var_type[j] != VAR_VARIABLE) continue;
+          s = jr_elem_id(sj.colptr, sj.rowid, dep, j);
+        }
+        if (nm == cap) {
+          cap *= 2;
+          m->map_s = (int *)realloc(m->map_s, sizeof(int) * cap);
+          m->map_r = (int *)realloc(m->map_r, sizeof(int) * cap);
+          m->map_p = (int *)realloc(m->map_p, sizeof(int) * cap);
+        }
+        m->map_s[nm] = s;
+        m->map_r[nm] = e;
+        m->map_p[nm] = pid;
+        ++nm;
+      }
     }
+  m->n_map = nm;
   free(sj.colptr);
   free(sj.rowid);
   lu_symbolic(&m->lu, m->n_dep, m->sj_colptr, m->sj_rowid);
@@ -997,6 +1468,17 @@ int om_build(OracleMech *m) {
 void om_free(OracleMech *m) {
   if (!m) return;
   for (int i = 0; i < m->n_rxn; ++i) free(m->rx[i].aq_thr);
+  free(m->sub_type);
+  free(m->sub_ioff);
+  free(m->sub_foff);
+  free(m->sub_eoff);
+  free(m->sub_int);
+  free(m->sub_flt);
+  free(m->pj_colptr);
+  free(m->pj_rowid);
+  free(m->map_s);
+  free(m->map_r);
+  free(m->map_p);
   free(m->var_type);
   free(m->int_data);
   free(m->float_data);
@@ -1022,7 +1504,16 @@ void om_free(OracleMech *m) {
 }
 
 int om_n_dep_var(const OracleMech *m) { return m->n_dep; }
-int om_n_rxn_env_data(const OracleMech *m) { return m->n_env + m->n_aero_env; }
+int om_n_rxn_env_data(const OracleMech *m) { return m->n_env + m->n_aero_env + m->n_sub_env; }
+int om_n_param_jac_elem(const OracleMech *m) { return m->n_param_jac; }
+int om_n_mapped_values(const OracleMech *m) { return m->n_map; }
+void om_get_jac_map(const OracleMech *m, int *triplets) {
+  for (int i = 0; i < m->n_map; ++i) {
+    triplets[3 * i] = m->map_s[i];
+    triplets[3 * i + 1] = m->map_r[i];
+    triplets[3 * i + 2] = m->map_p[i];
+  }
+}
 int om_n_rxn_jac_elem(const OracleMech *m) { return m->n_rxn_jac; }
 int om_n_solver_jac_elem(const OracleMech *m) { return m->n_solver_jac; }
 int om_n_lu_elem(const OracleMech *m) { return m->lu.nnz; }
@@ -1137,6 +1628,10 @@ void om_update_env(const OracleMech *m, const double *env, double *rxn_env) {
         break;
     }
   }
+  /* sub_model_update_env_state (src/sub_model_solver.c:264-295): both
+   * sub-model types keep PPM_TO_RH_ as their one env parameter */
+  for (int k = 0; k < m->n_sub; ++k)
+    rxn_env[m->n_env + m->n_aero_env + m->sub_eoff[k]] = ppm_to_rh(T, P);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1156,8 +1651,18 @@ static void add_value(long double *P, long double *L, int d, long double v) {
  * would drive the product below zero within one step
  * (src/rxns/rxn_arrhenius.c:131-165).  Contributions are split by sign into
  * production and loss sums (src/time_derivative.c:90-97). */
-void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
+void om_deriv(const OracleMech *m, const double *state_in, const double *rxn_env,
               double time_step, double *deriv, double *r_p, double *r_l) {
+  /* the sub-models first write their computed species into (a copy of) the
+   * state, as f does (src/camp_solver.c:907-911) */
+  double *tmp = NULL;
+  const double *state = state_in;
+  if (m->n_sub > 0) {
+    tmp = (double *)zalloc(sizeof(double) * m->n_state);
+    memcpy(tmp, state_in, sizeof(double) * m->n_state);
+    sub_calculate(m, tmp, rxn_env);
+    state = tmp;
+  }
   long double *P = (long double *)zalloc(sizeof(long double) * m->n_dep * 2);
   long double *L = P + m->n_dep;
   for (int i = 0; i < m->n_rxn; ++i) {
@@ -1301,12 +1806,23 @@ void om_deriv(const OracleMech *m, const double *state, const double *rxn_env,
     if (r_l) r_l[d] = (double)L[d];
   }
   free(P);
+  free(tmp);
 }
 
 /* src/rxns/rxn_arrhenius.c:178-212 and src/Jacobian.c:223-241, then the
- * jac_map fold with unit parameters (src/camp_solver.c:1096-1106). */
-void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
+ * jac_map fold with the sub-model parameters (src/camp_solver.c:1063-1106):
+ * J_solver[s] += J_rxn[r] * J_params[p], J_params[0] = 1. */
+void om_jac(const OracleMech *m, const double *state_in, const double *rxn_env,
             double time_step, double *jvals) {
+  double *tmp = (double *)zalloc(sizeof(double) * (m->n_state + m->n_param_jac + 1));
+  double *JP = tmp + m->n_state;
+  const double *state = state_in;
+  if (m->n_sub > 0) {
+    memcpy(tmp, state_in, sizeof(double) * m->n_state);
+    sub_calculate(m, tmp, rxn_env);
+    state = tmp;
+  }
+  sub_jacobian(m, state, rxn_env, JP);
   long double *P = (long double *)zalloc(sizeof(long double) * m->n_rxn_jac * 2);
   long double *L = P + m->n_rxn_jac;
   for (int i = 0; i < m->n_rxn; ++i) {
@@ -1505,11 +2021,10 @@ void om_jac(const OracleMech *m, const double *state, const double *rxn_env,
     }
   }
   for (int s = 0; s < m->n_solver_jac; ++s) jvals[s] = 0.0;
-  for (int e = 0; e < m->n_rxn_jac; ++e) {
-    int s = m->rxn_to_solver[e];
-    if (s >= 0) jvals[s] += (double)(P[e] - L[e]);
-  }
+  for (int i = 0; i < m->n_map; ++i)
+    jvals[m->map_s[i]] += (double)(P[m->map_r[i]] - L[m->map_r[i]]) * JP[m->map_p[i]];
   free(P);
+  free(tmp);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -2375,7 +2890,7 @@ static void *solve_job(void *arg) {
   b.ctx = &ctx;
   for (int c = jb->c0; c < jb->c1; ++c) {
     double *st = jb->state + (size_t)c * ns;
-    double *re = jb->rxn_env + (size_t)c * (m->n_env + m->n_aero_env);
+    double *re = jb->rxn_env + (size_t)c * om_n_rxn_env_data(m);
     /* solver_run: dependent values clamped to >= TINY, constants too
      * (src/camp_solver.c:554-567); rate constants from env (:587-603) */
     for (int i = 0, d = 0; i < ns; ++i) {

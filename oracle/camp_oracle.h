@@ -9,7 +9,11 @@
  *     PHOTOLYSIS types (src/rxns/rxn_*.c), with long double accumulators
  *     as in src/time_derivative.c and src/Jacobian.c;
  *   - the Jacobian sparsity build and DERIV_ID/JAC_ID update
- *     (src/Jacobian.c, src/camp_solver.c:1417-1712);
+ *     (src/Jacobian.c, src/camp_solver.c:1417-1712), with the sub-model
+ *     parameter Jacobian and the J_rxn x J_params fold;
+ *   - the ZSR aerosol-water and PD-FiTE activity sub-models
+ *     (src/sub_models/sub_model_ZSR_aerosol_water.c,
+ *     src/sub_models/sub_model_PDFiTE.c), run before every f and J;
  *   - a sparse LU of I - gamma*J on a Markowitz diagonal-pivot order (the
  *     reference uses SuiteSparse KLU, which is not in the reference tree);
  *   - the variable-order BDF integrator of CVODE (Hindmarsh et al., ACM TOMS
@@ -68,6 +72,10 @@ int om_add_aero_rep(OracleMech *m, int type, int n_int, int n_float, int n_env,
  * representation part follows the reaction env parameters */
 int om_set_aero_env(const OracleMech *m, double *rxn_env_cell, int rep, int section,
                     int what, double value);
+/* sub_model_add_condensed_data: ZSR aerosol water (2) and PD-FiTE (3);
+ * ints without the type slot.  Returns 0, or 2 for another type. */
+int om_add_sub_model(OracleMech *m, int type, int n_int, int n_float, int n_env,
+                     const int *ints, const double *floats);
 int om_build(OracleMech *m);
 /* the absolute tolerances (per state variable) that set the aqueous
  * equilibrium's minimum water, as solver_initialize's do; om_solve sets
@@ -97,6 +105,11 @@ int om_set_experiment(OracleMech *m, double guard_step, int positivity);
 
 int om_n_dep_var(const OracleMech *m);
 int om_n_rxn_env_data(const OracleMech *m);
+int om_n_param_jac_elem(const OracleMech *m);
+int om_n_mapped_values(const OracleMech *m);
+/* the solver-Jacobian fold as (solver id, reaction-Jacobian id, parameter
+ * id) triplets, src/camp_solver.c:1649-1681 */
+void om_get_jac_map(const OracleMech *m, int *triplets);
 int om_n_rxn_jac_elem(const OracleMech *m);
 int om_n_solver_jac_elem(const OracleMech *m);
 int om_n_lu_elem(const OracleMech *m);

@@ -85,6 +85,8 @@ def oracle_lib():
             "om_n_solver_jac_elem",
             "om_n_lu_elem",
             "om_rxn_int_data_size",
+            "om_n_param_jac_elem",
+            "om_n_mapped_values",
         ):
             getattr(lib, name).restype = C.c_int
             getattr(lib, name).argtypes = [vp]
@@ -92,6 +94,9 @@ def oracle_lib():
         lib.om_get_solver_jac.argtypes = [vp, _i32p, _i32p]
         lib.om_get_rxn_int_data.argtypes = [vp, _i32p]
         lib.om_get_lu_order.argtypes = [vp, _i32p]
+        lib.om_get_jac_map.argtypes = [vp, _i32p]
+        lib.om_add_sub_model.restype = C.c_int
+        lib.om_add_sub_model.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p]
         lib.om_set_photo_rate.restype = C.c_int
         lib.om_set_photo_rate.argtypes = [vp, _f64p, C.c_int, C.c_double]
         lib.om_set_rate.restype = C.c_int
@@ -201,8 +206,14 @@ class OracleModel:
                                         np.ascontiguousarray(a.ints, np.int32),
                                         np.ascontiguousarray(a.floats, np.float64)) != 0:
                 raise ValueError(f"oracle rejected aerosol representation type {a.rep_type}")
-        if self.lib.om_build(self.h) != 0:
-            raise RuntimeError("oracle sparsity build failed")
+        for sm in mech.sub_models:
+            if self.lib.om_add_sub_model(self.h, sm.sub_type, sm.ints.size, sm.floats.size,
+                                         sm.n_env, np.ascontiguousarray(sm.ints, np.int32),
+                                         np.ascontiguousarray(sm.floats, np.float64)) != 0:
+                raise ValueError(f"oracle rejected sub-model type {sm.sub_type}")
+        rc = self.lib.om_build(self.h)
+        if rc != 0:
+            raise RuntimeError(f"oracle sparsity build failed (code {rc})")
         # the mechanism's tolerances, as solver_initialize would pass them
         self.lib.om_set_abs_tol(self.h, np.ascontiguousarray(mech.abs_tol, np.float64))
         self.n_dep = self.lib.om_n_dep_var(self.h)
@@ -238,6 +249,13 @@ class OracleModel:
         ri = np.zeros(max(self.n_rxn_jac, 1), np.int32)
         self.lib.om_get_rxn_jac(self.h, cp, ri)
         return cp, ri[: self.n_rxn_jac]
+
+    def jac_map(self):
+        """(solver id, reaction-Jacobian id, parameter id) per mapped value."""
+        n = self.lib.om_n_mapped_values(self.h)
+        out = np.zeros(3 * max(n, 1), np.int32)
+        self.lib.om_get_jac_map(self.h, out)
+        return out[: 3 * n].reshape(n, 3)
 
     def rxn_int_data(self):
         out = np.zeros(self.lib.om_rxn_int_data_size(self.h), np.int32)

@@ -42,8 +42,12 @@ def cb05_ref():
 # code: cb05cl_ae5, the gas phase of MONARCH mod37 (cb05 with dry
 # deposition, emissions and the wet deposition of one aqueous phase), and
 # mod37 with its SOA scheme (SIMPOL partitioning into the modal/binned
-# aerosol representation)
-GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas", "monarch_mod37_soa", "monarch_mod37_aero")
+# aerosol representation), mod37 with SOA, cloud/rain HL and aqueous
+# equilibria, and the shipped MONARCH mod37 test configuration
+# (test/monarch/config_monarch_mod37.json), whose aerosol water and ion-pair
+# activity coefficients the ZSR and PD-FiTE sub-models compute
+GOLDEN_MECHS = ("cb05cl_ae5", "monarch_mod37_gas", "monarch_mod37_soa", "monarch_mod37_aero",
+                "monarch_mod37_shipped")
 
 
 @pytest.fixture(scope="session")
@@ -65,6 +69,13 @@ def mod37_aero():
     from camp_b200.mechanism import Mechanism
 
     return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_aero.mech.json"))
+
+
+@pytest.fixture(scope="session")
+def mod37_shipped():
+    from camp_b200.mechanism import Mechanism
+
+    return Mechanism.load(os.path.join(GOLDEN, "monarch_mod37_shipped.mech.json"))
 
 
 @pytest.fixture(scope="session", params=GOLDEN_MECHS)

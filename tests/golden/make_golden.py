@@ -35,8 +35,16 @@ Outputs (all small):
                          (inorganic_reactions.json; their ion pairs'
                          activity coefficients are constant species here, as
                          without the PDFiTE sub-model)
+  monarch_mod37_shipped.mech.json
+                         test/monarch/config_monarch_mod37.json as shipped:
+                         cb05cl_ae5, the SOA scheme, HL partitioning of SULF,
+                         HNO3 and NH3 into the aqueous sulfate phase, its
+                         aqueous equilibria, and the ZSR aerosol-water and
+                         PD-FiTE activity sub-models that make the phase's
+                         water and ion-pair activity coefficients functions
+                         of the state
   cb05cl_ae5_ref.npz, monarch_mod37_gas_ref.npz, monarch_mod37_soa_ref.npz,
-  monarch_mod37_aero_ref.npz
+  monarch_mod37_aero_ref.npz, monarch_mod37_shipped_ref.npz
                          outputs of the reference's own C code
                          (oracle/_ref/libcamp_ref.so, compiled from the
                          reference sources) on seeded cell states:
@@ -133,6 +141,20 @@ def mod37_aero(ref_root: str):
                                   name="monarch_mod37_aero")
 
 
+def mod37_shipped(ref_root: str):
+    """test/monarch/config_monarch_mod37.json as shipped: cb05cl_ae5, the
+    mod37 species, aerosol phases and representation, HL partitioning of
+    SULF / HNO3 / NH3 with the ZSR aerosol-water sub-model, the PD-FiTE
+    activity sub-model, the aqueous equilibria and the 2-product SOA scheme
+    (the config's build-tree paths ``mechanisms_run`` map to ``mechanisms``)."""
+    from camp_b200.aerosol import load_aerosol_mechanism
+    from camp_b200.mechanism import expand_config
+
+    cfg = os.path.join(ref_root, "test/monarch/config_monarch_mod37.json")
+    files = expand_config(cfg, lambda p: p.replace("mechanisms_run", "mechanisms"))
+    return load_aerosol_mechanism(files, name="monarch_mod37_shipped")
+
+
 def edge_cells(mech, cells):
     """Appends edge-case cells to a seeded batch."""
     st, env, ph = cells.state.copy(), cells.env.copy(), cells.photo_rates.copy()
@@ -179,6 +201,7 @@ def main(ref_root: str, only: list[str] | None = None) -> None:
         "monarch_mod37_gas": lambda: mod37_gas(ref_root),
         "monarch_mod37_soa": lambda: mod37_soa(ref_root),
         "monarch_mod37_aero": lambda: mod37_aero(ref_root),
+        "monarch_mod37_shipped": lambda: mod37_shipped(ref_root),
     }
     for tag, make in makers.items():
         if not only or tag in only:
@@ -229,4 +252,5 @@ def write_fixture(mech, tag: str) -> None:
 
 if __name__ == "__main__":
     # make_golden.py [REFERENCE_ROOT [TAG ...]]: all fixtures, or the named ones
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CAMP_REFERENCE_ROOT", "/root/reference"),
+         sys.argv[2:] or None)

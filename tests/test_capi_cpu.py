@@ -42,6 +42,9 @@ def test_sparsity_via_c_abi(golden, lib):
     assert np.array_equal(ri, ref["solver_rowid"])
     # DERIV_ID_/JAC_ID_ of every reaction, bit for bit
     assert np.array_equal(s.rxn_int_data(), ref["rxn_int_data"])
+    # the fold J_solver += J_rxn * J_params, triplet for triplet (sub-model
+    # parameters on the shipped mod37 configuration)
+    assert np.array_equal(s.jac_map(), ref["jac_map"])
     perm = s.lu_order()
     assert sorted(perm.tolist()) == list(range(mech.n_dep_var))
     if mech.name == "cb05cl_ae5":

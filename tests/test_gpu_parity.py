@@ -1,8 +1,9 @@
 """GPU parity: the CUDA path through the C ABI against the reference's C
 derivative/Jacobian (golden fixtures: cb05cl_ae5, the gas phase of MONARCH
 mod37 with its deposition and emission reactions, mod37 with SIMPOL SOA
-partitioning, and with HL partitioning into cloud and rain water as well)
-and against the CPU oracle's solve."""
+partitioning, with HL partitioning into cloud and rain water as well, and
+the shipped mod37 test configuration with its ZSR aerosol-water and PD-FiTE
+activity sub-models) and against the CPU oracle's solve."""
 import numpy as np
 import pytest
 
@@ -139,6 +140,16 @@ def test_mod37_aero_solve_matches_oracle(mod37_aero, precision):
     (the LU without HL's zero element partials; the oracle factors the
     reference's full pattern)."""
     _check_solve(mod37_aero, precision=precision, seed=19 + precision,
+                 bulk_rel=1e-7 if precision == 0 else 1e-4)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mod37_shipped_solve_matches_oracle(mod37_shipped, precision):
+    """The shipped MONARCH mod37 test configuration: the ZSR sub-model
+    computes the sulfate mode's aerosol water and PD-FiTE four ion-pair
+    activity coefficients before every f and J, and the Jacobian chains
+    their parameter partials (J_rxn x J_params) into the solver Jacobian."""
+    _check_solve(mod37_shipped, precision=precision, seed=23 + precision,
                  bulk_rel=1e-7 if precision == 0 else 1e-4)
 
 

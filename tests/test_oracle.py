@@ -34,6 +34,8 @@ def test_sparsity_bit_exact(gom):
     assert np.array_equal(rri, ref["rxn_rowid"])
     # DERIV_ID_/JAC_ID_ written back into the packed ints
     assert np.array_equal(om.rxn_int_data(), ref["rxn_int_data"])
+    # the fold J_solver += J_rxn * J_params, entry for entry
+    assert np.array_equal(om.jac_map(), ref["jac_map"])
 
 
 def test_sizes(om):
