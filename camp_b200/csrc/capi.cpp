@@ -1017,9 +1017,16 @@ void* camp_b200_solver_from_json(const char* const* files, int n_files, int n_ce
     rp_f += (int)r.floats.size();
     rp_e += r.n_env;
   }
+  int sm_i = 0, sm_f = 0, sm_e = 0;
+  for (const auto& m : lm.subs) {
+    sm_i += (int)m.ints.size();
+    sm_f += (int)m.floats.size();
+    sm_e += m.n_env;
+  }
   void* sd = solver_new((int)lm.species.size(), n_cells, lm.var_type.data(), (int)lm.rxns.size(),
                         lm.n_int(), lm.n_float(), lm.n_env(), (int)lm.phases.size(), ph_i, ph_f,
-                        (int)lm.reps.size(), rp_i, rp_f, rp_e, 0, 0, 0, 0);
+                        (int)lm.reps.size(), rp_i, rp_f, rp_e, (int)lm.subs.size(), sm_i, sm_f,
+                        sm_e);
   if (!sd) return nullptr;
   // reactions, then phases and representations, the order of
   // camp_solver_data%initialize (src/camp_solver_data.F90:635-700)
@@ -1032,6 +1039,9 @@ void* camp_b200_solver_from_json(const char* const* files, int n_files, int n_ce
   for (auto& r : lm.reps)
     aero_rep_add_condensed_data(r.type, (int)r.ints.size(), (int)r.floats.size(), r.n_env,
                                 r.ints.data(), r.floats.data(), sd);
+  for (auto& m : lm.subs)
+    sub_model_add_condensed_data(m.type, (int)m.ints.size(), (int)m.floats.size(), m.n_env,
+                                 m.ints.data(), m.floats.data(), sd);
   Solver* s = S(sd);
   if (s->add_error) {
     set_error("camp_b200_solver_from_json: " + s->add_error_msg);
@@ -1075,10 +1085,17 @@ int camp_b200_get_var_type(void* solver_data, int* out) {
 int camp_b200_get_aero_data(void* solver_data, int which, int index, int* n_int, int* n_float,
                             int* ints, double* floats) {
   const Model& m = *S(solver_data)->model;
-  const int count = which == 0 ? m.n_aero_phase() : which == 1 ? m.n_aero_rep() : -1;
+  const int count = which == 0   ? m.n_aero_phase()
+                    : which == 1 ? m.n_aero_rep()
+                    : which == 2 ? m.n_sub_model()
+                                 : -1;
   if (index < 0 || index >= count) return -1;
-  const std::vector<int>& I = which == 0 ? m.aero_phase_int(index) : m.aero_rep_int(index);
-  const std::vector<double>& F = which == 0 ? m.aero_phase_float(index) : m.aero_rep_float(index);
+  const std::vector<int>& I = which == 0   ? m.aero_phase_int(index)
+                              : which == 1 ? m.aero_rep_int(index)
+                                           : m.sub_model_int(index);
+  const std::vector<double>& F = which == 0   ? m.aero_phase_float(index)
+                                 : which == 1 ? m.aero_rep_float(index)
+                                              : m.sub_model_float(index);
   if (n_int) *n_int = (int)I.size();
   if (n_float) *n_float = (int)F.size();
   if (ints) std::copy(I.begin(), I.end(), ints);

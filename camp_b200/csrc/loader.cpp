@@ -1,6 +1,7 @@
 // CAMP JSON input -> state layout and packed gas-phase reactions (loader.hpp).
 #include "loader.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <map>
@@ -820,6 +821,351 @@ bool pack_wet_deposition(const Json& r, const std::vector<Rep>& reps,
   return true;
 }
 
+// --- sub-models: ZSR aerosol water and PD-FiTE activity ------------------
+
+// 1-based state ids of (phase, species) over every representation's
+// instances, in representation and instance order
+std::vector<int> instance_ids(const std::vector<Rep>& reps, const std::vector<LoadedPhase>& ph,
+                              const std::string& phase, const std::string& spec) {
+  std::vector<int> out;
+  for (const Rep& r : reps)
+    for (const std::string& un : r.names(ph, &phase, &spec)) out.push_back(r.state_id(un));
+  return out;
+}
+
+// state id of spec relative to the aerosol water of the same instance; the
+// same for every instance (the Fortran packers' relative ids)
+bool relative_id(const std::vector<Rep>& reps, const std::vector<LoadedPhase>& ph,
+                 const std::string& phase, const std::string& spec,
+                 const std::vector<int>& water_ids, int* rel, std::string* err) {
+  const std::vector<int> ids = instance_ids(reps, ph, phase, spec);
+  if (ids.size() != water_ids.size() || ids.empty()) {
+    *err = "Incorrect number of instances of '" + spec + "' in phase '" + phase + "'";
+    return false;
+  }
+  *rel = ids[0] - water_ids[0];
+  for (size_t k = 1; k < ids.size(); ++k)
+    if (ids[k] - water_ids[k] != *rel) {
+      *err = "'" + spec + "' is not at the same place in every instance of '" + phase + "'";
+      return false;
+    }
+  return true;
+}
+
+// the two ions of a neutral ion pair: name, quantity, molecular weight, charge
+struct Ion {
+  std::string name;
+  int qty;
+  double mw;
+  int charge;
+};
+bool ion_pair_ions(const Json& ions, const SpeciesDb& db, const std::string& what,
+                   std::vector<Ion>* out, std::string* err) {
+  if (ions.obj.size() != 2) {
+    *err = "Invalid number of unique ions for ion pair in " + what;
+    return false;
+  }
+  int total = 0;
+  for (const auto& kv : ions.obj) {
+    bool ok = true;
+    int qty = 1;
+    if (const Json* q = kv.second.get("qty")) qty = (int)SpeciesDb::as_number(*q, &ok);
+    if (!db.spec.count(kv.first)) {
+      *err = "Missing species properties for ion '" + kv.first + "' in " + what;
+      return false;
+    }
+    double mw = 0.0, charge = 0.0;
+    if (!db.number(kv.first, "molecular weight [kg mol-1]", &mw, err) ||
+        !db.number(kv.first, "charge", &charge, err))
+      return false;
+    if ((int)charge == 0) {
+      *err = "Neutral species '" + kv.first + "' not allowed in an ion pair in " + what;
+      return false;
+    }
+    total += qty * (int)charge;
+    out->push_back({kv.first, qty, mw, (int)charge});
+  }
+  if (total != 0) {
+    *err = "Charge imbalance for an ion pair in " + what;
+    return false;
+  }
+  return true;
+}
+
+// sub_model_ZSR_aerosol_water_t%initialize
+// (src/sub_models/sub_model_ZSR_aerosol_water.F90:215-500): the layout the
+// C sub-model reads (src/sub_models/sub_model_ZSR_aerosol_water.c:27-71),
+// ion ids relative to the instance's water, Jacobian ids left at 0
+bool pack_zsr(const Json& o, const SpeciesDb& db, const std::map<std::string, int>& gas_index,
+              const std::vector<Rep>& reps, const std::vector<LoadedPhase>& ph,
+              LoadedSubModel* out, std::string* err) {
+  const std::string what = "ZSR aerosol water";
+  const std::string* phase = json_str(o, "aerosol phase");
+  const std::string* water = json_str(o, "aerosol-phase water");
+  const std::string* gw = json_str(o, "gas-phase water");
+  if (!phase || !water || !gw) {
+    *err = what + ": missing aerosol phase, aerosol-phase water or gas-phase water";
+    return false;
+  }
+  if (!db.spec.count(*water) || db.var_type(*water) != kConstant) {
+    *err = "ZSR calculated species " + *water + " must be of tracer type CONSTANT";
+    return false;
+  }
+  const std::vector<int> water_ids = instance_ids(reps, ph, *phase, *water);
+  const int np = (int)water_ids.size();
+  if (np == 0) {
+    *err = "Aerosol phase '" + *phase + "' not present in any aerosol representation for " + what;
+    return false;
+  }
+  const Json* pairs = o.get("ion pairs");
+  if (!pairs || pairs->obj.empty()) {
+    *err = "Empty ion pair set in " + what;
+    return false;
+  }
+  if (!gas_index.count(*gw)) {
+    *err = "Cannot find gas-phase water species '" + *gw + "' for " + what;
+    return false;
+  }
+  const int n = (int)pairs->obj.size();
+  int n_int = 5 + np + 2 * n, n_flt = 0;
+  for (const auto& kv : pairs->obj) {
+    const std::string* t = json_str(kv.second, "type");
+    if (t && *t == "JACOBSON") {
+      const Json* y = kv.second.get("Y_j");
+      n_int += 6 + 3 * np;
+      n_flt += 3 + (y ? (int)y->arr.size() : 0);
+    } else if (t && *t == "EQSAM") {
+      const Json* ions = kv.second.get("ions");
+      const int ni = ions ? (int)ions->obj.size() : 0;
+      n_int += 2 + np + (1 + np) * ni;
+      n_flt += 3 + ni;
+    } else {
+      *err = "Invalid activity type specified for " + what;
+      return false;
+    }
+  }
+  std::vector<int> I(n_int, 0);
+  std::vector<double> F(n_flt, 0.0);
+  I[0] = np;
+  I[1] = gas_index.at(*gw);
+  I[2] = n;
+  I[3] = n_int;
+  I[4] = n_flt;
+  for (int p = 0; p < np; ++p) I[5 + p] = water_ids[p];
+  int ii = 5 + np + 2 * n, ff = 0, x = 0;
+  bool ok = true;
+  for (const auto& kv : pairs->obj) {
+    const Json& pr = kv.second;
+    I[5 + np + x] = ii + 1;
+    I[5 + np + n + x] = ff + 1;
+    ++x;
+    if (*json_str(pr, "type") == "JACOBSON") {
+      I[ii] = 1;
+      const Json* y = pr.get("Y_j");
+      const int ny = y ? (int)y->arr.size() : 0;
+      I[ii + 5] = ny;
+      for (int k = 0; k < ny; ++k) F[ff + 3 + k] = SpeciesDb::as_number(y->arr[k], &ok);
+      const Json* low = pr.get("low RH");
+      if (!low) {
+        *err = "Missing 'low RH' value for ion pair '" + kv.first + "' in " + what;
+        return false;
+      }
+      F[ff] = SpeciesDb::as_number(*low, &ok);
+      const Json* ions = pr.get("ions");
+      std::vector<Ion> ion;
+      if (!ions || !ion_pair_ions(*ions, db, what, &ion, err)) {
+        if (!ions) *err = "Missing ions for ion pair '" + kv.first + "' in " + what;
+        return false;
+      }
+      for (const Ion& io : ion) {
+        int rel = 0;
+        if (!relative_id(reps, ph, *phase, io.name, water_ids, &rel, err)) return false;
+        if (io.charge > 0) {
+          I[ii + 1] = io.qty;
+          F[ff + 1] = io.mw;
+          I[ii + 3] = rel;
+        } else {
+          I[ii + 2] = io.qty;
+          F[ff + 2] = io.mw;
+          I[ii + 4] = rel;
+        }
+      }
+      ii += 6 + 3 * np;
+      ff += 3 + ny;
+    } else {
+      const Json* ions = pr.get("ions");
+      const int ni = ions ? (int)ions->obj.size() : 0;
+      const Json *nw = pr.get("NW"), *zw = pr.get("ZW"), *mw = pr.get("MW");
+      if (!nw || !zw || !mw) {
+        *err = "Missing NW, ZW or MW for ion pair '" + kv.first + "' in " + what;
+        return false;
+      }
+      F[ff] = SpeciesDb::as_number(*nw, &ok);
+      F[ff + 1] = SpeciesDb::as_number(*zw, &ok);
+      F[ff + 2] = SpeciesDb::as_number(*mw, &ok);
+      I[ii] = 2;
+      I[ii + 1] = ni;
+      for (int k = 0; k < ni; ++k) {
+        const std::string& iname = ions->obj[k].first;
+        double imw = 0.0;
+        if (!db.spec.count(iname) || !db.number(iname, "molecular weight [kg mol-1]", &imw, err)) {
+          *err = "Missing molecular weight for ion '" + iname + "' in " + what;
+          return false;
+        }
+        F[ff + 3 + k] = imw;
+        if (!relative_id(reps, ph, *phase, iname, water_ids, &I[ii + 2 + np + k], err))
+          return false;
+      }
+      ii += 2 + np + (1 + np) * ni;
+      ff += 3 + ni;
+    }
+  }
+  if (!ok) {
+    *err = "non-numeric parameter in " + what;
+    return false;
+  }
+  out->type = 2;
+  out->ints = std::move(I);
+  out->floats = std::move(F);
+  out->n_env = 1;
+  return true;
+}
+
+// sub_model_PDFiTE_t%initialize (src/sub_models/sub_model_PDFiTE.F90:
+// 250-700): the ion pairs of "calculate for" in order, then every further
+// interaction partner in order of first appearance (no interactions of its
+// own); ints and floats start at 9999 as the Fortran packer leaves unused
+// slots
+bool pack_pdfite(const Json& o, const SpeciesDb& db, const std::map<std::string, int>& gas_index,
+                 const std::vector<Rep>& reps, const std::vector<LoadedPhase>& ph,
+                 LoadedSubModel* out, std::string* err) {
+  const std::string what = "PD-FiTE activity sub-model";
+  const std::string* phase = json_str(o, "aerosol phase");
+  const std::string* water = json_str(o, "aerosol-phase water");
+  const std::string* gw = json_str(o, "gas-phase water");
+  if (!phase || !water || !gw) {
+    *err = what + ": missing aerosol phase, aerosol-phase water or gas-phase water";
+    return false;
+  }
+  const std::vector<int> water_ids = instance_ids(reps, ph, *phase, *water);
+  const int np = (int)water_ids.size();
+  if (np == 0) {
+    *err = "Aerosol phase '" + *phase + "' not present in any aerosol representation for " + what;
+    return false;
+  }
+  if (!gas_index.count(*gw)) {
+    *err = "Cannot find gas-phase water species '" + *gw + "' for " + what;
+    return false;
+  }
+  const Json* calc = o.get("calculate for");
+  std::vector<std::string> names;
+  int n_inter = 0, n_flt_inter = 0;
+  if (calc)
+    for (const auto& kv : calc->obj) names.push_back(kv.first);
+  if (calc)
+    for (const auto& kv : calc->obj) {
+      const Json* inter = kv.second.get("interactions");
+      if (!inter) continue;
+      for (const Json& it : inter->arr) {
+        ++n_inter;
+        const Json* b = it.get("B");
+        n_flt_inter += 2 + (b ? (int)b->arr.size() : 0);
+        const std::string* ip = json_str(it, "ion pair");
+        if (!ip) {
+          *err = "Missing ion pair of an interaction in " + what;
+          return false;
+        }
+        if (std::find(names.begin(), names.end(), *ip) == names.end()) names.push_back(*ip);
+      }
+    }
+  const int n = (int)names.size(), n_calc = calc ? (int)calc->obj.size() : 0;
+  const int n_int = 5 + np + 3 * n_inter + (8 + (1 + 2 * n) * np) * n;
+  const int n_flt = n_flt_inter + 4 * n;
+  std::vector<int> I(n_int, 9999);
+  std::vector<double> F(n_flt, 9999.0);
+  I[0] = np;
+  I[1] = gas_index.at(*gw);
+  I[2] = n;
+  I[3] = n_int;
+  I[4] = n_flt;
+  for (int p = 0; p < np; ++p) I[5 + p] = water_ids[p];
+  int ii = 5 + np + 2 * n, ff = 0;
+  bool ok = true;
+  for (int x = 0; x < n; ++x) {
+    const std::string& pname = names[x];
+    I[5 + np + x] = ii + 1;
+    I[5 + np + n + x] = ff + 1;
+    if (!db.spec.count(pname) || db.var_type(pname) != kActivity) {
+      *err = "Ion pair '" + pname + "' must have type ION_PAIR in " + what;
+      return false;
+    }
+    if (!relative_id(reps, ph, *phase, pname, water_ids, &I[ii], err)) return false;
+    const Json* ions = db.prop(pname, "ions");
+    std::vector<Ion> ion;
+    if (!ions || !ion_pair_ions(*ions, db, what, &ion, err)) {
+      if (!ions) *err = "Missing ions for ion pair '" + pname + "' in " + what;
+      return false;
+    }
+    for (const Ion& io : ion) {
+      int rel = 0;
+      if (!relative_id(reps, ph, *phase, io.name, water_ids, &rel, err)) return false;
+      if (io.charge > 0) {
+        I[ii + 1] = io.qty;
+        F[ff] = io.mw;
+        I[ii + 3] = rel;
+      } else {
+        I[ii + 2] = io.qty;
+        F[ff + 1] = io.mw;
+        I[ii + 4] = rel;
+      }
+    }
+    ff += 4;
+    const int base = ii;
+    ii += 6 + (1 + 2 * n) * np;
+    if (x < n_calc) {
+      const Json* inter = calc->obj[x].second.get("interactions");
+      const int ni = inter ? (int)inter->arr.size() : 0;
+      I[base + 5] = ni;
+      const int ob = base + 6 + (1 + 2 * n) * np;
+      for (int y = 0; y < ni; ++y) {
+        const Json& it = inter->arr[y];
+        I[ob + 2 * ni + y] = ff + 1;
+        I[ob + ni + y] =
+            (int)(std::find(names.begin(), names.end(), *json_str(it, "ion pair")) -
+                  names.begin()) + 1;
+        const Json *lo = it.get("min RH"), *hi = it.get("max RH"), *b = it.get("B");
+        if (!lo || !hi || !b) {
+          *err = "Missing min RH, max RH or B for ion pair '" + pname + "' in " + what;
+          return false;
+        }
+        const double vlo = SpeciesDb::as_number(*lo, &ok), vhi = SpeciesDb::as_number(*hi, &ok);
+        if (!(vlo >= 0.0 && vlo < 1.0) || !(vhi > 0.0 && vhi <= 1.0)) {
+          *err = "Invalid RH range for ion pair '" + pname + "' in " + what;
+          return false;
+        }
+        const int nb = (int)b->arr.size();
+        I[ob + y] = nb;
+        F[ff] = vlo;
+        F[ff + 1] = vhi;
+        for (int z = 0; z < nb; ++z) F[ff + 2 + z] = SpeciesDb::as_number(b->arr[z], &ok);
+        ff += 2 + nb;
+        ii += 3;
+      }
+    } else {
+      I[base + 5] = 0;
+    }
+  }
+  if (!ok) {
+    *err = "non-numeric parameter in " + what;
+    return false;
+  }
+  out->type = 3;
+  out->ints = std::move(I);
+  out->floats = std::move(F);
+  out->n_env = 1;
+  return true;
+}
+
 }  // namespace
 
 int LoadedMechanism::n_int() const {
@@ -844,8 +1190,16 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
   SpeciesDb db;
   std::vector<std::pair<std::string, std::vector<const Json*>>> mechs;
   std::vector<std::pair<std::string, std::vector<std::string>>> phase_json;
-  std::vector<const Json*> rep_json;
+  std::vector<const Json*> rep_json, sub_json;
   bool have_rel = false;
+  // camp_core keeps the sub-models in priority order: a new one goes before
+  // the first of larger priority (src/camp_core.F90:575-605; ZSR 1, PD-FiTE 2,
+  // src/sub_models/sub_model_ZSR_aerosol_water.F90:705-714,
+  // src/sub_models/sub_model_PDFiTE.F90:865-874)
+  auto priority = [](const Json* o) {
+    const Json* t = o->get("type");
+    return t && t->str == "SUB_MODEL_ZSR_AEROSOL_WATER" ? 1.0 : 2.0;
+  };
   for (size_t f = 0; f < files.size(); ++f) {
     if (!read_json_file(files[f], &docs[f], err)) return false;
     const Json* data = docs[f].get("camp-data");
@@ -885,8 +1239,19 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
         }
         rep_json.push_back(&o);
       } else if (type.rfind("SUB_MODEL_", 0) == 0) {
-        *err = "sub-model " + type + " is not supported";
-        return false;
+        if (type != "SUB_MODEL_ZSR_AEROSOL_WATER" && type != "SUB_MODEL_PDFITE") {
+          *err = "sub-model " + type + " is not supported";
+          return false;
+        }
+        const std::string name = o.get("name") ? o.get("name")->str : "";
+        for (const Json* q : sub_json)
+          if (q->get("name") && q->get("name")->str == name) {
+            *err = "sub-model '" + name + "' is defined twice";
+            return false;
+          }
+        size_t at = 0;
+        while (at < sub_json.size() && !(priority(&o) < priority(sub_json[at]))) ++at;
+        sub_json.insert(sub_json.begin() + (long)at, &o);
       } else if (type == "RELATIVE_TOLERANCE") {
         bool ok = true;
         const double v = o.get("value") ? SpeciesDb::as_number(*o.get("value"), &ok) : 0.0;
@@ -977,6 +1342,16 @@ bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism*
     if (r.type == kPhotolysis) r.ints[2] = next_id++;
     if (r.type == kFirstOrderLoss || r.type == kEmission || r.type == kWetDeposition)
       r.ints[0] = next_id++;
+  }
+  out->subs.clear();
+  for (const Json* o : sub_json) {
+    LoadedSubModel sm;
+    const bool zsr = o->get("type")->str == "SUB_MODEL_ZSR_AEROSOL_WATER";
+    if (!(zsr ? pack_zsr(*o, db, gas_index, reps, out->phases, &sm, err)
+              : pack_pdfite(*o, db, gas_index, reps, out->phases, &sm, err)))
+      return false;
+    sm.name = o->get("name") ? o->get("name")->str : "";
+    out->subs.push_back(std::move(sm));
   }
   out->name = mechs.empty() ? "mechanism" : mechs[0].first;
   return true;

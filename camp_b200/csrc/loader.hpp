@@ -34,6 +34,15 @@ struct LoadedRep {
   int n_env = 0;
 };
 
+// sub_model_add_condensed_data arguments (ints without the type slot)
+struct LoadedSubModel {
+  int type = 0;
+  std::string name;
+  std::vector<int> ints;
+  std::vector<double> floats;
+  int n_env = 0;
+};
+
 struct LoadedMechanism {
   std::string name;
   // state variables in order: the gas-phase species, then each aerosol
@@ -45,6 +54,8 @@ struct LoadedMechanism {
   std::vector<LoadedRxn> rxns;
   std::vector<LoadedPhase> phases;
   std::vector<LoadedRep> reps;
+  // ZSR aerosol water and PD-FiTE activity, in camp_core's priority order
+  std::vector<LoadedSubModel> subs;
   int n_int() const;
   int n_float() const;
   int n_env() const;
@@ -56,8 +67,9 @@ struct LoadedMechanism {
 // HL_PHASE_TRANSFER, AQUEOUS_EQUILIBRIUM and WET_DEPOSITION over the phase
 // instances of the representations.  Reactions whose rate the host sets (PHOTOLYSIS,
 // FIRST_ORDER_LOSS, EMISSION, WET_DEPOSITION) get ids 1, 2, ... in mechanism
-// order; representations get ids 1, 2, ... in order.  Other representation
-// types and sub-models are refused.
+// order; representations get ids 1, 2, ... in order.  SUB_MODEL_ZSR_AEROSOL_
+// WATER and SUB_MODEL_PDFITE are packed in camp_core's priority order; other
+// representation types and sub-models are refused.
 bool load_mechanism_json(const std::vector<std::string>& files, LoadedMechanism* out,
                          std::string* err);
 

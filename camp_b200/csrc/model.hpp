@@ -269,6 +269,9 @@ class Model {
   bool add_sub_model(int type, int n_int, int n_float, int n_env, const int* ints,
                      const double* floats, std::string* err);
   int n_sub_model() const { return (int)sub_type_.size(); }
+  int sub_model_type(int k) const { return sub_type_[k]; }
+  const std::vector<int>& sub_model_int(int k) const { return sub_int_[k]; }
+  const std::vector<double>& sub_model_float(int k) const { return sub_flt_[k]; }
   // the sub-model parameter Jacobian (CSC over state variables, with the
   // dummy element (0, 0)) and the solver Jacobian fold as (solver id,
   // reaction-Jacobian id, parameter id) triplets

@@ -909,9 +909,9 @@ __device__ __noinline__ int dev_jac(const char* tb, const double* y, double h,
 // in the f scratch, after the partials in the J scratch), then for J the
 // parameter Jacobian P and the virtual slots V (rate partials against the
 // computed species), which the chain folds into the solver slots:
-// J[row][j] += V[row][c] * P[c][j] (src/camp_solver.c:1063-1106).  The
-// production / loss split jp / jl, where asked for, leaves the chained terms
-// out.
+// J[row][j] += V[row][c] * P[c][j] (src/camp_solver.c:1063-1106).  Where
+// the production / loss split jp / jl is asked for, each chained term adds to
+// the production part when positive and to the loss part when negative.
 __device__ __noinline__ int dev_f_aero(const char* tb, const double* y, double h,
                                        const double* keff, double* rates, double* fscr,
                                        double* out, int lane, double* rp = nullptr,
@@ -949,10 +949,19 @@ __device__ __noinline__ int dev_jac_aero(const char* tb, const double* y, double
   const uint32_t* ent = (const uint32_t*)(tb + o.ch_ent);
   #pragma unroll 1
   for (int g = lane; g < o.n_chain; g += 32) {
-    double s = (double)Jout[tgt[g]];
+    double s = (double)Jout[tgt[g]], sp = 0.0, sl = 0.0;
     #pragma unroll 1
-    for (int e = cptr[g]; e < cptr[g + 1]; ++e) s += V[ent[e] & 0xFFFFu] * P[ent[e] >> 16];
+    for (int e = cptr[g]; e < cptr[g + 1]; ++e) {
+      const double v = V[ent[e] & 0xFFFFu] * P[ent[e] >> 16];
+      s += v;
+      sp += v > 0.0 ? v : 0.0;
+      sl += v < 0.0 ? -v : 0.0;
+    }
     Jout[tgt[g]] = (JT)s;
+    if (jp) {
+      jp[tgt[g]] += sp;
+      jl[tgt[g]] += sl;
+    }
   }
   __syncwarp();
   return 0;

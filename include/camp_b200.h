@@ -376,9 +376,10 @@ int camp_b200_json_tolerances(void *solver_data, double *abs_tol, double *rel_to
 int camp_b200_get_var_type(void *solver_data, int *out);
 int camp_b200_rxn_float_data_size(void *solver_data);
 int camp_b200_get_rxn_float_data(void *solver_data, double *out);
-/* condensed data of aerosol phase (which 0) or representation (which 1)
- * `index` as added (aero_phase_add_condensed_data /
- * aero_rep_add_condensed_data; a representation's element counts are
+/* condensed data of aerosol phase (which 0), representation (which 1) or
+ * sub-model (which 2; ints without the type slot) `index` as added
+ * (aero_phase_add_condensed_data / aero_rep_add_condensed_data /
+ * sub_model_add_condensed_data; a representation's element counts are
  * written at solver_initialize): sizes into n_int / n_float and, where
  * non-NULL, the arrays; -1 for a bad index */
 int camp_b200_get_aero_data(void *solver_data, int which, int index, int *n_int,

@@ -148,9 +148,58 @@ def test_mod37_shipped_solve_matches_oracle(mod37_shipped, precision):
     """The shipped MONARCH mod37 test configuration: the ZSR sub-model
     computes the sulfate mode's aerosol water and PD-FiTE four ion-pair
     activity coefficients before every f and J, and the Jacobian chains
-    their parameter partials (J_rxn x J_params) into the solver Jacobian."""
-    _check_solve(mod37_shipped, precision=precision, seed=23 + precision,
-                 bulk_rel=1e-7 if precision == 0 else 1e-4)
+    their parameter partials (J_rxn x J_params) into the solver Jacobian.
+
+    Its fast aqueous equilibria make the outcome of a few log-uniform cells
+    (TOO_MUCH_WORK or not) depend on roundoff, so the per-cell outcomes are
+    held to the oracle's own floor: the oracle against itself with its
+    inputs perturbed at the form's resolution (1e-15 FP64, 1e-7 mixed).
+    Finished values and accuracy are checked as for the other mechanisms."""
+    import os
+
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import Solver
+    from oracle.oracle import OracleModel
+
+    mech, n = mod37_shipped, 192
+    cells = make_cells(mech, n, 23)
+    atol = np.full(mech.n_state_var, 1e-8)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=atol, rel_tol=1e-4)
+    s.set_precision(precision)
+    s.set_photo_rates(cells.photo_rates)
+    g = cells.state.copy()
+    s.solve(g, cells.env, 0.0, 60.0)
+    gst = s.cell_stats()["status"]
+    om = OracleModel(mech)
+    nt = os.cpu_count() or 1
+    _, cst, _, c = om.solve(cells.state.copy(), cells.env, cells.photo_rates, 0.0, 60.0, 1e-4,
+                            atol, n_threads=nt)
+    pert = cells.state.copy()
+    dep = mech.dep_index()
+    rng = np.random.default_rng(5)
+    pert[:, dep] *= 1.0 + (1e-15 if precision == 0 else 1e-7) * rng.standard_normal((n, len(dep)))
+    _, pst, _, _ = om.solve(pert, cells.env, cells.photo_rates, 0.0, 60.0, 1e-4, atol,
+                            n_threads=nt)
+    _, tst, _, tight = om.solve(cells.state.copy(), cells.env, cells.photo_rates, 0.0, 60.0,
+                                1e-8, np.full(mech.n_state_var, 1e-12), max_steps=100000,
+                                n_threads=nt)
+    floor = float(np.mean(pst == cst))
+    agree = float(np.mean(gst == cst))
+    print(f"\nshipped mod37, precision {precision}: outcome agreement {agree:.3f}, oracle floor "
+          f"{floor:.3f}; finished GPU {int((gst == 0).sum())}, oracle {int((cst == 0).sum())}")
+    assert agree >= floor - 0.03
+    ok = (gst == 0) & (cst == 0)
+    assert ok.sum() >= 0.5 * n
+    x, y = g[ok][:, dep], c[ok][:, dep]
+    big = np.abs(y) > 1e-6
+    assert np.median(np.abs(x - y)[big] / np.abs(y)[big]) < (1e-7 if precision == 0 else 1e-4)
+    both = ok & (tst == 0)
+    assert both.sum() >= 0.4 * n
+    eg = _tol_units(mech, g, tight, both)
+    ec = _tol_units(mech, c, tight, both)
+    assert np.median(eg) <= 2.0 * np.median(ec) + 1.0
+    assert np.percentile(eg, 90) <= 2.0 * np.percentile(ec, 90) + 5.0
 
 
 def test_aerosol_update_data_sets_columns(mod37_soa):

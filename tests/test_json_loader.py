@@ -59,8 +59,8 @@ def _compare(files, aerosol=False):
         lib.camp_b200_get_rxn_float_data(h, fa)
         py.lib.camp_b200_get_rxn_float_data(py._h, fb)
         np.testing.assert_array_equal(fa, fb)
-        # aerosol phases and representations as added
-        for which, objs in ((0, mech.aero_phases), (1, mech.aero_reps)):
+        # aerosol phases, representations and sub-models as added
+        for which, objs in ((0, mech.aero_phases), (1, mech.aero_reps), (2, mech.sub_models)):
             for k, o in enumerate(objs):
                 ni_, nf_ = C.c_int(), C.c_int()
                 assert lib.camp_b200_get_aero_data(h, which, k, C.byref(ni_), C.byref(nf_),
@@ -194,6 +194,18 @@ def test_mod37_aerosol_from_reference_files():
     _compare([os.path.join(REF_MOD37, f) for f in MOD37_AERO_FILES], aerosol=True)
 
 
+@pytest.mark.skipif(not os.path.isdir(REF_MOD37), reason="reference tree not present")
+def test_mod37_shipped_from_reference_files():
+    """test/monarch/config_monarch_mod37.json as shipped: its ZSR
+    aerosol-water and PD-FiTE activity sub-models packed by the C++ reader
+    exactly as the Python packer does."""
+    from camp_b200.mechanism import expand_config
+
+    cfg = os.path.join(REF_ROOT, "test", "monarch", "config_monarch_mod37.json")
+    files = expand_config(cfg, lambda p: p.replace("mechanisms_run", "mechanisms"))
+    _compare(files, aerosol=True)
+
+
 def test_aerosol_options(tmp_path):
     """A mode and LINEAR / LOG bin sets over two phases, a phase split over
     two objects, SIMPOL with an activity coefficient and with N*, HL and
@@ -240,15 +252,16 @@ def test_aerosol_options(tmp_path):
     _compare([p], aerosol=True)
 
 
-@pytest.mark.parametrize("obj", [
-    {"name": "sp", "type": "AERO_REP_SINGLE_PARTICLE"},
-    {"name": "zsr", "type": "SUB_MODEL_ZSR_AEROSOL_WATER"},
+@pytest.mark.parametrize("obj,msg", [
+    ({"name": "sp", "type": "AERO_REP_SINGLE_PARTICLE"}, "AERO_REP_SINGLE_PARTICLE"),
+    ({"name": "u", "type": "SUB_MODEL_UNIFAC"}, "SUB_MODEL_UNIFAC"),
+    ({"name": "zsr", "type": "SUB_MODEL_ZSR_AEROSOL_WATER"}, "missing aerosol phase"),
 ])
-def test_unsupported_aerosol_objects(tmp_path, obj):
+def test_unsupported_aerosol_objects(tmp_path, obj, msg):
     p = os.path.join(tmp_path, "x.json")
     with open(p, "w") as fh:
         json.dump({"camp-data": [{"name": "A", "type": "CHEM_SPEC"}, obj]}, fh)
     lib = _lib.load()
     arr = (C.c_char_p * 1)(p.encode())
     assert not lib.camp_b200_solver_from_json(arr, 1, 1)
-    assert obj["type"] in _lib.last_error()
+    assert msg in _lib.last_error()
