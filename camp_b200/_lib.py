@@ -63,7 +63,8 @@ EXPORTED = [
     "camp_b200_get_aero_data",
     "camp_b200_server_new", "camp_b200_server_add_solver",
     "camp_b200_server_submit", "camp_b200_server_wait", "camp_b200_server_pending",
-    "camp_b200_server_free",
+    "camp_b200_server_free", "camp_b200_server_open_column", "camp_b200_server_submit_column",
+    "camp_b200_server_read_column", "camp_b200_server_close_column",
 ]
 
 _lib = None
@@ -184,6 +185,14 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_server_pending.restype = ip
     lib.camp_b200_server_pending.argtypes = [vp]
     lib.camp_b200_server_free.argtypes = [vp]
+    lib.camp_b200_server_open_column.restype = C.c_long
+    lib.camp_b200_server_open_column.argtypes = [vp, ip, vp, ip]
+    lib.camp_b200_server_submit_column.restype = C.c_long
+    lib.camp_b200_server_submit_column.argtypes = [vp, C.c_long, vp, vp, dp, dp]
+    lib.camp_b200_server_read_column.restype = ip
+    lib.camp_b200_server_read_column.argtypes = [vp, C.c_long, vp]
+    lib.camp_b200_server_close_column.restype = ip
+    lib.camp_b200_server_close_column.argtypes = [vp, C.c_long]
     _lib = lib
     return lib
 

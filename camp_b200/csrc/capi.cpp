@@ -987,6 +987,36 @@ int camp_b200_server_pending(void* server) {
 
 void camp_b200_server_free(void* server) { delete static_cast<campb::Server*>(server); }
 
+long camp_b200_server_open_column(void* server, int mech, const double* state, int n_cells) {
+  std::string err;
+  const long id = static_cast<campb::Server*>(server)->open_column(mech, state, n_cells, &err);
+  if (id < 0) set_error("camp_b200_server_open_column: " + err);
+  return id;
+}
+
+long camp_b200_server_submit_column(void* server, long column, const double* env,
+                                    const double* photo, double t_initial, double t_final) {
+  std::string err;
+  const long id = static_cast<campb::Server*>(server)->submit_column(column, env, photo,
+                                                                      t_initial, t_final, &err);
+  if (id < 0) set_error("camp_b200_server_submit_column: " + err);
+  return id;
+}
+
+int camp_b200_server_read_column(void* server, long column, double* state) {
+  std::string err;
+  const int rc = static_cast<campb::Server*>(server)->read_column(column, state, &err);
+  if (rc < 0) set_error("camp_b200_server_read_column: " + err);
+  return rc;
+}
+
+int camp_b200_server_close_column(void* server, long column) {
+  std::string err;
+  const int rc = static_cast<campb::Server*>(server)->close_column(column, &err);
+  if (rc < 0) set_error("camp_b200_server_close_column: " + err);
+  return rc;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

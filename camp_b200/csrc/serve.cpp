@@ -15,6 +15,12 @@
 // returned to the budgets.  Each cell's integration is independent of which
 // request, batch, slot or SM runs it, so a result is the same alone and in
 // the mix.
+//
+// A device-resident column keeps its concentrations in the device budget
+// between its host steps: a step copies them into the batch and back with
+// device-to-device copies, so only the step's env and host-set rates cross
+// PCIe.  A column's steps run in submission order, one at a time; other
+// requests pass a column whose previous step is still running.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -45,6 +51,7 @@ size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 struct Server::Req {
   long id = 0;
   int mech = 0;
+  long column = -1;         // device-resident column, or -1 (caller's state)
   double* state = nullptr;  // caller's arrays
   const double* env = nullptr;
   const double* photo = nullptr;
@@ -210,7 +217,8 @@ void Server::loop() {
       s.batch.reset();
       progress = true;
     }
-    // admissions: the oldest request and every later queued request of its
+    // admissions: the oldest admissible request (a column's step waits for
+    // its previous one) and every later admissible queued request of its
     // mechanism (up to max_batch_cells_) form the next batch
     while (!queue_.empty()) {
       int free_slot = -1;
@@ -220,16 +228,25 @@ void Server::loop() {
           break;
         }
       if (free_slot < 0) break;
-      const int mech = requests_[queue_.front()]->mech;
-      std::vector<long> take;
-      int cells = 0;
+      std::vector<long> take, cols;
+      int cells = 0, mech = -1;
       for (long id : queue_) {
         const Req& r = *requests_[id];
-        if (r.mech != mech) continue;
+        if (mech >= 0 && r.mech != mech) continue;
+        if (r.column >= 0 && (columns_[r.column].running ||
+                              std::find(cols.begin(), cols.end(), r.column) != cols.end())) {
+          // a later step of a column waits behind its earlier one
+          if (std::find(cols.begin(), cols.end(), r.column) == cols.end())
+            cols.push_back(r.column);
+          continue;
+        }
         if (!take.empty() && cells + r.n > max_batch_cells_) break;
+        mech = r.mech;
         take.push_back(id);
         cells += r.n;
+        if (r.column >= 0) cols.push_back(r.column);
       }
+      if (take.empty()) break;
       // shrink the batch until its buffers fit what the budgets have free
       char *d = nullptr, *h = nullptr;
       size_t bytes = 0;
@@ -249,6 +266,8 @@ void Server::loop() {
         take.resize(keep);
       }
       if (take.empty()) break;  // the head waits until memory frees up
+      for (long id : take)
+        if (requests_[id]->column >= 0) columns_[requests_[id]->column].running = true;
       auto b = std::make_unique<Batch>();
       b->mech = mech;
       b->reqs = take;
@@ -287,8 +306,9 @@ void Server::start(std::unique_ptr<Batch> bp, int slot) {
     Req& r = *requests_[id];
     r.t_start = now;
     b.first.push_back(c0);
-    std::memcpy(b.h_buf + sizeof(double) * (size_t)c0 * m.n_state, r.state,
-                sizeof(double) * (size_t)r.n * m.n_state);
+    if (r.column < 0)
+      std::memcpy(b.h_buf + sizeof(double) * (size_t)c0 * m.n_state, r.state,
+                  sizeof(double) * (size_t)r.n * m.n_state);
     std::memcpy(b.h_buf + b.off_env + sizeof(double) * 2 * (size_t)c0, r.env,
                 sizeof(double) * 2 * (size_t)r.n);
     if (m.n_photo > 0)
@@ -304,13 +324,31 @@ void Server::start(std::unique_ptr<Batch> bp, int slot) {
   std::string err;
   bool ok = cudaMemcpyAsync(b.d_buf, b.h_buf, b.off_stats, cudaMemcpyHostToDevice, s.stream) ==
             cudaSuccess;
+  // resident columns: their concentrations from the device, after the host
+  // range above (stream order)
+  for (size_t k = 0; k < b.reqs.size() && ok; ++k) {
+    const Req& r = *requests_[b.reqs[k]];
+    if (r.column < 0) continue;
+    ok = cudaMemcpyAsync(b.d_buf + sizeof(double) * (size_t)b.first[k] * m.n_state,
+                         columns_[r.column].d_state, sizeof(double) * (size_t)r.n * m.n_state,
+                         cudaMemcpyDeviceToDevice, s.stream) == cudaSuccess;
+  }
   ok = ok && m.engine->launch_solve_slot(
                  (double*)b.d_buf, (const double*)(b.d_buf + b.off_env),
                  (const double*)(b.d_buf + b.off_photo), (CellStats*)(b.d_buf + b.off_stats),
                  (const double*)(b.d_buf + b.off_tspan), n, m.settings, s.scratch,
                  s.scratch_bytes, m.engine->sm_count(), s.stream, &err);
-  ok = ok && cudaMemcpyAsync(b.h_buf, b.d_buf, sizeof(double) * (size_t)n * m.n_state,
-                             cudaMemcpyDeviceToHost, s.stream) == cudaSuccess;
+  // results: a caller's column back to the host, a resident column back to
+  // its device memory
+  for (size_t k = 0; k < b.reqs.size() && ok; ++k) {
+    const Req& r = *requests_[b.reqs[k]];
+    const size_t off = sizeof(double) * (size_t)b.first[k] * m.n_state;
+    const size_t len = sizeof(double) * (size_t)r.n * m.n_state;
+    ok = (r.column < 0 ? cudaMemcpyAsync(b.h_buf + off, b.d_buf + off, len,
+                                         cudaMemcpyDeviceToHost, s.stream)
+                       : cudaMemcpyAsync(columns_[r.column].d_state, b.d_buf + off, len,
+                                         cudaMemcpyDeviceToDevice, s.stream)) == cudaSuccess;
+  }
   ok = ok && cudaMemcpyAsync(b.h_buf + b.off_stats, b.d_buf + b.off_stats,
                              sizeof(CellStats) * (size_t)n, cudaMemcpyDeviceToHost,
                              s.stream) == cudaSuccess;
@@ -342,10 +380,16 @@ void Server::finish(Batch& b) {
       r.stats.resize(r.n);
       std::memcpy(r.stats.data(), b.h_buf + b.off_stats + sizeof(CellStats) * (size_t)c0,
                   sizeof(CellStats) * (size_t)r.n);
-      std::memcpy(r.state, b.h_buf + sizeof(double) * (size_t)c0 * m.n_state,
-                  sizeof(double) * (size_t)r.n * m.n_state);
+      if (r.column < 0)
+        std::memcpy(r.state, b.h_buf + sizeof(double) * (size_t)c0 * m.n_state,
+                    sizeof(double) * (size_t)r.n * m.n_state);
       for (const auto& c : r.stats)
         if (c.status != 0) r.rc = 1;
+    }
+    if (r.column >= 0) {
+      Column& col = columns_[r.column];
+      col.running = false;
+      --col.queued;
     }
     r.t_done = now;
     r.done = true;
@@ -374,6 +418,96 @@ int Server::wait(long id, double* latency_ms, std::vector<CellStats>* stats, std
 int Server::pending() {
   std::lock_guard<std::mutex> lk(mu_);
   return (int)requests_.size();
+}
+
+long Server::open_column(int mech, const double* state, int n, std::string* err) {
+  std::lock_guard<std::mutex> lk(mu_);
+  if (mech < 0 || mech >= (int)mechs_.size() || n <= 0 || !state) {
+    *err = "invalid column";
+    return -1;
+  }
+  const size_t bytes = sizeof(double) * (size_t)n * mechs_[mech].n_state;
+  char* d = dev_.alloc(bytes);
+  if (!d) {
+    *err = "the device budget has no room for the column";
+    return -1;
+  }
+  if (cudaMemcpy(d, state, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    dev_.release(d);
+    *err = "column copy to the device failed";
+    return -1;
+  }
+  Column c;
+  c.mech = mech;
+  c.n = n;
+  c.d_state = d;
+  const long id = next_column_++;
+  columns_[id] = c;
+  return id;
+}
+
+long Server::submit_column(long column, const double* env, const double* photo, double t0,
+                           double t1, std::string* err) {
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = columns_.find(column);
+  if (it == columns_.end() || !env) {
+    *err = "unknown column or no env";
+    return -1;
+  }
+  const Mech& m = mechs_[it->second.mech];
+  if (m.n_photo > 0 && !photo) {
+    *err = "the mechanism has host-set rates: they are required";
+    return -1;
+  }
+  auto r = std::make_unique<Req>();
+  r->id = next_id_++;
+  r->mech = it->second.mech;
+  r->column = column;
+  r->env = env;
+  r->photo = photo;
+  r->n = it->second.n;
+  r->t0 = t0;
+  r->t1 = t1;
+  r->t_submit = now_s();
+  ++it->second.queued;
+  const long id = r->id;
+  queue_.push_back(id);
+  requests_[id] = std::move(r);
+  cv_.notify_all();
+  return id;
+}
+
+bool Server::column_idle(long column) {
+  auto it = columns_.find(column);
+  return it == columns_.end() || it->second.queued == 0;
+}
+
+int Server::read_column(long column, double* state, std::string* err) {
+  std::unique_lock<std::mutex> lk(mu_);
+  if (!columns_.count(column) || !state) {
+    *err = "unknown column";
+    return -1;
+  }
+  cv_.wait(lk, [&] { return column_idle(column); });
+  const Column& c = columns_[column];
+  if (cudaMemcpy(state, c.d_state, sizeof(double) * (size_t)c.n * mechs_[c.mech].n_state,
+                 cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *err = "column copy from the device failed";
+    return -1;
+  }
+  return 0;
+}
+
+int Server::close_column(long column, std::string* err) {
+  std::unique_lock<std::mutex> lk(mu_);
+  if (!columns_.count(column)) {
+    *err = "unknown column";
+    return -1;
+  }
+  cv_.wait(lk, [&] { return column_idle(column); });
+  dev_.release(columns_[column].d_state);
+  columns_.erase(column);
+  return 0;
 }
 
 }  // namespace campb

@@ -82,10 +82,31 @@ class Server {
   int wait(long id, double* latency_ms, std::vector<CellStats>* stats, std::string* err);
   int pending();
 
+  // Device-resident columns: the column's concentrations are copied to the
+  // device once (open_column) and stay there; each submit_column advances
+  // them over one host step, taking only the step's env and host-set rates
+  // from the host, and the next step of a column starts when its previous
+  // one is done.  read_column copies the current concentrations back (after
+  // the column's queued steps), close_column returns its memory.  Each step
+  // restarts the BDF history, as every solver_run of the reference does
+  // (CVodeReInit), so k steps of a column equal k solver_run calls.
+  long open_column(int mech, const double* state, int n, std::string* err);
+  long submit_column(long column, const double* env, const double* photo, double t0, double t1,
+                     std::string* err);
+  int read_column(long column, double* state, std::string* err);
+  int close_column(long column, std::string* err);
+
  private:
   struct Req;
   struct Batch;
   struct Slot;
+  struct Column {
+    int mech = 0, n = 0;
+    char* d_state = nullptr;  // n * n_state doubles in the device budget
+    int queued = 0;           // submitted steps not yet finished
+    bool running = false;     // a step is in a launched batch
+  };
+  bool column_idle(long column);
   struct Mech {
     Engine* engine;
     SolveSettings settings;
@@ -104,6 +125,8 @@ class Server {
   std::vector<Mech> mechs_;
   std::vector<Slot> slots_;
   std::map<long, std::unique_ptr<Req>> requests_;
+  std::map<long, Column> columns_;
+  long next_column_ = 0;
   int max_batch_cells_ = 16384;
   std::deque<long> queue_;
   long next_id_ = 0;

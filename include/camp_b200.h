@@ -345,6 +345,25 @@ int camp_b200_server_wait(void *server, long request, double *latency_ms,
 int camp_b200_server_pending(void *server);
 void camp_b200_server_free(void *server);
 
+/* Device-resident columns.  open_column copies a column's concentrations
+ * (state [n_cells*n_state_var], host) into the server's device budget once
+ * and returns the column id, or -1.  submit_column queues one host step of
+ * it: only env [n_cells*2] and photo [n_cells*n_photo] come from the host
+ * (valid until camp_b200_server_wait returns for the request id it
+ * returns); the concentrations stay on the device, and a column's steps run
+ * one after another in submission order while other requests pass them.
+ * Every step restarts the BDF history as solver_run does, so k steps equal k
+ * solver_run calls.  read_column copies the concentrations after the
+ * column's queued steps into state; close_column waits for them and returns
+ * the memory.  0 or -1 with camp_b200_last_error() set. */
+long camp_b200_server_open_column(void *server, int mech, const double *state,
+                                  int n_cells);
+long camp_b200_server_submit_column(void *server, long column, const double *env,
+                                    const double *photo, double t_initial,
+                                    double t_final);
+int camp_b200_server_read_column(void *server, long column, double *state);
+int camp_b200_server_close_column(void *server, long column);
+
 /* ---------------------------------------------------------------------- */
 /* CAMP JSON input without the Fortran camp_core                            */
 /* ---------------------------------------------------------------------- */

@@ -82,6 +82,58 @@ def test_serving_mix_equals_alone(cb05, mod37_aero):
     server.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_resident_column_equals_successive_solver_runs(cb05, mod37_aero, precision):
+    """Device-resident columns: three host steps of each column, submitted
+    back to back and interleaved with ordinary requests, give the
+    concentrations of three solver_run calls on the same cells (a column's
+    steps run in order; its concentrations never leave the device between
+    them)."""
+    from camp_b200.cells import make_cells, photo_base_rates
+    from camp_b200.serve import Server
+
+    mechs = [(cb05, photo_base_rates(cb05)), (mod37_aero, photo_base_rates(mod37_aero))]
+    solvers = [_solver(m, 160, precision=precision) for m, _ in mechs]
+    server = Server(n_slots=4, device_mb=512, host_mb=128)
+    ids = [server.add_solver(s) for s in solvers]
+    cols = []
+    for k, (mech, base) in enumerate(mechs):
+        c = make_cells(mech, 60 + 40 * k, 300 + k, photo_base=base)
+        cols.append((k, c, server.open_column(ids[k], c.state)))
+    steps = (0.0, 60.0, 360.0, 1260.0)
+    extra = []
+    col_reqs = {cid: [] for _, _, cid in cols}
+    for j in range(3):
+        for k, c, cid in cols:
+            col_reqs[cid].append(server.submit_column(cid, c.env, c.photo_rates, steps[j],
+                                                      steps[j + 1]))
+        # an ordinary request of cb05 between the column steps
+        o = make_cells(cb05, 30, 400 + j, photo_base=mechs[0][1])
+        st = o.state.copy()
+        extra.append((server.submit(ids[0], st, o.env, o.photo_rates, 0.0, 60.0), o, st))
+    for k, c, cid in cols:
+        for rid in col_reqs[cid]:
+            rc, ms, out, stats = server.wait(rid)
+            assert rc in (0, 1) and out is None and ms > 0
+        dev = server.read_column(cid)
+        s = _solver(mechs[k][0], c.n_cells, precision=precision)
+        s.set_photo_rates(c.photo_rates)
+        ref = c.state.copy()
+        for j in range(3):
+            s.solve(ref, c.env, steps[j], steps[j + 1])
+        np.testing.assert_allclose(dev, ref, rtol=RTOL, atol=0)
+        server.close_column(cid)
+    for rid, o, st in extra:
+        rc, ms, out, stats = server.wait(rid)
+        s = _solver(cb05, o.n_cells, precision=precision)
+        s.set_photo_rates(o.photo_rates)
+        alone = o.state.copy()
+        s.solve(alone, o.env, 0.0, 60.0)
+        np.testing.assert_allclose(out, alone, rtol=RTOL, atol=0)
+    assert server.pending() == 0
+    server.close()
+
+
 def test_graph_launch_keeps_results(cb05):
     """The device step launched as a CUDA graph (updated per run) gives the
     results of the plain launches, over runs with changing arguments."""
