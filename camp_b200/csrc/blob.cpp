@@ -393,6 +393,9 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
     o.n_pj = t.n_pj;
     o.sm_keff = t.sm_keff;
     o.sm_rec = w.put(rec);
+    std::vector<int> cv_state;
+    for (const SubProgram& g : t.cv) cv_state.push_back(g.state);
+    o.sm_state = w.put(u16(cv_state));
     o.sm_int = w.put(ints);
     o.sm_flt = w.put(flts);
     o.n_virt = t.n_virt;

@@ -73,6 +73,7 @@ struct BlobOff {
   // values sit after the pseudo-rates (f) or the partials (J), the
   // parameter partials and the virtual slots after the values.
   int n_cv, n_pj, sm_keff, sm_rec, sm_int, sm_flt;
+  int sm_state;  // state index of each computed species (uint16)
   // virtual Jacobian slots: partial lists (uint16 pointers, n_virt + 1, and
   // uint16 partial indices); the chain by target slot: target (uint16),
   // entry pointers (uint16, n_chain + 1), entries (uint32: virtual slot |

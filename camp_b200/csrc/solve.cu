@@ -1829,9 +1829,22 @@ __global__ void __launch_bounds__(32 * (AERO ? kMaxCellsAero : kMaxCellsPerBlock
     const double t0 = a.tspan ? a.tspan[2 * (size_t)cell] : a.t0;
     const double t1 = a.tspan ? a.tspan[2 * (size_t)cell + 1] : a.t1;
     int flag = c.integrate(t0, t1);
-    if (flag == OK)
+    if (flag == OK) {
       #pragma unroll 1
       for (int i = lane; i < c.n; i += 32) st[dep_state[i]] = c.y[i] > 0.0 ? c.y[i] : 0.0;
+      if constexpr (AERO) {
+        // the species the sub-models compute, at the final concentrations
+        const BlobOff& o = *reinterpret_cast<const BlobOff*>(smem);
+        if (o.n_cv > 0) {
+          __syncwarp();
+          double* cv = c.rates + o.n_rates;
+          sub_model_eval(smem, c.y, c.keff, cv, nullptr, lane);
+          const uint16_t* cs = (const uint16_t*)(smem + o.sm_state);
+          #pragma unroll 1
+          for (int k = lane; k < o.n_cv; k += 32) st[cs[k]] = cv[k];
+        }
+      }
+    }
     if (lane == 0) {
       CellStats s;
       s.status = flag;

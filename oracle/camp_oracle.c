@@ -2916,6 +2916,8 @@ static void *solve_job(void *arg) {
         st[i] = y[d] > 0.0 ? y[d] : 0.0;
         ++d;
       }
+    /* the species the sub-models compute, at the final concentrations */
+    if (m->n_sub > 0) sub_calculate(m, st, re);
   }
   free(wk.mem);
   free(atol);
