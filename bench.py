@@ -54,6 +54,7 @@ MOD37_AERO_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_aero.mech
 # test/monarch/config_monarch_mod37.json as shipped (with the ZSR / PD-FiTE
 # sub-models)
 MOD37_SHIPPED_FILE = os.path.join(ROOT, "tests", "golden", "monarch_mod37_shipped.mech.json")
+MECH_FILES = {"cb05cl_ae5": MECH_FILE, "monarch_mod37_shipped": MOD37_SHIPPED_FILE}
 METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 column latency"
 # DRAM bytes (read + write) per cell of one solve launch, from an ncu capture
 # of the solve kernel on 2 000 cells (3.19 MB); the launch's traffic grows
@@ -70,6 +71,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=100000)
+    ap.add_argument("--mech", default="cb05cl_ae5", choices=sorted(MECH_FILES),
+                    help="mechanism of the main workload (cb05cl_ae5 is the metric's)")
     ap.add_argument("--dt", type=float, default=60.0)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
@@ -261,7 +264,7 @@ def run_reference_arm(args):
         return
     from camp_b200.mechanism import Mechanism
 
-    mech = Mechanism.load(MECH_FILE)
+    mech = Mechanism.load(MECH_FILES[args.mech])
     positions = sequence_positions(args.steps, args.warmup)
     cb = cpu_sample_run(mech, args.cpu_sample, positions, args.dt, args.max_steps,
                         args.cpu_one_core)
@@ -508,7 +511,7 @@ def run_gpu_arm(args):
     from camp_b200.mechanism import Mechanism
     from camp_b200.solver import FP64, MIXED, Solver
 
-    mech = Mechanism.load(MECH_FILE)
+    mech = Mechanism.load(MECH_FILES[args.mech])
     n = args.cells
     from camp_b200 import replicas
 
@@ -683,7 +686,7 @@ def run_gpu_arm(args):
                  if prec == MIXED else "f64",
         "data": "synthetic",
         "config": {
-            "workload": f"cb05cl_ae5, {n} cells per GPU, host steps of {args.dt:g} s "
+            "workload": f"{args.mech}, {n} cells per GPU, host steps of {args.dt:g} s "
                         "(10-step sequence), rtol 1e-4, atol 1e-8 ppm, max "
                         f"{args.max_steps} internal steps; value counts cells that finish "
                         "their host step",
