@@ -614,12 +614,15 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
     set_error("camp_b200_autotune: host to device copy failed");
     return -1;
   }
-  // candidates: resident cells per block, where the Nordsieck history lives,
-  // and the LU strategy; the precision and kernel organisation stay as set
+  // candidates: the warp-per-cell kernel with its resident cells per block,
+  // where the Nordsieck history lives and the LU strategy, and the
+  // lane-per-cell kernel (32 cells per warp) where the mechanism has its
+  // tables; the precision stays as set
   campb::SolveSettings base = s->settings, best = s->settings;
   double best_ms = -1.0;
   const bool cost_order = s->cost_order;
   s->cost_order = false;
+  std::vector<campb::SolveSettings> cands;
   for (int lu = 0; lu <= 1; ++lu)
     for (int hg = 0; hg <= 1; ++hg) {
       campb::SolveSettings c = base;
@@ -633,21 +636,29 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
       for (int w : ws) {
         c.warps_per_block = w;
         c.blocks_per_sm = 1;
-        s->settings = c;
-        if (cudaMemcpyAsync(ds, state, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            !run_common(s, ds, de, n_cells, t_initial, t_final, st, true)) {
-          s->settings = base;
-          s->cost_order = cost_order;
-          set_error("camp_b200_autotune: trial run failed: " + std::string(camp_b200_last_error()));
-          return -1;
-        }
-        const double ms = s->engine->last_kernel_ms();
-        if (best_ms < 0.0 || ms < best_ms) {
-          best_ms = ms;
-          best = c;
-        }
+        cands.push_back(c);
       }
     }
+  if (s->engine->lane_tables()) {
+    campb::SolveSettings c = base;
+    c.kernel = 1;
+    cands.push_back(c);
+  }
+  for (const campb::SolveSettings& c : cands) {
+    s->settings = c;
+    if (cudaMemcpyAsync(ds, state, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        !run_common(s, ds, de, n_cells, t_initial, t_final, st, true)) {
+      s->settings = base;
+      s->cost_order = cost_order;
+      set_error("camp_b200_autotune: trial run failed: " + std::string(camp_b200_last_error()));
+      return -1;
+    }
+    const double ms = s->engine->last_kernel_ms();
+    if (best_ms < 0.0 || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
   s->settings = best;
   s->tuned_ms = best_ms;
   s->cost_order = cost_order;
@@ -663,6 +674,8 @@ int camp_b200_get_tuning(void* solver_data, int* warps_per_block, int* hist_glob
   if (sample_ms) *sample_ms = s->tuned_ms;
   return 0;
 }
+
+int camp_b200_get_kernel(void* solver_data) { return S(solver_data)->settings.kernel; }
 
 int camp_b200_set_kernel(void* solver_data, int kernel, int place) {
   if (kernel != 0 && kernel != 1) {

@@ -80,6 +80,8 @@ class Engine {
   // false (with the reason) when the mechanism exceeds the warp-per-cell
   // tables, so that only the lane-per-cell kernel can run it
   bool warp_tables(std::string* err) const;
+  // the lane-per-cell kernel's tables were built (it runs this mechanism)
+  bool lane_tables() const;
   // Serving slots: a launch on caller-provided buffers and scratch (from
   // slot_scratch_bytes for at most max_blocks blocks), so several launches
   // can be in flight on different streams; d_tspan holds each cell's

@@ -2551,6 +2551,8 @@ bool Engine::warp_tables(std::string* err) const {
   return false;
 }
 
+bool Engine::lane_tables() const { return impl_->lanes_ok; }
+
 size_t Engine::slot_scratch_bytes(const SolveSettings& s, int max_blocks) const {
   const Impl* I = impl_;
   if (!I->warp_ok) return 0;

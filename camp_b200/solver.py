@@ -120,7 +120,7 @@ class Solver:
         self.lib.camp_b200_get_tuning(self._h, C.byref(w), C.byref(hg), C.byref(lu),
                                       C.byref(ms))
         return {"warps_per_block": w.value, "hist_global": hg.value, "lu_mode": lu.value,
-                "sample_ms": ms.value}
+                "sample_ms": ms.value, "kernel": int(self.lib.camp_b200_get_kernel(self._h))}
 
     def set_graph(self, enable: bool) -> None:
         """Launch each run's device step as one CUDA graph."""

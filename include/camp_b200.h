@@ -196,17 +196,22 @@ int camp_b200_set_graph(void *solver_data, int enable);
  * which leaves shared memory for more resident cells.  The autotuner picks. */
 int camp_b200_set_layout(void *solver_data, int hist_global);
 /* Autotuner: solves the given sample of cells (host buffers, state is not
- * modified) once per candidate launch configuration -- cells per block, the
- * history layout of camp_b200_set_layout and the LU mode of
- * camp_b200_set_lu_mode -- for the current precision, and keeps the fastest
- * by kernel time.  Use a sample representative of the cells to be solved
- * (a few thousand cells, the host step of the run).  0 or -1. */
+ * modified) once per candidate launch configuration -- for the warp-per-cell
+ * kernel the cells per block, the history layout of camp_b200_set_layout and
+ * the LU mode of camp_b200_set_lu_mode, and the lane-per-cell kernel (32
+ * cells per warp) where the mechanism has its tables -- for the current
+ * precision, and keeps the fastest by kernel time.  Use a sample
+ * representative of the cells to be solved (a few thousand cells, the host
+ * step of the run).  0 or -1. */
 int camp_b200_autotune(void *solver_data, const double *state, const double *env,
                        int n_cells, double t_initial, double t_final);
 /* The launch configuration in use and the autotuner's sample time (ms, -1
  * when not tuned). */
 int camp_b200_get_tuning(void *solver_data, int *warps_per_block, int *hist_global,
                          int *lu_mode, double *sample_ms);
+/* The kernel in use: 0 warp per cell, 1 lane per cell (camp_b200_set_kernel,
+ * or the autotuner's choice). */
+int camp_b200_get_kernel(void *solver_data);
 /* Orders the cells of the next run by decreasing internal step count of the
  * previous run (longest-first scheduling of the persistent kernel). */
 int camp_b200_set_cost_ordering(void *solver_data, int enable);
