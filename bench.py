@@ -99,6 +99,9 @@ def parse():
     ap.add_argument("--serve-rates", default="5,10,20,30,40",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=8.0)
+    ap.add_argument("--synth-cells", type=int, default=0,
+                    help="cells of the 200-species / 600-reaction synthetic mechanism (0: skip)")
+    ap.add_argument("--synth-dt", type=float, default=0.5)
     ap.add_argument("--serve-columns", type=int, default=256,
                     help="device-resident columns in the serving pool")
     return ap.parse_args()
@@ -451,7 +454,7 @@ def counted_flops(model: dict, stats) -> float:
 # ---------------------------------------------------------------------------
 # First host step of other mechanisms
 # ---------------------------------------------------------------------------
-def run_first_step(mech, args, dev, stream, n):
+def run_first_step(mech, args, dev, stream, n, cells=None, dt=None):
     """n seeded cells of another mechanism over the first host step of the
     sequence (every cell from its seeded state), mixed and FP64,
     device-resident, longest-first order from a previous identical run;
@@ -461,11 +464,12 @@ def run_first_step(mech, args, dev, stream, n):
     from camp_b200.cells import make_cells
     from camp_b200.solver import FP64, MIXED, Solver
 
-    cells = make_cells(mech, n, SEED)
+    cells = cells if cells is not None else make_cells(mech, n, SEED)
+    dt = args.dt if dt is None else dt
     init = torch.from_numpy(cells.state).to(dev)
     env = torch.from_numpy(cells.env).to(dev)
     photo = torch.from_numpy(np.ascontiguousarray(cells.photo_rates)).to(dev)
-    out = {"mechanism": mech.name, "cells": n, "host_step_s": args.dt,
+    out = {"mechanism": mech.name, "cells": n, "host_step_s": dt,
            "note": "first host step of the sequence, cells ordered longest-first from an "
                    "identical previous run; device time (CUDA events)"}
     for name, p in (("mixed", MIXED), ("fp64", FP64)):
@@ -482,7 +486,7 @@ def run_first_step(mech, args, dev, stream, n):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            s.launch_device(st, env, n, 0.0, args.dt, stream)
+            s.launch_device(st, env, n, 0.0, dt, stream)
             e1.record(stream)
             s.sync_status(stream)
             torch.cuda.synchronize()
@@ -647,6 +651,21 @@ def run_gpu_arm(args):
         mod37_aero = run_first_step(Mechanism.load(MOD37_AERO_FILE), args, dev, stream, 10000)
         mod37_shipped = run_first_step(Mechanism.load(MOD37_SHIPPED_FILE), args, dev, stream,
                                        10000)
+    synth = None
+    if world == 1 and args.synth_cells > 0:
+        # the seeded 200-species / 600-reaction mechanism on the lane-per-cell
+        # kernel, at the host step every oracle cell finishes (its cells gain
+        # molecules in every reaction: at 300 s none finishes)
+        import tempfile
+
+        from camp_b200.cells import make_cells
+        from camp_b200.synth import load_synthetic
+
+        with tempfile.TemporaryDirectory() as td:
+            smech, sbase = load_synthetic(td, 200, 600)
+        scells = make_cells(smech, args.synth_cells, SEED, conc_lo=1e-8, photo_base=sbase)
+        synth = run_first_step(smech, args, dev, stream, args.synth_cells, cells=scells,
+                               dt=args.synth_dt)
     fm = flop_model(mech, solver)
     if rank != 0:
         solver.free()
@@ -731,6 +750,7 @@ def run_gpu_arm(args):
         "mod37_soa": mod37_soa,
         "mod37_aero": mod37_aero,
         "mod37_shipped": mod37_shipped,
+        "synthetic_200sp_600rxn": synth,
     }
     print(json.dumps(line), flush=True)
     solver.free()
