@@ -308,9 +308,10 @@ SERVE_P99_TARGET_MS = 2500.0  # stated p99 target of the serving loop
 def serving_run(args, precision):
     """Open-loop Poisson arrivals of column steps at each rate against a pool
     of device-resident columns: 10-200 cells per column, 70 % cb05cl_ae5 and
-    30 % the shipped MONARCH mod37 configuration (cb05 + the mod37 gas,
-    aerosol, HL, aqueous-equilibrium, SOA chemistry and the ZSR / PD-FiTE
-    sub-models); each arrival advances one column of the pool by a host step
+    30 % MONARCH mod37 with its SOA scheme (cb05 + dry deposition,
+    emissions, wet deposition and SIMPOL partitioning of the 2-product SOA
+    into the modal/binned representation, the "monarch_mod37" of the
+    workload); each arrival advances one column of the pool by a host step
     of 60, 300 or 900 s (a column's steps run in order, its concentrations
     stay on the device between them).  Latency is submit-to-completion inside
     the library.  Reported: p50 / p99 per offered rate, and the highest
@@ -321,7 +322,7 @@ def serving_run(args, precision):
     from camp_b200.solver import Solver
 
     cb05 = Mechanism.load(MECH_FILE)
-    mod37 = Mechanism.load(MOD37_SHIPPED_FILE)
+    mod37 = Mechanism.load(MOD37_SOA_FILE)
     mechs = [(cb05, photo_base_rates(cb05)), (mod37, photo_base_rates(mod37))]
     solvers = []
     for m, _ in mechs:
@@ -390,11 +391,11 @@ def serving_run(args, precision):
     for s in solvers:
         s.free()
     held = [r["offered_rps"] for r in out if r["p99_ms"] <= SERVE_P99_TARGET_MS]
-    return {"mix": "70% cb05cl_ae5 / 30% monarch_mod37 as shipped (test/monarch/"
-                   "config_monarch_mod37.json: cb05 + mod37 gas, aerosol, HL, aqueous "
-                   "equilibrium, SOA and ZSR / PD-FiTE sub-models); pool of "
-                   f"{len(pool)} device-resident columns of 10-200 cells; each arrival one host "
-                   "step of 60/300/900 s of a random column; Poisson arrivals",
+    return {"mix": "70% cb05cl_ae5 / 30% monarch_mod37 with SOA (cb05 + dry deposition, "
+                   "emissions, wet deposition, SIMPOL partitioning into the modal/binned "
+                   f"representation); pool of {len(pool)} device-resident columns of 10-200 "
+                   "cells; each arrival one host step of 60/300/900 s of a random column; "
+                   "Poisson arrivals",
             "precision": "mixed" if precision == 1 else "fp64", "slots": 8,
             "seconds_per_rate": args.serve_seconds,
             "p99_target_ms": SERVE_P99_TARGET_MS,
