@@ -57,6 +57,7 @@ EXPORTED = [
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
     "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
     "camp_b200_n_mapped_values", "camp_b200_get_jac_map", "camp_b200_get_kernel",
+    "camp_b200_check_precision",
     "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_solver_from_json",
     "camp_b200_n_state_var", "camp_b200_state_name", "camp_b200_json_tolerances",
     "camp_b200_get_var_type", "camp_b200_rxn_float_data_size", "camp_b200_get_rxn_float_data",
@@ -113,6 +114,8 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_set_lu_mode.argtypes = [vp, ip]
     lib.camp_b200_autotune.restype = ip
     lib.camp_b200_autotune.argtypes = [vp, _f64p, _f64p, ip, dp, dp]
+    lib.camp_b200_check_precision.restype = ip
+    lib.camp_b200_check_precision.argtypes = [vp, _f64p, _f64p, ip, dp, _f64p]
     lib.camp_b200_get_kernel.restype = ip
     lib.camp_b200_get_kernel.argtypes = [vp]
     lib.camp_b200_get_tuning.restype = ip

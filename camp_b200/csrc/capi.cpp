@@ -917,6 +917,22 @@ int camp_b200_eval_jac(void* solver_data, const double* state, const double* env
   return 0;
 }
 
+int camp_b200_check_precision(void* solver_data, const double* state, const double* env,
+                              int n_cells, double h, double* rel_err) {
+  Solver* s = S(solver_data);
+  if (!s->ready || n_cells <= 0 || n_cells > s->n_cells || !state || !env || !rel_err) {
+    set_error("camp_b200_check_precision: solver not ready, bad sizes or missing outputs");
+    return -1;
+  }
+  std::string err;
+  if (!s->engine->check_precision(state, env, s->n_photo ? s->photo.data() : nullptr, n_cells,
+                                  h, s->settings.rtol, rel_err, &err)) {
+    set_error("camp_b200_check_precision: " + err);
+    return -1;
+  }
+  return 0;
+}
+
 int camp_b200_check_jac(void* solver_data, const double* state, const double* env, int n_cells,
                         double h, double rel_tol, double abs_tol, double* worst_rel,
                         int* n_failed) {

@@ -66,6 +66,12 @@ class Engine {
   // Finite-difference audit of the analytic Jacobian (debug tool): per cell,
   // elements that fail at every step size and the worst best-step relative
   // difference (-1: f or J could not be evaluated at this state).
+  // Precision audit: per cell, the error-weighted RMS difference between the
+  // FP32 and the FP64 solve of M = I - h J for a tolerance-sized right-hand
+  // side, relative to the FP64 solution's (-1 where f / J or a factorization
+  // fails at the state)
+  bool check_precision(const double* h_state, const double* h_env, const double* h_photo,
+                       int n_cells, double h, double rtol, double* rel_err, std::string* err);
   bool check_jac(const double* h_state, const double* h_env, const double* h_photo,
                  int n_cells, double h, double rel_tol, double abs_tol, double* worst,
                  int* nfail, std::string* err);

@@ -2057,6 +2057,64 @@ bool lanes_launch(const DevMech& m, const void* d_blob, const LaneOff& off, doub
                   void** scrlt, size_t* caplt, double t0, double t1, const SolveSettings& s,
                   int sm_count, int max_smem, void* stream, std::string* err);
 
+// Precision audit: per cell, the Jacobian at its state, M = I - h J
+// factored on the fixed order in precision LT and solved for a right-hand
+// side of tolerance size (b_i = +-(rtol |y_i| + atol_i), signs from a fixed
+// hash of i); the solution goes to x.  Run once in FP64 and once in FP32, the
+// host compares them in the error-weighted norm: the accuracy the mixed
+// form's Newton iteration has to refine.
+struct PrecArgs {
+  EvalArgs e;   // tables, layout (LU in LT), state, env, photo, h
+  void* jbuf;   // [n_cells * n_jac] of LT
+  double rtol;
+  double* x;    // [n_cells * n]
+  int* bad;     // [n_cells]: 1 when f / J or the factorization failed
+};
+
+template <typename LT>
+__global__ void precision_kernel(PrecArgs p) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ unsigned long long tma_bar;
+  const EvalArgs& a = p.e;
+  if (!stage_tables(smem, a.blob, a.stage_bytes, &tma_bar, a.err)) return;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int cell = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (cell >= a.n_cells) return;
+  char* base = smem + a.tab_bytes + (size_t)wib * a.lay.bytes;
+  const Tab t = make_tab(smem);
+  const DevMech& m = a.m;
+  double* y = (double*)(base + a.lay.y);
+  double* rates = (double*)(base + a.lay.rates);
+  double* keff = (double*)(base + a.lay.keff);
+  double* b = (double*)(base + a.lay.tempv);
+  LT* LU = (LT*)(base + a.lay.lu);
+  LT* z = (LT*)(base + a.lay.z);
+  LT* dinv = (LT*)(base + a.lay.dinv);
+  LT* J = (LT*)p.jbuf + (size_t)cell * t.n_jac;
+  const double* st = a.state + (size_t)cell * m.n_state;
+  #pragma unroll 1
+  for (int i = lane; i < t.n; i += 32) y[i] = st[t.dep_state[i]];
+  __syncwarp();
+  compute_keff(m, st, a.env[2 * cell], a.env[2 * cell + 1],
+               a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, keff, lane);
+  int r = has_simpol(smem) ? dev_jac_aero<LT>(smem, y, a.h, keff, rates, J, lane)
+                           : dev_jac<LT>(smem, y, a.h, keff, rates, J, lane);
+  bool ok = r == 0 && dev_form_factor<LT>(smem, J, a.h, LU, dinv, lane);
+  if (ok) {
+    #pragma unroll 1
+    for (int i = lane; i < t.n; i += 32) {
+      const double s = p.rtol * fabs(y[i]) + t.atol[i];
+      b[i] = ((i * 2654435761u) >> 13) & 1u ? s : -s;
+    }
+    __syncwarp();
+    dev_lsolve<LT>(smem, LU, dinv, b, z, lane);
+    #pragma unroll 1
+    for (int i = lane; i < t.n; i += 32) p.x[(size_t)cell * t.n + i] = b[i];
+  }
+  if (lane == 0) p.bad[cell] = ok ? 0 : 1;
+}
+
 struct Engine::Impl {
   DevMech m{};
   BlobOff off{};
@@ -2770,6 +2828,89 @@ bool Engine::eval_jac(const double* h_state, const double* h_env, const double* 
   CK(cudaDeviceSynchronize());
   CK(cudaMemcpy(jp, a.jp, sizeof(double) * nj, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(jl, a.jl, sizeof(double) * nj, cudaMemcpyDeviceToHost));
+  return true;
+}
+
+bool Engine::check_precision(const double* h_state, const double* h_env,
+                             const double* h_photo, int n_cells, double h, double rtol,
+                             double* rel_err, std::string* err) {
+  Impl* I = impl_;
+  if (!warp_tables(err)) return false;
+  const DevMech& m = I->m;
+  const int n = m.n;
+  const size_t ns = (size_t)n_cells * m.n_state, nx = (size_t)n_cells * n;
+  DevBuf bs, be, bp, bj, bx;
+  CK(bs.alloc(ns));
+  CK(be.alloc(2 * (size_t)n_cells));
+  CK(bp.alloc((size_t)n_cells * m.n_photo));
+  CK(bj.alloc((size_t)n_cells * m.n_jac));
+  CK(bx.alloc(2 * nx + (size_t)n_cells));
+  CK(cudaMemcpy(bs.p, h_state, sizeof(double) * ns, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(be.p, h_env, sizeof(double) * 2 * n_cells, cudaMemcpyHostToDevice));
+  if (m.n_photo > 0 && h_photo)
+    CK(cudaMemcpy(bp.p, h_photo, sizeof(double) * n_cells * m.n_photo, cudaMemcpyHostToDevice));
+  std::vector<double> x(2 * nx);
+  std::vector<int> bad(2 * (size_t)n_cells);
+  for (int pass = 0; pass < 2; ++pass) {
+    PrecArgs p{};
+    EvalArgs& a = p.e;
+    a.m = m;
+    a.off = I->off;
+    a.blob = I->d_blob;
+    a.tab_bytes = tab_bytes_of(I->off, 1);
+    a.stage_bytes = I->off.bytes;
+    a.err = I->d_counter + 1;
+    a.lay = make_layout(I->off, pass == 0 ? 8 : 4, true, true);
+    a.state = bs.p;
+    a.env = be.p;
+    a.photo = (m.n_photo > 0 && h_photo) ? bp.p : nullptr;
+    a.n_cells = n_cells;
+    a.h = h;
+    p.jbuf = bj.p;
+    p.rtol = rtol;
+    p.x = bx.p + (size_t)pass * nx;
+    p.bad = (int*)(bx.p + 2 * nx);
+    const int warps = std::max(1, std::min(8, (I->max_smem - a.tab_bytes) / a.lay.bytes));
+    const size_t smem = (size_t)a.tab_bytes + (size_t)warps * a.lay.bytes;
+    void* func = pass == 0 ? (void*)precision_kernel<double> : (void*)precision_kernel<float>;
+    CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void* args[] = {&p};
+    CK(cudaLaunchKernel(func, dim3((n_cells + warps - 1) / warps), dim3(warps * 32), args, smem,
+                        0));
+    CK(cudaGetLastError());
+    ++launches_;
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(x.data() + (size_t)pass * nx, p.x, sizeof(double) * nx,
+                  cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(bad.data() + (size_t)pass * n_cells, p.bad, sizeof(int) * n_cells,
+                  cudaMemcpyDeviceToHost));
+  }
+  // weights as the kernel's right-hand side: rtol |y| + atol per dependent
+  // variable (the atol of the blob, in dependent order)
+  std::vector<double> atol(n);
+  CK(cudaMemcpy(atol.data(), (const char*)I->d_blob + I->off.atol, sizeof(double) * n,
+                cudaMemcpyDeviceToHost));
+  std::vector<int> dep_state(n);
+  {
+    std::vector<uint16_t> ds(n);
+    CK(cudaMemcpy(ds.data(), (const char*)I->d_blob + I->off.dep_state, sizeof(uint16_t) * n,
+                  cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) dep_state[i] = ds[i];
+  }
+  for (int c = 0; c < n_cells; ++c) {
+    if (bad[c] || bad[(size_t)n_cells + c]) {
+      rel_err[c] = -1.0;
+      continue;
+    }
+    double num = 0.0, den = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double s = rtol * std::fabs(h_state[(size_t)c * m.n_state + dep_state[i]]) + atol[i];
+      const double x64 = x[(size_t)c * n + i], x32 = x[nx + (size_t)c * n + i];
+      num += ((x32 - x64) / s) * ((x32 - x64) / s);
+      den += (x64 / s) * (x64 / s);
+    }
+    rel_err[c] = den > 0.0 ? std::sqrt(num / den) : 0.0;
+  }
   return true;
 }
 

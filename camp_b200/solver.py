@@ -337,6 +337,18 @@ class Solver:
             raise SolverError(_lib.last_error())
         return nfail, worst
 
+    def check_precision(self, state, env, h: float) -> np.ndarray:
+        """Per cell, the error-weighted RMS difference of the FP32 and FP64
+        solves of I - h J at these states (see camp_b200_check_precision)."""
+        state = np.ascontiguousarray(state, np.float64)
+        env = np.ascontiguousarray(env, np.float64)
+        nc = state.shape[0]
+        out = np.zeros(nc, np.float64)
+        if self.lib.camp_b200_check_precision(self._h, state.reshape(-1), env.reshape(-1), nc,
+                                              float(h), out) < 0:
+            raise SolverError(_lib.last_error())
+        return out
+
     def eval_deriv(self, state, env, h):
         state = np.ascontiguousarray(state, np.float64)
         nc = state.shape[0]

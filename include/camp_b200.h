@@ -427,6 +427,20 @@ int camp_b200_check_jac(void *solver_data, const double *state, const double *en
                         int n_cells, double h, double rel_tol, double abs_tol,
                         double *worst_rel, int *n_failed);
 
+/* No counterpart in the reference (the check the mixed form needs): for
+ * n_cells states (host buffers) and the rates set for those cells, solves
+ * M = I - h J for a right-hand side of tolerance size (+-(rtol |y| + atol)
+ * per species) with M factored in FP32 and in FP64 on the solver's fixed
+ * order, and writes per cell the error-weighted RMS difference of the two
+ * solutions relative to the FP64 one's (-1 where f, J or a factorization
+ * fails at the state).  The mixed form's Newton iteration refines the FP32
+ * solves, which needs this well below 1: on cb05cl_ae5 and mod37 without
+ * sub-models it stays below 1e-2 at host-step sizes, on the shipped mod37
+ * configuration it reaches 0.7, where the FP64 form is the one to use.
+ * 0 or -1. */
+int camp_b200_check_precision(void *solver_data, const double *state, const double *env,
+                              int n_cells, double h, double *rel_err);
+
 #ifdef __cplusplus
 }
 #endif

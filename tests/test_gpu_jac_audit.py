@@ -30,3 +30,47 @@ def test_jacobian_matches_finite_differences(request, which, h):
     # estimate at some step (a guard switching inside every tried step would
     # be reported here, as by the reference's check)
     assert nfail.sum() <= 0.001 * n * n_jac, (nfail, worst)
+
+
+@pytest.mark.parametrize("which,limit", [("cb05", 0.05), ("mod37_aero", 0.05)])
+def test_precision_audit_small_where_mixed_is_at_equal_error(request, which, limit):
+    """The FP32 solve of I - h J at host-step sizes, against the FP64 one,
+    in the error-weighted norm: well below 1 on the mechanisms whose mixed
+    solves are at the oracle's accuracy (the Newton iteration refines it)."""
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import Solver
+
+    mech = request.getfixturevalue(which)
+    n = 32
+    cells = make_cells(mech, n, 23)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4)
+    s.set_photo_rates(cells.photo_rates)
+    for h in (0.01, 1.0, 60.0):
+        err = s.check_precision(cells.state, cells.env, h)
+        ok = err >= 0.0
+        assert ok.sum() >= n // 2
+        print(f"\n{which} h {h}: FP32 solve error median {np.median(err[ok]):.1e} "
+              f"max {err[ok].max():.1e}")
+        assert err[ok].max() < limit, (h, err[ok].max())
+
+
+def test_precision_audit_flags_the_shipped_configuration(mod37_shipped):
+    """On the shipped mod37 configuration (computed sulfate-mode water in
+    fast aqueous equilibria) the FP32 solve is far less accurate: the audit
+    flags it, and the FP64 form is the one to use there."""
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import Solver
+
+    mech = mod37_shipped
+    n = 32
+    cells = make_cells(mech, n, 23)
+    s = Solver(mech, n)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4)
+    s.set_photo_rates(cells.photo_rates)
+    err = s.check_precision(cells.state, cells.env, 1.0)
+    ok = err >= 0.0
+    assert ok.sum() >= n // 2
+    print(f"\nshipped mod37 h 1: FP32 solve error median {np.median(err[ok]):.1e} "
+          f"max {err[ok].max():.1e}")
+    assert err[ok].max() > 0.1
