@@ -435,8 +435,9 @@ int camp_b200_check_jac(void *solver_data, const double *state, const double *en
  * solutions relative to the FP64 one's (-1 where f, J or a factorization
  * fails at the state).  The mixed form's Newton iteration refines the FP32
  * solves, which needs this well below 1: on cb05cl_ae5 and mod37 without
- * sub-models it stays below 1e-2 at host-step sizes, on the shipped mod37
- * configuration it reaches 0.7, where the FP64 form is the one to use.
+ * sub-models it stays below 1e-2 at steps of 0.01-1 s (single cells reach
+ * 0.4 at a whole 60 s step), on the shipped mod37 configuration it reaches
+ * 0.7 at 1 s, where the FP64 form is the one to use.
  * 0 or -1. */
 int camp_b200_check_precision(void *solver_data, const double *state, const double *env,
                               int n_cells, double h, double *rel_err);
