@@ -59,7 +59,7 @@ METRIC = "cell-steps/s (cb05, 1e5 cells) mixed vs FP64 GPU @rtol1e-4; p50/p99 co
 # DRAM bytes (read + write) per cell of one solve launch, from an ncu capture
 # of the solve kernel on 2 000 cells (3.19 MB); the launch's traffic grows
 # with the cells it processes
-TRAFFIC_BYTES_PER_CELL = 3.187e6 / 2000
+TRAFFIC_BYTES_PER_CELL = 2.833e6 / 2000
 # nominal B200 FP64 (non-tensor) peak, for the algorithmic-flop fraction
 FP64_PEAK_TFLOPS = 40.0
 
