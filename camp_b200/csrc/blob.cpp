@@ -376,6 +376,11 @@ bool build_blob(const Tables& t, const std::vector<double>& atol_dep, std::vecto
   o.aq_rec = w.put(aq_rec);
   o.aq_sp = w.put(aq_sp);
   o.aq_sm = w.put(aq_sm);
+  {
+    std::vector<double> sim(aq_sm.size());
+    for (size_t k = 0; k < sim.size(); ++k) sim[k] = 1.0 / aq_sm[k];
+    o.aq_sim = w.put(sim);
+  }
   o.aq_cp = w.put(aq_cp);
   o.aq_cpm = w.put(aq_cpm);
   // sub-model programs, virtual slots and the chain

@@ -64,6 +64,7 @@ struct BlobOff {
   // computed participant its computed index | reactant << 15 (uint16) and
   // 1e3 / MW (double)
   int n_aq, aq_rec, aq_sp, aq_sm, aq_cp, aq_cpm;
+  int aq_sim;  // per slot MW / 1e3 (1 / aq_sm), double
   // J gather with unguarded products (SIMPOL): they lead each slot, and
   // jg_umid (uint16 per slot) is the slot's first loss entry
   int has_ug, jg_umid;

@@ -707,8 +707,8 @@ void Model::build_sub_programs() {
             g.ints.insert(g.ints.end(), {kZsrJacobson, deriv_ids_[c], deriv_ids_[a], v.zj_ny(x),
                                          param_elem_id(w, gw), param_elem_id(w, c),
                                          param_elem_id(w, a)});
-            g.flts.insert(g.flts.end(), {F[0], (double)v.zj_ncat(x), F[1], (double)v.zj_nan(x),
-                                         F[2]});
+            g.flts.insert(g.flts.end(), {F[0], 1.0 / (v.zj_ncat(x) * F[1] * 1000.0),
+                                         1.0 / (v.zj_nan(x) * F[2] * 1000.0)});
             for (int y = 0; y < v.zj_ny(x); ++y) g.flts.push_back(F[3 + y]);
           } else if (v.ztype(x) == kZsrEqsam) {
             g.ints.insert(g.ints.end(), {kZsrEqsam, v.ze_nion(x), param_elem_id(w, gw)});
@@ -717,7 +717,7 @@ void Model::build_sub_programs() {
               g.ints.insert(g.ints.end(), {deriv_ids_[s], param_elem_id(w, s)});
             }
             g.flts.insert(g.flts.end(), {F[0] * 55.51 * 18.01 / F[2] / 1000.0, F[1]});
-            for (int i = 0; i < v.ze_nion(x); ++i) g.flts.push_back(F[3 + i]);
+            for (int i = 0; i < v.ze_nion(x); ++i) g.flts.push_back(1.0 / F[3 + i]);
           } else {
             g.ints.push_back(0);  // unknown pair type: contributes nothing
           }
@@ -732,7 +732,7 @@ void Model::build_sub_programs() {
             g.ints.insert(g.ints.end(), {deriv_ids_[c], deriv_ids_[a], v.pd_ncat(j) + v.pd_nan(j),
                                          param_elem_id(gs, c), param_elem_id(gs, a)});
             const double* F = v.F + v.fl(j);
-            g.flts.insert(g.flts.end(), {F[0], F[1]});
+            g.flts.insert(g.flts.end(), {1.0 / (F[0] * 1.0e6), 1.0 / (F[1] * 1.0e6)});
           }
           for (int y = 0; y < v.pd_ninter(x); ++y) {
             g.ints.insert(g.ints.end(), {v.pd_pair(x, y), v.pd_nb(x, y)});

@@ -108,15 +108,17 @@ struct AqInst {
 //                 of d/d(gas water), d/d(cation), d/d(anion);
 //       EQSAM: ion count, parameter id of d/d(gas water), per ion its
 //              dependent index and parameter id;
-//     floats per pair: Jacobson: low RH, cation count, cation MW, anion
-//     count, anion MW, Y...; EQSAM: NW 55.51 18.01 / MW / 1000, ZW, ion MWs.
+//     floats per pair: Jacobson: low RH, 1 / (cation count x cation MW x
+//     1000), the same for the anion, Y...; EQSAM: NW 55.51 18.01 / MW / 1000,
+//     ZW, 1 / ion MW of each ion.
 //   PD-FiTE activity of pair x (kind 2), ints: kind, gas-water dependent
 //     index, pair count, x, interaction count, parameter id of d/d(gas
 //     water), per pair j: cation, anion (dependent indices), cation + anion
 //     stoichiometry, parameter ids of d/d(cation j), d/d(anion j); per
 //     interaction: its pair, B count;
-//     floats: per pair cation MW, anion MW; per interaction min RH, max RH,
-//     B...
+//     floats: per pair 1 / (cation MW x 1e6), 1 / (anion MW x 1e6) (moles
+//     per concentration, also the partials' factors); per interaction min
+//     RH, max RH, B...
 struct SubProgram {
   int state = -1;  // state index of the computed species
   std::vector<int> ints;

@@ -143,7 +143,7 @@ struct Tab {
   const uint16_t *lu_rowptr, *lu_col;
   const uint32_t *upd_ptr, *upd;
   const uint16_t *si_rec, *si_elem, *jg_umid, *aq_rec, *aq_sp, *aq_cp;
-  const double *si_ef, *aq_sm, *aq_cpm;
+  const double *si_ef, *aq_sm, *aq_cpm, *aq_sim;
   int n, n_rxn, n_jac, n_lu, n_fsplit, n_plev, n_flev, n_blev, n_simpol, has_ug, n_aq;
 };
 
@@ -179,6 +179,7 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.aq_rec = (const uint16_t*)(b + o.aq_rec);
   t.aq_sp = (const uint16_t*)(b + o.aq_sp);
   t.aq_sm = (const double*)(b + o.aq_sm);
+  t.aq_sim = (const double*)(b + o.aq_sim);
   t.aq_cp = (const uint16_t*)(b + o.aq_cp);
   t.aq_cpm = (const double*)(b + o.aq_cpm);
   t.n_aq = o.n_aq;
@@ -282,7 +283,9 @@ __device__ __forceinline__ bool rates_of(const Tab& t, const double* y, const do
 // ZSR aerosol water of one phase instance
 // (src/sub_models/sub_model_ZSR_aerosol_water.c:225-305, Jacobian :318-437)
 // from its program (SubProgram in model.hpp); P, when given, receives the
-// partials of the water against the gas-phase water and the ions.
+// partials of the water against the gas-phase water and the ions.  Ion
+// concentrations use the program's reciprocal factors (the reference divides
+// by count, MW and 1000 in turn: equal to rounding).
 __device__ double zsr_water(const int* I, const double* F, const double* y, double ppm,
                             double* P) {
   const double a_w = ppm * state_of(y[I[1]]);
@@ -296,34 +299,31 @@ __device__ double zsr_water(const int* I, const double* F, const double* y, doub
       const int ci = I[ii], ai = I[ii + 1], ny = I[ii + 2];
       const int pg = I[ii + 3], pc = I[ii + 4], pa = I[ii + 5];
       ii += 6;
-      const double low = F[fi], ncat = F[fi + 1], mwc = F[fi + 2], nan_ = F[fi + 3],
-                   mwa = F[fi + 4];
-      const double* Y = F + fi + 5;
-      fi += 5 + ny;
-      const double j_aw = a_w > low ? a_w : low;
-      double mol = 0.0;
+      const double low = F[fi], fc = F[fi + 1], fa = F[fi + 2];
+      const double* Y = F + fi + 3;
+      fi += 3 + ny;
+      const bool above = a_w > low;
+      const double j_aw = above ? a_w : low;
+      // Y_0 + Y_1 a + ... and its derivative in a, by Horner's rule
+      double mol = 0.0, dm = 0.0;
       #pragma unroll 1
-      for (int k = 0; k < ny; ++k) mol += Y[k] * dpow(j_aw, (double)k);
-      const double cat = ddiv(ddiv(ddiv(state_of(y[ci]), ncat), mwc), 1000.0);
-      const double an = ddiv(ddiv(ddiv(state_of(y[ai]), nan_), mwa), 1000.0);
+      for (int k = ny - 1; k >= 0; --k) {
+        dm = dm * j_aw + mol;
+        mol = mol * j_aw + Y[k];
+      }
+      const double cat = state_of(y[ci]) * fc, an = state_of(y[ai]) * fa;
       // smooth minimum of the ion concentrations (smoothing factor -100)
       const double ec = exp(-100.0 * cat), ea = exp(-100.0 * an);
-      const double conc = ddiv(cat * ec + an * ea, ec + ea);
-      W += ddiv(conc, mol * mol) * 1000.0;
+      const double inv_e = ddiv(1.0, ec + ea);
+      const double conc = (cat * ec + an * ea) * inv_e;
+      const double inv_m2 = ddiv(1.0, mol * mol);
+      W += conc * inv_m2 * 1000.0;
       if (P) {
-        double mj = Y[0], dm = 0.0;
-        #pragma unroll 1
-        for (int k = 1; k < ny; ++k) {
-          mj += Y[k] * dpow(j_aw, (double)k);
-          dm += Y[k] * k * dpow(j_aw, (double)(k - 1));
-        }
-        dm *= a_w > low ? ppm : 0.0;
-        const double den = (ec + ea) * (ec + ea);
-        const double dcc = ddiv(ec * ec + ec * ea * (1.0 + 100.0 * an - 100.0 * cat), den);
-        const double dca = ddiv(ea * ea + ec * ea * (1.0 + 100.0 * cat - 100.0 * an), den);
-        P[pg] += ddiv(-2.0 * conc, dpow(mj, 3.0)) * 1000.0 * dm;
-        P[pa] += ddiv(1.0, dpow(mj, 2.0)) * 1000.0 * dca * ddiv(1.0, nan_ * mwa * 1000.0);
-        P[pc] += ddiv(1.0, dpow(mj, 2.0)) * 1000.0 * dcc * ddiv(1.0, ncat * mwc * 1000.0);
+        const double dcc = (ec * ec + ec * ea * (1.0 + 100.0 * an - 100.0 * cat)) * inv_e * inv_e;
+        const double dca = (ea * ea + ec * ea * (1.0 + 100.0 * cat - 100.0 * an)) * inv_e * inv_e;
+        P[pg] += -2.0 * conc * inv_m2 * ddiv(1000.0, mol) * (above ? dm * ppm : 0.0);
+        P[pa] += inv_m2 * 1000.0 * dca * fa;
+        P[pc] += inv_m2 * 1000.0 * dcc * fc;
       }
     } else if (type == 2) {  // EQSAM (Metzger et al., 2002)
       const int nion = I[ii], pg = I[ii + 1];
@@ -334,6 +334,7 @@ __device__ double zsr_water(const int* I, const double* F, const double* y, doub
       e_aw = e_aw < 0.001 ? 0.001 : e_aw;
       const double base = pre * (ddiv(1.0, e_aw) - 1.0);
       const double mol = dpow(base, zw);
+      const double inv_mol = ddiv(1.0, mol);
       double dmol = 0.0;
       if (P) {
         const double de = (a_w > 0.99 || a_w < 0.001) ? 0.0 : ppm;
@@ -343,13 +344,13 @@ __device__ double zsr_water(const int* I, const double* F, const double* y, doub
       for (int k = 0; k < nion; ++k) {
         const int ion = I[ii], pid = I[ii + 1];
         ii += 2;
-        const double mw = F[fi++];
+        const double inv_mw = F[fi++];
         double c = state_of(y[ion]);
         c = c > 0.0 ? c : 0.0;
-        W += ddiv(ddiv(c, mw), mol);
+        W += c * inv_mw * inv_mol;
         if (P) {
-          P[pg] += ddiv(-c, mw * mol * mol) * dmol;
-          P[pid] += ddiv(c > 0.0 ? 1.0 : 0.0, mw * mol);
+          P[pg] += -c * inv_mw * inv_mol * inv_mol * dmol;
+          P[pid] += (c > 0.0 ? 1.0 : 0.0) * inv_mw * inv_mol;
         }
       }
     }
@@ -360,7 +361,9 @@ __device__ double zsr_water(const int* I, const double* F, const double* y, doub
 // PD-FiTE activity coefficient of one ion pair in one phase instance
 // (src/sub_models/sub_model_PDFiTE.c:167-259, Jacobian :273-432; Topping et
 // al. 2009, eq. 15) from its program; P, when given, receives its partials
-// against the gas-phase water and every ion.
+// against the gas-phase water and every ion.  Moles per concentration and
+// the partials' factors are the program's reciprocals; 1 / omega is taken
+// once.
 __device__ double pdfite_gamma(const int* I, const double* F, const double* y, double ppm,
                                double* P) {
   double a_w = ppm * state_of(y[I[1]]);
@@ -369,12 +372,13 @@ __device__ double pdfite_gamma(const int* I, const double* F, const double* y, d
   const int* pr = I + 6;              // per pair: cation, anion, stoichiometry, 2 param ids
   const int* it = pr + 5 * npair;     // per interaction: pair, B count
   const double* fb = F + 2 * npair;   // per interaction: min RH, max RH, B...
-  auto cn = [&](int j) { return ddiv(ddiv(state_of(y[pr[5 * j]]), F[2 * j]), 1000000.0); };
-  auto an = [&](int j) { return ddiv(ddiv(state_of(y[pr[5 * j + 1]]), F[2 * j + 1]), 1000000.0); };
+  auto cn = [&](int j) { return state_of(y[pr[5 * j]]) * F[2 * j]; };
+  auto an = [&](int j) { return state_of(y[pr[5 * j + 1]]) * F[2 * j + 1]; };
   double omega = 0.0;
   #pragma unroll 1
   for (int j = 0; j < npair; ++j)
     if (j != x) omega += 2.0 * pr[5 * j + 2] * cn(j) * an(j);
+  const double inv_omega = omega > 0.0 ? ddiv(1.0, omega) : 0.0;
   auto in_range = [&](double lo, double hi) {
     return !((a_w <= lo || a_w > hi) && !(a_w <= 0.0 && lo <= 0.0));
   };
@@ -389,11 +393,11 @@ __device__ double pdfite_gamma(const int* I, const double* F, const double* y, d
     if (!in_range(lo, hi)) continue;
     double li = 0.0;
     #pragma unroll 1
-    for (int z = 0; z < nb; ++z) li += B[z] * dpow(a_w, (double)z);
+    for (int z = nb - 1; z >= 0; --z) li = li * a_w + B[z];
     if (j == x)
       lng += li;
     else if (omega > 0.0)
-      lng += ddiv(li * cn(j) * an(j), omega);
+      lng += li * cn(j) * an(j) * inv_omega;
   }
   const double g = exp(lng);
   if (P) {
@@ -405,26 +409,27 @@ __device__ double pdfite_gamma(const int* I, const double* F, const double* y, d
       const double* B = fb + fi + 2;
       fi += 2 + nb;
       if (!in_range(lo, hi)) continue;
-      double li = B[0], dli = 0.0;
+      double li = 0.0, dli = 0.0;
       #pragma unroll 1
-      for (int z = 1; z < nb; ++z) {
-        li += B[z] * dpow(a_w, (double)z);
-        dli += B[z] * z * dpow(a_w, (double)(z - 1));
+      for (int z = nb - 1; z >= 0; --z) {
+        dli = dli * a_w + li;
+        li = li * a_w + B[z];
       }
       dli *= ppm;
       if (j == x) {
         P[pw] += g * dli;
       } else if (omega > 0.0) {
         const double cj = cn(j), aj = an(j);
-        P[pr[5 * j + 3]] += ddiv(g * li * aj, F[2 * j] * omega) * 1.0e-6;
-        P[pr[5 * j + 4]] += ddiv(g * li * cj, F[2 * j + 1] * omega) * 1.0e-6;
-        P[pw] += ddiv(g * cj * aj, omega) * dli;
-        const double s = ddiv(-g * li * cj * aj, omega * omega) * 2.0;
+        P[pr[5 * j + 3]] += g * li * aj * F[2 * j] * inv_omega;
+        P[pr[5 * j + 4]] += g * li * cj * F[2 * j + 1] * inv_omega;
+        P[pw] += g * cj * aj * inv_omega * dli;
+        const double s = -g * li * cj * aj * inv_omega * inv_omega * 2.0;
         #pragma unroll 1
         for (int q = 0; q < npair; ++q) {
           if (q == x) continue;
-          P[pr[5 * q + 3]] += ddiv(s * pr[5 * q + 2] * an(q), F[2 * q]) * 1.0e-6;
-          P[pr[5 * q + 4]] += ddiv(s * pr[5 * q + 2] * cn(q), F[2 * q + 1]) * 1.0e-6;
+          const double sq = s * pr[5 * q + 2];
+          P[pr[5 * q + 3]] += sq * an(q) * F[2 * q];
+          P[pr[5 * q + 4]] += sq * cn(q) * F[2 * q + 1];
         }
       }
     }
@@ -624,9 +629,9 @@ __device__ __noinline__ bool aq_rates(const char* tb, const double* y, const dou
     double* r = rates + rec[3];
     #pragma unroll 1
     for (int k = 0; k < S; ++k) {
-      const double m = t.aq_sm[s0 + k];
-      r[2 * k] = ddiv(k < R ? rf : rr, m);
-      r[2 * k + 1] = ddiv(k < R ? rr : rf, m);
+      const double im = t.aq_sim[s0 + k];
+      r[2 * k] = (k < R ? rf : rr) * im;
+      r[2 * k + 1] = (k < R ? rr : rf) * im;
       neg |= r[2 * k] < 0.0 || r[2 * k + 1] < 0.0;
     }
   }
@@ -652,10 +657,9 @@ __device__ __noinline__ void aq_partials(const char* tb, const double* y, const 
     #pragma unroll 1
     for (int a = 0; a < S; ++a) {
       const double rate = a < R ? rf : rr;
-      const double ca = state_of(y[t.aq_sp[s0 + a]]);
+      const double rc = rate != 0.0 ? ddiv(rate, state_of(y[t.aq_sp[s0 + a]])) : 0.0;
       #pragma unroll 1
-      for (int k = 0; k < S; ++k)
-        p[a * S + k] = rate != 0.0 ? ddiv(ddiv(rate, ca), t.aq_sm[s0 + k]) : 0.0;
+      for (int k = 0; k < S; ++k) p[a * S + k] = rc * t.aq_sim[s0 + k];
     }
     p += S * S;
     const int wcv = rec[6] & 0xFF;
@@ -665,17 +669,14 @@ __device__ __noinline__ void aq_partials(const char* tb, const double* y, const 
       const int nr = (rec[6] >> 8) & 0xF, np = rec[6] >> 12;
       const double dfw = ddiv(rf * (nr - 1), w), drw = ddiv(rr * (np - 1), w);
       #pragma unroll 1
-      for (int k = 0; k < S; ++k) {
-        const double m = t.aq_sm[s0 + k];
-        p[k] = k < R ? ddiv(dfw - drw, m) : ddiv(drw - dfw, m);
-      }
+      for (int k = 0; k < S; ++k) p[k] = (k < R ? dfw - drw : drw - dfw) * t.aq_sim[s0 + k];
       p += S;
     }
     if (rec[7]) {
       const double dg = ddiv(rr, cv[rec[7] - 1]);
       #pragma unroll 1
       for (int k = 0; k < S; ++k) {
-        const double v = ddiv(dg, t.aq_sm[s0 + k]);
+        const double v = dg * t.aq_sim[s0 + k];
         p[k] = k < R ? v : -v;
       }
       p += S;
@@ -686,10 +687,10 @@ __device__ __noinline__ void aq_partials(const char* tb, const double* y, const 
     for (int j = rec[8]; j < rec[8] + rec[9]; ++j, p += S) {
       const bool jr = (t.aq_cp[j] & 0x8000) != 0;
       const double rate = jr ? rf : rr;
-      const double ca = cv[t.aq_cp[j] & 0x7FFF];
+      const double rc = rate != 0.0 ? ddiv(rate, cv[t.aq_cp[j] & 0x7FFF]) : 0.0;
       #pragma unroll 1
       for (int k = 0; k < S; ++k) {
-        const double v = rate != 0.0 ? ddiv(ddiv(rate, ca), t.aq_sm[s0 + k]) : 0.0;
+        const double v = rc * t.aq_sim[s0 + k];
         p[k] = jr == (k < R) ? -v : v;
       }
     }
