@@ -101,7 +101,11 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=8.0)
     ap.add_argument("--synth-cells", type=int, default=0,
                     help="cells of the 200-species / 600-reaction synthetic mechanism (0: skip)")
-    ap.add_argument("--synth-dt", type=float, default=0.5)
+    ap.add_argument("--synth-dt", type=float, default=3.0,
+                    help="host step of the synthetic mechanism (s): the longest at which the "
+                         "oracle finishes every sampled cell")
+    ap.add_argument("--synth-lane-cells", type=int, default=2000,
+                    help="cells of the lane-per-cell comparison on the synthetic mechanism")
     ap.add_argument("--serve-columns", type=int, default=256,
                     help="device-resident columns in the serving pool")
     return ap.parse_args()
@@ -455,11 +459,12 @@ def counted_flops(model: dict, stats) -> float:
 # ---------------------------------------------------------------------------
 # First host step of other mechanisms
 # ---------------------------------------------------------------------------
-def run_first_step(mech, args, dev, stream, n, cells=None, dt=None):
+def run_first_step(mech, args, dev, stream, n, cells=None, dt=None, kernel=None):
     """n seeded cells of another mechanism over the first host step of the
     sequence (every cell from its seeded state), mixed and FP64,
     device-resident, longest-first order from a previous identical run;
-    device time of the second run."""
+    device time of the second run.  kernel: camp_b200_set_kernel's value
+    (None: the mechanism's default)."""
     import torch
 
     from camp_b200.cells import make_cells
@@ -478,6 +483,9 @@ def run_first_step(mech, args, dev, stream, n, cells=None, dt=None):
         s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4,
                      max_steps=args.max_steps)
         s.set_precision(p)
+        if kernel is not None:
+            s.set_kernel(kernel)
+        out["kernel"] = s.kernel()
         s.set_photo_rates_device(photo, n)
         s.set_cost_ordering(True)
         s.set_graph(not args.no_graph)
@@ -654,9 +662,10 @@ def run_gpu_arm(args):
                                        10000)
     synth = None
     if world == 1 and args.synth_cells > 0:
-        # the seeded 200-species / 600-reaction mechanism on the lane-per-cell
-        # kernel, at the host step every oracle cell finishes (its cells gain
-        # molecules in every reaction: at 300 s none finishes)
+        # the seeded 200-species / 600-reaction mechanism on its default
+        # (block-per-cell) kernel, and the lane-per-cell kernel on a smaller
+        # sample, at the host step every sampled oracle cell finishes (its
+        # cells gain molecules in every reaction: at 300 s none finishes)
         import tempfile
 
         from camp_b200.cells import make_cells
@@ -667,6 +676,11 @@ def run_gpu_arm(args):
         scells = make_cells(smech, args.synth_cells, SEED, conc_lo=1e-8, photo_base=sbase)
         synth = run_first_step(smech, args, dev, stream, args.synth_cells, cells=scells,
                                dt=args.synth_dt)
+        if args.synth_lane_cells > 0:
+            nl = min(args.synth_lane_cells, args.synth_cells)
+            lcells = make_cells(smech, nl, SEED, conc_lo=1e-8, photo_base=sbase)
+            synth["lane_kernel"] = run_first_step(smech, args, dev, stream, nl, cells=lcells,
+                                                  dt=args.synth_dt, kernel=1)
     fm = flop_model(mech, solver)
     if rank != 0:
         solver.free()

@@ -55,7 +55,8 @@ EXPORTED = [
     "camp_b200_set_photo_rates", "camp_b200_set_photo_rates_device", "camp_b200_get_cell_stats", "camp_b200_kernel_launches",
     "camp_b200_last_kernel_ms", "camp_b200_n_dep_var", "camp_b200_n_jac_elem",
     "camp_b200_n_lu_elem", "camp_b200_rxn_int_data_size", "camp_b200_get_solver_jac",
-    "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_eval_deriv",
+    "camp_b200_get_rxn_int_data", "camp_b200_get_lu_order", "camp_b200_get_block_tables",
+    "camp_b200_eval_deriv",
     "camp_b200_n_mapped_values", "camp_b200_get_jac_map", "camp_b200_get_kernel",
     "camp_b200_check_precision",
     "camp_b200_eval_jac", "camp_b200_check_jac", "camp_b200_solver_from_json",
@@ -155,6 +156,8 @@ def load(path: str = LIB_PATH):
     lib.camp_b200_get_solver_jac.argtypes = [vp, _i32p, _i32p]
     lib.camp_b200_get_rxn_int_data.argtypes = [vp, _i32p]
     lib.camp_b200_get_lu_order.argtypes = [vp, _i32p]
+    lib.camp_b200_get_block_tables.restype = C.c_long
+    lib.camp_b200_get_block_tables.argtypes = [vp, vp, C.c_long]
     lib.camp_b200_get_jac_map.restype = ip
     lib.camp_b200_get_jac_map.argtypes = [vp, _i32p]
     lib.camp_b200_eval_deriv.restype = ip

@@ -586,3 +586,218 @@ bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
 }
 
 }  // namespace campb
+
+namespace campb {
+
+bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
+                      std::vector<uint8_t>* blob, BlockOff* off, std::string* err) {
+  if (t.n_simpol > 0 || t.n_aq > 0 || t.n_cv > 0) {
+    *err = "the CTA-per-cell kernel does not evaluate SIMPOL, HL or aqueous equilibrium "
+           "reactions or sub-models";
+    return false;
+  }
+  const int n = t.n;
+  if (n < 1 || n > 1023 || t.n_rxn > 65535 || t.n_lu > 65535 || t.n_part > 65535 ||
+      t.n_jac > 32767) {
+    *err = "mechanism exceeds the CTA-kernel table encodings";
+    return false;
+  }
+  std::map<uint64_t, int> cid;
+  std::vector<double> coef;
+  auto coef_id = [&](double v) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    auto it = cid.find(b);
+    if (it != cid.end()) return it->second;
+    int id = (int)coef.size();
+    coef.push_back(v);
+    cid[b] = id;
+    return id;
+  };
+  // reactions
+  std::vector<uint32_t> rx_word(t.n_rxn), rx_vptr(t.n_rxn + 1);
+  for (int r = 0; r < t.n_rxn; ++r) {
+    const int v0 = t.rx_vptr[r], v1 = t.rx_vptr[r + 1];
+    if (v1 - v0 > 3) {
+      *err = "reaction " + std::to_string(r) + " has more than 3 variable reactants";
+      return false;
+    }
+    uint32_t w = (uint32_t)(v1 - v0) << 30;
+    for (int k = 0; k < v1 - v0; ++k) w |= (uint32_t)t.rx_vdep[v0 + k] << (10 * k);
+    rx_word[r] = w;
+    rx_vptr[r] = (uint32_t)v0;
+  }
+  rx_vptr[t.n_rxn] = (uint32_t)t.rx_vptr[t.n_rxn];
+  // f gather in the species lists' own order
+  std::vector<uint32_t> fg_ptr(n + 1), fg_ent(t.fg_rxn.size());
+  for (int i = 0; i <= n; ++i) fg_ptr[i] = (uint32_t)t.fg_ptr[i];
+  for (size_t e = 0; e < fg_ent.size(); ++e)
+    fg_ent[e] = (uint32_t)t.fg_rxn[e] | ((uint32_t)coef_id(t.fg_coef[e]) << 16) |
+                ((uint32_t)(t.fg_prod[e] == FG_PRODUCT ? 1 : 0) << 31);
+  // J gather: losses, then guarded products, per slot
+  std::vector<uint32_t> jg_ptr(t.n_jac + 1), jg_mid(t.n_jac), jg_w0;
+  std::vector<uint16_t> jg_w1, jg_row(t.n_jac);
+  for (int e = 0; e < t.n_jac; ++e) {
+    jg_ptr[e] = (uint32_t)jg_w0.size();
+    for (int pass = 0; pass < 2; ++pass) {
+      if (pass == 1) jg_mid[e] = (uint32_t)jg_w0.size();
+      for (int g = t.jg_ptr[e]; g < t.jg_ptr[e + 1]; ++g) {
+        if (t.jg_ind[g] == -2) {
+          *err = "the CTA-per-cell kernel has no unguarded Jacobian products";
+          return false;
+        }
+        if ((t.jg_ind[g] == -1) != (pass == 0)) continue;
+        jg_w0.push_back((uint32_t)t.jg_part[g] | ((uint32_t)coef_id(t.jg_coef[g]) << 16));
+        jg_w1.push_back((uint16_t)(t.jg_ind[g] >= 0 ? t.jg_ind[g] + 1 : 0));
+      }
+    }
+    jg_row[e] = (uint16_t)t.jg_row[e];
+  }
+  jg_ptr[t.n_jac] = (uint32_t)jg_w0.size();
+  if (coef.size() > 32767) {
+    *err = "too many distinct yields for the table encoding";
+    return false;
+  }
+  // LU: sorted rows, the diagonal in every row
+  for (int i = 0; i < n; ++i) {
+    for (int q = t.lu_rowptr[i] + 1; q < t.lu_rowptr[i + 1]; ++q)
+      if (t.lu_col[q] <= t.lu_col[q - 1]) {
+        *err = "internal: LU row columns not sorted";
+        return false;
+      }
+    if (t.lu_col[t.lu_diag[i]] != i) {
+      *err = "internal: LU diagonal position";
+      return false;
+    }
+  }
+  std::vector<uint16_t> lu_src(t.n_lu, 0);
+  for (int e = 0; e < t.n_jac; ++e) lu_src[t.jg_lupos[e]] = (uint16_t)(e + 1);
+  for (int i = 0; i < n; ++i) lu_src[t.lu_diag[i]] |= 0x8000u;
+  // position lookup and the trailing dense block: the smallest r0 with every
+  // (i, j), i, j >= r0, present
+  std::vector<int> pos((size_t)n * n, -1);
+  for (int i = 0; i < n; ++i)
+    for (int q = t.lu_rowptr[i]; q < t.lu_rowptr[i + 1]; ++q)
+      pos[(size_t)i * n + t.lu_col[q]] = q;
+  int r0 = n - 1;
+  for (int c = n - 2; c >= 0; --c) {
+    bool full = true;
+    for (int i = c; i < n && full; ++i)
+      full = pos[(size_t)i * n + c] >= 0 && pos[(size_t)c * n + i] >= 0;
+    if (!full) break;
+    r0 = c;
+  }
+  std::vector<uint16_t> dpos(n - r0), ub(r0);
+  for (int i = r0; i < n; ++i) dpos[i - r0] = (uint16_t)pos[(size_t)i * n + r0];
+  for (int i = 0; i < r0; ++i) {
+    int q = t.lu_rowptr[i + 1];
+    while (q > t.lu_diag[i] + 1 && t.lu_col[q - 1] >= r0) --q;
+    ub[i] = (uint16_t)q;
+  }
+  // head pivots: L entries of each column, and the update target of every
+  // (L entry, U entry) pair
+  std::vector<uint32_t> lk_ptr(r0 + 1, 0), tg_ptr(r0 + 1, 0);
+  std::vector<uint16_t> lk_pos, tg;
+  for (int k = 0; k < r0; ++k) {
+    lk_ptr[k] = (uint32_t)lk_pos.size();
+    tg_ptr[k] = (uint32_t)tg.size();
+    for (int i = k + 1; i < n; ++i) {
+      const int q = pos[(size_t)i * n + k];
+      if (q < 0) continue;
+      lk_pos.push_back((uint16_t)q);
+      for (int p = t.lu_diag[k] + 1; p < t.lu_rowptr[k + 1]; ++p) {
+        const int d = pos[(size_t)i * n + t.lu_col[p]];
+        if (d < 0) {
+          *err = "internal: LU fill pattern not closed";
+          return false;
+        }
+        tg.push_back((uint16_t)d);
+      }
+    }
+  }
+  lk_ptr[r0] = (uint32_t)lk_pos.size();
+  tg_ptr[r0] = (uint32_t)tg.size();
+  // head row levels: forward over the L entries, backward over the U entries
+  // with columns < r0 (the dense block's values reach head rows in one pass)
+  std::vector<int> flev(r0, 0), blev(r0, 0);
+  int n_hf = 0, n_hb = 0;
+  for (int i = 0; i < r0; ++i) {
+    int l = 0;
+    for (int q = t.lu_rowptr[i]; q < t.lu_diag[i]; ++q) l = std::max(l, flev[t.lu_col[q]] + 1);
+    flev[i] = l;
+    n_hf = std::max(n_hf, l + 1);
+  }
+  for (int i = r0 - 1; i >= 0; --i) {
+    int l = 0;
+    for (int q = t.lu_diag[i] + 1; q < ub[i]; ++q) l = std::max(l, blev[t.lu_col[q]] + 1);
+    blev[i] = l;
+    n_hb = std::max(n_hb, l + 1);
+  }
+  auto levels = [&](const std::vector<int>& lev, int nl, std::vector<uint16_t>* ptr,
+                    std::vector<uint16_t>* rows) {
+    ptr->assign(nl + 1, 0);
+    rows->clear();
+    for (int l = 0; l < nl; ++l) {
+      (*ptr)[l] = (uint16_t)rows->size();
+      for (int i = 0; i < (int)lev.size(); ++i)
+        if (lev[i] == l) rows->push_back((uint16_t)i);
+    }
+    (*ptr)[nl] = (uint16_t)rows->size();
+  };
+  std::vector<uint16_t> hf_ptr, hf_rows, hb_ptr, hb_rows;
+  levels(flev, n_hf, &hf_ptr, &hf_rows);
+  levels(blev, n_hb, &hb_ptr, &hb_rows);
+  auto u16 = [](const std::vector<int>& v) {
+    std::vector<uint16_t> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = (uint16_t)v[i];
+    return o;
+  };
+  Writer w;
+  w.buf.resize(256, 0);
+  static_assert(sizeof(BlockOff) <= 256, "BlockOff must fit the blob header");
+  BlockOff o{};
+  o.n = n;
+  o.n_rxn = t.n_rxn;
+  o.n_part = t.n_part;
+  o.n_jac = t.n_jac;
+  o.n_lu = t.n_lu;
+  o.n_coef = (int)coef.size();
+  o.r0 = r0;
+  o.n_hf = n_hf;
+  o.n_hb = n_hb;
+  o.rx_word = w.put(rx_word);
+  o.rx_vptr = w.put(rx_vptr);
+  o.coef = w.put(coef);
+  o.fg_ptr = w.put(fg_ptr);
+  o.fg_ent = w.put(fg_ent);
+  o.jg_ptr = w.put(jg_ptr);
+  o.jg_mid = w.put(jg_mid);
+  o.jg_w0 = w.put(jg_w0);
+  o.jg_w1 = w.put(jg_w1);
+  o.jg_row = w.put(jg_row);
+  o.lu_src = w.put(lu_src);
+  o.lu_perm = w.put(u16(t.lu_perm));
+  o.lu_rowptr = w.put(u16(t.lu_rowptr));
+  o.lu_col = w.put(u16(t.lu_col));
+  o.lu_diag = w.put(u16(t.lu_diag));
+  o.dpos = w.put(dpos);
+  o.ub = w.put(ub);
+  o.lk_ptr = w.put(lk_ptr);
+  o.lk_pos = w.put(lk_pos);
+  o.tg_ptr = w.put(tg_ptr);
+  o.tg = w.put(tg);
+  o.hf_ptr = w.put(hf_ptr);
+  o.hf_rows = w.put(hf_rows);
+  o.hb_ptr = w.put(hb_ptr);
+  o.hb_rows = w.put(hb_rows);
+  o.dep_state = w.put(u16(t.dep_state));
+  o.atol = w.put(atol_dep);
+  w.buf.resize((w.buf.size() + 15) & ~size_t(15), 0);
+  o.bytes = (int)w.buf.size();
+  memcpy(w.buf.data(), &o, sizeof(o));
+  blob->swap(w.buf);
+  *off = o;
+  return true;
+}
+
+}  // namespace campb

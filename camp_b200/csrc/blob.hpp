@@ -120,3 +120,51 @@ bool build_lane_blob(const Tables& t, const std::vector<double>& atol_dep,
                      std::vector<uint8_t>* blob, LaneOff* off, std::string* err);
 
 }  // namespace campb
+
+namespace campb {
+
+// Tables of the CTA-per-cell kernel (one thread block per cell), for
+// mechanisms whose LU is too large for the warp-per-cell tables.  The block
+// reads them from global memory through L1.  The LU is row-wise in pivot
+// order with sorted columns; its trailing rows r0..n-1 form a dense block
+// (every column r0..n-1 present), addressed without tables: entry (i, j) of
+// that block sits at dpos[i - r0] + (j - r0).  The sparse head (pivots and
+// rows before r0) is factored pivot by pivot from tabulated update targets
+// and solved by row levels.  Offsets in bytes from the start of the blob.
+struct BlockOff {
+  int bytes;
+  int n, n_rxn, n_part, n_jac, n_lu, n_coef;
+  int r0;          // first row (pivot) of the trailing dense block
+  int n_hf, n_hb;  // forward / backward row levels of the head rows
+  // reactions: variable reactants (nv<<30 | d2<<20 | d1<<10 | d0, uint32)
+  // and the first rate partial of each (uint32, n_rxn + 1)
+  int rx_word, rx_vptr;
+  int coef;  // double
+  // f gather by species: pointers (uint32, n + 1), entries (uint32: term |
+  // coef<<16 | guarded product<<31)
+  int fg_ptr, fg_ent;
+  // J gather by solver slot: pointers (uint32, n_jac + 1), first guarded
+  // product (uint32), entries (uint32: partial | coef<<16), guard species + 1
+  // (uint16), row species (uint16)
+  int jg_ptr, jg_mid, jg_w0, jg_w1, jg_row;
+  // per LU position: J slot + 1 (0 = none) | diagonal<<15 (uint16)
+  int lu_src;
+  // LU structure (uint16): pivot -> dependent index, row pointers, columns,
+  // diagonal positions
+  int lu_perm, lu_rowptr, lu_col, lu_diag;
+  int dpos;  // per dense row: position of its column r0 (uint16)
+  int ub;    // per head row: first position with a column >= r0 (uint16)
+  // head pivots k < r0: L entries of column k (pointers uint32, r0 + 1;
+  // positions uint16) and the update targets, row-major over (L entry, U
+  // entry of row k) (pointers uint32, r0 + 1; positions uint16)
+  int lk_ptr, lk_pos, tg_ptr, tg;
+  // head row levels (pointers uint16, levels + 1; rows uint16)
+  int hf_ptr, hf_rows, hb_ptr, hb_rows;
+  int dep_state;  // uint16
+  int atol;       // double
+};
+
+bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
+                      std::vector<uint8_t>* blob, BlockOff* off, std::string* err);
+
+}  // namespace campb

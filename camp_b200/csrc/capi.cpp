@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "blob.hpp"
 #include "engine.hpp"
 #include "loader.hpp"
 #include "model.hpp"
@@ -616,8 +617,8 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
   }
   // candidates: the warp-per-cell kernel with its resident cells per block,
   // where the Nordsieck history lives and the LU strategy, and the
-  // lane-per-cell kernel (32 cells per warp) where the mechanism has its
-  // tables; the precision stays as set
+  // lane-per-cell kernel (32 cells per warp) and the block-per-cell kernel
+  // where the mechanism has their tables; the precision stays as set
   campb::SolveSettings base = s->settings, best = s->settings;
   double best_ms = -1.0;
   const bool cost_order = s->cost_order;
@@ -642,6 +643,11 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
   if (s->engine->lane_tables()) {
     campb::SolveSettings c = base;
     c.kernel = 1;
+    cands.push_back(c);
+  }
+  if (s->engine->block_tables()) {
+    campb::SolveSettings c = base;
+    c.kernel = 2;
     cands.push_back(c);
   }
   for (const campb::SolveSettings& c : cands) {
@@ -675,11 +681,14 @@ int camp_b200_get_tuning(void* solver_data, int* warps_per_block, int* hist_glob
   return 0;
 }
 
-int camp_b200_get_kernel(void* solver_data) { return S(solver_data)->settings.kernel; }
+int camp_b200_get_kernel(void* solver_data) {
+  const Solver* s = S(solver_data);
+  return s->ready ? s->engine->effective_kernel(s->settings) : s->settings.kernel;
+}
 
 int camp_b200_set_kernel(void* solver_data, int kernel, int place) {
-  if (kernel != 0 && kernel != 1) {
-    set_error("camp_b200_set_kernel: kernel must be 0 or 1");
+  if (kernel < 0 || kernel > 2) {
+    set_error("camp_b200_set_kernel: kernel must be 0, 1 or 2");
     return -1;
   }
   S(solver_data)->settings.kernel = kernel;
@@ -864,6 +873,24 @@ int camp_b200_get_jac_map(void* solver_data, int* triplets) {
   std::copy(m.jac_map().begin(), m.jac_map().end(), triplets);
   return 0;
 }
+long camp_b200_get_block_tables(void* solver_data, void* out, long capacity) {
+  const Model& m = *S(solver_data)->model;
+  if (!m.built()) {
+    set_error("camp_b200_get_block_tables: sparsity not built");
+    return -1;
+  }
+  std::vector<uint8_t> blob;
+  campb::BlockOff off{};
+  std::string err;
+  if (!campb::build_block_blob(m.tables(), std::vector<double>(m.tables().n, 0.0), &blob, &off,
+                               &err)) {
+    set_error("camp_b200_get_block_tables: " + err);
+    return -1;
+  }
+  if (out && capacity >= (long)blob.size()) memcpy(out, blob.data(), blob.size());
+  return (long)blob.size();
+}
+
 int camp_b200_get_lu_order(void* solver_data, int* perm) {
   const Model& m = *S(solver_data)->model;
   if (!m.built()) return -1;

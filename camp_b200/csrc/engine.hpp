@@ -26,7 +26,7 @@ struct SolveSettings {
   int warps_per_block = 0; // 0 = as many as fit
   int blocks_per_sm = 1;
   int lu_mode = 0;         // 0 = level schedule over the warp, 1 = one lane
-  int kernel = 0;          // 0 = warp per cell, 1 = lane per cell
+  int kernel = 0;          // 0 = warp per cell, 1 = lane per cell, 2 = block per cell
   int lane_place = 7;      // lane kernel: bit0 y, bit1 LU, bit2 z in shared memory
   int use_graph = 0;       // warp kernel: launch the device step as a CUDA graph
   int hist_global = 0;     // warp kernel: Nordsieck history + rate constants in
@@ -88,6 +88,12 @@ class Engine {
   bool warp_tables(std::string* err) const;
   // the lane-per-cell kernel's tables were built (it runs this mechanism)
   bool lane_tables() const;
+  // the CTA-per-cell kernel's tables were built (it runs this mechanism)
+  bool block_tables() const;
+  // the kernel a launch with these settings runs (kernel 0 on a mechanism
+  // beyond the warp tables: the CTA form where it has its tables, else the
+  // lane form)
+  int effective_kernel(const SolveSettings& s) const;
   // Serving slots: a launch on caller-provided buffers and scratch (from
   // slot_scratch_bytes for at most max_blocks blocks), so several launches
   // can be in flight on different streams; d_tspan holds each cell's
@@ -104,6 +110,9 @@ class Engine {
 
  private:
   bool ensure(void** p, size_t* cap, size_t bytes, std::string* err);
+  bool launch_block(double* d_state, const double* d_env, const double* d_photo,
+                    const int* d_order, int n_cells, double t0, double t1,
+                    const SolveSettings& s, void* stream, std::string* err);
   bool launch_graph(struct SolveArgs& a, const struct WarpLaunch& w, int precision,
                     void* stream, std::string* err);
   void fill_args(struct SolveArgs* a, const struct WarpLaunch& w, const SolveSettings& s,

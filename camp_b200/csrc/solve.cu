@@ -1178,9 +1178,17 @@ __device__ __noinline__ void dev_lsolve_seq(const char* tb, const LT* LU, const 
 // ---------------------------------------------------------------------------
 // BDF integrator state of one cell (warp-uniform scalars)
 // ---------------------------------------------------------------------------
-template <typename LT, bool AERO>
+#include "block.cuh"
+
+// One cell's CVODE BDF integration, run by one warp (lane-strided vector
+// loops, warp reductions).  BLK: the CTA-per-cell form, whose heavy
+// operations (f, J, factorization, solves) run on the whole block through
+// blk::call (block.cuh) while this warp keeps the control.
+template <typename LT, bool AERO, bool BLK = false>
 struct Cell {
   const char* tb;     // shared-memory tables
+  blk::Cmd* cmd;      // CTA form: the command slot and the operations' arrays
+  const blk::Ctx<LT>* bx;
   const double* atol;
   int lu_mode;        // 0 = level schedule over the lanes, 1 = one lane
   int lane, n;
@@ -1208,7 +1216,14 @@ struct Cell {
     return dsqrt(ddiv(warp_sum(s), (double)n));
   }
   __device__ int f(const double* yy, double* out) {
-    if constexpr (AERO)
+    if constexpr (BLK) {
+      bool bad = false;
+      #pragma unroll 1
+      for (int i = lane; i < n; i += 32) bad |= yy[i] < -kSmall;
+      if (warp_any(bad)) return 1;
+      blk::call<LT>(cmd, *bx, blk::OP_F, yy, out, h > 0.0 ? h : h0);
+      return 0;
+    } else if constexpr (AERO)
       return dev_f_aero(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
     else
       return dev_f(tb, yy, h > 0.0 ? h : h0, keff, rates, fscr, out, lane);
@@ -1391,12 +1406,21 @@ struct Cell {
       nstlj = nst;
       jcur = 1;
       int jr;
-      if constexpr (AERO)
+      if constexpr (BLK) {
+        bool bad = false;
+        #pragma unroll 1
+        for (int i = lane; i < n; i += 32) bad |= ypred[i] < -kSmall;
+        if (warp_any(bad)) return 1;
+        blk::call<LT>(cmd, *bx, blk::OP_JAC, ypred, nullptr, h > 0.0 ? h : h0);
+        jr = 0;
+      } else if constexpr (AERO) {
         jr = dev_jac_aero<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane);
-      else
+      } else {
         jr = dev_jac<LT>(tb, ypred, h > 0.0 ? h : h0, keff, rates, J, lane);
+      }
       if (jr) return 1;
     }
+    if constexpr (BLK) return blk::call<LT>(cmd, *bx, blk::OP_FACTOR, nullptr, nullptr, gamma);
     const bool ok = lu_mode ? dev_form_factor_seq<LT>(tb, J, gamma, LU, dinv, lane)
                             : dev_form_factor<LT>(tb, J, gamma, LU, dinv, lane);
     return ok ? 0 : 1;
@@ -1410,7 +1434,9 @@ struct Cell {
       for (int i = lane; i < n; i += 32)
         tempv[i] = gamma * ftemp[i] - (rl1 * (zb + (1) * n)[i] + acor[i]);
       __syncwarp();
-      if (lu_mode)
+      if constexpr (BLK)
+        blk::call<LT>(cmd, *bx, blk::OP_SOLVE, nullptr, nullptr, 0.0);
+      else if (lu_mode)
         dev_lsolve_seq<LT>(tb, LU, dinv, tempv, z, lane);
       else
         dev_lsolve<LT>(tb, LU, dinv, tempv, z, lane);
@@ -1864,6 +1890,144 @@ __global__ void __launch_bounds__(32 * (AERO ? kMaxCellsAero : kMaxCellsPerBlock
   }
 }
 
+// ---------------------------------------------------------------------------
+// CTA-per-cell kernel (block.cuh): one block per cell; warp 0 runs the BDF
+// control, every warp runs its f, J, factorization and solves
+// ---------------------------------------------------------------------------
+struct BlkLayout {  // byte offsets in the block's shared memory (zn -1: global)
+  int ctx, ctl, y, ewt, acor, ftemp, tempv, part, keff, dinv, z, zn, lu, bytes;
+};
+
+struct BlkArgs {
+  DevMech m;
+  const char* blob;  // BlockOff tables in global memory
+  BlkLayout lay;
+  double* state;
+  const double* env;
+  const double* photo;
+  const int* order;
+  const double* tspan;
+  int n_cells;
+  int* counter;
+  CellStats* stats;
+  void* jscratch;    // per-block solver Jacobian slots
+  double* hist;      // per-block Nordsieck history when not in shared memory
+  int hist_stride;   // doubles per block in hist
+  double t0, t1, rtol;
+  int max_steps, maxncf, maxnef;
+};
+
+// FP32 LU: half the shared memory, two cells per SM, so the register budget
+// is that of two blocks
+template <typename LT>
+__global__ void __launch_bounds__(blk::kThreads, sizeof(LT) == 4 ? 2 : 1)
+    block_kernel(BlkArgs a) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ blk::Cmd cmd;
+  __shared__ int s_idx;
+  const BlkLayout& L = a.lay;
+  blk::Ctx<LT>* cx = reinterpret_cast<blk::Ctx<LT>*>(smem + L.ctx);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    blk::Ctx<LT> c;
+    c.t = blk::make_tab(a.blob);
+    c.keff = (const double*)(smem + L.keff);
+    c.part = (double*)(smem + L.part);
+    c.J = (LT*)a.jscratch + (size_t)blockIdx.x * c.t.n_jac;
+    c.LU = (LT*)(smem + L.lu);
+    c.dinv = (LT*)(smem + L.dinv);
+    c.z = (LT*)(smem + L.z);
+    c.rhs = (double*)(smem + L.tempv);
+    *cx = c;
+  }
+  blk::bsync();
+  const DevMech& m = a.m;
+  #pragma unroll 1
+  for (;;) {
+    if (threadIdx.x == 0) s_idx = atomicAdd(a.counter, 1);
+    blk::bsync();
+    const int idx = s_idx;
+    if (idx >= a.n_cells) break;
+    if (warp != 0) {
+      blk::serve<LT>(&cmd, *cx);
+      continue;
+    }
+    Cell<LT, false, true> c;
+    c.tb = nullptr;
+    c.cmd = &cmd;
+    c.bx = cx;
+    c.atol = cx->t.atol;
+    c.lane = lane;
+    c.n = cx->t.n;
+    c.zb = L.zn >= 0 ? (double*)(smem + L.zn) : a.hist + (size_t)blockIdx.x * a.hist_stride;
+    double* ctl = (double*)(smem + L.ctl);
+    c.tau = ctl;
+    c.tq = ctl + (LMAX + 2);
+    c.l = ctl + (LMAX + 2) + 8;
+    c.ewt = (double*)(smem + L.ewt);
+    c.acor = (double*)(smem + L.acor);
+    c.y = (double*)(smem + L.y);
+    c.ftemp = (double*)(smem + L.ftemp);
+    c.tempv = (double*)(smem + L.tempv);
+    c.rates = (double*)(smem + L.part);
+    c.keff = (double*)(smem + L.keff);
+    c.fscr = nullptr;
+    c.LU = cx->LU;
+    c.z = cx->z;
+    c.dinv = cx->dinv;
+    c.J = cx->J;
+    c.rtol = a.rtol;
+    c.max_steps = a.max_steps;
+    c.maxncf = a.maxncf;
+    c.maxnef = a.maxnef;
+    c.lu_mode = 0;
+    const uint16_t* dep_state = cx->t.dep_state;
+    const int cell = a.order ? a.order[idx] : idx;
+    double* st = a.state + (size_t)cell * m.n_state;
+    // solver_run: dependent values clamped to >= TINY, constants clamped in
+    // place (src/camp_solver.c:554-567)
+    #pragma unroll 1
+    for (int i = lane; i < c.n; i += 32) {
+      const double v = st[__ldg(dep_state + i)];
+      c.y[i] = v > kTiny ? v : kTiny;
+    }
+    #pragma unroll 1
+    for (int j = lane; j < m.n_const; j += 32) {
+      const int s = ldg(m.const_state + j);
+      const double v = st[s];
+      st[s] = v > kTiny ? v : kTiny;
+    }
+    __syncwarp();
+    const double T = a.env[2 * (size_t)cell], P = a.env[2 * (size_t)cell + 1];
+    compute_keff(m, st, T, P, a.photo ? a.photo + (size_t)cell * m.n_photo : nullptr, c.keff,
+                 lane);
+    __syncwarp();
+    const double t0 = a.tspan ? a.tspan[2 * (size_t)cell] : a.t0;
+    const double t1 = a.tspan ? a.tspan[2 * (size_t)cell + 1] : a.t1;
+    const int flag = c.integrate(t0, t1);
+    if (flag == OK) {
+      #pragma unroll 1
+      for (int i = lane; i < c.n; i += 32)
+        st[__ldg(dep_state + i)] = c.y[i] > 0.0 ? c.y[i] : 0.0;
+    }
+    if (lane == 0) {
+      CellStats s;
+      s.status = flag;
+      s.nst = c.nst;
+      s.nfe = c.nfe;
+      s.nsetups = c.nsetups;
+      s.netf = c.netf;
+      s.nni = c.nni;
+      s.ncfn = c.ncfn;
+      s.nje = c.nje;
+      s.hu = c.hu;
+      s.hcur = c.next_h;
+      a.stats[cell] = s;
+    }
+    blk::finish(&cmd);
+  }
+}
+
 struct EvalArgs {
   DevMech m;
   BlobOff off;
@@ -2123,8 +2287,10 @@ struct Engine::Impl {
   // the warp-per-cell tables use 16-bit encodings; a mechanism beyond them
   // (e.g. an LU with hundreds of thousands of Schur updates) runs on the
   // lane-per-cell kernel only, and warp_why says why
-  bool warp_ok = true, lanes_ok = true;
-  std::string warp_why, lanes_why;
+  bool warp_ok = true, lanes_ok = true, blk_ok = false;
+  std::string warp_why, lanes_why, blk_why;
+  BlockOff boff{};
+  void* d_bblob = nullptr;
   LaneOff loff{};
   void* d_lblob = nullptr;
   void *d_scr64 = nullptr, *d_scrlt = nullptr;
@@ -2161,6 +2327,7 @@ Engine::~Engine() {
   cudaFree(I->d_tables);
   cudaFree(I->d_blob);
   cudaFree(I->d_lblob);
+  cudaFree(I->d_bblob);
   cudaFree(I->d_scr64);
   cudaFree(I->d_scrlt);
   cudaFree(I->d_state);
@@ -2348,8 +2515,18 @@ bool Engine::init(const Model& model, const std::vector<double>& atol_dep, int c
   I->d_lblob = nullptr;
   I->lanes_why.clear();
   I->lanes_ok = build_lane_blob(t, atol_dep, &lblob, &I->loff, &I->lanes_why);
-  if (!I->warp_ok && !I->lanes_ok) {
-    *err = "mechanism fits neither kernel: " + I->warp_why + "; " + I->lanes_why;
+  std::vector<uint8_t> bblob;
+  if (I->d_bblob) cudaFree(I->d_bblob);
+  I->d_bblob = nullptr;
+  I->blk_why.clear();
+  I->blk_ok = build_block_blob(t, atol_dep, &bblob, &I->boff, &I->blk_why);
+  if (I->blk_ok) {
+    CK(cudaMalloc(&I->d_bblob, bblob.size()));
+    CK(cudaMemcpy(I->d_bblob, bblob.data(), bblob.size(), cudaMemcpyHostToDevice));
+  }
+  if (!I->warp_ok && !I->lanes_ok && !I->blk_ok) {
+    *err = "mechanism fits no kernel: " + I->warp_why + "; " + I->lanes_why + "; " +
+           I->blk_why;
     return false;
   }
   if (I->lanes_ok) {
@@ -2496,13 +2673,138 @@ void Engine::fill_args(SolveArgs* a, const WarpLaunch& w, const SolveSettings& s
   a->lu_mode = s.lu_mode;
 }
 
+// shared-memory layout of one block of the CTA-per-cell kernel
+static BlkLayout make_blk_layout(const BlockOff& o, int lt, bool zn_in_smem) {
+  BlkLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const int r = (int)off;
+    off = (off + bytes + 15) & ~size_t(15);
+    return r;
+  };
+  const size_t n = (size_t)o.n;
+  L.ctx = take(sizeof(blk::Ctx<double>));
+  L.ctl = take(sizeof(double) * (LMAX + 2 + 8 + LMAX + 1));
+  L.y = take(8 * n);
+  L.ewt = take(8 * n);
+  L.acor = take(8 * n);
+  L.ftemp = take(8 * n);
+  L.tempv = take(8 * n);
+  L.part = take(8 * (size_t)std::max(o.n_rxn, o.n_part));
+  L.keff = take(8 * (size_t)o.n_rxn);
+  L.dinv = take((size_t)lt * n);
+  L.z = take((size_t)lt * n);
+  L.zn = zn_in_smem ? take(8 * LMAX * n) : -1;
+  L.lu = take((size_t)lt * o.n_lu);
+  L.bytes = (int)off;
+  return L;
+}
+
+static void* block_kernel_fn(int precision) {
+  return precision == 1 ? (void*)block_kernel<float> : (void*)block_kernel<double>;
+}
+
+struct BlkLaunch {
+  int grid = 0, lt = 8, per_sm = 0;
+  BlkLayout lay{};
+};
+
+// the layout that fits the most blocks per SM (the Nordsieck history in
+// shared memory on a tie), one block per cell at most
+static bool plan_blk_launch(const BlockOff& o, int sm_count, int max_smem, int precision,
+                            int n_cells, BlkLaunch* b, std::string* err) {
+  b->lt = precision == 1 ? 4 : 8;
+  void* fn = block_kernel_fn(precision);
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  b->per_sm = 0;
+  for (int zs = 1; zs >= 0; --zs) {
+    const BlkLayout L = make_blk_layout(o, b->lt, zs == 1);
+    if (L.bytes > max_smem) continue;
+    int nb = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, blk::kThreads, (size_t)L.bytes));
+    if (nb > b->per_sm) {
+      b->per_sm = nb;
+      b->lay = L;
+    }
+  }
+  if (b->per_sm < 1) {
+    *err = "mechanism too large for the CTA-per-cell shared-memory layout";
+    return false;
+  }
+  b->grid = std::max(1, std::min(sm_count * b->per_sm, n_cells));
+  return true;
+}
+
+bool Engine::block_tables() const { return impl_->blk_ok; }
+
+int Engine::effective_kernel(const SolveSettings& s) const {
+  if (s.kernel != 0) return s.kernel;
+  if (impl_->warp_ok) return 0;
+  return impl_->blk_ok ? 2 : 1;
+}
+
+bool Engine::launch_block(double* d_state, const double* d_env, const double* d_photo,
+                          const int* d_order, int n_cells, double t0, double t1,
+                          const SolveSettings& s, void* stream, std::string* err) {
+  Impl* I = impl_;
+  if (!I->blk_ok) {
+    *err = "the CTA-per-cell kernel cannot run this mechanism: " + I->blk_why;
+    return false;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  BlkLaunch b;
+  if (!plan_blk_launch(I->boff, I->sm_count, I->max_smem, s.precision, n_cells, &b, err))
+    return false;
+  if (!ensure(&I->d_stats, &I->c_stats, sizeof(CellStats) * (size_t)n_cells, err)) return false;
+  if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)b.lt * I->boff.n_jac * b.grid, err))
+    return false;
+  const int hist_stride = b.lay.zn >= 0 ? 0 : (LMAX * I->boff.n + 31) & ~31;
+  if (hist_stride &&
+      !ensure(&I->d_hist, &I->c_hist, sizeof(double) * (size_t)hist_stride * b.grid, err))
+    return false;
+  BlkArgs a{};
+  a.m = I->m;
+  a.blob = (const char*)I->d_bblob;
+  a.lay = b.lay;
+  a.state = d_state;
+  a.env = d_env;
+  a.photo = I->m.n_photo > 0 ? d_photo : nullptr;
+  a.order = d_order;
+  a.tspan = nullptr;
+  a.n_cells = n_cells;
+  a.counter = I->d_counter;
+  a.stats = (CellStats*)I->d_stats;
+  a.jscratch = I->d_jscratch;
+  a.hist = (double*)I->d_hist;
+  a.hist_stride = hist_stride;
+  a.t0 = t0;
+  a.t1 = t1;
+  a.rtol = s.rtol;
+  a.max_steps = s.max_steps;
+  a.maxncf = s.max_conv_fails;
+  a.maxnef = s.max_conv_fails;
+  void* fn = block_kernel_fn(s.precision);
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, b.lay.bytes));
+  void* args[] = {&a};
+  CK(cudaEventRecord(I->ev0, st));
+  CK(cudaMemsetAsync(I->d_counter, 0, sizeof(int), st));
+  CK(cudaLaunchKernel(fn, dim3(b.grid), dim3(blk::kThreads), args, (size_t)b.lay.bytes, st));
+  CK(cudaEventRecord(I->ev1, st));
+  I->ev_pending = true;
+  ++launches_;
+  return true;
+}
+
 bool Engine::launch_solve(double* d_state, const double* d_env, const double* d_photo,
                           const int* d_order, int n_cells, double t0, double t1,
                           const SolveSettings& s, void* stream, std::string* err) {
   Impl* I = impl_;
   if (n_cells <= 0) return true;
   cudaStream_t st = (cudaStream_t)stream;
-  if (s.kernel == 1 || !I->warp_ok) {
+  const int kern = effective_kernel(s);
+  if (kern == 2)
+    return launch_block(d_state, d_env, d_photo, d_order, n_cells, t0, t1, s, stream, err);
+  if (kern == 1) {
     if (!I->lanes_ok) {
       *err = "the lane-per-cell kernel cannot run this mechanism: " + I->lanes_why;
       return false;
@@ -2606,7 +2908,7 @@ bool Engine::warp_tables(std::string* err) const {
   if (impl_->warp_ok) return true;
   *err = "this entry point runs the warp-per-cell kernel, whose tables this mechanism "
          "exceeds (" + impl_->warp_why + "); solver_run and the device runs use the "
-         "lane-per-cell kernel for it";
+         "block-per-cell or lane-per-cell kernel for it";
   return false;
 }
 

@@ -137,7 +137,8 @@ class Solver:
             raise SolverError(_lib.last_error())
 
     def set_kernel(self, kernel: int, place: int = -1) -> None:
-        """0 = warp per cell, 1 = lane per cell (place: shared-memory bits)."""
+        """0 = warp per cell, 1 = lane per cell (place: shared-memory bits),
+        2 = block per cell."""
         if self.lib.camp_b200_set_kernel(self._h, int(kernel), int(place)) != 0:
             raise SolverError(_lib.last_error())
 
@@ -284,6 +285,10 @@ class Solver:
                        ("hcur", np.float64)])
         return np.frombuffer(bytes(arr), dtype=dt).copy()
 
+    def kernel(self) -> int:
+        """The kernel solver_run uses: 0 warp, 1 lane, 2 block per cell."""
+        return int(self.lib.camp_b200_get_kernel(self._h))
+
     def kernel_launches(self) -> int:
         return int(self.lib.camp_b200_kernel_launches(self._h))
 
@@ -322,6 +327,16 @@ class Solver:
 
     def n_lu(self) -> int:
         return int(self.lib.camp_b200_n_lu_elem(self._h))
+
+    def block_tables(self) -> bytes:
+        """The block-per-cell kernel's tables as built on the host (the
+        BlockOff header, then its sections)."""
+        n = int(self.lib.camp_b200_get_block_tables(self._h, None, 0))
+        if n < 0:
+            raise SolverError(_lib.last_error())
+        buf = (C.c_uint8 * n)()
+        self.lib.camp_b200_get_block_tables(self._h, buf, n)
+        return bytes(buf)
 
     def check_jac(self, state, env, h: float, rel_tol: float = 1e-4, abs_tol: float = 1e-9):
         """Finite-difference audit of the device Jacobian at these states;

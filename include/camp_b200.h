@@ -181,8 +181,12 @@ int camp_b200_set_launch(void *solver_data, int warps_per_block, int blocks_per_
  * (fewer warp synchronisations).  The autotuner picks per mechanism. */
 int camp_b200_set_lu_mode(void *solver_data, int mode);
 /* Kernel organisation: 0 = one warp per cell (lanes share a cell's sparse
- * work), 1 = one lane per cell (32 cells per warp share every instruction).
- * place (lane kernel only): bit 0 keeps the state y, bit 1 the LU factors and
+ * work), 1 = one lane per cell (32 cells per warp share every instruction),
+ * 2 = one thread block per cell (the cell's LU in the block's shared memory,
+ * f, J, factorization and solves on all its warps; gas-phase mechanisms, for
+ * LUs beyond the warp kernel's tables).  With 0 on a mechanism beyond the
+ * warp kernel's tables the solve runs the block form where it has its
+ * tables, else the lane form.  place (lane kernel only): bit 0 keeps the state y, bit 1 the LU factors and
  * bit 2 the solve vector in shared memory; the rest of a cell's working set
  * lives in a lane-interleaved global scratch.  -1 keeps the current value. */
 int camp_b200_set_kernel(void *solver_data, int kernel, int place);
@@ -199,7 +203,8 @@ int camp_b200_set_layout(void *solver_data, int hist_global);
  * modified) once per candidate launch configuration -- for the warp-per-cell
  * kernel the cells per block, the history layout of camp_b200_set_layout and
  * the LU mode of camp_b200_set_lu_mode, and the lane-per-cell kernel (32
- * cells per warp) where the mechanism has its tables -- for the current
+ * cells per warp) and the block-per-cell kernel where the mechanism has
+ * their tables -- for the current
  * precision, and keeps the fastest by kernel time.  Use a sample
  * representative of the cells to be solved (a few thousand cells, the host
  * step of the run).  0 or -1. */
@@ -209,8 +214,9 @@ int camp_b200_autotune(void *solver_data, const double *state, const double *env
  * when not tuned). */
 int camp_b200_get_tuning(void *solver_data, int *warps_per_block, int *hist_global,
                          int *lu_mode, double *sample_ms);
-/* The kernel in use: 0 warp per cell, 1 lane per cell (camp_b200_set_kernel,
- * or the autotuner's choice). */
+/* The kernel solver_run uses: 0 warp per cell, 1 lane per cell, 2 block per
+ * cell (camp_b200_set_kernel, the autotuner's choice, or the form a
+ * mechanism beyond the warp kernel's tables falls back to). */
 int camp_b200_get_kernel(void *solver_data);
 /* Orders the cells of the next run by decreasing internal step count of the
  * previous run (longest-first scheduling of the persistent kernel). */
@@ -297,6 +303,12 @@ int camp_b200_rxn_int_data_size(void *solver_data);
 int camp_b200_get_solver_jac(void *solver_data, int *col_ptrs, int *row_ids);
 int camp_b200_get_rxn_int_data(void *solver_data, int *out);
 int camp_b200_get_lu_order(void *solver_data, int *perm);
+/* The block-per-cell kernel's tables (the BlockOff header of blob.hpp, then
+ * its sections; absolute tolerances zeroed), built on the host from the
+ * sparsity: returns their size in bytes and copies them to out when
+ * capacity allows; -1 (with camp_b200_last_error) when the mechanism has no
+ * such tables. */
+long camp_b200_get_block_tables(void *solver_data, void *out, long capacity);
 /* The solver-Jacobian fold J_solver[s] += J_rxn[r] * J_params[p] as (s, r,
  * p) triplets in the reference's order (src/camp_solver.c:1649-1681; p = 0
  * is the unit parameter, the others the sub-model parameter Jacobian's

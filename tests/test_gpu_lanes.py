@@ -1,14 +1,15 @@
-"""The lane-per-cell kernel, and the large synthetic mechanism that only it
-runs.
+"""The lane-per-cell and block-per-cell kernels, and the large synthetic
+mechanism that only they run.
 
 The lane kernel (one lane per cell, 32 cells of a warp sharing every table
-read) is a second CUDA implementation of the same per-cell BDF solve; on
-cb05cl_ae5 and the mod37 gas phase it must reach the warp kernel's outcomes
-and values.  The synthetic 200-species / 600-reaction mechanism has an LU of
-18 681 entries with 622 765 Schur updates, beyond the warp kernel's 16-bit
-schedules: solver_initialize keeps only the lane kernel for it (tables read
-from global memory), solver_run uses it, and the warp-only entry points say
-why they refuse.
+read) and the block kernel (one thread block per cell, the cell's LU in
+shared memory) are two more CUDA implementations of the same per-cell BDF
+solve; on cb05cl_ae5 and the mod37 gas phase each must reach the warp
+kernel's outcomes and values.  The synthetic 200-species / 600-reaction
+mechanism has an LU of 18 681 entries with 622 765 Schur updates, beyond the
+warp kernel's 16-bit schedules: solver_run uses the block kernel for it by
+default (the lane kernel on request), and the warp-only entry points say why
+they refuse.
 
 The synthetic mechanism gains molecules in every reaction (1-4 unit-yield
 products from 1-2 reactants), so its concentrations grow quickly: at a 300 s
@@ -72,9 +73,10 @@ def _same_accuracy(mech, a, b, tight, rows):
         np.percentile(ea, 90), np.percentile(eb, 90))
 
 
+@pytest.mark.parametrize("kernel", [1, 2])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("which", ["cb05", "mod37"])
-def test_lane_kernel_matches_warp_kernel(request, which, precision):
+def test_lane_kernel_matches_warp_kernel(request, which, precision, kernel):
     """Same outcomes as the warp kernel, and the reference algorithm's
     accuracy (the oracle at equal tolerances), both against the tight
     solution.  The error distributions need a few dozen finishing cells: on
@@ -85,7 +87,7 @@ def test_lane_kernel_matches_warp_kernel(request, which, precision):
     mech = request.getfixturevalue(which)
     cells = make_cells(mech, 64, 23)
     _, xw, sw = _solve(mech, cells, precision, 0, 60.0, 1500)
-    _, xl, sl = _solve(mech, cells, precision, 1, 60.0, 1500)
+    _, xl, sl = _solve(mech, cells, precision, kernel, 60.0, 1500)
     assert np.mean(sw == sl) >= 0.9
     _, ost, _, yo = OracleModel(mech).solve(cells.state.copy(), cells.env, cells.photo_rates,
                                             0.0, 60.0, 1e-4, np.full(mech.n_state_var, 1e-8),
@@ -106,14 +108,17 @@ def large():
         return load_synthetic(td, 200, 600)
 
 
+@pytest.mark.parametrize("kernel", [None, 1])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_large_mechanism_matches_oracle(large, precision):
+def test_large_mechanism_matches_oracle(large, precision, kernel):
+    """The default (block) and the lane kernel against the oracle."""
     from camp_b200.cells import make_cells
     from oracle.oracle import OracleModel
 
     mech, base = large
     cells = make_cells(mech, 32, 29, conc_lo=1e-8, photo_base=base)
-    s, x, st = _solve(mech, cells, precision, None, T_LARGE, 10000)
+    s, x, st = _solve(mech, cells, precision, kernel, T_LARGE, 10000)
+    assert s.kernel() == (2 if kernel is None else kernel)
     nf, ost, _, y = OracleModel(mech).solve(cells.state.copy(), cells.env, cells.photo_rates,
                                             0.0, T_LARGE, 1e-4, np.full(mech.n_state_var, 1e-8),
                                             n_threads=os.cpu_count() or 1)
