@@ -2715,11 +2715,16 @@ static bool plan_blk_launch(const BlockOff& o, int sm_count, int max_smem, int p
                             int n_cells, BlkLaunch* b, std::string* err) {
   b->lt = precision == 1 ? 4 : 8;
   void* fn = block_kernel_fn(precision);
-  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+  // the kernel's static shared memory (the command slot) counts against the
+  // same per-block limit
+  cudaFuncAttributes fa{};
+  CK(cudaFuncGetAttributes(&fa, fn));
+  const int max_dyn = max_smem - (int)fa.sharedSizeBytes;
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
   b->per_sm = 0;
   for (int zs = 1; zs >= 0; --zs) {
     const BlkLayout L = make_blk_layout(o, b->lt, zs == 1);
-    if (L.bytes > max_smem) continue;
+    if (L.bytes > max_dyn) continue;
     int nb = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, blk::kThreads, (size_t)L.bytes));
     if (nb > b->per_sm) {
