@@ -24,7 +24,7 @@ CXXFLAGS = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", "-lineinfo"]
 SOURCES = ["model.cpp", "blob.cpp", "json.cpp", "loader.cpp", "capi.cpp", "serve.cpp", "solve.cu",
            "lanes.cu"]
 HEADERS = ["model.hpp", "engine.hpp", "blob.hpp", "json.hpp", "loader.hpp", "serve.hpp",
-           "bdf_consts.hpp", "rates.cuh",
+           "bdf_consts.hpp", "rates.cuh", "block.cuh",
            os.path.join("..", "..", "include", "camp_b200.h")]
 
 

@@ -687,6 +687,11 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
     if (!full) break;
     r0 = c;
   }
+  if (n - r0 > kBlockMaxDense) {
+    *err = "the LU's trailing dense block (" + std::to_string(n - r0) +
+           " rows) exceeds the CTA kernel's " + std::to_string(kBlockMaxDense);
+    return false;
+  }
   std::vector<uint16_t> dpos(n - r0), ub(r0);
   for (int i = r0; i < n; ++i) dpos[i - r0] = (uint16_t)pos[(size_t)i * n + r0];
   for (int i = 0; i < r0; ++i) {
@@ -694,26 +699,38 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
     while (q > t.lu_diag[i] + 1 && t.lu_col[q - 1] >= r0) --q;
     ub[i] = (uint16_t)q;
   }
-  // head pivots: L entries of each column, and the update target of every
-  // (L entry, U entry) pair
-  std::vector<uint32_t> lk_ptr(r0 + 1, 0), tg_ptr(r0 + 1, 0);
-  std::vector<uint16_t> lk_pos, tg;
+  // head pivots: L entries of each column (row order), and the tabulated
+  // update targets: head rows against every U entry of row k, dense rows
+  // against the U entries in head columns
+  std::vector<uint32_t> lk_ptr(r0 + 1, 0), lk_mid(std::max(r0, 1), 0), tg_ptr(r0 + 1, 0);
+  std::vector<uint16_t> lk_pos, lk_row, tg;
   for (int k = 0; k < r0; ++k) {
     lk_ptr[k] = (uint32_t)lk_pos.size();
     tg_ptr[k] = (uint32_t)tg.size();
+    std::vector<int> rows;
     for (int i = k + 1; i < n; ++i) {
       const int q = pos[(size_t)i * n + k];
       if (q < 0) continue;
+      rows.push_back(i);
       lk_pos.push_back((uint16_t)q);
-      for (int p = t.lu_diag[k] + 1; p < t.lu_rowptr[k + 1]; ++p) {
-        const int d = pos[(size_t)i * n + t.lu_col[p]];
-        if (d < 0) {
-          *err = "internal: LU fill pattern not closed";
-          return false;
-        }
-        tg.push_back((uint16_t)d);
-      }
+      lk_row.push_back((uint16_t)i);
     }
+    lk_mid[k] = (uint32_t)lk_ptr[k];
+    for (int i : rows)
+      if (i < r0) ++lk_mid[k];
+    for (int pass = 0; pass < 2; ++pass)
+      for (int i : rows) {
+        if ((i >= r0) != (pass == 1)) continue;
+        const int p1 = pass == 0 ? t.lu_rowptr[k + 1] : ub[k];
+        for (int p = t.lu_diag[k] + 1; p < p1; ++p) {
+          const int d = pos[(size_t)i * n + t.lu_col[p]];
+          if (d < 0) {
+            *err = "internal: LU fill pattern not closed";
+            return false;
+          }
+          tg.push_back((uint16_t)d);
+        }
+      }
   }
   lk_ptr[r0] = (uint32_t)lk_pos.size();
   tg_ptr[r0] = (uint32_t)tg.size();
@@ -747,6 +764,25 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
   std::vector<uint16_t> hf_ptr, hf_rows, hb_ptr, hb_rows;
   levels(flev, n_hf, &hf_ptr, &hf_rows);
   levels(blev, n_hb, &hb_ptr, &hb_rows);
+  // the solve's staged section
+  std::vector<uint16_t> stage;
+  auto sec = [&](const std::vector<uint16_t>& v) {
+    const int off = (int)stage.size();
+    stage.insert(stage.end(), v.begin(), v.end());
+    return off;
+  };
+  std::vector<uint16_t> ndoff(n + 1, 0), ndcol, dbase(n - r0);
+  for (int i = 0; i < n; ++i) {
+    ndoff[i] = (uint16_t)ndcol.size();
+    const int q1 = i < r0 ? t.lu_rowptr[i + 1] : dpos[i - r0];
+    for (int q = t.lu_rowptr[i]; q < q1; ++q) ndcol.push_back((uint16_t)t.lu_col[q]);
+  }
+  ndoff[n] = (uint16_t)ndcol.size();
+  for (int i = r0; i < n; ++i) dbase[i - r0] = (uint16_t)(dpos[i - r0] - r0);
+  if (ndcol.size() > 65535) {
+    *err = "mechanism exceeds the CTA-kernel table encodings";
+    return false;
+  }
   auto u16 = [](const std::vector<int>& v) {
     std::vector<uint16_t> o(v.size());
     for (size_t i = 0; i < v.size(); ++i) o[i] = (uint16_t)v[i];
@@ -784,6 +820,8 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
   o.ub = w.put(ub);
   o.lk_ptr = w.put(lk_ptr);
   o.lk_pos = w.put(lk_pos);
+  o.lk_row = w.put(lk_row);
+  o.lk_mid = w.put(lk_mid);
   o.tg_ptr = w.put(tg_ptr);
   o.tg = w.put(tg);
   o.hf_ptr = w.put(hf_ptr);
@@ -792,6 +830,20 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
   o.hb_rows = w.put(hb_rows);
   o.dep_state = w.put(u16(t.dep_state));
   o.atol = w.put(atol_dep);
+  o.sg_rowptr = sec(u16(t.lu_rowptr));
+  o.sg_diag = sec(u16(t.lu_diag));
+  o.sg_ub = sec(ub);
+  o.sg_perm = sec(u16(t.lu_perm));
+  o.sg_hf_ptr = sec(hf_ptr);
+  o.sg_hf_rows = sec(hf_rows);
+  o.sg_hb_ptr = sec(hb_ptr);
+  o.sg_hb_rows = sec(hb_rows);
+  o.sg_ndoff = sec(ndoff);
+  o.sg_ndcol = sec(ndcol);
+  o.sg_dbase = sec(dbase);
+  stage.resize((stage.size() + 7) & ~size_t(7), 0);  // whole 16-byte units
+  o.sg_len = (int)stage.size();
+  o.stage = w.put(stage);
   w.buf.resize((w.buf.size() + 15) & ~size_t(15), 0);
   o.bytes = (int)w.buf.size();
   memcpy(w.buf.data(), &o, sizeof(o));

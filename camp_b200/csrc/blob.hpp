@@ -154,15 +154,33 @@ struct BlockOff {
   int lu_perm, lu_rowptr, lu_col, lu_diag;
   int dpos;  // per dense row: position of its column r0 (uint16)
   int ub;    // per head row: first position with a column >= r0 (uint16)
-  // head pivots k < r0: L entries of column k (pointers uint32, r0 + 1;
-  // positions uint16) and the update targets, row-major over (L entry, U
-  // entry of row k) (pointers uint32, r0 + 1; positions uint16)
-  int lk_ptr, lk_pos, tg_ptr, tg;
+  // head pivots k < r0: L entries of column k in row order (pointers
+  // uint32, r0 + 1; positions and rows uint16), the first of them in a
+  // dense row (uint32 per pivot), and the tabulated update targets (pointers
+  // uint32, r0 + 1; positions uint16): the head rows' L entries against
+  // every U entry of row k, then the dense rows' against the U entries of
+  // row k in head columns, row-major.  The dense rows' updates in dense
+  // columns are addressed through the dense block.
+  int lk_ptr, lk_pos, lk_row, lk_mid, tg_ptr, tg;
   // head row levels (pointers uint16, levels + 1; rows uint16)
   int hf_ptr, hf_rows, hb_ptr, hb_rows;
   int dep_state;  // uint16
   int atol;       // double
+  // the solve's tables, one uint16 section the block copies into shared
+  // memory (stage: byte offset, sg_len: elements); element offsets inside:
+  // row pointers (n + 1), diagonals (n), head rows' ub (r0), permutation
+  // (n), head levels (forward pointers and rows, backward pointers and
+  // rows), per row the first of its non-dense entries in ndcol (n + 1; the
+  // head rows' entries, the dense rows' head-column entries) and their
+  // columns, and the dense rows' bases (dpos - r0, m)
+  int stage, sg_len;
+  int sg_rowptr, sg_diag, sg_ub, sg_perm, sg_hf_ptr, sg_hf_rows, sg_hb_ptr, sg_hb_rows;
+  int sg_ndoff, sg_ndcol, sg_dbase;
 };
+
+// the largest trailing dense block the CTA kernel holds in registers
+// (a 16 x 16 thread grid, 7 x 7 entries per thread)
+constexpr int kBlockMaxDense = 112;
 
 bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
                       std::vector<uint8_t>* blob, BlockOff* off, std::string* err);

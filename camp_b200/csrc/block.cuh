@@ -21,20 +21,38 @@
 //
 // The factorization is right-looking, one barrier per pivot: the updates of
 // pivot k (targets (i, j), i, j > k) never touch column k or row k, so they
-// run in parallel, and the L entries of column k are scaled by the pivot's
-// reciprocal during pivot k + 1 (nothing reads or writes them there).  Each
-// target receives its updates in increasing pivot order, as in the row-wise
-// (up-looking) form.  The trailing dense block of the LU is addressed without
-// tables; the sparse head uses tabulated targets.  The solves handle the
-// sparse head by row levels and the dense block by panels of 32 columns: one
-// warp solves the panel's triangle with shuffles, all warps update the rows
-// beyond it (one row per warp, one column per lane).
+// run in parallel.  Each target receives its updates in increasing pivot
+// order, as in the row-wise (up-looking) form.  The trailing dense block of
+// the LU (up to 112 x 112) lives in registers for the whole factorization:
+// the block's threads form a 16 x 16 grid, thread (p, q) holding the dense
+// entries (p + 16 s, q + 16 t); every pivot is a rank-1 update of those
+// registers from two vectors exchanged through shared memory (the pivot's
+// column of multipliers and its row of U), so the dense block's Schur
+// updates cost no shared-memory traffic.  The sparse head pivots update the
+// head rows and the dense rows' head columns in shared memory from
+// tabulated targets and the dense block through the same exchange (their
+// columns and rows scattered into zeroed vectors); their L entries are
+// scaled by the pivot's reciprocal during pivot k + 1.  The exchange
+// vectors rotate over three buffers, so a pivot's scatter never meets a
+// slower warp's reads of the previous pivot's vectors and each buffer is
+// zeroed two pivots after its use.
+//
+// The solves read their tables from shared memory (a section of the blob
+// each block copies once): the sparse head by row levels, the dense rows'
+// head columns and the head rows' dense columns one row per warp, and the
+// dense block's triangles on one warp with the block's values in registers
+// (the column value broadcast by a shuffle), without barriers.
 #pragma once
 
 namespace blk {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kTile = 7;    // factorization: dense entries per thread and dimension
+constexpr int kSlots = 4;   // solves: dense rows per lane
+constexpr int kMaxDense = campb::kBlockMaxDense;  // = 16 * kTile <= 32 * kSlots
+static_assert(kMaxDense == 16 * kTile && kMaxDense <= 32 * kSlots, "dense block tiling");
+constexpr int kXBuf = 3 * 2 * kMaxDense;  // exchange vectors (LT elements)
 
 enum Op : int { OP_EXIT = 0, OP_F = 1, OP_JAC = 2, OP_FACTOR = 3, OP_SOLVE = 4 };
 
@@ -47,11 +65,12 @@ struct Cmd {
 
 struct Tab {
   const uint32_t *rx_word, *rx_vptr, *fg_ptr, *fg_ent, *jg_ptr, *jg_mid, *jg_w0;
-  const uint32_t *lk_ptr, *tg_ptr;
-  const uint16_t *jg_w1, *jg_row, *lu_src, *lu_perm, *lu_rowptr, *lu_col, *lu_diag;
-  const uint16_t *dpos, *ub, *lk_pos, *tg, *hf_ptr, *hf_rows, *hb_ptr, *hb_rows, *dep_state;
+  const uint32_t *lk_ptr, *lk_mid, *tg_ptr;
+  const uint16_t *jg_w1, *jg_row, *lu_src, *lk_pos, *lk_row, *tg, *dep_state, *stage;
   const double *coef, *atol;
-  int n, n_rxn, n_jac, n_lu, r0, n_hf, n_hb;
+  int n, n_rxn, n_jac, n_lu, r0, n_hf, n_hb, sg_len;
+  int sg_rowptr, sg_diag, sg_ub, sg_perm, sg_hf_ptr, sg_hf_rows, sg_hb_ptr, sg_hb_rows;
+  int sg_ndoff, sg_ndcol, sg_dbase;
 };
 
 __device__ __forceinline__ Tab make_tab(const char* b) {
@@ -65,23 +84,16 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.jg_mid = (const uint32_t*)(b + o.jg_mid);
   t.jg_w0 = (const uint32_t*)(b + o.jg_w0);
   t.lk_ptr = (const uint32_t*)(b + o.lk_ptr);
+  t.lk_mid = (const uint32_t*)(b + o.lk_mid);
   t.tg_ptr = (const uint32_t*)(b + o.tg_ptr);
   t.jg_w1 = (const uint16_t*)(b + o.jg_w1);
   t.jg_row = (const uint16_t*)(b + o.jg_row);
   t.lu_src = (const uint16_t*)(b + o.lu_src);
-  t.lu_perm = (const uint16_t*)(b + o.lu_perm);
-  t.lu_rowptr = (const uint16_t*)(b + o.lu_rowptr);
-  t.lu_col = (const uint16_t*)(b + o.lu_col);
-  t.lu_diag = (const uint16_t*)(b + o.lu_diag);
-  t.dpos = (const uint16_t*)(b + o.dpos);
-  t.ub = (const uint16_t*)(b + o.ub);
   t.lk_pos = (const uint16_t*)(b + o.lk_pos);
+  t.lk_row = (const uint16_t*)(b + o.lk_row);
   t.tg = (const uint16_t*)(b + o.tg);
-  t.hf_ptr = (const uint16_t*)(b + o.hf_ptr);
-  t.hf_rows = (const uint16_t*)(b + o.hf_rows);
-  t.hb_ptr = (const uint16_t*)(b + o.hb_ptr);
-  t.hb_rows = (const uint16_t*)(b + o.hb_rows);
   t.dep_state = (const uint16_t*)(b + o.dep_state);
+  t.stage = (const uint16_t*)(b + o.stage);
   t.coef = (const double*)(b + o.coef);
   t.atol = (const double*)(b + o.atol);
   t.n = o.n;
@@ -91,6 +103,18 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.r0 = o.r0;
   t.n_hf = o.n_hf;
   t.n_hb = o.n_hb;
+  t.sg_len = o.sg_len;
+  t.sg_rowptr = o.sg_rowptr;
+  t.sg_diag = o.sg_diag;
+  t.sg_ub = o.sg_ub;
+  t.sg_perm = o.sg_perm;
+  t.sg_hf_ptr = o.sg_hf_ptr;
+  t.sg_hf_rows = o.sg_hf_rows;
+  t.sg_hb_ptr = o.sg_hb_ptr;
+  t.sg_hb_rows = o.sg_hb_rows;
+  t.sg_ndoff = o.sg_ndoff;
+  t.sg_ndcol = o.sg_ndcol;
+  t.sg_dbase = o.sg_dbase;
   return t;
 }
 
@@ -111,11 +135,15 @@ struct Ctx {
   Tab t;
   const double* keff;
   double* part;  // term rates (f) or rate partials (J)
+  LT* xbuf;      // the factorization's exchange vectors (over part)
   LT* J;         // solver Jacobian slots (global)
   LT* LU;
   LT* dinv;
   LT* z;
   double* rhs;   // right-hand side and solution of the solves
+  // the staged solve tables
+  const uint16_t *rowptr, *diag, *ub, *perm, *hf_ptr, *hf_rows, *hb_ptr, *hb_rows;
+  const uint16_t *ndoff, *ndcol, *dbase;
 };
 
 // f(y) into out (src/time_derivative.c:90-97 with the negative-yield guard
@@ -223,68 +251,160 @@ template <typename LT>
 __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
   const Tab& t = c.t;
   LT* LU = c.LU;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n = t.n, r0 = t.r0, m = n - r0;
   #pragma unroll 1
-  for (int p = threadIdx.x; p < t.n_lu; p += kThreads) {
+  for (int p = tid; p < t.n_lu; p += kThreads) {
     const int s = __ldg(t.lu_src + p);
     double v = (s & 0x7FFF) ? -gamma * (double)c.J[(s & 0x7FFF) - 1] : 0.0;
     if (s & 0x8000) v += 1.0;
     LU[p] = (LT)v;
   }
+  #pragma unroll 1
+  for (int e = tid; e < kXBuf; e += kThreads) c.xbuf[e] = (LT)0;
   bsync();
-  const int n = t.n, r0 = t.r0;
+  // this thread's entries of the dense block: (p + 16 s, q + 16 u)
+  const int p = tid >> 4, q = tid & 15;
+  LT a[kTile][kTile];
+  #pragma unroll
+  for (int s = 0; s < kTile; ++s)
+  #pragma unroll
+    for (int u = 0; u < kTile; ++u) {
+      const int di = p + 16 * s, dj = q + 16 * u;
+      a[s][u] = (di < m && dj < m) ? LU[c.dbase[di] + r0 + dj] : (LT)0;
+    }
   bool bad = false;
   LT dprev = (LT)0;
+  // sparse head pivots
   #pragma unroll 1
-  for (int k = 0; k < n; ++k) {
-    const LT piv = LU[__ldg(t.lu_diag + k)];
+  for (int k = 0; k < r0; ++k) {
+    LT* lb = c.xbuf + (k % 3) * (2 * kMaxDense);
+    LT* ubf = lb + kMaxDense;
+    const LT piv = LU[c.diag[k]];
     const bool pb = (piv == (LT)0) || !isfinite((double)piv);
     bad |= pb;
     const LT dk = pb ? (LT)0 : (LT)(1.0 / (double)piv);
-    if (threadIdx.x == 0) c.dinv[k] = dk;
-    // scale the L entries of column k - 1 (its updates ran at pivot k - 1)
+    if (tid == 0) c.dinv[k] = dk;
+    // the buffer two pivots on (last read before the previous barrier)
+    LT* nb = c.xbuf + ((k + 1) % 3) * (2 * kMaxDense);
+    #pragma unroll 1
+    for (int e = tid; e < 2 * kMaxDense; e += kThreads) nb[e] = (LT)0;
     if (k > 0) {
-      const int kp = k - 1;
-      if (kp < r0) {
-        const uint32_t a1 = __ldg(t.lk_ptr + kp + 1);
-        #pragma unroll 1
-        for (uint32_t a = __ldg(t.lk_ptr + kp) + threadIdx.x; a < a1; a += kThreads)
-          LU[__ldg(t.lk_pos + a)] *= dprev;
-      } else {
-        #pragma unroll 1
-        for (int i = k + threadIdx.x; i < n; i += kThreads)
-          LU[__ldg(t.dpos + i - r0) + (kp - r0)] *= dprev;
-      }
-    }
-    if (k < r0) {
-      const uint32_t a0 = __ldg(t.lk_ptr + k), na = __ldg(t.lk_ptr + k + 1) - a0;
-      const int u0 = __ldg(t.lu_diag + k) + 1;
-      const int nu = (int)__ldg(t.lu_rowptr + k + 1) - u0;
-      const uint16_t* tg = t.tg + __ldg(t.tg_ptr + k);
+      const uint32_t e1 = __ldg(t.lk_ptr + k);
       #pragma unroll 1
-      for (uint32_t a = warp; a < na; a += kWarps) {
-        const LT l = LU[__ldg(t.lk_pos + a0 + a)] * dk;
-        const uint16_t* ta = tg + (size_t)a * nu;
-        #pragma unroll 2
-        for (int b = lane; b < nu; b += 32) {
-          const int d = __ldg(ta + b);
-          LU[d] -= l * LU[u0 + b];
-        }
-      }
-    } else {
-      // dense block: rows and columns k+1..n-1
-      const LT* uk = LU + (__ldg(t.dpos + k - r0) - r0);
-      #pragma unroll 1
-      for (int i = k + 1 + warp; i < n; i += kWarps) {
-        LT* ri = LU + (__ldg(t.dpos + i - r0) - r0);
-        const LT l = ri[k] * dk;
-        #pragma unroll 2
-        for (int j = k + 1 + lane; j < n; j += 32) ri[j] -= l * uk[j];
-      }
+      for (uint32_t e = __ldg(t.lk_ptr + k - 1) + tid; e < e1; e += kThreads)
+        LU[__ldg(t.lk_pos + e)] *= dprev;
     }
+    const uint32_t a0 = __ldg(t.lk_ptr + k), am = __ldg(t.lk_mid + k),
+                   a1 = __ldg(t.lk_ptr + k + 1);
+    const int u0 = c.diag[k] + 1, uh = c.ub[k], u1 = c.rowptr[k + 1];
+    const int nu = u1 - u0, nuh = uh - u0;
+    const uint16_t* tg = t.tg + __ldg(t.tg_ptr + k);
+    // head rows against every U entry of row k
+    #pragma unroll 1
+    for (uint32_t e = a0 + warp; e < am; e += kWarps) {
+      const LT l = LU[__ldg(t.lk_pos + e)] * dk;
+      const uint16_t* ta = tg + (size_t)(e - a0) * nu;
+      #pragma unroll 2
+      for (int b = lane; b < nu; b += 32) LU[__ldg(ta + b)] -= l * LU[u0 + b];
+    }
+    // dense rows against the U entries in head columns; their multipliers
+    // into the exchange column
+    const uint16_t* tgb = tg + (size_t)(am - a0) * nu;
+    #pragma unroll 1
+    for (uint32_t e = am + warp; e < a1; e += kWarps) {
+      const LT l = LU[__ldg(t.lk_pos + e)] * dk;
+      const uint16_t* ta = tgb + (size_t)(e - am) * nuh;
+      #pragma unroll 2
+      for (int b = lane; b < nuh; b += 32) LU[__ldg(ta + b)] -= l * LU[u0 + b];
+      if (lane == 0) lb[__ldg(t.lk_row + e) - r0] = l;
+    }
+    // row k's U entries in dense columns into the exchange row
+    const uint16_t* cols = c.ndcol + c.ndoff[k] - c.rowptr[k];
+    #pragma unroll 1
+    for (int b = uh + tid; b < u1; b += kThreads) ubf[cols[b] - r0] = LU[b];
     bsync();
+    LT lv[kTile], uv[kTile];
+    #pragma unroll
+    for (int s = 0; s < kTile; ++s) lv[s] = (p + 16 * s < m) ? lb[p + 16 * s] : (LT)0;
+    #pragma unroll
+    for (int u = 0; u < kTile; ++u) uv[u] = (q + 16 * u < m) ? ubf[q + 16 * u] : (LT)0;
+    #pragma unroll
+    for (int s = 0; s < kTile; ++s)
+    #pragma unroll
+      for (int u = 0; u < kTile; ++u) a[s][u] -= lv[s] * uv[u];
     dprev = dk;
   }
+  // dense pivots: kk = 16 s0 + kq, held by the threads with q == kq
+  // (column), p == kq (row) and both (pivot)
+  #pragma unroll
+  for (int s0 = 0; s0 < kTile; ++s0) {
+    #pragma unroll 1
+    for (int kq = 0; kq < 16; ++kq) {
+      const int kk = 16 * s0 + kq;
+      if (kk >= m) break;
+      const int k = r0 + kk;
+      LT* lb = c.xbuf + (k % 3) * (2 * kMaxDense);
+      LT* ubf = lb + kMaxDense;
+      if (q == kq) {
+        #pragma unroll
+        for (int s = 0; s < kTile; ++s) {
+          const int di = p + 16 * s;
+          if (di > kk && di < m) lb[di] = a[s][s0];
+        }
+        if (p == kq) lb[kk] = a[s0][s0];
+      }
+      if (p == kq) {
+        #pragma unroll
+        for (int u = 0; u < kTile; ++u) {
+          const int dj = q + 16 * u;
+          if (dj > kk && dj < m) ubf[dj] = a[s0][u];
+        }
+      }
+      if (kk == 0 && r0 > 0) {
+        // the last head column's L entries
+        const uint32_t e1 = __ldg(t.lk_ptr + r0);
+        #pragma unroll 1
+        for (uint32_t e = __ldg(t.lk_ptr + r0 - 1) + tid; e < e1; e += kThreads)
+          LU[__ldg(t.lk_pos + e)] *= dprev;
+      }
+      bsync();
+      const LT piv = lb[kk];
+      const bool pb = (piv == (LT)0) || !isfinite((double)piv);
+      bad |= pb;
+      const LT dk = pb ? (LT)0 : (LT)(1.0 / (double)piv);
+      if (tid == 0) c.dinv[k] = dk;
+      LT lv[kTile], uv[kTile];
+      #pragma unroll
+      for (int s = 0; s < kTile; ++s) {
+        const int di = p + 16 * s;
+        lv[s] = (di > kk && di < m) ? lb[di] * dk : (LT)0;
+      }
+      #pragma unroll
+      for (int u = 0; u < kTile; ++u) {
+        const int dj = q + 16 * u;
+        uv[u] = (dj > kk && dj < m) ? ubf[dj] : (LT)0;
+      }
+      if (q == kq) {
+        #pragma unroll
+        for (int s = 0; s < kTile; ++s)
+          if (p + 16 * s > kk) a[s][s0] *= dk;
+      }
+      #pragma unroll
+      for (int s = 0; s < kTile; ++s)
+      #pragma unroll
+        for (int u = 0; u < kTile; ++u)
+          if (p + 16 * s > kk && q + 16 * u > kk) a[s][u] -= lv[s] * uv[u];
+    }
+  }
+  #pragma unroll
+  for (int s = 0; s < kTile; ++s)
+  #pragma unroll
+    for (int u = 0; u < kTile; ++u) {
+      const int di = p + 16 * s, dj = q + 16 * u;
+      if (di < m && dj < m) LU[c.dbase[di] + r0 + dj] = a[s][u];
+    }
+  bsync();
   return !bad;
 }
 
@@ -294,109 +414,101 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
   const Tab& t = c.t;
   const LT* LU = c.LU;
   LT* z = c.z;
-  const int n = t.n, r0 = t.r0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = t.n, r0 = t.r0, m = n - r0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   #pragma unroll 1
-  for (int k = threadIdx.x; k < n; k += kThreads) z[k] = (LT)c.rhs[__ldg(t.lu_perm + k)];
+  for (int k = tid; k < n; k += kThreads) z[k] = (LT)c.rhs[c.perm[k]];
   bsync();
   // forward: head rows by levels
   #pragma unroll 1
   for (int l = 0; l < t.n_hf; ++l) {
-    const int p1 = __ldg(t.hf_ptr + l + 1);
+    const int p1 = c.hf_ptr[l + 1];
     #pragma unroll 1
-    for (int p = __ldg(t.hf_ptr + l) + threadIdx.x; p < p1; p += kThreads) {
-      const int i = __ldg(t.hf_rows + p);
+    for (int pp = c.hf_ptr[l] + tid; pp < p1; pp += kThreads) {
+      const int i = c.hf_rows[pp];
+      const int q0 = c.rowptr[i], ne = c.diag[i] - q0;
+      const uint16_t* cols = c.ndcol + c.ndoff[i];
       LT acc = z[i];
-      const int d = __ldg(t.lu_diag + i);
-      #pragma unroll 1
-      for (int q = __ldg(t.lu_rowptr + i); q < d; ++q) acc -= LU[q] * z[__ldg(t.lu_col + q)];
+      #pragma unroll 4
+      for (int e = 0; e < ne; ++e) acc -= LU[q0 + e] * z[cols[e]];
       z[i] = acc;
     }
     bsync();
   }
-  // forward: the head columns of the dense rows, one row per warp
   if (r0 > 0) {
+    // forward: the head columns of the dense rows, one row per warp
     #pragma unroll 1
     for (int i = r0 + warp; i < n; i += kWarps) {
-      const int q1 = __ldg(t.dpos + i - r0);
+      const int q0 = c.rowptr[i], e0 = c.ndoff[i], ne = c.ndoff[i + 1] - e0;
       LT v = (LT)0;
-      #pragma unroll 1
-      for (int q = __ldg(t.lu_rowptr + i) + lane; q < q1; q += 32)
-        v += LU[q] * z[__ldg(t.lu_col + q)];
+      #pragma unroll 2
+      for (int e = lane; e < ne; e += 32) v += LU[q0 + e] * z[c.ndcol[e0 + e]];
       v = lane_sum(v);
       if (lane == 0) z[i] -= v;
     }
     bsync();
   }
-  // forward: dense block by panels
-  #pragma unroll 1
-  for (int c0 = r0; c0 < n; c0 += 32) {
-    const int c1 = min(c0 + 32, n), w = c1 - c0;
-    if (warp == 0) {
-      const int i = c0 + lane;
-      const bool own = lane < w;
-      LT zi = own ? z[i] : (LT)0;
-      const LT* ri = own ? LU + (__ldg(t.dpos + i - r0) - r0) : LU;
-      #pragma unroll 1
-      for (int kk = 0; kk < w - 1; ++kk) {
-        const LT zk = __shfl_sync(0xffffffffu, zi, kk);
-        if (own && lane > kk) zi -= ri[c0 + kk] * zk;
-      }
-      if (own) z[i] = zi;
+  // the dense block on warp 0: lane holds dense rows lane + 32 s
+  if (warp == 0) {
+    LT zr[kSlots];
+    int base[kSlots];
+    #pragma unroll
+    for (int s = 0; s < kSlots; ++s) {
+      const int d = 32 * s + lane;
+      zr[s] = d < m ? z[r0 + d] : (LT)0;
+      base[s] = d < m ? c.dbase[d] + r0 : 0;
     }
-    bsync();
-    if (c1 < n) {
-      const LT zc = lane < w ? z[c0 + lane] : (LT)0;
-      #pragma unroll 1
-      for (int i = c1 + warp; i < n; i += kWarps) {
-        const LT* ri = LU + (__ldg(t.dpos + i - r0) - r0);
-        LT v = lane < w ? ri[c0 + lane] * zc : (LT)0;
-        v = lane_sum(v);
-        if (lane == 0) z[i] -= v;
+    // forward: unit lower triangle
+    #pragma unroll
+    for (int sl = 0; sl < kSlots; ++sl) {
+      if (32 * sl < m) {
+        const int w = min(32, m - 32 * sl);
+        #pragma unroll 1
+        for (int ln = 0; ln < w; ++ln) {
+          const int kk = 32 * sl + ln;
+          const LT zk = __shfl_sync(0xffffffffu, zr[sl], ln);
+          #pragma unroll
+          for (int s = sl; s < kSlots; ++s) {
+            const int d = 32 * s + lane;
+            if (d > kk && d < m) zr[s] -= LU[base[s] + kk] * zk;
+          }
+        }
       }
-      bsync();
     }
-  }
-  // backward: dense block by panels, last first
-  const int np = (n - r0 + 31) / 32;
-  #pragma unroll 1
-  for (int pp = np - 1; pp >= 0; --pp) {
-    const int c0 = r0 + 32 * pp, c1 = min(c0 + 32, n), w = c1 - c0;
-    if (warp == 0) {
-      const int i = c0 + lane;
-      const bool own = lane < w;
-      LT zi = own ? z[i] : (LT)0;
-      const LT di = own ? c.dinv[i] : (LT)0;
-      const LT* ri = own ? LU + (__ldg(t.dpos + i - r0) - r0) : LU;
-      #pragma unroll 1
-      for (int kk = w - 1; kk >= 0; --kk) {
-        if (lane == kk) zi *= di;
-        const LT zk = __shfl_sync(0xffffffffu, zi, kk);
-        if (own && lane < kk) zi -= ri[c0 + kk] * zk;
+    // backward: upper triangle, each row finished by its pivot's reciprocal
+    #pragma unroll
+    for (int sl = kSlots - 1; sl >= 0; --sl) {
+      if (32 * sl < m) {
+        const int w = min(32, m - 32 * sl);
+        #pragma unroll 1
+        for (int ln = w - 1; ln >= 0; --ln) {
+          const int kk = 32 * sl + ln;
+          if (lane == ln) zr[sl] *= c.dinv[r0 + kk];
+          const LT zk = __shfl_sync(0xffffffffu, zr[sl], ln);
+          #pragma unroll
+          for (int s = 0; s <= sl; ++s) {
+            const int d = 32 * s + lane;
+            if (d < kk) zr[s] -= LU[base[s] + kk] * zk;
+          }
+        }
       }
-      if (own) z[i] = zi;
     }
-    bsync();
-    if (c0 > r0) {
-      const LT zc = lane < w ? z[c0 + lane] : (LT)0;
-      #pragma unroll 1
-      for (int i = r0 + warp; i < c0; i += kWarps) {
-        const LT* ri = LU + (__ldg(t.dpos + i - r0) - r0);
-        LT v = lane < w ? ri[c0 + lane] * zc : (LT)0;
-        v = lane_sum(v);
-        if (lane == 0) z[i] -= v;
-      }
-      bsync();
+    #pragma unroll
+    for (int s = 0; s < kSlots; ++s) {
+      const int d = 32 * s + lane;
+      if (d < m) z[r0 + d] = zr[s];
     }
   }
+  bsync();
   if (r0 > 0) {
     // backward: the dense columns of the head rows, one row per warp
     #pragma unroll 1
     for (int i = warp; i < r0; i += kWarps) {
-      const int q1 = __ldg(t.lu_rowptr + i + 1);
+      const int q0 = c.rowptr[i], e0 = c.ndoff[i] - q0;
+      const int q1 = c.rowptr[i + 1];
       LT v = (LT)0;
-      #pragma unroll 1
-      for (int q = __ldg(t.ub + i) + lane; q < q1; q += 32) v += LU[q] * z[__ldg(t.lu_col + q)];
+      #pragma unroll 2
+      for (int qq = c.ub[i] + lane; qq < q1; qq += 32) v += LU[qq] * z[c.ndcol[e0 + qq]];
       v = lane_sum(v);
       if (lane == 0) z[i] -= v;
     }
@@ -404,21 +516,22 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
     // backward: head rows by levels
     #pragma unroll 1
     for (int l = 0; l < t.n_hb; ++l) {
-      const int p1 = __ldg(t.hb_ptr + l + 1);
+      const int p1 = c.hb_ptr[l + 1];
       #pragma unroll 1
-      for (int p = __ldg(t.hb_ptr + l) + threadIdx.x; p < p1; p += kThreads) {
-        const int i = __ldg(t.hb_rows + p);
+      for (int pp = c.hb_ptr[l] + tid; pp < p1; pp += kThreads) {
+        const int i = c.hb_rows[pp];
+        const uint16_t* cols = c.ndcol + c.ndoff[i] - c.rowptr[i];
         LT acc = z[i];
-        const int q1 = __ldg(t.ub + i);
-        #pragma unroll 1
-        for (int q = __ldg(t.lu_diag + i) + 1; q < q1; ++q) acc -= LU[q] * z[__ldg(t.lu_col + q)];
+        const int q1 = c.ub[i];
+        #pragma unroll 4
+        for (int qq = c.diag[i] + 1; qq < q1; ++qq) acc -= LU[qq] * z[cols[qq]];
         z[i] = acc * c.dinv[i];
       }
       bsync();
     }
   }
   #pragma unroll 1
-  for (int k = threadIdx.x; k < n; k += kThreads) c.rhs[__ldg(t.lu_perm + k)] = (double)z[k];
+  for (int k = tid; k < n; k += kThreads) c.rhs[c.perm[k]] = (double)z[k];
   bsync();
 }
 

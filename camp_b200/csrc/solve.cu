@@ -1895,7 +1895,7 @@ __global__ void __launch_bounds__(32 * (AERO ? kMaxCellsAero : kMaxCellsPerBlock
 // control, every warp runs its f, J, factorization and solves
 // ---------------------------------------------------------------------------
 struct BlkLayout {  // byte offsets in the block's shared memory (zn -1: global)
-  int ctx, ctl, y, ewt, acor, ftemp, tempv, part, keff, dinv, z, zn, lu, bytes;
+  int ctx, ctl, y, ewt, acor, ftemp, tempv, part, keff, dinv, z, zn, sg, lu, bytes;
 };
 
 struct BlkArgs {
@@ -1933,12 +1933,33 @@ __global__ void __launch_bounds__(blk::kThreads, sizeof(LT) == 4 ? 2 : 1)
     c.t = blk::make_tab(a.blob);
     c.keff = (const double*)(smem + L.keff);
     c.part = (double*)(smem + L.part);
+    c.xbuf = (LT*)(smem + L.part);
     c.J = (LT*)a.jscratch + (size_t)blockIdx.x * c.t.n_jac;
     c.LU = (LT*)(smem + L.lu);
     c.dinv = (LT*)(smem + L.dinv);
     c.z = (LT*)(smem + L.z);
     c.rhs = (double*)(smem + L.tempv);
+    const uint16_t* sg = (const uint16_t*)(smem + L.sg);
+    c.rowptr = sg + c.t.sg_rowptr;
+    c.diag = sg + c.t.sg_diag;
+    c.ub = sg + c.t.sg_ub;
+    c.perm = sg + c.t.sg_perm;
+    c.hf_ptr = sg + c.t.sg_hf_ptr;
+    c.hf_rows = sg + c.t.sg_hf_rows;
+    c.hb_ptr = sg + c.t.sg_hb_ptr;
+    c.hb_rows = sg + c.t.sg_hb_rows;
+    c.ndoff = sg + c.t.sg_ndoff;
+    c.ndcol = sg + c.t.sg_ndcol;
+    c.dbase = sg + c.t.sg_dbase;
     *cx = c;
+  }
+  {
+    // the solve's tables into shared memory (16-byte units)
+    const campb::BlockOff& o = *reinterpret_cast<const campb::BlockOff*>(a.blob);
+    const uint4* src = reinterpret_cast<const uint4*>(a.blob + o.stage);
+    uint4* dst = reinterpret_cast<uint4*>(smem + L.sg);
+    #pragma unroll 1
+    for (int e = threadIdx.x; e < o.sg_len / 8; e += blk::kThreads) dst[e] = src[e];
   }
   blk::bsync();
   const DevMech& m = a.m;
@@ -2690,11 +2711,13 @@ static BlkLayout make_blk_layout(const BlockOff& o, int lt, bool zn_in_smem) {
   L.acor = take(8 * n);
   L.ftemp = take(8 * n);
   L.tempv = take(8 * n);
-  L.part = take(8 * (size_t)std::max(o.n_rxn, o.n_part));
+  // term rates / partials, and during a factorization its exchange vectors
+  L.part = take(std::max(8 * (size_t)std::max(o.n_rxn, o.n_part), (size_t)lt * blk::kXBuf));
   L.keff = take(8 * (size_t)o.n_rxn);
   L.dinv = take((size_t)lt * n);
   L.z = take((size_t)lt * n);
   L.zn = zn_in_smem ? take(8 * LMAX * n) : -1;
+  L.sg = take(2 * (size_t)o.sg_len);
   L.lu = take((size_t)lt * o.n_lu);
   L.bytes = (int)off;
   return L;

@@ -1,16 +1,18 @@
 """Tables of the block-per-cell kernel, checked on the CPU.
 
 The block-per-cell kernel (camp_b200/csrc/block.cuh) factors I - gamma*J
-right-looking, one pivot at a time: the sparse head pivots from tabulated
-update targets, the trailing dense block of the LU by computed addresses, the
-L entries of column k scaled during pivot k + 1; it solves the head rows by
-levels and the dense block by panels of 32 columns.  These tests replay that
-schedule in numpy on the tables the library builds (every index the kernel
-reads comes from them) for a random matrix with the mechanism's LU pattern,
-and check the factors and the solution against dense linear algebra.  They
-also check the tables' invariants: the dense block is dense, each head
-pivot's targets are the pattern's (L entry, U entry) products, the levels
-respect every dependency.
+right-looking, one pivot at a time: the sparse head pivots' updates of the
+head rows and of the dense rows' head columns from tabulated targets, their
+updates of the trailing dense block and the dense pivots' by that block's
+addressing (the kernel keeps it in registers), the head L entries of column
+k scaled during pivot k + 1; it solves the head rows by levels, the border
+entries one row at a time and the dense block's triangles in order, all
+from the staged table section.  These tests replay that schedule in numpy on
+the tables the library builds (every index the kernel reads comes from
+them) for a random matrix with the mechanism's LU pattern, and check the
+factors and the solution against dense linear algebra.  They also check the
+tables' invariants: the dense block is dense, the staged section matches the
+LU structure, the levels respect every dependency.
 """
 import struct
 
@@ -19,7 +21,10 @@ import pytest
 
 FIELDS = ("bytes n n_rxn n_part n_jac n_lu n_coef r0 n_hf n_hb rx_word rx_vptr coef fg_ptr "
           "fg_ent jg_ptr jg_mid jg_w0 jg_w1 jg_row lu_src lu_perm lu_rowptr lu_col lu_diag "
-          "dpos ub lk_ptr lk_pos tg_ptr tg hf_ptr hf_rows hb_ptr hb_rows dep_state atol").split()
+          "dpos ub lk_ptr lk_pos lk_row lk_mid tg_ptr tg hf_ptr hf_rows hb_ptr hb_rows "
+          "dep_state atol stage sg_len sg_rowptr sg_diag sg_ub sg_perm sg_hf_ptr sg_hf_rows "
+          "sg_hb_ptr sg_hb_rows sg_ndoff sg_ndcol sg_dbase").split()
+MAX_DENSE = 112
 
 
 def parse(blob: bytes) -> dict:
@@ -40,12 +45,22 @@ def parse(blob: bytes) -> dict:
     t["ub"] = arr("ub", np.uint16, r0)
     t["lk_ptr"] = arr("lk_ptr", np.uint32, r0 + 1)
     t["lk_pos"] = arr("lk_pos", np.uint16, int(t["lk_ptr"][-1]))
+    t["lk_row"] = arr("lk_row", np.uint16, int(t["lk_ptr"][-1]))
+    t["lk_mid"] = arr("lk_mid", np.uint32, r0)
     t["tg_ptr"] = arr("tg_ptr", np.uint32, r0 + 1)
     t["tg"] = arr("tg", np.uint16, int(t["tg_ptr"][-1]))
     t["hf_ptr"] = arr("hf_ptr", np.uint16, o["n_hf"] + 1)
     t["hf_rows"] = arr("hf_rows", np.uint16, int(t["hf_ptr"][-1]))
     t["hb_ptr"] = arr("hb_ptr", np.uint16, o["n_hb"] + 1)
     t["hb_rows"] = arr("hb_rows", np.uint16, int(t["hb_ptr"][-1]))
+    sg = arr("stage", np.uint16, o["sg_len"])
+    assert o["stage"] % 16 == 0 and o["sg_len"] % 8 == 0
+    lens = {"rowptr": n + 1, "diag": n, "ub": r0, "perm": n, "hf_ptr": o["n_hf"] + 1,
+            "hf_rows": len(t["hf_rows"]), "hb_ptr": o["n_hb"] + 1, "hb_rows": len(t["hb_rows"]),
+            "ndoff": n + 1}
+    t["sg"] = {k: sg[o["sg_" + k]:o["sg_" + k] + v] for k, v in lens.items()}
+    t["sg"]["ndcol"] = sg[o["sg_ndcol"]:o["sg_ndcol"] + int(t["sg"]["ndoff"][-1])]
+    t["sg"]["dbase"] = sg[o["sg_dbase"]:o["sg_dbase"] + n - r0]
     return t
 
 
@@ -60,75 +75,92 @@ def pattern(t) -> np.ndarray:
 def factor(t, LU):
     """op_factor's schedule on the values LU (in place); returns dinv."""
     n, r0 = t["n"], t["r0"]
-    diag, rowptr, dpos = t["lu_diag"], t["lu_rowptr"], t["dpos"]
+    m = n - r0
+    sg = t["sg"]
+    diag, rowptr, ub, ndoff, ndcol, dbase = (sg["diag"], sg["rowptr"], sg["ub"], sg["ndoff"],
+                                             sg["ndcol"], sg["dbase"])
+    # the dense block, as the kernel's registers hold it
+    A = np.array([[LU[dbase[i] + r0 + j] for j in range(m)] for i in range(m)])
     dinv = np.zeros(n)
     dprev = 0.0
-    for k in range(n):
+    for k in range(r0):
         dk = 1.0 / LU[diag[k]]
         dinv[k] = dk
         if k > 0:
-            kp = k - 1
-            if kp < r0:
-                LU[t["lk_pos"][t["lk_ptr"][kp]:t["lk_ptr"][kp + 1]]] *= dprev
-            else:
-                LU[dpos[k - r0:] + (kp - r0)] *= dprev
-        if k < r0:
-            lk = t["lk_pos"][t["lk_ptr"][k]:t["lk_ptr"][k + 1]]
-            u0 = diag[k] + 1
-            nu = rowptr[k + 1] - u0
-            tg = t["tg"][t["tg_ptr"][k]:t["tg_ptr"][k] + len(lk) * nu].reshape(len(lk), nu)
-            upd = np.outer(LU[lk] * dk, LU[u0:u0 + nu])
-            # targets of one pivot are distinct: a plain scatter
-            assert len(np.unique(tg)) == tg.size
-            LU[tg.ravel()] -= upd.ravel()
-        else:
-            uk = dpos[k - r0] - r0
-            for i in range(k + 1, n):
-                ri = dpos[i - r0] - r0
-                l = LU[ri + k] * dk
-                LU[ri + k + 1:ri + n] -= l * LU[uk + k + 1:uk + n]
+            LU[t["lk_pos"][t["lk_ptr"][k - 1]:t["lk_ptr"][k]]] *= dprev
+        a0, am, a1 = t["lk_ptr"][k], t["lk_mid"][k], t["lk_ptr"][k + 1]
+        u0, uh, u1 = diag[k] + 1, ub[k], rowptr[k + 1]
+        nu, nuh = u1 - u0, uh - u0
+        tg = t["tg"][t["tg_ptr"][k]:t["tg_ptr"][k + 1]]
+        assert len(tg) == (am - a0) * nu + (a1 - am) * nuh
+        assert all(t["lk_row"][a0:am] < r0) and all(t["lk_row"][am:a1] >= r0)
+        lh = LU[t["lk_pos"][a0:am]] * dk
+        ld = LU[t["lk_pos"][am:a1]] * dk
+        ta = tg[:(am - a0) * nu].reshape(am - a0, nu)
+        tb = tg[(am - a0) * nu:].reshape(a1 - am, nuh)
+        upd_a = np.outer(lh, LU[u0:u1])
+        upd_b = np.outer(ld, LU[u0:uh])
+        # every target of one pivot is distinct, and none is in the dense block
+        both = np.concatenate([ta.ravel(), tb.ravel()])
+        assert len(np.unique(both)) == both.size
+        LU[ta.ravel()] -= upd_a.ravel()
+        LU[tb.ravel()] -= upd_b.ravel()
+        # the exchange column and row into the dense block
+        lcol = np.zeros(m)
+        lcol[t["lk_row"][am:a1] - r0] = ld
+        urow = np.zeros(m)
+        cols = ndcol[ndoff[k] - rowptr[k] + np.arange(uh, u1)]
+        assert all(cols >= r0)
+        urow[cols - r0] = LU[uh:u1]
+        A -= np.outer(lcol, urow)
         dprev = dk
+    for kk in range(m):
+        k = r0 + kk
+        if kk == 0 and r0 > 0:
+            LU[t["lk_pos"][t["lk_ptr"][r0 - 1]:t["lk_ptr"][r0]]] *= dprev
+        dk = 1.0 / A[kk, kk]
+        dinv[k] = dk
+        A[kk + 1:, kk] *= dk
+        A[kk + 1:, kk + 1:] -= np.outer(A[kk + 1:, kk], A[kk, kk + 1:])
+    for i in range(m):
+        LU[dbase[i] + r0:dbase[i] + r0 + m] = A[i]
     return dinv
 
 
 def solve(t, LU, dinv, rhs):
-    """op_solve's schedule: rhs (dependent order) -> M^{-1} rhs."""
+    """op_solve's schedule on the staged tables: rhs (dependent order) ->
+    M^{-1} rhs."""
     n, r0 = t["n"], t["r0"]
-    perm, rowptr, col, diag, dpos, ub = (t["lu_perm"], t["lu_rowptr"], t["lu_col"],
-                                         t["lu_diag"], t["dpos"], t["ub"])
+    m = n - r0
+    sg = t["sg"]
+    perm, rowptr, diag, ub, ndoff, ndcol, dbase = (sg["perm"], sg["rowptr"], sg["diag"],
+                                                   sg["ub"], sg["ndoff"], sg["ndcol"],
+                                                   sg["dbase"])
+
+    def cols(i, q0, q1):  # columns of positions q0..q1 of row i (non-dense entries)
+        return ndcol[ndoff[i] + q0 - rowptr[i]:ndoff[i] + q1 - rowptr[i]]
+
     z = rhs[perm].copy()
     for lv in range(t["n_hf"]):
-        rows = t["hf_rows"][t["hf_ptr"][lv]:t["hf_ptr"][lv + 1]]
-        new = {i: z[i] - LU[rowptr[i]:diag[i]] @ z[col[rowptr[i]:diag[i]]] for i in rows}
+        rows = sg["hf_rows"][sg["hf_ptr"][lv]:sg["hf_ptr"][lv + 1]]
+        new = {i: z[i] - LU[rowptr[i]:diag[i]] @ z[cols(i, rowptr[i], diag[i])] for i in rows}
         for i, v in new.items():
             z[i] = v
     for i in range(r0, n):
-        q0, q1 = rowptr[i], dpos[i - r0]
-        z[i] -= LU[q0:q1] @ z[col[q0:q1]]
-    for c0 in range(r0, n, 32):
-        c1 = min(c0 + 32, n)
-        for i in range(c0, c1):
-            ri = dpos[i - r0] - r0
-            z[i] -= LU[ri + c0:ri + i] @ z[c0:i]
-        for i in range(c1, n):
-            ri = dpos[i - r0] - r0
-            z[i] -= LU[ri + c0:ri + c1] @ z[c0:c1]
-    np_ = (n - r0 + 31) // 32
-    for pp in range(np_ - 1, -1, -1):
-        c0 = r0 + 32 * pp
-        c1 = min(c0 + 32, n)
-        for i in range(c1 - 1, c0 - 1, -1):
-            ri = dpos[i - r0] - r0
-            z[i] = (z[i] - LU[ri + i + 1:ri + c1] @ z[i + 1:c1]) * dinv[i]
-        for i in range(r0, c0):
-            ri = dpos[i - r0] - r0
-            z[i] -= LU[ri + c0:ri + c1] @ z[c0:c1]
+        ne = ndoff[i + 1] - ndoff[i]
+        z[i] -= LU[rowptr[i]:rowptr[i] + ne] @ z[ndcol[ndoff[i]:ndoff[i] + ne]]
+    for kk in range(m):  # dense forward, column by column
+        for d in range(kk + 1, m):
+            z[r0 + d] -= LU[dbase[d] + r0 + kk] * z[r0 + kk]
+    for kk in range(m - 1, -1, -1):  # dense backward
+        z[r0 + kk] *= dinv[r0 + kk]
+        for d in range(kk):
+            z[r0 + d] -= LU[dbase[d] + r0 + kk] * z[r0 + kk]
     for i in range(r0):
-        q0, q1 = ub[i], rowptr[i + 1]
-        z[i] -= LU[q0:q1] @ z[col[q0:q1]]
+        z[i] -= LU[ub[i]:rowptr[i + 1]] @ z[cols(i, ub[i], rowptr[i + 1])]
     for lv in range(t["n_hb"]):
-        rows = t["hb_rows"][t["hb_ptr"][lv]:t["hb_ptr"][lv + 1]]
-        new = {i: (z[i] - LU[diag[i] + 1:ub[i]] @ z[col[diag[i] + 1:ub[i]]]) * dinv[i]
+        rows = sg["hb_rows"][sg["hb_ptr"][lv]:sg["hb_ptr"][lv + 1]]
+        new = {i: (z[i] - LU[diag[i] + 1:ub[i]] @ z[cols(i, diag[i] + 1, ub[i])]) * dinv[i]
                for i in rows}
         for i, v in new.items():
             z[i] = v
@@ -190,6 +222,17 @@ def _invariants(t):
     n, r0 = t["n"], t["r0"]
     P = pattern(t)
     assert P[r0:, r0:].all()
+    assert n - r0 <= MAX_DENSE
+    # the staged section is the LU structure
+    sg = t["sg"]
+    for k in ("rowptr", "diag", "perm"):
+        assert np.array_equal(sg[k], t["lu_" + k])
+    assert np.array_equal(sg["ub"], t["ub"])
+    assert np.array_equal(sg["dbase"], t["dpos"] - r0)
+    for i in range(n):
+        q1 = t["lu_rowptr"][i + 1] if i < r0 else t["dpos"][i - r0]
+        assert np.array_equal(sg["ndcol"][sg["ndoff"][i]:sg["ndoff"][i + 1]],
+                              t["lu_col"][t["lu_rowptr"][i]:q1])
     assert r0 == 0 or not (P[r0 - 1:, r0 - 1].all() and P[r0 - 1, r0 - 1:].all())
     for i in range(r0, n):
         assert t["lu_col"][t["dpos"][i - r0]] == r0
