@@ -104,8 +104,9 @@ def parse():
     ap.add_argument("--synth-dt", type=float, default=3.0,
                     help="host step of the synthetic mechanism (s): the longest at which the "
                          "oracle finishes every sampled cell")
-    ap.add_argument("--synth-lane-cells", type=int, default=2000,
-                    help="cells of the lane-per-cell comparison on the synthetic mechanism")
+    ap.add_argument("--synth-lane-cells", type=int, default=0,
+                    help="cells of the lane-per-cell comparison on the synthetic mechanism "
+                         "(0: skip; it runs ~0.2 cell-steps/s at the 3 s step)")
     ap.add_argument("--serve-columns", type=int, default=256,
                     help="device-resident columns in the serving pool")
     return ap.parse_args()
@@ -459,12 +460,13 @@ def counted_flops(model: dict, stats) -> float:
 # ---------------------------------------------------------------------------
 # First host step of other mechanisms
 # ---------------------------------------------------------------------------
-def run_first_step(mech, args, dev, stream, n, cells=None, dt=None, kernel=None):
+def run_first_step(mech, args, dev, stream, n, cells=None, dt=None, kernel=None, reps=2):
     """n seeded cells of another mechanism over the first host step of the
     sequence (every cell from its seeded state), mixed and FP64,
-    device-resident, longest-first order from a previous identical run;
-    device time of the second run.  kernel: camp_b200_set_kernel's value
-    (None: the mechanism's default)."""
+    device-resident; with reps=2 longest-first order from a previous
+    identical run, device time of the second run (reps=1: one run in seeded
+    order).  kernel: camp_b200_set_kernel's value (None: the mechanism's
+    default)."""
     import torch
 
     from camp_b200.cells import make_cells
@@ -476,8 +478,10 @@ def run_first_step(mech, args, dev, stream, n, cells=None, dt=None, kernel=None)
     env = torch.from_numpy(cells.env).to(dev)
     photo = torch.from_numpy(np.ascontiguousarray(cells.photo_rates)).to(dev)
     out = {"mechanism": mech.name, "cells": n, "host_step_s": dt,
-           "note": "first host step of the sequence, cells ordered longest-first from an "
-                   "identical previous run; device time (CUDA events)"}
+           "note": ("first host step of the sequence, cells ordered longest-first from an "
+                    "identical previous run; device time (CUDA events)") if reps > 1 else
+                   "first host step of the sequence, seeded cell order; device time (CUDA "
+                   "events)"}
     for name, p in (("mixed", MIXED), ("fp64", FP64)):
         s = Solver(mech, n)
         s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4,
@@ -487,9 +491,9 @@ def run_first_step(mech, args, dev, stream, n, cells=None, dt=None, kernel=None)
             s.set_kernel(kernel)
         out["kernel"] = s.kernel()
         s.set_photo_rates_device(photo, n)
-        s.set_cost_ordering(True)
+        s.set_cost_ordering(reps > 1)
         s.set_graph(not args.no_graph)
-        for rep in range(2):
+        for rep in range(reps):
             st = init.clone()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -675,12 +679,12 @@ def run_gpu_arm(args):
             smech, sbase = load_synthetic(td, 200, 600)
         scells = make_cells(smech, args.synth_cells, SEED, conc_lo=1e-8, photo_base=sbase)
         synth = run_first_step(smech, args, dev, stream, args.synth_cells, cells=scells,
-                               dt=args.synth_dt)
+                               dt=args.synth_dt, reps=1)
         if args.synth_lane_cells > 0:
             nl = min(args.synth_lane_cells, args.synth_cells)
             lcells = make_cells(smech, nl, SEED, conc_lo=1e-8, photo_base=sbase)
             synth["lane_kernel"] = run_first_step(smech, args, dev, stream, nl, cells=lcells,
-                                                  dt=args.synth_dt, kernel=1)
+                                                  dt=args.synth_dt, kernel=1, reps=1)
     fm = flop_model(mech, solver)
     if rank != 0:
         solver.free()

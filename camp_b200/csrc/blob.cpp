@@ -841,6 +841,15 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
   o.sg_ndoff = sec(ndoff);
   o.sg_ndcol = sec(ndcol);
   o.sg_dbase = sec(dbase);
+  if (lk_ptr[r0] > 65535 || tg_ptr[r0] > 65535) {
+    *err = "mechanism exceeds the CTA-kernel table encodings";
+    return false;
+  }
+  std::vector<uint16_t> hlk(lk_ptr.begin(), lk_ptr.end()), hmid(r0), htg(tg_ptr.begin(), tg_ptr.end());
+  for (int k = 0; k < r0; ++k) hmid[k] = (uint16_t)lk_mid[k];
+  o.sg_hlk = sec(hlk);
+  o.sg_hmid = sec(hmid);
+  o.sg_htg = sec(htg);
   stage.resize((stage.size() + 7) & ~size_t(7), 0);  // whole 16-byte units
   o.sg_len = (int)stage.size();
   o.stage = w.put(stage);

@@ -176,6 +176,9 @@ struct BlockOff {
   int stage, sg_len;
   int sg_rowptr, sg_diag, sg_ub, sg_perm, sg_hf_ptr, sg_hf_rows, sg_hb_ptr, sg_hb_rows;
   int sg_ndoff, sg_ndcol, sg_dbase;
+  // and the head pivots' pointers: lk_ptr (r0 + 1), lk_mid (r0), tg_ptr
+  // (r0 + 1), as uint16
+  int sg_hlk, sg_hmid, sg_htg;
 };
 
 // the largest trailing dense block the CTA kernel holds in registers

@@ -70,7 +70,7 @@ struct Tab {
   const double *coef, *atol;
   int n, n_rxn, n_jac, n_lu, r0, n_hf, n_hb, sg_len;
   int sg_rowptr, sg_diag, sg_ub, sg_perm, sg_hf_ptr, sg_hf_rows, sg_hb_ptr, sg_hb_rows;
-  int sg_ndoff, sg_ndcol, sg_dbase;
+  int sg_ndoff, sg_ndcol, sg_dbase, sg_hlk, sg_hmid, sg_htg;
 };
 
 __device__ __forceinline__ Tab make_tab(const char* b) {
@@ -115,6 +115,9 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.sg_ndoff = o.sg_ndoff;
   t.sg_ndcol = o.sg_ndcol;
   t.sg_dbase = o.sg_dbase;
+  t.sg_hlk = o.sg_hlk;
+  t.sg_hmid = o.sg_hmid;
+  t.sg_htg = o.sg_htg;
   return t;
 }
 
@@ -133,9 +136,10 @@ __device__ __forceinline__ T lane_sum(T v) {
 template <typename LT>
 struct Ctx {
   Tab t;
-  const double* keff;
-  double* part;  // term rates (f) or rate partials (J)
-  LT* xbuf;      // the factorization's exchange vectors (over part)
+  const double* keff;  // rate constants (global, per block)
+  double* part;        // term rates (f)
+  double* jpart;       // rate partials (J; global, per block)
+  LT* xbuf;            // the factorization's exchange vectors (over part)
   LT* J;         // solver Jacobian slots (global)
   LT* LU;
   LT* dinv;
@@ -144,6 +148,7 @@ struct Ctx {
   // the staged solve tables
   const uint16_t *rowptr, *diag, *ub, *perm, *hf_ptr, *hf_rows, *hb_ptr, *hb_rows;
   const uint16_t *ndoff, *ndcol, *dbase;
+  const uint16_t *hlk, *hmid, *htg;  // head pivots' L-list and target pointers
 };
 
 // f(y) into out (src/time_derivative.c:90-97 with the negative-yield guard
@@ -201,7 +206,7 @@ __device__ __noinline__ void op_f(const Ctx<LT>& c, const double* y, double* out
 template <typename LT>
 __device__ __noinline__ void op_jac(const Ctx<LT>& c, const double* y, double h) {
   const Tab& t = c.t;
-  double* part = c.part;
+  double* part = c.jpart;
   #pragma unroll 1
   for (int r = threadIdx.x; r < t.n_rxn; r += kThreads) {
     const uint32_t w = __ldg(t.rx_word + r);
@@ -289,20 +294,17 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
     LT* nb = c.xbuf + ((k + 1) % 3) * (2 * kMaxDense);
     #pragma unroll 1
     for (int e = tid; e < 2 * kMaxDense; e += kThreads) nb[e] = (LT)0;
+    const int a0 = c.hlk[k], am = c.hmid[k], a1 = c.hlk[k + 1];
     if (k > 0) {
-      const uint32_t e1 = __ldg(t.lk_ptr + k);
       #pragma unroll 1
-      for (uint32_t e = __ldg(t.lk_ptr + k - 1) + tid; e < e1; e += kThreads)
-        LU[__ldg(t.lk_pos + e)] *= dprev;
+      for (int e = c.hlk[k - 1] + tid; e < a0; e += kThreads) LU[__ldg(t.lk_pos + e)] *= dprev;
     }
-    const uint32_t a0 = __ldg(t.lk_ptr + k), am = __ldg(t.lk_mid + k),
-                   a1 = __ldg(t.lk_ptr + k + 1);
     const int u0 = c.diag[k] + 1, uh = c.ub[k], u1 = c.rowptr[k + 1];
     const int nu = u1 - u0, nuh = uh - u0;
-    const uint16_t* tg = t.tg + __ldg(t.tg_ptr + k);
+    const uint16_t* tg = t.tg + c.htg[k];
     // head rows against every U entry of row k
-    #pragma unroll 1
-    for (uint32_t e = a0 + warp; e < am; e += kWarps) {
+    #pragma unroll 2
+    for (int e = a0 + warp; e < am; e += kWarps) {
       const LT l = LU[__ldg(t.lk_pos + e)] * dk;
       const uint16_t* ta = tg + (size_t)(e - a0) * nu;
       #pragma unroll 2
@@ -311,8 +313,8 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
     // dense rows against the U entries in head columns; their multipliers
     // into the exchange column
     const uint16_t* tgb = tg + (size_t)(am - a0) * nu;
-    #pragma unroll 1
-    for (uint32_t e = am + warp; e < a1; e += kWarps) {
+    #pragma unroll 2
+    for (int e = am + warp; e < a1; e += kWarps) {
       const LT l = LU[__ldg(t.lk_pos + e)] * dk;
       const uint16_t* ta = tgb + (size_t)(e - am) * nuh;
       #pragma unroll 2
@@ -363,10 +365,9 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
       }
       if (kk == 0 && r0 > 0) {
         // the last head column's L entries
-        const uint32_t e1 = __ldg(t.lk_ptr + r0);
+        const int e1 = c.hlk[r0];
         #pragma unroll 1
-        for (uint32_t e = __ldg(t.lk_ptr + r0 - 1) + tid; e < e1; e += kThreads)
-          LU[__ldg(t.lk_pos + e)] *= dprev;
+        for (int e = c.hlk[r0 - 1] + tid; e < e1; e += kThreads) LU[__ldg(t.lk_pos + e)] *= dprev;
       }
       bsync();
       const LT piv = lb[kk];
@@ -385,16 +386,17 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
         const int dj = q + 16 * u;
         uv[u] = (dj > kk && dj < m) ? ubf[dj] : (LT)0;
       }
-      if (q == kq) {
-        #pragma unroll
-        for (int s = 0; s < kTile; ++s)
-          if (p + 16 * s > kk) a[s][s0] *= dk;
+      // branch-free: lv / uv are zero outside the trailing rows / columns,
+      // so the update leaves row kk, column kk and the rest unchanged there
+      #pragma unroll
+      for (int s = 0; s < kTile; ++s) {
+        const bool sc = q == kq && p + 16 * s > kk;
+        a[s][s0] = sc ? a[s][s0] * dk : a[s][s0];
       }
       #pragma unroll
       for (int s = 0; s < kTile; ++s)
       #pragma unroll
-        for (int u = 0; u < kTile; ++u)
-          if (p + 16 * s > kk && q + 16 * u > kk) a[s][u] -= lv[s] * uv[u];
+        for (int u = 0; u < kTile; ++u) a[s][u] -= lv[s] * uv[u];
     }
   }
   #pragma unroll
@@ -458,7 +460,11 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
       zr[s] = d < m ? z[r0 + d] : (LT)0;
       base[s] = d < m ? c.dbase[d] + r0 : 0;
     }
-    // forward: unit lower triangle
+    // forward: unit lower triangle; each column's entries are loaded one
+    // step ahead, off the shuffle -> FMA chain
+    LT col[kSlots];
+    #pragma unroll
+    for (int s = 0; s < kSlots; ++s) col[s] = LU[base[s]];
     #pragma unroll
     for (int sl = 0; sl < kSlots; ++sl) {
       if (32 * sl < m) {
@@ -466,16 +472,25 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
         #pragma unroll 1
         for (int ln = 0; ln < w; ++ln) {
           const int kk = 32 * sl + ln;
+          const int kn = min(kk + 1, m - 1);
+          LT nxt[kSlots];
+          #pragma unroll
+          for (int s = sl; s < kSlots; ++s) nxt[s] = LU[base[s] + kn];
           const LT zk = __shfl_sync(0xffffffffu, zr[sl], ln);
           #pragma unroll
           for (int s = sl; s < kSlots; ++s) {
-            const int d = 32 * s + lane;
-            if (d > kk && d < m) zr[s] -= LU[base[s] + kk] * zk;
+            const LT v = zr[s] - col[s] * zk;
+            zr[s] = 32 * s + lane > kk ? v : zr[s];
+            col[s] = nxt[s];
           }
         }
       }
     }
-    // backward: upper triangle, each row finished by its pivot's reciprocal
+    // backward: upper triangle, each row finished by its pivot's
+    // reciprocal; the next column's entries and reciprocal loaded ahead
+    #pragma unroll
+    for (int s = 0; s < kSlots; ++s) col[s] = LU[base[s] + m - 1];
+    LT dcur = c.dinv[r0 + m - 1];
     #pragma unroll
     for (int sl = kSlots - 1; sl >= 0; --sl) {
       if (32 * sl < m) {
@@ -483,13 +498,20 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
         #pragma unroll 1
         for (int ln = w - 1; ln >= 0; --ln) {
           const int kk = 32 * sl + ln;
-          if (lane == ln) zr[sl] *= c.dinv[r0 + kk];
+          const int kn = max(kk - 1, 0);
+          LT nxt[kSlots];
+          #pragma unroll
+          for (int s = 0; s <= sl; ++s) nxt[s] = LU[base[s] + kn];
+          const LT dnxt = c.dinv[r0 + kn];
+          zr[sl] = lane == ln ? zr[sl] * dcur : zr[sl];
           const LT zk = __shfl_sync(0xffffffffu, zr[sl], ln);
           #pragma unroll
           for (int s = 0; s <= sl; ++s) {
-            const int d = 32 * s + lane;
-            if (d < kk) zr[s] -= LU[base[s] + kk] * zk;
+            const LT v = zr[s] - col[s] * zk;
+            zr[s] = 32 * s + lane < kk ? v : zr[s];
+            col[s] = nxt[s];
           }
+          dcur = dnxt;
         }
       }
     }

@@ -1895,7 +1895,7 @@ __global__ void __launch_bounds__(32 * (AERO ? kMaxCellsAero : kMaxCellsPerBlock
 // control, every warp runs its f, J, factorization and solves
 // ---------------------------------------------------------------------------
 struct BlkLayout {  // byte offsets in the block's shared memory (zn -1: global)
-  int ctx, ctl, y, ewt, acor, ftemp, tempv, part, keff, dinv, z, zn, sg, lu, bytes;
+  int ctx, ctl, y, ewt, acor, ftemp, tempv, part, dinv, z, zn, sg, lu, bytes;
 };
 
 struct BlkArgs {
@@ -1913,6 +1913,8 @@ struct BlkArgs {
   void* jscratch;    // per-block solver Jacobian slots
   double* hist;      // per-block Nordsieck history when not in shared memory
   int hist_stride;   // doubles per block in hist
+  double* gscr;      // per-block rate constants and rate partials
+  int gscr_stride;   // doubles per block in gscr
   double t0, t1, rtol;
   int max_steps, maxncf, maxnef;
 };
@@ -1931,7 +1933,8 @@ __global__ void __launch_bounds__(blk::kThreads, sizeof(LT) == 4 ? 2 : 1)
   if (threadIdx.x == 0) {
     blk::Ctx<LT> c;
     c.t = blk::make_tab(a.blob);
-    c.keff = (const double*)(smem + L.keff);
+    c.keff = a.gscr + (size_t)blockIdx.x * a.gscr_stride;
+    c.jpart = a.gscr + (size_t)blockIdx.x * a.gscr_stride + c.t.n_rxn;
     c.part = (double*)(smem + L.part);
     c.xbuf = (LT*)(smem + L.part);
     c.J = (LT*)a.jscratch + (size_t)blockIdx.x * c.t.n_jac;
@@ -1951,6 +1954,9 @@ __global__ void __launch_bounds__(blk::kThreads, sizeof(LT) == 4 ? 2 : 1)
     c.ndoff = sg + c.t.sg_ndoff;
     c.ndcol = sg + c.t.sg_ndcol;
     c.dbase = sg + c.t.sg_dbase;
+    c.hlk = sg + c.t.sg_hlk;
+    c.hmid = sg + c.t.sg_hmid;
+    c.htg = sg + c.t.sg_htg;
     *cx = c;
   }
   {
@@ -1991,7 +1997,7 @@ __global__ void __launch_bounds__(blk::kThreads, sizeof(LT) == 4 ? 2 : 1)
     c.ftemp = (double*)(smem + L.ftemp);
     c.tempv = (double*)(smem + L.tempv);
     c.rates = (double*)(smem + L.part);
-    c.keff = (double*)(smem + L.keff);
+    c.keff = const_cast<double*>(cx->keff);
     c.fscr = nullptr;
     c.LU = cx->LU;
     c.z = cx->z;
@@ -2711,9 +2717,9 @@ static BlkLayout make_blk_layout(const BlockOff& o, int lt, bool zn_in_smem) {
   L.acor = take(8 * n);
   L.ftemp = take(8 * n);
   L.tempv = take(8 * n);
-  // term rates / partials, and during a factorization its exchange vectors
-  L.part = take(std::max(8 * (size_t)std::max(o.n_rxn, o.n_part), (size_t)lt * blk::kXBuf));
-  L.keff = take(8 * (size_t)o.n_rxn);
+  // term rates, and during a factorization its exchange vectors (the rate
+  // constants and partials live in global scratch)
+  L.part = take(std::max(8 * (size_t)o.n_rxn, (size_t)lt * blk::kXBuf));
   L.dinv = take((size_t)lt * n);
   L.z = take((size_t)lt * n);
   L.zn = zn_in_smem ? take(8 * LMAX * n) : -1;
@@ -2787,8 +2793,9 @@ bool Engine::launch_block(double* d_state, const double* d_env, const double* d_
   if (!ensure(&I->d_jscratch, &I->c_jscratch, (size_t)b.lt * I->boff.n_jac * b.grid, err))
     return false;
   const int hist_stride = b.lay.zn >= 0 ? 0 : (LMAX * I->boff.n + 31) & ~31;
-  if (hist_stride &&
-      !ensure(&I->d_hist, &I->c_hist, sizeof(double) * (size_t)hist_stride * b.grid, err))
+  const int gscr_stride = (I->boff.n_rxn + I->boff.n_part + 31) & ~31;
+  if (!ensure(&I->d_hist, &I->c_hist,
+              sizeof(double) * (size_t)(hist_stride + gscr_stride) * b.grid, err))
     return false;
   BlkArgs a{};
   a.m = I->m;
@@ -2805,6 +2812,8 @@ bool Engine::launch_block(double* d_state, const double* d_env, const double* d_
   a.jscratch = I->d_jscratch;
   a.hist = (double*)I->d_hist;
   a.hist_stride = hist_stride;
+  a.gscr = (double*)I->d_hist + (size_t)hist_stride * b.grid;
+  a.gscr_stride = gscr_stride;
   a.t0 = t0;
   a.t1 = t1;
   a.rtol = s.rtol;

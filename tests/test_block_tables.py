@@ -23,7 +23,7 @@ FIELDS = ("bytes n n_rxn n_part n_jac n_lu n_coef r0 n_hf n_hb rx_word rx_vptr c
           "fg_ent jg_ptr jg_mid jg_w0 jg_w1 jg_row lu_src lu_perm lu_rowptr lu_col lu_diag "
           "dpos ub lk_ptr lk_pos lk_row lk_mid tg_ptr tg hf_ptr hf_rows hb_ptr hb_rows "
           "dep_state atol stage sg_len sg_rowptr sg_diag sg_ub sg_perm sg_hf_ptr sg_hf_rows "
-          "sg_hb_ptr sg_hb_rows sg_ndoff sg_ndcol sg_dbase").split()
+          "sg_hb_ptr sg_hb_rows sg_ndoff sg_ndcol sg_dbase sg_hlk sg_hmid sg_htg").split()
 MAX_DENSE = 112
 
 
@@ -61,6 +61,9 @@ def parse(blob: bytes) -> dict:
     t["sg"] = {k: sg[o["sg_" + k]:o["sg_" + k] + v] for k, v in lens.items()}
     t["sg"]["ndcol"] = sg[o["sg_ndcol"]:o["sg_ndcol"] + int(t["sg"]["ndoff"][-1])]
     t["sg"]["dbase"] = sg[o["sg_dbase"]:o["sg_dbase"] + n - r0]
+    t["sg"]["hlk"] = sg[o["sg_hlk"]:o["sg_hlk"] + r0 + 1]
+    t["sg"]["hmid"] = sg[o["sg_hmid"]:o["sg_hmid"] + r0]
+    t["sg"]["htg"] = sg[o["sg_htg"]:o["sg_htg"] + r0 + 1]
     return t
 
 
@@ -88,10 +91,10 @@ def factor(t, LU):
         dinv[k] = dk
         if k > 0:
             LU[t["lk_pos"][t["lk_ptr"][k - 1]:t["lk_ptr"][k]]] *= dprev
-        a0, am, a1 = t["lk_ptr"][k], t["lk_mid"][k], t["lk_ptr"][k + 1]
+        a0, am, a1 = sg["hlk"][k], sg["hmid"][k], sg["hlk"][k + 1]
         u0, uh, u1 = diag[k] + 1, ub[k], rowptr[k + 1]
         nu, nuh = u1 - u0, uh - u0
-        tg = t["tg"][t["tg_ptr"][k]:t["tg_ptr"][k + 1]]
+        tg = t["tg"][sg["htg"][k]:sg["htg"][k + 1]]
         assert len(tg) == (am - a0) * nu + (a1 - am) * nuh
         assert all(t["lk_row"][a0:am] < r0) and all(t["lk_row"][am:a1] >= r0)
         lh = LU[t["lk_pos"][a0:am]] * dk
@@ -229,6 +232,8 @@ def _invariants(t):
         assert np.array_equal(sg[k], t["lu_" + k])
     assert np.array_equal(sg["ub"], t["ub"])
     assert np.array_equal(sg["dbase"], t["dpos"] - r0)
+    assert np.array_equal(sg["hlk"], t["lk_ptr"]) and np.array_equal(sg["hmid"], t["lk_mid"])
+    assert np.array_equal(sg["htg"], t["tg_ptr"])
     for i in range(n):
         q1 = t["lu_rowptr"][i + 1] if i < r0 else t["dpos"][i - r0]
         assert np.array_equal(sg["ndcol"][sg["ndoff"][i]:sg["ndoff"][i + 1]],
