@@ -40,8 +40,9 @@
 // The solves read their tables from shared memory (a section of the blob
 // each block copies once): the sparse head by row levels, the dense rows'
 // head columns and the head rows' dense columns one row per warp, and the
-// dense block's triangles on one warp with the block's values in registers
-// (the column value broadcast by a shuffle), without barriers.
+// dense block's triangles by panels of 16 columns (half a warp solves the
+// panel's triangle with shuffles, every thread then updates one row beyond
+// it).
 #pragma once
 
 namespace blk {
@@ -49,9 +50,8 @@ namespace blk {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kTile = 7;    // factorization: dense entries per thread and dimension
-constexpr int kSlots = 4;   // solves: dense rows per lane
-constexpr int kMaxDense = campb::kBlockMaxDense;  // = 16 * kTile <= 32 * kSlots
-static_assert(kMaxDense == 16 * kTile && kMaxDense <= 32 * kSlots, "dense block tiling");
+constexpr int kMaxDense = campb::kBlockMaxDense;  // = 16 * kTile
+static_assert(kMaxDense == 16 * kTile, "dense block tiling");
 constexpr int kXBuf = 3 * 2 * kMaxDense;  // exchange vectors (LT elements)
 
 enum Op : int { OP_EXIT = 0, OP_F = 1, OP_JAC = 2, OP_FACTOR = 3, OP_SOLVE = 4 };
@@ -450,78 +450,74 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
     }
     bsync();
   }
-  // the dense block on warp 0: lane holds dense rows lane + 32 s
-  if (warp == 0) {
-    LT zr[kSlots];
-    int base[kSlots];
-    #pragma unroll
-    for (int s = 0; s < kSlots; ++s) {
-      const int d = 32 * s + lane;
-      zr[s] = d < m ? z[r0 + d] : (LT)0;
-      base[s] = d < m ? c.dbase[d] + r0 : 0;
-    }
-    // forward: unit lower triangle; each column's entries are loaded one
-    // step ahead, off the shuffle -> FMA chain
-    LT col[kSlots];
-    #pragma unroll
-    for (int s = 0; s < kSlots; ++s) col[s] = LU[base[s]];
-    #pragma unroll
-    for (int sl = 0; sl < kSlots; ++sl) {
-      if (32 * sl < m) {
-        const int w = min(32, m - 32 * sl);
-        #pragma unroll 1
-        for (int ln = 0; ln < w; ++ln) {
-          const int kk = 32 * sl + ln;
-          const int kn = min(kk + 1, m - 1);
-          LT nxt[kSlots];
-          #pragma unroll
-          for (int s = sl; s < kSlots; ++s) nxt[s] = LU[base[s] + kn];
-          const LT zk = __shfl_sync(0xffffffffu, zr[sl], ln);
-          #pragma unroll
-          for (int s = sl; s < kSlots; ++s) {
-            const LT v = zr[s] - col[s] * zk;
-            zr[s] = 32 * s + lane > kk ? v : zr[s];
-            col[s] = nxt[s];
-          }
-        }
+  // the dense block by panels of 16 columns: half of warp 0 solves the
+  // panel's triangle (a lane per row, the column value broadcast by a
+  // shuffle), then every thread updates one row beyond the panel
+  const int np = (m + 15) / 16;
+  #pragma unroll 1
+  for (int pp = 0; pp < np; ++pp) {
+    const int c0 = 16 * pp, c1 = min(c0 + 16, m), w = c1 - c0;
+    if (warp == 0) {
+      const int d = c0 + (lane & 15);
+      const bool own = lane < w;
+      LT zi = own ? z[r0 + d] : (LT)0;
+      const LT* ri = LU + (own ? c.dbase[d] + r0 : 0);
+      #pragma unroll 1
+      for (int kk = 0; kk < w - 1; ++kk) {
+        const LT lk = ri[c0 + kk];
+        const LT zk = __shfl_sync(0xffffffffu, zi, kk);
+        const LT v = zi - lk * zk;
+        zi = lane > kk ? v : zi;
       }
+      if (own) z[r0 + d] = zi;
     }
-    // backward: upper triangle, each row finished by its pivot's
-    // reciprocal; the next column's entries and reciprocal loaded ahead
-    #pragma unroll
-    for (int s = 0; s < kSlots; ++s) col[s] = LU[base[s] + m - 1];
-    LT dcur = c.dinv[r0 + m - 1];
-    #pragma unroll
-    for (int sl = kSlots - 1; sl >= 0; --sl) {
-      if (32 * sl < m) {
-        const int w = min(32, m - 32 * sl);
-        #pragma unroll 1
-        for (int ln = w - 1; ln >= 0; --ln) {
-          const int kk = 32 * sl + ln;
-          const int kn = max(kk - 1, 0);
-          LT nxt[kSlots];
-          #pragma unroll
-          for (int s = 0; s <= sl; ++s) nxt[s] = LU[base[s] + kn];
-          const LT dnxt = c.dinv[r0 + kn];
-          zr[sl] = lane == ln ? zr[sl] * dcur : zr[sl];
-          const LT zk = __shfl_sync(0xffffffffu, zr[sl], ln);
-          #pragma unroll
-          for (int s = 0; s <= sl; ++s) {
-            const LT v = zr[s] - col[s] * zk;
-            zr[s] = 32 * s + lane < kk ? v : zr[s];
-            col[s] = nxt[s];
-          }
-          dcur = dnxt;
-        }
+    bsync();
+    if (c1 < m) {
+      #pragma unroll 1
+      for (int d = c1 + tid; d < m; d += kThreads) {
+        const LT* ri = LU + c.dbase[d] + r0;
+        LT acc = (LT)0;
+        #pragma unroll 4
+        for (int cc = c0; cc < c1; ++cc) acc += ri[cc] * z[r0 + cc];
+        z[r0 + d] -= acc;
       }
-    }
-    #pragma unroll
-    for (int s = 0; s < kSlots; ++s) {
-      const int d = 32 * s + lane;
-      if (d < m) z[r0 + d] = zr[s];
+      bsync();
     }
   }
-  bsync();
+  // backward, last panel first: the panel's triangle finished by each
+  // row's pivot reciprocal, then the rows above the panel
+  #pragma unroll 1
+  for (int pp = np - 1; pp >= 0; --pp) {
+    const int c0 = 16 * pp, c1 = min(c0 + 16, m), w = c1 - c0;
+    if (warp == 0) {
+      const int d = c0 + (lane & 15);
+      const bool own = lane < w;
+      LT zi = own ? z[r0 + d] : (LT)0;
+      const LT di = own ? c.dinv[r0 + d] : (LT)0;
+      const LT* ri = LU + (own ? c.dbase[d] + r0 : 0);
+      #pragma unroll 1
+      for (int kk = w - 1; kk >= 0; --kk) {
+        const LT uk = ri[c0 + kk];
+        zi = lane == kk ? zi * di : zi;
+        const LT zk = __shfl_sync(0xffffffffu, zi, kk);
+        const LT v = zi - uk * zk;
+        zi = lane < kk ? v : zi;
+      }
+      if (own) z[r0 + d] = zi;
+    }
+    bsync();
+    if (c0 > 0) {
+      #pragma unroll 1
+      for (int d = tid; d < c0; d += kThreads) {
+        const LT* ri = LU + c.dbase[d] + r0;
+        LT acc = (LT)0;
+        #pragma unroll 4
+        for (int cc = c0; cc < c1; ++cc) acc += ri[cc] * z[r0 + cc];
+        z[r0 + d] -= acc;
+      }
+      bsync();
+    }
+  }
   if (r0 > 0) {
     // backward: the dense columns of the head rows, one row per warp
     #pragma unroll 1

@@ -617,8 +617,10 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
   }
   // candidates: the warp-per-cell kernel with its resident cells per block,
   // where the Nordsieck history lives and the LU strategy, and the
-  // lane-per-cell kernel (32 cells per warp) and the block-per-cell kernel
-  // where the mechanism has their tables; the precision stays as set
+  // block-per-cell kernel where the mechanism has their tables; the
+  // lane-per-cell kernel (32 cells per warp, 14-30x slower than the warp
+  // kernel on cb05 and ~2000x slower than the block kernel on a 200-species
+  // mechanism) only where neither has; the precision stays as set
   campb::SolveSettings base = s->settings, best = s->settings;
   double best_ms = -1.0;
   const bool cost_order = s->cost_order;
@@ -640,7 +642,7 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
         cands.push_back(c);
       }
     }
-  if (s->engine->lane_tables()) {
+  if (s->engine->lane_tables() && cands.empty() && !s->engine->block_tables()) {
     campb::SolveSettings c = base;
     c.kernel = 1;
     cands.push_back(c);

@@ -202,9 +202,9 @@ int camp_b200_set_layout(void *solver_data, int hist_global);
 /* Autotuner: solves the given sample of cells (host buffers, state is not
  * modified) once per candidate launch configuration -- for the warp-per-cell
  * kernel the cells per block, the history layout of camp_b200_set_layout and
- * the LU mode of camp_b200_set_lu_mode, and the lane-per-cell kernel (32
- * cells per warp) and the block-per-cell kernel where the mechanism has
- * their tables -- for the current
+ * the LU mode of camp_b200_set_lu_mode, and the block-per-cell kernel where
+ * the mechanism has its tables (the lane-per-cell kernel only where neither
+ * has) -- for the current
  * precision, and keeps the fastest by kernel time.  Use a sample
  * representative of the cells to be solved (a few thousand cells, the host
  * step of the run).  0 or -1. */

@@ -152,13 +152,22 @@ def solve(t, LU, dinv, rhs):
     for i in range(r0, n):
         ne = ndoff[i + 1] - ndoff[i]
         z[i] -= LU[rowptr[i]:rowptr[i] + ne] @ z[ndcol[ndoff[i]:ndoff[i] + ne]]
-    for kk in range(m):  # dense forward, column by column
-        for d in range(kk + 1, m):
-            z[r0 + d] -= LU[dbase[d] + r0 + kk] * z[r0 + kk]
-    for kk in range(m - 1, -1, -1):  # dense backward
-        z[r0 + kk] *= dinv[r0 + kk]
-        for d in range(kk):
-            z[r0 + d] -= LU[dbase[d] + r0 + kk] * z[r0 + kk]
+    npan = (m + 15) // 16  # dense block by panels of 16 columns
+    for pp in range(npan):
+        c0, c1 = 16 * pp, min(16 * pp + 16, m)
+        for kk in range(c0, c1):  # the panel's triangle
+            for d in range(kk + 1, c1):
+                z[r0 + d] -= LU[dbase[d] + r0 + kk] * z[r0 + kk]
+        for d in range(c1, m):  # the rows beyond it
+            z[r0 + d] -= LU[dbase[d] + r0 + c0:dbase[d] + r0 + c1] @ z[r0 + c0:r0 + c1]
+    for pp in range(npan - 1, -1, -1):
+        c0, c1 = 16 * pp, min(16 * pp + 16, m)
+        for kk in range(c1 - 1, c0 - 1, -1):
+            z[r0 + kk] *= dinv[r0 + kk]
+            for d in range(c0, kk):
+                z[r0 + d] -= LU[dbase[d] + r0 + kk] * z[r0 + kk]
+        for d in range(c0):
+            z[r0 + d] -= LU[dbase[d] + r0 + c0:dbase[d] + r0 + c1] @ z[r0 + c0:r0 + c1]
     for i in range(r0):
         z[i] -= LU[ub[i]:rowptr[i + 1]] @ z[cols(i, ub[i], rowptr[i + 1])]
     for lv in range(t["n_hb"]):
