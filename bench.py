@@ -99,8 +99,9 @@ def parse():
     ap.add_argument("--serve-rates", default="5,10,20,30,40",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=8.0)
-    ap.add_argument("--synth-cells", type=int, default=0,
-                    help="cells of the 200-species / 600-reaction synthetic mechanism (0: skip)")
+    ap.add_argument("--synth-cells", type=int, default=20000,
+                    help="cells of the 200-species / 600-reaction synthetic mechanism (0: skip; "
+                         "about a minute at 2e4 cells, five at 1e5)")
     ap.add_argument("--synth-dt", type=float, default=3.0,
                     help="host step of the synthetic mechanism (s): the longest at which the "
                          "oracle finishes every sampled cell")
