@@ -107,7 +107,7 @@ def parse():
                          "oracle finishes every sampled cell")
     ap.add_argument("--synth-lane-cells", type=int, default=0,
                     help="cells of the lane-per-cell comparison on the synthetic mechanism "
-                         "(0: skip; it runs ~0.2 cell-steps/s at the 3 s step)")
+                         "(0: skip; 11x slower than the block-per-cell kernel)")
     ap.add_argument("--serve-columns", type=int, default=256,
                     help="device-resident columns in the serving pool")
     return ap.parse_args()

@@ -619,7 +619,7 @@ int camp_b200_autotune(void* solver_data, const double* state, const double* env
   // where the Nordsieck history lives and the LU strategy, and the
   // block-per-cell kernel where the mechanism has their tables; the
   // lane-per-cell kernel (32 cells per warp, 14-30x slower than the warp
-  // kernel on cb05 and ~2000x slower than the block kernel on a 200-species
+  // kernel on cb05 and 11x slower than the block kernel on a 200-species
   // mechanism) only where neither has; the precision stays as set
   campb::SolveSettings base = s->settings, best = s->settings;
   double best_ms = -1.0;
