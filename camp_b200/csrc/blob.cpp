@@ -703,10 +703,11 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
   // update targets: head rows against every U entry of row k, dense rows
   // against the U entries in head columns
   std::vector<uint32_t> lk_ptr(r0 + 1, 0), lk_mid(std::max(r0, 1), 0), tg_ptr(r0 + 1, 0);
-  std::vector<uint16_t> lk_pos, lk_row, tg;
+  std::vector<uint16_t> lk_pos, lk_row;
+  std::vector<uint64_t> hrec;
   for (int k = 0; k < r0; ++k) {
     lk_ptr[k] = (uint32_t)lk_pos.size();
-    tg_ptr[k] = (uint32_t)tg.size();
+    tg_ptr[k] = (uint32_t)hrec.size();
     std::vector<int> rows;
     for (int i = k + 1; i < n; ++i) {
       const int q = pos[(size_t)i * n + k];
@@ -722,18 +723,21 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
       for (int i : rows) {
         if ((i >= r0) != (pass == 1)) continue;
         const int p1 = pass == 0 ? t.lu_rowptr[k + 1] : ub[k];
+        const int lpos = pos[(size_t)i * n + k];
         for (int p = t.lu_diag[k] + 1; p < p1; ++p) {
           const int d = pos[(size_t)i * n + t.lu_col[p]];
           if (d < 0) {
             *err = "internal: LU fill pattern not closed";
             return false;
           }
-          tg.push_back((uint16_t)d);
+          hrec.push_back((uint64_t)d | ((uint64_t)lpos << 16) | ((uint64_t)p << 32));
         }
       }
   }
   lk_ptr[r0] = (uint32_t)lk_pos.size();
-  tg_ptr[r0] = (uint32_t)tg.size();
+  tg_ptr[r0] = (uint32_t)hrec.size();
+  std::vector<uint32_t> lk(lk_pos.size());
+  for (size_t e = 0; e < lk.size(); ++e) lk[e] = (uint32_t)lk_pos[e] | ((uint32_t)lk_row[e] << 16);
   // head row levels: forward over the L entries, backward over the U entries
   // with columns < r0 (the dense block's values reach head rows in one pass)
   std::vector<int> flev(r0, 0), blev(r0, 0);
@@ -819,11 +823,10 @@ bool build_block_blob(const Tables& t, const std::vector<double>& atol_dep,
   o.dpos = w.put(dpos);
   o.ub = w.put(ub);
   o.lk_ptr = w.put(lk_ptr);
-  o.lk_pos = w.put(lk_pos);
-  o.lk_row = w.put(lk_row);
+  o.lk = w.put(lk);
   o.lk_mid = w.put(lk_mid);
   o.tg_ptr = w.put(tg_ptr);
-  o.tg = w.put(tg);
+  o.hrec = w.put(hrec);
   o.hf_ptr = w.put(hf_ptr);
   o.hf_rows = w.put(hf_rows);
   o.hb_ptr = w.put(hb_ptr);

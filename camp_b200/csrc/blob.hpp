@@ -155,13 +155,14 @@ struct BlockOff {
   int dpos;  // per dense row: position of its column r0 (uint16)
   int ub;    // per head row: first position with a column >= r0 (uint16)
   // head pivots k < r0: L entries of column k in row order (pointers
-  // uint32, r0 + 1; positions and rows uint16), the first of them in a
-  // dense row (uint32 per pivot), and the tabulated update targets (pointers
-  // uint32, r0 + 1; positions uint16): the head rows' L entries against
-  // every U entry of row k, then the dense rows' against the U entries of
-  // row k in head columns, row-major.  The dense rows' updates in dense
-  // columns are addressed through the dense block.
-  int lk_ptr, lk_pos, lk_row, lk_mid, tg_ptr, tg;
+  // uint32, r0 + 1; entries uint32: position | row << 16), the first of
+  // them in a dense row (uint32 per pivot), and the tabulated updates
+  // (pointers uint32, r0 + 1; records uint64: target | L position << 16 |
+  // U position << 32): the head rows' L entries against every U entry of
+  // row k, then the dense rows' against the U entries of row k in head
+  // columns, row-major.  The dense rows' updates in dense columns are
+  // addressed through the dense block.
+  int lk_ptr, lk, lk_mid, tg_ptr, hrec;
   // head row levels (pointers uint16, levels + 1; rows uint16)
   int hf_ptr, hf_rows, hb_ptr, hb_rows;
   int dep_state;  // uint16

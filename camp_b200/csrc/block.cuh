@@ -30,9 +30,10 @@
 // column of multipliers and its row of U), so the dense block's Schur
 // updates cost no shared-memory traffic.  The sparse head pivots update the
 // head rows and the dense rows' head columns in shared memory from
-// tabulated targets and the dense block through the same exchange (their
-// columns and rows scattered into zeroed vectors); their L entries are
-// scaled by the pivot's reciprocal during pivot k + 1.  The exchange
+// tabulated update records and the dense block through the same exchange
+// (their columns and rows scattered into zeroed vectors); each thread's
+// records of the next pivot are loaded while the current one runs, and each
+// column's L entries are scaled right after its pivot's barrier.  The exchange
 // vectors rotate over three buffers, so a pivot's scatter never meets a
 // slower warp's reads of the previous pivot's vectors and each buffer is
 // zeroed two pivots after its use.
@@ -65,8 +66,9 @@ struct Cmd {
 
 struct Tab {
   const uint32_t *rx_word, *rx_vptr, *fg_ptr, *fg_ent, *jg_ptr, *jg_mid, *jg_w0;
-  const uint32_t *lk_ptr, *lk_mid, *tg_ptr;
-  const uint16_t *jg_w1, *jg_row, *lu_src, *lk_pos, *lk_row, *tg, *dep_state, *stage;
+  const uint32_t *lk_ptr, *lk_mid, *tg_ptr, *lk;
+  const uint64_t* hrec;
+  const uint16_t *jg_w1, *jg_row, *lu_src, *dep_state, *stage;
   const double *coef, *atol;
   int n, n_rxn, n_jac, n_lu, r0, n_hf, n_hb, sg_len;
   int sg_rowptr, sg_diag, sg_ub, sg_perm, sg_hf_ptr, sg_hf_rows, sg_hb_ptr, sg_hb_rows;
@@ -89,9 +91,8 @@ __device__ __forceinline__ Tab make_tab(const char* b) {
   t.jg_w1 = (const uint16_t*)(b + o.jg_w1);
   t.jg_row = (const uint16_t*)(b + o.jg_row);
   t.lu_src = (const uint16_t*)(b + o.lu_src);
-  t.lk_pos = (const uint16_t*)(b + o.lk_pos);
-  t.lk_row = (const uint16_t*)(b + o.lk_row);
-  t.tg = (const uint16_t*)(b + o.tg);
+  t.lk = (const uint32_t*)(b + o.lk);
+  t.hrec = (const uint64_t*)(b + o.hrec);
   t.dep_state = (const uint16_t*)(b + o.dep_state);
   t.stage = (const uint16_t*)(b + o.stage);
   t.coef = (const double*)(b + o.coef);
@@ -256,7 +257,7 @@ template <typename LT>
 __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
   const Tab& t = c.t;
   LT* LU = c.LU;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const int n = t.n, r0 = t.r0, m = n - r0;
   #pragma unroll 1
   for (int p = tid; p < t.n_lu; p += kThreads) {
@@ -279,8 +280,24 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
       a[s][u] = (di < m && dj < m) ? LU[c.dbase[di] + r0 + dj] : (LT)0;
     }
   bool bad = false;
-  LT dprev = (LT)0;
-  // sparse head pivots
+  // sparse head pivots.  A pivot's work is a list of update records
+  // (target, L entry, U entry) and its column's L entries; thread tid takes
+  // records tid + 256 j and L entry tid.  The first kPre records and the L
+  // entry of pivot k + 1 are loaded while pivot k runs, so the L2 latency
+  // of the tables overlaps the previous pivot's work and barrier.
+  constexpr int kPre = 4;
+  constexpr uint64_t kNone = ~0ull;
+  uint64_t rq[kPre];
+  uint32_t lq = 0xFFFFFFFFu;
+  auto fetch = [&](int k) {
+    const int q0 = c.htg[k], nq = c.htg[k + 1] - q0;
+    #pragma unroll
+    for (int j = 0; j < kPre; ++j)
+      rq[j] = tid + kThreads * j < nq ? __ldg(t.hrec + q0 + tid + kThreads * j) : kNone;
+    const int e0 = c.hlk[k], ne = c.hlk[k + 1] - e0;
+    lq = tid < ne ? __ldg(t.lk + e0 + tid) : 0xFFFFFFFFu;
+  };
+  if (r0 > 0) fetch(0);
   #pragma unroll 1
   for (int k = 0; k < r0; ++k) {
     LT* lb = c.xbuf + (k % 3) * (2 * kMaxDense);
@@ -294,38 +311,48 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
     LT* nb = c.xbuf + ((k + 1) % 3) * (2 * kMaxDense);
     #pragma unroll 1
     for (int e = tid; e < 2 * kMaxDense; e += kThreads) nb[e] = (LT)0;
-    const int a0 = c.hlk[k], am = c.hmid[k], a1 = c.hlk[k + 1];
-    if (k > 0) {
-      #pragma unroll 1
-      for (int e = c.hlk[k - 1] + tid; e < a0; e += kThreads) LU[__ldg(t.lk_pos + e)] *= dprev;
+    uint64_t cr[kPre];
+    #pragma unroll
+    for (int j = 0; j < kPre; ++j) cr[j] = rq[j];
+    const uint32_t cl = lq;
+    if (k + 1 < r0) fetch(k + 1);
+    // the tabulated updates (targets of one pivot are distinct)
+    #pragma unroll
+    for (int j = 0; j < kPre; ++j) {
+      const uint64_t r = cr[j];
+      if (r != kNone) {
+        const int tg = (int)(r & 0xFFFFu), lp = (int)((r >> 16) & 0xFFFFu);
+        const int up = (int)((r >> 32) & 0xFFFFu);
+        LU[tg] -= (LU[lp] * dk) * LU[up];
+      }
     }
-    const int u0 = c.diag[k] + 1, uh = c.ub[k], u1 = c.rowptr[k + 1];
-    const int nu = u1 - u0, nuh = uh - u0;
-    const uint16_t* tg = t.tg + c.htg[k];
-    // head rows against every U entry of row k
-    #pragma unroll 2
-    for (int e = a0 + warp; e < am; e += kWarps) {
-      const LT l = LU[__ldg(t.lk_pos + e)] * dk;
-      const uint16_t* ta = tg + (size_t)(e - a0) * nu;
-      #pragma unroll 2
-      for (int b = lane; b < nu; b += 32) LU[__ldg(ta + b)] -= l * LU[u0 + b];
+    const int q0 = c.htg[k], nq = c.htg[k + 1] - q0;
+    #pragma unroll 1
+    for (int e = tid + kThreads * kPre; e < nq; e += kThreads) {
+      const uint64_t r = __ldg(t.hrec + q0 + e);
+      const int tg = (int)(r & 0xFFFFu), lp = (int)((r >> 16) & 0xFFFFu);
+      const int up = (int)((r >> 32) & 0xFFFFu);
+      LU[tg] -= (LU[lp] * dk) * LU[up];
     }
-    // dense rows against the U entries in head columns; their multipliers
-    // into the exchange column
-    const uint16_t* tgb = tg + (size_t)(am - a0) * nu;
-    #pragma unroll 2
-    for (int e = am + warp; e < a1; e += kWarps) {
-      const LT l = LU[__ldg(t.lk_pos + e)] * dk;
-      const uint16_t* ta = tgb + (size_t)(e - am) * nuh;
-      #pragma unroll 2
-      for (int b = lane; b < nuh; b += 32) LU[__ldg(ta + b)] -= l * LU[u0 + b];
-      if (lane == 0) lb[__ldg(t.lk_row + e) - r0] = l;
+    // the dense rows' multipliers into the exchange column
+    const int e0 = c.hlk[k], ne = c.hlk[k + 1] - e0;
+    if (cl != 0xFFFFFFFFu && (int)(cl >> 16) >= r0) lb[(cl >> 16) - r0] = LU[cl & 0xFFFFu] * dk;
+    #pragma unroll 1
+    for (int e = tid + kThreads; e < ne; e += kThreads) {
+      const uint32_t w = __ldg(t.lk + e0 + e);
+      if ((int)(w >> 16) >= r0) lb[(w >> 16) - r0] = LU[w & 0xFFFFu] * dk;
     }
     // row k's U entries in dense columns into the exchange row
+    const int uh = c.ub[k], u1 = c.rowptr[k + 1];
     const uint16_t* cols = c.ndcol + c.ndoff[k] - c.rowptr[k];
     #pragma unroll 1
     for (int b = uh + tid; b < u1; b += kThreads) ubf[cols[b] - r0] = LU[b];
     bsync();
+    // column k's L entries scaled (nothing reads or writes them until the
+    // solves: the next pivots' updates lie right of column k)
+    if (cl != 0xFFFFFFFFu) LU[cl & 0xFFFFu] *= dk;
+    #pragma unroll 1
+    for (int e = tid + kThreads; e < ne; e += kThreads) LU[__ldg(t.lk + e0 + e) & 0xFFFFu] *= dk;
     LT lv[kTile], uv[kTile];
     #pragma unroll
     for (int s = 0; s < kTile; ++s) lv[s] = (p + 16 * s < m) ? lb[p + 16 * s] : (LT)0;
@@ -335,7 +362,6 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
     for (int s = 0; s < kTile; ++s)
     #pragma unroll
       for (int u = 0; u < kTile; ++u) a[s][u] -= lv[s] * uv[u];
-    dprev = dk;
   }
   // dense pivots: kk = 16 s0 + kq, held by the threads with q == kq
   // (column), p == kq (row) and both (pivot)
@@ -362,12 +388,6 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
           const int dj = q + 16 * u;
           if (dj > kk && dj < m) ubf[dj] = a[s0][u];
         }
-      }
-      if (kk == 0 && r0 > 0) {
-        // the last head column's L entries
-        const int e1 = c.hlk[r0];
-        #pragma unroll 1
-        for (int e = c.hlk[r0 - 1] + tid; e < e1; e += kThreads) LU[__ldg(t.lk_pos + e)] *= dprev;
       }
       bsync();
       const LT piv = lb[kk];

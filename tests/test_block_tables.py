@@ -21,7 +21,7 @@ import pytest
 
 FIELDS = ("bytes n n_rxn n_part n_jac n_lu n_coef r0 n_hf n_hb rx_word rx_vptr coef fg_ptr "
           "fg_ent jg_ptr jg_mid jg_w0 jg_w1 jg_row lu_src lu_perm lu_rowptr lu_col lu_diag "
-          "dpos ub lk_ptr lk_pos lk_row lk_mid tg_ptr tg hf_ptr hf_rows hb_ptr hb_rows "
+          "dpos ub lk_ptr lk lk_mid tg_ptr hrec hf_ptr hf_rows hb_ptr hb_rows "
           "dep_state atol stage sg_len sg_rowptr sg_diag sg_ub sg_perm sg_hf_ptr sg_hf_rows "
           "sg_hb_ptr sg_hb_rows sg_ndoff sg_ndcol sg_dbase sg_hlk sg_hmid sg_htg").split()
 MAX_DENSE = 112
@@ -44,11 +44,14 @@ def parse(blob: bytes) -> dict:
     t["dpos"] = arr("dpos", np.uint16, n - r0)
     t["ub"] = arr("ub", np.uint16, r0)
     t["lk_ptr"] = arr("lk_ptr", np.uint32, r0 + 1)
-    t["lk_pos"] = arr("lk_pos", np.uint16, int(t["lk_ptr"][-1]))
-    t["lk_row"] = arr("lk_row", np.uint16, int(t["lk_ptr"][-1]))
+    lk = arr("lk", np.uint32, int(t["lk_ptr"][-1]))
+    t["lk_pos"], t["lk_row"] = lk & 0xFFFF, lk >> 16
     t["lk_mid"] = arr("lk_mid", np.uint32, r0)
     t["tg_ptr"] = arr("tg_ptr", np.uint32, r0 + 1)
-    t["tg"] = arr("tg", np.uint16, int(t["tg_ptr"][-1]))
+    rec = np.frombuffer(blob, dtype=np.uint64, count=int(t["tg_ptr"][-1]), offset=o["hrec"])
+    t["rec_tg"] = (rec & 0xFFFF).astype(np.int64)
+    t["rec_l"] = ((rec >> 16) & 0xFFFF).astype(np.int64)
+    t["rec_u"] = ((rec >> 32) & 0xFFFF).astype(np.int64)
     t["hf_ptr"] = arr("hf_ptr", np.uint16, o["n_hf"] + 1)
     t["hf_rows"] = arr("hf_rows", np.uint16, int(t["hf_ptr"][-1]))
     t["hb_ptr"] = arr("hb_ptr", np.uint16, o["n_hb"] + 1)
@@ -85,29 +88,28 @@ def factor(t, LU):
     # the dense block, as the kernel's registers hold it
     A = np.array([[LU[dbase[i] + r0 + j] for j in range(m)] for i in range(m)])
     dinv = np.zeros(n)
-    dprev = 0.0
+    dense_pos = set()
+    for i in range(m):
+        dense_pos.update(range(dbase[i] + r0, dbase[i] + r0 + m))
     for k in range(r0):
         dk = 1.0 / LU[diag[k]]
         dinv[k] = dk
-        if k > 0:
-            LU[t["lk_pos"][t["lk_ptr"][k - 1]:t["lk_ptr"][k]]] *= dprev
         a0, am, a1 = sg["hlk"][k], sg["hmid"][k], sg["hlk"][k + 1]
         u0, uh, u1 = diag[k] + 1, ub[k], rowptr[k + 1]
         nu, nuh = u1 - u0, uh - u0
-        tg = t["tg"][sg["htg"][k]:sg["htg"][k + 1]]
-        assert len(tg) == (am - a0) * nu + (a1 - am) * nuh
+        q0, q1 = sg["htg"][k], sg["htg"][k + 1]
+        assert q1 - q0 == (am - a0) * nu + (a1 - am) * nuh
         assert all(t["lk_row"][a0:am] < r0) and all(t["lk_row"][am:a1] >= r0)
-        lh = LU[t["lk_pos"][a0:am]] * dk
-        ld = LU[t["lk_pos"][am:a1]] * dk
-        ta = tg[:(am - a0) * nu].reshape(am - a0, nu)
-        tb = tg[(am - a0) * nu:].reshape(a1 - am, nuh)
-        upd_a = np.outer(lh, LU[u0:u1])
-        upd_b = np.outer(ld, LU[u0:uh])
+        tg, lp, up = t["rec_tg"][q0:q1], t["rec_l"][q0:q1], t["rec_u"][q0:q1]
+        # the records' L entries are column k's, their U entries row k's
+        assert set(lp) <= set(t["lk_pos"][a0:a1]) and all((up >= u0) & (up < u1))
         # every target of one pivot is distinct, and none is in the dense block
-        both = np.concatenate([ta.ravel(), tb.ravel()])
-        assert len(np.unique(both)) == both.size
-        LU[ta.ravel()] -= upd_a.ravel()
-        LU[tb.ravel()] -= upd_b.ravel()
+        assert len(np.unique(tg)) == tg.size and not dense_pos & set(tg.tolist())
+        upd = (LU[lp] * dk) * LU[up]
+        ld = LU[t["lk_pos"][am:a1]] * dk
+        LU[tg] -= upd
+        # column k's L entries scaled after its updates
+        LU[t["lk_pos"][a0:a1]] *= dk
         # the exchange column and row into the dense block
         lcol = np.zeros(m)
         lcol[t["lk_row"][am:a1] - r0] = ld
@@ -116,11 +118,8 @@ def factor(t, LU):
         assert all(cols >= r0)
         urow[cols - r0] = LU[uh:u1]
         A -= np.outer(lcol, urow)
-        dprev = dk
     for kk in range(m):
         k = r0 + kk
-        if kk == 0 and r0 > 0:
-            LU[t["lk_pos"][t["lk_ptr"][r0 - 1]:t["lk_ptr"][r0]]] *= dprev
         dk = 1.0 / A[kk, kk]
         dinv[k] = dk
         A[kk + 1:, kk] *= dk
