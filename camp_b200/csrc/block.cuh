@@ -430,6 +430,26 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
   return !bad;
 }
 
+// sum of row[cc] * x[cc] over one panel's columns c0..c1-1 (at most 16):
+// four partial sums, so the loads and products overlap
+template <typename LT>
+__device__ __forceinline__ LT panel_dot(const LT* row, const LT* x, int c0, int c1) {
+  LT a0 = (LT)0, a1 = (LT)0, a2 = (LT)0, a3 = (LT)0;
+  if (c1 - c0 == 16) {
+    #pragma unroll
+    for (int cc = 0; cc < 16; cc += 4) {
+      a0 += row[c0 + cc] * x[c0 + cc];
+      a1 += row[c0 + cc + 1] * x[c0 + cc + 1];
+      a2 += row[c0 + cc + 2] * x[c0 + cc + 2];
+      a3 += row[c0 + cc + 3] * x[c0 + cc + 3];
+    }
+  } else {
+    #pragma unroll 1
+    for (int cc = c0; cc < c1; ++cc) a0 += row[cc] * x[cc];
+  }
+  return (a0 + a1) + (a2 + a3);
+}
+
 // rhs <- (LU)^{-1} rhs, through z in the LU's type
 template <typename LT>
 __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
@@ -482,12 +502,15 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
       const bool own = lane < w;
       LT zi = own ? z[r0 + d] : (LT)0;
       const LT* ri = LU + (own ? c.dbase[d] + r0 : 0);
-      #pragma unroll 1
-      for (int kk = 0; kk < w - 1; ++kk) {
-        const LT lk = ri[c0 + kk];
-        const LT zk = __shfl_sync(0xffffffffu, zi, kk);
-        const LT v = zi - lk * zk;
-        zi = lane > kk ? v : zi;
+      // unrolled: the row's entries load ahead of the shuffle chain
+      #pragma unroll
+      for (int kk = 0; kk < 15; ++kk) {
+        if (kk < w - 1) {
+          const LT lk = ri[c0 + kk];
+          const LT zk = __shfl_sync(0xffffffffu, zi, kk);
+          const LT v = zi - lk * zk;
+          zi = lane > kk ? v : zi;
+        }
       }
       if (own) z[r0 + d] = zi;
     }
@@ -496,10 +519,7 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
       #pragma unroll 1
       for (int d = c1 + tid; d < m; d += kThreads) {
         const LT* ri = LU + c.dbase[d] + r0;
-        LT acc = (LT)0;
-        #pragma unroll 4
-        for (int cc = c0; cc < c1; ++cc) acc += ri[cc] * z[r0 + cc];
-        z[r0 + d] -= acc;
+        z[r0 + d] -= panel_dot(ri, z + r0, c0, c1);
       }
       bsync();
     }
@@ -515,13 +535,15 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
       LT zi = own ? z[r0 + d] : (LT)0;
       const LT di = own ? c.dinv[r0 + d] : (LT)0;
       const LT* ri = LU + (own ? c.dbase[d] + r0 : 0);
-      #pragma unroll 1
-      for (int kk = w - 1; kk >= 0; --kk) {
-        const LT uk = ri[c0 + kk];
-        zi = lane == kk ? zi * di : zi;
-        const LT zk = __shfl_sync(0xffffffffu, zi, kk);
-        const LT v = zi - uk * zk;
-        zi = lane < kk ? v : zi;
+      #pragma unroll
+      for (int kk = 15; kk >= 0; --kk) {
+        if (kk < w) {
+          const LT uk = ri[c0 + kk];
+          zi = lane == kk ? zi * di : zi;
+          const LT zk = __shfl_sync(0xffffffffu, zi, kk);
+          const LT v = zi - uk * zk;
+          zi = lane < kk ? v : zi;
+        }
       }
       if (own) z[r0 + d] = zi;
     }
@@ -530,10 +552,7 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
       #pragma unroll 1
       for (int d = tid; d < c0; d += kThreads) {
         const LT* ri = LU + c.dbase[d] + r0;
-        LT acc = (LT)0;
-        #pragma unroll 4
-        for (int cc = c0; cc < c1; ++cc) acc += ri[cc] * z[r0 + cc];
-        z[r0 + d] -= acc;
+        z[r0 + d] -= panel_dot(ri, z + r0, c0, c1);
       }
       bsync();
     }
