@@ -380,7 +380,13 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
           const int di = p + 16 * s;
           if (di > kk && di < m) lb[di] = a[s][s0];
         }
-        if (p == kq) lb[kk] = a[s0][s0];
+        if (p == kq) {
+          // the pivot's owner publishes its reciprocal (0 for a zero or
+          // non-finite pivot), so no other thread divides
+          const LT pv = a[s0][s0];
+          const bool pbad = (pv == (LT)0) || !isfinite((double)pv);
+          lb[kk] = pbad ? (LT)0 : (LT)(1.0 / (double)pv);
+        }
       }
       if (p == kq) {
         #pragma unroll
@@ -390,10 +396,8 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
         }
       }
       bsync();
-      const LT piv = lb[kk];
-      const bool pb = (piv == (LT)0) || !isfinite((double)piv);
-      bad |= pb;
-      const LT dk = pb ? (LT)0 : (LT)(1.0 / (double)piv);
+      const LT dk = lb[kk];
+      bad |= dk == (LT)0;
       if (tid == 0) c.dinv[k] = dk;
       LT lv[kTile], uv[kTile];
       #pragma unroll
@@ -413,10 +417,16 @@ __device__ __noinline__ bool op_factor(const Ctx<LT>& c, double gamma) {
         const bool sc = q == kq && p + 16 * s > kk;
         a[s][s0] = sc ? a[s][s0] * dk : a[s][s0];
       }
+      // tile rows / columns wholly at or before the pivot are finished:
+      // the branch is the same for the whole block
       #pragma unroll
-      for (int s = 0; s < kTile; ++s)
-      #pragma unroll
-        for (int u = 0; u < kTile; ++u) a[s][u] -= lv[s] * uv[u];
+      for (int s = 0; s < kTile; ++s) {
+        if (16 * s + 15 > kk) {
+          #pragma unroll
+          for (int u = 0; u < kTile; ++u)
+            if (16 * u + 15 > kk) a[s][u] -= lv[s] * uv[u];
+        }
+      }
     }
   }
   #pragma unroll
@@ -479,7 +489,7 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
   }
   if (r0 > 0) {
     // forward: the head columns of the dense rows, one row per warp
-    #pragma unroll 1
+    #pragma unroll 2
     for (int i = r0 + warp; i < n; i += kWarps) {
       const int q0 = c.rowptr[i], e0 = c.ndoff[i], ne = c.ndoff[i + 1] - e0;
       LT v = (LT)0;
@@ -559,7 +569,7 @@ __device__ __noinline__ void op_solve(const Ctx<LT>& c) {
   }
   if (r0 > 0) {
     // backward: the dense columns of the head rows, one row per warp
-    #pragma unroll 1
+    #pragma unroll 2
     for (int i = warp; i < r0; i += kWarps) {
       const int q0 = c.rowptr[i], e0 = c.ndoff[i] - q0;
       const int q1 = c.rowptr[i + 1];
