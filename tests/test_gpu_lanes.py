@@ -141,3 +141,22 @@ def test_large_mechanism_warp_entry_points_refuse(large):
     s.set_photo_rates(cells.photo_rates)
     with pytest.raises(SolverError, match="warp-per-cell"):
         s.eval_deriv(cells.state, cells.env, 1.0)
+
+
+def test_large_mechanism_autotune_keeps_block_kernel(large):
+    """On a mechanism beyond the warp tables the autotuner times the
+    block-per-cell kernel (the lane kernel only where no other has tables)
+    and the tuned solver still solves."""
+    from camp_b200.cells import make_cells
+    from camp_b200.solver import Solver
+
+    mech, base = large
+    cells = make_cells(mech, 64, 33, conc_lo=1e-8, photo_base=base)
+    s = Solver(mech, 64)
+    s.initialize(abs_tol=np.full(mech.n_state_var, 1e-8), rel_tol=1e-4)
+    s.set_photo_rates(cells.photo_rates)
+    tuned = s.autotune(cells.state, cells.env, 0.0, T_LARGE)
+    assert tuned["kernel"] == 2 and tuned["sample_ms"] > 0
+    x = cells.state.copy()
+    s.solve(x, cells.env, 0.0, T_LARGE)
+    assert np.mean(s.cell_stats()["status"] == 0) >= 0.9
