@@ -185,3 +185,20 @@ def test_variable_water_is_refused(tmp_path, case, lib):
     s.build_sparsity_only()
     assert not s.ready
     assert "constant" in _lib.last_error()
+
+
+def test_kernel_setting(cb05, lib):
+    """camp_b200_set_kernel takes the three kernel forms (0 warp, 1 lane,
+    2 block per cell) and refuses anything else; before solver_initialize
+    camp_b200_get_kernel reports the setting."""
+    from camp_b200.solver import Solver, SolverError
+
+    s = Solver(cb05, 4)
+    s.build_sparsity_only()
+    for k in (2, 1, 0):
+        s.set_kernel(k)
+        if not s.ready:
+            assert s.kernel() == k
+    for bad in (-1, 3):
+        with pytest.raises(SolverError, match="kernel must be 0, 1 or 2"):
+            s.set_kernel(bad)
