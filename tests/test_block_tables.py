@@ -292,3 +292,21 @@ def test_aerosol_mechanism_has_no_block_tables(mod37_aero):
     s.build_sparsity_only()
     with pytest.raises(SolverError, match="CTA-per-cell"):
         s.block_tables()
+
+
+def test_dense_block_beyond_registers_is_refused():
+    """A larger random mechanism (250 species, 800 reactions) fills to a
+    dense trailing block of more than 112 rows, beyond the 16 x 16 threads x
+    7 x 7 entries the factorization holds in registers: the tables refuse it
+    with the reason, and such a mechanism runs on the lane-per-cell kernel."""
+    import tempfile
+
+    from camp_b200.solver import Solver, SolverError
+    from camp_b200.synth import load_synthetic
+
+    with tempfile.TemporaryDirectory() as td:
+        mech, _ = load_synthetic(td, 250, 800)
+    s = Solver(mech, 4)
+    s.build_sparsity_only()
+    with pytest.raises(SolverError, match=r"trailing dense block \(\d+ rows\) exceeds"):
+        s.block_tables()
